@@ -1,0 +1,189 @@
+/*
+ * pkdecon.h -- C ABI of libpkdecon.so, a B200 (sm_100a) implementation of PetaKit5D's
+ * Richardson-Lucy deconvolution hot path.
+ *
+ * Conventions shared by every entry point (they are MATLAB's, so a MEX gateway passes its arrays
+ * straight through):
+ *   - volumes are column-major [ny nx nz] (y fastest), dims[] = {ny, nx, nz} = size(I) in MATLAB;
+ *   - PSFs are float32 column-major with their own dims[];
+ *   - bounding boxes are 1-based inclusive [y1 x1 z1 y2 x2 z2] (crop3d_mex.c:54-59 convention);
+ *   - every call returns a pk_status; on failure pk_last_error() gives a message (thread-local);
+ *   - the caller owns host buffers; the library owns device memory, streams and caches in pk_ctx;
+ *   - calls on one pk_ctx are serialised by the library.
+ */
+#ifndef PKDECON_H
+#define PKDECON_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define PK_API __attribute__((visibility("default")))
+#else
+#define PK_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    PK_OK = 0,
+    PK_ERR_INVALID = 1,      /* bad argument (MATLAB error(...) in the reference) */
+    PK_ERR_UNSUPPORTED = 2,  /* size / option this build does not handle */
+    PK_ERR_CUDA = 3,         /* CUDA runtime error */
+    PK_ERR_NOMEM = 4,        /* device allocation failed or over the memory budget */
+    PK_ERR_BUSY = 5,         /* server queue full */
+    PK_ERR_TIMEOUT = 6,      /* bounded wait expired */
+    PK_ERR_CANCELLED = 7,    /* request cancelled */
+    PK_ERR_EMPTY_OTF_MASK = 8 /* omw_backprojector_generation.m:50-52 */
+} pk_status;
+
+typedef enum { PK_U16 = 0, PK_F32 = 1, PK_F64 = 2 } pk_dtype;
+
+typedef struct pk_ctx pk_ctx;
+
+/* Name/value parameters of decon_lucy_function.m:21-36 and decon_lucy_omw_function.m:12-30. */
+typedef struct {
+    double background;     /* Background ([] -> 0) */
+    double damp_factor;    /* dampFactor, default 1 */
+    double scale_factor;   /* scaleFactor, default 1 */
+    double decon_offset;   /* deconOffset, default 0 */
+    int32_t edge_erosion;  /* EdgeErosion, default 0 */
+    int32_t save16bit;     /* save16bit, default 1: output uint16, else float32 */
+    int32_t has_bbox;      /* bbox given (non-empty) */
+    int64_t bbox[6];       /* 1-based inclusive [y1 x1 z1 y2 x2 z2] */
+} pk_decon_params;
+
+/* Fill *p with the reference defaults. */
+PK_API void pk_params_default(pk_decon_params* p);
+
+/* ---------------------------------------------------------------- context */
+/* Replaces the per-function `persistent` OTF caches of decon_lucy_function.m:61-77 and
+ * decon_lucy_omw_function.m:53-73 with an explicit context bound to one device. */
+PK_API pk_ctx* pk_ctx_create(int device);
+PK_API void pk_ctx_destroy(pk_ctx* ctx);
+/* Drop cached OTFs and work buffers (the demo's reset(gpuDevice), demo_RL_deconvolution.m:164-167). */
+PK_API pk_status pk_ctx_reset(pk_ctx* ctx);
+PK_API const char* pk_last_error(void);
+PK_API const char* pk_version(void);
+
+/* Output extent for dims/params: the bbox size when has_bbox, else dims. */
+PK_API pk_status pk_output_dims(const int64_t dims[3], const pk_decon_params* p, int64_t out_dims[3]);
+
+/* ---------------------------------------------------------------- the drop-in calls (host buffers) */
+/* [J_2, ~, k] = decon_lucy_function(I, PSF, NUMIT, ...)  -- decon_lucy_function.m:1-213.
+ * in: host volume of type in_type; out: host buffer of pk_output_dims() voxels, uint16 when
+ * params->save16bit else float32.  *iters_run (may be NULL) receives k. */
+PK_API pk_status pk_decon_lucy(pk_ctx* ctx, const void* in, pk_dtype in_type, const int64_t dims[3],
+                        const float* psf, const int64_t psf_dims[3], int32_t numit,
+                        const pk_decon_params* params, void* out, int32_t* iters_run);
+
+/* J = decon_lucy_omw_function(I, PSF_f, PSF_b, NUMIT, ...)  -- decon_lucy_omw_function.m:1-177. */
+PK_API pk_status pk_decon_lucy_omw(pk_ctx* ctx, const void* in, pk_dtype in_type, const int64_t dims[3],
+                            const float* psf_f, const int64_t psf_f_dims[3],
+                            const float* psf_b, const int64_t psf_b_dims[3], int32_t numit,
+                            const pk_decon_params* params, void* out);
+
+/* Device-pointer forms of the two calls (the gateway's mxGPUArray path): `in`/`out` are device
+ * pointers, the work is queued on `stream` (a cudaStream_t, NULL = the context's stream) and the
+ * call returns without synchronising. */
+PK_API pk_status pk_decon_lucy_device(pk_ctx* ctx, const void* d_in, pk_dtype in_type, const int64_t dims[3],
+                               const float* psf, const int64_t psf_dims[3], int32_t numit,
+                               const pk_decon_params* params, void* d_out, void* stream);
+PK_API pk_status pk_decon_lucy_omw_device(pk_ctx* ctx, const void* d_in, pk_dtype in_type, const int64_t dims[3],
+                                   const float* psf_f, const int64_t psf_f_dims[3],
+                                   const float* psf_b, const int64_t psf_b_dims[3], int32_t numit,
+                                   const pk_decon_params* params, void* d_out, void* stream);
+
+/* ---------------------------------------------------------------- OTF / FFT building blocks */
+/* decon_psf2otf(PSF./sum(PSF), dims) (decon_psf2otf.m:1-46), returned as the half spectrum:
+ * complex64 (interleaved re,im), column-major [floor(ny/2)+1, nx, nz]. */
+PK_API pk_status pk_psf2otf(pk_ctx* ctx, const float* psf, const int64_t psf_dims[3], const int64_t dims[3],
+                     float* otf_half);
+
+/* Forward 3D R2C / inverse unnormalised C2R of device float32 volumes (half-spectrum layout as
+ * above).  Used by tests of the transform itself. */
+PK_API pk_status pk_fft3_r2c_device(pk_ctx* ctx, const float* d_in, const int64_t dims[3], float* d_spec, void* stream);
+PK_API pk_status pk_fft3_c2r_device(pk_ctx* ctx, const float* d_spec, const int64_t dims[3], float* d_out, void* stream);
+
+/* ---------------------------------------------------------------- backprojectors */
+/* [b_omw, OTF_bp_omw, abs_OTF_c, OTF_mask] = omw_backprojector_generation(psf, alpha, skewed, ...)
+ * (omw_backprojector_generation.m:1-166).  skewed: -1 = [] (auto-detect), 0 = false, 1 = true.
+ * b_omw: float32 of psf_dims.  Optional outputs (NULL to skip): otf_bp_omw complex64 interleaved,
+ * abs_otf_c float32, otf_mask uint8; all of psf_dims (mask z-extent folded back when skewed). */
+PK_API pk_status pk_omw_backprojector(pk_ctx* ctx, const float* psf, const int64_t psf_dims[3], double alpha,
+                               int32_t skewed, double otf_cum_thresh, double otf_area_thresh,
+                               double hann_lo, double hann_hi, double min_int_thresh,
+                               float* b_omw, float* otf_bp_omw, float* abs_otf_c, uint8_t* otf_mask);
+
+/* [PSF_bp, OTF_bp] = BackProjector(PSF_fp, 'wiener-butterworth', alpha, beta, n, resFlag, iRes)
+ * (third_parties/WBDeconvolution/BackProjector.m:67-233).  psf_bp: float64 of psf_dims;
+ * otf_bp (NULL to skip): complex128 interleaved. */
+PK_API pk_status pk_wb_backprojector(pk_ctx* ctx, const float* psf, const int64_t psf_dims[3], double alpha,
+                              double beta, int32_t n, int32_t res_flag, const double ires[3],
+                              double* psf_bp, double* otf_bp);
+
+/* ---------------------------------------------------------------- chunking helpers (host) */
+/* findGoodFactorNumber(n, direction, allowOddSeven)  -- utils/findGoodFactorNumber.m:1-26. */
+PK_API int64_t pk_find_good_factor_number(int64_t n, int32_t direction, int32_t allow_odd_seven);
+
+/* XR_zarrChunkCoordinatesExtraction(volSize, ...) -- stitch/XR_zarrChunkCoordinatesExtraction.m:1-83.
+ * Returns the number of chunks; when the three output arrays are non-NULL they receive n*6 int64
+ * (1-based inclusive boxes, chunks in y-fastest order). bbox may be NULL. */
+PK_API int64_t pk_chunk_coordinates(const int64_t vol_size[3], const int64_t batch_size[3],
+                             const int64_t block_size[3], const int64_t* bbox, int32_t same_batch_size,
+                             const int64_t border[3], int64_t* batch_bboxes, int64_t* region_bboxes,
+                             int64_t* local_bboxes);
+
+/* ---------------------------------------------------------------- batched chunks */
+/* One chunk of a batched call: a column-major uint16/float volume with its own PSF pair (psf_b
+ * NULL for traditional RL) and its output crop (deconBbox, RLdecon_for_zarr_block.m:146-158). */
+typedef struct {
+    const void* in;            /* host or device volume (see pk_batch_decon's `device`) */
+    int64_t dims[3];
+    int32_t psf_id;            /* index into the psf arrays passed to pk_batch_decon */
+    int32_t has_bbox;
+    int64_t bbox[6];
+    void* out;                 /* output buffer (pk_output_dims voxels) */
+} pk_chunk;
+
+/* Deconvolve n chunks with OMW (method 1) or Biggs RL (method 0), numit iterations.
+ * psf_f[i]/psf_b[i] with dims psf_dims[i] are the PSF pairs referenced by chunk psf_id.
+ * pad_good: 1 = pad each chunk (zeros after background removal, at the high end of each axis) to
+ * findGoodFactorNumber sizes so chunks share transform sizes; 0 = exact sizes (reference math).
+ * device: 1 when chunk in/out are device pointers. */
+PK_API pk_status pk_batch_decon(pk_ctx* ctx, int32_t method, int32_t n, const pk_chunk* chunks, pk_dtype in_type,
+                         int32_t npsf, const float* const* psf_f, const float* const* psf_b,
+                         const int64_t* psf_dims, int32_t numit, const pk_decon_params* params,
+                         int32_t pad_good, int32_t device);
+
+/* ---------------------------------------------------------------- serving */
+typedef struct pk_server pk_server;
+
+typedef struct {
+    int64_t budget_bytes;      /* HBM admission budget for in-flight work buffers */
+    int32_t max_batch;         /* max requests advanced together */
+    int32_t queue_capacity;    /* max queued (not yet admitted) requests */
+} pk_server_config;
+
+/* Register a PSF pair (psf_b NULL for RL-only) under psf_id; OTFs are cached per (psf_id, size). */
+PK_API pk_server* pk_server_create(pk_ctx* ctx, const pk_server_config* cfg);
+PK_API pk_status pk_server_add_psf(pk_server* s, int32_t psf_id, const float* psf_f, const float* psf_b,
+                            const int64_t psf_dims[3]);
+/* Submit a request: host uint16 volume (copied at submit), method 1 = OMW, 0 = RL.
+ * Returns a request id (>= 0) or -pk_status. */
+PK_API int64_t pk_server_submit(pk_server* s, const uint16_t* vol, const int64_t dims[3], int32_t psf_id,
+                         int32_t method, int32_t numit, const pk_decon_params* params);
+/* Wait up to timeout_ms for request id; on PK_OK the result is copied to out (pk_output_dims voxels)
+ * and *latency_ms receives submit-to-done time. */
+PK_API pk_status pk_server_wait(pk_server* s, int64_t id, void* out, int32_t timeout_ms, double* latency_ms);
+PK_API pk_status pk_server_cancel(pk_server* s, int64_t id);
+/* stats[0..3] = completed, rejected, peak in-flight bytes, rounds run. */
+PK_API pk_status pk_server_stats(pk_server* s, int64_t stats[4]);
+PK_API void pk_server_destroy(pk_server* s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PKDECON_H */

@@ -1,0 +1,10 @@
+"""petakit5d_b200: B200 (sm_100a) Richardson-Lucy / OMW deconvolution behind a MATLAB-style C ABI.
+
+Modules:
+  decon          -- decon_lucy_function / decon_lucy_omw_function drop-ins (and device-pointer forms)
+  backprojector  -- omw_backprojector_generation / BackProjector('wiener-butterworth')
+  chunking       -- findGoodFactorNumber, XR_zarrChunkCoordinatesExtraction, batched chunk decon
+  serve          -- device-resident serving loop with continuous batching
+  synth          -- seeded synthetic volumes and PSFs
+"""
+__version__ = "0.1.0"

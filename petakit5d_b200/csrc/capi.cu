@@ -1,0 +1,359 @@
+// extern "C" entry points of libpkdecon.so (declared in include/pkdecon.h).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "pk_internal.h"
+
+static thread_local std::string g_err;
+
+void pk_set_error(const std::string& msg) { g_err = msg; }
+pk_status pk_fail(pk_status st, const std::string& msg) {
+    g_err = msg;
+    return st;
+}
+
+pk_status pk_make_otf(pk_ctx* ctx, const float* h_psf, const int64_t pd[3], int ny, int nx, int nz, double scale,
+                      float2* d_otf, cudaStream_t st);
+
+namespace {
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+size_t dtype_size(pk_dtype t) { return t == PK_U16 ? 2 : t == PK_F32 ? 4 : 8; }
+
+pk_status check_ctx(pk_ctx* ctx) {
+    if (!ctx) return pk_fail(PK_ERR_INVALID, "null pk_ctx");
+    return PK_OK;
+}
+
+pk_status check_dims(const int64_t d[3], const char* what) {
+    if (!d) return pk_fail(PK_ERR_INVALID, std::string(what) + " dims must not be NULL");
+    for (int i = 0; i < 3; i++)
+        if (d[i] < 1) return pk_fail(PK_ERR_INVALID, std::string(what) + " is empty");
+    return PK_OK;
+}
+
+pk_status check_psf(const float* psf, const int64_t d[3], const char* what) {
+    pk_status s = check_dims(d, what);
+    if (s != PK_OK) return s;
+    if (!psf) return pk_fail(PK_ERR_INVALID, std::string(what) + " must not be NULL");
+    return PK_OK;
+}
+
+cudaStream_t pick_stream(pk_ctx* ctx, void* stream) { return stream ? (cudaStream_t)stream : ctx->stream; }
+
+}  // namespace
+
+extern "C" {
+
+void pk_params_default(pk_decon_params* p) {
+    if (!p) return;
+    memset(p, 0, sizeof(*p));
+    p->background = 0.0;
+    p->damp_factor = 1.0;
+    p->scale_factor = 1.0;
+    p->decon_offset = 0.0;
+    p->edge_erosion = 0;
+    p->save16bit = 1;
+    p->has_bbox = 0;
+}
+
+const char* pk_last_error(void) { return g_err.c_str(); }
+const char* pk_version(void) { return "pkdecon 0.1 (sm_100a)"; }
+
+pk_ctx* pk_ctx_create(int device) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) {
+        cudaGetLastError();
+        pk_set_error("no CUDA device " + std::to_string(device));
+        return nullptr;
+    }
+    DeviceGuard g(device);
+    pk_ctx* ctx = new pk_ctx();
+    ctx->device = device;
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        pk_set_error("cudaStreamCreate failed");
+        delete ctx;
+        return nullptr;
+    }
+    return ctx;
+}
+
+static void release_all(pk_ctx* ctx) {
+    cudaStreamSynchronize(ctx->stream);
+    for (auto& kv : ctx->otf) cudaFree(kv.second.d);
+    ctx->otf.clear();
+    for (auto& s : ctx->scratch)
+        if (s.first) cudaFree(s.first);
+    ctx->scratch.clear();
+    if (ctx->prog_buf) cudaFree(ctx->prog_buf);
+    ctx->prog_buf = nullptr;
+    ctx->prog_cap = 0;
+    if (ctx->d_counter) cudaFree(ctx->d_counter);
+    ctx->d_counter = nullptr;
+}
+
+void pk_ctx_destroy(pk_ctx* ctx) {
+    if (!ctx) return;
+    {
+        std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+        DeviceGuard g(ctx->device);
+        release_all(ctx);
+        for (auto& kv : ctx->tw) cudaFree(kv.second.d);
+        ctx->tw.clear();
+        for (void* p : ctx->host_pinned) cudaFreeHost(p);
+        ctx->host_pinned.clear();
+        cudaStreamDestroy(ctx->stream);
+    }
+    delete ctx;
+}
+
+pk_status pk_ctx_reset(pk_ctx* ctx) {
+    pk_status s = check_ctx(ctx);
+    if (s != PK_OK) return s;
+    std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+    DeviceGuard g(ctx->device);
+    release_all(ctx);
+    return PK_OK;
+}
+
+pk_status pk_output_dims(const int64_t dims[3], const pk_decon_params* p, int64_t out[3]) {
+    if (!dims || !out) return pk_fail(PK_ERR_INVALID, "NULL dims");
+    for (int i = 0; i < 3; i++) out[i] = dims[i];
+    if (p && p->has_bbox)
+        for (int i = 0; i < 3; i++) out[i] = p->bbox[i + 3] - p->bbox[i] + 1;
+    return PK_OK;
+}
+
+static pk_status decon_device(pk_ctx* ctx, int method, const void* d_in, pk_dtype in_type, const int64_t dims[3],
+                              const float* psf_f, const int64_t psf_f_dims[3], const float* psf_b,
+                              const int64_t psf_b_dims[3], int32_t numit, const pk_decon_params* params,
+                              void* d_out, cudaStream_t st) {
+    pk_status s;
+    if ((s = check_ctx(ctx)) != PK_OK) return s;
+    if ((s = check_dims(dims, "input volume")) != PK_OK) return s;
+    if ((s = check_psf(psf_f, psf_f_dims, "PSF")) != PK_OK) return s;
+    if (method == 1 && (s = check_psf(psf_b, psf_b_dims, "PSF_b")) != PK_OK) return s;
+    if (!d_in || !d_out) return pk_fail(PK_ERR_INVALID, "NULL input/output buffer");
+    if (in_type != PK_U16 && in_type != PK_F32 && in_type != PK_F64) return pk_fail(PK_ERR_INVALID, "bad input dtype");
+    pk_decon_params def;
+    if (!params) {
+        pk_params_default(&def);
+        params = &def;
+    }
+    std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+    DeviceGuard g(ctx->device);
+    return pk_decon_run(ctx, method, d_in, in_type, dims, psf_f, psf_f_dims, psf_b, psf_b_dims, numit, params,
+                        d_out, st);
+}
+
+static pk_status decon_host(pk_ctx* ctx, int method, const void* in, pk_dtype in_type, const int64_t dims[3],
+                            const float* psf_f, const int64_t psf_f_dims[3], const float* psf_b,
+                            const int64_t psf_b_dims[3], int32_t numit, const pk_decon_params* params, void* out) {
+    pk_status s;
+    if ((s = check_ctx(ctx)) != PK_OK) return s;
+    if ((s = check_dims(dims, "input volume")) != PK_OK) return s;
+    if (!in || !out) return pk_fail(PK_ERR_INVALID, "NULL input/output buffer");
+    if (in_type != PK_U16 && in_type != PK_F32 && in_type != PK_F64) return pk_fail(PK_ERR_INVALID, "bad input dtype");
+    pk_decon_params def;
+    if (!params) {
+        pk_params_default(&def);
+        params = &def;
+    }
+    std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+    DeviceGuard g(ctx->device);
+    const size_t N = (size_t)dims[0] * dims[1] * dims[2];
+    int64_t od[3];
+    pk_output_dims(dims, params, od);
+    const size_t outb = (size_t)od[0] * od[1] * od[2] * (params->save16bit ? 2 : 4);
+    void *d_in, *d_out;
+    if ((s = pk_scratch(ctx, 9, N * dtype_size(in_type), &d_in)) != PK_OK) return s;
+    if ((s = pk_scratch(ctx, 10, outb, &d_out)) != PK_OK) return s;
+    cudaStream_t st = ctx->stream;
+    PK_CUDA(cudaMemcpyAsync(d_in, in, N * dtype_size(in_type), cudaMemcpyHostToDevice, st));
+    s = decon_device(ctx, method, d_in, in_type, dims, psf_f, psf_f_dims, psf_b, psf_b_dims, numit, params, d_out, st);
+    if (s != PK_OK) {
+        cudaStreamSynchronize(st);
+        return s;
+    }
+    PK_CUDA(cudaMemcpyAsync(out, d_out, outb, cudaMemcpyDeviceToHost, st));
+    PK_CUDA(cudaStreamSynchronize(st));
+    return PK_OK;
+}
+
+pk_status pk_decon_lucy(pk_ctx* ctx, const void* in, pk_dtype in_type, const int64_t dims[3], const float* psf,
+                        const int64_t psf_dims[3], int32_t numit, const pk_decon_params* params, void* out,
+                        int32_t* iters_run) {
+    pk_status s = decon_host(ctx, 0, in, in_type, dims, psf, psf_dims, nullptr, nullptr, numit, params, out);
+    if (s == PK_OK && iters_run) *iters_run = numit;
+    return s;
+}
+
+pk_status pk_decon_lucy_omw(pk_ctx* ctx, const void* in, pk_dtype in_type, const int64_t dims[3],
+                            const float* psf_f, const int64_t psf_f_dims[3], const float* psf_b,
+                            const int64_t psf_b_dims[3], int32_t numit, const pk_decon_params* params, void* out) {
+    return decon_host(ctx, 1, in, in_type, dims, psf_f, psf_f_dims, psf_b, psf_b_dims, numit, params, out);
+}
+
+pk_status pk_decon_lucy_device(pk_ctx* ctx, const void* d_in, pk_dtype in_type, const int64_t dims[3],
+                               const float* psf, const int64_t psf_dims[3], int32_t numit,
+                               const pk_decon_params* params, void* d_out, void* stream) {
+    if (!ctx) return pk_fail(PK_ERR_INVALID, "null pk_ctx");
+    return decon_device(ctx, 0, d_in, in_type, dims, psf, psf_dims, nullptr, nullptr, numit, params, d_out,
+                        pick_stream(ctx, stream));
+}
+
+pk_status pk_decon_lucy_omw_device(pk_ctx* ctx, const void* d_in, pk_dtype in_type, const int64_t dims[3],
+                                   const float* psf_f, const int64_t psf_f_dims[3], const float* psf_b,
+                                   const int64_t psf_b_dims[3], int32_t numit, const pk_decon_params* params,
+                                   void* d_out, void* stream) {
+    if (!ctx) return pk_fail(PK_ERR_INVALID, "null pk_ctx");
+    return decon_device(ctx, 1, d_in, in_type, dims, psf_f, psf_f_dims, psf_b, psf_b_dims, numit, params, d_out,
+                        pick_stream(ctx, stream));
+}
+
+pk_status pk_psf2otf(pk_ctx* ctx, const float* psf, const int64_t psf_dims[3], const int64_t dims[3],
+                     float* otf_half) {
+    pk_status s;
+    if ((s = check_ctx(ctx)) != PK_OK) return s;
+    if ((s = check_psf(psf, psf_dims, "PSF")) != PK_OK) return s;
+    if ((s = check_dims(dims, "output size")) != PK_OK) return s;
+    if (!otf_half) return pk_fail(PK_ERR_INVALID, "NULL output");
+    std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+    DeviceGuard g(ctx->device);
+    const int ny = (int)dims[0], nx = (int)dims[1], nz = (int)dims[2];
+    const size_t nb = sizeof(float2) * (size_t)(ny / 2 + 1) * nx * nz;
+    void* d;
+    if ((s = pk_scratch(ctx, 10, nb, &d)) != PK_OK) return s;
+    if ((s = pk_make_otf(ctx, psf, psf_dims, ny, nx, nz, 1.0, (float2*)d, ctx->stream)) != PK_OK) return s;
+    PK_CUDA(cudaMemcpyAsync(otf_half, d, nb, cudaMemcpyDeviceToHost, ctx->stream));
+    PK_CUDA(cudaStreamSynchronize(ctx->stream));
+    return PK_OK;
+}
+
+static pk_status fft3(pk_ctx* ctx, int inverse, const float* d_a, const int64_t dims[3], float* d_b, void* stream) {
+    pk_status s;
+    if ((s = check_ctx(ctx)) != PK_OK) return s;
+    if ((s = check_dims(dims, "volume")) != PK_OK) return s;
+    if (!d_a || !d_b) return pk_fail(PK_ERR_INVALID, "NULL buffer");
+    std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+    DeviceGuard g(ctx->device);
+    VolDesc d;
+    if ((s = pk_init_desc(ctx, (int)dims[0], (int)dims[1], (int)dims[2], &d)) != PK_OK) return s;
+    cudaStream_t st = pick_stream(ctx, stream);
+    PkProgram prog;
+    if (!inverse) {
+        d.src = d_a;
+        d.S = (float2*)d_b;
+        pk_program_add(prog, PK_STEP_Y, Y_R2C, {d});
+        pk_program_add(prog, PK_STEP_X, XZ_FWD, {d});
+        pk_program_add(prog, PK_STEP_Z, XZ_FWD, {d});
+    } else {
+        // the inverse runs in place on a work copy of the spectrum
+        void* w;
+        const size_t nb = sizeof(float2) * pk_spec_elems(d);
+        if ((s = pk_scratch(ctx, 5, nb, &w)) != PK_OK) return s;
+        PK_CUDA(cudaMemcpyAsync(w, d_a, nb, cudaMemcpyDeviceToDevice, st));
+        d.S = (float2*)w;
+        d.dst = d_b;
+        pk_program_add(prog, PK_STEP_Z, XZ_INV, {d});
+        pk_program_add(prog, PK_STEP_X, XZ_INV, {d});
+        pk_program_add(prog, PK_STEP_Y, Y_C2R, {d});
+    }
+    if ((s = pk_program_upload(ctx, prog, st)) != PK_OK) return s;
+    return pk_program_launch(prog, st);
+}
+
+pk_status pk_fft3_r2c_device(pk_ctx* ctx, const float* d_in, const int64_t dims[3], float* d_spec, void* stream) {
+    return fft3(ctx, 0, d_in, dims, d_spec, stream);
+}
+
+pk_status pk_fft3_c2r_device(pk_ctx* ctx, const float* d_spec, const int64_t dims[3], float* d_out, void* stream) {
+    return fft3(ctx, 1, d_spec, dims, d_out, stream);
+}
+
+// ------------------------------------------------------------------ chunking helpers
+static void factorize(int64_t n, std::vector<int64_t>& f) {
+    f.clear();
+    for (int64_t p = 2; p * p <= n; p++)
+        while (n % p == 0) {
+            f.push_back(p);
+            n /= p;
+        }
+    if (n > 1 || f.empty()) f.push_back(n);
+}
+
+int64_t pk_find_good_factor_number(int64_t n, int32_t direction, int32_t allow_odd_seven) {
+    if (n < 1) return n;
+    if (direction == 0) direction = 1;
+    std::vector<int64_t> f;
+    int64_t g = n;
+    factorize(g, f);
+    while (f.back() > 7 || (!allow_odd_seven && f.front() > 2 && f.back() == 7)) {
+        g += direction;
+        if (g < 1) return -1;
+        factorize(g, f);
+    }
+    return g;
+}
+
+int64_t pk_chunk_coordinates(const int64_t vol[3], const int64_t batch_size[3], const int64_t block_size[3],
+                             const int64_t* bbox, int32_t same_batch_size, const int64_t border[3],
+                             int64_t* batch_bb, int64_t* region_bb, int64_t* local_bb) {
+    if (!vol || !batch_size || !block_size || !border) return -1;
+    int64_t ws[3], we[3], wsz[3], bs[3], blk[3], nsub[3];
+    for (int i = 0; i < 3; i++) {
+        ws[i] = bbox ? bbox[i] : 1;
+        we[i] = bbox ? bbox[i + 3] : vol[i];
+        wsz[i] = we[i] - ws[i] + 1;
+        if (wsz[i] < 1 || batch_size[i] < 1 || block_size[i] < 1) return -1;
+        bs[i] = std::min(wsz[i], batch_size[i]);
+        blk[i] = std::min(wsz[i], block_size[i]);
+        bs[i] = (bs[i] + blk[i] - 1) / blk[i] * blk[i];
+        nsub[i] = (wsz[i] + bs[i] - 1) / bs[i];
+    }
+    const int64_t n = nsub[0] * nsub[1] * nsub[2];
+    if (!batch_bb || !region_bb || !local_bb) return n;
+    int64_t c = 0;
+    for (int64_t z = 0; z < nsub[2]; z++)
+        for (int64_t x = 0; x < nsub[1]; x++)
+            for (int64_t y = 0; y < nsub[0]; y++, c++) {
+                const int64_t sub[3] = {y, x, z};
+                int64_t r[6], b[6], l[6];
+                for (int i = 0; i < 3; i++) {
+                    r[i] = sub[i] * bs[i] + ws[i];
+                    r[i + 3] = std::min(r[i] + bs[i] - 1, we[i]);
+                    b[i] = r[i];
+                    b[i + 3] = r[i + 3];
+                    if (same_batch_size) b[i] = b[i + 3] - bs[i] + 1;
+                    b[i] = std::max<int64_t>(1, b[i] - border[i]);
+                    b[i + 3] = std::min(vol[i], b[i + 3] + border[i]);
+                }
+                for (int i = 0; i < 3; i++) {
+                    l[i] = r[i] - b[i] + 1;
+                    l[i + 3] = l[i] + (r[i + 3] - r[i]);
+                }
+                for (int i = 0; i < 6; i++) {
+                    batch_bb[c * 6 + i] = b[i];
+                    local_bb[c * 6 + i] = l[i];
+                    region_bb[c * 6 + i] = r[i] - ws[i % 3] + 1;
+                }
+            }
+    return n;
+}
+
+}  // extern "C"

@@ -1,0 +1,438 @@
+// Drivers of the two iterations: OTF preparation and the launch programs of
+// decon_lucy_omw_function (OMW / WB backprojector RL) and decon_lucy_function (Biggs RL).
+//
+// Per OMW iteration (decon_lucy_omw_function.m:105-113) the program is
+//   [y: c = C2R(S); Jn = max(c*Jo,0); S = R2C(Jn)] x-fwd  z(OTF_f)  x-inv
+//   [y: c = C2R(S); r = I / max(c,eps); S = R2C(r)] x-fwd  z(OTF_b)  x-inv
+// where the first y pass of a call is [raw -> I; S = R2C(I)] and the last one writes the
+// post-processed, cropped output directly (decon_lucy_omw_function.m:146-177).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "pk_internal.h"
+
+namespace {
+
+__global__ void k_psf_sum(const float* __restrict__ psf, long long n, double* out) {
+    __shared__ double s[256];
+    double a = 0.0;
+    for (long long i = threadIdx.x; i < n; i += blockDim.x) a += (double)psf[i];
+    s[threadIdx.x] = a;
+    __syncthreads();
+    for (int k = 128; k > 0; k >>= 1) {
+        if ((int)threadIdx.x < k) s[threadIdx.x] += s[threadIdx.x + k];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = s[0];
+}
+
+// Pad (post) to the volume, circshift by -floor(psz/2), normalise by the float64 sum
+// (decon_psf2otf.m:25-27 with PSF./sum(PSF(:)) in float64).
+__global__ void k_psf_scatter(const float* __restrict__ psf, int py, int px, int pz, const double* __restrict__ sum,
+                              float* __restrict__ vol, int ny, int nx, int nz) {
+    const long long n = (long long)py * px * pz;
+    const double s = *sum;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int y = (int)(i % py);
+        const int x = (int)((i / py) % px);
+        const int z = (int)(i / ((long long)py * px));
+        int ty = y - py / 2; if (ty < 0) ty += ny;
+        int tx = x - px / 2; if (tx < 0) tx += nx;
+        int tz = z - pz / 2; if (tz < 0) tz += nz;
+        vol[(long long)ty + (long long)ny * (tx + (long long)nx * tz)] = (float)((double)psf[i] / s);
+    }
+}
+
+// numit == 0: J = I, post-processing only.
+__global__ void k_post_identity(VolDesc d) {
+    const long long n = d.nrows * d.ny;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const long long row = i / d.ny;
+        const int y = (int)(i - row * d.ny);
+        const int x = (int)(row % d.nx), z = (int)(row / d.nx);
+        if (y < d.bb0[0] || y > d.bb1[0] || x < d.bb0[1] || x > d.bb1[1] || z < d.bb0[2] || z > d.bb1[2]) continue;
+        float J = d.I[i];
+        if (d.damp > 1.f) {
+            const float dI = __fmul_rn(d.damp, d.I[i]);
+            J = __fadd_rn((J <= dI) ? J : 0.f, fminf(J, (J >= dI) ? dI : 0.f));
+        }
+        if (d.scale_mode == 1) J = __fmul_rn(J, d.scale);
+        else if (d.scale_mode == 2) {
+            int m = 1;
+            if (d.mask_mode == 1 || d.mask_mode == 3) m = d.mask8[i] != 0;
+            else if (d.mask_mode == 2) {
+                const int E = d.erosion;
+                m = d.mask8[i] != 0 && y >= E && y < d.ny - E && x >= E && x < d.nx - E && z >= E && z < d.nz - E;
+            }
+            J = __fmul_rn(__fadd_rn(__fmul_rn(J, d.scale), d.offset), (float)m);
+        }
+        const long long oy = d.bb1[0] - d.bb0[0] + 1, ox = d.bb1[1] - d.bb0[1] + 1;
+        const long long oi = (long long)(y - d.bb0[0]) + oy * ((long long)(x - d.bb0[1]) + ox * (long long)(z - d.bb0[2]));
+        if (d.save16) {
+            float r = roundf(J);
+            if (!(r >= 0.f)) r = 0.f;
+            if (r > 65535.f) r = 65535.f;
+            ((uint16_t*)d.out)[oi] = (uint16_t)r;
+        } else {
+            ((float*)d.out)[oi] = J;
+        }
+    }
+}
+
+// ---- irregular-mask edge erosion (decon_mask_edge_erosion.m:18-29)
+__global__ void k_mask_faces(uint8_t* m, int ny, int nx, int nz) {
+    const long long n = (long long)ny * nx * nz;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int y = (int)(i % ny);
+        const int x = (int)((i / ny) % nx);
+        const int z = (int)(i / ((long long)ny * nx));
+        if (y == 0 || y == ny - 1 || x == 0 || x == nx - 1 || z == 0 || z == nz - 1) m[i] = 0;
+    }
+}
+
+// erosion with a 2D (per z-slice) neighbourhood given as (dy, dx) offsets; outside counts as true
+__global__ void k_erode_xy(const uint8_t* __restrict__ in, uint8_t* __restrict__ out, int ny, int nx, int nz,
+                           const int2* __restrict__ offs, int noff) {
+    const long long n = (long long)ny * nx * nz;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int y = (int)(i % ny);
+        const int x = (int)((i / ny) % nx);
+        const long long zo = (i / ((long long)ny * nx)) * (long long)ny * nx;
+        uint8_t v = in[i];
+        for (int k = 0; v && k < noff; k++) {
+            const int yy = y + offs[k].x, xx = x + offs[k].y;
+            if (yy < 0 || yy >= ny || xx < 0 || xx >= nx) continue;
+            v = in[zo + yy + (long long)ny * xx];
+        }
+        out[i] = v;
+    }
+}
+
+__global__ void k_erode_z(const uint8_t* __restrict__ in, uint8_t* __restrict__ out, int ny, int nx, int nz, int h) {
+    const long long n = (long long)ny * nx * nz;
+    const long long plane = (long long)ny * nx;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int z = (int)(i / plane);
+        uint8_t v = in[i];
+        for (int o = -h; v && o <= h; o++) {
+            const int zz = z + o;
+            if (zz < 0 || zz >= nz) continue;
+            v = in[i + (long long)o * plane];
+        }
+        out[i] = v;
+    }
+}
+
+uint64_t fnv1a(const void* p, size_t n, uint64_t h = 1469598103934665603ULL) {
+    const unsigned char* b = (const unsigned char*)p;
+    for (size_t i = 0; i < n; i++) {
+        h ^= b[i];
+        h *= 1099511628211ULL;
+    }
+    return h;
+}
+
+int grid_for(long long n) {
+    long long g = (n + 255) / 256;
+    if (g > 148LL * 32) g = 148LL * 32;
+    if (g < 1) g = 1;
+    return (int)g;
+}
+
+}  // namespace
+
+// strel('disk', R) neighbourhood (default N = 4 approximation), as (dy, dx) offsets.
+std::vector<int2> pk_disk_offsets(int R) {
+    std::vector<std::pair<int, int>> pts;
+    if (R < 3) {
+        for (int a = -R; a <= R; a++)
+            for (int b = -R; b <= R; b++)
+                if (a * a + b * b <= R * R) pts.push_back({a, b});
+    } else {
+        // radial decomposition into four periodic lines (Adams 1993; Jones & Soille 1996)
+        const double theta = M_PI / 8.0;
+        const double k = 2.0 * R / (1.0 / std::tan(theta) + 1.0 / std::sin(theta));
+        const int vy[4] = {1, 1, 0, -1}, vx[4] = {0, 1, 1, 1};
+        std::vector<std::pair<int, int>> cur{{0, 0}};
+        auto minkowski = [&](int dy, int dx, int rp) {
+            std::vector<std::pair<int, int>> nxt;
+            for (auto& p : cur)
+                for (int m = -rp; m <= rp; m++) nxt.push_back({p.first + m * dy, p.second + m * dx});
+            std::sort(nxt.begin(), nxt.end());
+            nxt.erase(std::unique(nxt.begin(), nxt.end()), nxt.end());
+            cur.swap(nxt);
+        };
+        for (int q = 0; q < 4; q++) {
+            const int rp = (int)std::floor(k / std::sqrt((double)(vy[q] * vy[q] + vx[q] * vx[q])));
+            minkowski(vy[q], vx[q], rp);
+        }
+        int rmax = 0;
+        for (auto& p : cur) rmax = std::max(rmax, p.first);
+        const int len = 2 * (R - rmax - 1) + 1;
+        if (len >= 3) {
+            minkowski(0, 1, len / 2);
+            minkowski(1, 0, len / 2);
+        }
+        pts = cur;
+    }
+    std::vector<int2> out;
+    for (auto& p : pts) out.push_back(make_int2(p.first, p.second));
+    return out;
+}
+
+pk_status pk_scratch(pk_ctx* ctx, int slot, size_t bytes, void** ptr) {
+    if ((int)ctx->scratch.size() <= slot) ctx->scratch.resize(slot + 1, {nullptr, 0});
+    auto& s = ctx->scratch[slot];
+    if (s.second < bytes) {
+        if (s.first) cudaFree(s.first);
+        s.first = nullptr;
+        s.second = 0;
+        cudaError_t e = cudaMalloc(&s.first, bytes);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return pk_fail(PK_ERR_NOMEM, "device allocation of " + std::to_string(bytes) + " bytes failed: " + cudaGetErrorString(e));
+        }
+        s.second = bytes;
+    }
+    *ptr = s.first;
+    return PK_OK;
+}
+
+enum { SL_I = 0, SL_J = 1, SL_JB = 2, SL_Y = 3, SL_J4 = 4, SL_S = 5, SL_MASK = 6, SL_MASK2 = 7, SL_PART = 8,
+       SL_IN = 9, SL_OUT = 10, SL_PSF = 11, SL_SUM = 12, SL_OFFS = 13 };
+
+// Half-spectrum OTF of a PSF at the volume size, scaled by `scale` (1/N for the iterations).
+pk_status pk_make_otf(pk_ctx* ctx, const float* h_psf, const int64_t pd[3], int ny, int nx, int nz, double scale,
+                      float2* d_otf, cudaStream_t st) {
+    const long long pn = (long long)pd[0] * pd[1] * pd[2];
+    if (pd[0] > ny || pd[1] > nx || pd[2] > nz) return pk_fail(PK_ERR_INVALID, "outSizeIsSmallerThanPsfSize");
+    void *d_psf, *d_sum, *d_vol;
+    pk_status s;
+    if ((s = pk_scratch(ctx, SL_PSF, sizeof(float) * pn, &d_psf)) != PK_OK) return s;
+    if ((s = pk_scratch(ctx, SL_SUM, sizeof(double) * 2, &d_sum)) != PK_OK) return s;
+    if ((s = pk_scratch(ctx, SL_JB, sizeof(float) * (size_t)ny * nx * nz, &d_vol)) != PK_OK) return s;
+    PK_CUDA(cudaMemcpyAsync(d_psf, h_psf, sizeof(float) * pn, cudaMemcpyHostToDevice, st));
+    PK_CUDA(cudaMemsetAsync(d_vol, 0, sizeof(float) * (size_t)ny * nx * nz, st));
+    k_psf_sum<<<1, 256, 0, st>>>((const float*)d_psf, pn, (double*)d_sum);
+    k_psf_scatter<<<grid_for(pn), 256, 0, st>>>((const float*)d_psf, (int)pd[0], (int)pd[1], (int)pd[2],
+                                                 (const double*)d_sum, (float*)d_vol, ny, nx, nz);
+    PK_CUDA(cudaGetLastError());
+    VolDesc d;
+    if ((s = pk_init_desc(ctx, ny, nx, nz, &d)) != PK_OK) return s;
+    d.src = (const float*)d_vol;
+    d.S = d_otf;
+    d.xz_scale = (float)scale;
+    PkProgram prog;
+    pk_program_add(prog, PK_STEP_Y, Y_R2C, {d});
+    pk_program_add(prog, PK_STEP_X, XZ_FWD, {d});
+    pk_program_add(prog, PK_STEP_Z, XZ_FWD_SCALE, {d});
+    if ((s = pk_program_upload(ctx, prog, st)) == PK_OK) s = pk_program_launch(prog, st);
+    return s;
+}
+
+pk_status pk_get_otf(pk_ctx* ctx, const float* h_psf, const int64_t pd[3], int ny, int nx, int nz,
+                     const float2** d_otf, cudaStream_t st) {
+    const long long pn = (long long)pd[0] * pd[1] * pd[2];
+    uint64_t h = fnv1a(h_psf, sizeof(float) * pn);
+    h = fnv1a(pd, sizeof(int64_t) * 3, h);
+    auto key = std::make_tuple(h, ny, nx, nz);
+    auto it = ctx->otf.find(key);
+    if (it != ctx->otf.end()) { *d_otf = it->second.d; return PK_OK; }
+    OtfEntry e;
+    e.bytes = sizeof(float2) * (size_t)(ny / 2 + 1) * nx * nz;
+    cudaError_t ce = cudaMalloc(&e.d, e.bytes);
+    if (ce != cudaSuccess) { cudaGetLastError(); return pk_fail(PK_ERR_NOMEM, "OTF allocation failed"); }
+    const double N = (double)ny * nx * nz;
+    pk_status s = pk_make_otf(ctx, h_psf, pd, ny, nx, nz, 1.0 / N, e.d, st);
+    if (s != PK_OK) { cudaFree(e.d); return s; }
+    ctx->otf[key] = e;
+    *d_otf = e.d;
+    return PK_OK;
+}
+
+static void set_post(VolDesc& d, const pk_decon_params* p, int mask_mode, void* d_out) {
+    const bool off = p->decon_offset != 0.0, ero = p->edge_erosion > 0;
+    d.damp = (float)p->damp_factor;
+    d.scale = (float)p->scale_factor;
+    d.offset = (float)p->decon_offset;
+    d.erosion = p->edge_erosion;
+    if (p->scale_factor != 1.0 || off || ero) d.scale_mode = (off || ero) ? 2 : 1;
+    else d.scale_mode = 0;
+    d.mask_mode = d.scale_mode == 2 ? mask_mode : 0;
+    d.save16 = p->save16bit ? 1 : 0;
+    d.out = d_out;
+    if (p->has_bbox) {
+        for (int i = 0; i < 3; i++) {
+            d.bb0[i] = (int)p->bbox[i] - 1;
+            d.bb1[i] = (int)p->bbox[i + 3] - 1;
+        }
+    }
+}
+
+pk_status pk_check_params(const int64_t dims[3], const pk_decon_params* p) {
+    if (!p) return pk_fail(PK_ERR_INVALID, "params must not be NULL");
+    if (dims[0] < 1 || dims[1] < 1 || dims[2] < 1) return pk_fail(PK_ERR_INVALID, "empty input volume");
+    if (p->has_bbox) {
+        for (int i = 0; i < 3; i++) {
+            if (p->bbox[i] < 1 || p->bbox[i + 3] > dims[i] || p->bbox[i] > p->bbox[i + 3])
+                return pk_fail(PK_ERR_INVALID, "bbox is outside the volume (Index exceeds array bounds)");
+        }
+    }
+    return PK_OK;
+}
+
+pk_status pk_decon_run(pk_ctx* ctx, int method, const void* d_in, pk_dtype in_type, const int64_t dims[3],
+                       const float* psf_f, const int64_t psf_f_dims[3], const float* psf_b,
+                       const int64_t psf_b_dims[3], int numit, const pk_decon_params* p, void* d_out,
+                       cudaStream_t st) {
+    pk_status s;
+    if ((s = pk_check_params(dims, p)) != PK_OK) return s;
+    if (numit < 0) return pk_fail(PK_ERR_INVALID, "NUMIT must be non-negative");
+    const int ny = (int)dims[0], nx = (int)dims[1], nz = (int)dims[2];
+    const size_t N = (size_t)ny * nx * nz;
+    VolDesc d;
+    if ((s = pk_init_desc(ctx, ny, nx, nz, &d)) != PK_OK) return s;
+    const float2 *otf_f = nullptr, *otf_b = nullptr;
+    if ((s = pk_get_otf(ctx, psf_f, psf_f_dims, ny, nx, nz, &otf_f, st)) != PK_OK) return s;
+    if (method == 1 && (s = pk_get_otf(ctx, psf_b, psf_b_dims, ny, nx, nz, &otf_b, st)) != PK_OK) return s;
+    void *I, *J, *JB = nullptr, *Yb = nullptr, *J4 = nullptr, *S, *mask = nullptr, *part = nullptr;
+    if ((s = pk_scratch(ctx, SL_I, sizeof(float) * N, &I)) != PK_OK) return s;
+    if ((s = pk_scratch(ctx, SL_J, sizeof(float) * N, &J)) != PK_OK) return s;
+    if ((s = pk_scratch(ctx, SL_S, sizeof(float2) * pk_spec_elems(d), &S)) != PK_OK) return s;
+    if (method == 0) {
+        if ((s = pk_scratch(ctx, SL_JB, sizeof(float) * N, &JB)) != PK_OK) return s;
+        if ((s = pk_scratch(ctx, SL_Y, sizeof(float) * N, &Yb)) != PK_OK) return s;
+        if ((s = pk_scratch(ctx, SL_J4, sizeof(float) * N, &J4)) != PK_OK) return s;
+        if ((s = pk_scratch(ctx, SL_PART, sizeof(double) * (2 + 2 * (size_t)d.blocksY), &part)) != PK_OK) return s;
+    }
+    const bool need_mask = p->decon_offset != 0.0 || p->edge_erosion > 0;
+    if (need_mask && (s = pk_scratch(ctx, SL_MASK, N, &mask)) != PK_OK) return s;
+    unsigned int* zc = nullptr;
+    if (p->edge_erosion > 0) {
+        if (!ctx->d_counter) PK_CUDA(cudaMalloc(&ctx->d_counter, sizeof(unsigned int)));
+        zc = ctx->d_counter;
+        PK_CUDA(cudaMemsetAsync(zc, 0, sizeof(unsigned int), st));
+    }
+
+    // first pass: raw -> I (and the mask), S = R2C(I)
+    d.raw = d_in;
+    d.raw_type = in_type;
+    d.bg_f = (float)p->background;
+    {
+        double b = std::floor(std::fabs(p->background) + 0.5);
+        if (p->background < 0) b = 0;
+        if (!(b == b)) b = 0;
+        d.bg16 = (int)std::min(b, 65535.0);
+    }
+    d.I = (float*)I;
+    d.mask8 = (uint8_t*)mask;
+    d.write_mask = need_mask ? 1 : 0;
+    d.zero_count = zc;
+    d.S = (float2*)S;
+    PkProgram prog;
+    pk_program_add(prog, PK_STEP_Y, Y_PRE, {d});
+    int mask_mode = need_mask ? 1 : 0;
+    if (p->edge_erosion > 0) {
+        // the erosion branch depends on whether the raw mask is full (decon_mask_edge_erosion.m:8)
+        if ((s = pk_program_upload(ctx, prog, st)) != PK_OK) return s;
+        if ((s = pk_program_launch(prog, st)) != PK_OK) return s;
+        prog = PkProgram();
+        unsigned int zeros = 0;
+        PK_CUDA(cudaMemcpyAsync(&zeros, zc, sizeof(zeros), cudaMemcpyDeviceToHost, st));
+        PK_CUDA(cudaStreamSynchronize(st));
+        if (zeros == 0) {
+            mask_mode = 2;
+        } else {
+            mask_mode = 3;
+            void *m2, *offs;
+            if ((s = pk_scratch(ctx, SL_MASK2, N, &m2)) != PK_OK) return s;
+            std::vector<int2> disk = pk_disk_offsets(p->edge_erosion - 1);
+            if ((s = pk_scratch(ctx, SL_OFFS, sizeof(int2) * disk.size(), &offs)) != PK_OK) return s;
+            PK_CUDA(cudaMemcpyAsync(offs, disk.data(), sizeof(int2) * disk.size(), cudaMemcpyHostToDevice, st));
+            k_mask_faces<<<grid_for((long long)N), 256, 0, st>>>((uint8_t*)mask, ny, nx, nz);
+            k_erode_xy<<<grid_for((long long)N), 256, 0, st>>>((const uint8_t*)mask, (uint8_t*)m2, ny, nx, nz,
+                                                                (const int2*)offs, (int)disk.size());
+            k_erode_z<<<grid_for((long long)N), 256, 0, st>>>((const uint8_t*)m2, (uint8_t*)mask, ny, nx, nz,
+                                                               p->edge_erosion - 1);
+            PK_CUDA(cudaGetLastError());
+            PK_CUDA(cudaStreamSynchronize(st));  // disk offsets are a host temporary
+        }
+    }
+
+    VolDesc base = d;
+    base.raw = nullptr;
+    base.zero_count = nullptr;
+    base.write_mask = 0;
+    if (numit == 0) {
+        if (!prog.steps.empty()) {
+            if ((s = pk_program_upload(ctx, prog, st)) != PK_OK) return s;
+            if ((s = pk_program_launch(prog, st)) != PK_OK) return s;
+        }
+        VolDesc f = base;
+        set_post(f, p, mask_mode, d_out);
+        k_post_identity<<<grid_for((long long)N), 256, 0, st>>>(f);
+        PK_CUDA(cudaGetLastError());
+        return PK_OK;
+    }
+    if (method == 1) {
+        for (int it = 1; it <= numit; it++) {
+            VolDesc cf = base; cf.otf = otf_f; cf.conj = 0;
+            VolDesc cb = base; cb.otf = otf_b; cb.conj = 0;
+            pk_program_add(prog, PK_STEP_X, XZ_FWD, {base});
+            pk_program_add(prog, PK_STEP_Z, XZ_CONV, {cf});
+            pk_program_add(prog, PK_STEP_X, XZ_INV, {base});
+            pk_program_add(prog, PK_STEP_Y, Y_RATIO, {base});
+            pk_program_add(prog, PK_STEP_X, XZ_FWD, {base});
+            pk_program_add(prog, PK_STEP_Z, XZ_CONV, {cb});
+            pk_program_add(prog, PK_STEP_X, XZ_INV, {base});
+            VolDesc u = base;
+            u.Jo = it == 1 ? (const float*)I : (const float*)J;
+            u.Jn = (float*)J;
+            if (it < numit) {
+                pk_program_add(prog, PK_STEP_Y, Y_UPDATE, {u});
+            } else {
+                set_post(u, p, mask_mode, d_out);
+                pk_program_add(prog, PK_STEP_Y, Y_FINAL, {u});
+            }
+        }
+    } else {
+        float* Jb[2] = {(float*)J, (float*)JB};
+        base.partials = (double*)part;
+        for (int k = 1; k <= numit; k++) {
+            if (k >= 2) {
+                VolDesc r = base;
+                r.J2 = Jb[k % 2];
+                r.J3 = k == 2 ? (const float*)I : Jb[(k - 1) % 2];
+                r.Yb = (float*)Yb;
+                r.lam_on = k >= 3 ? 1 : 0;
+                pk_program_add(prog, PK_STEP_Y, Y_RLPRE, {r});
+            }
+            VolDesc cf = base; cf.otf = otf_f; cf.conj = 0;
+            VolDesc cb = base; cb.otf = otf_f; cb.conj = 1;
+            pk_program_add(prog, PK_STEP_X, XZ_FWD, {base});
+            pk_program_add(prog, PK_STEP_Z, XZ_CONV, {cf});
+            pk_program_add(prog, PK_STEP_X, XZ_INV, {base});
+            pk_program_add(prog, PK_STEP_Y, Y_RATIO, {base});
+            pk_program_add(prog, PK_STEP_X, XZ_FWD, {base});
+            pk_program_add(prog, PK_STEP_Z, XZ_CONV, {cb});
+            pk_program_add(prog, PK_STEP_X, XZ_INV, {base});
+            VolDesc u = base;
+            u.Yb = k == 1 ? (float*)I : (float*)Yb;
+            if (k < numit) {
+                u.J4 = (float*)J4;
+                u.rl_first = k == 1 ? 1 : 0;
+                u.J2n = Jb[(k + 1) % 2];
+                pk_program_add(prog, PK_STEP_Y, Y_RLUPD, {u});
+                pk_program_add(prog, PK_STEP_LAMBDA, 0, {u});
+            } else {
+                set_post(u, p, mask_mode, d_out);
+                pk_program_add(prog, PK_STEP_Y, Y_RLFINAL, {u});
+            }
+        }
+    }
+    if ((s = pk_program_upload(ctx, prog, st)) != PK_OK) return s;
+    return pk_program_launch(prog, st);
+}

@@ -1,0 +1,157 @@
+// Internal types of libpkdecon: per-volume descriptors read by the pass kernels, transform plans,
+// and the context.  Layout conventions:
+//   real volume  : float  v[z][x][y]            (column-major [ny nx nz], y fastest)
+//   half spectrum: float2 S[z][x][k], k < Py     (Py = floor(ny/2)+1; real transform along y)
+// A 3D transform is three kinds of pass: a y pass over contiguous rows (real<->half-spectrum,
+// with the per-voxel arithmetic of the iteration folded into its load/store), and two strided
+// complex passes over x and z on tiles of T adjacent k-columns.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/pkdecon.h"
+
+#define PK_MAXST 16   // max radix stages per axis
+#define PK_PPT 16     // max complex points per thread per stage
+
+// ------------------------------------------------------------------ device-visible structs
+struct AxisDev {
+    int n;            // complex transform length along the axis
+    int nst;          // number of radix stages
+    int rad[PK_MAXST];
+    const float2* tw; // tw[k] = exp(-2 pi i k / twN), k < twN (device, cached per twN)
+    int twN;          // table length
+    int twStride;     // twN / n
+};
+
+// Pass modes of the y kernel.
+enum YMode : int {
+    Y_R2C = 0,        // src float rows -> S                           (plain forward / OTF prep)
+    Y_PRE = 1,        // raw rows -> I (written), mask8 -> S           (first pass of a call)
+    Y_RATIO = 2,      // S -> c; r = I / max(c, eps) -> S              (OMW / RL middle)
+    Y_UPDATE = 3,     // S -> c; Jn = max(c * Jo, 0) (written) -> S    (OMW iteration boundary)
+    Y_FINAL = 4,      // S -> c; J = max(c * Jo, 0); post -> out       (OMW last)
+    Y_RLPRE = 5,      // Y = max(J2 + lam (J2 - J3), 0) (written) -> S (RL iteration start)
+    Y_RLUPD = 6,      // S -> c; J2n = max(Y * c, 0), J4 = J2n - Y, lam partials
+    Y_RLFINAL = 7,    // S -> c; J = max(Y * c, 0); post -> out
+    Y_C2R = 8         // S -> float rows (plain inverse, unnormalised)
+};
+
+enum XZMode : int { XZ_FWD = 0, XZ_INV = 1, XZ_CONV = 2, XZ_FWD_SCALE = 3 };
+
+struct VolDesc {
+    // geometry
+    int ny, nx, nz;
+    int M;            // y-pass complex length: ny/2 (even ny) or ny (odd ny)
+    int Py;           // spectrum row pitch, floor(ny/2)+1
+    int odd;
+    long long nrows;  // nx * nz
+    int Ly, Tx, Tz;   // lines per CTA (y pass), k-columns per CTA (x / z passes)
+    int blocksY, blocksX, blocksZ;
+    AxisDev ay, ax, az;
+    // buffers
+    const void* raw; int raw_type;   // Y_PRE source (pk_dtype)
+    const float* src; float* dst;    // Y_R2C source / Y_C2R destination
+    float* I;                        // background-subtracted input
+    const float* Jo; float* Jn;      // OMW estimate (old / new; may alias)
+    float* Yb; float* J4; const float* J3;  // RL: Y, J4 buffers, previous estimate
+    const float* J2;                 // RL: current estimate (read in Y_RLPRE)
+    float* J2n;                      // RL: next estimate (Y_RLUPD / Y_RLFINAL write)
+    float2* S;                       // half spectrum (work)
+    const float2* otf; int conj;     // XZ_CONV
+    int xz_dir;                      // XZ_FWD / XZ_INV selection for an X launch
+    float xz_scale;                  // XZ_FWD_SCALE factor
+    double* partials;                // RL: 2 doubles per y-pass CTA
+    int lam_on;                      // RL: lambda from partials (iteration >= 3) else 0
+    int rl_first;                    // RL: Y_RLUPD without an old J4 (iteration 1)
+    // pre / post
+    float bg_f; int bg16;
+    uint8_t* mask8; int write_mask;  // Y_PRE: write raw ~= 0
+    unsigned int* zero_count;        // Y_PRE: number of raw zeros (erosion branch choice)
+    int mask_mode;                   // post: 0 none, 1 mask8 as is, 2 full-mask border erosion, 3 mask8 eroded
+    float damp; float scale; float offset; int erosion; int scale_mode; // scale_mode: 0 none, 1 scale, 2 (J*s+o)*mask
+    int save16; void* out;
+    int bb0[3], bb1[3];              // 0-based inclusive crop box (y, x, z)
+};
+
+// ------------------------------------------------------------------ host side
+struct AxisPlan {
+    int n = 0, nst = 0;
+    int rad[PK_MAXST] = {0};
+};
+
+bool pk_make_axis_plan(int n, AxisPlan* p);   // radix factorisation (any n >= 1)
+
+struct TwTable { float2* d = nullptr; int n = 0; };
+
+struct OtfEntry {
+    float2* d = nullptr;      // pre-scaled (1/N) half spectrum
+    size_t bytes = 0;
+};
+
+struct pk_ctx_impl;
+
+struct pk_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::recursive_mutex mu;
+    std::map<int, TwTable> tw;                                   // twN -> table
+    // OTF cache: key = (psf content hash, ny, nx, nz)
+    std::map<std::tuple<uint64_t, int, int, int>, OtfEntry> otf;
+    std::vector<std::pair<void*, size_t>> scratch;               // reusable device buffers by slot
+    void* prog_buf = nullptr; size_t prog_cap = 0;               // uploaded program descriptors
+    unsigned int* d_counter = nullptr;
+    std::vector<void*> host_pinned;
+};
+
+// error helpers (capi.cpp)
+void pk_set_error(const std::string& msg);
+pk_status pk_fail(pk_status st, const std::string& msg);
+#define PK_CUDA(call)                                                                   \
+    do {                                                                                \
+        cudaError_t _e = (call);                                                        \
+        if (_e != cudaSuccess)                                                          \
+            return pk_fail(PK_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(_e)); \
+    } while (0)
+
+// plans / descriptors (fft_kernels.cu)
+pk_status pk_get_twiddles(pk_ctx* ctx, int twN, const float2** out);
+pk_status pk_fill_axis(pk_ctx* ctx, int n, int twN, AxisDev* a);
+pk_status pk_init_desc(pk_ctx* ctx, int ny, int nx, int nz, VolDesc* d);
+size_t pk_spec_elems(const VolDesc& d);   // complex elements of the half spectrum
+
+// launch programs (passes.cu)
+enum { PK_STEP_Y = 0, PK_STEP_X = 1, PK_STEP_Z = 2, PK_STEP_LAMBDA = 3 };
+struct PkStep {
+    int kind = 0, mode = 0, nvol = 0, desc_off = 0, prefix_off = 0, grid = 0;
+    size_t smem = 0;
+};
+struct PkProgram {
+    std::vector<VolDesc> descs;
+    std::vector<int> prefix;
+    std::vector<PkStep> steps;
+    VolDesc* d_desc = nullptr; int* d_prefix = nullptr;   // inside the context's program buffer
+};
+void pk_program_add(PkProgram& prog, int kind, int mode, const std::vector<VolDesc>& vols);
+pk_status pk_program_upload(pk_ctx* ctx, PkProgram& prog, cudaStream_t st);
+pk_status pk_program_launch(PkProgram& prog, cudaStream_t st);
+int pk_program_kernel_count(const PkProgram& prog);
+
+// scratch buffers
+pk_status pk_scratch(pk_ctx* ctx, int slot, size_t bytes, void** ptr);
+
+// decon drivers (decon.cu)
+pk_status pk_get_otf(pk_ctx* ctx, const float* h_psf, const int64_t psf_dims[3], int ny, int nx, int nz,
+                     const float2** d_otf, cudaStream_t st);
+pk_status pk_decon_run(pk_ctx* ctx, int method, const void* d_in, pk_dtype in_type, const int64_t dims[3],
+                       const float* psf_f, const int64_t psf_f_dims[3], const float* psf_b,
+                       const int64_t psf_b_dims[3], int numit, const pk_decon_params* p, void* d_out,
+                       cudaStream_t st);

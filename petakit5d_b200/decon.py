@@ -1,0 +1,164 @@
+"""Drop-in host API for the deconvolution hot path, mirroring the reference MATLAB functions.
+
+``decon_lucy_function`` and ``decon_lucy_omw_function`` take the same positional arguments and
+name/value parameters as microscopeDataProcessing/decon/decon_lucy_function.m:1-36 and
+decon_lucy_omw_function.m:1-30 and return the same outputs.  Arrays are indexed like MATLAB
+(``I[y, x, z]``, ``size(I) == I.shape``); they are passed to libpkdecon.so in column-major order.
+Parameter names are matched case-insensitively, as the reference's inputParser does.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import _lib
+from ._lib import PK_F32, PK_F64, PK_U16, DeconParams, check, i64x3, lib, ptr
+
+_DEFAULTS = {"background": None, "usegpu": True, "save16bit": True, "dampfactor": 1.0, "scalefactor": 1.0,
+             "deconoffset": 0.0, "edgeerosion": 0, "bbox": None, "debug": False, "debug_folder": "./debug/",
+             "savestep": 1}
+
+
+def _parse(kw):
+    opts = dict(_DEFAULTS)
+    ctx = kw.pop("ctx", None)
+    for k, v in kw.items():
+        key = k.lower()
+        if key not in opts:
+            raise TypeError(f"'{k}' is not a recognized parameter")
+        opts[key] = v
+    if not opts["usegpu"]:
+        raise ValueError("useGPU=false: this implementation runs on the GPU only (no CPU path)")
+    if opts["debug"]:
+        raise NotImplementedError("debug=true (err_mat and intermediate TIFFs) is not supported")
+    return opts, ctx
+
+
+def _params(opts):
+    p = DeconParams()
+    lib.pk_params_default(p)
+    bg = opts["background"]
+    p.background = 0.0 if bg is None or (hasattr(bg, "__len__") and len(bg) == 0) else float(bg)
+    p.damp_factor = float(opts["dampfactor"])
+    p.scale_factor = float(opts["scalefactor"])
+    p.decon_offset = float(opts["deconoffset"])
+    p.edge_erosion = int(opts["edgeerosion"])
+    p.save16bit = 1 if opts["save16bit"] else 0
+    bb = opts["bbox"]
+    if bb is not None and len(bb) > 0:
+        if len(bb) != 6:
+            raise ValueError("bbox must have 6 elements [y1 x1 z1 y2 x2 z2]")
+        p.has_bbox = 1
+        for i in range(6):
+            p.bbox[i] = int(bb[i])
+    return p
+
+
+def _volume(I):
+    a = np.asarray(I)
+    if a.ndim > 3:
+        raise ValueError("only 2D/3D volumes are supported")
+    while a.ndim < 3:
+        a = a[..., None]
+    if a.dtype == np.uint16:
+        t = PK_U16
+    elif a.dtype == np.float32:
+        t = PK_F32
+    elif a.dtype == np.float64:
+        t = PK_F64
+    else:
+        a = a.astype(np.float32)
+        t = PK_F32
+    return np.asfortranarray(a), t
+
+
+def _psf(P):
+    a = np.asarray(P, dtype=np.float32)
+    while a.ndim < 3:
+        a = a[..., None]
+    return np.asfortranarray(a)
+
+
+def _out(dims, p):
+    od = i64x3([0, 0, 0])
+    check(lib.pk_output_dims(i64x3(dims), p, od))
+    shape = tuple(int(v) for v in od)
+    return np.empty(shape, dtype=np.uint16 if p.save16bit else np.float32, order="F")
+
+
+def decon_lucy_function(I, PSF, NUMIT, **kw):
+    """[J_2, err_mat, k] = decon_lucy_function(I, PSF, NUMIT, ...) (Biggs-accelerated RL)."""
+    opts, ctx = _parse(kw)
+    ctx = ctx or _lib.default_context()
+    vol, t = _volume(I)
+    psf = _psf(PSF)
+    p = _params(opts)
+    out = _out(vol.shape, p)
+    k = _lib.C.c_int32(0)
+    check(lib.pk_decon_lucy(ctx.handle, ptr(vol), t, i64x3(vol.shape), ptr(psf), i64x3(psf.shape), int(NUMIT), p,
+                            ptr(out), _lib.C.byref(k)))
+    return _squeeze_like(out, I), np.zeros((int(NUMIT), 4)), int(k.value)
+
+
+def decon_lucy_omw_function(I, PSF_f, PSF_b, NUMIT, **kw):
+    """[J, err_mat] = decon_lucy_omw_function(I, PSF_f, PSF_b, NUMIT, ...) (OMW / WB backprojector RL)."""
+    opts, ctx = _parse(kw)
+    ctx = ctx or _lib.default_context()
+    vol, t = _volume(I)
+    pf = _psf(PSF_f)
+    pb = _psf(PSF_b)
+    p = _params(opts)
+    out = _out(vol.shape, p)
+    check(lib.pk_decon_lucy_omw(ctx.handle, ptr(vol), t, i64x3(vol.shape), ptr(pf), i64x3(pf.shape), ptr(pb),
+                                i64x3(pb.shape), int(NUMIT), p, ptr(out)))
+    return _squeeze_like(out, I), np.zeros((int(NUMIT), 4))
+
+
+def _squeeze_like(out, I):
+    nd = np.asarray(I).ndim
+    if nd < 3 and out.shape[2] == 1:
+        out = out[..., 0]
+        if nd < 2 and out.shape[1] == 1:
+            out = out[:, 0]
+    return out
+
+
+def decon_device(method, d_in, in_dtype, dims, psf_f, psf_b=None, numit=2, ctx=None, stream=None, **kw):
+    """Device-pointer call (``d_in``/``d_out`` are device pointers or torch CUDA tensors).
+
+    method: 'omw' or 'rl'.  Returns the DeconParams used and writes into ``kw['out']``.
+    """
+    opts, _ = _parse({k: v for k, v in kw.items() if k != "out"})
+    ctx = ctx or _lib.default_context()
+    out = kw["out"]
+    p = _params(opts)
+    t = {"uint16": PK_U16, "float32": PK_F32, "float64": PK_F64}[str(in_dtype).replace("torch.", "")]
+    pf = _psf(psf_f)
+    s = ptr(stream) if stream is not None else None
+    if method == "omw":
+        pb = _psf(psf_b)
+        check(lib.pk_decon_lucy_omw_device(ctx.handle, ptr(d_in), t, i64x3(dims), ptr(pf), i64x3(pf.shape),
+                                           ptr(pb), i64x3(pb.shape), int(numit), p, ptr(out), s))
+    else:
+        check(lib.pk_decon_lucy_device(ctx.handle, ptr(d_in), t, i64x3(dims), ptr(pf), i64x3(pf.shape), int(numit),
+                                       p, ptr(out), s))
+    return p
+
+
+def psf2otf_half(psf, dims, ctx=None):
+    """decon_psf2otf(PSF./sum(PSF(:)), dims) as the half spectrum ``[floor(ny/2)+1, nx, nz]`` complex64."""
+    ctx = ctx or _lib.default_context()
+    pf = _psf(psf)
+    d = [int(v) for v in dims] + [1] * (3 - len(dims))
+    out = np.empty((d[0] // 2 + 1, d[1], d[2]), dtype=np.complex64, order="F")
+    check(lib.pk_psf2otf(ctx.handle, ptr(pf), i64x3(pf.shape), i64x3(d), ptr(out)))
+    return out
+
+
+def fft3_r2c(d_in, dims, d_spec, ctx=None, stream=None):
+    ctx = ctx or _lib.default_context()
+    check(lib.pk_fft3_r2c_device(ctx.handle, ptr(d_in), i64x3(dims), ptr(d_spec), ptr(stream) if stream else None))
+
+
+def fft3_c2r(d_spec, dims, d_out, ctx=None, stream=None):
+    ctx = ctx or _lib.default_context()
+    check(lib.pk_fft3_c2r_device(ctx.handle, ptr(d_spec), i64x3(dims), ptr(d_out), ptr(stream) if stream else None))

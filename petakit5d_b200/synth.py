@@ -1,0 +1,147 @@
+"""Seeded synthetic volumes and PSFs for the deconvolution workloads.
+
+The reference's demo runs on a light-sheet dataset that is downloaded at run time
+(demos/demo_RL_deconvolution.m:43); these generators stand in for it.  Volumes are numpy arrays
+indexed ``[y, x, z]`` (MATLAB order) in Fortran (column-major) memory order, so their bytes are
+exactly what a MATLAB caller would hand to the C ABI.  All randomness comes from numpy's PCG64
+with an explicit seed.
+
+Workloads (sizes are x, y, z):
+  * ``puncta_volume``        -- Gaussian puncta (sigma 1 voxel, amplitude U[200, 2000]) at uniform
+                                positions plus a background, convolved with the PSF, Poisson noise.
+  * ``gaussian_psf``         -- anisotropic Gaussian PSF, peak at the 1-based index floor(size/2)+1.
+  * ``lobed_psf``            -- Gaussian PSF plus two side lobes at +-dz along z.
+  * ``sinusoid_background``  -- smooth 3D sinusoid background (period, amplitude, offset).
+  * ``chunk_workload``       -- uneven chunks with overlap borders and per-chunk PSF ids.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+__all__ = ["gaussian_psf", "lobed_psf", "puncta_volume", "sinusoid_background", "chunk_workload",
+           "single_volume_workload", "LLSM_PSF", "SMALL_PSF"]
+
+
+def _rng(seed):
+    return np.random.Generator(np.random.PCG64(int(seed)))
+
+
+def gaussian_psf(size_yxz=(31, 31, 41), sigma_xy=1.3, sigma_z=3.0, lobes=(), lobe_amp=0.0):
+    """Normalised (sum 1, float32) Gaussian PSF; ``lobes`` are extra z offsets with ``lobe_amp``."""
+    ny, nx, nz = size_yxz
+    cy, cx, cz = ny // 2, nx // 2, nz // 2
+    y = (np.arange(ny) - cy)[:, None, None].astype(np.float64)
+    x = (np.arange(nx) - cx)[None, :, None].astype(np.float64)
+    z = (np.arange(nz) - cz)[None, None, :].astype(np.float64)
+    lat = np.exp(-(y * y + x * x) / (2 * sigma_xy ** 2))
+    p = lat * np.exp(-(z * z) / (2 * sigma_z ** 2))
+    for dz in lobes:
+        p = p + lobe_amp * lat * np.exp(-((z - dz) ** 2) / (2 * sigma_z ** 2))
+    p /= p.sum()
+    return np.asfortranarray(p.astype(np.float32))
+
+
+def lobed_psf(size_yxz=(64, 64, 101), sigma_xy=1.5, sigma_z=4.0, lobe_dz=12, lobe_amp=0.15):
+    return gaussian_psf(size_yxz, sigma_xy, sigma_z, lobes=(-lobe_dz, lobe_dz), lobe_amp=lobe_amp)
+
+
+SMALL_PSF = dict(size_yxz=(31, 31, 41), sigma_xy=1.3, sigma_z=3.0)
+LLSM_PSF = dict(size_yxz=(64, 64, 101), sigma_xy=1.5, sigma_z=4.0, lobe_dz=12, lobe_amp=0.15)
+
+
+def sinusoid_background(shape_yxz, period=200.0, amplitude=300.0, offset=100.0):
+    """offset + amplitude * (1 + sin(2 pi y/P) sin(2 pi x/P) sin(2 pi z/P)) / 2  (>= offset)."""
+    ny, nx, nz = shape_yxz
+    w = 2 * np.pi / period
+    sy = np.sin(w * np.arange(ny))[:, None, None]
+    sx = np.sin(w * np.arange(nx))[None, :, None]
+    sz = np.sin(w * np.arange(nz))[None, None, :]
+    return offset + amplitude * 0.5 * (1.0 + sy * sx * sz)
+
+
+def _render_puncta(shape, n, rng, sigma=1.0, amp=(200.0, 2000.0), radius=4):
+    ny, nx, nz = shape
+    img = np.zeros(shape, dtype=np.float64)
+    pos = rng.uniform(0.0, 1.0, size=(n, 3)) * np.array([ny, nx, nz], dtype=np.float64)
+    a = rng.uniform(amp[0], amp[1], size=n)
+    base = np.floor(pos).astype(np.int64)
+    off = np.arange(-radius, radius + 1)
+    oy, ox, oz = np.meshgrid(off, off, off, indexing="ij")
+    oy, ox, oz = oy.ravel(), ox.ravel(), oz.ravel()
+    step = 4096
+    for s in range(0, n, step):
+        b = base[s:s + step]
+        p = pos[s:s + step]
+        iy = b[:, 0:1] + oy[None, :]
+        ix = b[:, 1:2] + ox[None, :]
+        iz = b[:, 2:3] + oz[None, :]
+        d2 = (iy - p[:, 0:1]) ** 2 + (ix - p[:, 1:2]) ** 2 + (iz - p[:, 2:3]) ** 2
+        v = a[s:s + step, None] * np.exp(-d2 / (2 * sigma * sigma))
+        np.add.at(img, (iy % ny, ix % nx, iz % nz), v)
+    return img
+
+
+def _circular_blur(img, psf):
+    """Circular convolution with the PSF, centred the way decon_psf2otf centres it."""
+    import scipy.fft as sfft
+    shape = img.shape
+    big = np.zeros(shape, dtype=np.float64)
+    ps = psf.shape
+    big[:ps[0], :ps[1], :ps[2]] = psf
+    big = np.roll(big, shift=tuple(-(np.array(ps) // 2)), axis=(0, 1, 2))
+    ax = (2, 1, 0)
+    H = sfft.rfftn(big, axes=ax, workers=-1)
+    out = sfft.irfftn(sfft.rfftn(img, axes=ax, workers=-1) * H, s=(shape[2], shape[1], shape[0]), axes=ax, workers=-1)
+    return out
+
+
+def puncta_volume(shape_yxz, n_puncta, psf, seed, background=100.0):
+    """uint16 volume: puncta + background (scalar or array), blurred by ``psf``, Poisson noise."""
+    rng = _rng(seed)
+    img = _render_puncta(tuple(shape_yxz), int(n_puncta), rng)
+    clean = _circular_blur(img, psf) + background
+    clean = np.maximum(clean, 0.0)
+    noisy = rng.poisson(clean)
+    return np.asfortranarray(np.clip(noisy, 0, 65535).astype(np.uint16))
+
+
+def single_volume_workload(kind, seed=1):
+    """(volume, psf) for the single-volume workloads.
+
+    ``kind='rl_small'``: 128x128x64 (x,y,z), 200 puncta, background 100, 31x31x41 Gaussian PSF.
+    ``kind='omw_llsm'``: 512x512x256, 20 000 puncta over a sinusoid background, 64x64x101 lobed PSF.
+    """
+    if kind == "rl_small":
+        psf = gaussian_psf(**SMALL_PSF)
+        vol = puncta_volume((128, 128, 64), 200, psf, seed, background=100.0)
+        return vol, psf
+    if kind == "omw_llsm":
+        psf = lobed_psf(**LLSM_PSF)
+        shape = (512, 512, 256)
+        vol = puncta_volume(shape, 20000, psf, seed, background=sinusoid_background(shape))
+        return vol, psf
+    raise ValueError(kind)
+
+
+def chunk_workload(n_chunks=96, seed=3, border=16, core_xy=(192, 256, 320, 384), core_z=(96, 128, 192, 256),
+                   sigmas=(1.3, 1.5, 1.8), density=200.0 / (128 * 128 * 64)):
+    """Uneven chunks with ``border`` overlap voxels per side; returns (chunks, psfs, psf_ids, bboxes).
+
+    Each chunk is core + 2*border per axis; its output region (1-based inclusive deconBbox,
+    ``[y1 x1 z1 y2 x2 z2]``) is the core.  Content follows the small-volume generator (same puncta
+    density, background 100) blurred by the chunk's PSF.
+    """
+    rng = _rng(seed)
+    psfs = [gaussian_psf((31, 31, 41), s, 3.0) for s in sigmas]
+    chunks, ids, bboxes = [], [], []
+    for i in range(n_chunks):
+        cy = int(rng.choice(core_xy))
+        cx = int(rng.choice(core_xy))
+        cz = int(rng.choice(core_z))
+        pid = int(rng.integers(0, len(psfs)))
+        shape = (cy + 2 * border, cx + 2 * border, cz + 2 * border)
+        n = int(round(density * np.prod(shape)))
+        chunks.append(puncta_volume(shape, n, psfs[pid], seed * 100003 + i, background=100.0))
+        ids.append(pid)
+        bboxes.append([border + 1, border + 1, border + 1, border + cy, border + cx, border + cz])
+    return chunks, psfs, ids, bboxes
