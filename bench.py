@@ -1,0 +1,379 @@
+"""Benchmark of the OMW deconvolution hot path (one JSON line on rank 0).
+
+Workload (default, ``--workload omw_llsm``): one 512x512x256 (x,y,z) uint16 volume, 20 000 Gaussian
+puncta over a sinusoid background with Poisson noise, a 64x64x101 two-lobed PSF, OMW RL with 2
+iterations, background 100, uint16 output.  A "step" deconvolves one volume.
+
+  value  : Mvoxel/s with the input resident in HBM (device-pointer C-ABI call per step, CUDA events on
+           the library's stream, max over ranks).  The working set (0.9 GB) is far larger than L2.
+  e2e    : Mvoxel/s through the host-buffer C-ABI call (pinned host input and output; H2D of the raw
+           volume and D2H of the result inside the timed region).
+  roofline: the dominant kernel's algorithmic HBM bytes per launch / its mean CUDA-event duration.
+  cpu_baseline: the CPU restatement of the reference (oracle, float32, scipy.fft on all host cores)
+           on one full volume, OTFs cached as the reference caches them.
+  cufft_comparator: the same iteration written with torch.fft (cuFFT) + elementwise ops on the same
+           resident input, timed the same way; a comparator only.
+
+``--impl reference`` times the reference's CPU path (the oracle restatement; MATLAB is not available)
+on the host cores with the same metric.  Under torchrun every rank runs an independent replica
+(the path shards by volume; no data-path collective): weak scaling.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "deconvolved Mvoxel/s (OMW, 2 iter) @rel-L2<=1e-4"
+ITERS = 2
+BACKGROUND = 100.0
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+                for n, v in zip(names, r[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(n)
+            except Exception:
+                continue
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_workload(seed):
+    from petakit5d_b200 import synth
+    vol, psf = synth.single_volume_workload("omw_llsm", seed=seed)
+    psf_b = np.asfortranarray(psf[::-1, ::-1, ::-1])   # traditional backprojector (flipped PSF)
+    return vol, psf, psf_b
+
+
+def cpu_restatement_rate(vol, psf, psf_b, steps=1, warmup=0):
+    """Oracle float32 OMW on host cores (OTFs prepared once, as the reference's persistent cache does)."""
+    from oracle import decon as O
+    shape = vol.shape
+    otf_f = O.psf2otf_half(O.normalize_psf(psf, np.float32), shape, np.float32)
+    otf_b = O.psf2otf_half(O.normalize_psf(psf_b, np.float32), shape, np.float32)
+    eps = np.float32(O.EPS)
+
+    def one():
+        I, _ = O.preprocess(vol, BACKGROUND, False, np.float32)
+        J = I
+        for _ in range(ITERS):
+            CX = np.fmax(O.conv_half(J, otf_f), eps)
+            J = np.fmax(O.conv_half(I / CX, otf_b) * J, np.float32(0))
+        return O.to_uint16(J)
+
+    for _ in range(warmup):
+        one()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        one()
+    dt = (time.perf_counter() - t0) / steps
+    return np.prod(shape) / dt / 1e6, dt
+
+
+def torch_omw(I16, otf_f, otf_b, iters):
+    """cuFFT comparator: the same OMW iteration with torch.fft on a (nz, nx, ny) tensor."""
+    import torch
+    I = (I16.to(torch.int32) - int(BACKGROUND)).clamp_min(0).to(torch.float32)
+    J = I
+    shp = I.shape
+    for _ in range(iters):
+        CX = torch.fft.irfftn(torch.fft.rfftn(J) * otf_f, s=shp).clamp_min(2.0 ** -52)
+        J = (torch.fft.irfftn(torch.fft.rfftn(I / CX) * otf_b, s=shp) * J).clamp_min(0)
+    return torch.round(J).clamp(0, 65535).to(torch.int32)
+
+
+def torch_otf(psf, shape_zxy, device):
+    import torch
+    p = np.asarray(psf, np.float64)
+    p = (p / p.sum()).astype(np.float32)
+    ny, nx, nz = p.shape
+    big = np.zeros((shape_zxy[2], shape_zxy[1], shape_zxy[0]), np.float32)   # (ny, nx, nz)
+    big[:ny, :nx, :nz] = p
+    big = np.roll(big, shift=(-(ny // 2), -(nx // 2), -(nz // 2)), axis=(0, 1, 2))
+    t = torch.from_numpy(np.ascontiguousarray(big.transpose(2, 1, 0))).to(device)
+    return torch.fft.rfftn(t)
+
+
+def run_ours(args, rank, world, device):
+    import torch
+    from petakit5d_b200 import _lib
+    from petakit5d_b200 import decon as D
+
+    vol, psf, psf_b = make_workload(seed=1 + rank)
+    ny, nx, nz = vol.shape
+    N = ny * nx * nz
+    ctx = _lib.Context(device.index)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=device)
+    d_in = torch.from_numpy(np.ascontiguousarray(vol.T).view(np.int16)).to(device)   # (nz, nx, ny) = column-major
+    d_out = torch.empty((nz, nx, ny), dtype=torch.int16, device=device)
+
+    def step():
+        D.decon_device("omw", d_in, "uint16", vol.shape, psf, psf_b, ITERS, out=d_out, ctx=ctx,
+                       stream=ctx.stream, Background=BACKGROUND)
+
+    torch.cuda.synchronize(device)
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(device)
+
+    # -- value: resident input, device-pointer C-ABI call, events on the library stream
+    clocks = ClockSampler(device.index)
+    clocks.start()
+    time.sleep(0.3)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize(device)
+    l0 = ctx.kernel_launches
+    ctx.profile(True)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize(device)
+    ctx.profile(False)
+    launches = ctx.kernel_launches - l0
+    if world > 1:
+        torch.distributed.barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    prof = ctx.profile_read()
+    ms_t = torch.tensor([ms], device=device)
+    if world > 1:
+        torch.distributed.all_reduce(ms_t, op=torch.distributed.ReduceOp.MAX)
+    ms = float(ms_t.item())
+
+    # -- e2e: host-buffer C-ABI call, pinned host buffers, copies inside the timed region
+    h_in_t = torch.from_numpy(np.ascontiguousarray(vol.T).view(np.int16)).pin_memory()
+    h_out_t = torch.empty((nz, nx, ny), dtype=torch.int16).pin_memory()
+    h_in = h_in_t.numpy().view(np.uint16).T          # (ny, nx, nz) Fortran view of pinned memory
+    h_out = h_out_t.numpy()
+    p = D._params({"background": BACKGROUND, "dampfactor": 1.0, "scalefactor": 1.0, "deconoffset": 0.0,
+                   "edgeerosion": 0, "save16bit": True, "bbox": None})
+    pf = np.asfortranarray(psf, np.float32)
+    pb = np.asfortranarray(psf_b, np.float32)
+
+    def e2e_step():
+        _lib.check(_lib.lib.pk_decon_lucy_omw(ctx.handle, h_in.ctypes.data, _lib.PK_U16, _lib.i64x3(vol.shape),
+                                              pf.ctypes.data, _lib.i64x3(pf.shape), pb.ctypes.data,
+                                              _lib.i64x3(pb.shape), ITERS, p, h_out.ctypes.data))
+
+    for _ in range(max(1, args.warmup)):
+        e2e_step()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize(device)
+    e0.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize(device)
+    e2e_ms_t = torch.tensor([e0.elapsed_time(e1) / args.steps], device=device)
+    if world > 1:
+        torch.distributed.all_reduce(e2e_ms_t, op=torch.distributed.ReduceOp.MAX)
+    e2e_ms = float(e2e_ms_t.item())
+    # the host-buffer result must equal the device-pointer result
+    same = bool(np.array_equal(h_out, d_out.cpu().numpy()))
+
+    # -- cuFFT comparator on the same resident input
+    cst = torch.cuda.Stream(device)
+    with torch.cuda.stream(cst):
+        of = torch_otf(psf, vol.shape, device)
+        ob = torch_otf(psf_b, vol.shape, device)
+        I16 = d_in.view(torch.int16).to(torch.int32) & 0xFFFF
+        for _ in range(2):
+            torch_omw(I16, of, ob, ITERS)
+        c0 = torch.cuda.Event(enable_timing=True)
+        c1 = torch.cuda.Event(enable_timing=True)
+        c0.record(cst)
+        for _ in range(args.steps):
+            torch_omw(I16, of, ob, ITERS)
+        c1.record(cst)
+    torch.cuda.synchronize(device)
+    cufft_ms = c0.elapsed_time(c1) / args.steps
+
+    peak, peak_kind = _peaks()
+    dom = max(prof.items(), key=lambda kv: kv[1]["ms"]) if prof else None
+    roof = None
+    if dom:
+        kind, rec = dom
+        per_ms = rec["ms"] / rec["launches"]
+        achieved = rec["bytes"] / (per_ms * 1e-3) / 1e9
+        traffic = None
+        try:
+            with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as f:
+                tj = json.load(f)
+            if kind in tj:
+                traffic = tj[kind]["dram_bytes_per_launch"]
+        except Exception:
+            pass
+        roof = {"bound": "hbm", "kernel": kind, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "peak_source": peak_kind, "traffic": traffic,
+                "algorithmic_bytes_per_launch": rec["bytes"], "ms_per_launch": round(per_ms, 5)}
+    call_bytes = N * (64 * ITERS + 12)
+    kernels = {k: {"launches": v["launches"], "ms_per_launch": round(v["ms"] / v["launches"], 5),
+                   "GBps": round(v["bytes"] / (v["ms"] / v["launches"] * 1e-3) / 1e9, 1),
+                   "share": round(v["ms"] / sum(x["ms"] for x in prof.values()), 4)} for k, v in prof.items()}
+    return {
+        "ms": ms, "N": N, "launches": launches, "clocks": clk, "roofline": roof, "kernels": kernels,
+        "e2e_ms": e2e_ms, "same": same, "cufft_ms": cufft_ms, "call_bytes": call_bytes, "vol": vol, "psf": psf,
+        "psf_b": psf_b, "peak": peak, "peak_kind": peak_kind,
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ncu-case", action="store_true",
+                    help="run two device calls of the workload and exit (the case profiled with ncu)")
+    args = ap.parse_args()
+    if args.ncu_case:
+        import torch
+        from petakit5d_b200 import decon as D
+        vol, psf, psf_b = make_workload(seed=1)
+        d_in = torch.from_numpy(np.ascontiguousarray(vol.T).view(np.int16)).cuda()
+        d_out = torch.empty_like(d_in)
+        for _ in range(2):
+            D.decon_device("omw", d_in, "uint16", vol.shape, psf, psf_b, ITERS, out=d_out, Background=BACKGROUND)
+        torch.cuda.synchronize()
+        return
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    config = {"workload": "omw_llsm: 512x512x256 (x,y,z) uint16, 20k puncta + sinusoid bg + Poisson, "
+                          "64x64x101 lobed PSF, flipped-PSF backprojector, OMW 2 iterations, uint16 out",
+              "volume_xyz": [512, 512, 256], "psf_yxz": [64, 64, 101], "iterations": ITERS,
+              "background": BACKGROUND, "parallelism": f"replicas x{world}",
+              "l2": "working set 0.9 GB >> 126 MB L2 (no flush needed)"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        vol, psf, psf_b = make_workload(seed=1)
+        cores = os.cpu_count()
+        rate, dt = cpu_restatement_rate(vol, psf, psf_b, steps=args.steps, warmup=args.warmup)
+        print(json.dumps({
+            "impl": "reference", "metric": METRIC, "value": round(rate, 3), "unit": "Mvoxel/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt * 1e3, 1),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": config,
+            "cpu_baseline": {"value": round(rate, 3), "unit": "Mvoxel/s", "cores": cores, "kind": "port",
+                             "sample": "one full 512x512x256 volume per step (oracle float32 restatement, "
+                                       "scipy.fft on all cores, OTFs cached)"},
+            "e2e": {"value": round(rate, 3), "unit": "Mvoxel/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "MATLAB (the reference runtime) is not installed; the reference arm is the CPU restatement "
+                    "of decon_lucy_omw_function.m (useGPU=false path)",
+        }), flush=True)
+        return
+
+    import torch
+    if world > 1:
+        torch.distributed.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=120))
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    r = run_ours(args, rank, world, device)
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank != 0:
+        return
+    N = r["N"]
+    value = N * world / (r["ms"] * 1e-3) / 1e6
+    e2e = N * world / (r["e2e_ms"] * 1e-3) / 1e6
+    line = {
+        "metric": METRIC, "value": round(value, 1), "unit": "Mvoxel/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(r["ms"], 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator; the reference's demo dataset is "
+                                                     "not available offline)",
+        "config": config,
+        "e2e": {"value": round(e2e, 1), "unit": "Mvoxel/s", "ms_per_step": round(r["e2e_ms"], 4),
+                "h2d_bytes_per_step": 2 * N, "d2h_bytes_per_step": 2 * N, "matches_device_call": r["same"]},
+        "gpu_launches": r["launches"],
+        "roofline": r["roofline"],
+        "call_roofline": {"algorithmic_bytes": r["call_bytes"], "achieved": round(r["call_bytes"] / (r["ms"] * 1e-3) / 1e9, 1),
+                          "peak": r["peak"], "frac": round(r["call_bytes"] / (r["ms"] * 1e-3) / 1e9 / r["peak"], 4),
+                          "unit": "GB/s", "note": "N*(64*iters+12) bytes per call"},
+        "kernels": r["kernels"],
+        "cufft_comparator": {"value": round(N / (r["cufft_ms"] * 1e-3) / 1e6, 1), "unit": "Mvoxel/s",
+                             "ms_per_step": round(r["cufft_ms"], 3)},
+        "clocks": r["clocks"],
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        rate, dt = cpu_restatement_rate(r["vol"], r["psf"], r["psf_b"], steps=1, warmup=0)
+        line["cpu_baseline"] = {"value": round(rate, 3), "unit": "Mvoxel/s", "cores": os.cpu_count(), "kind": "port",
+                                "sample": "one full 512x512x256 volume (oracle float32, scipy.fft on all cores, "
+                                          f"OTFs cached), {dt:.1f} s"}
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

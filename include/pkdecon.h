@@ -68,6 +68,17 @@ PK_API pk_status pk_ctx_reset(pk_ctx* ctx);
 PK_API const char* pk_last_error(void);
 PK_API const char* pk_version(void);
 
+/* The context's CUDA stream (a cudaStream_t); host-buffer calls run on it. */
+PK_API void* pk_ctx_stream(pk_ctx* ctx);
+/* Number of kernels this context has launched so far. */
+PK_API int64_t pk_ctx_kernel_launches(pk_ctx* ctx);
+/* Per-kernel-kind device timing: while enabled, every pass launch is bracketed by CUDA events on
+ * its stream.  pk_ctx_profile_read writes a JSON object {kind: {"launches", "ms", "bytes"}} where
+ * "bytes" is the algorithmic HBM traffic of one launch (minimum bytes the pass must move); it
+ * synchronises the recorded events and returns the JSON length (truncated to cap-1). */
+PK_API pk_status pk_ctx_profile(pk_ctx* ctx, int32_t enable);
+PK_API int32_t pk_ctx_profile_read(pk_ctx* ctx, char* buf, int32_t cap);
+
 /* Output extent for dims/params: the bbox size when has_bbox, else dims. */
 PK_API pk_status pk_output_dims(const int64_t dims[3], const pk_decon_params* p, int64_t out_dims[3]);
 

@@ -57,6 +57,10 @@ _SIGS = {
     "pk_ctx_reset": (C.c_int, [P]),
     "pk_last_error": (C.c_char_p, []),
     "pk_version": (C.c_char_p, []),
+    "pk_ctx_stream": (P, [P]),
+    "pk_ctx_kernel_launches": (C.c_int64, [P]),
+    "pk_ctx_profile": (C.c_int, [P, C.c_int32]),
+    "pk_ctx_profile_read": (C.c_int32, [P, C.c_char_p, C.c_int32]),
     "pk_output_dims": (C.c_int, [I64x3, C.POINTER(DeconParams), I64x3]),
     "pk_decon_lucy": (C.c_int, [P, P, C.c_int, I64x3, P, I64x3, C.c_int32, C.POINTER(DeconParams), P,
                                 C.POINTER(C.c_int32)]),
@@ -144,6 +148,24 @@ class Context:
             raise PkError(PK_ERR_CUDA, last_error())
         self.handle = h
         self.device = device
+
+    @property
+    def stream(self):
+        return lib.pk_ctx_stream(self.handle)
+
+    @property
+    def kernel_launches(self):
+        return int(lib.pk_ctx_kernel_launches(self.handle))
+
+    def profile(self, enable=True):
+        check(lib.pk_ctx_profile(self.handle, 1 if enable else 0))
+
+    def profile_read(self):
+        import json
+        n = lib.pk_ctx_profile_read(self.handle, None, 0)
+        buf = C.create_string_buffer(n + 1)
+        lib.pk_ctx_profile_read(self.handle, buf, n + 1)
+        return json.loads(buf.value.decode())
 
     def reset(self):
         check(lib.pk_ctx_reset(self.handle))

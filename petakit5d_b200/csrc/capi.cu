@@ -100,9 +100,12 @@ static void release_all(pk_ctx* ctx) {
     for (auto& s : ctx->scratch)
         if (s.first) cudaFree(s.first);
     ctx->scratch.clear();
-    if (ctx->prog_buf) cudaFree(ctx->prog_buf);
-    ctx->prog_buf = nullptr;
-    ctx->prog_cap = 0;
+    for (auto& sl : ctx->slots) {
+        if (sl.d) cudaFree(sl.d);
+        if (sl.h) cudaFreeHost(sl.h);
+        if (sl.ev) cudaEventDestroy(sl.ev);
+        sl = pk_ctx::ProgSlot();
+    }
     if (ctx->d_counter) cudaFree(ctx->d_counter);
     ctx->d_counter = nullptr;
 }
@@ -116,6 +119,8 @@ void pk_ctx_destroy(pk_ctx* ctx) {
         for (auto& kv : ctx->tw) cudaFree(kv.second.d);
         ctx->tw.clear();
         for (void* p : ctx->host_pinned) cudaFreeHost(p);
+    for (auto& r : ctx->prof) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
+    for (auto e : ctx->ev_pool) cudaEventDestroy(e);
         ctx->host_pinned.clear();
         cudaStreamDestroy(ctx->stream);
     }
@@ -129,6 +134,53 @@ pk_status pk_ctx_reset(pk_ctx* ctx) {
     DeviceGuard g(ctx->device);
     release_all(ctx);
     return PK_OK;
+}
+
+void* pk_ctx_stream(pk_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int64_t pk_ctx_kernel_launches(pk_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+pk_status pk_ctx_profile(pk_ctx* ctx, int32_t enable) {
+    pk_status s = check_ctx(ctx);
+    if (s != PK_OK) return s;
+    std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+    ctx->prof_on = enable != 0;
+    return PK_OK;
+}
+
+int32_t pk_ctx_profile_read(pk_ctx* ctx, char* buf, int32_t cap) {
+    if (!ctx) return -1;
+    std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+    DeviceGuard g(ctx->device);
+    std::map<std::string, std::tuple<long long, double, double>> agg;
+    for (auto& r : ctx->prof) {
+        cudaEventSynchronize(r.b);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, r.a, r.b);
+        auto& t = agg[r.kind];
+        std::get<0>(t) += 1;
+        std::get<1>(t) += ms;
+        std::get<2>(t) = r.bytes;
+        ctx->ev_pool.push_back(r.a);
+        ctx->ev_pool.push_back(r.b);
+    }
+    ctx->prof.clear();
+    std::string js = "{";
+    bool first = true;
+    for (auto& kv : agg) {
+        char tmp[256];
+        snprintf(tmp, sizeof(tmp), "%s\"%s\": {\"launches\": %lld, \"ms\": %.6f, \"bytes\": %.0f}", first ? "" : ", ",
+                 kv.first.c_str(), std::get<0>(kv.second), std::get<1>(kv.second), std::get<2>(kv.second));
+        js += tmp;
+        first = false;
+    }
+    js += "}";
+    if (buf && cap > 0) {
+        const int n = std::min((int)js.size(), cap - 1);
+        memcpy(buf, js.data(), n);
+        buf[n] = 0;
+    }
+    return (int32_t)js.size();
 }
 
 pk_status pk_output_dims(const int64_t dims[3], const pk_decon_params* p, int64_t out[3]) {
@@ -275,7 +327,7 @@ static pk_status fft3(pk_ctx* ctx, int inverse, const float* d_a, const int64_t 
         pk_program_add(prog, PK_STEP_Y, Y_C2R, {d});
     }
     if ((s = pk_program_upload(ctx, prog, st)) != PK_OK) return s;
-    return pk_program_launch(prog, st);
+    return pk_program_launch(ctx, prog, st);
 }
 
 pk_status pk_fft3_r2c_device(pk_ctx* ctx, const float* d_in, const int64_t dims[3], float* d_spec, void* stream) {

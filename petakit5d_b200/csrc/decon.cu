@@ -126,13 +126,24 @@ __global__ void k_erode_z(const uint8_t* __restrict__ in, uint8_t* __restrict__ 
     }
 }
 
-uint64_t fnv1a(const void* p, size_t n, uint64_t h = 1469598103934665603ULL) {
+// 64-bit content hash of a host buffer (word-wise multiply-xorshift), the OTF cache key
+uint64_t content_hash(const void* p, size_t n, uint64_t h = 0x243F6A8885A308D3ULL) {
     const unsigned char* b = (const unsigned char*)p;
-    for (size_t i = 0; i < n; i++) {
-        h ^= b[i];
-        h *= 1099511628211ULL;
+    size_t i = 0;
+    for (; i + 8 <= n; i += 8) {
+        uint64_t w;
+        memcpy(&w, b + i, 8);
+        h ^= w;
+        h *= 0x9E3779B97F4A7C15ULL;
+        h ^= h >> 29;
     }
-    return h;
+    for (; i < n; i++) {
+        h ^= b[i];
+        h *= 0x100000001B3ULL;
+    }
+    h ^= n;
+    h *= 0xBF58476D1CE4E5B9ULL;
+    return h ^ (h >> 31);
 }
 
 int grid_for(long long n) {
@@ -229,15 +240,15 @@ pk_status pk_make_otf(pk_ctx* ctx, const float* h_psf, const int64_t pd[3], int 
     pk_program_add(prog, PK_STEP_Y, Y_R2C, {d});
     pk_program_add(prog, PK_STEP_X, XZ_FWD, {d});
     pk_program_add(prog, PK_STEP_Z, XZ_FWD_SCALE, {d});
-    if ((s = pk_program_upload(ctx, prog, st)) == PK_OK) s = pk_program_launch(prog, st);
+    if ((s = pk_program_upload(ctx, prog, st)) == PK_OK) s = pk_program_launch(ctx, prog, st);
     return s;
 }
 
 pk_status pk_get_otf(pk_ctx* ctx, const float* h_psf, const int64_t pd[3], int ny, int nx, int nz,
                      const float2** d_otf, cudaStream_t st) {
     const long long pn = (long long)pd[0] * pd[1] * pd[2];
-    uint64_t h = fnv1a(h_psf, sizeof(float) * pn);
-    h = fnv1a(pd, sizeof(int64_t) * 3, h);
+    uint64_t h = content_hash(h_psf, sizeof(float) * pn);
+    h = content_hash(pd, sizeof(int64_t) * 3, h);
     auto key = std::make_tuple(h, ny, nx, nz);
     auto it = ctx->otf.find(key);
     if (it != ctx->otf.end()) { *d_otf = it->second.d; return PK_OK; }
@@ -338,7 +349,7 @@ pk_status pk_decon_run(pk_ctx* ctx, int method, const void* d_in, pk_dtype in_ty
     if (p->edge_erosion > 0) {
         // the erosion branch depends on whether the raw mask is full (decon_mask_edge_erosion.m:8)
         if ((s = pk_program_upload(ctx, prog, st)) != PK_OK) return s;
-        if ((s = pk_program_launch(prog, st)) != PK_OK) return s;
+        if ((s = pk_program_launch(ctx, prog, st)) != PK_OK) return s;
         prog = PkProgram();
         unsigned int zeros = 0;
         PK_CUDA(cudaMemcpyAsync(&zeros, zc, sizeof(zeros), cudaMemcpyDeviceToHost, st));
@@ -369,7 +380,7 @@ pk_status pk_decon_run(pk_ctx* ctx, int method, const void* d_in, pk_dtype in_ty
     if (numit == 0) {
         if (!prog.steps.empty()) {
             if ((s = pk_program_upload(ctx, prog, st)) != PK_OK) return s;
-            if ((s = pk_program_launch(prog, st)) != PK_OK) return s;
+            if ((s = pk_program_launch(ctx, prog, st)) != PK_OK) return s;
         }
         VolDesc f = base;
         set_post(f, p, mask_mode, d_out);
@@ -434,5 +445,5 @@ pk_status pk_decon_run(pk_ctx* ctx, int method, const void* d_in, pk_dtype in_ty
         }
     }
     if ((s = pk_program_upload(ctx, prog, st)) != PK_OK) return s;
-    return pk_program_launch(prog, st);
+    return pk_program_launch(ctx, prog, st);
 }

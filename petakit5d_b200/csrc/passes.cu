@@ -9,6 +9,7 @@
 //          XZ_CONV runs forward FFT, OTF multiply and inverse FFT on the tile in shared memory.
 // Every launch covers a list of volumes (descriptors + block prefix), so the batched and served
 // paths reuse the same kernels as the single-volume call.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -499,30 +500,91 @@ void pk_program_add(PkProgram& prog, int kind, int mode, const std::vector<VolDe
 }
 
 pk_status pk_program_upload(pk_ctx* ctx, PkProgram& prog, cudaStream_t st) {
-    // Copies are stream ordered, so reusing the context's buffer is safe for work queued on `st`;
-    // a pageable-source cudaMemcpyAsync has staged the host data when it returns.
     const size_t dbytes = sizeof(VolDesc) * prog.descs.size();
     const size_t pbytes = sizeof(int) * prog.prefix.size();
     const size_t need = dbytes + pbytes;
-    if (ctx->prog_cap < need) {
-        if (ctx->prog_buf) cudaFree(ctx->prog_buf);  // synchronises the device
-        ctx->prog_buf = nullptr;
-        ctx->prog_cap = 0;
-        PK_CUDA(cudaMalloc(&ctx->prog_buf, need));
-        ctx->prog_cap = need;
+    const int si = ctx->next_slot;
+    ctx->next_slot = (ctx->next_slot + 1) % 4;
+    pk_ctx::ProgSlot& sl = ctx->slots[si];
+    if (sl.used) PK_CUDA(cudaEventSynchronize(sl.ev));   // launches that read this slot are done
+    sl.used = false;
+    if (!sl.ev) PK_CUDA(cudaEventCreateWithFlags(&sl.ev, cudaEventDisableTiming));
+    if (sl.cap < need) {
+        if (sl.d) cudaFree(sl.d);
+        if (sl.h) cudaFreeHost(sl.h);
+        sl.d = sl.h = nullptr;
+        sl.cap = 0;
+        const size_t cap = std::max(need, (size_t)64 * 1024);
+        PK_CUDA(cudaMalloc(&sl.d, cap));
+        PK_CUDA(cudaMallocHost(&sl.h, cap));
+        sl.cap = cap;
     }
-    PK_CUDA(cudaMemcpyAsync(ctx->prog_buf, prog.descs.data(), dbytes, cudaMemcpyHostToDevice, st));
-    PK_CUDA(cudaMemcpyAsync((char*)ctx->prog_buf + dbytes, prog.prefix.data(), pbytes, cudaMemcpyHostToDevice, st));
-    prog.d_desc = (VolDesc*)ctx->prog_buf;
-    prog.d_prefix = (int*)((char*)ctx->prog_buf + dbytes);
+    memcpy(sl.h, prog.descs.data(), dbytes);
+    memcpy((char*)sl.h + dbytes, prog.prefix.data(), pbytes);
+    PK_CUDA(cudaMemcpyAsync(sl.d, sl.h, need, cudaMemcpyHostToDevice, st));
+    prog.d_desc = (VolDesc*)sl.d;
+    prog.d_prefix = (int*)((char*)sl.d + dbytes);
+    prog.slot = si;
     return PK_OK;
 }
 
-pk_status pk_program_launch(PkProgram& prog, cudaStream_t st) {
+const char* pk_step_name(const PkStep& s) {
+    static const char* yn[] = {"y_r2c", "y_pre", "y_ratio", "y_update", "y_final", "y_rlpre", "y_rlupd", "y_rlfinal", "y_c2r"};
+    static const char* xn[] = {"x_fwd", "x_inv", "x_conv", "x_fwd_scale"};
+    static const char* zn[] = {"z_fwd", "z_inv", "z_conv", "z_fwd_scale"};
+    if (s.kind == PK_STEP_Y) return yn[s.mode];
+    if (s.kind == PK_STEP_X) return xn[s.mode];
+    if (s.kind == PK_STEP_Z) return zn[s.mode];
+    return "lambda";
+}
+
+// Algorithmic HBM bytes of one launch: the minimum each pass must read and write.
+double pk_step_bytes(const PkStep& s, const VolDesc* descs) {
+    double b = 0;
+    for (int i = 0; i < s.nvol; i++) {
+        const VolDesc& d = descs[i];
+        const double N = (double)d.nrows * d.ny, Sb = 8.0 * d.Py * (double)d.nrows;
+        const double ob = (double)(d.bb1[0] - d.bb0[0] + 1) * (d.bb1[1] - d.bb0[1] + 1) * (d.bb1[2] - d.bb0[2] + 1) * (d.save16 ? 2 : 4);
+        if (s.kind == PK_STEP_Y) {
+            switch (s.mode) {
+                case Y_R2C: b += 4 * N + Sb; break;
+                case Y_PRE: b += (d.raw_type == PK_U16 ? 2 : d.raw_type == PK_F32 ? 4 : 8) * N + 4 * N + Sb + (d.write_mask ? N : 0); break;
+                case Y_RATIO: b += 2 * Sb + 4 * N; break;
+                case Y_UPDATE: b += 2 * Sb + 8 * N; break;
+                case Y_FINAL: b += Sb + 4 * N + (d.damp > 1.f ? 4 * N : 0) + ob; break;
+                case Y_RLPRE: b += 12 * N + Sb; break;
+                case Y_RLUPD: b += Sb + (d.rl_first ? 12 : 16) * N; break;
+                case Y_RLFINAL: b += Sb + 4 * N + ob; break;
+                case Y_C2R: b += Sb + 4 * N; break;
+            }
+        } else if (s.kind == PK_STEP_X || s.kind == PK_STEP_Z) {
+            b += (s.mode == XZ_CONV ? 3 : 2) * Sb;
+        } else {
+            b += 16.0 * d.blocksY;
+        }
+    }
+    return b;
+}
+
+pk_status pk_program_launch(pk_ctx* ctx, PkProgram& prog, cudaStream_t st) {
     for (const PkStep& s : prog.steps) {
         const VolDesc* dd = prog.d_desc + s.desc_off;
         const int* dp = prog.d_prefix + s.prefix_off;
         if (s.grid == 0) continue;
+        pk_ctx::ProfRec rec;
+        if (ctx && ctx->prof_on) {
+            auto take = [&]() {
+                cudaEvent_t e;
+                if (!ctx->ev_pool.empty()) { e = ctx->ev_pool.back(); ctx->ev_pool.pop_back(); }
+                else cudaEventCreate(&e);
+                return e;
+            };
+            rec.kind = pk_step_name(s);
+            rec.bytes = pk_step_bytes(s, prog.descs.data() + s.desc_off);
+            rec.a = take();
+            rec.b = take();
+            cudaEventRecord(rec.a, st);
+        }
         if (s.kind == PK_STEP_Y) {
             switch (s.mode) {
                 case Y_R2C: launch_y_mode<Y_R2C>(s.grid, s.smem, dd, dp, s.nvol, st); break;
@@ -549,6 +611,16 @@ pk_status pk_program_launch(PkProgram& prog, cudaStream_t st) {
             k_lambda<<<s.nvol, 256, 0, st>>>(dd, s.nvol);
         }
         PK_CUDA(cudaGetLastError());
+        if (ctx) ctx->launches++;
+        if (ctx && ctx->prof_on) {
+            cudaEventRecord(rec.b, st);
+            ctx->prof.push_back(rec);
+        }
+    }
+    if (ctx && prog.slot >= 0) {
+        pk_ctx::ProgSlot& sl = ctx->slots[prog.slot];
+        PK_CUDA(cudaEventRecord(sl.ev, st));
+        sl.used = true;
     }
     return PK_OK;
 }

@@ -107,9 +107,19 @@ struct pk_ctx {
     // OTF cache: key = (psf content hash, ny, nx, nz)
     std::map<std::tuple<uint64_t, int, int, int>, OtfEntry> otf;
     std::vector<std::pair<void*, size_t>> scratch;               // reusable device buffers by slot
-    void* prog_buf = nullptr; size_t prog_cap = 0;               // uploaded program descriptors
+    // uploaded program descriptors: a ring of pinned-host + device slots, each reused only after
+    // the event recorded behind the launches that read it has completed
+    struct ProgSlot { void* d = nullptr; void* h = nullptr; size_t cap = 0; cudaEvent_t ev = nullptr; bool used = false; };
+    ProgSlot slots[4];
+    int next_slot = 0;
     unsigned int* d_counter = nullptr;
     std::vector<void*> host_pinned;
+    long long launches = 0;                                      // kernels launched
+    // per-kind profiling (pk_ctx_profile)
+    bool prof_on = false;
+    struct ProfRec { std::string kind; cudaEvent_t a, b; double bytes; };
+    std::vector<ProfRec> prof;
+    std::vector<cudaEvent_t> ev_pool;
 };
 
 // error helpers (capi.cpp)
@@ -138,11 +148,14 @@ struct PkProgram {
     std::vector<VolDesc> descs;
     std::vector<int> prefix;
     std::vector<PkStep> steps;
-    VolDesc* d_desc = nullptr; int* d_prefix = nullptr;   // inside the context's program buffer
+    VolDesc* d_desc = nullptr; int* d_prefix = nullptr;   // inside one of the context's program slots
+    int slot = -1;
 };
 void pk_program_add(PkProgram& prog, int kind, int mode, const std::vector<VolDesc>& vols);
 pk_status pk_program_upload(pk_ctx* ctx, PkProgram& prog, cudaStream_t st);
-pk_status pk_program_launch(PkProgram& prog, cudaStream_t st);
+pk_status pk_program_launch(pk_ctx* ctx, PkProgram& prog, cudaStream_t st);
+double pk_step_bytes(const PkStep& s, const VolDesc* descs);
+const char* pk_step_name(const PkStep& s);
 int pk_program_kernel_count(const PkProgram& prog);
 
 // scratch buffers
