@@ -145,14 +145,15 @@ def torch_omw(I16, otf_f, otf_b, iters):
     return torch.round(J).clamp(0, 65535).to(torch.int32)
 
 
-def torch_otf(psf, shape_zxy, device):
+def torch_otf(psf, shape_yxz, device):
+    """decon_psf2otf at the volume size as a torch half spectrum on the (nz, nx, ny) layout."""
     import torch
     p = np.asarray(psf, np.float64)
     p = (p / p.sum()).astype(np.float32)
-    ny, nx, nz = p.shape
-    big = np.zeros((shape_zxy[2], shape_zxy[1], shape_zxy[0]), np.float32)   # (ny, nx, nz)
-    big[:ny, :nx, :nz] = p
-    big = np.roll(big, shift=(-(ny // 2), -(nx // 2), -(nz // 2)), axis=(0, 1, 2))
+    py, px, pz = p.shape
+    big = np.zeros(tuple(shape_yxz), np.float32)
+    big[:py, :px, :pz] = p
+    big = np.roll(big, shift=(-(py // 2), -(px // 2), -(pz // 2)), axis=(0, 1, 2))
     t = torch.from_numpy(np.ascontiguousarray(big.transpose(2, 1, 0))).to(device)
     return torch.fft.rfftn(t)
 

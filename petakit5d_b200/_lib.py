@@ -162,9 +162,11 @@ class Context:
 
     def profile_read(self):
         import json
-        n = lib.pk_ctx_profile_read(self.handle, None, 0)
-        buf = C.create_string_buffer(n + 1)
-        lib.pk_ctx_profile_read(self.handle, buf, n + 1)
+        cap = 1 << 20
+        buf = C.create_string_buffer(cap)
+        n = lib.pk_ctx_profile_read(self.handle, buf, cap)
+        if n >= cap:
+            raise PkError(PK_ERR_INVALID, "profile record larger than the read buffer")
         return json.loads(buf.value.decode())
 
     def reset(self):

@@ -1,0 +1,494 @@
+// Pass kernels, templated on the transform plan of the axis they transform (plan 0 = runtime
+// engine).  The per-voxel mode of a y pass is a run-time argument.  Global loads are gathered
+// into registers in batches before any shared-memory store, so each thread keeps many loads in
+// flight.
+#pragma once
+#include "fft_ct.cuh"
+#include "pk_internal.h"
+
+#define PK_EPS_F 2.220446049250313e-16f  // single(eps) = 2^-52
+
+namespace pkpass {
+using namespace pkfft;
+
+__device__ __forceinline__ int find_vol(const int* __restrict__ prefix, int nvol, int b) {
+    int lo = 0, hi = nvol - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (prefix[mid] <= b) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ float u16_of(float J) {
+    float r = roundf(J);             // half away from zero, like MATLAB uint16()
+    if (!(r >= 0.f)) r = 0.f;        // negatives and NaN -> 0
+    if (r > 65535.f) r = 65535.f;
+    return r;
+}
+
+// Ampere-style asynchronous global->shared copies (LDGSTS): issued without registers, completed
+// by commit/wait groups, so a CTA keeps its whole tile (and the epilogue's inputs) in flight.
+__device__ __forceinline__ void cp8(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp4(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp16(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// post-processing of one voxel and the cropped store (decon_lucy_omw_function.m:146-177)
+__device__ __forceinline__ void post_store(const VolDesc& d, float J, long long row, int y) {
+    const int x = (int)(row % d.nx);
+    const int z = (int)(row / d.nx);
+    if (y < d.bb0[0] || y > d.bb1[0] || x < d.bb0[1] || x > d.bb1[1] || z < d.bb0[2] || z > d.bb1[2]) return;
+    const long long vi = row * d.ny + y;
+    if (d.damp > 1.f) {
+        const float dI = __fmul_rn(d.damp, d.I[vi]);
+        const float a = (J <= dI) ? J : 0.f;
+        const float b = (J >= dI) ? dI : 0.f;
+        J = __fadd_rn(a, fminf(J, b));
+    }
+    if (d.scale_mode == 1) {
+        J = __fmul_rn(J, d.scale);
+    } else if (d.scale_mode == 2) {
+        int m = 1;
+        if (d.mask_mode == 1 || d.mask_mode == 3) m = d.mask8[vi] != 0;
+        else if (d.mask_mode == 2) {
+            const int E = d.erosion;
+            m = d.mask8[vi] != 0 && y >= E && y < d.ny - E && x >= E && x < d.nx - E && z >= E && z < d.nz - E;
+        }
+        J = __fmul_rn(__fadd_rn(__fmul_rn(J, d.scale), d.offset), (float)m);
+    }
+    const long long oy = d.bb1[0] - d.bb0[0] + 1, ox = d.bb1[1] - d.bb0[1] + 1;
+    const long long oi = (long long)(y - d.bb0[0]) + oy * ((long long)(x - d.bb0[1]) + ox * (long long)(z - d.bb0[2]));
+    if (d.save16) ((uint16_t*)d.out)[oi] = (uint16_t)u16_of(J);
+    else ((float*)d.out)[oi] = J;
+}
+
+__device__ __forceinline__ bool mode_from_spec(int m) {
+    return m == Y_RATIO || m == Y_UPDATE || m == Y_FINAL || m == Y_RLUPD || m == Y_RLFINAL || m == Y_C2R;
+}
+__device__ __forceinline__ bool mode_to_spec(int m) {
+    return m == Y_R2C || m == Y_PRE || m == Y_RATIO || m == Y_UPDATE || m == Y_RLPRE;
+}
+
+// Load two consecutive reals (even ny) or one (odd ny) of a float volume.
+__device__ __forceinline__ float2 ld2(const float* p, long long vi, bool odd) {
+    if (!odd) return *reinterpret_cast<const float2*>(p + vi);
+    return make_float2(p[vi], 0.f);
+}
+__device__ __forceinline__ void st2(float* p, long long vi, float2 v, bool odd) {
+    if (!odd) *reinterpret_cast<float2*>(p + vi) = v;
+    else p[vi] = v.x;
+}
+
+template <int P, bool INV>
+__device__ __forceinline__ void fft_y(float2* buf, const AxisDev& A, const float2* tw, int L, int tid) {
+    if constexpr (P == 0) {
+        TileGeom g{L, A.n, A.n, 1, false};
+        fft_lines<INV>(buf, A, tw, g, tid, PK_THREADS);
+    } else {
+        run_plan<P, 0, 1, plan_lines_y(kPlans[P].n), false, INV>(buf, tw, tid);
+    }
+}
+
+template <int P, bool INV>
+__device__ __forceinline__ void fft_xz(float2* buf, const AxisDev& A, const float2* tw, int T, int tid) {
+    if constexpr (P == 0) {
+        TileGeom g{T, A.n, 1, T, true};
+        fft_lines<INV>(buf, A, tw, g, tid, PK_THREADS);
+    } else {
+        run_plan<P, 0, 1, plan_cols_xz(kPlans[P].n), true, INV>(buf, tw, tid);
+    }
+}
+
+// Per-voxel operation of a y-pass mode on a pair of reals (x = element y, y = element y+1; for odd
+// ny only .x is live).  a0/a1 are the mode's gathered inputs for the same voxels.
+__device__ __forceinline__ float2 voxel_pair(const VolDesc& d, int mode, float2 c, float2 a0, float2 a1, long long row,
+                                             int y, bool two, float lam, double& acc0, double& acc1) {
+    float2 r = make_float2(0.f, 0.f);
+    const long long vi = row * d.ny + y;
+    switch (mode) {
+        case Y_R2C: r = a0; break;
+        case Y_RATIO:
+            r.x = __fdiv_rn(a0.x, fmaxf(c.x, PK_EPS_F));
+            r.y = two ? __fdiv_rn(a0.y, fmaxf(c.y, PK_EPS_F)) : 0.f;
+            break;
+        case Y_UPDATE:
+            r.x = fmaxf(__fmul_rn(c.x, a0.x), 0.f);
+            r.y = two ? fmaxf(__fmul_rn(c.y, a0.y), 0.f) : 0.f;
+            st2(d.Jn, vi, r, !two);
+            break;
+        case Y_FINAL:
+            post_store(d, fmaxf(__fmul_rn(c.x, a0.x), 0.f), row, y);
+            if (two) post_store(d, fmaxf(__fmul_rn(c.y, a0.y), 0.f), row, y + 1);
+            break;
+        case Y_RLPRE: {
+            r.x = fmaxf(__fadd_rn(a0.x, __fmul_rn(lam, __fsub_rn(a0.x, a1.x))), 0.f);
+            r.y = two ? fmaxf(__fadd_rn(a0.y, __fmul_rn(lam, __fsub_rn(a0.y, a1.y))), 0.f) : 0.f;
+            st2(d.Yb, vi, r, !two);
+            break;
+        }
+        case Y_RLUPD: {
+            float2 j2n, diff;
+            j2n.x = fmaxf(__fmul_rn(a0.x, c.x), 0.f);
+            j2n.y = two ? fmaxf(__fmul_rn(a0.y, c.y), 0.f) : 0.f;
+            diff.x = __fsub_rn(j2n.x, a0.x);
+            diff.y = __fsub_rn(j2n.y, a0.y);
+            if (!d.rl_first) {
+                acc0 += (double)__fmul_rn(diff.x, a1.x);
+                acc1 += (double)__fmul_rn(a1.x, a1.x);
+                if (two) {
+                    acc0 += (double)__fmul_rn(diff.y, a1.y);
+                    acc1 += (double)__fmul_rn(a1.y, a1.y);
+                }
+            }
+            st2(d.J4, vi, diff, !two);
+            st2(d.J2n, vi, j2n, !two);
+            break;
+        }
+        case Y_RLFINAL:
+            post_store(d, fmaxf(__fmul_rn(a0.x, c.x), 0.f), row, y);
+            if (two) post_store(d, fmaxf(__fmul_rn(a0.y, c.y), 0.f), row, y + 1);
+            break;
+        case Y_C2R: st2(d.dst, vi, c, !two); break;
+        default: break;
+    }
+    return r;
+}
+
+// Number of per-voxel input arrays a y-pass mode stages in shared memory.
+__host__ __device__ inline int y_aux_arrays(int mode) {
+    switch (mode) {
+        case Y_RLPRE: case Y_RLUPD: return 2;
+        case Y_C2R: return 0;
+        default: return 1;
+    }
+}
+
+template <int P>
+__global__ void __launch_bounds__(PK_THREADS, 3) k_y(const VolDesc* __restrict__ descs, const int* __restrict__ prefix,
+                                                     int nvol, int mode) {
+    extern __shared__ float2 smem[];
+    constexpr int NT = PK_THREADS;
+    const int vol = find_vol(prefix, nvol, blockIdx.x);
+    const VolDesc& d = descs[vol];
+    const int lb = blockIdx.x - prefix[vol];
+    const int tid = threadIdx.x;
+    const AxisDev& A = d.ay;
+    const int M = P == 0 ? d.M : kPlans[P].n;
+    const int L = P == 0 ? d.Ly : plan_lines_y(kPlans[P].n);
+    const bool odd = d.odd;
+    const int Py = d.Py, ny = d.ny;
+    // shared memory: tw[M] | twrc[M+1] (even ny) | buf[padded L*M] | nyq[L] | aux0[L*M] | aux1[L*M]
+    float2* tw = smem;
+    float2* twrc = smem + M;
+    float2* buf = twrc + (odd ? 0 : M + 1);
+    float2* nyq = buf + padded_size(L * M);
+    float2* aux0 = nyq + L;
+    float2* aux1 = aux0 + L * M;
+    const long long row0 = (long long)lb * L;
+    const int Lc = (int)min((long long)L, d.nrows - row0);
+    const bool spec_in = mode_from_spec(mode), spec_out = mode_to_spec(mode);
+
+    // ---- issue the asynchronous loads: group A = spectrum rows, group B = per-voxel inputs
+    if (spec_in) {
+        const float2* S0 = d.S + row0 * (long long)Py;
+        const int nin = Lc * Py;
+        for (int idx = tid; idx < nin; idx += NT) {
+            const int l = idx / Py, k = idx - l * Py;
+            if (!odd && k == M) cp8(&nyq[l], S0 + idx);
+            else cp8(&buf[pad(l * M + k)], S0 + idx);
+        }
+    }
+    cp_commit();
+    const float* pa0 = nullptr;
+    const float* pa1 = nullptr;
+    switch (mode) {
+        case Y_R2C: pa0 = d.src; break;
+        case Y_RATIO: pa0 = d.I; break;
+        case Y_UPDATE: case Y_FINAL: pa0 = d.Jo; break;
+        case Y_RLPRE: pa0 = d.J2; pa1 = d.J3; break;
+        case Y_RLUPD: pa0 = d.Yb; pa1 = d.rl_first ? nullptr : d.J4; break;
+        case Y_RLFINAL: pa0 = d.Yb; break;
+        default: break;
+    }
+    const int nvox = Lc * M;
+    const long long v0 = row0 * (long long)ny;
+    const bool raw_sync = mode == Y_PRE && (d.raw_type == PK_F64 || (d.raw_type == PK_U16 && odd));
+    if (mode == Y_PRE && !raw_sync) {
+        for (int idx = tid; idx < nvox; idx += NT) {
+            const int l = idx / M, k = idx - l * M;
+            const long long vi = v0 + (long long)l * ny + (odd ? k : 2 * k);
+            if (d.raw_type == PK_U16) cp4(&aux0[idx], (const uint16_t*)d.raw + vi);
+            else if (!odd) cp8(&aux0[idx], (const float*)d.raw + vi);
+            else cp4(&aux0[idx], (const float*)d.raw + vi);
+        }
+    } else if (pa0) {
+        for (int idx = tid; idx < nvox; idx += NT) {
+            const int l = idx / M, k = idx - l * M;
+            const long long vi = v0 + (long long)l * ny + (odd ? k : 2 * k);
+            if (!odd) {
+                cp8(&aux0[idx], pa0 + vi);
+                if (pa1) cp8(&aux1[idx], pa1 + vi);
+            } else {
+                cp4(&aux0[idx], pa0 + vi);
+                if (pa1) cp4(&aux1[idx], pa1 + vi);
+            }
+        }
+    }
+    cp_commit();
+    // tables (plain loads; they stay in L2)
+    for (int i = tid; i < M; i += NT) tw[i] = A.tw[i];
+    if (!odd)
+        for (int i = tid; i <= M; i += NT) twrc[i] = d.tw_rc[i];
+    double acc0 = 0.0, acc1 = 0.0;
+    unsigned zeros = 0;
+    const float lam = (mode == Y_RLPRE && d.lam_on) ? (float)d.partials[0] : 0.f;  // partials[0] = lambda
+
+    if (spec_in) {
+        cp_wait<1>();
+        __syncthreads();
+        // packed inverse sequence, in place: Z[k] = (X[k] + X*[M-k]) + i (X[k] - X*[M-k]) W_ny^{-k}
+        if (!odd) {
+            const int half = M / 2 + 1;
+            const int np = Lc * half;
+            for (int p = tid; p < np; p += NT) {
+                const int l = p / half, k = p - l * half;
+                const float2 xk = buf[pad(l * M + k)];
+                const float2 xm = k == 0 ? nyq[l] : buf[pad(l * M + (M - k))];
+                {
+                    const float2 a = xk, b = conjf2(xm);
+                    float2 w = twrc[k];
+                    w.y = -w.y;
+                    const float2 s2 = cadd(a, b), t2 = cmul(csub(a, b), w);
+                    buf[pad(l * M + k)] = make_float2(s2.x - t2.y, s2.y + t2.x);
+                }
+                if (k != 0 && 2 * k != M) {
+                    const float2 a = xm, b = conjf2(xk);
+                    float2 w = twrc[M - k];
+                    w.y = -w.y;
+                    const float2 s2 = cadd(a, b), t2 = cmul(csub(a, b), w);
+                    buf[pad(l * M + (M - k))] = make_float2(s2.x - t2.y, s2.y + t2.x);
+                }
+            }
+        } else {
+            const int nf = Lc * (ny - Py);
+            for (int p = tid; p < nf; p += NT) {
+                const int l = p / (ny - Py), k = Py + (p - l * (ny - Py));
+                buf[pad(l * M + k)] = conjf2(buf[pad(l * M + (ny - k))]);
+            }
+        }
+        __syncthreads();
+        fft_y<P, true>(buf, A, tw, L, tid);
+    }
+    cp_wait<0>();
+    __syncthreads();
+
+    // ---- per-voxel phase
+    for (int idx = tid; idx < nvox; idx += NT) {
+        const int l = idx / M, k = idx - l * M;
+        const long long row = row0 + l;
+        const int y = odd ? k : 2 * k;
+        float2 out;
+        if (mode == Y_PRE) {
+            // raw -> I = sat(raw - bg) (uint16) or max(raw - bg, 0); mask = raw ~= 0
+            const long long vi = row * (long long)ny + y;
+            float2 I;
+            bool nz0, nz1 = true;
+            if (d.raw_type == PK_U16) {
+                unsigned r0, r1 = 1;
+                if (!raw_sync) {
+                    const ushort2 q = *reinterpret_cast<const ushort2*>(&aux0[idx]);
+                    r0 = q.x;
+                    r1 = q.y;
+                } else {
+                    r0 = ((const uint16_t*)d.raw)[vi];
+                }
+                nz0 = r0 != 0;
+                nz1 = r1 != 0;
+                I.x = r0 > (unsigned)d.bg16 ? (float)(r0 - (unsigned)d.bg16) : 0.f;
+                I.y = r1 > (unsigned)d.bg16 ? (float)(r1 - (unsigned)d.bg16) : 0.f;
+            } else if (d.raw_type == PK_F32) {
+                const float2 r = aux0[idx];
+                nz0 = r.x != 0.f;
+                if (!odd) nz1 = r.y != 0.f;
+                I.x = fmaxf(__fsub_rn(r.x, d.bg_f), 0.f);
+                I.y = fmaxf(__fsub_rn(r.y, d.bg_f), 0.f);
+            } else {
+                const double* rp = (const double*)d.raw;
+                const double r0 = rp[vi], r1 = odd ? 1.0 : rp[vi + 1];
+                nz0 = r0 != 0.0;
+                nz1 = r1 != 0.0;
+                I.x = fmaxf(__fsub_rn((float)r0, d.bg_f), 0.f);
+                I.y = fmaxf(__fsub_rn((float)r1, d.bg_f), 0.f);
+            }
+            if (odd) {
+                I.y = 0.f;
+                nz1 = true;
+            }
+            st2(d.I, vi, I, odd);
+            if (d.write_mask) {
+                d.mask8[vi] = nz0 ? 1 : 0;
+                if (!odd) d.mask8[vi + 1] = nz1 ? 1 : 0;
+            }
+            zeros += (nz0 ? 0u : 1u) + (nz1 ? 0u : 1u);
+            out = I;
+        } else {
+            const float2 cval = spec_in ? buf[pad(idx)] : make_float2(0.f, 0.f);
+            out = voxel_pair(d, mode, cval, pa0 ? aux0[idx] : make_float2(0.f, 0.f), pa1 ? aux1[idx] : make_float2(0.f, 0.f),
+                             row, y, !odd, lam, acc0, acc1);
+        }
+        if (spec_out) buf[pad(idx)] = odd ? make_float2(out.x, 0.f) : out;
+    }
+
+    if (spec_out) {
+        __syncthreads();
+        fft_y<P, false>(buf, A, tw, L, tid);
+        const int nout = Lc * Py;
+        float2* S0 = d.S + row0 * (long long)Py;
+        for (int idx = tid; idx < nout; idx += NT) {
+            const int l = idx / Py, k = idx - l * Py;
+            float2 X;
+            if (!odd) {
+                const float2 zk = buf[pad(l * M + (k == M ? 0 : k))];
+                const float2 zc = conjf2(buf[pad(l * M + (k == 0 ? 0 : M - k))]);
+                const float2 fe = make_float2(0.5f * (zk.x + zc.x), 0.5f * (zk.y + zc.y));
+                const float2 df = csub(zk, zc);
+                const float2 fo = make_float2(0.5f * df.y, -0.5f * df.x);  // (zk - zc) / (2i)
+                X = cadd(fe, cmul(twrc[k], fo));
+            } else {
+                X = buf[pad(l * M + k)];
+            }
+            S0[idx] = X;
+        }
+    }
+
+    if (mode == Y_RLUPD) {
+        // deterministic block reduction of the two lambda sums
+        __shared__ double r0[NT], r1[NT];
+        r0[tid] = acc0;
+        r1[tid] = acc1;
+        __syncthreads();
+        for (int s = NT / 2; s > 0; s >>= 1) {
+            if (tid < s) {
+                r0[tid] += r0[tid + s];
+                r1[tid] += r1[tid + s];
+            }
+            __syncthreads();
+        }
+        if (tid == 0) {
+            d.partials[2 + 2 * lb] = r0[0];
+            d.partials[3 + 2 * lb] = r1[0];
+        }
+    }
+    if (mode == Y_PRE && d.zero_count) {
+        __shared__ unsigned zc;
+        if (tid == 0) zc = 0;
+        __syncthreads();
+        if (zeros) atomicAdd(&zc, zeros);
+        __syncthreads();
+        if (tid == 0 && zc) atomicAdd(d.zero_count, zc);
+    }
+}
+
+template <int P>
+__global__ void __launch_bounds__(PK_THREADS, 3) k_xz(const VolDesc* __restrict__ descs, const int* __restrict__ prefix,
+                                                      int nvol, int axis, int mode) {
+    extern __shared__ float2 smem[];
+    constexpr int NT = PK_THREADS;
+    const int vol = find_vol(prefix, nvol, blockIdx.x);
+    const VolDesc& d = descs[vol];
+    const int lb = blockIdx.x - prefix[vol];
+    const int tid = threadIdx.x;
+    const AxisDev& A = axis == 1 ? d.ax : d.az;
+    const int n = P == 0 ? A.n : kPlans[P].n;
+    const int T = P == 0 ? (axis == 1 ? d.Tx : d.Tz) : plan_cols_xz(kPlans[P].n);
+    const int Py = d.Py;
+    const int ctiles = (Py + T - 1) / T;
+    const int outer = lb / ctiles;
+    const int k0 = (lb - outer * ctiles) * T;
+    long long base, es;
+    if (axis == 1) { base = (long long)outer * d.nx * Py; es = Py; }
+    else { base = (long long)outer * Py; es = (long long)d.nx * Py; }
+    // shared memory: tw[n] | buf[padded T*n] | otf[T*n] (XZ_CONV)
+    float2* tw = smem;
+    float2* buf = smem + n;
+    float2* hbuf = buf + padded_size(T * n);
+    const int P_ = T * n;
+    const bool conv = mode == XZ_CONV;
+    for (int idx = tid; idx < P_; idx += NT) {
+        const int e = idx / T, t = idx - e * T;
+        if (k0 + t < Py) cp8(&buf[pad(idx)], d.S + base + e * es + k0 + t);
+        else buf[pad(idx)] = make_float2(0.f, 0.f);
+    }
+    cp_commit();
+    if (conv) {
+        for (int idx = tid; idx < P_; idx += NT) {
+            const int e = idx / T, t = idx - e * T;
+            if (k0 + t < Py) cp8(&hbuf[idx], d.otf + base + e * es + k0 + t);
+        }
+    }
+    cp_commit();
+    for (int i = tid; i < n; i += NT) tw[i] = A.tw[i];
+    cp_wait<1>();
+    __syncthreads();
+    if (mode == XZ_INV) fft_xz<P, true>(buf, A, tw, T, tid);
+    else fft_xz<P, false>(buf, A, tw, T, tid);
+    if (conv) {
+        cp_wait<0>();
+        __syncthreads();
+        const bool cj = d.conj;
+        for (int idx = tid; idx < P_; idx += NT) {
+            const int t = idx % T;
+            if (k0 + t < Py) {
+                float2 hv = hbuf[idx];
+                if (cj) hv.y = -hv.y;
+                buf[pad(idx)] = cmul(buf[pad(idx)], hv);
+            }
+        }
+        __syncthreads();
+        fft_xz<P, true>(buf, A, tw, T, tid);
+    }
+    const float sc = mode == XZ_FWD_SCALE ? d.xz_scale : 1.f;
+    for (int idx = tid; idx < P_; idx += NT) {
+        const int e = idx / T, t = idx - e * T;
+        if (k0 + t < Py) {
+            float2 v = buf[pad(idx)];
+            if (mode == XZ_FWD_SCALE) v = make_float2(v.x * sc, v.y * sc);
+            d.S[base + e * es + k0 + t] = v;
+        }
+    }
+}
+
+struct KernelTable {
+    void (*y[kNumPlans])(const VolDesc*, const int*, int, int);
+    void (*xz[kNumPlans])(const VolDesc*, const int*, int, int, int);
+};
+
+template <int P, int HI>
+struct Register {
+    static void fill(KernelTable& t) {
+        t.y[P] = k_y<P>;
+        t.xz[P] = k_xz<P>;
+        cudaFuncSetAttribute(k_y<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        cudaFuncSetAttribute(k_xz<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        Register<P + 1, HI>::fill(t);
+    }
+};
+template <int HI>
+struct Register<HI, HI> {
+    static void fill(KernelTable&) {}
+};
+
+}  // namespace pkpass

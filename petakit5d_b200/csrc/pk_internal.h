@@ -20,16 +20,19 @@
 #include "../../include/pkdecon.h"
 
 #define PK_MAXST 16   // max radix stages per axis
+#ifndef PK_PPT
 #define PK_PPT 16     // max complex points per thread per stage
+#endif
 
 // ------------------------------------------------------------------ device-visible structs
 struct AxisDev {
     int n;            // complex transform length along the axis
-    int nst;          // number of radix stages
+    int nst;          // number of radix stages (runtime engine)
     int rad[PK_MAXST];
-    const float2* tw; // tw[k] = exp(-2 pi i k / twN), k < twN (device, cached per twN)
-    int twN;          // table length
-    int twStride;     // twN / n
+    const float2* tw; // tw[k] = exp(-2 pi i k / n), k < n (device, cached per n)
+    int twN;          // table length (= n)
+    int twStride;     // 1
+    int plan;         // compile-time plan id (0 = runtime engine)
 };
 
 // Pass modes of the y kernel.
@@ -55,6 +58,7 @@ struct VolDesc {
     int odd;
     long long nrows;  // nx * nz
     int Ly, Tx, Tz;   // lines per CTA (y pass), k-columns per CTA (x / z passes)
+    const float2* tw_rc;  // exp(-2 pi i k / ny), k < ny: the real/half-spectrum split (even ny)
     int blocksY, blocksX, blocksZ;
     AxisDev ay, ax, az;
     // buffers
@@ -141,7 +145,7 @@ size_t pk_spec_elems(const VolDesc& d);   // complex elements of the half spectr
 // launch programs (passes.cu)
 enum { PK_STEP_Y = 0, PK_STEP_X = 1, PK_STEP_Z = 2, PK_STEP_LAMBDA = 3 };
 struct PkStep {
-    int kind = 0, mode = 0, nvol = 0, desc_off = 0, prefix_off = 0, grid = 0;
+    int kind = 0, mode = 0, plan = 0, nvol = 0, desc_off = 0, prefix_off = 0, grid = 0;
     size_t smem = 0;
 };
 struct PkProgram {

@@ -1,0 +1,85 @@
+// Compile-time transform plans.  Each entry is a transform length and its radix sequence; the pass
+// kernels are instantiated once per entry, so every stage runs with constant radix, stride and
+// twiddle step (straight-line code, no register spills).  Lengths without an entry use plan 0,
+// the runtime-radix engine (any length, slower).
+#pragma once
+
+#define PK_THREADS 256        // threads per pass CTA
+#define PK_TILE_POINTS 4096   // complex points one CTA holds (16 per thread)
+
+struct PlanDef {
+    int n;
+    int nst;
+    int rad[8];
+};
+
+// Radices 2/3/4/5/8/16 have register butterflies; 7, 9, 11, 13, 17 run as unrolled direct DFTs.
+constexpr PlanDef kPlans[] = {
+    {0, 0, {0}},                  // 0: runtime engine
+    {1, 0, {0}},
+    {2, 1, {2}},
+    {4, 1, {4}},
+    {8, 1, {8}},
+    {16, 1, {16}},
+    {32, 2, {16, 2}},
+    {64, 2, {16, 4}},
+    {128, 2, {16, 8}},
+    {256, 2, {16, 16}},
+    {512, 3, {16, 16, 2}},
+    {1024, 3, {16, 16, 4}},
+    {2048, 3, {16, 16, 8}},
+    {4096, 3, {16, 16, 16}},
+    {48, 2, {16, 3}},
+    {80, 2, {16, 5}},
+    {96, 3, {16, 2, 3}},
+    {112, 2, {16, 7}},
+    {144, 2, {16, 9}},
+    {160, 3, {16, 2, 5}},
+    {176, 2, {16, 11}},
+    {180, 3, {4, 9, 5}},
+    {192, 3, {16, 4, 3}},
+    {208, 2, {16, 13}},
+    {210, 4, {2, 3, 5, 7}},
+    {224, 3, {16, 2, 7}},
+    {240, 3, {16, 3, 5}},
+    {272, 2, {16, 17}},
+    {288, 3, {16, 2, 9}},
+    {320, 3, {16, 4, 5}},
+    {352, 3, {16, 2, 11}},
+    {360, 3, {8, 9, 5}},
+    {384, 3, {16, 8, 3}},
+    {416, 3, {16, 2, 13}},
+    {420, 4, {4, 3, 5, 7}},
+    {448, 3, {16, 4, 7}},
+    {480, 4, {16, 2, 3, 5}},
+    {544, 3, {16, 2, 17}},
+    {576, 3, {16, 4, 9}},
+    {640, 3, {16, 8, 5}},
+    {720, 3, {16, 9, 5}},
+    {768, 3, {16, 16, 3}},
+    {960, 4, {16, 4, 3, 5}},
+    {1152, 3, {16, 8, 9}},
+    {1280, 3, {16, 16, 5}},
+    {1536, 4, {16, 16, 2, 3}},
+};
+constexpr int kNumPlans = sizeof(kPlans) / sizeof(kPlans[0]);
+
+constexpr int plan_product(int p) {
+    int v = 1;
+    for (int i = 0; i < kPlans[p].nst; i++) v *= kPlans[p].rad[i];
+    return v;
+}
+
+// Lines (y pass, contiguous) and columns (x/z passes, a power of two for sector-aligned rows) per tile.
+constexpr int plan_lines_y(int n) { return n >= 1 ? (PK_TILE_POINTS / n > 0 ? PK_TILE_POINTS / n : 1) : 1; }
+constexpr int plan_cols_xz(int n) {
+    int t = 1;
+    while (t * 2 * n <= PK_TILE_POINTS) t *= 2;
+    return t;
+}
+
+inline int pk_find_plan(int n) {
+    for (int p = 1; p < kNumPlans; p++)
+        if (kPlans[p].n == n && plan_product(p) == n) return p;
+    return 0;
+}
