@@ -281,6 +281,11 @@ static void set_post(VolDesc& d, const pk_decon_params* p, int mask_mode, void* 
             d.bb1[i] = (int)p->bbox[i + 3] - 1;
         }
     }
+    const int dims[3] = {d.ny, d.nx, d.nz};
+    d.crop = 0;
+    for (int i = 0; i < 3; i++)
+        if (d.bb0[i] != 0 || d.bb1[i] != dims[i] - 1) d.crop = 1;
+    d.need_xz = d.crop || d.mask_mode == 2;
 }
 
 pk_status pk_check_params(const int64_t dims[3], const pk_decon_params* p) {

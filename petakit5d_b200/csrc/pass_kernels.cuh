@@ -46,12 +46,17 @@ __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_grou
 template <int N>
 __device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-// post-processing of one voxel and the cropped store (decon_lucy_omw_function.m:146-177)
+// post-processing of one voxel and the cropped store (decon_lucy_omw_function.m:146-177).
+// x/z of the row are only derived when a crop box or the border-erosion mask needs them.
 __device__ __forceinline__ void post_store(const VolDesc& d, float J, long long row, int y) {
-    const int x = (int)(row % d.nx);
-    const int z = (int)(row / d.nx);
-    if (y < d.bb0[0] || y > d.bb1[0] || x < d.bb0[1] || x > d.bb1[1] || z < d.bb0[2] || z > d.bb1[2]) return;
     const long long vi = row * d.ny + y;
+    int x = 0, z = 0;
+    if (d.need_xz) {
+        const unsigned r = (unsigned)row;
+        z = (int)(r / (unsigned)d.nx);
+        x = (int)(r - (unsigned)z * (unsigned)d.nx);
+        if (y < d.bb0[0] || y > d.bb1[0] || x < d.bb0[1] || x > d.bb1[1] || z < d.bb0[2] || z > d.bb1[2]) return;
+    }
     if (d.damp > 1.f) {
         const float dI = __fmul_rn(d.damp, d.I[vi]);
         const float a = (J <= dI) ? J : 0.f;
@@ -69,8 +74,11 @@ __device__ __forceinline__ void post_store(const VolDesc& d, float J, long long 
         }
         J = __fmul_rn(__fadd_rn(__fmul_rn(J, d.scale), d.offset), (float)m);
     }
-    const long long oy = d.bb1[0] - d.bb0[0] + 1, ox = d.bb1[1] - d.bb0[1] + 1;
-    const long long oi = (long long)(y - d.bb0[0]) + oy * ((long long)(x - d.bb0[1]) + ox * (long long)(z - d.bb0[2]));
+    long long oi = vi;
+    if (d.crop) {
+        const long long oy = d.bb1[0] - d.bb0[0] + 1, ox = d.bb1[1] - d.bb0[1] + 1;
+        oi = (long long)(y - d.bb0[0]) + oy * ((long long)(x - d.bb0[1]) + ox * (long long)(z - d.bb0[2]));
+    }
     if (d.save16) ((uint16_t*)d.out)[oi] = (uint16_t)u16_of(J);
     else ((float*)d.out)[oi] = J;
 }

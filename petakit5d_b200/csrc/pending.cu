@@ -3,14 +3,6 @@
 
 extern "C" {
 
-pk_status pk_omw_backprojector(pk_ctx*, const float*, const int64_t[3], double, int32_t, double, double, double,
-                               double, double, float*, float*, float*, uint8_t*) {
-    return pk_fail(PK_ERR_UNSUPPORTED, "pk_omw_backprojector: not built yet");
-}
-pk_status pk_wb_backprojector(pk_ctx*, const float*, const int64_t[3], double, double, int32_t, int32_t,
-                              const double[3], double*, double*) {
-    return pk_fail(PK_ERR_UNSUPPORTED, "pk_wb_backprojector: not built yet");
-}
 pk_status pk_batch_decon(pk_ctx*, int32_t, int32_t, const pk_chunk*, pk_dtype, int32_t, const float* const*,
                          const float* const*, const int64_t*, int32_t, const pk_decon_params*, int32_t, int32_t) {
     return pk_fail(PK_ERR_UNSUPPORTED, "pk_batch_decon: not built yet");

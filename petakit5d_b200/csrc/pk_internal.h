@@ -84,6 +84,8 @@ struct VolDesc {
     float damp; float scale; float offset; int erosion; int scale_mode; // scale_mode: 0 none, 1 scale, 2 (J*s+o)*mask
     int save16; void* out;
     int bb0[3], bb1[3];              // 0-based inclusive crop box (y, x, z)
+    int crop;                        // crop box smaller than the volume
+    int need_xz;                     // post needs x/z of a voxel (crop or border erosion)
 };
 
 // ------------------------------------------------------------------ host side
