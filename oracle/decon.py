@@ -93,7 +93,7 @@ def preprocess(I, background, need_mask, dtype=np.float32):
         out = np.where(I > b, I.astype(np.int64) - b, 0).astype(dtype)
     else:
         x = I.astype(dtype)
-        out = np.maximum(x - dtype(bg), dtype(0))
+        out = np.fmax(x - dtype(bg), dtype(0))          # MATLAB max ignores NaN
     return out, mask
 
 
@@ -212,9 +212,9 @@ def decon_lucy_omw(I, psf_f, psf_b, numit, background=None, save16bit=True, damp
     J = Ipre
     for _ in range(int(numit)):                                # :105-113
         CX = conv_half(J, otf_f)
-        CX = np.maximum(CX, eps)
+        CX = np.fmax(CX, eps)
         J = conv_half(Ipre / CX, otf_b) * J
-        J = np.maximum(J, dtype(0))
+        J = np.fmax(J, dtype(0))
     if return_float:
         return J
     return postprocess(J, Ipre, I_mask, damp, scale, offset, edge_erosion, save16bit, bbox)
@@ -243,11 +243,11 @@ def decon_lucy(I, psf, numit, background=None, save16bit=True, damp=1.0, scale=1
             J4 = J2 - Y
         elif k == 2:                                           # :129-130
             J4 = J2 - Y
-        Y = np.maximum(J2 + dtype(lam) * (J2 - J3), dtype(0))   # :132
-        RB = np.maximum(conv_half(Y, H), eps)                  # :136
+        Y = np.fmax(J2 + dtype(lam) * (J2 - J3), dtype(0))      # :132
+        RB = np.fmax(conv_half(Y, H), eps)                     # :136
         RB = Ipre / RB                                         # :138
         J3 = J2                                                # :141
-        J2 = np.maximum(Y * conv_half(RB, Hc), dtype(0))        # :142
+        J2 = np.fmax(Y * conv_half(RB, Hc), dtype(0))           # :142
         if lambdas is not None:
             lambdas.append(lam)
     if return_float:
@@ -256,6 +256,7 @@ def decon_lucy(I, psf, numit, background=None, save16bit=True, damp=1.0, scale=1
 
 
 def rel_l2(a, b):
-    a = np.asarray(a, dtype=np.float64)
-    b = np.asarray(b, dtype=np.float64)
+    cplx = np.iscomplexobj(a) or np.iscomplexobj(b)
+    a = np.asarray(a, dtype=np.complex128 if cplx else np.float64)
+    b = np.asarray(b, dtype=np.complex128 if cplx else np.float64)
     return float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-300))

@@ -1,0 +1,127 @@
+"""Chunked deconvolution: the callers of the hot path for volumes split into overlapping chunks.
+
+* ``find_good_factor_number``  -- utils/findGoodFactorNumber.m:1-26
+* ``zarr_chunk_coordinates``   -- microscopeDataProcessing/stitch/XR_zarrChunkCoordinatesExtraction.m:1-83
+* ``border_size``              -- ``round((size(psf)+10)/2)`` (RLdecon_large_in_memory.m:177)
+* ``batch_decon``              -- many chunks in shared launches (pk_batch_decon)
+* ``decon_large_in_memory``    -- RLdecon_large_in_memory.m:177-260: chunk grid with borders, decon of
+                                  every chunk cropped to its region (deconBbox), paste back
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import PK_F32, PK_F64, PK_U16, Chunk, check, i64x3, lib, ptr
+from .decon import _params, _parse, _psf
+
+
+def find_good_factor_number(n, direction=1, allow_odd_seven=False):
+    return int(lib.pk_find_good_factor_number(int(n), int(direction), 1 if allow_odd_seven else 0))
+
+
+def border_size(psf_size):
+    return [int(np.floor((s + 10) / 2.0 + 0.5)) for s in psf_size]
+
+
+def zarr_chunk_coordinates(vol_size, batch_size=(1024, 1024, 1024), block_size=(256, 256, 256), bbox=None,
+                           same_batch_size=True, border=50):
+    """(batchBBoxes, regionBBoxes, localBBoxes) as n x 6 int64 arrays, 1-based inclusive."""
+    border = list(np.broadcast_to(np.asarray(border, dtype=np.int64), (3,)))
+    block = list(np.broadcast_to(np.asarray(block_size, dtype=np.int64), (3,)))
+    bb = None
+    if bbox is not None and len(bbox) == 6:
+        bb = (C.c_int64 * 6)(*[int(v) for v in bbox])
+    n = lib.pk_chunk_coordinates(i64x3(vol_size), i64x3(batch_size), i64x3(block), bb, 1 if same_batch_size else 0,
+                                 i64x3(border), None, None, None)
+    if n < 0:
+        raise ValueError("invalid chunk grid arguments")
+    out = [np.zeros((n, 6), np.int64) for _ in range(3)]
+    lib.pk_chunk_coordinates(i64x3(vol_size), i64x3(batch_size), i64x3(block), bb, 1 if same_batch_size else 0,
+                             i64x3(border), ptr(out[0]), ptr(out[1]), ptr(out[2]))
+    return tuple(out)
+
+
+_TYPES = {np.dtype(np.uint16): PK_U16, np.dtype(np.float32): PK_F32, np.dtype(np.float64): PK_F64}
+
+
+def batch_decon(chunks, psfs, psf_ids, numit=2, method="omw", psfs_b=None, bboxes=None, pad_good=False, ctx=None,
+                outputs=None, **kw):
+    """Deconvolve ``chunks`` (list of [y, x, z] arrays of one dtype) in shared launches.
+
+    ``psfs[psf_ids[i]]`` (and ``psfs_b[...]`` for OMW) is chunk i's PSF pair; ``bboxes[i]`` its 1-based
+    inclusive output crop (deconBbox) or None.  Returns the list of outputs (uint16 when save16bit).
+    For the host->device copies to overlap the compute, pass chunks in pinned memory.
+    """
+    opts, _ = _parse(dict(kw))
+    ctx = ctx or _lib.default_context()
+    m = {"omw": 1, "rl": 0}[method]
+    if m == 1 and psfs_b is None:
+        raise ValueError("OMW needs backprojectors (psfs_b)")
+    vols = [np.asfortranarray(c) for c in chunks]
+    dt = {v.dtype for v in vols}
+    if len(dt) != 1 or next(iter(dt)) not in _TYPES:
+        raise ValueError("all chunks must share one dtype among uint16/float32/float64")
+    t = _TYPES[next(iter(dt))]
+    pf = [_psf(p) for p in psfs]
+    shapes = {p.shape for p in pf}
+    pb = [_psf(p) for p in psfs_b] if psfs_b is not None else None
+    if pb is not None:
+        for a, b in zip(pf, pb):
+            if a.shape != b.shape:
+                raise ValueError("PSF_f and PSF_b of one id must have the same size")
+    del shapes
+    p = _params(opts)
+    n = len(vols)
+    arr = (Chunk * n)()
+    outs = []
+    for i, v in enumerate(vols):
+        q = _params(opts)
+        bb = None if bboxes is None else bboxes[i]
+        if bb is not None and len(bb) == 6:
+            q.has_bbox = 1
+            for k in range(6):
+                q.bbox[k] = int(bb[k])
+        od = i64x3([0, 0, 0])
+        check(lib.pk_output_dims(i64x3(v.shape), q, od))
+        o = outputs[i] if outputs is not None else np.empty(tuple(od), np.uint16 if p.save16bit else np.float32, order="F")
+        outs.append(o)
+        arr[i].in_ = v.ctypes.data
+        arr[i].dims = i64x3(v.shape)
+        arr[i].psf_id = int(psf_ids[i])
+        arr[i].has_bbox = q.has_bbox
+        for k in range(6):
+            arr[i].bbox[k] = q.bbox[k]
+        arr[i].out = o.ctypes.data
+    npsf = len(pf)
+    fptrs = (C.c_void_p * npsf)(*[a.ctypes.data for a in pf])
+    bptrs = (C.c_void_p * npsf)(*[a.ctypes.data for a in pb]) if pb is not None else None
+    dims = np.array([list(a.shape) for a in pf], dtype=np.int64).ravel()
+    check(lib.pk_batch_decon(ctx.handle, m, n, arr, t, npsf, fptrs, bptrs, dims.ctypes.data, int(numit), p,
+                             1 if pad_good else 0, 0))
+    return outs
+
+
+def decon_large_in_memory(volume, psf, numit=2, method="omw", psf_b=None, batch_size=(512, 512, 512), ctx=None,
+                          pad_good=False, **kw):
+    """RLdecon_large_in_memory.m:177-260 on one GPU: chunk grid with BorderSize = round((size(psf)+10)/2)
+    (sameBatchSize false), every chunk deconvolved and cropped to its region, pasted into the output."""
+    vol = np.asfortranarray(volume)
+    border = border_size(np.asarray(psf).shape[:3])
+    bb, rb, _ = zarr_chunk_coordinates(vol.shape, batch_size=batch_size, block_size=batch_size, same_batch_size=False,
+                                       border=border)
+    chunks, boxes = [], []
+    for b, r in zip(bb, rb):
+        chunks.append(np.asfortranarray(vol[b[0] - 1:b[3], b[1] - 1:b[4], b[2] - 1:b[5]]))
+        st = r[:3] - b[:3] + 1
+        en = r[3:] - b[:3] + 1
+        boxes.append([*st, *en])
+    outs = batch_decon(chunks, [psf], [0] * len(chunks), numit, method, [psf_b] if psf_b is not None else None,
+                       boxes, pad_good, ctx, **kw)
+    save16 = kw.get("save16bit", kw.get("Save16bit", True))
+    out = np.empty(vol.shape, np.uint16 if save16 else np.float32, order="F")
+    for r, o in zip(rb, outs):
+        out[r[0] - 1:r[3], r[1] - 1:r[4], r[2] - 1:r[5]] = o
+    return out

@@ -212,8 +212,8 @@ pk_status pk_scratch(pk_ctx* ctx, int slot, size_t bytes, void** ptr) {
     return PK_OK;
 }
 
-enum { SL_I = 0, SL_J = 1, SL_JB = 2, SL_Y = 3, SL_J4 = 4, SL_S = 5, SL_MASK = 6, SL_MASK2 = 7, SL_PART = 8,
-       SL_IN = 9, SL_OUT = 10, SL_PSF = 11, SL_SUM = 12, SL_OFFS = 13 };
+enum { SL_ARENA = 0, SL_JB = 2, SL_S = 5, SL_MASK2 = 7, SL_IN = 9, SL_OUT = 10, SL_PSF = 11, SL_SUM = 12,
+       SL_OFFS = 13, SL_ZC = 14 };
 
 // Half-spectrum OTF of a PSF at the volume size, scaled by `scale` (1/N for the iterations).
 pk_status pk_make_otf(pk_ctx* ctx, const float* h_psf, const int64_t pd[3], int ny, int nx, int nz, double scale,
@@ -264,7 +264,7 @@ pk_status pk_get_otf(pk_ctx* ctx, const float* h_psf, const int64_t pd[3], int n
     return PK_OK;
 }
 
-static void set_post(VolDesc& d, const pk_decon_params* p, int mask_mode, void* d_out) {
+void set_post(VolDesc& d, const pk_decon_params* p, int mask_mode, void* d_out) {
     const bool off = p->decon_offset != 0.0, ero = p->edge_erosion > 0;
     d.damp = (float)p->damp_factor;
     d.scale = (float)p->scale_factor;
@@ -300,6 +300,197 @@ pk_status pk_check_params(const int64_t dims[3], const pk_decon_params* p) {
     return PK_OK;
 }
 
+// ------------------------------------------------------------------ multi-volume runner
+// Bytes of the work buffers one job needs (256-byte aligned pieces).
+static size_t al256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+size_t pk_job_bytes(int method, const int dims[3], bool need_mask, int blocksY) {
+    const size_t N = (size_t)dims[0] * dims[1] * dims[2];
+    const size_t spec = sizeof(float2) * (size_t)(dims[0] / 2 + 1) * dims[1] * dims[2];
+    size_t b = al256(4 * N) * 2 + al256(spec);                       // I, J, S
+    if (method == 0) b += al256(4 * N) * 3 + al256(sizeof(double) * (2 + 2 * (size_t)blocksY));  // JB, Y, J4, partials
+    if (need_mask) b += al256(N);
+    return b;
+}
+
+void pk_job_carve(DeconJob& j, int method, bool need_mask, int blocksY, char* arena) {
+    const size_t N = (size_t)j.dims[0] * j.dims[1] * j.dims[2];
+    const size_t spec = sizeof(float2) * (size_t)(j.dims[0] / 2 + 1) * j.dims[1] * j.dims[2];
+    size_t o = 0;
+    auto take = [&](size_t b) { char* p = arena + o; o += al256(b); return p; };
+    j.I = (float*)take(4 * N);
+    j.J = (float*)take(4 * N);
+    j.S = (float2*)take(spec);
+    if (method == 0) {
+        j.JB = (float*)take(4 * N);
+        j.Yb = (float*)take(4 * N);
+        j.J4 = (float*)take(4 * N);
+        j.part = (double*)take(sizeof(double) * (2 + 2 * (size_t)blocksY));
+    }
+    if (need_mask) j.mask = (uint8_t*)take(N);
+}
+
+static void set_post_job(VolDesc& d, const pk_decon_params* p, int mask_mode, const DeconJob& j) {
+    pk_decon_params q = *p;
+    q.has_bbox = j.has_bbox;
+    for (int i = 0; i < 6; i++) q.bbox[i] = j.bbox[i];
+    if (!j.has_bbox && (j.rdims[0] != j.dims[0] || j.rdims[1] != j.dims[1] || j.rdims[2] != j.dims[2])) {
+        // padded transform: the output is the raw extent
+        q.has_bbox = 1;
+        for (int i = 0; i < 3; i++) {
+            q.bbox[i] = 1;
+            q.bbox[i + 3] = j.rdims[i];
+        }
+    }
+    set_post(d, &q, mask_mode, j.d_out);
+}
+
+pk_status pk_decon_multi(pk_ctx* ctx, int method, std::vector<DeconJob>& jobs, pk_dtype in_type, int numit,
+                         const pk_decon_params* p, cudaStream_t st) {
+    pk_status s;
+    if (numit < 0) return pk_fail(PK_ERR_INVALID, "NUMIT must be non-negative");
+    const size_t nj = jobs.size();
+    if (nj == 0) return PK_OK;
+    const bool need_mask = p->decon_offset != 0.0 || p->edge_erosion > 0;
+    std::vector<VolDesc> base(nj);
+    unsigned int* zc = nullptr;
+    if (p->edge_erosion > 0) {
+        void* z;
+        if ((s = pk_scratch(ctx, SL_ZC, sizeof(unsigned int) * nj, &z)) != PK_OK) return s;
+        zc = (unsigned int*)z;
+        PK_CUDA(cudaMemsetAsync(zc, 0, sizeof(unsigned int) * nj, st));
+    }
+    double b16 = std::floor(std::fabs(p->background) + 0.5);
+    if (p->background < 0 || !(b16 == b16)) b16 = 0;
+    for (size_t i = 0; i < nj; i++) {
+        DeconJob& j = jobs[i];
+        VolDesc& d = base[i];
+        if ((s = pk_init_desc(ctx, j.dims[0], j.dims[1], j.dims[2], &d)) != PK_OK) return s;
+        d.raw = j.d_raw;
+        d.raw_type = in_type;
+        for (int k = 0; k < 3; k++) d.rdims[k] = j.rdims[k];
+        d.padded = j.rdims[0] != j.dims[0] || j.rdims[1] != j.dims[1] || j.rdims[2] != j.dims[2];
+        d.bg_f = (float)p->background;
+        d.bg16 = (int)std::min(b16, 65535.0);
+        d.I = j.I;
+        d.mask8 = j.mask;
+        d.write_mask = need_mask ? 1 : 0;
+        d.zero_count = zc ? zc + i : nullptr;
+        d.S = j.S;
+        d.partials = j.part;
+    }
+    PkProgram prog;
+    pk_program_add(prog, PK_STEP_Y, Y_PRE, base);
+    std::vector<int> mask_mode(nj, need_mask ? 1 : 0);
+    if (p->edge_erosion > 0) {
+        // the erosion branch depends on whether the raw mask is full (decon_mask_edge_erosion.m:8)
+        if ((s = pk_program_upload(ctx, prog, st)) != PK_OK) return s;
+        if ((s = pk_program_launch(ctx, prog, st)) != PK_OK) return s;
+        prog = PkProgram();
+        std::vector<unsigned int> zeros(nj, 0);
+        PK_CUDA(cudaMemcpyAsync(zeros.data(), zc, sizeof(unsigned int) * nj, cudaMemcpyDeviceToHost, st));
+        PK_CUDA(cudaStreamSynchronize(st));
+        std::vector<int2> disk = pk_disk_offsets(p->edge_erosion - 1);
+        for (size_t i = 0; i < nj; i++) {
+            if (zeros[i] == 0) { mask_mode[i] = 2; continue; }
+            mask_mode[i] = 3;
+            DeconJob& j = jobs[i];
+            const int ny = j.dims[0], nx = j.dims[1], nz = j.dims[2];
+            const size_t N = (size_t)ny * nx * nz;
+            void *m2, *offs;
+            if ((s = pk_scratch(ctx, SL_MASK2, N, &m2)) != PK_OK) return s;
+            if ((s = pk_scratch(ctx, SL_OFFS, sizeof(int2) * disk.size(), &offs)) != PK_OK) return s;
+            PK_CUDA(cudaMemcpyAsync(offs, disk.data(), sizeof(int2) * disk.size(), cudaMemcpyHostToDevice, st));
+            k_mask_faces<<<grid_for((long long)N), 256, 0, st>>>(j.mask, ny, nx, nz);
+            k_erode_xy<<<grid_for((long long)N), 256, 0, st>>>(j.mask, (uint8_t*)m2, ny, nx, nz, (const int2*)offs,
+                                                                (int)disk.size());
+            k_erode_z<<<grid_for((long long)N), 256, 0, st>>>((const uint8_t*)m2, j.mask, ny, nx, nz, p->edge_erosion - 1);
+            PK_CUDA(cudaGetLastError());
+            PK_CUDA(cudaStreamSynchronize(st));  // the offsets are a host temporary, m2 is reused
+        }
+    }
+    for (VolDesc& d : base) {
+        d.raw = nullptr;
+        d.zero_count = nullptr;
+        d.write_mask = 0;
+    }
+    if (numit == 0) {
+        if (!prog.steps.empty()) {
+            if ((s = pk_program_upload(ctx, prog, st)) != PK_OK) return s;
+            if ((s = pk_program_launch(ctx, prog, st)) != PK_OK) return s;
+        }
+        for (size_t i = 0; i < nj; i++) {
+            VolDesc f = base[i];
+            set_post_job(f, p, mask_mode[i], jobs[i]);
+            k_post_identity<<<grid_for((long long)f.nrows * f.ny), 256, 0, st>>>(f);
+            PK_CUDA(cudaGetLastError());
+        }
+        return PK_OK;
+    }
+    auto with = [&](auto fn) {
+        std::vector<VolDesc> v(nj);
+        for (size_t i = 0; i < nj; i++) {
+            v[i] = base[i];
+            fn(v[i], jobs[i], (int)i);
+        }
+        return v;
+    };
+    auto conv = [&](int which) {
+        pk_program_add(prog, PK_STEP_X, XZ_FWD, base);
+        pk_program_add(prog, PK_STEP_Z, XZ_CONV, with([&](VolDesc& d, DeconJob& j, int) {
+            if (method == 1) { d.otf = which ? j.otf_b : j.otf_f; d.conj = 0; }
+            else { d.otf = j.otf_f; d.conj = which; }
+        }));
+        pk_program_add(prog, PK_STEP_X, XZ_INV, base);
+    };
+    if (method == 1) {
+        for (int it = 1; it <= numit; it++) {
+            conv(0);
+            pk_program_add(prog, PK_STEP_Y, Y_RATIO, base);
+            conv(1);
+            const bool last = it == numit;
+            pk_program_add(prog, PK_STEP_Y, last ? Y_FINAL : Y_UPDATE, with([&](VolDesc& d, DeconJob& j, int i) {
+                d.Jo = it == 1 ? j.I : j.J;
+                d.Jn = j.J;
+                if (last) set_post_job(d, p, mask_mode[i], j);
+            }));
+        }
+    } else {
+        for (int k = 1; k <= numit; k++) {
+            if (k >= 2) {
+                pk_program_add(prog, PK_STEP_Y, Y_RLPRE, with([&](VolDesc& d, DeconJob& j, int) {
+                    float* Jb[2] = {j.J, j.JB};
+                    d.J2 = Jb[k % 2];
+                    d.J3 = k == 2 ? j.I : Jb[(k - 1) % 2];
+                    d.Yb = j.Yb;
+                    d.lam_on = k >= 3 ? 1 : 0;
+                }));
+            }
+            conv(0);
+            pk_program_add(prog, PK_STEP_Y, Y_RATIO, base);
+            conv(1);
+            if (k < numit) {
+                auto u = with([&](VolDesc& d, DeconJob& j, int) {
+                    float* Jb[2] = {j.J, j.JB};
+                    d.Yb = k == 1 ? j.I : j.Yb;
+                    d.J4 = j.J4;
+                    d.rl_first = k == 1 ? 1 : 0;
+                    d.J2n = Jb[(k + 1) % 2];
+                });
+                pk_program_add(prog, PK_STEP_Y, Y_RLUPD, u);
+                pk_program_add(prog, PK_STEP_LAMBDA, 0, u);
+            } else {
+                pk_program_add(prog, PK_STEP_Y, Y_RLFINAL, with([&](VolDesc& d, DeconJob& j, int i) {
+                    d.Yb = k == 1 ? j.I : j.Yb;
+                    set_post_job(d, p, mask_mode[i], j);
+                }));
+            }
+        }
+    }
+    if ((s = pk_program_upload(ctx, prog, st)) != PK_OK) return s;
+    return pk_program_launch(ctx, prog, st);
+}
+
 pk_status pk_decon_run(pk_ctx* ctx, int method, const void* d_in, pk_dtype in_type, const int64_t dims[3],
                        const float* psf_f, const int64_t psf_f_dims[3], const float* psf_b,
                        const int64_t psf_b_dims[3], int numit, const pk_decon_params* p, void* d_out,
@@ -307,148 +498,21 @@ pk_status pk_decon_run(pk_ctx* ctx, int method, const void* d_in, pk_dtype in_ty
     pk_status s;
     if ((s = pk_check_params(dims, p)) != PK_OK) return s;
     if (numit < 0) return pk_fail(PK_ERR_INVALID, "NUMIT must be non-negative");
-    const int ny = (int)dims[0], nx = (int)dims[1], nz = (int)dims[2];
-    const size_t N = (size_t)ny * nx * nz;
+    DeconJob j;
+    for (int i = 0; i < 3; i++) j.dims[i] = j.rdims[i] = (int)dims[i];
     VolDesc d;
-    if ((s = pk_init_desc(ctx, ny, nx, nz, &d)) != PK_OK) return s;
-    const float2 *otf_f = nullptr, *otf_b = nullptr;
-    if ((s = pk_get_otf(ctx, psf_f, psf_f_dims, ny, nx, nz, &otf_f, st)) != PK_OK) return s;
-    if (method == 1 && (s = pk_get_otf(ctx, psf_b, psf_b_dims, ny, nx, nz, &otf_b, st)) != PK_OK) return s;
-    void *I, *J, *JB = nullptr, *Yb = nullptr, *J4 = nullptr, *S, *mask = nullptr, *part = nullptr;
-    if ((s = pk_scratch(ctx, SL_I, sizeof(float) * N, &I)) != PK_OK) return s;
-    if ((s = pk_scratch(ctx, SL_J, sizeof(float) * N, &J)) != PK_OK) return s;
-    if ((s = pk_scratch(ctx, SL_S, sizeof(float2) * pk_spec_elems(d), &S)) != PK_OK) return s;
-    if (method == 0) {
-        if ((s = pk_scratch(ctx, SL_JB, sizeof(float) * N, &JB)) != PK_OK) return s;
-        if ((s = pk_scratch(ctx, SL_Y, sizeof(float) * N, &Yb)) != PK_OK) return s;
-        if ((s = pk_scratch(ctx, SL_J4, sizeof(float) * N, &J4)) != PK_OK) return s;
-        if ((s = pk_scratch(ctx, SL_PART, sizeof(double) * (2 + 2 * (size_t)d.blocksY), &part)) != PK_OK) return s;
-    }
+    if ((s = pk_init_desc(ctx, j.dims[0], j.dims[1], j.dims[2], &d)) != PK_OK) return s;
+    if ((s = pk_get_otf(ctx, psf_f, psf_f_dims, j.dims[0], j.dims[1], j.dims[2], &j.otf_f, st)) != PK_OK) return s;
+    if (method == 1 && (s = pk_get_otf(ctx, psf_b, psf_b_dims, j.dims[0], j.dims[1], j.dims[2], &j.otf_b, st)) != PK_OK)
+        return s;
     const bool need_mask = p->decon_offset != 0.0 || p->edge_erosion > 0;
-    if (need_mask && (s = pk_scratch(ctx, SL_MASK, N, &mask)) != PK_OK) return s;
-    unsigned int* zc = nullptr;
-    if (p->edge_erosion > 0) {
-        if (!ctx->d_counter) PK_CUDA(cudaMalloc(&ctx->d_counter, sizeof(unsigned int)));
-        zc = ctx->d_counter;
-        PK_CUDA(cudaMemsetAsync(zc, 0, sizeof(unsigned int), st));
-    }
-
-    // first pass: raw -> I (and the mask), S = R2C(I)
-    d.raw = d_in;
-    d.raw_type = in_type;
-    d.bg_f = (float)p->background;
-    {
-        double b = std::floor(std::fabs(p->background) + 0.5);
-        if (p->background < 0) b = 0;
-        if (!(b == b)) b = 0;
-        d.bg16 = (int)std::min(b, 65535.0);
-    }
-    d.I = (float*)I;
-    d.mask8 = (uint8_t*)mask;
-    d.write_mask = need_mask ? 1 : 0;
-    d.zero_count = zc;
-    d.S = (float2*)S;
-    PkProgram prog;
-    pk_program_add(prog, PK_STEP_Y, Y_PRE, {d});
-    int mask_mode = need_mask ? 1 : 0;
-    if (p->edge_erosion > 0) {
-        // the erosion branch depends on whether the raw mask is full (decon_mask_edge_erosion.m:8)
-        if ((s = pk_program_upload(ctx, prog, st)) != PK_OK) return s;
-        if ((s = pk_program_launch(ctx, prog, st)) != PK_OK) return s;
-        prog = PkProgram();
-        unsigned int zeros = 0;
-        PK_CUDA(cudaMemcpyAsync(&zeros, zc, sizeof(zeros), cudaMemcpyDeviceToHost, st));
-        PK_CUDA(cudaStreamSynchronize(st));
-        if (zeros == 0) {
-            mask_mode = 2;
-        } else {
-            mask_mode = 3;
-            void *m2, *offs;
-            if ((s = pk_scratch(ctx, SL_MASK2, N, &m2)) != PK_OK) return s;
-            std::vector<int2> disk = pk_disk_offsets(p->edge_erosion - 1);
-            if ((s = pk_scratch(ctx, SL_OFFS, sizeof(int2) * disk.size(), &offs)) != PK_OK) return s;
-            PK_CUDA(cudaMemcpyAsync(offs, disk.data(), sizeof(int2) * disk.size(), cudaMemcpyHostToDevice, st));
-            k_mask_faces<<<grid_for((long long)N), 256, 0, st>>>((uint8_t*)mask, ny, nx, nz);
-            k_erode_xy<<<grid_for((long long)N), 256, 0, st>>>((const uint8_t*)mask, (uint8_t*)m2, ny, nx, nz,
-                                                                (const int2*)offs, (int)disk.size());
-            k_erode_z<<<grid_for((long long)N), 256, 0, st>>>((const uint8_t*)m2, (uint8_t*)mask, ny, nx, nz,
-                                                               p->edge_erosion - 1);
-            PK_CUDA(cudaGetLastError());
-            PK_CUDA(cudaStreamSynchronize(st));  // disk offsets are a host temporary
-        }
-    }
-
-    VolDesc base = d;
-    base.raw = nullptr;
-    base.zero_count = nullptr;
-    base.write_mask = 0;
-    if (numit == 0) {
-        if (!prog.steps.empty()) {
-            if ((s = pk_program_upload(ctx, prog, st)) != PK_OK) return s;
-            if ((s = pk_program_launch(ctx, prog, st)) != PK_OK) return s;
-        }
-        VolDesc f = base;
-        set_post(f, p, mask_mode, d_out);
-        k_post_identity<<<grid_for((long long)N), 256, 0, st>>>(f);
-        PK_CUDA(cudaGetLastError());
-        return PK_OK;
-    }
-    if (method == 1) {
-        for (int it = 1; it <= numit; it++) {
-            VolDesc cf = base; cf.otf = otf_f; cf.conj = 0;
-            VolDesc cb = base; cb.otf = otf_b; cb.conj = 0;
-            pk_program_add(prog, PK_STEP_X, XZ_FWD, {base});
-            pk_program_add(prog, PK_STEP_Z, XZ_CONV, {cf});
-            pk_program_add(prog, PK_STEP_X, XZ_INV, {base});
-            pk_program_add(prog, PK_STEP_Y, Y_RATIO, {base});
-            pk_program_add(prog, PK_STEP_X, XZ_FWD, {base});
-            pk_program_add(prog, PK_STEP_Z, XZ_CONV, {cb});
-            pk_program_add(prog, PK_STEP_X, XZ_INV, {base});
-            VolDesc u = base;
-            u.Jo = it == 1 ? (const float*)I : (const float*)J;
-            u.Jn = (float*)J;
-            if (it < numit) {
-                pk_program_add(prog, PK_STEP_Y, Y_UPDATE, {u});
-            } else {
-                set_post(u, p, mask_mode, d_out);
-                pk_program_add(prog, PK_STEP_Y, Y_FINAL, {u});
-            }
-        }
-    } else {
-        float* Jb[2] = {(float*)J, (float*)JB};
-        base.partials = (double*)part;
-        for (int k = 1; k <= numit; k++) {
-            if (k >= 2) {
-                VolDesc r = base;
-                r.J2 = Jb[k % 2];
-                r.J3 = k == 2 ? (const float*)I : Jb[(k - 1) % 2];
-                r.Yb = (float*)Yb;
-                r.lam_on = k >= 3 ? 1 : 0;
-                pk_program_add(prog, PK_STEP_Y, Y_RLPRE, {r});
-            }
-            VolDesc cf = base; cf.otf = otf_f; cf.conj = 0;
-            VolDesc cb = base; cb.otf = otf_f; cb.conj = 1;
-            pk_program_add(prog, PK_STEP_X, XZ_FWD, {base});
-            pk_program_add(prog, PK_STEP_Z, XZ_CONV, {cf});
-            pk_program_add(prog, PK_STEP_X, XZ_INV, {base});
-            pk_program_add(prog, PK_STEP_Y, Y_RATIO, {base});
-            pk_program_add(prog, PK_STEP_X, XZ_FWD, {base});
-            pk_program_add(prog, PK_STEP_Z, XZ_CONV, {cb});
-            pk_program_add(prog, PK_STEP_X, XZ_INV, {base});
-            VolDesc u = base;
-            u.Yb = k == 1 ? (float*)I : (float*)Yb;
-            if (k < numit) {
-                u.J4 = (float*)J4;
-                u.rl_first = k == 1 ? 1 : 0;
-                u.J2n = Jb[(k + 1) % 2];
-                pk_program_add(prog, PK_STEP_Y, Y_RLUPD, {u});
-                pk_program_add(prog, PK_STEP_LAMBDA, 0, {u});
-            } else {
-                set_post(u, p, mask_mode, d_out);
-                pk_program_add(prog, PK_STEP_Y, Y_RLFINAL, {u});
-            }
-        }
-    }
-    if ((s = pk_program_upload(ctx, prog, st)) != PK_OK) return s;
-    return pk_program_launch(ctx, prog, st);
+    void* arena;
+    if ((s = pk_scratch(ctx, SL_ARENA, pk_job_bytes(method, j.dims, need_mask, d.blocksY), &arena)) != PK_OK) return s;
+    pk_job_carve(j, method, need_mask, d.blocksY, (char*)arena);
+    j.d_raw = d_in;
+    j.d_out = d_out;
+    j.has_bbox = p->has_bbox;
+    for (int i = 0; i < 6; i++) j.bbox[i] = p->bbox[i];
+    std::vector<DeconJob> jobs{j};
+    return pk_decon_multi(ctx, method, jobs, in_type, numit, p, st);
 }

@@ -233,7 +233,7 @@ __global__ void __launch_bounds__(PK_THREADS, 3) k_y(const VolDesc* __restrict__
     }
     const int nvox = Lc * M;
     const long long v0 = row0 * (long long)ny;
-    const bool raw_sync = mode == Y_PRE && (d.raw_type == PK_F64 || (d.raw_type == PK_U16 && odd));
+    const bool raw_sync = mode == Y_PRE && (d.padded || d.raw_type == PK_F64 || (d.raw_type == PK_U16 && odd));
     if (mode == Y_PRE && !raw_sync) {
         for (int idx = tid; idx < nvox; idx += NT) {
             const int l = idx / M, k = idx - l * M;
@@ -314,32 +314,46 @@ __global__ void __launch_bounds__(PK_THREADS, 3) k_y(const VolDesc* __restrict__
             const long long vi = row * (long long)ny + y;
             float2 I;
             bool nz0, nz1 = true;
-            if (d.raw_type == PK_U16) {
-                unsigned r0, r1 = 1;
-                if (!raw_sync) {
-                    const ushort2 q = *reinterpret_cast<const ushort2*>(&aux0[idx]);
-                    r0 = q.x;
-                    r1 = q.y;
-                } else {
-                    r0 = ((const uint16_t*)d.raw)[vi];
+            if (raw_sync) {
+                // scalar loads through the raw extent (padded transforms read zeros outside it)
+                const unsigned ur = (unsigned)row;
+                const int z = (int)(ur / (unsigned)d.nx), x = (int)(ur - (unsigned)z * (unsigned)d.nx);
+                float v[2] = {0.f, 0.f};
+                bool nzv[2] = {true, true};
+                for (int e = 0; e < (odd ? 1 : 2); e++) {
+                    const int yy = y + e;
+                    if (yy >= d.rdims[0] || x >= d.rdims[1] || z >= d.rdims[2]) { v[e] = 0.f; continue; }
+                    const long long ri = yy + (long long)d.rdims[0] * (x + (long long)d.rdims[1] * z);
+                    if (d.raw_type == PK_U16) {
+                        const unsigned r = ((const uint16_t*)d.raw)[ri];
+                        nzv[e] = r != 0;
+                        v[e] = r > (unsigned)d.bg16 ? (float)(r - (unsigned)d.bg16) : 0.f;
+                    } else if (d.raw_type == PK_F32) {
+                        const float r = ((const float*)d.raw)[ri];
+                        nzv[e] = r != 0.f;
+                        v[e] = fmaxf(__fsub_rn(r, d.bg_f), 0.f);
+                    } else {
+                        const double r = ((const double*)d.raw)[ri];
+                        nzv[e] = r != 0.0;
+                        v[e] = fmaxf(__fsub_rn((float)r, d.bg_f), 0.f);
+                    }
                 }
+                I = make_float2(v[0], v[1]);
+                nz0 = nzv[0];
+                nz1 = nzv[1];
+            } else if (d.raw_type == PK_U16) {
+                const ushort2 q = *reinterpret_cast<const ushort2*>(&aux0[idx]);
+                const unsigned r0 = q.x, r1 = q.y;
                 nz0 = r0 != 0;
                 nz1 = r1 != 0;
                 I.x = r0 > (unsigned)d.bg16 ? (float)(r0 - (unsigned)d.bg16) : 0.f;
                 I.y = r1 > (unsigned)d.bg16 ? (float)(r1 - (unsigned)d.bg16) : 0.f;
-            } else if (d.raw_type == PK_F32) {
+            } else {
                 const float2 r = aux0[idx];
                 nz0 = r.x != 0.f;
                 if (!odd) nz1 = r.y != 0.f;
                 I.x = fmaxf(__fsub_rn(r.x, d.bg_f), 0.f);
                 I.y = fmaxf(__fsub_rn(r.y, d.bg_f), 0.f);
-            } else {
-                const double* rp = (const double*)d.raw;
-                const double r0 = rp[vi], r1 = odd ? 1.0 : rp[vi + 1];
-                nz0 = r0 != 0.0;
-                nz1 = r1 != 0.0;
-                I.x = fmaxf(__fsub_rn((float)r0, d.bg_f), 0.f);
-                I.y = fmaxf(__fsub_rn((float)r1, d.bg_f), 0.f);
             }
             if (odd) {
                 I.y = 0.f;

@@ -3,10 +3,6 @@
 
 extern "C" {
 
-pk_status pk_batch_decon(pk_ctx*, int32_t, int32_t, const pk_chunk*, pk_dtype, int32_t, const float* const*,
-                         const float* const*, const int64_t*, int32_t, const pk_decon_params*, int32_t, int32_t) {
-    return pk_fail(PK_ERR_UNSUPPORTED, "pk_batch_decon: not built yet");
-}
 pk_server* pk_server_create(pk_ctx*, const pk_server_config*) { return nullptr; }
 pk_status pk_server_add_psf(pk_server*, int32_t, const float*, const float*, const int64_t[3]) { return PK_ERR_UNSUPPORTED; }
 int64_t pk_server_submit(pk_server*, const uint16_t*, const int64_t[3], int32_t, int32_t, int32_t,

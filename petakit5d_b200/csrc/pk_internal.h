@@ -63,6 +63,7 @@ struct VolDesc {
     AxisDev ay, ax, az;
     // buffers
     const void* raw; int raw_type;   // Y_PRE source (pk_dtype)
+    int rdims[3]; int padded;        // raw extent; padded = transform extent larger (zeros beyond)
     const float* src; float* dst;    // Y_R2C source / Y_C2R destination
     float* I;                        // background-subtracted input
     const float* Jo; float* Jn;      // OMW estimate (old / new; may alias)
@@ -170,6 +171,27 @@ pk_status pk_scratch(pk_ctx* ctx, int slot, size_t bytes, void** ptr);
 // decon drivers (decon.cu)
 pk_status pk_get_otf(pk_ctx* ctx, const float* h_psf, const int64_t psf_dims[3], int ny, int nx, int nz,
                      const float2** d_otf, cudaStream_t st);
+// one volume of a multi-volume run: inputs, transform extent, OTFs, outputs and work buffers
+struct DeconJob {
+    const void* d_raw = nullptr;
+    int rdims[3] = {0, 0, 0};   // raw extent
+    int dims[3] = {0, 0, 0};    // transform extent (>= raw; the excess reads as zeros)
+    const float2* otf_f = nullptr;
+    const float2* otf_b = nullptr;
+    void* d_out = nullptr;
+    int has_bbox = 0;
+    int64_t bbox[6] = {0, 0, 0, 0, 0, 0};
+    float *I = nullptr, *J = nullptr, *JB = nullptr, *Yb = nullptr, *J4 = nullptr;
+    float2* S = nullptr;
+    uint8_t* mask = nullptr;
+    double* part = nullptr;
+};
+size_t pk_job_bytes(int method, const int dims[3], bool need_mask, int blocksY);
+void pk_job_carve(DeconJob& j, int method, bool need_mask, int blocksY, char* arena);
+pk_status pk_decon_multi(pk_ctx* ctx, int method, std::vector<DeconJob>& jobs, pk_dtype in_type, int numit,
+                         const pk_decon_params* p, cudaStream_t st);
+pk_status pk_check_params(const int64_t dims[3], const pk_decon_params* p);
+
 pk_status pk_decon_run(pk_ctx* ctx, int method, const void* d_in, pk_dtype in_type, const int64_t dims[3],
                        const float* psf_f, const int64_t psf_f_dims[3], const float* psf_b,
                        const int64_t psf_b_dims[3], int numit, const pk_decon_params* p, void* d_out,
