@@ -1,0 +1,493 @@
+// Serving loop with continuous batching (pk_server_*).
+//
+// Requests (volume, PSF id, method, iterations) are copied at submit and queued.  A scheduler
+// thread admits them while their device buffers fit the HBM budget, keeps their iterates resident
+// in HBM, and runs rounds: each round is one launch program with four pass slots (y, x, z, x);
+// every active request contributes its next pending pass to the slot of that kind, so requests
+// at different iterations and of different methods share launches, and a new request joins at
+// the next round.  The per-request arithmetic is the same as the single-volume call's (each CTA
+// works on one volume, lambda sums are per request), so a result does not depend on the mix.
+// Request volumes are staged in pinned memory at submit and uploaded on a copy stream; the client
+// that waits for a request copies its result out and releases the request's device memory.
+// All waits are host-side with timeouts; no kernel waits on another.
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "pk_internal.h"
+
+void set_post(VolDesc& d, const pk_decon_params* p, int mask_mode, void* d_out);
+
+namespace {
+
+using clk = std::chrono::steady_clock;
+
+struct PsfEntry {
+    std::vector<float> f, b;
+    int64_t dims[3];
+    bool has_b = false;
+};
+
+struct Step {
+    int kind, mode;
+    VolDesc d;
+};
+
+enum ReqState { RQ_QUEUED, RQ_ACTIVE, RQ_DONE, RQ_FAILED, RQ_CANCELLED };
+
+struct Request {
+    int64_t id;
+    uint16_t* vol = nullptr;         // pinned staging copy of the input
+    size_t vol_bytes = 0;
+    int64_t dims[3];
+    int psf_id, method, numit;
+    pk_decon_params params;
+    ReqState state = RQ_QUEUED;
+    pk_status err = PK_OK;
+    std::string msg;
+    clk::time_point t_submit, t_done;
+    // device state
+    void* dev = nullptr;             // one allocation: raw | out | work arena
+    size_t dev_bytes = 0;
+    void* d_out = nullptr;
+    size_t out_bytes = 0;
+    std::deque<Step> steps;
+    cudaEvent_t ev_up = nullptr;     // upload finished
+    cudaEvent_t ev_done = nullptr;   // last pass finished
+    bool last_queued = false;
+    bool collected = false;          // the waiter took the result
+};
+
+size_t al256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+}  // namespace
+
+struct pk_server {
+    pk_ctx* ctx = nullptr;
+    pk_server_config cfg{};
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::map<int32_t, PsfEntry> psfs;
+    std::map<int64_t, std::shared_ptr<Request>> reqs;
+    std::deque<std::shared_ptr<Request>> queue;
+    std::vector<std::shared_ptr<Request>> active;
+    std::atomic<bool> stop{false};
+    std::thread th;
+    int64_t next_id = 0;
+    int64_t completed = 0, rejected = 0, rounds = 0;
+    size_t inflight = 0, peak_inflight = 0;
+    cudaStream_t up = nullptr, down = nullptr;
+
+    void loop();
+    pk_status admit(const std::shared_ptr<Request>& r);
+    void build_steps(Request& r, const VolDesc& base, const float2* otf_f, const float2* otf_b);
+    void finish(const std::shared_ptr<Request>& r, pk_status st, const std::string& msg);
+    void release(const std::shared_ptr<Request>& r);
+};
+
+void pk_server::release(const std::shared_ptr<Request>& r) {
+    if (r->dev) {
+        cudaFreeAsync(r->dev, ctx->stream);
+        inflight -= r->dev_bytes;
+        r->dev = nullptr;
+    }
+    if (r->vol) {
+        cudaFreeHost(r->vol);
+        r->vol = nullptr;
+    }
+    if (r->ev_up) { cudaEventDestroy(r->ev_up); r->ev_up = nullptr; }
+    if (r->ev_done) { cudaEventDestroy(r->ev_done); r->ev_done = nullptr; }
+}
+
+// Mark a request finished; on success its device result stays until the waiter collects it.
+void pk_server::finish(const std::shared_ptr<Request>& r, pk_status st, const std::string& msg) {
+    r->err = st;
+    r->msg = msg;
+    if (st != PK_OK) release(r);
+    else if (r->vol) {
+        cudaFreeHost(r->vol);
+        r->vol = nullptr;
+    }
+    if (r->state != RQ_CANCELLED) r->state = st == PK_OK ? RQ_DONE : RQ_FAILED;
+    r->t_done = clk::now();
+    if (st == PK_OK) completed++;
+    cv_done.notify_all();
+}
+
+// The request's pass sequence (the single-volume program of decon.cu, step by step).
+void pk_server::build_steps(Request& r, const VolDesc& b, const float2* otf_f, const float2* otf_b) {
+    auto push = [&](int kind, int mode, const VolDesc& d) { r.steps.push_back(Step{kind, mode, d}); };
+    char* arena = (char*)r.dev + al256((size_t)b.nrows * b.ny * 2) + al256(r.out_bytes);
+    DeconJob j;
+    for (int k = 0; k < 3; k++) j.dims[k] = j.rdims[k] = (int)r.dims[k];
+    pk_job_carve(j, r.method, false, b.blocksY, arena);
+    VolDesc base = b;
+    base.I = j.I;
+    base.S = j.S;
+    base.partials = j.part;
+    VolDesc pre = base;
+    pre.raw = r.dev;
+    pre.raw_type = PK_U16;
+    for (int k = 0; k < 3; k++) pre.rdims[k] = (int)r.dims[k];
+    pre.bg_f = (float)r.params.background;
+    double b16 = std::floor(std::fabs(r.params.background) + 0.5);
+    if (r.params.background < 0 || !(b16 == b16)) b16 = 0;
+    pre.bg16 = (int)std::min(b16, 65535.0);
+    push(PK_STEP_Y, Y_PRE, pre);
+    auto conv = [&](int which) {
+        VolDesc z = base;
+        if (r.method == 1) { z.otf = which ? otf_b : otf_f; z.conj = 0; }
+        else { z.otf = otf_f; z.conj = which; }
+        push(PK_STEP_X, XZ_FWD, base);
+        push(PK_STEP_Z, XZ_CONV, z);
+        push(PK_STEP_X, XZ_INV, base);
+    };
+    if (r.method == 1) {
+        for (int it = 1; it <= r.numit; it++) {
+            conv(0);
+            push(PK_STEP_Y, Y_RATIO, base);
+            conv(1);
+            VolDesc u = base;
+            u.Jo = it == 1 ? j.I : j.J;
+            u.Jn = j.J;
+            if (it < r.numit) push(PK_STEP_Y, Y_UPDATE, u);
+            else {
+                set_post(u, &r.params, 0, r.d_out);
+                push(PK_STEP_Y, Y_FINAL, u);
+            }
+        }
+    } else {
+        float* Jb[2] = {j.J, j.JB};
+        for (int k = 1; k <= r.numit; k++) {
+            if (k >= 2) {
+                VolDesc q = base;
+                q.J2 = Jb[k % 2];
+                q.J3 = k == 2 ? j.I : Jb[(k - 1) % 2];
+                q.Yb = j.Yb;
+                q.lam_on = k >= 3 ? 1 : 0;
+                push(PK_STEP_Y, Y_RLPRE, q);
+            }
+            conv(0);
+            push(PK_STEP_Y, Y_RATIO, base);
+            conv(1);
+            VolDesc u = base;
+            u.Yb = k == 1 ? j.I : j.Yb;
+            if (k < r.numit) {
+                u.J4 = j.J4;
+                u.rl_first = k == 1 ? 1 : 0;
+                u.J2n = Jb[(k + 1) % 2];
+                push(PK_STEP_Y, Y_RLUPD, u);
+                push(PK_STEP_LAMBDA, 0, u);
+            } else {
+                set_post(u, &r.params, 0, r.d_out);
+                push(PK_STEP_Y, Y_RLFINAL, u);
+            }
+        }
+    }
+}
+
+pk_status pk_server::admit(const std::shared_ptr<Request>& r) {
+    pk_ctx* c = ctx;
+    VolDesc b;
+    pk_status s = pk_init_desc(c, (int)r->dims[0], (int)r->dims[1], (int)r->dims[2], &b);
+    if (s != PK_OK) return s;
+    const PsfEntry& pe = psfs[r->psf_id];
+    const float2 *of = nullptr, *ob = nullptr;
+    if ((s = pk_get_otf(c, pe.f.data(), pe.dims, b.ny, b.nx, b.nz, &of, c->stream)) != PK_OK) return s;
+    if (r->method == 1 && (s = pk_get_otf(c, pe.b.data(), pe.dims, b.ny, b.nx, b.nz, &ob, c->stream)) != PK_OK) return s;
+    const size_t raw_b = (size_t)b.nrows * b.ny * 2;
+    int64_t od[3];
+    pk_output_dims(r->dims, &r->params, od);
+    r->out_bytes = (size_t)od[0] * od[1] * od[2] * (r->params.save16bit ? 2 : 4);
+    const int dims[3] = {b.ny, b.nx, b.nz};
+    r->dev_bytes = al256(raw_b) + al256(r->out_bytes) + pk_job_bytes(r->method, dims, false, b.blocksY);
+    if (!r->ev_up) PK_CUDA(cudaEventCreateWithFlags(&r->ev_up, cudaEventDisableTiming));
+    if (!r->ev_done) PK_CUDA(cudaEventCreateWithFlags(&r->ev_done, cudaEventDisableTiming));
+    cudaError_t e = cudaMallocAsync(&r->dev, r->dev_bytes, c->stream);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        r->dev = nullptr;
+        return pk_fail(PK_ERR_NOMEM, "request allocation failed");
+    }
+    inflight += r->dev_bytes;
+    peak_inflight = std::max(peak_inflight, inflight);
+    r->d_out = (char*)r->dev + al256(raw_b);
+    // upload on the copy stream (pinned source); the compute stream waits for it before the first pass
+    PK_CUDA(cudaEventRecord(r->ev_up, c->stream));          // the allocation is ordered on the compute stream
+    PK_CUDA(cudaStreamWaitEvent(up, r->ev_up, 0));
+    PK_CUDA(cudaMemcpyAsync(r->dev, r->vol, raw_b, cudaMemcpyHostToDevice, up));
+    PK_CUDA(cudaEventRecord(r->ev_up, up));
+    PK_CUDA(cudaStreamWaitEvent(c->stream, r->ev_up, 0));
+    build_steps(*r, b, of, ob);
+    r->state = RQ_ACTIVE;
+    return PK_OK;
+}
+
+void pk_server::loop() {
+    cudaSetDevice(ctx->device);
+    const int kinds[4] = {PK_STEP_Y, PK_STEP_X, PK_STEP_Z, PK_STEP_X};
+    while (!stop.load()) {
+        std::unique_lock<std::mutex> lk(mu);
+        // finished requests (last pass complete)
+        for (auto it = active.begin(); it != active.end();) {
+            auto& r = *it;
+            if (r->state == RQ_CANCELLED) {       // cancelled requests leave at a round boundary
+                cudaStreamSynchronize(ctx->stream);
+                finish(r, PK_ERR_CANCELLED, "cancelled");
+                it = active.erase(it);
+            } else if (r->last_queued && cudaEventQuery(r->ev_done) == cudaSuccess) {
+                finish(r, PK_OK, "");
+                it = active.erase(it);
+            } else {
+                ++it;
+            }
+        }
+        // admission against the budget
+        while (!queue.empty() && (int)active.size() < cfg.max_batch) {
+            auto r = queue.front();
+            if (r->state == RQ_CANCELLED) {
+                queue.pop_front();
+                finish(r, PK_ERR_CANCELLED, "cancelled");
+                continue;
+            }
+            VolDesc tmp;
+            size_t need = 0;
+            {
+                std::lock_guard<std::recursive_mutex> cl(ctx->mu);
+                if (pk_init_desc(ctx, (int)r->dims[0], (int)r->dims[1], (int)r->dims[2], &tmp) == PK_OK) {
+                    const int dims[3] = {tmp.ny, tmp.nx, tmp.nz};
+                    need = pk_job_bytes(r->method, dims, false, tmp.blocksY) + 4 * (size_t)tmp.nrows * tmp.ny;
+                }
+            }
+            if (inflight + need > (size_t)cfg.budget_bytes && !active.empty()) break;  // wait for memory
+            queue.pop_front();
+            pk_status s;
+            {
+                std::lock_guard<std::recursive_mutex> cl(ctx->mu);
+                s = admit(r);
+            }
+            if (s != PK_OK) {
+                finish(r, s, pk_last_error());
+                continue;
+            }
+            active.push_back(r);
+        }
+        bool work = false;
+        for (auto& r : active)
+            if (!r->steps.empty()) work = true;
+        if (!work) {
+            cv_work.wait_for(lk, std::chrono::milliseconds(1));
+            continue;
+        }
+        // one round: slots y, x, z, x; lambda steps ride with their y slot
+        std::vector<std::shared_ptr<Request>> batch(active.begin(), active.end());
+        lk.unlock();
+        {
+            std::lock_guard<std::recursive_mutex> cl(ctx->mu);
+            PkProgram prog;
+            for (int slot = 0; slot < 4; slot++) {
+                std::map<int, std::vector<VolDesc>> by_mode;
+                std::vector<VolDesc> lam;
+                for (auto& r : batch) {
+                    if (r->steps.empty() || r->steps.front().kind != kinds[slot]) continue;
+                    Step st = r->steps.front();
+                    r->steps.pop_front();
+                    by_mode[st.mode].push_back(st.d);
+                    if (!r->steps.empty() && r->steps.front().kind == PK_STEP_LAMBDA) {
+                        lam.push_back(r->steps.front().d);
+                        r->steps.pop_front();
+                    }
+                }
+                for (auto& kv : by_mode) pk_program_add(prog, kinds[slot], kv.first, kv.second);
+                if (!lam.empty()) pk_program_add(prog, PK_STEP_LAMBDA, 0, lam);
+            }
+            pk_status s = pk_program_upload(ctx, prog, ctx->stream);
+            if (s == PK_OK) s = pk_program_launch(ctx, prog, ctx->stream);
+            if (s != PK_OK) {
+                std::lock_guard<std::mutex> l2(mu);
+                for (auto& r : batch) finish(r, s, pk_last_error());
+                active.clear();
+                continue;
+            }
+            // requests whose last pass is queued: mark the point their result is complete
+            for (auto& r : batch) {
+                if (!r->steps.empty() || r->last_queued) continue;
+                cudaEventRecord(r->ev_done, ctx->stream);
+                r->last_queued = true;
+            }
+        }
+        lk.lock();
+        rounds++;
+    }
+}
+
+extern "C" {
+
+pk_server* pk_server_create(pk_ctx* ctx, const pk_server_config* cfg) {
+    if (!ctx) {
+        pk_set_error("null pk_ctx");
+        return nullptr;
+    }
+    pk_server* s = new pk_server();
+    s->ctx = ctx;
+    s->cfg.budget_bytes = cfg && cfg->budget_bytes > 0 ? cfg->budget_bytes : (int64_t)150e9;
+    s->cfg.max_batch = cfg && cfg->max_batch > 0 ? cfg->max_batch : 64;
+    s->cfg.queue_capacity = cfg && cfg->queue_capacity > 0 ? cfg->queue_capacity : 1024;
+    cudaSetDevice(ctx->device);
+    if (cudaStreamCreateWithFlags(&s->up, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&s->down, cudaStreamNonBlocking) != cudaSuccess) {
+        pk_set_error("stream creation failed");
+        delete s;
+        return nullptr;
+    }
+    s->th = std::thread([s] { s->loop(); });
+    return s;
+}
+
+pk_status pk_server_add_psf(pk_server* s, int32_t psf_id, const float* psf_f, const float* psf_b,
+                            const int64_t psf_dims[3]) {
+    if (!s || !psf_f || !psf_dims) return pk_fail(PK_ERR_INVALID, "bad arguments");
+    const int64_t n = psf_dims[0] * psf_dims[1] * psf_dims[2];
+    if (n < 1) return pk_fail(PK_ERR_INVALID, "empty PSF");
+    std::lock_guard<std::mutex> lk(s->mu);
+    PsfEntry e;
+    e.f.assign(psf_f, psf_f + n);
+    if (psf_b) {
+        e.b.assign(psf_b, psf_b + n);
+        e.has_b = true;
+    }
+    for (int i = 0; i < 3; i++) e.dims[i] = psf_dims[i];
+    s->psfs[psf_id] = std::move(e);
+    return PK_OK;
+}
+
+int64_t pk_server_submit(pk_server* s, const uint16_t* vol, const int64_t dims[3], int32_t psf_id, int32_t method,
+                         int32_t numit, const pk_decon_params* params) {
+    if (!s || !vol || !dims) return -(int64_t)pk_fail(PK_ERR_INVALID, "bad arguments");
+    if (method != 0 && method != 1) return -(int64_t)pk_fail(PK_ERR_INVALID, "method must be 0 (RL) or 1 (OMW)");
+    if (numit < 1) return -(int64_t)pk_fail(PK_ERR_INVALID, "NUMIT must be >= 1 for served requests");
+    pk_decon_params p;
+    if (params) p = *params;
+    else pk_params_default(&p);
+    if (p.decon_offset != 0.0 || p.edge_erosion > 0)
+        return -(int64_t)pk_fail(PK_ERR_UNSUPPORTED, "served requests do not take deconOffset/EdgeErosion");
+    pk_status st = pk_check_params(dims, &p);
+    if (st != PK_OK) return -(int64_t)st;
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto it = s->psfs.find(psf_id);
+    if (it == s->psfs.end()) return -(int64_t)pk_fail(PK_ERR_INVALID, "unknown psf_id");
+    if (method == 1 && !it->second.has_b) return -(int64_t)pk_fail(PK_ERR_INVALID, "psf_id has no backprojector");
+    if ((int)s->queue.size() >= s->cfg.queue_capacity) {
+        s->rejected++;
+        return -(int64_t)pk_fail(PK_ERR_BUSY, "queue full");
+    }
+    lk.unlock();
+    auto r = std::make_shared<Request>();
+    const int64_t n = dims[0] * dims[1] * dims[2];
+    r->vol_bytes = (size_t)n * 2;
+    cudaSetDevice(s->ctx->device);
+    if (cudaMallocHost(&r->vol, r->vol_bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return -(int64_t)pk_fail(PK_ERR_NOMEM, "pinned staging allocation failed");
+    }
+    memcpy(r->vol, vol, r->vol_bytes);
+    lk.lock();
+    r->id = s->next_id++;
+    for (int i = 0; i < 3; i++) r->dims[i] = dims[i];
+    r->psf_id = psf_id;
+    r->method = method;
+    r->numit = numit;
+    r->params = p;
+    r->t_submit = clk::now();
+    s->reqs[r->id] = r;
+    s->queue.push_back(r);
+    s->cv_work.notify_all();
+    return r->id;
+}
+
+pk_status pk_server_wait(pk_server* s, int64_t id, void* out, int32_t timeout_ms, double* latency_ms) {
+    if (!s) return pk_fail(PK_ERR_INVALID, "null server");
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto it = s->reqs.find(id);
+    if (it == s->reqs.end()) return pk_fail(PK_ERR_INVALID, "unknown request id");
+    auto r = it->second;
+    const bool ok = s->cv_done.wait_for(lk, std::chrono::milliseconds(std::max(0, timeout_ms)), [&] {
+        return r->state == RQ_DONE || r->state == RQ_FAILED || (r->state == RQ_CANCELLED && r->t_done != clk::time_point());
+    });
+    if (!ok) return pk_fail(PK_ERR_TIMEOUT, "request not finished within the timeout");
+    if (r->state == RQ_CANCELLED) {
+        s->reqs.erase(id);
+        return pk_fail(PK_ERR_CANCELLED, "request cancelled");
+    }
+    if (r->state == RQ_FAILED) {
+        const pk_status e = r->err;
+        const std::string m = r->msg;
+        s->reqs.erase(id);
+        return pk_fail(e, m);
+    }
+    s->reqs.erase(id);
+    lk.unlock();
+    // the result is complete on the device: copy it out on a stream of this thread, then free
+    cudaSetDevice(s->ctx->device);
+    cudaError_t e = cudaSuccess;
+    if (out) e = cudaMemcpyAsync(out, r->d_out, r->out_bytes, cudaMemcpyDeviceToHost, s->down);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->down);
+    const auto t_out = clk::now();
+    lk.lock();
+    s->release(r);
+    lk.unlock();
+    if (e != cudaSuccess) return pk_fail(PK_ERR_CUDA, std::string("result copy: ") + cudaGetErrorString(e));
+    if (latency_ms) *latency_ms = std::chrono::duration<double, std::milli>(t_out - r->t_submit).count();
+    return PK_OK;
+}
+
+pk_status pk_server_cancel(pk_server* s, int64_t id) {
+    if (!s) return pk_fail(PK_ERR_INVALID, "null server");
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->reqs.find(id);
+    if (it == s->reqs.end()) return pk_fail(PK_ERR_INVALID, "unknown request id");
+    if (it->second->state == RQ_QUEUED || it->second->state == RQ_ACTIVE) it->second->state = RQ_CANCELLED;
+    s->cv_work.notify_all();
+    return PK_OK;
+}
+
+pk_status pk_server_stats(pk_server* s, int64_t stats[4]) {
+    if (!s || !stats) return pk_fail(PK_ERR_INVALID, "bad arguments");
+    std::lock_guard<std::mutex> lk(s->mu);
+    stats[0] = s->completed;
+    stats[1] = s->rejected;
+    stats[2] = (int64_t)s->peak_inflight;
+    stats[3] = s->rounds;
+    return PK_OK;
+}
+
+void pk_server_destroy(pk_server* s) {
+    if (!s) return;
+    s->stop.store(true);
+    s->cv_work.notify_all();
+    if (s->th.joinable()) s->th.join();
+    {
+        std::lock_guard<std::recursive_mutex> cl(s->ctx->mu);
+        cudaSetDevice(s->ctx->device);
+        cudaStreamSynchronize(s->ctx->stream);
+        std::lock_guard<std::mutex> lk(s->mu);
+        for (auto& kv : s->reqs) s->release(kv.second);
+        for (auto& r : s->queue) s->release(r);
+        for (auto& r : s->active) s->release(r);
+        cudaStreamSynchronize(s->ctx->stream);
+        cudaStreamDestroy(s->up);
+        cudaStreamDestroy(s->down);
+    }
+    delete s;
+}
+
+}  // extern "C"
