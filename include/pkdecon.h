@@ -107,6 +107,23 @@ PK_API pk_status pk_decon_lucy_omw_device(pk_ctx* ctx, const void* d_in, pk_dtyp
                                    const float* psf_b, const int64_t psf_b_dims[3], int32_t numit,
                                    const pk_decon_params* params, void* d_out, void* stream);
 
+/* OMW deconvolution for callers that cannot allocate GPU memory (no counterpart in the reference).
+ * Some callers must not call cudaMalloc -- code running under another runtime's device-memory
+ * manager, or an allocation-free section such as an acquisition loop -- so this call allocates no
+ * device memory and calls no allocating CUDA or library routine: every work buffer, both OTFs, the
+ * twiddle tables and the launch descriptors live in one array compiled into the library (about
+ * 32.4 MB, held on each GPU that loads the library until exit).  d_in/d_out are device pointers,
+ * the PSFs host arrays; the work is queued on `stream` (a cudaStream_t, NULL = default stream) of
+ * the calling thread's current device.  Limit: 1,048,576 voxels per volume (larger ones return
+ * PK_ERR_UNSUPPORTED); deconOffset and EdgeErosion are not supported.  Every call shares the array
+ * and leaves its contents behind, so calls that overlap on the GPU race: issue them one after
+ * another on one stream.  The first call on a device looks up the array's address and should come
+ * before any stream capture. */
+PK_API pk_status pk_decon_lucy_omw_noalloc(const void* d_in, pk_dtype in_type, const int64_t dims[3],
+                                           const float* psf_f, const int64_t psf_f_dims[3],
+                                           const float* psf_b, const int64_t psf_b_dims[3], int32_t numit,
+                                           const pk_decon_params* params, void* d_out, void* stream);
+
 /* ---------------------------------------------------------------- OTF / FFT building blocks */
 /* decon_psf2otf(PSF./sum(PSF), dims) (decon_psf2otf.m:1-46), returned as the half spectrum:
  * complex64 (interleaved re,im), column-major [floor(ny/2)+1, nx, nz]. */

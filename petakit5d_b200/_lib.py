@@ -69,6 +69,8 @@ _SIGS = {
     "pk_decon_lucy_device": (C.c_int, [P, P, C.c_int, I64x3, P, I64x3, C.c_int32, C.POINTER(DeconParams), P, P]),
     "pk_decon_lucy_omw_device": (C.c_int, [P, P, C.c_int, I64x3, P, I64x3, P, I64x3, C.c_int32,
                                            C.POINTER(DeconParams), P, P]),
+    "pk_decon_lucy_omw_noalloc": (C.c_int, [P, C.c_int, I64x3, P, I64x3, P, I64x3, C.c_int32,
+                                            C.POINTER(DeconParams), P, P]),
     "pk_psf2otf": (C.c_int, [P, P, I64x3, I64x3, P]),
     "pk_fft3_r2c_device": (C.c_int, [P, P, I64x3, P, P]),
     "pk_fft3_c2r_device": (C.c_int, [P, P, I64x3, P, P]),
