@@ -101,11 +101,21 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def make_workload(seed):
+WB = dict(alpha=0.005, beta=1e-3, n=8, res_flag=1)   # Wiener-Butterworth backprojector, Butterworth order 8
+
+
+def make_workload(seed, reference=False):
+    """The headline volume, its PSF and the Wiener-Butterworth backprojector of that PSF (generated
+    by the library for our arm, by the CPU restatement for the reference arm)."""
     from petakit5d_b200 import synth
     vol, psf = synth.single_volume_workload("omw_llsm", seed=seed)
-    psf_b = np.asfortranarray(psf[::-1, ::-1, ::-1])   # traditional backprojector (flipped PSF)
-    return vol, psf, psf_b
+    if reference:
+        from oracle import backprojector as OB
+        pb, _ = OB.wb_backprojector(psf, alpha=WB["alpha"], beta=WB["beta"], n=WB["n"], res_flag=WB["res_flag"])
+    else:
+        from petakit5d_b200 import backprojector as B
+        pb, _ = B.BackProjector(psf, "wiener-butterworth", WB["alpha"], WB["beta"], WB["n"], WB["res_flag"])
+    return vol, psf, np.asfortranarray(pb.astype(np.float32))
 
 
 def cpu_restatement_rate(vol, psf, psf_b, steps=1, warmup=0):
@@ -293,6 +303,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="omw_llsm", choices=["omw_llsm", "rl_small", "batched", "served", "large"])
+    ap.add_argument("--rate", type=float, default=200.0, help="served: Poisson arrival rate (requests/s)")
+    ap.add_argument("--requests", type=int, default=240, help="served: number of requests")
     ap.add_argument("--ncu-case", action="store_true",
                     help="run two device calls of the workload and exit (the case profiled with ncu)")
     args = ap.parse_args()
@@ -307,11 +320,15 @@ def main():
         torch.cuda.synchronize()
         return
 
+    if args.workload != "omw_llsm":
+        WORKLOADS[args.workload](args)
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     config = {"workload": "omw_llsm: 512x512x256 (x,y,z) uint16, 20k puncta + sinusoid bg + Poisson, "
-                          "64x64x101 lobed PSF, flipped-PSF backprojector, OMW 2 iterations, uint16 out",
+                          "64x64x101 lobed PSF, Wiener-Butterworth backprojector (alpha 0.005, beta 1e-3, "
+                          "order 8), OMW 2 iterations, uint16 out",
               "volume_xyz": [512, 512, 256], "psf_yxz": [64, 64, 101], "iterations": ITERS,
               "background": BACKGROUND, "parallelism": f"replicas x{world}",
               "l2": "working set 0.9 GB >> 126 MB L2 (no flush needed)"}
@@ -319,7 +336,7 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        vol, psf, psf_b = make_workload(seed=1)
+        vol, psf, psf_b = make_workload(seed=1, reference=True)
         cores = os.cpu_count()
         rate, dt = cpu_restatement_rate(vol, psf, psf_b, steps=args.steps, warmup=args.warmup)
         print(json.dumps({
@@ -375,6 +392,361 @@ def main():
                                           f"OTFs cached), {dt:.1f} s"}
     print(json.dumps(line), flush=True)
 
+
+
+# ====================================================================== further workloads
+def _events(stream):
+    import torch
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def _emit(line):
+    print(json.dumps(line), flush=True)
+
+
+def _u16_dev(vol, device):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(vol.T).view(np.int16)).to(device)
+
+
+def wl_rl_small(args):
+    """Config 1: one 128x128x64 volume, 31x31x41 Gaussian PSF, Biggs RL 20 iterations, float32 out."""
+    import torch
+    from petakit5d_b200 import _lib
+    from petakit5d_b200 import decon as D
+    from petakit5d_b200 import synth
+    from oracle import decon as O
+    if args.impl == "reference":
+        vol, psf = synth.single_volume_workload("rl_small", seed=1)
+        t0 = time.perf_counter()
+        for _ in range(max(1, args.steps)):
+            O.decon_lucy(vol, psf, 20, background=100, save16bit=False)
+        dt = (time.perf_counter() - t0) / max(1, args.steps)
+        v = vol.size / dt / 1e6
+        _emit({"impl": "reference", "metric": "deconvolved Mvoxel/s (RL, 20 iter)", "value": round(v, 3),
+               "unit": "Mvoxel/s", "workload": "rl_small", "cpu_baseline": {"value": round(v, 3), "unit": "Mvoxel/s",
+               "cores": os.cpu_count(), "kind": "port", "sample": "one 128x128x64 volume per step"}})
+        return
+    device = torch.device("cuda", 0)
+    vol, psf = synth.single_volume_workload("rl_small", seed=1)
+    ctx = _lib.Context(0)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=device)
+    d_in = _u16_dev(vol, device)
+    d_out = torch.empty(vol.T.shape, dtype=torch.float32, device=device)
+    step = lambda: D.decon_device("rl", d_in, "uint16", vol.shape, psf, None, 20, out=d_out, ctx=ctx,
+                                  stream=ctx.stream, Background=100.0, save16bit=False)
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    e0, e1 = _events(stream)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    J = d_out.cpu().numpy().transpose(2, 1, 0)
+    ref = O.decon_lucy(vol, psf, 20, background=100, save16bit=False, dtype=np.float32)
+    ref64 = O.decon_lucy(vol, psf, 20, background=100, save16bit=False, dtype=np.float64)
+    t0 = time.perf_counter()
+    O.decon_lucy(vol, psf, 20, background=100, save16bit=False)
+    cpu_dt = time.perf_counter() - t0
+    _emit({"metric": "deconvolved Mvoxel/s (RL, 20 iter)", "workload": "rl_small 128x128x64, 31x31x41 PSF",
+           "value": round(vol.size / (ms * 1e-3) / 1e6, 1), "unit": "Mvoxel/s", "ms_per_step": round(ms, 4),
+           "rel_l2_vs_fp32_oracle": O.rel_l2(J, ref), "rel_l2_vs_fp64_oracle": O.rel_l2(J, ref64),
+           "cpu_baseline": {"value": round(vol.size / cpu_dt / 1e6, 3), "unit": "Mvoxel/s", "cores": os.cpu_count(),
+                            "kind": "port", "sample": "one volume"}})
+
+
+def _chunk_set(device, n_chunks=96, seed=3, border=16):
+    """Config 3 chunks generated on the GPU, copied to pinned host memory (numpy views)."""
+    import torch
+    from petakit5d_b200 import synth
+    rng = np.random.Generator(np.random.PCG64(seed))
+    psfs = [synth.gaussian_psf((31, 31, 41), s, 3.0) for s in (1.3, 1.5, 1.8)]
+    chunks, ids, boxes, pinned = [], [], [], []
+    density = 200.0 / (128 * 128 * 64)
+    for i in range(n_chunks):
+        cy, cx = int(rng.choice((192, 256, 320, 384))), int(rng.choice((192, 256, 320, 384)))
+        cz = int(rng.choice((96, 128, 192, 256)))
+        pid = int(rng.integers(0, 3))
+        shape = (cy + 2 * border, cx + 2 * border, cz + 2 * border)
+        t = synth.puncta_volume_torch(shape, int(round(density * np.prod(shape))), psfs[pid], seed * 1000 + i,
+                                      100.0, device=device)
+        h = t.cpu().pin_memory()
+        pinned.append(h)
+        chunks.append(h.numpy().view(np.uint16).T)      # (ny, nx, nz) Fortran view of pinned memory
+        ids.append(pid)
+        boxes.append([border + 1, border + 1, border + 1, border + cy, border + cx, border + cz])
+    torch.cuda.empty_cache()
+    return chunks, pinned, psfs, ids, boxes
+
+
+def wl_batched(args):
+    """Config 3: 96 uneven chunks with 16-voxel borders, 3 PSFs, OMW 2 iterations; batched call
+    (shared launches, pipelined copies) against 96 plain per-chunk calls, host buffers both ways."""
+    import torch
+    from petakit5d_b200 import _lib
+    from petakit5d_b200 import backprojector as B
+    from petakit5d_b200 import chunking as K
+    from petakit5d_b200 import decon as D
+    device = torch.device("cuda", 0)
+    chunks, pinned, psfs, ids, boxes = _chunk_set(device)
+    if args.impl == "reference":
+        from oracle import backprojector as OB
+        from oracle import decon as O
+        bps = [OB.omw_backprojector_generation(p, 0.005, False, otf_cum_thresh=0.6)[0] for p in psfs]
+        t0 = time.perf_counter()
+        nvox = 0
+        sample = chunks[:4]
+        for c, pid, bb in zip(sample, ids[:4], boxes[:4]):
+            O.decon_lucy_omw(c, psfs[pid], bps[pid], 2, background=100, bbox=bb)
+            nvox += (bb[3] - bb[0] + 1) * (bb[4] - bb[1] + 1) * (bb[5] - bb[2] + 1)
+        v = nvox / (time.perf_counter() - t0) / 1e6
+        _emit({"impl": "reference", "metric": "batched OMW Mvoxel/s (output core voxels)", "value": round(v, 3),
+               "unit": "Mvoxel/s", "workload": "batched", "cpu_baseline": {"value": round(v, 3), "unit": "Mvoxel/s",
+               "cores": os.cpu_count(), "kind": "port", "sample": "first 4 of the 96 chunks"}})
+        return
+    bps = [B.omw_backprojector_generation(p, 0.005, False, OTFCumThresh=0.6)[0] for p in psfs]
+    ctx = _lib.Context(0)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=device)
+    core = sum((b[3] - b[0] + 1) * (b[4] - b[1] + 1) * (b[5] - b[2] + 1) for b in boxes)
+    outs = [np.empty((b[3] - b[0] + 1, b[4] - b[1] + 1, b[5] - b[2] + 1), np.uint16, order="F") for b in boxes]
+    pouts = []
+    for i, o in enumerate(outs):       # pinned outputs
+        t = torch.empty(o.shape[::-1], dtype=torch.int16).pin_memory()
+        pouts.append(t)
+        outs[i] = t.numpy().view(np.uint16).T
+
+    def batched():
+        K.batch_decon(chunks, psfs, ids, 2, "omw", bps, boxes, ctx=ctx, outputs=outs, Background=100)
+
+    def plain():
+        for c, pid, bb, o in zip(chunks, ids, boxes, outs):
+            p = D._params({"background": 100.0, "dampfactor": 1.0, "scalefactor": 1.0, "deconoffset": 0.0,
+                           "edgeerosion": 0, "save16bit": True, "bbox": bb})
+            pf = np.asfortranarray(psfs[pid], np.float32)
+            pb = np.asfortranarray(bps[pid], np.float32)
+            _lib.check(_lib.lib.pk_decon_lucy_omw(ctx.handle, c.ctypes.data, _lib.PK_U16, _lib.i64x3(c.shape),
+                                                  pf.ctypes.data, _lib.i64x3(pf.shape), pb.ctypes.data,
+                                                  _lib.i64x3(pb.shape), 2, p, o.ctypes.data))
+
+    res = {}
+    for name, fn in (("plain", plain), ("batched", batched)):
+        fn()                                   # warm-up (OTFs cached)
+        torch.cuda.synchronize()
+        reps = max(1, min(args.steps, 3))
+        e0, e1 = _events(stream)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        res[name] = e0.elapsed_time(e1) / reps
+    ref_out = [o.copy() for o in outs]
+    batched()
+    same = all(np.array_equal(a, b) for a, b in zip(ref_out, outs))
+    _emit({"metric": "batched OMW Mvoxel/s (output core voxels, host buffers, copies included)",
+           "workload": "96 uneven chunks (core x,y in {192..384}, z in {96..256}, +16 borders), 3 PSFs, OMW x2",
+           "value": round(core / (res["batched"] * 1e-3) / 1e6, 1), "unit": "Mvoxel/s",
+           "plain_per_chunk": round(core / (res["plain"] * 1e-3) / 1e6, 1),
+           "speedup_vs_plain": round(res["plain"] / res["batched"], 3), "ms_batched": round(res["batched"], 2),
+           "ms_plain": round(res["plain"], 2), "batched_equals_plain": same, "core_voxels": int(core)})
+
+
+def wl_served(args):
+    """Config 4: open-loop Poisson requests (90% chunk sizes, 10% 768x768x384; 80% OMW x2, 20% RL x10;
+    3 PSFs; 150 GB budget) through the continuous-batching server, against the same requests run one
+    after another with the plain host call."""
+    import threading
+    import torch
+    from petakit5d_b200 import _lib
+    from petakit5d_b200 import backprojector as B
+    from petakit5d_b200 import serve as SV
+    from petakit5d_b200 import synth
+    device = torch.device("cuda", 0)
+    rng = np.random.Generator(np.random.PCG64(17))
+    psfs = [synth.gaussian_psf((31, 31, 41), s, 3.0) for s in (1.3, 1.5, 1.8)]
+    bps = [B.omw_backprojector_generation(p, 0.005, False, OTFCumThresh=0.6)[0] for p in psfs]
+    pool = {}
+    keep = []
+
+    def volume(shape):
+        if shape not in pool:
+            t = synth.puncta_volume_torch(shape, int(np.prod(shape) * 200 / (128 * 128 * 64)), psfs[0],
+                                          len(pool) + 5, 100.0, device=device)
+            h = t.cpu().pin_memory()
+            keep.append(h)
+            pool[shape] = h.numpy().view(np.uint16).T
+        return pool[shape]
+
+    reqs = []
+    for i in range(args.requests):
+        if rng.random() < 0.9:
+            shape = (int(rng.choice((192, 256, 320, 384))) + 32, int(rng.choice((192, 256, 320, 384))) + 32,
+                     int(rng.choice((96, 128, 192, 256))) + 32)
+        else:
+            shape = (768, 768, 384)
+        method = "omw" if rng.random() < 0.8 else "rl"
+        reqs.append((volume(shape), int(rng.integers(0, 3)), method, 2 if method == "omw" else 10))
+    torch.cuda.empty_cache()
+    arrivals = np.cumsum(rng.exponential(1.0 / args.rate, size=len(reqs)))
+    nvox = sum(int(np.prod(r[0].shape)) for r in reqs)
+    ctx = _lib.Context(0)
+    srv = SV.Server(ctx, budget_bytes=150e9, max_batch=64, borrow_inputs=True)
+    for i in range(3):
+        srv.add_psf(i, psfs[i], bps[i])
+    # warm-up: every (size, psf) OTF, and the kernels
+    warm = [srv.submit(v, pid, m, 1, Background=100) for v, pid, m, _ in reqs[:8]]
+    for w in warm:
+        srv.wait(w)
+    lat = [None] * len(reqs)
+    ids = [None] * len(reqs)
+    done = threading.Semaphore(0)
+
+    def waiter(q):
+        while True:
+            i = q.get()
+            if i is None:
+                return
+            _, ms = srv.wait(ids[i])
+            lat[i] = ms
+            done.release()
+
+    import queue
+    q = queue.Queue()
+    ws = [threading.Thread(target=waiter, args=(q,), daemon=True) for _ in range(8)]
+    for w in ws:
+        w.start()
+    t0 = time.perf_counter()
+    for i, (v, pid, m, it) in enumerate(reqs):
+        now = time.perf_counter() - t0
+        if arrivals[i] > now:
+            time.sleep(arrivals[i] - now)
+        ids[i] = srv.submit(v, pid, m, it, Background=100)
+        q.put(i)
+    for _ in reqs:
+        done.acquire()
+    wall = time.perf_counter() - t0
+    for _ in ws:
+        q.put(None)
+    st = srv.stats()
+    srv.close()
+    # the same requests, one plain host call after another
+    out = {}
+    t1 = time.perf_counter()
+    for v, pid, m, it in reqs:
+        o = out.setdefault(v.shape, np.empty(v.shape, np.uint16, order="F"))
+        p = D_params()
+        pf = np.asfortranarray(psfs[pid], np.float32)
+        if m == "omw":
+            pb = np.asfortranarray(bps[pid], np.float32)
+            _lib.check(_lib.lib.pk_decon_lucy_omw(ctx.handle, v.ctypes.data, _lib.PK_U16, _lib.i64x3(v.shape),
+                                                  pf.ctypes.data, _lib.i64x3(pf.shape), pb.ctypes.data,
+                                                  _lib.i64x3(pb.shape), it, p, o.ctypes.data))
+        else:
+            _lib.check(_lib.lib.pk_decon_lucy(ctx.handle, v.ctypes.data, _lib.PK_U16, _lib.i64x3(v.shape),
+                                              pf.ctypes.data, _lib.i64x3(pf.shape), it, p, o.ctypes.data, None))
+    plain = time.perf_counter() - t1
+    L = np.array(lat)
+    _emit({"metric": "served Mvoxel/s and request latency", "workload":
+           f"{len(reqs)} open-loop Poisson requests at {args.rate} req/s (90% chunk sizes, 10% 768x768x384; 80% OMW x2, "
+           "20% RL x10; 3 PSFs; 150 GB budget)",
+           "value": round(nvox / wall / 1e6, 1), "unit": "Mvoxel/s",
+           "latency_ms": {"p50": round(float(np.percentile(L, 50)), 2), "p95": round(float(np.percentile(L, 95)), 2),
+                          "p99": round(float(np.percentile(L, 99)), 2), "max": round(float(L.max()), 2)},
+           "plain_sequential": round(nvox / plain / 1e6, 1), "speedup_vs_plain": round(plain / wall, 3),
+           "wall_s": round(wall, 3), "plain_s": round(plain, 3), "rounds": st["rounds"],
+           "peak_inflight_GB": round(st["peak_inflight_bytes"] / 1e9, 2)})
+
+
+def D_params():
+    from petakit5d_b200 import decon as D
+    return D._params({"background": 100.0, "dampfactor": 1.0, "scalefactor": 1.0, "deconoffset": 0.0,
+                      "edgeerosion": 0, "save16bit": True, "bbox": None})
+
+
+def wl_large(args):
+    """Config 5: 2048x2048x1024 volume (2M puncta), OMW x2 with the small PSF, whole volume resident
+    in HBM and as 512^3 chunks with 32-voxel overlap through the batched path (device buffers)."""
+    import torch
+    from petakit5d_b200 import _lib
+    from petakit5d_b200 import backprojector as B
+    from petakit5d_b200 import chunking as K
+    from petakit5d_b200 import decon as D
+    from petakit5d_b200 import synth
+    device = torch.device("cuda", 0)
+    shape = (2048, 2048, 1024)
+    psf = synth.gaussian_psf((31, 31, 41), 1.3, 3.0)
+    bp = B.omw_backprojector_generation(psf, 0.005, False, OTFCumThresh=0.6)[0]
+    d_in = synth.puncta_volume_torch(shape, 2_000_000, psf, 7, 100.0, device=device)
+    torch.cuda.empty_cache()
+    N = int(np.prod(shape))
+    ctx = _lib.Context(0)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=device)
+    d_out = torch.empty_like(d_in)
+    run = lambda: D.decon_device("omw", d_in, "uint16", shape, psf, bp, 2, out=d_out, ctx=ctx, stream=ctx.stream,
+                                 Background=100.0)
+    run()
+    torch.cuda.synchronize()
+    e0, e1 = _events(stream)
+    e0.record(stream)
+    run()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    whole_ms = e0.elapsed_time(e1)
+    ctx.reset()
+    # chunked: 512^3 regions, border 32, through the batched path on device buffers
+    bb, rb, _ = K.zarr_chunk_coordinates(shape, (512, 512, 512), (512, 512, 512), None, False, 32)
+    chunks, outs, boxes = [], [], []
+    for b, r in zip(bb, rb):
+        c = d_in[b[2] - 1:b[5], b[1] - 1:b[4], b[0] - 1:b[3]].contiguous()
+        chunks.append(c)
+        st_ = r[:3] - b[:3] + 1
+        en = r[3:] - b[:3] + 1
+        boxes.append([*st_, *en])
+        outs.append(torch.empty((en[2] - st_[2] + 1, en[1] - st_[1] + 1, en[0] - st_[0] + 1), dtype=torch.int16,
+                                device=device))
+    n = len(chunks)
+    arr = (_lib.Chunk * n)()
+    for i, (c, o, bx) in enumerate(zip(chunks, outs, boxes)):
+        arr[i].in_ = c.data_ptr()
+        arr[i].dims = _lib.i64x3((c.shape[2], c.shape[1], c.shape[0]))
+        arr[i].psf_id = 0
+        arr[i].has_bbox = 1
+        for k in range(6):
+            arr[i].bbox[k] = int(bx[k])
+        arr[i].out = o.data_ptr()
+    pf = np.asfortranarray(psf, np.float32)
+    pb = np.asfortranarray(bp, np.float32)
+    fp = (_lib.C.c_void_p * 1)(pf.ctypes.data)
+    bpp = (_lib.C.c_void_p * 1)(pb.ctypes.data)
+    dims = np.array(pf.shape, np.int64)
+    p = D_params()
+    call = lambda: _lib.check(_lib.lib.pk_batch_decon(ctx.handle, 1, n, arr, _lib.PK_U16, 1, fp, bpp, dims.ctypes.data, 2,
+                                                      p, 0, 1))
+    call()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    call()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    chunk_ms = e0.elapsed_time(e1)
+    stitched = torch.empty_like(d_in)
+    for r, o in zip(rb, outs):
+        stitched[r[2] - 1:r[5], r[1] - 1:r[4], r[0] - 1:r[3]] = o
+    a = d_out.view(torch.int16).to(torch.int32) & 0xFFFF
+    b2 = stitched.view(torch.int16).to(torch.int32) & 0xFFFF
+    gap = float(torch.linalg.vector_norm((a - b2).double()) / torch.linalg.vector_norm(a.double()))
+    _emit({"metric": "deconvolved Mvoxel/s (OMW, 2 iter), whole volume vs 512^3 chunks",
+           "workload": "2048x2048x1024 uint16, 2M puncta, 31x31x41 PSF, OMW backprojector, OMW x2",
+           "value": round(N / (whole_ms * 1e-3) / 1e6, 1), "unit": "Mvoxel/s", "ms_whole": round(whole_ms, 2),
+           "chunked_value": round(N / (chunk_ms * 1e-3) / 1e6, 1), "ms_chunked": round(chunk_ms, 2),
+           "chunks": n, "rel_l2_whole_vs_chunked": gap,
+           "reference_cpu": "not run (the float32 CPU restatement needs ~100 GB of host RAM for this volume)"})
+
+
+WORKLOADS = {"rl_small": wl_rl_small, "batched": wl_batched, "served": wl_served, "large": wl_large}
 
 if __name__ == "__main__":
     main()

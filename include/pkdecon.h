@@ -193,13 +193,15 @@ typedef struct {
     int64_t budget_bytes;      /* HBM admission budget for in-flight work buffers */
     int32_t max_batch;         /* max requests advanced together */
     int32_t queue_capacity;    /* max queued (not yet admitted) requests */
+    int32_t borrow_inputs;     /* 0: copy each volume at submit; 1: read the caller's buffer (keep it
+                                  valid, ideally pinned, until pk_server_wait returns) */
 } pk_server_config;
 
 /* Register a PSF pair (psf_b NULL for RL-only) under psf_id; OTFs are cached per (psf_id, size). */
 PK_API pk_server* pk_server_create(pk_ctx* ctx, const pk_server_config* cfg);
 PK_API pk_status pk_server_add_psf(pk_server* s, int32_t psf_id, const float* psf_f, const float* psf_b,
                             const int64_t psf_dims[3]);
-/* Submit a request: host uint16 volume (copied at submit), method 1 = OMW, 0 = RL.
+/* Submit a request: host uint16 volume (copied at submit unless borrow_inputs), method 1 = OMW, 0 = RL.
  * Returns a request id (>= 0) or -pk_status. */
 PK_API int64_t pk_server_submit(pk_server* s, const uint16_t* vol, const int64_t dims[3], int32_t psf_id,
                          int32_t method, int32_t numit, const pk_decon_params* params);

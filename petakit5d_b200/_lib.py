@@ -44,7 +44,8 @@ class Chunk(C.Structure):
 
 
 class ServerConfig(C.Structure):
-    _fields_ = [("budget_bytes", C.c_int64), ("max_batch", C.c_int32), ("queue_capacity", C.c_int32)]
+    _fields_ = [("budget_bytes", C.c_int64), ("max_batch", C.c_int32), ("queue_capacity", C.c_int32),
+                ("borrow_inputs", C.c_int32)]
 
 
 I64x3 = C.c_int64 * 3

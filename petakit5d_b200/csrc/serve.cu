@@ -46,7 +46,8 @@ enum ReqState { RQ_QUEUED, RQ_ACTIVE, RQ_DONE, RQ_FAILED, RQ_CANCELLED };
 
 struct Request {
     int64_t id;
-    uint16_t* vol = nullptr;         // pinned staging copy of the input
+    uint16_t* vol = nullptr;         // pinned staging copy of the input (copy mode)
+    const uint16_t* src = nullptr;   // the bytes the upload reads (staging copy or the caller's buffer)
     size_t vol_bytes = 0;
     int64_t dims[3];
     int psf_id, method, numit;
@@ -224,7 +225,7 @@ pk_status pk_server::admit(const std::shared_ptr<Request>& r) {
     // upload on the copy stream (pinned source); the compute stream waits for it before the first pass
     PK_CUDA(cudaEventRecord(r->ev_up, c->stream));          // the allocation is ordered on the compute stream
     PK_CUDA(cudaStreamWaitEvent(up, r->ev_up, 0));
-    PK_CUDA(cudaMemcpyAsync(r->dev, r->vol, raw_b, cudaMemcpyHostToDevice, up));
+    PK_CUDA(cudaMemcpyAsync(r->dev, r->src, raw_b, cudaMemcpyHostToDevice, up));
     PK_CUDA(cudaEventRecord(r->ev_up, up));
     PK_CUDA(cudaStreamWaitEvent(c->stream, r->ev_up, 0));
     build_steps(*r, b, of, ob);
@@ -342,6 +343,7 @@ pk_server* pk_server_create(pk_ctx* ctx, const pk_server_config* cfg) {
     s->cfg.budget_bytes = cfg && cfg->budget_bytes > 0 ? cfg->budget_bytes : (int64_t)150e9;
     s->cfg.max_batch = cfg && cfg->max_batch > 0 ? cfg->max_batch : 64;
     s->cfg.queue_capacity = cfg && cfg->queue_capacity > 0 ? cfg->queue_capacity : 1024;
+    s->cfg.borrow_inputs = cfg ? cfg->borrow_inputs : 0;
     cudaSetDevice(ctx->device);
     if (cudaStreamCreateWithFlags(&s->up, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&s->down, cudaStreamNonBlocking) != cudaSuccess) {
@@ -394,12 +396,17 @@ int64_t pk_server_submit(pk_server* s, const uint16_t* vol, const int64_t dims[3
     auto r = std::make_shared<Request>();
     const int64_t n = dims[0] * dims[1] * dims[2];
     r->vol_bytes = (size_t)n * 2;
-    cudaSetDevice(s->ctx->device);
-    if (cudaMallocHost(&r->vol, r->vol_bytes) != cudaSuccess) {
-        cudaGetLastError();
-        return -(int64_t)pk_fail(PK_ERR_NOMEM, "pinned staging allocation failed");
+    if (s->cfg.borrow_inputs) {
+        r->src = vol;
+    } else {
+        cudaSetDevice(s->ctx->device);
+        if (cudaMallocHost(&r->vol, r->vol_bytes) != cudaSuccess) {
+            cudaGetLastError();
+            return -(int64_t)pk_fail(PK_ERR_NOMEM, "pinned staging allocation failed");
+        }
+        memcpy(r->vol, vol, r->vol_bytes);
+        r->src = r->vol;
     }
-    memcpy(r->vol, vol, r->vol_bytes);
     lk.lock();
     r->id = s->next_id++;
     for (int i = 0; i < 3; i++) r->dims[i] = dims[i];

@@ -21,9 +21,12 @@ from .decon import _params, _parse
 
 
 class Server:
-    def __init__(self, ctx=None, budget_bytes=150e9, max_batch=64, queue_capacity=1024):
+    def __init__(self, ctx=None, budget_bytes=150e9, max_batch=64, queue_capacity=1024, borrow_inputs=False):
+        """borrow_inputs: read each submitted array in place (keep it alive and unchanged, ideally in
+        pinned memory, until wait() returns) instead of copying it at submit."""
         self.ctx = ctx or _lib.default_context()
-        cfg = ServerConfig(int(budget_bytes), int(max_batch), int(queue_capacity))
+        cfg = ServerConfig(int(budget_bytes), int(max_batch), int(queue_capacity), 1 if borrow_inputs else 0)
+        self._borrowed = {}
         h = lib.pk_server_create(self.ctx.handle, cfg)
         if not h:
             raise PkError(_lib.PK_ERR_INVALID, _lib.last_error())
@@ -47,6 +50,8 @@ class Server:
                                    int(numit), p)
         if rid < 0:
             raise PkError(-rid, _lib.last_error())
+        if self._borrowed is not None:
+            self._borrowed[rid] = v            # keep the borrowed buffer alive until wait()
         od = i64x3([0, 0, 0])
         check(lib.pk_output_dims(i64x3(v.shape), p, od))
         self._meta[rid] = (tuple(od), np.uint16 if p.save16bit else np.float32)
@@ -59,6 +64,7 @@ class Server:
         st = lib.pk_server_wait(self.handle, int(rid), ptr(out), int(timeout_ms), C.byref(lat))
         if st != _lib.PK_ERR_TIMEOUT:
             self._meta.pop(rid, None)
+            self._borrowed.pop(rid, None)
         check(st)
         return out, lat.value
 

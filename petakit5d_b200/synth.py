@@ -145,3 +145,67 @@ def chunk_workload(n_chunks=96, seed=3, border=16, core_xy=(192, 256, 320, 384),
         ids.append(pid)
         bboxes.append([border + 1, border + 1, border + 1, border + cy, border + cx, border + cz])
     return chunks, psfs, ids, bboxes
+
+
+# ---------------------------------------------------------------- GPU generator for large workloads
+def puncta_volume_torch(shape_yxz, n_puncta, psf, seed, background=100.0, device="cuda", sinusoid=None):
+    """The same recipe as ``puncta_volume`` run with torch on ``device`` (for volumes too large to
+    generate quickly on the host).  Returns an int16 tensor shaped (nz, nx, ny) whose bits are the
+    uint16 voxels, i.e. the column-major [ny nx nz] volume.  ``sinusoid``: dict of
+    ``sinusoid_background`` arguments added to ``background``."""
+    import torch
+    ny, nx, nz = (int(v) for v in shape_yxz)
+    g = torch.Generator(device=device)
+    g.manual_seed(int(seed))
+    img = torch.zeros(nz * nx * ny, dtype=torch.float32, device=device)
+    n = int(n_puncta)
+    radius = 4
+    off = torch.arange(-radius, radius + 1, device=device)
+    oz, ox, oy = torch.meshgrid(off, off, off, indexing="ij")
+    oy, ox, oz = oy.reshape(1, -1), ox.reshape(1, -1), oz.reshape(1, -1)
+    dims = torch.tensor([ny, nx, nz], device=device, dtype=torch.float32)
+    step = 1 << 16
+    for s in range(0, n, step):
+        m = min(step, n - s)
+        pos = torch.rand((m, 3), generator=g, device=device) * dims
+        amp = 200.0 + 1800.0 * torch.rand((m, 1), generator=g, device=device)
+        b = torch.floor(pos).to(torch.int64)
+        iy, ix, iz = b[:, 0:1] + oy, b[:, 1:2] + ox, b[:, 2:3] + oz
+        d2 = (iy - pos[:, 0:1]) ** 2 + (ix - pos[:, 1:2]) ** 2 + (iz - pos[:, 2:3]) ** 2
+        val = amp * torch.exp(-d2 / 2.0)
+        idx = (iy % ny) + ny * ((ix % nx) + nx * (iz % nz))
+        img.index_add_(0, idx.reshape(-1), val.reshape(-1))
+        del pos, amp, b, iy, ix, iz, d2, val, idx
+    img = img.view(nz, nx, ny)
+    p = np.asarray(psf, np.float64)
+    p = (p / p.sum()).astype(np.float32)
+    py, px, pz = p.shape
+    ker = torch.zeros((nz, nx, ny), dtype=torch.float32, device=device)
+    ker[:pz, :px, :py] = torch.from_numpy(np.ascontiguousarray(p.transpose(2, 1, 0))).to(device)
+    ker = torch.roll(ker, shifts=(-(pz // 2), -(px // 2), -(py // 2)), dims=(0, 1, 2))
+    H = torch.fft.rfftn(ker)
+    del ker
+    F = torch.fft.rfftn(img)
+    del img
+    F *= H
+    del H
+    clean = torch.fft.irfftn(F, s=(nz, nx, ny))
+    del F
+    clean += float(background)
+    if sinusoid is not None:
+        period = float(sinusoid.get("period", 200.0))
+        amp = float(sinusoid.get("amplitude", 300.0))
+        offv = float(sinusoid.get("offset", 100.0))
+        w = 2 * np.pi / period
+        sy = torch.sin(w * torch.arange(ny, device=device, dtype=torch.float32)).view(1, 1, ny)
+        sx = torch.sin(w * torch.arange(nx, device=device, dtype=torch.float32)).view(1, nx, 1)
+        sz = torch.sin(w * torch.arange(nz, device=device, dtype=torch.float32)).view(nz, 1, 1)
+        clean += offv + amp * 0.5 * (1.0 + sz * sx * sy)
+    clean.clamp_(min=0)
+    noisy = torch.poisson(clean, generator=g)
+    del clean
+    noisy.clamp_(0, 65535)
+    v = noisy.to(torch.int32)
+    del noisy
+    v = torch.where(v > 32767, v - 65536, v).to(torch.int16)
+    return v
