@@ -1,0 +1,163 @@
+// MEX gateway: MATLAB -> libpkdecon.so.  Build inside MATLAB with
+//   mex -R2018a pkdecon_mex.cpp -I<repo>/include -L<repo>/petakit5d_b200/lib -lpkdecon
+// (mex.h comes with MATLAB; this file is not compiled by the repository's own build).
+//
+//   J        = pkdecon_mex('omw', I, PSF_f, PSF_b, NUMIT, opts)   % decon_lucy_omw_function
+//   [J, k]   = pkdecon_mex('rl', I, PSF, NUMIT, opts)             % decon_lucy_function
+//   [b, otf, absc, mask] = pkdecon_mex('omw_bp', psf, alpha, skewed, thresh, area, hann, minInt)
+//   [bp, otf] = pkdecon_mex('wb_bp', psf, alpha, beta, n, resFlag, iRes)
+//   pkdecon_mex('reset')                                           % reset(gpuDevice) analogue
+// opts: struct with the reference's name/value fields (Background, save16bit, dampFactor,
+// scaleFactor, deconOffset, EdgeErosion, bbox).  Errors are raised with mexErrMsgIdAndTxt using the
+// identifier "pkdecon:<status>" and pk_last_error() (the convention of crop3d_mex.c:36-63).
+#include <cstring>
+#include <string>
+
+#include "mex.h"
+#include "pkdecon.h"
+
+static pk_ctx* g_ctx = nullptr;
+
+static void at_exit() {
+    if (g_ctx) pk_ctx_destroy(g_ctx);
+    g_ctx = nullptr;
+}
+
+static pk_ctx* ctx() {
+    if (!g_ctx) {
+        g_ctx = pk_ctx_create(0);
+        if (!g_ctx) mexErrMsgIdAndTxt("pkdecon:cuda", "%s", pk_last_error());
+        mexAtExit(at_exit);
+    }
+    return g_ctx;
+}
+
+static void check(pk_status s) {
+    static const char* names[] = {"ok", "invalid", "unsupported", "cuda", "nomem", "busy", "timeout", "cancelled",
+                                  "emptyOTFMask"};
+    if (s != PK_OK) {
+        std::string id = std::string("pkdecon:") + (s >= 0 && s <= 8 ? names[s] : "unknown");
+        mexErrMsgIdAndTxt(id.c_str(), "%s", pk_last_error());
+    }
+}
+
+static void dims3(const mxArray* a, int64_t d[3]) {
+    const mwSize nd = mxGetNumberOfDimensions(a);
+    const mwSize* s = mxGetDimensions(a);
+    if (nd > 3) mexErrMsgIdAndTxt("pkdecon:invalid", "at most 3 dimensions");
+    for (int i = 0; i < 3; i++) d[i] = i < (int)nd ? (int64_t)s[i] : 1;
+}
+
+static double field(const mxArray* opts, const char* name, double def) {
+    if (!opts || !mxIsStruct(opts)) return def;
+    const mxArray* f = mxGetField(opts, 0, name);
+    if (!f || mxIsEmpty(f)) return def;
+    return mxGetScalar(f);
+}
+
+static void params(const mxArray* opts, pk_decon_params* p) {
+    pk_params_default(p);
+    p->background = field(opts, "Background", 0.0);
+    p->save16bit = field(opts, "save16bit", 1.0) != 0;
+    p->damp_factor = field(opts, "dampFactor", 1.0);
+    p->scale_factor = field(opts, "scaleFactor", 1.0);
+    p->decon_offset = field(opts, "deconOffset", 0.0);
+    p->edge_erosion = (int32_t)field(opts, "EdgeErosion", 0.0);
+    const mxArray* bb = opts && mxIsStruct(opts) ? mxGetField(opts, 0, "bbox") : nullptr;
+    if (bb && !mxIsEmpty(bb)) {
+        if (mxGetNumberOfElements(bb) != 6) mexErrMsgIdAndTxt("pkdecon:invalid", "bbox must have 6 elements");
+        const double* v = mxGetPr(bb);
+        p->has_bbox = 1;
+        for (int i = 0; i < 6; i++) p->bbox[i] = (int64_t)v[i];
+    }
+}
+
+static pk_dtype dtype_of(const mxArray* a) {
+    switch (mxGetClassID(a)) {
+        case mxUINT16_CLASS: return PK_U16;
+        case mxSINGLE_CLASS: return PK_F32;
+        case mxDOUBLE_CLASS: return PK_F64;
+        default: mexErrMsgIdAndTxt("pkdecon:invalid", "I must be uint16, single or double");
+    }
+    return PK_U16;
+}
+
+static const float* single_psf(const mxArray* a) {
+    if (mxGetClassID(a) != mxSINGLE_CLASS) mexErrMsgIdAndTxt("pkdecon:invalid", "PSFs must be single (use single(psf))");
+    return (const float*)mxGetData(a);
+}
+
+static mxArray* make_out(const int64_t od[3], bool u16) {
+    const mwSize d[3] = {(mwSize)od[0], (mwSize)od[1], (mwSize)od[2]};
+    return mxCreateNumericArray(3, d, u16 ? mxUINT16_CLASS : mxSINGLE_CLASS, mxREAL);
+}
+
+void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
+    if (nrhs < 1 || !mxIsChar(prhs[0])) mexErrMsgIdAndTxt("pkdecon:invalid", "first argument: command string");
+    char cmd[32];
+    mxGetString(prhs[0], cmd, sizeof(cmd));
+    if (!strcmp(cmd, "reset")) {
+        check(pk_ctx_reset(ctx()));
+        return;
+    }
+    if (!strcmp(cmd, "omw") || !strcmp(cmd, "rl")) {
+        const bool omw = !strcmp(cmd, "omw");
+        const int base = omw ? 5 : 4;
+        if (nrhs < base) mexErrMsgIdAndTxt("pkdecon:invalid", "not enough arguments");
+        const mxArray* I = prhs[1];
+        int64_t d[3], pf[3], pb[3], od[3];
+        dims3(I, d);
+        dims3(prhs[2], pf);
+        pk_decon_params p;
+        params(nrhs > base ? prhs[base] : nullptr, &p);
+        pk_output_dims(d, &p, od);
+        plhs[0] = make_out(od, p.save16bit != 0);
+        if (omw) {
+            dims3(prhs[3], pb);
+            check(pk_decon_lucy_omw(ctx(), mxGetData(I), dtype_of(I), d, single_psf(prhs[2]), pf, single_psf(prhs[3]),
+                                    pb, (int32_t)mxGetScalar(prhs[4]), &p, mxGetData(plhs[0])));
+        } else {
+            int32_t k = 0;
+            check(pk_decon_lucy(ctx(), mxGetData(I), dtype_of(I), d, single_psf(prhs[2]), pf,
+                                (int32_t)mxGetScalar(prhs[3]), &p, mxGetData(plhs[0]), &k));
+            if (nlhs > 1) plhs[1] = mxCreateDoubleScalar(k);
+        }
+        return;
+    }
+    if (!strcmp(cmd, "omw_bp")) {
+        if (nrhs < 8) mexErrMsgIdAndTxt("pkdecon:invalid", "omw_bp: psf, alpha, skewed, thresh, area, hann, minInt");
+        int64_t pd[3];
+        dims3(prhs[1], pd);
+        const int32_t skewed = mxIsEmpty(prhs[3]) ? -1 : (mxGetScalar(prhs[3]) != 0);
+        const double* hann = mxGetPr(prhs[6]);
+        const mwSize dd[3] = {(mwSize)pd[0], (mwSize)pd[1], (mwSize)pd[2]};
+        plhs[0] = mxCreateNumericArray(3, dd, mxSINGLE_CLASS, mxREAL);
+        mxArray* otf = mxCreateNumericArray(3, dd, mxSINGLE_CLASS, mxCOMPLEX);   // interleaved (R2018a API)
+        mxArray* absc = mxCreateNumericArray(3, dd, mxSINGLE_CLASS, mxREAL);
+        mxArray* mask = mxCreateNumericArray(3, dd, mxUINT8_CLASS, mxREAL);
+        check(pk_omw_backprojector(ctx(), single_psf(prhs[1]), pd, mxGetScalar(prhs[2]), skewed, mxGetScalar(prhs[4]),
+                                   mxGetScalar(prhs[5]), hann[0], hann[1], mxGetScalar(prhs[7]),
+                                   (float*)mxGetData(plhs[0]), (float*)mxGetComplexSingles(otf),
+                                   (float*)mxGetData(absc), (uint8_t*)mxGetData(mask)));
+        if (nlhs > 1) plhs[1] = otf; else mxDestroyArray(otf);
+        if (nlhs > 2) plhs[2] = absc; else mxDestroyArray(absc);
+        if (nlhs > 3) plhs[3] = mask; else mxDestroyArray(mask);
+        return;
+    }
+    if (!strcmp(cmd, "wb_bp")) {
+        if (nrhs < 6) mexErrMsgIdAndTxt("pkdecon:invalid", "wb_bp: psf, alpha, beta, n, resFlag[, iRes]");
+        int64_t pd[3];
+        dims3(prhs[1], pd);
+        double ires[3] = {0, 0, 0};
+        if (nrhs > 6 && mxGetNumberOfElements(prhs[6]) == 3) memcpy(ires, mxGetPr(prhs[6]), sizeof(ires));
+        const mwSize dd[3] = {(mwSize)pd[0], (mwSize)pd[1], (mwSize)pd[2]};
+        plhs[0] = mxCreateNumericArray(3, dd, mxDOUBLE_CLASS, mxREAL);
+        mxArray* otf = mxCreateNumericArray(3, dd, mxDOUBLE_CLASS, mxCOMPLEX);
+        check(pk_wb_backprojector(ctx(), single_psf(prhs[1]), pd, mxGetScalar(prhs[2]), mxGetScalar(prhs[3]),
+                                  (int32_t)mxGetScalar(prhs[4]), (int32_t)mxGetScalar(prhs[5]), ires,
+                                  mxGetPr(plhs[0]), (double*)mxGetComplexDoubles(otf)));
+        if (nlhs > 1) plhs[1] = otf; else mxDestroyArray(otf);
+        return;
+    }
+    mexErrMsgIdAndTxt("pkdecon:invalid", "unknown command '%s'", cmd);
+}
