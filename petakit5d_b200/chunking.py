@@ -125,3 +125,11 @@ def decon_large_in_memory(volume, psf, numit=2, method="omw", psf_b=None, batch_
     for r, o in zip(rb, outs):
         out[r[0] - 1:r[3], r[1] - 1:r[4], r[2] - 1:r[5]] = o
     return out
+
+
+def shard(n_items, rank, world):
+    """Indices of ``n_items`` independent chunks / requests owned by ``rank`` of ``world`` replicas
+    (round robin).  The path has no exchange step, so replicas need no data-path collective."""
+    if world < 1 or not 0 <= rank < world:
+        raise ValueError("bad rank/world")
+    return list(range(rank, int(n_items), world))

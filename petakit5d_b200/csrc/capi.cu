@@ -288,11 +288,13 @@ pk_status pk_psf2otf(pk_ctx* ctx, const float* psf, const int64_t psf_dims[3], c
     std::lock_guard<std::recursive_mutex> lk(ctx->mu);
     DeviceGuard g(ctx->device);
     const int ny = (int)dims[0], nx = (int)dims[1], nz = (int)dims[2];
-    const size_t nb = sizeof(float2) * (size_t)(ny / 2 + 1) * nx * nz;
+    const int Py = ny / 2 + 1, Pp = Py + (Py & 1);
+    const size_t nb = sizeof(float2) * (size_t)Pp * nx * nz;
     void* d;
     if ((s = pk_scratch(ctx, 10, nb, &d)) != PK_OK) return s;
     if ((s = pk_make_otf(ctx, psf, psf_dims, ny, nx, nz, 1.0, (float2*)d, ctx->stream)) != PK_OK) return s;
-    PK_CUDA(cudaMemcpyAsync(otf_half, d, nb, cudaMemcpyDeviceToHost, ctx->stream));
+    PK_CUDA(cudaMemcpy2DAsync(otf_half, sizeof(float2) * Py, d, sizeof(float2) * Pp, sizeof(float2) * Py,
+                              (size_t)nx * nz, cudaMemcpyDeviceToHost, ctx->stream));
     PK_CUDA(cudaStreamSynchronize(ctx->stream));
     return PK_OK;
 }
@@ -308,26 +310,27 @@ static pk_status fft3(pk_ctx* ctx, int inverse, const float* d_a, const int64_t 
     if ((s = pk_init_desc(ctx, (int)dims[0], (int)dims[1], (int)dims[2], &d)) != PK_OK) return s;
     cudaStream_t st = pick_stream(ctx, stream);
     PkProgram prog;
+    // the transforms run on a pitched work spectrum; the caller's spectrum is dense [Py nx nz]
+    void* w;
+    if ((s = pk_scratch(ctx, 5, sizeof(float2) * pk_spec_elems(d), &w)) != PK_OK) return s;
+    const size_t rows = (size_t)d.nrows, wb = sizeof(float2) * d.Py, pb = sizeof(float2) * d.Pp;
+    d.S = (float2*)w;
     if (!inverse) {
         d.src = d_a;
-        d.S = (float2*)d_b;
         pk_program_add(prog, PK_STEP_Y, Y_R2C, {d});
         pk_program_add(prog, PK_STEP_X, XZ_FWD, {d});
         pk_program_add(prog, PK_STEP_Z, XZ_FWD, {d});
     } else {
-        // the inverse runs in place on a work copy of the spectrum
-        void* w;
-        const size_t nb = sizeof(float2) * pk_spec_elems(d);
-        if ((s = pk_scratch(ctx, 5, nb, &w)) != PK_OK) return s;
-        PK_CUDA(cudaMemcpyAsync(w, d_a, nb, cudaMemcpyDeviceToDevice, st));
-        d.S = (float2*)w;
+        PK_CUDA(cudaMemcpy2DAsync(w, pb, d_a, wb, wb, rows, cudaMemcpyDeviceToDevice, st));
         d.dst = d_b;
         pk_program_add(prog, PK_STEP_Z, XZ_INV, {d});
         pk_program_add(prog, PK_STEP_X, XZ_INV, {d});
         pk_program_add(prog, PK_STEP_Y, Y_C2R, {d});
     }
     if ((s = pk_program_upload(ctx, prog, st)) != PK_OK) return s;
-    return pk_program_launch(ctx, prog, st);
+    if ((s = pk_program_launch(ctx, prog, st)) != PK_OK) return s;
+    if (!inverse) PK_CUDA(cudaMemcpy2DAsync(d_b, wb, w, pb, wb, rows, cudaMemcpyDeviceToDevice, st));
+    return PK_OK;
 }
 
 pk_status pk_fft3_r2c_device(pk_ctx* ctx, const float* d_in, const int64_t dims[3], float* d_spec, void* stream) {

@@ -253,7 +253,8 @@ pk_status pk_get_otf(pk_ctx* ctx, const float* h_psf, const int64_t pd[3], int n
     auto it = ctx->otf.find(key);
     if (it != ctx->otf.end()) { *d_otf = it->second.d; return PK_OK; }
     OtfEntry e;
-    e.bytes = sizeof(float2) * (size_t)(ny / 2 + 1) * nx * nz;
+    const int Py = ny / 2 + 1;
+    e.bytes = sizeof(float2) * (size_t)(Py + (Py & 1)) * nx * nz;
     cudaError_t ce = cudaMalloc(&e.d, e.bytes);
     if (ce != cudaSuccess) { cudaGetLastError(); return pk_fail(PK_ERR_NOMEM, "OTF allocation failed"); }
     const double N = (double)ny * nx * nz;
@@ -304,9 +305,14 @@ pk_status pk_check_params(const int64_t dims[3], const pk_decon_params* p) {
 // Bytes of the work buffers one job needs (256-byte aligned pieces).
 static size_t al256(size_t b) { return (b + 255) & ~(size_t)255; }
 
+static size_t spec_bytes(const int dims[3]) {
+    const int Py = dims[0] / 2 + 1;
+    return sizeof(float2) * (size_t)(Py + (Py & 1)) * dims[1] * dims[2];
+}
+
 size_t pk_job_bytes(int method, const int dims[3], bool need_mask, int blocksY) {
     const size_t N = (size_t)dims[0] * dims[1] * dims[2];
-    const size_t spec = sizeof(float2) * (size_t)(dims[0] / 2 + 1) * dims[1] * dims[2];
+    const size_t spec = spec_bytes(dims);
     size_t b = al256(4 * N) * 2 + al256(spec);                       // I, J, S
     if (method == 0) b += al256(4 * N) * 3 + al256(sizeof(double) * (2 + 2 * (size_t)blocksY));  // JB, Y, J4, partials
     if (need_mask) b += al256(N);
@@ -315,7 +321,7 @@ size_t pk_job_bytes(int method, const int dims[3], bool need_mask, int blocksY) 
 
 void pk_job_carve(DeconJob& j, int method, bool need_mask, int blocksY, char* arena) {
     const size_t N = (size_t)j.dims[0] * j.dims[1] * j.dims[2];
-    const size_t spec = sizeof(float2) * (size_t)(j.dims[0] / 2 + 1) * j.dims[1] * j.dims[2];
+    const size_t spec = spec_bytes(j.dims);
     size_t o = 0;
     auto take = [&](size_t b) { char* p = arena + o; o += al256(b); return p; };
     j.I = (float*)take(4 * N);

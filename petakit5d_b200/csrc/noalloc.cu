@@ -193,7 +193,10 @@ extern "C" pk_status pk_decon_lucy_omw_noalloc(const void* d_in, pk_dtype in_typ
     char* base = (char*)g_addr[dev];
 
     // ---- layout of the array: work buffers | twiddle tables | descriptors | prefixes | sum
-    const size_t spec_b = sizeof(float2) * (size_t)(ny / 2 + 1) * nx * nz;
+    const int Pyv = ny / 2 + 1;
+    const size_t spec_b = sizeof(float2) * (size_t)(Pyv + (Pyv & 1)) * nx * nz;
+    if (2 * al256(4 * N) + 3 * al256(spec_b) > kWorkBytes)
+        return pk_fail(PK_ERR_UNSUPPORTED, "volume's spectrum does not fit the no-allocation scratch (1048576 voxels)");
     float* I = (float*)base;
     float* J = (float*)(base + al256(4 * N));
     float2* S = (float2*)(base + 2 * al256(4 * N));
@@ -219,6 +222,7 @@ extern "C" pk_status pk_decon_lucy_omw_noalloc(const void* d_in, pk_dtype in_typ
     v.odd = ny & 1;
     v.M = M;
     v.Py = ny / 2 + 1;
+    v.Pp = v.Py + (v.Py & 1);
     v.nrows = (long long)nx * nz;
     if (!axis(M, tw_y, &v.ay) || !axis(nx, tw_x, &v.ax) || !axis(nz, tw_z, &v.az))
         return pk_fail(PK_ERR_UNSUPPORTED, "transform length needs too many radix stages");

@@ -211,12 +211,13 @@ __global__ void __launch_bounds__(PK_THREADS, 3) k_y(const VolDesc* __restrict__
 
     // ---- issue the asynchronous loads: group A = spectrum rows, group B = per-voxel inputs
     if (spec_in) {
-        const float2* S0 = d.S + row0 * (long long)Py;
+        const int Pp = d.Pp;
+        const float2* S0 = d.S + row0 * (long long)Pp;
         const int nin = Lc * Py;
         for (int idx = tid; idx < nin; idx += NT) {
             const int l = idx / Py, k = idx - l * Py;
-            if (!odd && k == M) cp8(&nyq[l], S0 + idx);
-            else cp8(&buf[pad(l * M + k)], S0 + idx);
+            if (!odd && k == M) cp8(&nyq[l], S0 + l * Pp + k);
+            else cp8(&buf[pad(l * M + k)], S0 + l * Pp + k);
         }
     }
     cp_commit();
@@ -378,7 +379,8 @@ __global__ void __launch_bounds__(PK_THREADS, 3) k_y(const VolDesc* __restrict__
         __syncthreads();
         fft_y<P, false>(buf, A, tw, L, tid);
         const int nout = Lc * Py;
-        float2* S0 = d.S + row0 * (long long)Py;
+        const int Pp = d.Pp;
+        float2* S0 = d.S + row0 * (long long)Pp;
         for (int idx = tid; idx < nout; idx += NT) {
             const int l = idx / Py, k = idx - l * Py;
             float2 X;
@@ -392,7 +394,7 @@ __global__ void __launch_bounds__(PK_THREADS, 3) k_y(const VolDesc* __restrict__
             } else {
                 X = buf[pad(l * M + k)];
             }
-            S0[idx] = X;
+            S0[l * Pp + k] = X;
         }
     }
 
@@ -441,8 +443,8 @@ __global__ void __launch_bounds__(PK_THREADS, 3) k_xz(const VolDesc* __restrict_
     const int outer = lb / ctiles;
     const int k0 = (lb - outer * ctiles) * T;
     long long base, es;
-    if (axis == 1) { base = (long long)outer * d.nx * Py; es = Py; }
-    else { base = (long long)outer * Py; es = (long long)d.nx * Py; }
+    if (axis == 1) { base = (long long)outer * d.nx * d.Pp; es = d.Pp; }
+    else { base = (long long)outer * d.Pp; es = (long long)d.nx * d.Pp; }
     // shared memory: tw[n] | buf[padded T*n] | otf[T*n] (XZ_CONV)
     float2* tw = smem;
     float2* buf = smem + n;
@@ -493,9 +495,113 @@ __global__ void __launch_bounds__(PK_THREADS, 3) k_xz(const VolDesc* __restrict_
     }
 }
 
+// Persistent x/z pass for compile-time plans: each CTA walks tiles t = blockIdx.x, + gridDim.x, ...
+// with two tile buffers, so the cp.async loads of its next tile run while it transforms the current
+// one (and, for XZ_CONV, the OTF tile of the current one lands during the forward transform).
+template <int P>
+__global__ void __launch_bounds__(PK_THREADS, 2) k_xzp(const VolDesc* __restrict__ descs, const int* __restrict__ prefix,
+                                                       int nvol, int axis, int mode) {
+    extern __shared__ float2 smem[];
+    constexpr int NT = PK_THREADS;
+    constexpr int n = kPlans[P].n;
+    constexpr int T = plan_cols_xz(n);
+    constexpr int P_ = T * n;
+    const int tid = threadIdx.x;
+    const int total = prefix[nvol];
+    float2* tw = smem;
+    float2* const bufA = smem + n;
+    float2* const bufB = smem + n + padded_size(P_);
+    float2* hbuf = smem + n + 2 * padded_size(P_);
+    const bool conv = mode == XZ_CONV;
+    {
+        const AxisDev& A0 = axis == 1 ? descs[0].ax : descs[0].az;  // every volume of the launch has this n
+        for (int i = tid; i < n; i += NT) tw[i] = A0.tw[i];
+    }
+    struct Tile { const VolDesc* d; long long base, es; int k0, Py; };
+    auto locate = [&](int t) {
+        Tile r;
+        const int vol = find_vol(prefix, nvol, t);
+        r.d = &descs[vol];
+        const int lb = t - prefix[vol];
+        r.Py = r.d->Py;
+        const int ctiles = (r.Py + T - 1) / T;
+        const int outer = lb / ctiles;
+        r.k0 = (lb - outer * ctiles) * T;
+        if (axis == 1) { r.base = (long long)outer * r.d->nx * r.d->Pp; r.es = r.d->Pp; }
+        else { r.base = (long long)outer * r.d->Pp; r.es = (long long)r.d->nx * r.d->Pp; }
+        return r;
+    };
+    auto load = [&](const Tile& r, float2* dst, const float2* src) {
+        for (int idx = tid; idx < P_; idx += NT) {
+            const int e = idx / T, t = idx - e * T;
+            if (r.k0 + t < r.Py) cp8(&dst[pad(idx)], src + r.base + e * r.es + r.k0 + t);
+            else dst[pad(idx)] = make_float2(0.f, 0.f);
+        }
+    };
+    int t = blockIdx.x;
+    int cur = 0;
+    Tile tc;
+    if (t < total) {
+        tc = locate(t);
+        load(tc, bufA, tc.d->S);
+    }
+    cp_commit();
+    for (; t < total; t += gridDim.x) {
+        const int tn = t + gridDim.x;
+        Tile tnx;
+        if (tn < total) {
+            tnx = locate(tn);
+            load(tnx, cur ? bufA : bufB, tnx.d->S);
+        }
+        cp_commit();                                   // group: next tile
+        if (conv) {
+            for (int idx = tid; idx < P_; idx += NT) {
+                const int e = idx / T, tt = idx - e * T;
+                if (tc.k0 + tt < tc.Py) cp8(&hbuf[idx], tc.d->otf + tc.base + e * tc.es + tc.k0 + tt);
+            }
+        }
+        cp_commit();                                   // group: OTF of this tile
+        cp_wait<2>();                                  // this tile's data has landed (own copies)
+        __syncthreads();                               // ... and everybody else's
+        float2* buf = cur ? bufB : bufA;
+        if (mode == XZ_INV) run_plan<P, 0, 1, T, true, true>(buf, tw, tid);
+        else run_plan<P, 0, 1, T, true, false>(buf, tw, tid);
+        if (conv) {
+            cp_wait<1>();
+            __syncthreads();
+            const bool cj = tc.d->conj;
+            for (int idx = tid; idx < P_; idx += NT) {
+                const int tt = idx % T;
+                if (tc.k0 + tt < tc.Py) {
+                    float2 hv = hbuf[idx];
+                    if (cj) hv.y = -hv.y;
+                    buf[pad(idx)] = cmul(buf[pad(idx)], hv);
+                }
+            }
+            __syncthreads();
+            run_plan<P, 0, 1, T, true, true>(buf, tw, tid);
+        }
+        const float sc = mode == XZ_FWD_SCALE ? tc.d->xz_scale : 1.f;
+        float2* S = tc.d->S;
+        for (int idx = tid; idx < P_; idx += NT) {
+            const int e = idx / T, tt = idx - e * T;
+            if (tc.k0 + tt < tc.Py) {
+                float2 v = buf[pad(idx)];
+                if (mode == XZ_FWD_SCALE) v = make_float2(v.x * sc, v.y * sc);
+                S[tc.base + e * tc.es + tc.k0 + tt] = v;
+            }
+        }
+        __syncthreads();                               // buf is refilled two tiles later
+        cur ^= 1;
+        tc = tnx;
+    }
+    cp_wait<0>();
+}
+
 struct KernelTable {
     void (*y[kNumPlans])(const VolDesc*, const int*, int, int);
     void (*xz[kNumPlans])(const VolDesc*, const int*, int, int, int);
+    void (*xzp[kNumPlans])(const VolDesc*, const int*, int, int, int);   // persistent form (plans > 0)
 };
 
 template <int P, int HI>
@@ -503,6 +609,12 @@ struct Register {
     static void fill(KernelTable& t) {
         t.y[P] = k_y<P>;
         t.xz[P] = k_xz<P>;
+        if constexpr (P > 0) {
+            t.xzp[P] = k_xzp<P>;
+            cudaFuncSetAttribute(k_xzp<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        } else {
+            t.xzp[P] = nullptr;
+        }
         cudaFuncSetAttribute(k_y<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
         cudaFuncSetAttribute(k_xz<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
         Register<P + 1, HI>::fill(t);

@@ -31,6 +31,27 @@ void pk_fill_kernels_d(pkpass::KernelTable& t);
 
 namespace {
 
+int sm_count() {
+    static int n = 0;
+    if (!n) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        if (n <= 0) n = 148;
+    }
+    return n;
+}
+
+// PK_XZ_PERSISTENT=0 selects the one-tile-per-CTA form (for comparisons)
+bool persistent_xz() {
+    static int v = -1;
+    if (v < 0) {
+        const char* e = getenv("PK_XZ_PERSISTENT");
+        v = (e && e[0] == '0') ? 0 : 1;
+    }
+    return v == 1;
+}
+
 const pkpass::KernelTable& kernels() {
     static pkpass::KernelTable t;
     static std::once_flag once;
@@ -145,6 +166,7 @@ pk_status pk_init_desc(pk_ctx* ctx, int ny, int nx, int nz, VolDesc* d) {
     d->odd = ny & 1;
     d->M = d->odd ? ny : ny / 2;
     d->Py = ny / 2 + 1;
+    d->Pp = d->Py + (d->Py & 1);
     d->nrows = (long long)nx * nz;
     const int P = PK_TILE_POINTS;  // complex points one CTA holds
     if (d->M > P || nx > P || nz > P)
@@ -170,7 +192,7 @@ pk_status pk_init_desc(pk_ctx* ctx, int ny, int nx, int nz, VolDesc* d) {
     return PK_OK;
 }
 
-size_t pk_spec_elems(const VolDesc& d) { return (size_t)d.Py * (size_t)d.nrows; }
+size_t pk_spec_elems(const VolDesc& d) { return (size_t)d.Pp * (size_t)d.nrows; }
 
 // ------------------------------------------------------------------ programs
 // A program is the full launch sequence of a call (or of a batch / serving round): every step's
@@ -311,6 +333,14 @@ pk_status pk_program_launch(pk_ctx* ctx, PkProgram& prog, cudaStream_t st) {
         }
         if (s.kind == PK_STEP_Y) {
             kt.y[s.plan]<<<s.grid, kThreads, s.smem, st>>>(dd, dp, s.nvol, s.mode);
+        } else if ((s.kind == PK_STEP_X || s.kind == PK_STEP_Z) && s.plan > 0 && persistent_xz()) {
+            // persistent, double-buffered form: two tile buffers (+ the OTF tile), a few CTAs per SM
+            const VolDesc& v0 = prog.descs[s.desc_off];
+            const int n = s.kind == PK_STEP_X ? v0.ax.n : v0.az.n;
+            const int T = plan_cols_xz(n);
+            const size_t sm = sizeof(float2) * (n + 2 * padded_size(T * n) + (s.mode == XZ_CONV ? T * n : 0));
+            const int grid = std::min(s.grid, sm_count() * 2);
+            kt.xzp[s.plan]<<<grid, kThreads, sm, st>>>(dd, dp, s.nvol, s.kind == PK_STEP_X ? 1 : 2, s.mode);
         } else if (s.kind == PK_STEP_X || s.kind == PK_STEP_Z) {
             kt.xz[s.plan]<<<s.grid, kThreads, s.smem, st>>>(dd, dp, s.nvol, s.kind == PK_STEP_X ? 1 : 2, s.mode);
         } else if (s.kind == PK_STEP_LAMBDA) {

@@ -1,7 +1,8 @@
 // Internal types of libpkdecon: per-volume descriptors read by the pass kernels, transform plans,
 // and the context.  Layout conventions:
 //   real volume  : float  v[z][x][y]            (column-major [ny nx nz], y fastest)
-//   half spectrum: float2 S[z][x][k], k < Py     (Py = floor(ny/2)+1; real transform along y)
+//   half spectrum: float2 S[z][x][k], k < Py     (Py = floor(ny/2)+1; real transform along y),
+//                  row pitch Pp = Py rounded up to even
 // A 3D transform is three kinds of pass: a y pass over contiguous rows (real<->half-spectrum,
 // with the per-voxel arithmetic of the iteration folded into its load/store), and two strided
 // complex passes over x and z on tiles of T adjacent k-columns.
@@ -54,7 +55,8 @@ struct VolDesc {
     // geometry
     int ny, nx, nz;
     int M;            // y-pass complex length: ny/2 (even ny) or ny (odd ny)
-    int Py;           // spectrum row pitch, floor(ny/2)+1
+    int Py;           // spectrum bins per row, floor(ny/2)+1
+    int Pp;           // spectrum row pitch (Py rounded up to even: rows start 16-byte aligned)
     int odd;
     long long nrows;  // nx * nz
     int Ly, Tx, Tz;   // lines per CTA (y pass), k-columns per CTA (x / z passes)
