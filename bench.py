@@ -404,6 +404,13 @@ def _emit(line):
     print(json.dumps(line), flush=True)
 
 
+_T0 = time.perf_counter()
+
+
+def _log(msg):
+    print(f"[{time.perf_counter() - _T0:8.1f}s] {msg}", file=sys.stderr, flush=True)
+
+
 def _u16_dev(vol, device):
     import torch
     return torch.from_numpy(np.ascontiguousarray(vol.T).view(np.int16)).to(device)
@@ -491,7 +498,9 @@ def wl_batched(args):
     from petakit5d_b200 import chunking as K
     from petakit5d_b200 import decon as D
     device = torch.device("cuda", 0)
+    _log("batched: generating 96 chunks")
     chunks, pinned, psfs, ids, boxes = _chunk_set(device)
+    _log("batched: generated")
     if args.impl == "reference":
         from oracle import backprojector as OB
         from oracle import decon as O
@@ -543,6 +552,7 @@ def wl_batched(args):
         e1.record(stream)
         torch.cuda.synchronize()
         res[name] = e0.elapsed_time(e1) / reps
+        _log(f"batched: {name} {res[name]:.1f} ms")
     ref_out = [o.copy() for o in outs]
     batched()
     same = all(np.array_equal(a, b) for a, b in zip(ref_out, outs))
@@ -596,10 +606,22 @@ def wl_served(args):
     srv = SV.Server(ctx, budget_bytes=150e9, max_batch=64, borrow_inputs=True)
     for i in range(3):
         srv.add_psf(i, psfs[i], bps[i])
-    # warm-up: every (size, psf) OTF, and the kernels
-    warm = [srv.submit(v, pid, m, 1, Background=100) for v, pid, m, _ in reqs[:8]]
+    _log(f"served: {len(reqs)} requests, {len(pool)} distinct sizes generated")
+    # warm-up: every (size, PSF, method) combination once, so the OTFs are cached as a running
+    # server's would be, and the kernels are loaded
+    seen = {}
+    for v, pid, m, _ in reqs:
+        seen[(v.shape, pid, m)] = v
+    warm = [srv.submit(v, pid, m, 1, Background=100) for (shp, pid, m), v in seen.items()]
     for w in warm:
         srv.wait(w)
+    _log(f"served: warm-up of {len(warm)} combinations done")
+    outs = {}
+    for v, _, _, _ in reqs:
+        if v.shape not in outs:
+            t = torch.empty(v.shape[::-1], dtype=torch.int16).pin_memory()
+            keep.append(t)
+            outs[v.shape] = t.numpy().view(np.uint16).T
     lat = [None] * len(reqs)
     ids = [None] * len(reqs)
     done = threading.Semaphore(0)
@@ -609,7 +631,7 @@ def wl_served(args):
             i = q.get()
             if i is None:
                 return
-            _, ms = srv.wait(ids[i])
+            _, ms = srv.wait(ids[i], out=outs[reqs[i][0].shape])
             lat[i] = ms
             done.release()
 
@@ -628,15 +650,15 @@ def wl_served(args):
     for _ in reqs:
         done.acquire()
     wall = time.perf_counter() - t0
+    _log(f"served: {len(reqs)} requests done in {wall:.2f} s")
     for _ in ws:
         q.put(None)
     st = srv.stats()
     srv.close()
     # the same requests, one plain host call after another
-    out = {}
     t1 = time.perf_counter()
     for v, pid, m, it in reqs:
-        o = out.setdefault(v.shape, np.empty(v.shape, np.uint16, order="F"))
+        o = outs[v.shape]
         p = D_params()
         pf = np.asfortranarray(psfs[pid], np.float32)
         if m == "omw":
@@ -679,8 +701,10 @@ def wl_large(args):
     shape = (2048, 2048, 1024)
     psf = synth.gaussian_psf((31, 31, 41), 1.3, 3.0)
     bp = B.omw_backprojector_generation(psf, 0.005, False, OTFCumThresh=0.6)[0]
+    _log("large: generating 2048x2048x1024")
     d_in = synth.puncta_volume_torch(shape, 2_000_000, psf, 7, 100.0, device=device)
     torch.cuda.empty_cache()
+    _log("large: generated")
     N = int(np.prod(shape))
     ctx = _lib.Context(0)
     stream = torch.cuda.ExternalStream(ctx.stream, device=device)
@@ -695,6 +719,7 @@ def wl_large(args):
     e1.record(stream)
     torch.cuda.synchronize()
     whole_ms = e0.elapsed_time(e1)
+    _log(f"large: whole volume {whole_ms:.1f} ms")
     ctx.reset()
     # chunked: 512^3 regions, border 32, through the batched path on device buffers
     bb, rb, _ = K.zarr_chunk_coordinates(shape, (512, 512, 512), (512, 512, 512), None, False, 32)
@@ -732,6 +757,7 @@ def wl_large(args):
     e1.record(stream)
     torch.cuda.synchronize()
     chunk_ms = e0.elapsed_time(e1)
+    _log(f"large: {n} chunks {chunk_ms:.1f} ms")
     stitched = torch.empty_like(d_in)
     for r, o in zip(rb, outs):
         stitched[r[2] - 1:r[5], r[1] - 1:r[4], r[0] - 1:r[3]] = o

@@ -84,7 +84,7 @@ extern "C" pk_status pk_batch_decon(pk_ctx* ctx, int32_t method, int32_t n, cons
     size_t freeb = 0, totalb = 0;
     PK_CUDA(cudaMemGetInfo(&freeb, &totalb));
     const size_t budget = std::max<size_t>((size_t)(freeb * 0.40), 1ull << 28);
-    const int max_per_wave = device ? n : std::max(2, (n + 3) / 4);   // host mode: >= 4 waves to overlap copies
+    const int max_per_wave = device ? n : std::max(2, (n + 11) / 12);  // host mode: ~12 waves so copies overlap compute
     std::vector<std::vector<int>> waves;
     {
         std::vector<int> cur;

@@ -345,6 +345,16 @@ pk_server* pk_server_create(pk_ctx* ctx, const pk_server_config* cfg) {
     s->cfg.queue_capacity = cfg && cfg->queue_capacity > 0 ? cfg->queue_capacity : 1024;
     s->cfg.borrow_inputs = cfg ? cfg->borrow_inputs : 0;
     cudaSetDevice(ctx->device);
+    {
+        // request buffers come from the device's stream-ordered pool; keep freed blocks in the pool
+        // instead of returning them to the driver at every synchronisation (this process only)
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, ctx->device) == cudaSuccess) {
+            uint64_t thr = ~0ull;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+        }
+        cudaGetLastError();
+    }
     if (cudaStreamCreateWithFlags(&s->up, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&s->down, cudaStreamNonBlocking) != cudaSuccess) {
         pk_set_error("stream creation failed");

@@ -57,9 +57,14 @@ class Server:
         self._meta[rid] = (tuple(od), np.uint16 if p.save16bit else np.float32)
         return rid
 
-    def wait(self, rid, timeout_ms=600000):
+    def wait(self, rid, timeout_ms=600000, out=None):
+        """Wait for request ``rid``; returns (result, latency_ms).  ``out`` (optional) receives the
+        result (pinned memory makes the copy faster)."""
         shape, dt = self._meta[rid]
-        out = np.empty(shape, dt, order="F")
+        if out is None:
+            out = np.empty(shape, dt, order="F")
+        elif out.shape != shape or out.dtype != dt:
+            raise ValueError("out has the wrong shape or dtype")
         lat = C.c_double(0)
         st = lib.pk_server_wait(self.handle, int(rid), ptr(out), int(timeout_ms), C.byref(lat))
         if st != _lib.PK_ERR_TIMEOUT:
