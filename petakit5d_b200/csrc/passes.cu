@@ -42,12 +42,13 @@ int sm_count() {
     return n;
 }
 
-// PK_XZ_PERSISTENT=0 selects the one-tile-per-CTA form (for comparisons)
+// The persistent double-buffered x/z form (k_xzp) measured slower on B200 than one tile per CTA
+// (128 vs 80 registers: 2 instead of 3 CTAs per SM); PK_XZ_PERSISTENT=1 selects it.
 bool persistent_xz() {
     static int v = -1;
     if (v < 0) {
         const char* e = getenv("PK_XZ_PERSISTENT");
-        v = (e && e[0] == '0') ? 0 : 1;
+        v = (e && e[0] == '1') ? 1 : 0;
     }
     return v == 1;
 }

@@ -65,6 +65,7 @@ struct Request {
     cudaEvent_t ev_up = nullptr;     // upload finished
     cudaEvent_t ev_done = nullptr;   // last pass finished
     bool last_queued = false;
+    bool uploading = false;          // input still on its way to the device
     bool collected = false;          // the waiter took the result
 };
 
@@ -222,12 +223,13 @@ pk_status pk_server::admit(const std::shared_ptr<Request>& r) {
     inflight += r->dev_bytes;
     peak_inflight = std::max(peak_inflight, inflight);
     r->d_out = (char*)r->dev + al256(raw_b);
-    // upload on the copy stream (pinned source); the compute stream waits for it before the first pass
+    // upload on the copy stream (pinned source); the request joins rounds once the upload has
+    // completed, so a large upload never holds back the other requests' passes
     PK_CUDA(cudaEventRecord(r->ev_up, c->stream));          // the allocation is ordered on the compute stream
     PK_CUDA(cudaStreamWaitEvent(up, r->ev_up, 0));
     PK_CUDA(cudaMemcpyAsync(r->dev, r->src, raw_b, cudaMemcpyHostToDevice, up));
     PK_CUDA(cudaEventRecord(r->ev_up, up));
-    PK_CUDA(cudaStreamWaitEvent(c->stream, r->ev_up, 0));
+    r->uploading = true;
     build_steps(*r, b, of, ob);
     r->state = RQ_ACTIVE;
     return PK_OK;
@@ -283,14 +285,18 @@ void pk_server::loop() {
             active.push_back(r);
         }
         bool work = false;
-        for (auto& r : active)
-            if (!r->steps.empty()) work = true;
+        for (auto& r : active) {
+            if (r->uploading && cudaEventQuery(r->ev_up) == cudaSuccess) r->uploading = false;
+            if (!r->steps.empty() && !r->uploading) work = true;
+        }
         if (!work) {
             cv_work.wait_for(lk, std::chrono::milliseconds(1));
             continue;
         }
         // one round: slots y, x, z, x; lambda steps ride with their y slot
-        std::vector<std::shared_ptr<Request>> batch(active.begin(), active.end());
+        std::vector<std::shared_ptr<Request>> batch;
+        for (auto& r : active)
+            if (!r->uploading) batch.push_back(r);
         lk.unlock();
         {
             std::lock_guard<std::recursive_mutex> cl(ctx->mu);

@@ -148,11 +148,18 @@ def chunk_workload(n_chunks=96, seed=3, border=16, core_xy=(192, 256, 320, 384),
 
 
 # ---------------------------------------------------------------- GPU generator for large workloads
-def puncta_volume_torch(shape_yxz, n_puncta, psf, seed, background=100.0, device="cuda", sinusoid=None):
+def puncta_volume_torch(shape_yxz, n_puncta, psf, seed, background=100.0, device="cuda", sinusoid=None,
+                        gaussian_psf_sigmas=None):
     """The same recipe as ``puncta_volume`` run with torch on ``device`` (for volumes too large to
     generate quickly on the host).  Returns an int16 tensor shaped (nz, nx, ny) whose bits are the
     uint16 voxels, i.e. the column-major [ny nx nz] volume.  ``sinusoid``: dict of
-    ``sinusoid_background`` arguments added to ``background``."""
+    ``sinusoid_background`` arguments added to ``background``.
+
+    ``gaussian_psf_sigmas=(sigma_xy, sigma_z)``: the PSF is that Gaussian, so each blurred punctum is
+    rendered directly (a sigma-1 Gaussian convolved with the PSF is the Gaussian with the variances
+    added), which avoids a transform of the whole volume."""
+    if gaussian_psf_sigmas is not None:
+        return _blurred_puncta_torch(shape_yxz, n_puncta, gaussian_psf_sigmas, seed, background, device)
     import torch
     ny, nx, nz = (int(v) for v in shape_yxz)
     g = torch.Generator(device=device)
@@ -209,3 +216,42 @@ def puncta_volume_torch(shape_yxz, n_puncta, psf, seed, background=100.0, device
     del noisy
     v = torch.where(v > 32767, v - 65536, v).to(torch.int16)
     return v
+
+
+def _blurred_puncta_torch(shape_yxz, n_puncta, sigmas, seed, background, device):
+    import torch
+    ny, nx, nz = (int(v) for v in shape_yxz)
+    sxy, sz = float(sigmas[0]), float(sigmas[1])
+    vy = vx = 1.0 + sxy * sxy
+    vz = 1.0 + sz * sz
+    gain = (1.0 / np.sqrt(vy)) * (1.0 / np.sqrt(vx)) * (1.0 / np.sqrt(vz))   # per-axis sigma_1 / sqrt(var)
+    ry, rz = int(np.ceil(4 * np.sqrt(vy))), int(np.ceil(4 * np.sqrt(vz)))
+    g = torch.Generator(device=device)
+    g.manual_seed(int(seed))
+    img = torch.zeros(nz * nx * ny, dtype=torch.float32, device=device)
+    oy = torch.arange(-ry, ry + 1, device=device)
+    oz = torch.arange(-rz, rz + 1, device=device)
+    Z, X, Y = torch.meshgrid(oz, oy, oy, indexing="ij")
+    Y, X, Z = Y.reshape(1, -1), X.reshape(1, -1), Z.reshape(1, -1)
+    dims = torch.tensor([ny, nx, nz], device=device, dtype=torch.float32)
+    n = int(n_puncta)
+    step = 1 << 14
+    for s0 in range(0, n, step):
+        m = min(step, n - s0)
+        pos = torch.rand((m, 3), generator=g, device=device) * dims
+        amp = (200.0 + 1800.0 * torch.rand((m, 1), generator=g, device=device)) * gain
+        b = torch.floor(pos).to(torch.int64)
+        iy, ix, iz = b[:, 0:1] + Y, b[:, 1:2] + X, b[:, 2:3] + Z
+        e = (iy - pos[:, 0:1]) ** 2 / (2 * vy) + (ix - pos[:, 1:2]) ** 2 / (2 * vx) + (iz - pos[:, 2:3]) ** 2 / (2 * vz)
+        val = amp * torch.exp(-e)
+        idx = (iy % ny) + ny * ((ix % nx) + nx * (iz % nz))
+        img.index_add_(0, idx.reshape(-1), val.reshape(-1))
+        del pos, amp, b, iy, ix, iz, e, val, idx
+    img += float(background)
+    img.clamp_(min=0)
+    noisy = torch.poisson(img, generator=g)
+    del img
+    noisy.clamp_(0, 65535)
+    v = noisy.to(torch.int32)
+    del noisy
+    return torch.where(v > 32767, v - 65536, v).to(torch.int16).view(nz, nx, ny)
