@@ -218,40 +218,51 @@ def puncta_volume_torch(shape_yxz, n_puncta, psf, seed, background=100.0, device
     return v
 
 
-def _blurred_puncta_torch(shape_yxz, n_puncta, sigmas, seed, background, device):
+def _blurred_puncta_torch(shape_yxz, n_puncta, sigmas, seed, background, device, slab=64):
+    """Blurred Gaussian puncta rendered z-slab by z-slab (every tensor stays below 2^31 elements);
+    puncta wrap around every axis, as the circular blur of the host generator does."""
     import torch
     ny, nx, nz = (int(v) for v in shape_yxz)
     sxy, sz = float(sigmas[0]), float(sigmas[1])
     vy = vx = 1.0 + sxy * sxy
     vz = 1.0 + sz * sz
-    gain = (1.0 / np.sqrt(vy)) * (1.0 / np.sqrt(vx)) * (1.0 / np.sqrt(vz))   # per-axis sigma_1 / sqrt(var)
+    gain = 1.0 / np.sqrt(vy * vx * vz)                      # product of sigma_1 / sqrt(var) per axis
     ry, rz = int(np.ceil(4 * np.sqrt(vy))), int(np.ceil(4 * np.sqrt(vz)))
     g = torch.Generator(device=device)
     g.manual_seed(int(seed))
-    img = torch.zeros(nz * nx * ny, dtype=torch.float32, device=device)
+    n = int(n_puncta)
+    pos = torch.rand((n, 3), generator=g, device=device) * torch.tensor([ny, nx, nz], device=device, dtype=torch.float32)
+    amp = (200.0 + 1800.0 * torch.rand((n,), generator=g, device=device)) * gain
+    order = torch.argsort(pos[:, 2])
+    pos, amp = pos[order], amp[order]
+    zs = pos[:, 2].contiguous()
+    out = torch.empty((nz, nx, ny), dtype=torch.int16, device=device)
     oy = torch.arange(-ry, ry + 1, device=device)
     oz = torch.arange(-rz, rz + 1, device=device)
     Z, X, Y = torch.meshgrid(oz, oy, oy, indexing="ij")
     Y, X, Z = Y.reshape(1, -1), X.reshape(1, -1), Z.reshape(1, -1)
-    dims = torch.tensor([ny, nx, nz], device=device, dtype=torch.float32)
-    n = int(n_puncta)
-    step = 1 << 14
-    for s0 in range(0, n, step):
-        m = min(step, n - s0)
-        pos = torch.rand((m, 3), generator=g, device=device) * dims
-        amp = (200.0 + 1800.0 * torch.rand((m, 1), generator=g, device=device)) * gain
-        b = torch.floor(pos).to(torch.int64)
-        iy, ix, iz = b[:, 0:1] + Y, b[:, 1:2] + X, b[:, 2:3] + Z
-        e = (iy - pos[:, 0:1]) ** 2 / (2 * vy) + (ix - pos[:, 1:2]) ** 2 / (2 * vx) + (iz - pos[:, 2:3]) ** 2 / (2 * vz)
-        val = amp * torch.exp(-e)
-        idx = (iy % ny) + ny * ((ix % nx) + nx * (iz % nz))
-        img.index_add_(0, idx.reshape(-1), val.reshape(-1))
-        del pos, amp, b, iy, ix, iz, e, val, idx
-    img += float(background)
-    img.clamp_(min=0)
-    noisy = torch.poisson(img, generator=g)
-    del img
-    noisy.clamp_(0, 65535)
-    v = noisy.to(torch.int32)
-    del noisy
-    return torch.where(v > 32767, v - 65536, v).to(torch.int16).view(nz, nx, ny)
+    for z0 in range(0, nz, slab):
+        z1 = min(nz, z0 + slab)
+        img = torch.full(((z1 - z0) * nx * ny,), float(background), dtype=torch.float32, device=device)
+        for shift in (0.0, float(nz), -float(nz)):          # wrap-around copies near the z ends
+            lo = torch.searchsorted(zs, torch.tensor([z0 - rz - 1 - shift], device=device))
+            hi = torch.searchsorted(zs, torch.tensor([z1 + rz + 1 - shift], device=device))
+            i0, i1 = int(lo.item()), int(hi.item())
+            for c0 in range(i0, i1, 1 << 13):
+                c1 = min(i1, c0 + (1 << 13))
+                p = pos[c0:c1]
+                pz = p[:, 2:3] + shift
+                b = torch.floor(torch.cat([p[:, 0:2], pz], dim=1)).to(torch.int64)
+                iy, ix, iz = b[:, 0:1] + Y, b[:, 1:2] + X, b[:, 2:3] + Z
+                e = (iy - p[:, 0:1]) ** 2 / (2 * vy) + (ix - p[:, 1:2]) ** 2 / (2 * vx) + (iz - pz) ** 2 / (2 * vz)
+                val = amp[c0:c1, None] * torch.exp(-e)
+                keep = (iz >= z0) & (iz < z1)
+                idx = (iy % ny) + ny * ((ix % nx) + nx * (iz - z0))
+                img.index_add_(0, idx[keep], val[keep])
+                del p, pz, b, iy, ix, iz, e, val, keep, idx
+        img.clamp_(min=0)
+        noisy = torch.poisson(img, generator=g).clamp_(0, 65535).to(torch.int32)
+        del img
+        out[z0:z1] = torch.where(noisy > 32767, noisy - 65536, noisy).to(torch.int16).view(z1 - z0, nx, ny)
+        del noisy
+    return out
