@@ -7,7 +7,7 @@
 namespace pkfft {
 
 // Direct DFT butterfly for a compile-time radix (7, 9, 11, 13, 17): y_q = sum_m v_m W_R^{qm}, with
-// W_R^e = tw[e * wstep] read from the length-N root table.
+// W_R^e = tw[e * wstep].
 template <int R, bool INV>
 __device__ __forceinline__ void bf_direct(float2* v, const float2* __restrict__ tw, int wstep) {
     float2 w[R];
@@ -32,7 +32,9 @@ __device__ __forceinline__ void bf_direct(float2* v, const float2* __restrict__ 
     for (int q = 0; q < R; q++) v[q] = out[q];
 }
 
-template <int R, int NS, int N, int L, bool LF, bool INV>
+// One Stockham stage, shared -> shared.  tw is the plan's stage-ordered table; OFF is this stage's
+// section in it.
+template <int R, int NS, int N, int L, bool LF, bool INV, int OFF>
 __device__ __forceinline__ void stage_ct(float2* __restrict__ buf, const float2* __restrict__ tw, int tid) {
     constexpr int M = N / R;
     constexpr int B = L * M;
@@ -61,17 +63,15 @@ __device__ __forceinline__ void stage_ct(float2* __restrict__ buf, const float2*
             const int j = LF ? b / L : b % M;
             const int k = j % NS;
             if constexpr (NS > 1) {
-                constexpr int TSTEP = N / (NS * R);
-                const int t = k * TSTEP;
 #pragma unroll
                 for (int r = 1; r < R; r++) {
-                    float2 w = tw[r * t];
+                    float2 w = tw[OFF + (r - 1) * NS + k];
                     if (INV) w.y = -w.y;
                     v[i][r] = cmul(v[i][r], w);
                 }
             }
-            if constexpr (R == 2 || R == 3 || R == 4 || R == 5 || R == 8 || R == 16) bfly<R, INV>(v[i]);
-            else bf_direct<R, INV>(v[i], tw, N / R);
+            if constexpr (!direct_radix(R)) bfly<R, INV>(v[i]);
+            else bf_direct<R, INV>(v[i], tw + OFF + (NS > 1 ? (R - 1) * NS : 0), 1);
             const int a0 = l * LS + ((j - k) * R + k) * ES;
 #pragma unroll
             for (int r = 0; r < R; r++) buf[pad(a0 + r * NS * ES)] = v[i][r];
@@ -84,9 +84,139 @@ template <int P, int S, int NS, int L, bool LF, bool INV>
 __device__ __forceinline__ void run_plan(float2* buf, const float2* tw, int tid) {
     if constexpr (S < kPlans[P].nst) {
         constexpr int R = kPlans[P].rad[S];
-        stage_ct<R, NS, kPlans[P].n, L, LF, INV>(buf, tw, tid);
+        stage_ct<R, NS, kPlans[P].n, L, LF, INV, stage_tw_off(P, S)>(buf, tw, tid);
         run_plan<P, S + 1, NS * R, L, LF, INV>(buf, tw, tid);
     }
+}
+
+// ---- stages whose inputs come from / outputs go to HBM directly (registers <-> global), so a
+// transform makes two fewer passes over shared memory.  G is an accessor with
+//   bool ok(l, e); float2 ld(l, e); void st(l, e, v); float2 otf(l, e)
+// for element e of line l of the tile.
+
+// first stage (Ns = 1, no twiddles): global -> registers -> butterfly -> shared.  g.after_loads()
+// runs once the loads are issued (the caller stages tables and side inputs there).
+template <int R, int N, int L, bool LF, bool INV, class G>
+__device__ __forceinline__ void stage_g2s(float2* __restrict__ buf, const G& g, int tid) {
+    static_assert(R == 2 || R == 3 || R == 4 || R == 5 || R == 8 || R == 16, "first stage needs a register butterfly");
+    constexpr int M = N / R;
+    constexpr int B = L * M;
+    constexpr int NT = PK_THREADS;
+    constexpr int MAXB = (B + NT - 1) / NT;
+    constexpr int LS = LF ? 1 : N;
+    constexpr int ES = LF ? L : 1;
+    float2 v[MAXB][R];
+#pragma unroll
+    for (int i = 0; i < MAXB; i++) {
+        const int b = tid + i * NT;
+        if (B % NT == 0 || b < B) {
+            const int l = LF ? b % L : b / M;
+            const int j = LF ? b / L : b % M;
+#pragma unroll
+            for (int r = 0; r < R; r++) v[i][r] = g.ld(l, j + r * M);
+        }
+    }
+    g.after_loads();
+#pragma unroll
+    for (int i = 0; i < MAXB; i++) {
+        const int b = tid + i * NT;
+        if (B % NT == 0 || b < B) {
+            const int l = LF ? b % L : b / M;
+            const int j = LF ? b / L : b % M;
+            bfly<R, INV>(v[i]);
+            const int a0 = l * LS + j * R * ES;
+#pragma unroll
+            for (int r = 0; r < R; r++) buf[pad(a0 + r * ES)] = v[i][r];
+        }
+    }
+    __syncthreads();
+}
+
+// last stage: shared -> registers -> twiddle, butterfly [x OTF] -> global (TO_GLOBAL) or shared
+template <int R, int NS, int N, int L, bool LF, bool INV, int OFF, bool MUL, bool TO_GLOBAL, class G>
+__device__ __forceinline__ void stage_s2x(float2* __restrict__ buf, const float2* __restrict__ tw, const G& g, int tid) {
+    constexpr int M = N / R;
+    constexpr int B = L * M;
+    constexpr int NT = PK_THREADS;
+    constexpr int MAXB = (B + NT - 1) / NT;
+    constexpr int LS = LF ? 1 : N;
+    constexpr int ES = LF ? L : 1;
+    float2 v[MAXB][R];
+#pragma unroll
+    for (int i = 0; i < MAXB; i++) {
+        const int b = tid + i * NT;
+        if (B % NT == 0 || b < B) {
+            const int l = LF ? b % L : b / M;
+            const int j = LF ? b / L : b % M;
+            const int a0 = l * LS + j * ES;
+#pragma unroll
+            for (int r = 0; r < R; r++) v[i][r] = buf[pad(a0 + r * M * ES)];
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < MAXB; i++) {
+        const int b = tid + i * NT;
+        if (B % NT == 0 || b < B) {
+            const int l = LF ? b % L : b / M;
+            const int j = LF ? b / L : b % M;
+            const int k = j % NS;
+            if constexpr (NS > 1) {
+#pragma unroll
+                for (int r = 1; r < R; r++) {
+                    float2 w = tw[OFF + (r - 1) * NS + k];
+                    if (INV) w.y = -w.y;
+                    v[i][r] = cmul(v[i][r], w);
+                }
+            }
+            if constexpr (!direct_radix(R)) bfly<R, INV>(v[i]);
+            else bf_direct<R, INV>(v[i], tw + OFF + (NS > 1 ? (R - 1) * NS : 0), 1);
+#pragma unroll
+            for (int r = 0; r < R; r++) {
+                const int e = (j - k) * R + k + r * NS;
+                float2 o = v[i][r];
+                if constexpr (MUL) o = cmul(o, g.otf(l, e));
+                if constexpr (TO_GLOBAL) g.st(l, e, o);
+                else buf[pad(l * LS + e * ES)] = o;
+            }
+        }
+    }
+    if constexpr (!TO_GLOBAL) __syncthreads();
+}
+
+// middle stages S in [S0, S1) of plan P (shared -> shared)
+template <int P, int S, int S1, int NS, int L, bool LF, bool INV>
+__device__ __forceinline__ void run_mid(float2* buf, const float2* tw, int tid) {
+    if constexpr (S < S1) {
+        constexpr int R = kPlans[P].rad[S];
+        stage_ct<R, NS, kPlans[P].n, L, LF, INV, stage_tw_off(P, S)>(buf, tw, tid);
+        run_mid<P, S + 1, S1, NS * R, L, LF, INV>(buf, tw, tid);
+    }
+}
+
+// Whole transform of plan P (>= 2 stages) with HBM input and HBM or shared output.
+//   TO_GLOBAL: the last stage stores through g.st; else it leaves the result in shared memory
+//   MUL: the last stage multiplies by g.otf before storing (g.before_last() makes that table ready)
+template <int P, int L, bool LF, bool INV, bool MUL, bool TO_GLOBAL, class G>
+__device__ __forceinline__ void fft_g(float2* buf, const float2* tw, const G& g, int tid) {
+    constexpr int nst = kPlans[P].nst;
+    constexpr int N = kPlans[P].n;
+    static_assert(nst >= 2, "fft_g needs at least two stages");
+    stage_g2s<kPlans[P].rad[0], N, L, LF, INV>(buf, g, tid);
+    run_mid<P, 1, nst - 1, kPlans[P].rad[0], L, LF, INV>(buf, tw, tid);
+    if constexpr (MUL) g.before_last();
+    stage_s2x<kPlans[P].rad[nst - 1], plan_ns_before(P, nst - 1), N, L, LF, INV, stage_tw_off(P, nst - 1), MUL,
+              TO_GLOBAL>(buf, tw, g, tid);
+}
+
+// Transform of plan P starting from shared memory with the last stage going to HBM.
+template <int P, int L, bool LF, bool INV, class G>
+__device__ __forceinline__ void fft_s2g(float2* buf, const float2* tw, const G& g, int tid) {
+    constexpr int nst = kPlans[P].nst;
+    constexpr int N = kPlans[P].n;
+    run_mid<P, 0, nst - 1, 1, L, LF, INV>(buf, tw, tid);
+    stage_s2x<kPlans[P].rad[nst - 1], plan_ns_before(P, nst - 1), N, L, LF, INV, stage_tw_off(P, nst - 1), false,
+              true>(buf, tw, g, tid);
 }
 
 }  // namespace pkfft

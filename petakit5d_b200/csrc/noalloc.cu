@@ -96,20 +96,6 @@ __global__ void k_na_psf_scatter(const float* __restrict__ psf, int py, int px, 
 
 size_t al256(size_t b) { return (b + 255) & ~(size_t)255; }
 
-// roots exp(-2 pi i k / n), exact at the multiples of pi/2 (the same table the context builds)
-void fill_roots(float2* t, int n) {
-    for (int k = 0; k < n; k++) {
-        const double a = -2.0 * M_PI * (double)k / (double)n;
-        double c = std::cos(a), s = std::sin(a);
-        if ((4LL * k) % n == 0) {
-            const int q = (int)((4LL * k) / n) & 3;
-            c = q == 0 ? 1 : q == 2 ? -1 : 0;
-            s = q == 1 ? -1 : q == 3 ? 1 : 0;
-        }
-        t[k] = make_float2((float)c, (float)s);
-    }
-}
-
 bool axis(int n, const float2* dtw, AxisDev* a) {
     AxisPlan p;
     if (!pk_make_axis_plan(n, &p)) return false;
@@ -126,11 +112,11 @@ bool axis(int n, const float2* dtw, AxisDev* a) {
 
 size_t smem_for(int kind, int mode, const VolDesc& v) {
     if (kind == PK_STEP_Y)
-        return sizeof(float2) * (v.M + (v.odd ? 0 : v.M + 1) + pkfft::padded_size(v.Ly * v.M) + v.Ly +
+        return sizeof(float2) * (tw_slots(v.M) + (v.odd ? 0 : v.M + 1) + pkfft::padded_size(v.Ly * v.M) + v.Ly +
                                  (size_t)pkpass::y_aux_arrays(mode) * v.Ly * v.M);
     const AxisDev& A = kind == PK_STEP_X ? v.ax : v.az;
     const int T = kind == PK_STEP_X ? v.Tx : v.Tz;
-    return sizeof(float2) * (A.n + pkfft::padded_size(T * A.n) + (mode == XZ_CONV ? T * A.n : 0));
+    return sizeof(float2) * (tw_slots(A.n) + pkfft::padded_size(T * A.n) + (mode == XZ_CONV ? T * A.n : 0));
 }
 
 pkpass::KernelTable g_kt;
@@ -212,10 +198,10 @@ extern "C" pk_status pk_decon_lucy_omw_noalloc(const void* d_in, pk_dtype in_typ
     const float2* tw_z = tw_x + 4096;
 
     // ---- descriptors (the same geometry rules as the context path)
-    fill_roots(g_stage.tw, M);
-    if (!(ny & 1)) fill_roots(g_stage.tw + 4096, ny);
-    fill_roots(g_stage.tw + 4096 + 8192, nx);
-    fill_roots(g_stage.tw + 4096 + 8192 + 4096, nz);
+    pk_axis_table(M, g_stage.tw);
+    if (!(ny & 1)) pk_root_table(ny, g_stage.tw + 4096);
+    pk_axis_table(nx, g_stage.tw + 4096 + 8192);
+    pk_axis_table(nz, g_stage.tw + 4096 + 8192 + 4096);
     VolDesc v;
     memset(&v, 0, sizeof(v));
     v.ny = ny; v.nx = nx; v.nz = nz;

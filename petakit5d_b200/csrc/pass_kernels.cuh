@@ -198,9 +198,9 @@ __global__ void __launch_bounds__(PK_THREADS, 3) k_y(const VolDesc* __restrict__
     const int L = P == 0 ? d.Ly : plan_lines_y(kPlans[P].n);
     const bool odd = d.odd;
     const int Py = d.Py, ny = d.ny;
-    // shared memory: tw[M] | twrc[M+1] (even ny) | buf[padded L*M] | nyq[L] | aux0[L*M] | aux1[L*M]
+    // shared memory: tw[tw_slots(M)] | twrc[M+1] (even ny) | buf[padded L*M] | nyq[L] | aux0[L*M] | aux1[L*M]
     float2* tw = smem;
-    float2* twrc = smem + M;
+    float2* twrc = smem + tw_slots(M);
     float2* buf = twrc + (odd ? 0 : M + 1);
     float2* nyq = buf + padded_size(L * M);
     float2* aux0 = nyq + L;
@@ -213,11 +213,20 @@ __global__ void __launch_bounds__(PK_THREADS, 3) k_y(const VolDesc* __restrict__
     if (spec_in) {
         const int Pp = d.Pp;
         const float2* S0 = d.S + row0 * (long long)Pp;
-        const int nin = Lc * Py;
-        for (int idx = tid; idx < nin; idx += NT) {
-            const int l = idx / Py, k = idx - l * Py;
-            if (!odd && k == M) cp8(&nyq[l], S0 + l * Pp + k);
-            else cp8(&buf[pad(l * M + k)], S0 + l * Pp + k);
+        if (P > 0 && !odd) {
+            // Py = M + 1: bins 0..M-1 of each row into the tile, bin M (Nyquist) aside
+            for (int idx = tid; idx < Lc * M; idx += NT) {
+                const int l = idx / M, k = idx - l * M;
+                cp8(&buf[pad(idx)], S0 + l * Pp + k);
+            }
+            for (int l = tid; l < Lc; l += NT) cp8(&nyq[l], S0 + l * Pp + M);
+        } else {
+            const int nin = Lc * Py;
+            for (int idx = tid; idx < nin; idx += NT) {
+                const int l = idx / Py, k = idx - l * Py;
+                if (!odd && k == M) cp8(&nyq[l], S0 + l * Pp + k);
+                else cp8(&buf[pad(l * M + k)], S0 + l * Pp + k);
+            }
         }
     }
     cp_commit();
@@ -258,7 +267,7 @@ __global__ void __launch_bounds__(PK_THREADS, 3) k_y(const VolDesc* __restrict__
     }
     cp_commit();
     // tables (plain loads; they stay in L2)
-    for (int i = tid; i < M; i += NT) tw[i] = A.tw[i];
+    for (int i = tid; i < (P == 0 ? M : plan_tw_size(P)); i += NT) tw[i] = A.tw[i];
     if (!odd)
         for (int i = tid; i <= M; i += NT) twrc[i] = d.tw_rc[i];
     double acc0 = 0.0, acc1 = 0.0;
@@ -381,20 +390,41 @@ __global__ void __launch_bounds__(PK_THREADS, 3) k_y(const VolDesc* __restrict__
         const int nout = Lc * Py;
         const int Pp = d.Pp;
         float2* S0 = d.S + row0 * (long long)Pp;
-        for (int idx = tid; idx < nout; idx += NT) {
-            const int l = idx / Py, k = idx - l * Py;
-            float2 X;
-            if (!odd) {
-                const float2 zk = buf[pad(l * M + (k == M ? 0 : k))];
+        if (P > 0 && !odd) {
+            // X[k] = (Z[k] + Z*[M-k]) / 2 + W^k (Z[k] - Z*[M-k]) / 2i for k < M; X[M] from Z[0]
+            for (int idx = tid; idx < Lc * M; idx += NT) {
+                const int l = idx / M, k = idx - l * M;
+                const float2 zk = buf[pad(idx)];
                 const float2 zc = conjf2(buf[pad(l * M + (k == 0 ? 0 : M - k))]);
                 const float2 fe = make_float2(0.5f * (zk.x + zc.x), 0.5f * (zk.y + zc.y));
                 const float2 df = csub(zk, zc);
-                const float2 fo = make_float2(0.5f * df.y, -0.5f * df.x);  // (zk - zc) / (2i)
-                X = cadd(fe, cmul(twrc[k], fo));
-            } else {
-                X = buf[pad(l * M + k)];
+                const float2 fo = make_float2(0.5f * df.y, -0.5f * df.x);
+                S0[l * Pp + k] = cadd(fe, cmul(twrc[k], fo));
             }
-            S0[l * Pp + k] = X;
+            for (int l = tid; l < Lc; l += NT) {
+                const float2 zk = buf[pad(l * M)];
+                const float2 zc = conjf2(zk);
+                const float2 fe = make_float2(0.5f * (zk.x + zc.x), 0.5f * (zk.y + zc.y));
+                const float2 df = csub(zk, zc);
+                const float2 fo = make_float2(0.5f * df.y, -0.5f * df.x);
+                S0[l * Pp + M] = cadd(fe, cmul(twrc[M], fo));
+            }
+        } else {
+            for (int idx = tid; idx < nout; idx += NT) {
+                const int l = idx / Py, k = idx - l * Py;
+                float2 X;
+                if (!odd) {
+                    const float2 zk = buf[pad(l * M + (k == M ? 0 : k))];
+                    const float2 zc = conjf2(buf[pad(l * M + (k == 0 ? 0 : M - k))]);
+                    const float2 fe = make_float2(0.5f * (zk.x + zc.x), 0.5f * (zk.y + zc.y));
+                    const float2 df = csub(zk, zc);
+                    const float2 fo = make_float2(0.5f * df.y, -0.5f * df.x);  // (zk - zc) / (2i)
+                    X = cadd(fe, cmul(twrc[k], fo));
+                } else {
+                    X = buf[pad(l * M + k)];
+                }
+                S0[l * Pp + k] = X;
+            }
         }
     }
 
@@ -426,6 +456,58 @@ __global__ void __launch_bounds__(PK_THREADS, 3) k_y(const VolDesc* __restrict__
     }
 }
 
+// Tile of an x/z pass as seen by the register-IO stages: element e of column t is p[e*es + t];
+// columns at or beyond ncol read as zero and are not stored.  The tables (twiddles, OTF tile)
+// are staged into shared memory right after the first loads are issued.
+struct XZTile {
+    float2* p;             // S + tile origin
+    long long es;          // element stride along the transformed axis
+    int ncol;              // valid columns of the tile
+    float sc;              // output scale (XZ_FWD_SCALE), else 1
+    const float2* gtw;     // twiddle table (global)
+    const float2* gh;      // OTF at the tile origin (XZ_CONV), else null
+    float2* tw;            // shared twiddles
+    float2* h;             // shared OTF tile
+    int T, n, ntw, conj;
+    __device__ __forceinline__ float2 ld(int l, int e) const {
+        return l < ncol ? p[e * es + l] : make_float2(0.f, 0.f);
+    }
+    __device__ __forceinline__ void st(int l, int e, float2 v) const {
+        if (l < ncol) p[e * es + l] = make_float2(v.x * sc, v.y * sc);
+    }
+    __device__ __forceinline__ float2 otf(int l, int e) const {
+        float2 v = h[e * T + l];
+        if (conj) v.y = -v.y;
+        return v;
+    }
+    __device__ __forceinline__ void after_loads() const {
+        const int tid = threadIdx.x;
+        if (gh) {
+#pragma unroll 1
+            for (int idx = tid; idx < T * n; idx += PK_THREADS) {
+                const int e = idx / T, t = idx - e * T;
+                if (t < ncol) cp8(&h[idx], gh + e * es + t);
+            }
+            cp_commit();
+        }
+#pragma unroll 1
+        for (int i = tid; i < ntw; i += PK_THREADS) tw[i] = gtw[i];
+    }
+    __device__ __forceinline__ void before_last() const {
+        cp_wait<0>();
+        __syncthreads();
+    }
+    // Copy whose address fields the compiler cannot see through, so address arithmetic of a later
+    // transform is not hoisted into (and kept live across) an earlier one.
+    __device__ __forceinline__ XZTile fenced() const {
+        XZTile r = *this;
+        asm volatile("mov.b64 %0, %0;" : "+l"(r.p));
+        asm volatile("mov.b64 %0, %0;" : "+l"(r.es));
+        asm volatile("mov.b32 %0, %0;" : "+r"(r.ncol));
+        return r;
+    }
+};
+
 template <int P>
 __global__ void __launch_bounds__(PK_THREADS, 3) k_xz(const VolDesc* __restrict__ descs, const int* __restrict__ prefix,
                                                       int nvol, int axis, int mode) {
@@ -445,12 +527,28 @@ __global__ void __launch_bounds__(PK_THREADS, 3) k_xz(const VolDesc* __restrict_
     long long base, es;
     if (axis == 1) { base = (long long)outer * d.nx * d.Pp; es = d.Pp; }
     else { base = (long long)outer * d.Pp; es = (long long)d.nx * d.Pp; }
-    // shared memory: tw[n] | buf[padded T*n] | otf[T*n] (XZ_CONV)
+    // shared memory: tw[tw_slots(n)] | buf[padded T*n] | otf[T*n] (XZ_CONV)
     float2* tw = smem;
-    float2* buf = smem + n;
+    float2* buf = smem + tw_slots(n);
     float2* hbuf = buf + padded_size(T * n);
     const int P_ = T * n;
     const bool conv = mode == XZ_CONV;
+    if constexpr (P > 0 && kPlans[P].nst >= 2) {
+        // first stage loads from HBM into registers, last stage stores from registers to HBM; the
+        // OTF multiply runs inside the last forward stage
+        constexpr int TT = plan_cols_xz(kPlans[P].n);
+        const XZTile g{d.S + base + k0, es, Py - k0, mode == XZ_FWD_SCALE ? d.xz_scale : 1.f, A.tw,
+                       conv ? d.otf + base + k0 : nullptr, tw, hbuf, TT, kPlans[P].n, plan_tw_size(P), d.conj};
+        if (mode == XZ_INV) fft_g<P, TT, true, true, false, true>(buf, tw, g, tid);
+        else if (!conv) fft_g<P, TT, true, false, false, true>(buf, tw, g, tid);
+        else {
+            fft_g<P, TT, true, false, true, false>(buf, tw, g, tid);
+            int tid2 = tid;  // opaque copy: keeps the forward's index arithmetic from being reused here
+            asm volatile("mov.b32 %0, %0;" : "+r"(tid2));
+            fft_s2g<P, TT, true, true>(buf, tw, g.fenced(), tid2);
+        }
+        return;
+    }
     for (int idx = tid; idx < P_; idx += NT) {
         const int e = idx / T, t = idx - e * T;
         if (k0 + t < Py) cp8(&buf[pad(idx)], d.S + base + e * es + k0 + t);
@@ -464,7 +562,7 @@ __global__ void __launch_bounds__(PK_THREADS, 3) k_xz(const VolDesc* __restrict_
         }
     }
     cp_commit();
-    for (int i = tid; i < n; i += NT) tw[i] = A.tw[i];
+    for (int i = tid; i < (P == 0 ? n : plan_tw_size(P)); i += NT) tw[i] = A.tw[i];
     cp_wait<1>();
     __syncthreads();
     if (mode == XZ_INV) fft_xz<P, true>(buf, A, tw, T, tid);
@@ -495,113 +593,9 @@ __global__ void __launch_bounds__(PK_THREADS, 3) k_xz(const VolDesc* __restrict_
     }
 }
 
-// Persistent x/z pass for compile-time plans: each CTA walks tiles t = blockIdx.x, + gridDim.x, ...
-// with two tile buffers, so the cp.async loads of its next tile run while it transforms the current
-// one (and, for XZ_CONV, the OTF tile of the current one lands during the forward transform).
-template <int P>
-__global__ void __launch_bounds__(PK_THREADS, 2) k_xzp(const VolDesc* __restrict__ descs, const int* __restrict__ prefix,
-                                                       int nvol, int axis, int mode) {
-    extern __shared__ float2 smem[];
-    constexpr int NT = PK_THREADS;
-    constexpr int n = kPlans[P].n;
-    constexpr int T = plan_cols_xz(n);
-    constexpr int P_ = T * n;
-    const int tid = threadIdx.x;
-    const int total = prefix[nvol];
-    float2* tw = smem;
-    float2* const bufA = smem + n;
-    float2* const bufB = smem + n + padded_size(P_);
-    float2* hbuf = smem + n + 2 * padded_size(P_);
-    const bool conv = mode == XZ_CONV;
-    {
-        const AxisDev& A0 = axis == 1 ? descs[0].ax : descs[0].az;  // every volume of the launch has this n
-        for (int i = tid; i < n; i += NT) tw[i] = A0.tw[i];
-    }
-    struct Tile { const VolDesc* d; long long base, es; int k0, Py; };
-    auto locate = [&](int t) {
-        Tile r;
-        const int vol = find_vol(prefix, nvol, t);
-        r.d = &descs[vol];
-        const int lb = t - prefix[vol];
-        r.Py = r.d->Py;
-        const int ctiles = (r.Py + T - 1) / T;
-        const int outer = lb / ctiles;
-        r.k0 = (lb - outer * ctiles) * T;
-        if (axis == 1) { r.base = (long long)outer * r.d->nx * r.d->Pp; r.es = r.d->Pp; }
-        else { r.base = (long long)outer * r.d->Pp; r.es = (long long)r.d->nx * r.d->Pp; }
-        return r;
-    };
-    auto load = [&](const Tile& r, float2* dst, const float2* src) {
-        for (int idx = tid; idx < P_; idx += NT) {
-            const int e = idx / T, t = idx - e * T;
-            if (r.k0 + t < r.Py) cp8(&dst[pad(idx)], src + r.base + e * r.es + r.k0 + t);
-            else dst[pad(idx)] = make_float2(0.f, 0.f);
-        }
-    };
-    int t = blockIdx.x;
-    int cur = 0;
-    Tile tc;
-    if (t < total) {
-        tc = locate(t);
-        load(tc, bufA, tc.d->S);
-    }
-    cp_commit();
-    for (; t < total; t += gridDim.x) {
-        const int tn = t + gridDim.x;
-        Tile tnx;
-        if (tn < total) {
-            tnx = locate(tn);
-            load(tnx, cur ? bufA : bufB, tnx.d->S);
-        }
-        cp_commit();                                   // group: next tile
-        if (conv) {
-            for (int idx = tid; idx < P_; idx += NT) {
-                const int e = idx / T, tt = idx - e * T;
-                if (tc.k0 + tt < tc.Py) cp8(&hbuf[idx], tc.d->otf + tc.base + e * tc.es + tc.k0 + tt);
-            }
-        }
-        cp_commit();                                   // group: OTF of this tile
-        cp_wait<2>();                                  // this tile's data has landed (own copies)
-        __syncthreads();                               // ... and everybody else's
-        float2* buf = cur ? bufB : bufA;
-        if (mode == XZ_INV) run_plan<P, 0, 1, T, true, true>(buf, tw, tid);
-        else run_plan<P, 0, 1, T, true, false>(buf, tw, tid);
-        if (conv) {
-            cp_wait<1>();
-            __syncthreads();
-            const bool cj = tc.d->conj;
-            for (int idx = tid; idx < P_; idx += NT) {
-                const int tt = idx % T;
-                if (tc.k0 + tt < tc.Py) {
-                    float2 hv = hbuf[idx];
-                    if (cj) hv.y = -hv.y;
-                    buf[pad(idx)] = cmul(buf[pad(idx)], hv);
-                }
-            }
-            __syncthreads();
-            run_plan<P, 0, 1, T, true, true>(buf, tw, tid);
-        }
-        const float sc = mode == XZ_FWD_SCALE ? tc.d->xz_scale : 1.f;
-        float2* S = tc.d->S;
-        for (int idx = tid; idx < P_; idx += NT) {
-            const int e = idx / T, tt = idx - e * T;
-            if (tc.k0 + tt < tc.Py) {
-                float2 v = buf[pad(idx)];
-                if (mode == XZ_FWD_SCALE) v = make_float2(v.x * sc, v.y * sc);
-                S[tc.base + e * tc.es + tc.k0 + tt] = v;
-            }
-        }
-        __syncthreads();                               // buf is refilled two tiles later
-        cur ^= 1;
-        tc = tnx;
-    }
-    cp_wait<0>();
-}
-
 struct KernelTable {
     void (*y[kNumPlans])(const VolDesc*, const int*, int, int);
     void (*xz[kNumPlans])(const VolDesc*, const int*, int, int, int);
-    void (*xzp[kNumPlans])(const VolDesc*, const int*, int, int, int);   // persistent form (plans > 0)
 };
 
 template <int P, int HI>
@@ -609,12 +603,6 @@ struct Register {
     static void fill(KernelTable& t) {
         t.y[P] = k_y<P>;
         t.xz[P] = k_xz<P>;
-        if constexpr (P > 0) {
-            t.xzp[P] = k_xzp<P>;
-            cudaFuncSetAttribute(k_xzp<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-        } else {
-            t.xzp[P] = nullptr;
-        }
         cudaFuncSetAttribute(k_y<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
         cudaFuncSetAttribute(k_xz<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
         Register<P + 1, HI>::fill(t);

@@ -31,28 +31,6 @@ void pk_fill_kernels_d(pkpass::KernelTable& t);
 
 namespace {
 
-int sm_count() {
-    static int n = 0;
-    if (!n) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-        if (n <= 0) n = 148;
-    }
-    return n;
-}
-
-// The persistent double-buffered x/z form (k_xzp) measured slower on B200 than one tile per CTA
-// (128 vs 80 registers: 2 instead of 3 CTAs per SM); PK_XZ_PERSISTENT=1 selects it.
-bool persistent_xz() {
-    static int v = -1;
-    if (v < 0) {
-        const char* e = getenv("PK_XZ_PERSISTENT");
-        v = (e && e[0] == '1') ? 1 : 0;
-    }
-    return v == 1;
-}
-
 const pkpass::KernelTable& kernels() {
     static pkpass::KernelTable t;
     static std::once_flag once;
@@ -121,26 +99,70 @@ bool pk_make_axis_plan(int n, AxisPlan* p) {
     return true;
 }
 
+// root exp(-2 pi i k / n), exact at the multiples of pi/2 so symmetric bins stay symmetric
+static float2 root_of(int k, int n) {
+    const double a = -2.0 * M_PI * (double)k / (double)n;
+    double c = std::cos(a), s = std::sin(a);
+    if ((4LL * k) % n == 0) {
+        const int q = (int)((4LL * k) / n) & 3;
+        c = q == 0 ? 1 : q == 2 ? -1 : 0;
+        s = q == 1 ? -1 : q == 3 ? 1 : 0;
+    }
+    return make_float2((float)c, (float)s);
+}
+
+void pk_root_table(int n, float2* h) {
+    for (int k = 0; k < n; k++) h[k] = root_of(k, n);
+}
+
 pk_status pk_get_twiddles(pk_ctx* ctx, int twN, const float2** out) {
     auto it = ctx->tw.find(twN);
     if (it != ctx->tw.end()) { *out = it->second.d; return PK_OK; }
     std::vector<float2> h(twN);
-    for (int k = 0; k < twN; k++) {
-        // exact for the multiples of pi/2 so symmetric bins stay symmetric
-        const double a = -2.0 * M_PI * (double)k / (double)twN;
-        double c = std::cos(a), s = std::sin(a);
-        if ((4LL * k) % twN == 0) {
-            const int q = (int)((4LL * k) / twN) & 3;
-            c = q == 0 ? 1 : q == 2 ? -1 : 0;
-            s = q == 1 ? -1 : q == 3 ? 1 : 0;
-        }
-        h[k] = make_float2((float)c, (float)s);
-    }
+    pk_root_table(twN, h.data());
     TwTable t;
     t.n = twN;
     PK_CUDA(cudaMalloc(&t.d, sizeof(float2) * twN));
     PK_CUDA(cudaMemcpy(t.d, h.data(), sizeof(float2) * twN, cudaMemcpyHostToDevice));
     ctx->tw[twN] = t;
+    *out = t.d;
+    return PK_OK;
+}
+
+// Axis table of length-n transforms: the stage-ordered table of n's compile-time plan (entries
+// taken from the root table), else the root table itself.
+int pk_axis_table(int n, float2* out) {
+    const int p = pk_find_plan(n);
+    if (p == 0) {
+        pk_root_table(n, out);
+        return n;
+    }
+    int o = 0;
+    int ns = 1;
+    for (int s = 0; s < kPlans[p].nst; s++) {
+        const int R = kPlans[p].rad[s];
+        const int tstep = n / (ns * R);
+        if (ns > 1)
+            for (int r = 1; r < R; r++)
+                for (int k = 0; k < ns; k++) out[o++] = root_of(r * k * tstep, n);
+        if (direct_radix(R))
+            for (int e = 0; e < R; e++) out[o++] = root_of(e * (n / R), n);
+        ns *= R;
+    }
+    return o;
+}
+
+pk_status pk_get_axis_table(pk_ctx* ctx, int n, const float2** out) {
+    const int key = -n;   // root tables use the positive keys
+    auto it = ctx->tw.find(key);
+    if (it != ctx->tw.end()) { *out = it->second.d; return PK_OK; }
+    std::vector<float2> h(n + PK_TW_EXTRA);
+    const int cnt = pk_axis_table(n, h.data());
+    TwTable t;
+    t.n = cnt;
+    PK_CUDA(cudaMalloc(&t.d, sizeof(float2) * cnt));
+    PK_CUDA(cudaMemcpy(t.d, h.data(), sizeof(float2) * cnt, cudaMemcpyHostToDevice));
+    ctx->tw[key] = t;
     *out = t.d;
     return PK_OK;
 }
@@ -155,7 +177,7 @@ pk_status pk_fill_axis(pk_ctx* ctx, int n, int twN, AxisDev* a) {
     a->twN = twN;
     a->twStride = twN / n;
     a->plan = pk_find_plan(n);
-    return pk_get_twiddles(ctx, twN, &a->tw);
+    return pk_get_axis_table(ctx, n, &a->tw);
 }
 
 static const int kThreads = PK_THREADS;
@@ -201,11 +223,13 @@ size_t pk_spec_elems(const VolDesc& d) { return (size_t)d.Pp * (size_t)d.nrows; 
 // back to back without host synchronisation and can be captured into a CUDA graph.
 static size_t step_smem(int kind, int mode, const VolDesc& v) {
     if (kind == PK_STEP_Y)
-        return sizeof(float2) * (v.M + (v.odd ? 0 : v.M + 1) + padded_size(v.Ly * v.M) + v.Ly +
+        return sizeof(float2) * (tw_slots(v.M) + (v.odd ? 0 : v.M + 1) + padded_size(v.Ly * v.M) + v.Ly +
                                  (size_t)pkpass::y_aux_arrays(mode) * v.Ly * v.M);
     const bool conv = mode == XZ_CONV;
-    if (kind == PK_STEP_X) return sizeof(float2) * (v.ax.n + padded_size(v.Tx * v.ax.n) + (conv ? v.Tx * v.ax.n : 0));
-    if (kind == PK_STEP_Z) return sizeof(float2) * (v.az.n + padded_size(v.Tz * v.az.n) + (conv ? v.Tz * v.az.n : 0));
+    if (kind == PK_STEP_X)
+        return sizeof(float2) * (tw_slots(v.ax.n) + padded_size(v.Tx * v.ax.n) + (conv ? v.Tx * v.ax.n : 0));
+    if (kind == PK_STEP_Z)
+        return sizeof(float2) * (tw_slots(v.az.n) + padded_size(v.Tz * v.az.n) + (conv ? v.Tz * v.az.n : 0));
     return 0;
 }
 
@@ -334,14 +358,6 @@ pk_status pk_program_launch(pk_ctx* ctx, PkProgram& prog, cudaStream_t st) {
         }
         if (s.kind == PK_STEP_Y) {
             kt.y[s.plan]<<<s.grid, kThreads, s.smem, st>>>(dd, dp, s.nvol, s.mode);
-        } else if ((s.kind == PK_STEP_X || s.kind == PK_STEP_Z) && s.plan > 0 && persistent_xz()) {
-            // persistent, double-buffered form: two tile buffers (+ the OTF tile), a few CTAs per SM
-            const VolDesc& v0 = prog.descs[s.desc_off];
-            const int n = s.kind == PK_STEP_X ? v0.ax.n : v0.az.n;
-            const int T = plan_cols_xz(n);
-            const size_t sm = sizeof(float2) * (n + 2 * padded_size(T * n) + (s.mode == XZ_CONV ? T * n : 0));
-            const int grid = std::min(s.grid, sm_count() * 2);
-            kt.xzp[s.plan]<<<grid, kThreads, sm, st>>>(dd, dp, s.nvol, s.kind == PK_STEP_X ? 1 : 2, s.mode);
         } else if (s.kind == PK_STEP_X || s.kind == PK_STEP_Z) {
             kt.xz[s.plan]<<<s.grid, kThreads, s.smem, st>>>(dd, dp, s.nvol, s.kind == PK_STEP_X ? 1 : 2, s.mode);
         } else if (s.kind == PK_STEP_LAMBDA) {

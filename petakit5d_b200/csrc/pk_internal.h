@@ -30,7 +30,7 @@ struct AxisDev {
     int n;            // complex transform length along the axis
     int nst;          // number of radix stages (runtime engine)
     int rad[PK_MAXST];
-    const float2* tw; // tw[k] = exp(-2 pi i k / n), k < n (device, cached per n)
+    const float2* tw; // axis table (device, cached per n): stage-ordered for plan > 0, roots for plan 0
     int twN;          // table length (= n)
     int twStride;     // 1
     int plan;         // compile-time plan id (0 = runtime engine)
@@ -142,6 +142,8 @@ pk_status pk_fail(pk_status st, const std::string& msg);
     } while (0)
 
 // plans / descriptors (fft_kernels.cu)
+void pk_root_table(int n, float2* out);
+int pk_axis_table(int n, float2* out);   // writes at most n + PK_TW_EXTRA entries, returns the count
 pk_status pk_get_twiddles(pk_ctx* ctx, int twN, const float2** out);
 pk_status pk_fill_axis(pk_ctx* ctx, int n, int twN, AxisDev* a);
 pk_status pk_init_desc(pk_ctx* ctx, int ny, int nx, int nz, VolDesc* d);

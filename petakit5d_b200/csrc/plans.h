@@ -70,6 +70,33 @@ constexpr int plan_product(int p) {
     return v;
 }
 
+constexpr int plan_ns_before(int p, int s) {
+    int v = 1;
+    for (int i = 0; i < s; i++) v *= kPlans[p].rad[i];
+    return v;
+}
+constexpr bool direct_radix(int r) { return !(r == 2 || r == 3 || r == 4 || r == 5 || r == 8 || r == 16); }
+
+// Stage-ordered twiddle table of a compile-time plan: stage s (radix R, stride NS > 1) holds
+// W_N^{r k N/(NS R)} at [off_s + (r-1) NS + k] (r = 1..R-1, k < NS), so the threads of a warp read
+// consecutive entries; a direct-DFT radix appends its R roots W_R^e.  The table has N - 1 + (the
+// direct radices) entries.
+constexpr int stage_tw_size(int p, int s) {
+    const int ns = plan_ns_before(p, s), r = kPlans[p].rad[s];
+    return (ns > 1 ? (r - 1) * ns : 0) + (direct_radix(r) ? r : 0);
+}
+constexpr int stage_tw_off(int p, int s) {
+    int o = 0;
+    for (int i = 0; i < s; i++) o += stage_tw_size(p, i);
+    return o;
+}
+constexpr int plan_tw_size(int p) { return stage_tw_off(p, kPlans[p].nst); }
+
+// Shared-memory slots reserved for an axis table of length-n transforms (root table of n entries
+// for the runtime engine, stage-ordered table otherwise).
+#define PK_TW_EXTRA 32
+__host__ __device__ constexpr int tw_slots(int n) { return n + PK_TW_EXTRA; }
+
 // Lines (y pass, contiguous) and columns (x/z passes, a power of two for sector-aligned rows) per tile.
 constexpr int plan_lines_y(int n) { return n >= 1 ? (PK_TILE_POINTS / n > 0 ? PK_TILE_POINTS / n : 1) : 1; }
 constexpr int plan_cols_xz(int n) {
