@@ -184,6 +184,75 @@ __device__ __forceinline__ void stage_s2x(float2* __restrict__ buf, const float2
     if constexpr (!TO_GLOBAL) __syncthreads();
 }
 
+// Last stage kept in registers: shared -> registers, twiddle and butterfly; v[i][r] is then element
+// (j - k) R + k + r NS of line l (b = tid + i * PK_THREADS as in stage_ct).
+template <int R, int NS, int N, int L, bool LF, bool INV, int OFF>
+__device__ __forceinline__ void stage_s2r(const float2* __restrict__ buf, const float2* __restrict__ tw, int tid,
+                                          float2 (&v)[(L * (N / R) + PK_THREADS - 1) / PK_THREADS][R]) {
+    constexpr int M = N / R;
+    constexpr int B = L * M;
+    constexpr int NT = PK_THREADS;
+    constexpr int MAXB = (B + NT - 1) / NT;
+    constexpr int LS = LF ? 1 : N;
+    constexpr int ES = LF ? L : 1;
+#pragma unroll
+    for (int i = 0; i < MAXB; i++) {
+        const int b = tid + i * NT;
+        if (B % NT == 0 || b < B) {
+            const int l = LF ? b % L : b / M;
+            const int j = LF ? b / L : b % M;
+            const int a0 = l * LS + j * ES;
+#pragma unroll
+            for (int r = 0; r < R; r++) v[i][r] = buf[pad(a0 + r * M * ES)];
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < MAXB; i++) {
+        const int b = tid + i * NT;
+        if (B % NT == 0 || b < B) {
+            const int j = LF ? b / L : b % M;
+            const int k = j % NS;
+            if constexpr (NS > 1) {
+#pragma unroll
+                for (int r = 1; r < R; r++) {
+                    float2 w = tw[OFF + (r - 1) * NS + k];
+                    if (INV) w.y = -w.y;
+                    v[i][r] = cmul(v[i][r], w);
+                }
+            }
+            if constexpr (!direct_radix(R)) bfly<R, INV>(v[i]);
+            else bf_direct<R, INV>(v[i], tw + OFF + (NS > 1 ? (R - 1) * NS : 0), 1);
+        }
+    }
+}
+
+// First stage from registers: v[i][r] is element j + r (N / R) of line l; butterfly, store to shared.
+template <int R, int N, int L, bool LF, bool INV>
+__device__ __forceinline__ void stage_r2s(float2* __restrict__ buf, int tid,
+                                          float2 (&v)[(L * (N / R) + PK_THREADS - 1) / PK_THREADS][R]) {
+    static_assert(!direct_radix(R), "first stage needs a register butterfly");
+    constexpr int M = N / R;
+    constexpr int B = L * M;
+    constexpr int NT = PK_THREADS;
+    constexpr int MAXB = (B + NT - 1) / NT;
+    constexpr int LS = LF ? 1 : N;
+    constexpr int ES = LF ? L : 1;
+#pragma unroll
+    for (int i = 0; i < MAXB; i++) {
+        const int b = tid + i * NT;
+        if (B % NT == 0 || b < B) {
+            const int l = LF ? b % L : b / M;
+            const int j = LF ? b / L : b % M;
+            bfly<R, INV>(v[i]);
+            const int a0 = l * LS + j * R * ES;
+#pragma unroll
+            for (int r = 0; r < R; r++) buf[pad(a0 + r * ES)] = v[i][r];
+        }
+    }
+    __syncthreads();
+}
+
 // middle stages S in [S0, S1) of plan P (shared -> shared)
 template <int P, int S, int S1, int NS, int L, bool LF, bool INV>
 __device__ __forceinline__ void run_mid(float2* buf, const float2* tw, int tid) {

@@ -32,10 +32,7 @@
 #include "pk_internal.h"
 #include "plans.h"
 
-void pk_fill_kernels_a(pkpass::KernelTable& t);
-void pk_fill_kernels_b(pkpass::KernelTable& t);
-void pk_fill_kernels_c(pkpass::KernelTable& t);
-void pk_fill_kernels_d(pkpass::KernelTable& t);
+void pk_fill_all_kernels(pkpass::KernelTable& t);
 void set_post(VolDesc& d, const pk_decon_params* p, int mask_mode, void* d_out);
 
 #define PK_NOALLOC_MAX_VOXELS (1u << 20)
@@ -169,10 +166,7 @@ extern "C" pk_status pk_decon_lucy_omw_noalloc(const void* d_in, pk_dtype in_typ
         g_addr[dev] = a;
     }
     if (!g_kt_dev[dev]) {
-        pk_fill_kernels_a(g_kt);
-        pk_fill_kernels_b(g_kt);
-        pk_fill_kernels_c(g_kt);
-        pk_fill_kernels_d(g_kt);
+        pk_fill_all_kernels(g_kt);
         g_kt_dev[dev] = true;
     }
     cudaStream_t st = (cudaStream_t)stream;
@@ -267,7 +261,7 @@ extern "C" pk_status pk_decon_lucy_omw_noalloc(const void* d_in, pk_dtype in_typ
         const VolDesc& hv = h[di];
         const size_t smem = smem_for(kind, mode, hv);
         if (kind == PK_STEP_Y)
-            g_kt.y[hv.ay.plan]<<<hv.blocksY, PK_THREADS, smem, st>>>(ddesc + di, dprefix, 1, mode);
+            g_kt.y[hv.ay.plan][mode]<<<hv.blocksY, PK_THREADS, smem, st>>>(ddesc + di, dprefix, 1, mode);
         else if (kind == PK_STEP_X)
             g_kt.xz[hv.ax.plan]<<<hv.blocksX, PK_THREADS, smem, st>>>(ddesc + di, dprefix + 2, 1, 1, mode);
         else

@@ -129,8 +129,10 @@ __device__ __forceinline__ float2 voxel_pair(const VolDesc& d, int mode, float2 
     switch (mode) {
         case Y_R2C: r = a0; break;
         case Y_RATIO:
-            r.x = __fdiv_rn(a0.x, fmaxf(c.x, PK_EPS_F));
-            r.y = two ? __fdiv_rn(a0.y, fmaxf(c.y, PK_EPS_F)) : 0.f;
+            // __fdividef: at most 2 ulp from the rounded quotient for divisors in [2^-126, 2^126]
+            // (here max(c, eps) >= 2^-52), and no out-of-line slow path in the unrolled loop
+            r.x = __fdividef(a0.x, fmaxf(c.x, PK_EPS_F));
+            r.y = two ? __fdividef(a0.y, fmaxf(c.y, PK_EPS_F)) : 0.f;
             break;
         case Y_UPDATE:
             r.x = fmaxf(__fmul_rn(c.x, a0.x), 0.f);
@@ -175,6 +177,72 @@ __device__ __forceinline__ float2 voxel_pair(const VolDesc& d, int mode, float2 
     return r;
 }
 
+// Y_PRE on a pair of voxels: raw -> I = sat(raw - bg) (uint16) or max(raw - bg, 0) (written), mask =
+// raw ~= 0 (decon_lucy_omw_function.m:79-98).  a0 is the staged raw pair.
+__device__ __forceinline__ float2 pre_pair(const VolDesc& d, bool raw_sync, bool odd, float2 a0, long long row, int y,
+                                           unsigned& zeros) {
+    // raw -> I = sat(raw - bg) (uint16) or max(raw - bg, 0); mask = raw ~= 0
+    const long long vi = row * (long long)d.ny + y;
+    float2 I;
+    bool nz0, nz1 = true;
+    if (raw_sync) {
+        // scalar loads through the raw extent (padded transforms read zeros outside it)
+        const unsigned ur = (unsigned)row;
+        const int z = (int)(ur / (unsigned)d.nx), x = (int)(ur - (unsigned)z * (unsigned)d.nx);
+        float v[2] = {0.f, 0.f};
+        bool nzv[2] = {true, true};
+        for (int e = 0; e < (odd ? 1 : 2); e++) {
+            const int yy = y + e;
+            if (yy >= d.rdims[0] || x >= d.rdims[1] || z >= d.rdims[2]) { v[e] = 0.f; continue; }
+            const long long ri = yy + (long long)d.rdims[0] * (x + (long long)d.rdims[1] * z);
+            if (d.raw_type == PK_U16) {
+                const unsigned r = ((const uint16_t*)d.raw)[ri];
+                nzv[e] = r != 0;
+                v[e] = r > (unsigned)d.bg16 ? (float)(r - (unsigned)d.bg16) : 0.f;
+            } else if (d.raw_type == PK_F32) {
+                const float r = ((const float*)d.raw)[ri];
+                nzv[e] = r != 0.f;
+                v[e] = fmaxf(__fsub_rn(r, d.bg_f), 0.f);
+            } else {
+                const double r = ((const double*)d.raw)[ri];
+                nzv[e] = r != 0.0;
+                v[e] = fmaxf(__fsub_rn((float)r, d.bg_f), 0.f);
+            }
+        }
+        I = make_float2(v[0], v[1]);
+        nz0 = nzv[0];
+        nz1 = nzv[1];
+    } else if (d.raw_type == PK_U16) {
+        const ushort2 q = *reinterpret_cast<const ushort2*>(&a0);
+        const unsigned r0 = q.x, r1 = q.y;
+        nz0 = r0 != 0;
+        nz1 = r1 != 0;
+        I.x = r0 > (unsigned)d.bg16 ? (float)(r0 - (unsigned)d.bg16) : 0.f;
+        I.y = r1 > (unsigned)d.bg16 ? (float)(r1 - (unsigned)d.bg16) : 0.f;
+    } else {
+        const float2 r = a0;
+        nz0 = r.x != 0.f;
+        if (!odd) nz1 = r.y != 0.f;
+        I.x = fmaxf(__fsub_rn(r.x, d.bg_f), 0.f);
+        I.y = fmaxf(__fsub_rn(r.y, d.bg_f), 0.f);
+    }
+    if (odd) {
+        I.y = 0.f;
+        nz1 = true;
+    }
+    st2(d.I, vi, I, odd);
+    if (d.write_mask) {
+        d.mask8[vi] = nz0 ? 1 : 0;
+        if (!odd) d.mask8[vi + 1] = nz1 ? 1 : 0;
+    }
+    zeros += (nz0 ? 0u : 1u) + (nz1 ? 0u : 1u);
+    return I;
+}
+
+constexpr bool y_fusable(int p) {
+    return p > 0 && kPlans[p].nst >= 2 && kPlans[p].rad[0] == kPlans[p].rad[kPlans[p].nst - 1];
+}
+
 // Number of per-voxel input arrays a y-pass mode stages in shared memory.
 __host__ __device__ inline int y_aux_arrays(int mode) {
     switch (mode) {
@@ -184,9 +252,10 @@ __host__ __device__ inline int y_aux_arrays(int mode) {
     }
 }
 
-template <int P>
+template <int P, int MODE>
 __global__ void __launch_bounds__(PK_THREADS, 3) k_y(const VolDesc* __restrict__ descs, const int* __restrict__ prefix,
-                                                     int nvol, int mode) {
+                                                     int nvol, int) {
+    constexpr int mode = MODE;   // one kernel per mode: only that mode's code is in the kernel
     extern __shared__ float2 smem[];
     constexpr int NT = PK_THREADS;
     const int vol = find_vol(prefix, nvol, blockIdx.x);
@@ -308,8 +377,57 @@ __global__ void __launch_bounds__(PK_THREADS, 3) k_y(const VolDesc* __restrict__
             }
         }
         __syncthreads();
-        fft_y<P, true>(buf, A, tw, L, tid);
     }
+
+    bool fused = false;
+    if constexpr (y_fusable(P)) {
+        if (!odd) {
+            // The inverse transform's last stage and the forward transform's first stage have the
+            // same radix, so each thread holds the same elements after the one and before the
+            // other: the per-voxel phase runs on registers between them.
+            constexpr int N = kPlans[P].n, NST = kPlans[P].nst, R = kPlans[P].rad[0];
+            constexpr int LL = plan_lines_y(N), MS = N / R, MAXB = (LL * MS + NT - 1) / NT;
+            float2 v[MAXB][R];
+            if (spec_in) run_mid<P, 0, NST - 1, 1, LL, false, true>(buf, tw, tid);
+            cp_wait<0>();
+            __syncthreads();
+            if (spec_in)
+                stage_s2r<R, plan_ns_before(P, NST - 1), N, LL, false, true, stage_tw_off(P, NST - 1)>(buf, tw, tid, v);
+#pragma unroll
+            for (int i = 0; i < MAXB; i++) {
+                const int b = tid + i * NT;
+                if (MAXB * NT == LL * MS || b < LL * MS) {
+                    const int l = b / MS, j = b - l * MS;
+                    const long long row = row0 + l;
+#pragma unroll
+                    for (int r = 0; r < R; r++) {
+                        const int e = j + r * MS;
+                        float2 out = make_float2(0.f, 0.f);
+                        if (l < Lc) {
+                            const int idx = l * M + e;
+                            if (mode == Y_PRE) {
+                                out = pre_pair(d, raw_sync, false, aux0[idx], row, 2 * e, zeros);
+                            } else {
+                                out = voxel_pair(d, mode, spec_in ? v[i][r] : make_float2(0.f, 0.f),
+                                                 pa0 ? aux0[idx] : make_float2(0.f, 0.f),
+                                                 pa1 ? aux1[idx] : make_float2(0.f, 0.f), row, 2 * e, true, lam, acc0, acc1);
+                            }
+                        }
+                        v[i][r] = out;
+                    }
+                }
+            }
+            if (spec_out) {
+                int tid2 = tid;  // opaque copy: the inverse's index arithmetic is not kept live for reuse
+                asm volatile("mov.b32 %0, %0;" : "+r"(tid2));
+                stage_r2s<R, N, LL, false, false>(buf, tid2, v);
+                run_mid<P, 1, NST, R, LL, false, false>(buf, tw, tid2);
+            }
+            fused = true;
+        }
+    }
+    if (!fused) {
+    if (spec_in) fft_y<P, true>(buf, A, tw, L, tid);
     cp_wait<0>();
     __syncthreads();
 
@@ -320,62 +438,7 @@ __global__ void __launch_bounds__(PK_THREADS, 3) k_y(const VolDesc* __restrict__
         const int y = odd ? k : 2 * k;
         float2 out;
         if (mode == Y_PRE) {
-            // raw -> I = sat(raw - bg) (uint16) or max(raw - bg, 0); mask = raw ~= 0
-            const long long vi = row * (long long)ny + y;
-            float2 I;
-            bool nz0, nz1 = true;
-            if (raw_sync) {
-                // scalar loads through the raw extent (padded transforms read zeros outside it)
-                const unsigned ur = (unsigned)row;
-                const int z = (int)(ur / (unsigned)d.nx), x = (int)(ur - (unsigned)z * (unsigned)d.nx);
-                float v[2] = {0.f, 0.f};
-                bool nzv[2] = {true, true};
-                for (int e = 0; e < (odd ? 1 : 2); e++) {
-                    const int yy = y + e;
-                    if (yy >= d.rdims[0] || x >= d.rdims[1] || z >= d.rdims[2]) { v[e] = 0.f; continue; }
-                    const long long ri = yy + (long long)d.rdims[0] * (x + (long long)d.rdims[1] * z);
-                    if (d.raw_type == PK_U16) {
-                        const unsigned r = ((const uint16_t*)d.raw)[ri];
-                        nzv[e] = r != 0;
-                        v[e] = r > (unsigned)d.bg16 ? (float)(r - (unsigned)d.bg16) : 0.f;
-                    } else if (d.raw_type == PK_F32) {
-                        const float r = ((const float*)d.raw)[ri];
-                        nzv[e] = r != 0.f;
-                        v[e] = fmaxf(__fsub_rn(r, d.bg_f), 0.f);
-                    } else {
-                        const double r = ((const double*)d.raw)[ri];
-                        nzv[e] = r != 0.0;
-                        v[e] = fmaxf(__fsub_rn((float)r, d.bg_f), 0.f);
-                    }
-                }
-                I = make_float2(v[0], v[1]);
-                nz0 = nzv[0];
-                nz1 = nzv[1];
-            } else if (d.raw_type == PK_U16) {
-                const ushort2 q = *reinterpret_cast<const ushort2*>(&aux0[idx]);
-                const unsigned r0 = q.x, r1 = q.y;
-                nz0 = r0 != 0;
-                nz1 = r1 != 0;
-                I.x = r0 > (unsigned)d.bg16 ? (float)(r0 - (unsigned)d.bg16) : 0.f;
-                I.y = r1 > (unsigned)d.bg16 ? (float)(r1 - (unsigned)d.bg16) : 0.f;
-            } else {
-                const float2 r = aux0[idx];
-                nz0 = r.x != 0.f;
-                if (!odd) nz1 = r.y != 0.f;
-                I.x = fmaxf(__fsub_rn(r.x, d.bg_f), 0.f);
-                I.y = fmaxf(__fsub_rn(r.y, d.bg_f), 0.f);
-            }
-            if (odd) {
-                I.y = 0.f;
-                nz1 = true;
-            }
-            st2(d.I, vi, I, odd);
-            if (d.write_mask) {
-                d.mask8[vi] = nz0 ? 1 : 0;
-                if (!odd) d.mask8[vi + 1] = nz1 ? 1 : 0;
-            }
-            zeros += (nz0 ? 0u : 1u) + (nz1 ? 0u : 1u);
-            out = I;
+            out = pre_pair(d, raw_sync, odd, aux0[idx], row, y, zeros);
         } else {
             const float2 cval = spec_in ? buf[pad(idx)] : make_float2(0.f, 0.f);
             out = voxel_pair(d, mode, cval, pa0 ? aux0[idx] : make_float2(0.f, 0.f), pa1 ? aux1[idx] : make_float2(0.f, 0.f),
@@ -383,10 +446,13 @@ __global__ void __launch_bounds__(PK_THREADS, 3) k_y(const VolDesc* __restrict__
         }
         if (spec_out) buf[pad(idx)] = odd ? make_float2(out.x, 0.f) : out;
     }
-
     if (spec_out) {
         __syncthreads();
         fft_y<P, false>(buf, A, tw, L, tid);
+    }
+    }
+
+    if (spec_out) {
         const int nout = Lc * Py;
         const int Pp = d.Pp;
         float2* S0 = d.S + row0 * (long long)Pp;
@@ -593,17 +659,31 @@ __global__ void __launch_bounds__(PK_THREADS, 3) k_xz(const VolDesc* __restrict_
     }
 }
 
+constexpr int kYModes = Y_C2R + 1;
+
 struct KernelTable {
-    void (*y[kNumPlans])(const VolDesc*, const int*, int, int);
+    void (*y[kNumPlans][kYModes])(const VolDesc*, const int*, int, int);
     void (*xz[kNumPlans])(const VolDesc*, const int*, int, int, int);
+};
+
+template <int P, int MD>
+struct RegisterY {
+    static void fill(KernelTable& t) {
+        t.y[P][MD] = k_y<P, MD>;
+        cudaFuncSetAttribute(k_y<P, MD>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        RegisterY<P, MD + 1>::fill(t);
+    }
+};
+template <int P>
+struct RegisterY<P, kYModes> {
+    static void fill(KernelTable&) {}
 };
 
 template <int P, int HI>
 struct Register {
     static void fill(KernelTable& t) {
-        t.y[P] = k_y<P>;
+        RegisterY<P, 0>::fill(t);
         t.xz[P] = k_xz<P>;
-        cudaFuncSetAttribute(k_y<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
         cudaFuncSetAttribute(k_xz<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
         Register<P + 1, HI>::fill(t);
     }

@@ -28,19 +28,32 @@ void pk_fill_kernels_a(pkpass::KernelTable& t);
 void pk_fill_kernels_b(pkpass::KernelTable& t);
 void pk_fill_kernels_c(pkpass::KernelTable& t);
 void pk_fill_kernels_d(pkpass::KernelTable& t);
+void pk_fill_kernels_e(pkpass::KernelTable& t);
+void pk_fill_kernels_f(pkpass::KernelTable& t);
+void pk_fill_kernels_g(pkpass::KernelTable& t);
+void pk_fill_kernels_h(pkpass::KernelTable& t);
+void pk_fill_kernels_i(pkpass::KernelTable& t);
+
+// Every plan's kernels, with their shared-memory limits raised on the current device.
+void pk_fill_all_kernels(pkpass::KernelTable& t) {
+    memset(&t, 0, sizeof(t));
+    pk_fill_kernels_a(t);
+    pk_fill_kernels_b(t);
+    pk_fill_kernels_c(t);
+    pk_fill_kernels_d(t);
+    pk_fill_kernels_e(t);
+    pk_fill_kernels_f(t);
+    pk_fill_kernels_g(t);
+    pk_fill_kernels_h(t);
+    pk_fill_kernels_i(t);
+}
 
 namespace {
 
 const pkpass::KernelTable& kernels() {
     static pkpass::KernelTable t;
     static std::once_flag once;
-    std::call_once(once, [] {
-        memset(&t, 0, sizeof(t));
-        pk_fill_kernels_a(t);
-        pk_fill_kernels_b(t);
-        pk_fill_kernels_c(t);
-        pk_fill_kernels_d(t);
-    });
+    std::call_once(once, [] { pk_fill_all_kernels(t); });
     return t;
 }
 
@@ -357,7 +370,7 @@ pk_status pk_program_launch(pk_ctx* ctx, PkProgram& prog, cudaStream_t st) {
             cudaEventRecord(rec.a, st);
         }
         if (s.kind == PK_STEP_Y) {
-            kt.y[s.plan]<<<s.grid, kThreads, s.smem, st>>>(dd, dp, s.nvol, s.mode);
+            kt.y[s.plan][s.mode]<<<s.grid, kThreads, s.smem, st>>>(dd, dp, s.nvol, s.mode);
         } else if (s.kind == PK_STEP_X || s.kind == PK_STEP_Z) {
             kt.xz[s.plan]<<<s.grid, kThreads, s.smem, st>>>(dd, dp, s.nvol, s.kind == PK_STEP_X ? 1 : 2, s.mode);
         } else if (s.kind == PK_STEP_LAMBDA) {
