@@ -46,17 +46,9 @@ __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_grou
 template <int N>
 __device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-// post-processing of one voxel and the cropped store (decon_lucy_omw_function.m:146-177).
-// x/z of the row are only derived when a crop box or the border-erosion mask needs them.
-__device__ __forceinline__ void post_store(const VolDesc& d, float J, long long row, int y) {
-    const long long vi = row * d.ny + y;
-    int x = 0, z = 0;
-    if (d.need_xz) {
-        const unsigned r = (unsigned)row;
-        z = (int)(r / (unsigned)d.nx);
-        x = (int)(r - (unsigned)z * (unsigned)d.nx);
-        if (y < d.bb0[0] || y > d.bb1[0] || x < d.bb0[1] || x > d.bb1[1] || z < d.bb0[2] || z > d.bb1[2]) return;
-    }
+// Value of one voxel after the post-processing of decon_lucy_omw_function.m:146-177 (damping, then
+// scaling with offset and mask); x/z only matter to the border-erosion mask.
+__device__ __forceinline__ float post_value(const VolDesc& d, float J, long long vi, int x, int y, int z) {
     if (d.damp > 1.f) {
         const float dI = __fmul_rn(d.damp, d.I[vi]);
         const float a = (J <= dI) ? J : 0.f;
@@ -74,6 +66,21 @@ __device__ __forceinline__ void post_store(const VolDesc& d, float J, long long 
         }
         J = __fmul_rn(__fadd_rn(__fmul_rn(J, d.scale), d.offset), (float)m);
     }
+    return J;
+}
+
+__device__ __forceinline__ void row_xz(const VolDesc& d, long long row, int& x, int& z) {
+    const unsigned r = (unsigned)row;
+    z = (int)(r / (unsigned)d.nx);
+    x = (int)(r - (unsigned)z * (unsigned)d.nx);
+}
+
+__device__ __forceinline__ bool in_box(const VolDesc& d, int x, int y, int z) {
+    return !(y < d.bb0[0] || y > d.bb1[0] || x < d.bb0[1] || x > d.bb1[1] || z < d.bb0[2] || z > d.bb1[2]);
+}
+
+// Store of one post-processed voxel into the (cropped) output.
+__device__ __forceinline__ void out_store(const VolDesc& d, float J, long long vi, int x, int y, int z) {
     long long oi = vi;
     if (d.crop) {
         const long long oy = d.bb1[0] - d.bb0[0] + 1, ox = d.bb1[1] - d.bb0[1] + 1;
@@ -81,6 +88,18 @@ __device__ __forceinline__ void post_store(const VolDesc& d, float J, long long 
     }
     if (d.save16) ((uint16_t*)d.out)[oi] = (uint16_t)u16_of(J);
     else ((float*)d.out)[oi] = J;
+}
+
+// post-processing of one voxel and the cropped store.  x/z of the row are only derived when a crop
+// box or the border-erosion mask needs them.
+__device__ __forceinline__ void post_store(const VolDesc& d, float J, long long row, int y) {
+    const long long vi = row * d.ny + y;
+    int x = 0, z = 0;
+    if (d.need_xz) {
+        row_xz(d, row, x, z);
+        if (!in_box(d, x, y, z)) return;
+    }
+    out_store(d, post_value(d, J, vi, x, y, z), vi, x, y, z);
 }
 
 __device__ __forceinline__ bool mode_from_spec(int m) {
@@ -234,6 +253,27 @@ __device__ __forceinline__ float2 pre_pair(const VolDesc& d, bool raw_sync, bool
     if (d.write_mask) {
         d.mask8[vi] = nz0 ? 1 : 0;
         if (!odd) d.mask8[vi + 1] = nz1 ? 1 : 0;
+    }
+    zeros += (nz0 ? 0u : 1u) + (nz1 ? 0u : 1u);
+    return I;
+}
+
+// Y_PRE value of a staged raw pair (even ny, raw in the volume's own layout): I and the raw-zero count.
+__device__ __forceinline__ float2 pre_value(const VolDesc& d, float2 a0, unsigned& zeros) {
+    float2 I;
+    bool nz0, nz1;
+    if (d.raw_type == PK_U16) {
+        const ushort2 q = *reinterpret_cast<const ushort2*>(&a0);
+        const unsigned r0 = q.x, r1 = q.y;
+        nz0 = r0 != 0;
+        nz1 = r1 != 0;
+        I.x = r0 > (unsigned)d.bg16 ? (float)(r0 - (unsigned)d.bg16) : 0.f;
+        I.y = r1 > (unsigned)d.bg16 ? (float)(r1 - (unsigned)d.bg16) : 0.f;
+    } else {
+        nz0 = a0.x != 0.f;
+        nz1 = a0.y != 0.f;
+        I.x = fmaxf(__fsub_rn(a0.x, d.bg_f), 0.f);
+        I.y = fmaxf(__fsub_rn(a0.y, d.bg_f), 0.f);
     }
     zeros += (nz0 ? 0u : 1u) + (nz1 ? 0u : 1u);
     return I;
@@ -393,27 +433,123 @@ __global__ void __launch_bounds__(PK_THREADS, 3) k_y(const VolDesc* __restrict__
             __syncthreads();
             if (spec_in)
                 stage_s2r<R, plan_ns_before(P, NST - 1), N, LL, false, true, stage_tw_off(P, NST - 1)>(buf, tw, tid, v);
+            // phase 1: every value of the thread's elements, no global stores (so the descriptor
+            // fields stay in registers); phase 2: the stores of the mode's per-voxel outputs
+            constexpr bool kPost = mode == Y_FINAL || mode == Y_RLFINAL;
 #pragma unroll
             for (int i = 0; i < MAXB; i++) {
                 const int b = tid + i * NT;
                 if (MAXB * NT == LL * MS || b < LL * MS) {
                     const int l = b / MS, j = b - l * MS;
                     const long long row = row0 + l;
+                    int x = 0, z = 0;
+                    if (kPost && d.need_xz) row_xz(d, row, x, z);
 #pragma unroll
                     for (int r = 0; r < R; r++) {
                         const int e = j + r * MS;
                         float2 out = make_float2(0.f, 0.f);
                         if (l < Lc) {
                             const int idx = l * M + e;
-                            if (mode == Y_PRE) {
-                                out = pre_pair(d, raw_sync, false, aux0[idx], row, 2 * e, zeros);
-                            } else {
-                                out = voxel_pair(d, mode, spec_in ? v[i][r] : make_float2(0.f, 0.f),
-                                                 pa0 ? aux0[idx] : make_float2(0.f, 0.f),
-                                                 pa1 ? aux1[idx] : make_float2(0.f, 0.f), row, 2 * e, true, lam, acc0, acc1);
+                            const float2 c = spec_in ? v[i][r] : make_float2(0.f, 0.f);
+                            const float2 a0 = pa0 || mode == Y_PRE ? aux0[idx] : make_float2(0.f, 0.f);
+                            const float2 a1 = pa1 ? aux1[idx] : make_float2(0.f, 0.f);
+                            if constexpr (mode == Y_PRE) {
+                                if (raw_sync) out = pre_pair(d, true, false, a0, row, 2 * e, zeros);
+                                else out = pre_value(d, a0, zeros);
+                            } else if constexpr (mode == Y_R2C) {
+                                out = a0;
+                            } else if constexpr (mode == Y_RATIO) {
+                                out.x = __fdividef(a0.x, fmaxf(c.x, PK_EPS_F));
+                                out.y = __fdividef(a0.y, fmaxf(c.y, PK_EPS_F));
+                            } else if constexpr (mode == Y_UPDATE) {
+                                out.x = fmaxf(__fmul_rn(c.x, a0.x), 0.f);
+                                out.y = fmaxf(__fmul_rn(c.y, a0.y), 0.f);
+                            } else if constexpr (kPost) {
+                                const long long vi = row * (long long)ny + 2 * e;
+                                out.x = post_value(d, fmaxf(__fmul_rn(c.x, a0.x), 0.f), vi, x, 2 * e, z);
+                                out.y = post_value(d, fmaxf(__fmul_rn(c.y, a0.y), 0.f), vi + 1, x, 2 * e + 1, z);
+                            } else if constexpr (mode == Y_RLPRE) {
+                                out.x = fmaxf(__fadd_rn(a0.x, __fmul_rn(lam, __fsub_rn(a0.x, a1.x))), 0.f);
+                                out.y = fmaxf(__fadd_rn(a0.y, __fmul_rn(lam, __fsub_rn(a0.y, a1.y))), 0.f);
+                            } else if constexpr (mode == Y_RLUPD) {
+                                out.x = fmaxf(__fmul_rn(a0.x, c.x), 0.f);
+                                out.y = fmaxf(__fmul_rn(a0.y, c.y), 0.f);
+                                if (pa1) {   // not rl_first
+                                    acc0 += (double)__fmul_rn(__fsub_rn(out.x, a0.x), a1.x);
+                                    acc1 += (double)__fmul_rn(a1.x, a1.x);
+                                    acc0 += (double)__fmul_rn(__fsub_rn(out.y, a0.y), a1.y);
+                                    acc1 += (double)__fmul_rn(a1.y, a1.y);
+                                }
+                            } else if constexpr (mode == Y_C2R) {
+                                out = c;
                             }
                         }
                         v[i][r] = out;
+                    }
+                }
+            }
+            if constexpr (mode != Y_RATIO && mode != Y_R2C) {
+                float* p1 = nullptr;
+                float* p2 = nullptr;
+                uint8_t* mk = nullptr;
+                if constexpr (mode == Y_PRE) { p1 = raw_sync ? nullptr : d.I; mk = (raw_sync || !d.write_mask) ? nullptr : d.mask8; }
+                if constexpr (mode == Y_UPDATE) p1 = d.Jn;
+                if constexpr (mode == Y_RLPRE) p1 = d.Yb;
+                if constexpr (mode == Y_RLUPD) { p1 = d.J2n; p2 = d.J4; }
+                if constexpr (mode == Y_C2R) p1 = d.dst;
+                void* const o = kPost ? d.out : nullptr;
+                const bool vec_out = kPost && !d.crop &&
+                                     ((reinterpret_cast<uintptr_t>(o) & (d.save16 ? 3 : 7)) == 0);
+                const bool s16 = kPost && d.save16;
+#pragma unroll
+                for (int i = 0; i < MAXB; i++) {
+                    const int b = tid + i * NT;
+                    if (MAXB * NT == LL * MS || b < LL * MS) {
+                        const int l = b / MS, j = b - l * MS;
+                        if (l < Lc) {
+                            const long long row = row0 + l;
+                            int x = 0, z = 0;
+                            if (kPost && !vec_out && d.need_xz) row_xz(d, row, x, z);
+#pragma unroll
+                            for (int r = 0; r < R; r++) {
+                                const int e = j + r * MS;
+                                const long long vi = row * (long long)ny + 2 * e;
+                                const float2 val = v[i][r];
+                                if constexpr (kPost) {
+                                    if (vec_out) {
+                                        if (s16) {
+                                            const unsigned lo = (unsigned)u16_of(val.x), hi = (unsigned)u16_of(val.y);
+                                            *reinterpret_cast<unsigned*>((uint16_t*)o + vi) = lo | (hi << 16);
+                                        } else {
+                                            *reinterpret_cast<float2*>((float*)o + vi) = val;
+                                        }
+                                    } else {
+                                        if (!d.need_xz || in_box(d, x, 2 * e, z)) out_store(d, val.x, vi, x, 2 * e, z);
+                                        if (!d.need_xz || in_box(d, x, 2 * e + 1, z)) out_store(d, val.y, vi + 1, x, 2 * e + 1, z);
+                                    }
+                                } else {
+                                    if (p1) *reinterpret_cast<float2*>(p1 + vi) = val;
+                                    if constexpr (mode == Y_RLUPD) {
+                                        const float2 a0 = aux0[l * M + e];
+                                        *reinterpret_cast<float2*>(p2 + vi) =
+                                            make_float2(__fsub_rn(val.x, a0.x), __fsub_rn(val.y, a0.y));
+                                    }
+                                    if constexpr (mode == Y_PRE) {
+                                        if (mk) {
+                                            const float2 a0 = aux0[l * M + e];
+                                            unsigned m2;
+                                            if (d.raw_type == PK_U16) {
+                                                const ushort2 q = *reinterpret_cast<const ushort2*>(&a0);
+                                                m2 = (q.x != 0 ? 1u : 0u) | (q.y != 0 ? 0x100u : 0u);
+                                            } else {
+                                                m2 = (a0.x != 0.f ? 1u : 0u) | (a0.y != 0.f ? 0x100u : 0u);
+                                            }
+                                            *reinterpret_cast<uint16_t*>(mk + vi) = (uint16_t)m2;
+                                        }
+                                    }
+                                }
+                            }
+                        }
                     }
                 }
             }
@@ -613,48 +749,48 @@ __global__ void __launch_bounds__(PK_THREADS, 3) k_xz(const VolDesc* __restrict_
             asm volatile("mov.b32 %0, %0;" : "+r"(tid2));
             fft_s2g<P, TT, true, true>(buf, tw, g.fenced(), tid2);
         }
-        return;
-    }
-    for (int idx = tid; idx < P_; idx += NT) {
-        const int e = idx / T, t = idx - e * T;
-        if (k0 + t < Py) cp8(&buf[pad(idx)], d.S + base + e * es + k0 + t);
-        else buf[pad(idx)] = make_float2(0.f, 0.f);
-    }
-    cp_commit();
-    if (conv) {
+    } else {
         for (int idx = tid; idx < P_; idx += NT) {
             const int e = idx / T, t = idx - e * T;
-            if (k0 + t < Py) cp8(&hbuf[idx], d.otf + base + e * es + k0 + t);
+            if (k0 + t < Py) cp8(&buf[pad(idx)], d.S + base + e * es + k0 + t);
+            else buf[pad(idx)] = make_float2(0.f, 0.f);
         }
-    }
-    cp_commit();
-    for (int i = tid; i < (P == 0 ? n : plan_tw_size(P)); i += NT) tw[i] = A.tw[i];
-    cp_wait<1>();
-    __syncthreads();
-    if (mode == XZ_INV) fft_xz<P, true>(buf, A, tw, T, tid);
-    else fft_xz<P, false>(buf, A, tw, T, tid);
-    if (conv) {
-        cp_wait<0>();
-        __syncthreads();
-        const bool cj = d.conj;
-        for (int idx = tid; idx < P_; idx += NT) {
-            const int t = idx % T;
-            if (k0 + t < Py) {
-                float2 hv = hbuf[idx];
-                if (cj) hv.y = -hv.y;
-                buf[pad(idx)] = cmul(buf[pad(idx)], hv);
+        cp_commit();
+        if (conv) {
+            for (int idx = tid; idx < P_; idx += NT) {
+                const int e = idx / T, t = idx - e * T;
+                if (k0 + t < Py) cp8(&hbuf[idx], d.otf + base + e * es + k0 + t);
             }
         }
+        cp_commit();
+        for (int i = tid; i < (P == 0 ? n : plan_tw_size(P)); i += NT) tw[i] = A.tw[i];
+        cp_wait<1>();
         __syncthreads();
-        fft_xz<P, true>(buf, A, tw, T, tid);
-    }
-    const float sc = mode == XZ_FWD_SCALE ? d.xz_scale : 1.f;
-    for (int idx = tid; idx < P_; idx += NT) {
-        const int e = idx / T, t = idx - e * T;
-        if (k0 + t < Py) {
-            float2 v = buf[pad(idx)];
-            if (mode == XZ_FWD_SCALE) v = make_float2(v.x * sc, v.y * sc);
-            d.S[base + e * es + k0 + t] = v;
+        if (mode == XZ_INV) fft_xz<P, true>(buf, A, tw, T, tid);
+        else fft_xz<P, false>(buf, A, tw, T, tid);
+        if (conv) {
+            cp_wait<0>();
+            __syncthreads();
+            const bool cj = d.conj;
+            for (int idx = tid; idx < P_; idx += NT) {
+                const int t = idx % T;
+                if (k0 + t < Py) {
+                    float2 hv = hbuf[idx];
+                    if (cj) hv.y = -hv.y;
+                    buf[pad(idx)] = cmul(buf[pad(idx)], hv);
+                }
+            }
+            __syncthreads();
+            fft_xz<P, true>(buf, A, tw, T, tid);
+        }
+        const float sc = mode == XZ_FWD_SCALE ? d.xz_scale : 1.f;
+        for (int idx = tid; idx < P_; idx += NT) {
+            const int e = idx / T, t = idx - e * T;
+            if (k0 + t < Py) {
+                float2 v = buf[pad(idx)];
+                if (mode == XZ_FWD_SCALE) v = make_float2(v.x * sc, v.y * sc);
+                d.S[base + e * es + k0 + t] = v;
+            }
         }
     }
 }
