@@ -710,8 +710,14 @@ struct XZTile {
     }
 };
 
+// CTAs per SM the x/z kernel of plan P is compiled for: 4 (64 registers) for the lengths whose
+// stages fit that budget without spilling (512, 1024, 2048), else 3 (80 registers).
+constexpr int xz_min_blocks(int p) {
+    return p > 0 && (kPlans[p].n == 512 || kPlans[p].n == 1024 || kPlans[p].n == 2048) ? 4 : 3;
+}
+
 template <int P>
-__global__ void __launch_bounds__(PK_THREADS, 3) k_xz(const VolDesc* __restrict__ descs, const int* __restrict__ prefix,
+__global__ void __launch_bounds__(PK_THREADS, xz_min_blocks(P)) k_xz(const VolDesc* __restrict__ descs, const int* __restrict__ prefix,
                                                       int nvol, int axis, int mode) {
     extern __shared__ float2 smem[];
     constexpr int NT = PK_THREADS;
