@@ -274,14 +274,7 @@ def run_ours(args, rank, world, device):
         kind, rec = dom
         per_ms = rec["ms"] / rec["launches"]
         achieved = rec["bytes"] / (per_ms * 1e-3) / 1e9
-        traffic = None
-        try:
-            with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as f:
-                tj = json.load(f)
-            if kind in tj:
-                traffic = tj[kind]["dram_bytes_per_launch"]
-        except Exception:
-            pass
+        traffic = _ncu_traffic().get(kind)
         roof = {"bound": "hbm", "kernel": kind, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "peak_source": peak_kind, "traffic": traffic,
                 "algorithmic_bytes_per_launch": rec["bytes"], "ms_per_launch": round(per_ms, 5)}
@@ -294,6 +287,20 @@ def run_ours(args, rank, world, device):
         "e2e_ms": e2e_ms, "same": same, "cufft_ms": cufft_ms, "call_bytes": call_bytes, "vol": vol, "psf": psf,
         "psf_b": psf_b, "peak": peak, "peak_kind": peak_kind,
     }
+
+
+def _ncu_traffic():
+    """Per-launch DRAM bytes (read + write) of each pass kind from the committed ncu summary."""
+    out = {}
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic_omw_llsm_512x512x256.md")) as f:
+            for line in f:
+                cells = [c.strip() for c in line.strip().strip("|").split("|")]
+                if len(cells) == 2 and cells[1].isdigit():
+                    out[cells[0]] = int(cells[1])
+    except OSError:
+        pass
+    return out
 
 
 def main():
