@@ -32,6 +32,21 @@ __device__ __forceinline__ void bf_direct(float2* v, const float2* __restrict__ 
     for (int q = 0; q < R; q++) v[q] = out[q];
 }
 
+// Padded shared-memory index of a + r*STEP given pa = pad(a), with the carries of pad() resolved at
+// compile time where possible: STEP a multiple of 16 adds STEP*17/16 per step; RUN16 says that
+// (a mod 16) + r*STEP stays below 16 for every r used, so no spare slot is crossed.
+template <int STEP, bool RUN16>
+__device__ __forceinline__ int pstep(int a, int pa, int r) {
+    if constexpr (STEP % 16 == 0) return pa + r * (STEP + STEP / 16);
+    else if constexpr (RUN16) return pa + r * STEP;
+    else return pad(a + r * STEP);
+}
+
+// Stores of a first stage (Ns = 1) start at a multiple of R along a line of a line-major tile; with
+// R dividing 16 and lines a multiple of 16 long, the R outputs stay inside one 16-slot run.
+template <int R, int N, bool LF>
+constexpr bool first_run16() { return !LF && N % 16 == 0 && 16 % R == 0; }
+
 // One Stockham stage, shared -> shared.  tw is the plan's stage-ordered table; OFF is this stage's
 // section in it.
 template <int R, int NS, int N, int L, bool LF, bool INV, int OFF>
@@ -50,8 +65,9 @@ __device__ __forceinline__ void stage_ct(float2* __restrict__ buf, const float2*
             const int l = LF ? b % L : b / M;
             const int j = LF ? b / L : b % M;
             const int a0 = l * LS + j * ES;
+            const int p0 = pad(a0);
 #pragma unroll
-            for (int r = 0; r < R; r++) v[i][r] = buf[pad(a0 + r * M * ES)];
+            for (int r = 0; r < R; r++) v[i][r] = buf[pstep<M * ES, false>(a0, p0, r)];
         }
     }
     __syncthreads();
@@ -73,8 +89,10 @@ __device__ __forceinline__ void stage_ct(float2* __restrict__ buf, const float2*
             if constexpr (!direct_radix(R)) bfly<R, INV>(v[i]);
             else bf_direct<R, INV>(v[i], tw + OFF + (NS > 1 ? (R - 1) * NS : 0), 1);
             const int a0 = l * LS + ((j - k) * R + k) * ES;
+            const int p0 = pad(a0);
 #pragma unroll
-            for (int r = 0; r < R; r++) buf[pad(a0 + r * NS * ES)] = v[i][r];
+            for (int r = 0; r < R; r++)
+                buf[pstep<NS * ES, NS == 1 && first_run16<R, N, LF>()>(a0, p0, r)] = v[i][r];
         }
     }
     __syncthreads();
@@ -125,8 +143,9 @@ __device__ __forceinline__ void stage_g2s(float2* __restrict__ buf, const G& g, 
             const int j = LF ? b / L : b % M;
             bfly<R, INV>(v[i]);
             const int a0 = l * LS + j * R * ES;
+            const int p0 = pad(a0);
 #pragma unroll
-            for (int r = 0; r < R; r++) buf[pad(a0 + r * ES)] = v[i][r];
+            for (int r = 0; r < R; r++) buf[pstep<ES, first_run16<R, N, LF>()>(a0, p0, r)] = v[i][r];
         }
     }
     __syncthreads();
@@ -149,8 +168,9 @@ __device__ __forceinline__ void stage_s2x(float2* __restrict__ buf, const float2
             const int l = LF ? b % L : b / M;
             const int j = LF ? b / L : b % M;
             const int a0 = l * LS + j * ES;
+            const int p0 = pad(a0);
 #pragma unroll
-            for (int r = 0; r < R; r++) v[i][r] = buf[pad(a0 + r * M * ES)];
+            for (int r = 0; r < R; r++) v[i][r] = buf[pstep<M * ES, false>(a0, p0, r)];
         }
     }
     __syncthreads();
@@ -171,13 +191,15 @@ __device__ __forceinline__ void stage_s2x(float2* __restrict__ buf, const float2
             }
             if constexpr (!direct_radix(R)) bfly<R, INV>(v[i]);
             else bf_direct<R, INV>(v[i], tw + OFF + (NS > 1 ? (R - 1) * NS : 0), 1);
+            const int aw = l * LS + ((j - k) * R + k) * ES;
+            const int pw = pad(aw);
 #pragma unroll
             for (int r = 0; r < R; r++) {
                 const int e = (j - k) * R + k + r * NS;
                 float2 o = v[i][r];
                 if constexpr (MUL) o = cmul(o, g.otf(l, e));
                 if constexpr (TO_GLOBAL) g.st(l, e, o);
-                else buf[pad(l * LS + e * ES)] = o;
+                else buf[pstep<NS * ES, NS == 1 && first_run16<R, N, LF>()>(aw, pw, r)] = o;
             }
         }
     }
@@ -202,8 +224,9 @@ __device__ __forceinline__ void stage_s2r(const float2* __restrict__ buf, const 
             const int l = LF ? b % L : b / M;
             const int j = LF ? b / L : b % M;
             const int a0 = l * LS + j * ES;
+            const int p0 = pad(a0);
 #pragma unroll
-            for (int r = 0; r < R; r++) v[i][r] = buf[pad(a0 + r * M * ES)];
+            for (int r = 0; r < R; r++) v[i][r] = buf[pstep<M * ES, false>(a0, p0, r)];
         }
     }
     __syncthreads();
@@ -246,8 +269,9 @@ __device__ __forceinline__ void stage_r2s(float2* __restrict__ buf, int tid,
             const int j = LF ? b / L : b % M;
             bfly<R, INV>(v[i]);
             const int a0 = l * LS + j * R * ES;
+            const int p0 = pad(a0);
 #pragma unroll
-            for (int r = 0; r < R; r++) buf[pad(a0 + r * ES)] = v[i][r];
+            for (int r = 0; r < R; r++) buf[pstep<ES, first_run16<R, N, LF>()>(a0, p0, r)] = v[i][r];
         }
     }
     __syncthreads();
