@@ -279,7 +279,9 @@ __device__ __forceinline__ float2 pre_value(const VolDesc& d, float2 a0, unsigne
     return I;
 }
 
-constexpr bool y_fusable(int p) {
+// The plan's first and last radix agree: after a transform's last stage each thread holds the elements
+// the next transform's first stage needs.
+constexpr bool same_end_radix(int p) {
     return p > 0 && kPlans[p].nst >= 2 && kPlans[p].rad[0] == kPlans[p].rad[kPlans[p].nst - 1];
 }
 
@@ -420,7 +422,7 @@ __global__ void __launch_bounds__(PK_THREADS, 3) k_y(const VolDesc* __restrict__
     }
 
     bool fused = false;
-    if constexpr (y_fusable(P)) {
+    if constexpr (same_end_radix(P)) {
         if (!odd) {
             // The inverse transform's last stage and the forward transform's first stage have the
             // same radix, so each thread holds the same elements after the one and before the
@@ -749,7 +751,33 @@ __global__ void __launch_bounds__(PK_THREADS, xz_min_blocks(P)) k_xz(const VolDe
                        conv ? d.otf + base + k0 : nullptr, tw, hbuf, TT, kPlans[P].n, plan_tw_size(P), d.conj};
         if (mode == XZ_INV) fft_g<P, TT, true, true, false, true>(buf, tw, g, tid);
         else if (!conv) fft_g<P, TT, true, false, false, true>(buf, tw, g, tid);
-        else {
+        else if constexpr (same_end_radix(P)) {
+            // first and last radix agree: the forward transform's last stage leaves each thread the
+            // elements the inverse transform's first stage needs, so the OTF multiply runs on registers
+            // between them
+            constexpr int N = kPlans[P].n, NST = kPlans[P].nst, R = kPlans[P].rad[0];
+            constexpr int MS = N / R, MAXB = (TT * MS + NT - 1) / NT;
+            float2 v[MAXB][R];
+            stage_g2s<R, N, TT, true, false>(buf, g, tid);
+            run_mid<P, 1, NST - 1, R, TT, true, false>(buf, tw, tid);
+            g.before_last();
+            stage_s2r<R, plan_ns_before(P, NST - 1), N, TT, true, false, stage_tw_off(P, NST - 1)>(buf, tw, tid, v);
+#pragma unroll
+            for (int i = 0; i < MAXB; i++) {
+                const int b = tid + i * NT;
+                if (MAXB * NT == TT * MS || b < TT * MS) {
+                    const int l = b % TT, j = b / TT;
+#pragma unroll
+                    for (int r = 0; r < R; r++) v[i][r] = cmul(v[i][r], g.otf(l, j + r * MS));
+                }
+            }
+            int tid2 = tid;  // opaque copy: keeps the forward's index arithmetic from being reused here
+            asm volatile("mov.b32 %0, %0;" : "+r"(tid2));
+            stage_r2s<R, N, TT, true, true>(buf, tid2, v);
+            run_mid<P, 1, NST - 1, R, TT, true, true>(buf, tw, tid2);
+            stage_s2x<kPlans[P].rad[NST - 1], plan_ns_before(P, NST - 1), N, TT, true, true, stage_tw_off(P, NST - 1),
+                      false, true>(buf, tw, g.fenced(), tid2);
+        } else {
             fft_g<P, TT, true, false, true, false>(buf, tw, g, tid);
             int tid2 = tid;  // opaque copy: keeps the forward's index arithmetic from being reused here
             asm volatile("mov.b32 %0, %0;" : "+r"(tid2));
