@@ -95,6 +95,9 @@ pk_ctx* pk_ctx_create(int device) {
 
 static void release_all(pk_ctx* ctx) {
     cudaStreamSynchronize(ctx->stream);
+    for (auto& kv : ctx->graphs) cudaGraphExecDestroy(kv.second);
+    ctx->graphs.clear();
+    ctx->graph_seen.clear();
     for (auto& kv : ctx->otf) cudaFree(kv.second.d);
     ctx->otf.clear();
     for (auto& s : ctx->scratch)

@@ -349,7 +349,7 @@ double pk_step_bytes(const PkStep& s, const VolDesc* descs) {
     return b;
 }
 
-pk_status pk_program_launch(pk_ctx* ctx, PkProgram& prog, cudaStream_t st) {
+static pk_status launch_steps(pk_ctx* ctx, const PkProgram& prog, cudaStream_t st) {
     const pkpass::KernelTable& kt = kernels();
     for (const PkStep& s : prog.steps) {
         const VolDesc* dd = prog.d_desc + s.desc_off;
@@ -376,13 +376,126 @@ pk_status pk_program_launch(pk_ctx* ctx, PkProgram& prog, cudaStream_t st) {
         } else if (s.kind == PK_STEP_LAMBDA) {
             k_lambda<<<s.nvol, 256, 0, st>>>(dd, s.nvol);
         }
-        PK_CUDA(cudaGetLastError());
-        if (ctx) ctx->launches++;
+        const cudaError_t le = cudaGetLastError();
+        if (le != cudaSuccess)
+            return pk_fail(PK_ERR_CUDA, std::string("launch of ") + pk_step_name(s) + " (plan " + std::to_string(s.plan) +
+                                            ", grid " + std::to_string(s.grid) + ", smem " + std::to_string(s.smem) +
+                                            "): " + cudaGetErrorString(le));
         if (ctx && ctx->prof_on) {
             cudaEventRecord(rec.b, st);
             ctx->prof.push_back(rec);
         }
     }
+    return PK_OK;
+}
+
+// The program's launches as a graph of kernel nodes in launch order, built node by node (no stream
+// capture, so other threads' CUDA calls cannot disturb it).
+static bool build_graph(const PkProgram& prog, cudaGraphExec_t* out) {
+    const pkpass::KernelTable& kt = kernels();
+    cudaGraph_t g = nullptr;
+    if (cudaGraphCreate(&g, 0) != cudaSuccess) { cudaGetLastError(); return false; }
+    cudaGraphNode_t prev = nullptr;
+    bool ok = true;
+    for (const PkStep& s : prog.steps) {
+        if (s.grid == 0) continue;
+        const VolDesc* dd = prog.d_desc + s.desc_off;
+        const int* dp = prog.d_prefix + s.prefix_off;
+        int nvol = s.nvol, mode = s.mode, axis = s.kind == PK_STEP_X ? 1 : 2;
+        void* args5[] = {(void*)&dd, (void*)&dp, (void*)&nvol, (void*)&axis, (void*)&mode};
+        void* args4[] = {(void*)&dd, (void*)&dp, (void*)&nvol, (void*)&mode};
+        void* args2[] = {(void*)&dd, (void*)&nvol};
+        cudaKernelNodeParams p = {};
+        p.blockDim = dim3(kThreads);
+        p.gridDim = dim3(s.grid);
+        p.sharedMemBytes = (unsigned)s.smem;
+        if (s.kind == PK_STEP_Y) {
+            p.func = (void*)kt.y[s.plan][s.mode];
+            p.kernelParams = args4;
+        } else if (s.kind == PK_STEP_X || s.kind == PK_STEP_Z) {
+            p.func = (void*)kt.xz[s.plan];
+            p.kernelParams = args5;
+        } else {
+            p.func = (void*)k_lambda;
+            p.gridDim = dim3(s.nvol);
+            p.blockDim = dim3(256);
+            p.sharedMemBytes = 0;
+            p.kernelParams = args2;
+        }
+        cudaGraphNode_t node = nullptr;
+        if (cudaGraphAddKernelNode(&node, g, prev ? &prev : nullptr, prev ? 1 : 0, &p) != cudaSuccess) {
+            ok = false;
+            break;
+        }
+        prev = node;
+    }
+    if (ok && cudaGraphInstantiate(out, g, 0) != cudaSuccess) ok = false;
+    cudaGraphDestroy(g);
+    if (!ok) cudaGetLastError();
+    return ok;
+}
+
+static bool graphs_enabled() {
+    static int v = -1;
+    if (v < 0) {
+        const char* e = getenv("PK_NO_GRAPHS");
+        v = (e && e[0] == '1') ? 0 : 1;
+    }
+    return v == 1;
+}
+
+// Launches a program's kernels.  A program seen before with the same slot buffer, launch shapes and
+// parameter offsets replays a CUDA graph of its launches (the descriptors it reads are re-uploaded
+// into the same slot buffer before every launch, so the graph stays valid); per-kernel profiling
+// and a stream the caller is capturing take the direct path.
+pk_status pk_program_launch(pk_ctx* ctx, PkProgram& prog, cudaStream_t st) {
+    const int nk = pk_program_kernel_count(prog);
+    bool direct = !ctx || ctx->prof_on || prog.slot < 0 || !graphs_enabled() || nk < 2;
+    if (!direct) {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) {
+            cudaGetLastError();
+            direct = true;
+        } else if (cs != cudaStreamCaptureStatusNone) {
+            direct = true;
+        }
+    }
+    pk_status rs = PK_OK;
+    if (direct) {
+        rs = launch_steps(ctx, prog, st);
+    } else {
+        std::vector<long long> key;
+        key.reserve(2 + 8 * prog.steps.size());
+        key.push_back((long long)(uintptr_t)ctx->slots[prog.slot].d);
+        for (const PkStep& s : prog.steps) {
+            const long long v[] = {s.kind, s.mode, s.plan, s.nvol, s.grid, (long long)s.smem,
+                                   (long long)((const char*)(prog.d_desc + s.desc_off) - (const char*)ctx->slots[prog.slot].d),
+                                   (long long)((const char*)(prog.d_prefix + s.prefix_off) - (const char*)ctx->slots[prog.slot].d)};
+            key.insert(key.end(), v, v + 8);
+        }
+        auto it = ctx->graphs.find(key);
+        if (it == ctx->graphs.end() && ctx->graph_seen.size() >= 4096) ctx->graph_seen.clear();  // bounded
+        if (it != ctx->graphs.end()) {
+            PK_CUDA(cudaGraphLaunch(it->second, st));
+        } else if (ctx->graph_seen[key]++ == 0) {
+            rs = launch_steps(ctx, prog, st);   // first sighting: launch directly
+        } else {
+            if (ctx->graphs.size() >= 64) {   // bounded cache: start over (in-flight graphs are freed on completion)
+                for (auto& kv : ctx->graphs) cudaGraphExecDestroy(kv.second);
+                ctx->graphs.clear();
+                ctx->graph_seen.clear();
+            }
+            cudaGraphExec_t ge = nullptr;
+            if (build_graph(prog, &ge)) {
+                ctx->graphs[key] = ge;
+                PK_CUDA(cudaGraphLaunch(ge, st));
+            } else {
+                rs = launch_steps(ctx, prog, st);   // no graph: launch directly
+            }
+        }
+    }
+    if (rs != PK_OK) return rs;
+    if (ctx) ctx->launches += nk;
     if (ctx && prog.slot >= 0) {
         pk_ctx::ProgSlot& sl = ctx->slots[prog.slot];
         PK_CUDA(cudaEventRecord(sl.ev, st));

@@ -129,6 +129,10 @@ struct pk_ctx {
     struct ProfRec { std::string kind; cudaEvent_t a, b; double bytes; };
     std::vector<ProfRec> prof;
     std::vector<cudaEvent_t> ev_pool;
+    // CUDA graphs of repeated programs: key = slot buffer, launch shapes and parameter offsets.
+    // A program is captured the second time its key is seen and replayed from then on.
+    std::map<std::vector<long long>, cudaGraphExec_t> graphs;
+    std::map<std::vector<long long>, int> graph_seen;
 };
 
 // error helpers (capi.cpp)
