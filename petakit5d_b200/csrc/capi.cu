@@ -95,8 +95,11 @@ pk_ctx* pk_ctx_create(int device) {
 
 static void release_all(pk_ctx* ctx) {
     cudaStreamSynchronize(ctx->stream);
-    for (auto& kv : ctx->graphs) cudaGraphExecDestroy(kv.second);
-    ctx->graphs.clear();
+    if (ctx->h2d) { cudaStreamSynchronize(ctx->h2d); cudaStreamDestroy(ctx->h2d); ctx->h2d = nullptr; }
+    if (ctx->d2h) { cudaStreamSynchronize(ctx->d2h); cudaStreamDestroy(ctx->d2h); ctx->d2h = nullptr; }
+    for (auto e : ctx->io_ev) cudaEventDestroy(e);
+    ctx->io_ev.clear();
+    pk_release_graphs(ctx);
     ctx->graph_seen.clear();
     for (auto& kv : ctx->otf) cudaFree(kv.second.d);
     ctx->otf.clear();
@@ -197,7 +200,7 @@ pk_status pk_output_dims(const int64_t dims[3], const pk_decon_params* p, int64_
 static pk_status decon_device(pk_ctx* ctx, int method, const void* d_in, pk_dtype in_type, const int64_t dims[3],
                               const float* psf_f, const int64_t psf_f_dims[3], const float* psf_b,
                               const int64_t psf_b_dims[3], int32_t numit, const pk_decon_params* params,
-                              void* d_out, cudaStream_t st) {
+                              void* d_out, cudaStream_t st, HostStreamIO* io = nullptr) {
     pk_status s;
     if ((s = check_ctx(ctx)) != PK_OK) return s;
     if ((s = check_dims(dims, "input volume")) != PK_OK) return s;
@@ -213,7 +216,7 @@ static pk_status decon_device(pk_ctx* ctx, int method, const void* d_in, pk_dtyp
     std::lock_guard<std::recursive_mutex> lk(ctx->mu);
     DeviceGuard g(ctx->device);
     return pk_decon_run(ctx, method, d_in, in_type, dims, psf_f, psf_f_dims, psf_b, psf_b_dims, numit, params,
-                        d_out, st);
+                        d_out, st, io);
 }
 
 static pk_status decon_host(pk_ctx* ctx, int method, const void* in, pk_dtype in_type, const int64_t dims[3],
@@ -239,14 +242,28 @@ static pk_status decon_host(pk_ctx* ctx, int method, const void* in, pk_dtype in
     if ((s = pk_scratch(ctx, 9, N * dtype_size(in_type), &d_in)) != PK_OK) return s;
     if ((s = pk_scratch(ctx, 10, outb, &d_out)) != PK_OK) return s;
     cudaStream_t st = ctx->stream;
-    PK_CUDA(cudaMemcpyAsync(d_in, in, N * dtype_size(in_type), cudaMemcpyHostToDevice, st));
-    s = decon_device(ctx, method, d_in, in_type, dims, psf_f, psf_f_dims, psf_b, psf_b_dims, numit, params, d_out, st);
+    // the driver uploads the input (by z-slab where it can, overlapping the first passes) and, when it
+    // streams, downloads the result slab by slab on its copy stream as the last passes finish
+    HostStreamIO io;
+    io.h_in = in;
+    io.h_out = out;
+    io.in_esize = dtype_size(in_type);
+    io.out_esize = params->save16bit ? 2 : 4;
+    s = decon_device(ctx, method, d_in, in_type, dims, psf_f, psf_f_dims, psf_b, psf_b_dims, numit, params, d_out, st,
+                     &io);
     if (s != PK_OK) {
         cudaStreamSynchronize(st);
+        if (ctx->h2d) cudaStreamSynchronize(ctx->h2d);
+        if (ctx->d2h) cudaStreamSynchronize(ctx->d2h);
         return s;
     }
-    PK_CUDA(cudaMemcpyAsync(out, d_out, outb, cudaMemcpyDeviceToHost, st));
-    PK_CUDA(cudaStreamSynchronize(st));
+    if (io.active) {
+        PK_CUDA(cudaStreamSynchronize(ctx->d2h));
+        PK_CUDA(cudaStreamSynchronize(st));
+    } else {
+        PK_CUDA(cudaMemcpyAsync(out, d_out, outb, cudaMemcpyDeviceToHost, st));
+        PK_CUDA(cudaStreamSynchronize(st));
+    }
     return PK_OK;
 }
 

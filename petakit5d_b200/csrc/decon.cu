@@ -7,6 +7,7 @@
 // where the first y pass of a call is [raw -> I; S = R2C(I)] and the last one writes the
 // post-processed, cropped output directly (decon_lucy_omw_function.m:146-177).
 #include <algorithm>
+#include <cstdlib>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -126,24 +127,25 @@ __global__ void k_erode_z(const uint8_t* __restrict__ in, uint8_t* __restrict__ 
     }
 }
 
-// 64-bit content hash of a host buffer (word-wise multiply-xorshift), the OTF cache key
-uint64_t content_hash(const void* p, size_t n, uint64_t h = 0x243F6A8885A308D3ULL) {
-    const unsigned char* b = (const unsigned char*)p;
-    size_t i = 0;
-    for (; i + 8 <= n; i += 8) {
-        uint64_t w;
-        memcpy(&w, b + i, 8);
+// Cache key of a PSF: a 64-bit hash of its dims, its size and 256 evenly spaced values.  It only
+// picks the candidate entry; a hit is confirmed by comparing the whole PSF (memcmp runs near memory
+// speed, a full-content hash would cost a serial pass over the PSF on every call).
+uint64_t psf_key(const float* psf, const int64_t pd[3]) {
+    const size_t n = (size_t)pd[0] * pd[1] * pd[2];
+    uint64_t h = 0x243F6A8885A308D3ULL;
+    auto mix = [&](uint64_t w) {
         h ^= w;
         h *= 0x9E3779B97F4A7C15ULL;
         h ^= h >> 29;
+    };
+    for (int i = 0; i < 3; i++) mix((uint64_t)pd[i]);
+    const size_t samples = n < 256 ? n : 256;
+    for (size_t k = 0; k < samples; k++) {
+        uint32_t w;
+        memcpy(&w, psf + (n - 1) * k / (samples > 1 ? samples - 1 : 1), 4);
+        mix(w);
     }
-    for (; i < n; i++) {
-        h ^= b[i];
-        h *= 0x100000001B3ULL;
-    }
-    h ^= n;
-    h *= 0xBF58476D1CE4E5B9ULL;
-    return h ^ (h >> 31);
+    return h;
 }
 
 int grid_for(long long n) {
@@ -247,12 +249,22 @@ pk_status pk_make_otf(pk_ctx* ctx, const float* h_psf, const int64_t pd[3], int 
 pk_status pk_get_otf(pk_ctx* ctx, const float* h_psf, const int64_t pd[3], int ny, int nx, int nz,
                      const float2** d_otf, cudaStream_t st) {
     const long long pn = (long long)pd[0] * pd[1] * pd[2];
-    uint64_t h = content_hash(h_psf, sizeof(float) * pn);
-    h = content_hash(pd, sizeof(int64_t) * 3, h);
-    auto key = std::make_tuple(h, ny, nx, nz);
-    auto it = ctx->otf.find(key);
-    if (it != ctx->otf.end()) { *d_otf = it->second.d; return PK_OK; }
+    // open addressing on the key: an entry with the same key but another PSF moves this one on
+    uint64_t hk = psf_key(h_psf, pd);
+    for (;; hk++) {
+        auto it = ctx->otf.find(std::make_tuple(hk, ny, nx, nz));
+        if (it == ctx->otf.end()) break;
+        const OtfEntry& c = it->second;
+        if (c.pd[0] == pd[0] && c.pd[1] == pd[1] && c.pd[2] == pd[2] && (long long)c.psf.size() == pn &&
+            memcmp(c.psf.data(), h_psf, sizeof(float) * pn) == 0) {
+            *d_otf = c.d;
+            return PK_OK;
+        }
+    }
+    const auto key = std::make_tuple(hk, ny, nx, nz);
     OtfEntry e;
+    e.psf.assign(h_psf, h_psf + pn);
+    for (int i = 0; i < 3; i++) e.pd[i] = pd[i];
     const int Py = ny / 2 + 1;
     e.bytes = sizeof(float2) * (size_t)(Py + (Py & 1)) * nx * nz;
     cudaError_t ce = cudaMalloc(&e.d, e.bytes);
@@ -351,13 +363,76 @@ static void set_post_job(VolDesc& d, const pk_decon_params* p, int mask_mode, co
     set_post(d, &q, mask_mode, j.d_out);
 }
 
+// The z-slab [z0, z0 + nzs) of a volume descriptor as a volume of its own: y and x passes work
+// plane by plane, so a slab view runs them on those planes only.
+static VolDesc slab_view(const VolDesc& d, int z0, int nzs, size_t raw_esize, size_t out_esize) {
+    VolDesc v = d;
+    const size_t plane = (size_t)d.ny * d.nx;
+    const size_t off = (size_t)z0 * plane;
+    const int ctx_tiles = d.blocksX / d.nz;
+    v.nz = nzs;
+    v.nrows = (long long)d.nx * nzs;
+    v.blocksY = (int)((v.nrows + v.Ly - 1) / v.Ly);
+    v.blocksX = nzs * ctx_tiles;
+    v.blocksZ = 0;
+    v.rdims[2] = nzs;
+    v.bb1[2] = nzs - 1;
+    if (d.raw) v.raw = (const char*)d.raw + off * raw_esize;
+    if (d.src) v.src = d.src + off;
+    if (d.dst) v.dst = d.dst + off;
+    if (d.I) v.I = d.I + off;
+    if (d.Jo) v.Jo = d.Jo + off;
+    if (d.Jn) v.Jn = d.Jn + off;
+    if (d.Yb) v.Yb = d.Yb + off;
+    if (d.J4) v.J4 = d.J4 + off;
+    if (d.J3) v.J3 = d.J3 + off;
+    if (d.J2) v.J2 = d.J2 + off;
+    if (d.J2n) v.J2n = d.J2n + off;
+    if (d.mask8) v.mask8 = d.mask8 + off;
+    if (d.out) v.out = (char*)d.out + off * out_esize;
+    if (d.S) v.S = d.S + (size_t)z0 * d.nx * d.Pp;
+    return v;
+}
+
+static pk_status get_io_event(pk_ctx* ctx, size_t i, cudaEvent_t* e) {
+    while (ctx->io_ev.size() <= i) {
+        cudaEvent_t ev;
+        PK_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        ctx->io_ev.push_back(ev);
+    }
+    *e = ctx->io_ev[i];
+    return PK_OK;
+}
+
 pk_status pk_decon_multi(pk_ctx* ctx, int method, std::vector<DeconJob>& jobs, pk_dtype in_type, int numit,
-                         const pk_decon_params* p, cudaStream_t st) {
+                         const pk_decon_params* p, cudaStream_t st, HostStreamIO* io) {
     pk_status s;
     if (numit < 0) return pk_fail(PK_ERR_INVALID, "NUMIT must be non-negative");
     const size_t nj = jobs.size();
     if (nj == 0) return PK_OK;
     const bool need_mask = p->decon_offset != 0.0 || p->edge_erosion > 0;
+    // a single-volume call with host buffers streams its copies by z-slab when its first and last
+    // passes work plane by plane on the raw layout (no padding, crop, erosion or scalar raw path)
+    bool stream_io = false;
+    static const bool io_off = getenv("PK_NO_STREAM_IO") && getenv("PK_NO_STREAM_IO")[0] == '1';
+    if (io && io_off) {
+        const DeconJob& j = jobs[0];
+        const size_t N = (size_t)j.rdims[0] * j.rdims[1] * j.rdims[2];
+        PK_CUDA(cudaMemcpyAsync((void*)j.d_raw, io->h_in, N * io->in_esize, cudaMemcpyHostToDevice, st));
+    } else if (io) {
+        const DeconJob& j = jobs[0];
+        bool full_box = true;
+        if (j.has_bbox)
+            for (int i = 0; i < 3; i++)
+                if (j.bbox[i] != 1 || j.bbox[i + 3] != j.dims[i]) full_box = false;
+        stream_io = nj == 1 && numit >= 1 && full_box && p->edge_erosion == 0 && in_type != PK_F64 &&
+                    !(in_type == PK_U16 && (j.dims[0] & 1)) && j.dims[2] >= 16 && j.rdims[0] == j.dims[0] &&
+                    j.rdims[1] == j.dims[1] && j.rdims[2] == j.dims[2];
+        if (!stream_io) {
+            const size_t N = (size_t)j.rdims[0] * j.rdims[1] * j.rdims[2];
+            PK_CUDA(cudaMemcpyAsync((void*)j.d_raw, io->h_in, N * io->in_esize, cudaMemcpyHostToDevice, st));
+        }
+    }
     std::vector<VolDesc> base(nj);
     unsigned int* zc = nullptr;
     if (p->edge_erosion > 0) {
@@ -493,14 +568,84 @@ pk_status pk_decon_multi(pk_ctx* ctx, int method, std::vector<DeconJob>& jobs, p
             }
         }
     }
-    if ((s = pk_program_upload(ctx, prog, st)) != PK_OK) return s;
-    return pk_program_launch(ctx, prog, st);
+    // streamed host call: the first two passes (y pre-pass, x forward) and the last two (x inverse,
+    // final y pass) run slab by slab behind the slab copies
+    const size_t ns = prog.steps.size();
+    const DeconJob& j0 = jobs[0];
+    const bool io_uploaded = io && !stream_io;
+    if (stream_io)   // the program has the expected shape (checked, not assumed)
+        stream_io = ns >= 5 && prog.steps[0].kind == PK_STEP_Y && prog.steps[0].mode == Y_PRE &&
+                    prog.steps[1].kind == PK_STEP_X && prog.steps[1].mode == XZ_FWD &&
+                    prog.steps[ns - 2].kind == PK_STEP_X && prog.steps[ns - 2].mode == XZ_INV &&
+                    prog.steps[ns - 1].kind == PK_STEP_Y &&
+                    (prog.steps[ns - 1].mode == Y_FINAL || prog.steps[ns - 1].mode == Y_RLFINAL) &&
+                    !prog.descs[prog.steps[ns - 1].desc_off].need_xz;
+    if (!stream_io) {
+        if (io && !io_uploaded) {   // decided late: whole-volume upload before the program
+            const size_t N = (size_t)j0.rdims[0] * j0.rdims[1] * j0.rdims[2];
+            PK_CUDA(cudaMemcpyAsync((void*)j0.d_raw, io->h_in, N * io->in_esize, cudaMemcpyHostToDevice, st));
+        }
+        if ((s = pk_program_upload(ctx, prog, st)) != PK_OK) return s;
+        return pk_program_launch(ctx, prog, st);
+    }
+    if (!ctx->h2d) PK_CUDA(cudaStreamCreateWithFlags(&ctx->h2d, cudaStreamNonBlocking));
+    if (!ctx->d2h) PK_CUDA(cudaStreamCreateWithFlags(&ctx->d2h, cudaStreamNonBlocking));
+    io->active = true;
+    const int nz = j0.dims[2];
+    const int nslab = std::min(8, nz / 8);
+    const size_t plane = (size_t)j0.dims[0] * j0.dims[1];
+    const PkStep head[2] = {prog.steps[0], prog.steps[1]};
+    const PkStep tail[2] = {prog.steps[ns - 2], prog.steps[ns - 1]};
+    // one program for the whole call (per-slab heads, the middle, per-slab tails), so its descriptors
+    // go up in one small copy queued ahead of the slab uploads
+    PkProgram all;
+    all.no_graph = true;
+    std::vector<int> zb(nslab + 1);
+    for (int sl = 0; sl <= nslab; sl++) zb[sl] = (int)((long long)nz * sl / nslab);
+    for (int sl = 0; sl < nslab; sl++)
+        for (const PkStep& h : head)
+            pk_program_add(all, h.kind, h.mode, {slab_view(prog.descs[h.desc_off], zb[sl], zb[sl + 1] - zb[sl],
+                                                           io->in_esize, io->out_esize)});
+    const size_t mid0 = all.steps.size();
+    for (size_t k = 2; k + 2 < ns; k++) pk_program_add(all, prog.steps[k].kind, prog.steps[k].mode, {prog.descs[prog.steps[k].desc_off]});
+    const size_t tail0 = all.steps.size();
+    for (int sl = 0; sl < nslab; sl++)
+        for (const PkStep& t : tail)
+            pk_program_add(all, t.kind, t.mode, {slab_view(prog.descs[t.desc_off], zb[sl], zb[sl + 1] - zb[sl],
+                                                           io->in_esize, io->out_esize)});
+    if (all.steps.size() != tail0 + 2 * (size_t)nslab || mid0 != 2 * (size_t)nslab)
+        return pk_fail(PK_ERR_UNSUPPORTED, "streamed program layout");
+    if ((s = pk_program_upload(ctx, all, st)) != PK_OK) return s;
+    cudaEvent_t ev;
+    for (int sl = 0; sl < nslab; sl++) {   // every slab upload is queued before any wait on the host
+        if ((s = get_io_event(ctx, sl, &ev)) != PK_OK) return s;
+        PK_CUDA(cudaMemcpyAsync((char*)j0.d_raw + zb[sl] * plane * io->in_esize,
+                                (const char*)io->h_in + zb[sl] * plane * io->in_esize,
+                                (size_t)(zb[sl + 1] - zb[sl]) * plane * io->in_esize, cudaMemcpyHostToDevice, ctx->h2d));
+        PK_CUDA(cudaEventRecord(ev, ctx->h2d));
+    }
+    for (int sl = 0; sl < nslab; sl++) {
+        PK_CUDA(cudaStreamWaitEvent(st, ctx->io_ev[sl], 0));
+        if ((s = pk_program_launch_range(ctx, all, st, 2 * sl, 2 * sl + 2, false)) != PK_OK) return s;
+    }
+    if ((s = pk_program_launch_range(ctx, all, st, mid0, tail0, false)) != PK_OK) return s;
+    for (int sl = 0; sl < nslab; sl++) {
+        if ((s = pk_program_launch_range(ctx, all, st, tail0 + 2 * sl, tail0 + 2 * sl + 2, sl == nslab - 1)) != PK_OK)
+            return s;
+        if ((s = get_io_event(ctx, nslab + sl, &ev)) != PK_OK) return s;
+        PK_CUDA(cudaEventRecord(ev, st));
+        PK_CUDA(cudaStreamWaitEvent(ctx->d2h, ev, 0));
+        PK_CUDA(cudaMemcpyAsync((char*)io->h_out + zb[sl] * plane * io->out_esize,
+                                (const char*)j0.d_out + zb[sl] * plane * io->out_esize,
+                                (size_t)(zb[sl + 1] - zb[sl]) * plane * io->out_esize, cudaMemcpyDeviceToHost, ctx->d2h));
+    }
+    return PK_OK;
 }
 
 pk_status pk_decon_run(pk_ctx* ctx, int method, const void* d_in, pk_dtype in_type, const int64_t dims[3],
                        const float* psf_f, const int64_t psf_f_dims[3], const float* psf_b,
                        const int64_t psf_b_dims[3], int numit, const pk_decon_params* p, void* d_out,
-                       cudaStream_t st) {
+                       cudaStream_t st, HostStreamIO* io) {
     pk_status s;
     if ((s = pk_check_params(dims, p)) != PK_OK) return s;
     if (numit < 0) return pk_fail(PK_ERR_INVALID, "NUMIT must be non-negative");
@@ -520,5 +665,5 @@ pk_status pk_decon_run(pk_ctx* ctx, int method, const void* d_in, pk_dtype in_ty
     j.has_bbox = p->has_bbox;
     for (int i = 0; i < 6; i++) j.bbox[i] = p->bbox[i];
     std::vector<DeconJob> jobs{j};
-    return pk_decon_multi(ctx, method, jobs, in_type, numit, p, st);
+    return pk_decon_multi(ctx, method, jobs, in_type, numit, p, st, io);
 }

@@ -12,6 +12,8 @@
 // paths reuse the same kernels as the single-volume call.
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -349,9 +351,12 @@ double pk_step_bytes(const PkStep& s, const VolDesc* descs) {
     return b;
 }
 
-static pk_status launch_steps(pk_ctx* ctx, const PkProgram& prog, cudaStream_t st) {
+static pk_status launch_steps(pk_ctx* ctx, const PkProgram& prog, cudaStream_t st, size_t b = 0,
+                              size_t e = (size_t)-1) {
     const pkpass::KernelTable& kt = kernels();
-    for (const PkStep& s : prog.steps) {
+    e = std::min(e, prog.steps.size());
+    for (size_t si = b; si < e; si++) {
+        const PkStep& s = prog.steps[si];
         const VolDesc* dd = prog.d_desc + s.desc_off;
         const int* dp = prog.d_prefix + s.prefix_off;
         if (s.grid == 0) continue;
@@ -391,7 +396,7 @@ static pk_status launch_steps(pk_ctx* ctx, const PkProgram& prog, cudaStream_t s
 
 // The program's launches as a graph of kernel nodes in launch order, built node by node (no stream
 // capture, so other threads' CUDA calls cannot disturb it).
-static bool build_graph(const PkProgram& prog, cudaGraphExec_t* out) {
+static bool build_graph(const PkProgram& prog, const VolDesc* d_desc, const int* d_prefix, cudaGraphExec_t* out) {
     const pkpass::KernelTable& kt = kernels();
     cudaGraph_t g = nullptr;
     if (cudaGraphCreate(&g, 0) != cudaSuccess) { cudaGetLastError(); return false; }
@@ -399,8 +404,8 @@ static bool build_graph(const PkProgram& prog, cudaGraphExec_t* out) {
     bool ok = true;
     for (const PkStep& s : prog.steps) {
         if (s.grid == 0) continue;
-        const VolDesc* dd = prog.d_desc + s.desc_off;
-        const int* dp = prog.d_prefix + s.prefix_off;
+        const VolDesc* dd = d_desc + s.desc_off;
+        const int* dp = d_prefix + s.prefix_off;
         int nvol = s.nvol, mode = s.mode, axis = s.kind == PK_STEP_X ? 1 : 2;
         void* args5[] = {(void*)&dd, (void*)&dp, (void*)&nvol, (void*)&axis, (void*)&mode};
         void* args4[] = {(void*)&dd, (void*)&dp, (void*)&nvol, (void*)&mode};
@@ -423,13 +428,22 @@ static bool build_graph(const PkProgram& prog, cudaGraphExec_t* out) {
             p.kernelParams = args2;
         }
         cudaGraphNode_t node = nullptr;
-        if (cudaGraphAddKernelNode(&node, g, prev ? &prev : nullptr, prev ? 1 : 0, &p) != cudaSuccess) {
+        const cudaError_t ea = cudaGraphAddKernelNode(&node, g, prev ? &prev : nullptr, prev ? 1 : 0, &p);
+        if (ea != cudaSuccess) {
+            if (getenv("PK_DEBUG_GRAPHS")) fprintf(stderr, "graph node %s: %s\n", pk_step_name(s), cudaGetErrorString(ea));
             ok = false;
             break;
         }
         prev = node;
     }
-    if (ok && cudaGraphInstantiate(out, g, 0) != cudaSuccess) ok = false;
+    if (ok) {
+        const cudaError_t ei = cudaGraphInstantiate(out, g, 0);
+        if (ei != cudaSuccess) {
+            if (getenv("PK_DEBUG_GRAPHS")) fprintf(stderr, "graph instantiate: %s\n", cudaGetErrorString(ei));
+            ok = false;
+        }
+    }
+    if (getenv("PK_DEBUG_GRAPHS")) fprintf(stderr, "graph of %zu steps built: %d\n", prog.steps.size(), (int)ok);
     cudaGraphDestroy(g);
     if (!ok) cudaGetLastError();
     return ok;
@@ -444,13 +458,12 @@ static bool graphs_enabled() {
     return v == 1;
 }
 
-// Launches a program's kernels.  A program seen before with the same slot buffer, launch shapes and
-// parameter offsets replays a CUDA graph of its launches (the descriptors it reads are re-uploaded
-// into the same slot buffer before every launch, so the graph stays valid); per-kernel profiling
-// and a stream the caller is capturing take the direct path.
+// Launches a program's kernels.  A program seen before with the same launch shapes and descriptor
+// layout replays a CUDA graph of its launches, whose descriptor buffer is refreshed on the stream
+// before each replay; per-kernel profiling and a stream the caller is capturing take the direct path.
 pk_status pk_program_launch(pk_ctx* ctx, PkProgram& prog, cudaStream_t st) {
     const int nk = pk_program_kernel_count(prog);
-    bool direct = !ctx || ctx->prof_on || prog.slot < 0 || !graphs_enabled() || nk < 2;
+    bool direct = !ctx || ctx->prof_on || prog.slot < 0 || prog.no_graph || !graphs_enabled() || nk < 2;
     if (!direct) {
         cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
         if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) {
@@ -466,31 +479,47 @@ pk_status pk_program_launch(pk_ctx* ctx, PkProgram& prog, cudaStream_t st) {
     } else {
         std::vector<long long> key;
         key.reserve(2 + 8 * prog.steps.size());
-        key.push_back((long long)(uintptr_t)ctx->slots[prog.slot].d);
+        key.push_back((long long)prog.descs.size());
+        key.push_back((long long)prog.prefix.size());
         for (const PkStep& s : prog.steps) {
-            const long long v[] = {s.kind, s.mode, s.plan, s.nvol, s.grid, (long long)s.smem,
-                                   (long long)((const char*)(prog.d_desc + s.desc_off) - (const char*)ctx->slots[prog.slot].d),
-                                   (long long)((const char*)(prog.d_prefix + s.prefix_off) - (const char*)ctx->slots[prog.slot].d)};
+            const long long v[] = {s.kind, s.mode, s.plan, s.nvol, s.grid, (long long)s.smem, s.desc_off, s.prefix_off};
             key.insert(key.end(), v, v + 8);
         }
         auto it = ctx->graphs.find(key);
         if (it == ctx->graphs.end() && ctx->graph_seen.size() >= 4096) ctx->graph_seen.clear();  // bounded
-        if (it != ctx->graphs.end()) {
-            PK_CUDA(cudaGraphLaunch(it->second, st));
-        } else if (ctx->graph_seen[key]++ == 0) {
-            rs = launch_steps(ctx, prog, st);   // first sighting: launch directly
+        int* seen = it == ctx->graphs.end() ? &ctx->graph_seen[key] : nullptr;
+        if (seen && (*seen < 0 || (*seen)++ == 0)) {
+            rs = launch_steps(ctx, prog, st);   // first sighting (or no graph possible): launch directly
         } else {
-            if (ctx->graphs.size() >= 64) {   // bounded cache: start over (in-flight graphs are freed on completion)
-                for (auto& kv : ctx->graphs) cudaGraphExecDestroy(kv.second);
-                ctx->graphs.clear();
-                ctx->graph_seen.clear();
+            if (it == ctx->graphs.end()) {
+                if (ctx->graphs.size() >= 64) pk_release_graphs(ctx);   // bounded cache: start over
+                const size_t dbytes = sizeof(VolDesc) * prog.descs.size();
+                pk_ctx::GraphEntry e;
+                e.bytes = dbytes + sizeof(int) * prog.prefix.size();
+                bool ok = cudaMalloc(&e.d, e.bytes) == cudaSuccess && cudaMallocHost(&e.h, e.bytes) == cudaSuccess &&
+                          cudaEventCreateWithFlags(&e.ev, cudaEventDisableTiming) == cudaSuccess;
+                ok = ok && build_graph(prog, (const VolDesc*)e.d, (const int*)((char*)e.d + dbytes), &e.exec);
+                if (!ok) {
+                    cudaGetLastError();
+                    if (e.d) cudaFree(e.d);
+                    if (e.h) cudaFreeHost(e.h);
+                    if (e.ev) cudaEventDestroy(e.ev);
+                    *seen = -1;   // never try this program again
+                    rs = launch_steps(ctx, prog, st);
+                } else {
+                    it = ctx->graphs.emplace(key, e).first;
+                }
             }
-            cudaGraphExec_t ge = nullptr;
-            if (build_graph(prog, &ge)) {
-                ctx->graphs[key] = ge;
-                PK_CUDA(cudaGraphLaunch(ge, st));
-            } else {
-                rs = launch_steps(ctx, prog, st);   // no graph: launch directly
+            if (it != ctx->graphs.end()) {
+                pk_ctx::GraphEntry& e = it->second;
+                if (e.used) PK_CUDA(cudaEventSynchronize(e.ev));   // the previous refresh has been read
+                const size_t dbytes = sizeof(VolDesc) * prog.descs.size();
+                memcpy(e.h, prog.descs.data(), dbytes);
+                memcpy((char*)e.h + dbytes, prog.prefix.data(), sizeof(int) * prog.prefix.size());
+                PK_CUDA(cudaMemcpyAsync(e.d, e.h, e.bytes, cudaMemcpyHostToDevice, st));
+                PK_CUDA(cudaGraphLaunch(e.exec, st));
+                PK_CUDA(cudaEventRecord(e.ev, st));
+                e.used = true;
             }
         }
     }
@@ -502,6 +531,34 @@ pk_status pk_program_launch(pk_ctx* ctx, PkProgram& prog, cudaStream_t st) {
         sl.used = true;
     }
     return PK_OK;
+}
+
+// Launches steps [b, e) of an uploaded program directly (the caller orders them against other
+// streams between ranges); the last range of a program passes last = true, which marks its
+// descriptor slot busy until the work queued so far has run.
+pk_status pk_program_launch_range(pk_ctx* ctx, PkProgram& prog, cudaStream_t st, size_t b, size_t e, bool last) {
+    pk_status rs = launch_steps(ctx, prog, st, b, e);
+    if (rs != PK_OK) return rs;
+    for (size_t i = b; i < std::min(e, prog.steps.size()); i++) ctx->launches += prog.steps[i].grid > 0 ? 1 : 0;
+    if (last && prog.slot >= 0) {
+        pk_ctx::ProgSlot& sl = ctx->slots[prog.slot];
+        PK_CUDA(cudaEventRecord(sl.ev, st));
+        sl.used = true;
+    }
+    return PK_OK;
+}
+
+void pk_release_graphs(pk_ctx* ctx) {
+    for (auto& kv : ctx->graphs) {
+        pk_ctx::GraphEntry& e = kv.second;
+        if (e.ev) cudaEventSynchronize(e.ev);
+        if (e.exec) cudaGraphExecDestroy(e.exec);
+        if (e.d) cudaFree(e.d);
+        if (e.h) cudaFreeHost(e.h);
+        if (e.ev) cudaEventDestroy(e.ev);
+    }
+    ctx->graphs.clear();
+    ctx->graph_seen.clear();
 }
 
 int pk_program_kernel_count(const PkProgram& prog) {

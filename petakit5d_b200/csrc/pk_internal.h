@@ -104,6 +104,8 @@ struct TwTable { float2* d = nullptr; int n = 0; };
 struct OtfEntry {
     float2* d = nullptr;      // pre-scaled (1/N) half spectrum
     size_t bytes = 0;
+    std::vector<float> psf;   // the PSF it was made from (a cache hit compares the whole PSF)
+    int64_t pd[3] = {0, 0, 0};
 };
 
 struct pk_ctx_impl;
@@ -129,10 +131,22 @@ struct pk_ctx {
     struct ProfRec { std::string kind; cudaEvent_t a, b; double bytes; };
     std::vector<ProfRec> prof;
     std::vector<cudaEvent_t> ev_pool;
-    // CUDA graphs of repeated programs: key = slot buffer, launch shapes and parameter offsets.
-    // A program is captured the second time its key is seen and replayed from then on.
-    std::map<std::vector<long long>, cudaGraphExec_t> graphs;
+    // CUDA graphs of repeated programs: key = launch shapes and descriptor layout.  A program is
+    // built into a graph the second time its key is seen and replayed from then on; each graph reads
+    // its descriptors from a device buffer of its own, refreshed (stream-ordered) before each replay.
+    struct GraphEntry {
+        cudaGraphExec_t exec = nullptr;
+        void* d = nullptr;
+        void* h = nullptr;
+        size_t bytes = 0;
+        cudaEvent_t ev = nullptr;
+        bool used = false;
+    };
+    std::map<std::vector<long long>, GraphEntry> graphs;
     std::map<std::vector<long long>, int> graph_seen;
+    // copy streams and per-slab events of streamed host calls
+    cudaStream_t h2d = nullptr, d2h = nullptr;
+    std::vector<cudaEvent_t> io_ev;
 };
 
 // error helpers (capi.cpp)
@@ -165,10 +179,13 @@ struct PkProgram {
     std::vector<PkStep> steps;
     VolDesc* d_desc = nullptr; int* d_prefix = nullptr;   // inside one of the context's program slots
     int slot = -1;
+    bool no_graph = false;   // launch directly (e.g. per-slab programs of a streamed call)
 };
 void pk_program_add(PkProgram& prog, int kind, int mode, const std::vector<VolDesc>& vols);
 pk_status pk_program_upload(pk_ctx* ctx, PkProgram& prog, cudaStream_t st);
 pk_status pk_program_launch(pk_ctx* ctx, PkProgram& prog, cudaStream_t st);
+void pk_release_graphs(pk_ctx* ctx);
+pk_status pk_program_launch_range(pk_ctx* ctx, PkProgram& prog, cudaStream_t st, size_t b, size_t e, bool last);
 double pk_step_bytes(const PkStep& s, const VolDesc* descs);
 const char* pk_step_name(const PkStep& s);
 int pk_program_kernel_count(const PkProgram& prog);
@@ -196,11 +213,20 @@ struct DeconJob {
 };
 size_t pk_job_bytes(int method, const int dims[3], bool need_mask, int blocksY);
 void pk_job_carve(DeconJob& j, int method, bool need_mask, int blocksY, char* arena);
+// Host buffers of a single-volume call whose copies are streamed by z-slab: slab s of the input is
+// uploaded on h2d while the first passes of slab s-1 run, and slab s of the result is downloaded on
+// d2h as soon as the last passes of slab s are done.  The caller synchronises d2h.
+struct HostStreamIO {
+    const void* h_in = nullptr;
+    void* h_out = nullptr;
+    size_t in_esize = 0, out_esize = 0;
+    bool active = false;   // set by pk_decon_multi when the call could be streamed
+};
 pk_status pk_decon_multi(pk_ctx* ctx, int method, std::vector<DeconJob>& jobs, pk_dtype in_type, int numit,
-                         const pk_decon_params* p, cudaStream_t st);
+                         const pk_decon_params* p, cudaStream_t st, HostStreamIO* io = nullptr);
 pk_status pk_check_params(const int64_t dims[3], const pk_decon_params* p);
 
 pk_status pk_decon_run(pk_ctx* ctx, int method, const void* d_in, pk_dtype in_type, const int64_t dims[3],
                        const float* psf_f, const int64_t psf_f_dims[3], const float* psf_b,
                        const int64_t psf_b_dims[3], int numit, const pk_decon_params* p, void* d_out,
-                       cudaStream_t st);
+                       cudaStream_t st, HostStreamIO* io = nullptr);
