@@ -547,9 +547,34 @@ def wl_batched(args):
                                                   pf.ctypes.data, _lib.i64x3(pf.shape), pb.ctypes.data,
                                                   _lib.i64x3(pb.shape), 2, p, o.ctypes.data))
 
+    # the same batch with every chunk and output resident on the device (no copies): the compute bound
+    d_chunks = [pc.to(device) for pc in pinned]
+    d_outs = [torch.empty(o.shape[::-1], dtype=torch.int16, device=device) for o in outs]
+    arr = (_lib.Chunk * len(chunks))()
+    for i, (c, bb) in enumerate(zip(chunks, boxes)):
+        arr[i].in_ = d_chunks[i].data_ptr()
+        arr[i].dims = _lib.i64x3(c.shape)
+        arr[i].psf_id = int(ids[i])
+        arr[i].has_bbox = 1
+        for k in range(6):
+            arr[i].bbox[k] = int(bb[k])
+        arr[i].out = d_outs[i].data_ptr()
+    pfs = [np.asfortranarray(q, np.float32) for q in psfs]
+    pbs = [np.asfortranarray(q, np.float32) for q in bps]
+    fptrs = (_lib.C.c_void_p * len(pfs))(*[a.ctypes.data for a in pfs])
+    bptrs = (_lib.C.c_void_p * len(pbs))(*[a.ctypes.data for a in pbs])
+    pdims = np.array([list(a.shape) for a in pfs], dtype=np.int64).ravel()
+    pdev = D._params({"background": 100.0, "dampfactor": 1.0, "scalefactor": 1.0, "deconoffset": 0.0,
+                      "edgeerosion": 0, "save16bit": True, "bbox": None})
+
+    def resident():
+        _lib.check(_lib.lib.pk_batch_decon(ctx.handle, 1, len(chunks), arr, _lib.PK_U16, len(pfs), fptrs, bptrs,
+                                           pdims.ctypes.data, 2, pdev, 0, 1))
+
     res = {}
-    for name, fn in (("plain", plain), ("batched", batched)):
-        fn()                                   # warm-up (OTFs cached)
+    for name, fn in (("plain", plain), ("batched", batched), ("resident", resident)):
+        fn()                                   # warm-up: OTFs cached
+        fn()                                   # second warm-up: repeated programs become graphs
         torch.cuda.synchronize()
         reps = max(1, min(args.steps, 3))
         e0, e1 = _events(stream)
@@ -568,7 +593,10 @@ def wl_batched(args):
            "value": round(core / (res["batched"] * 1e-3) / 1e6, 1), "unit": "Mvoxel/s",
            "plain_per_chunk": round(core / (res["plain"] * 1e-3) / 1e6, 1),
            "speedup_vs_plain": round(res["plain"] / res["batched"], 3), "ms_batched": round(res["batched"], 2),
-           "ms_plain": round(res["plain"], 2), "batched_equals_plain": same, "core_voxels": int(core)})
+           "ms_plain": round(res["plain"], 2), "batched_equals_plain": same, "core_voxels": int(core),
+           "device_resident": {"value": round(core / (res["resident"] * 1e-3) / 1e6, 1), "unit": "Mvoxel/s",
+                               "ms": round(res["resident"], 2),
+                               "note": "same batch with chunks and outputs already in HBM (compute bound)"}})
 
 
 def wl_served(args):

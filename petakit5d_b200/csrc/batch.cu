@@ -85,12 +85,26 @@ extern "C" pk_status pk_batch_decon(pk_ctx* ctx, int32_t method, int32_t n, cons
     PK_CUDA(cudaMemGetInfo(&freeb, &totalb));
     const size_t budget = std::max<size_t>((size_t)(freeb * 0.40), 1ull << 28);
     const int max_per_wave = device ? n : std::max(2, (n + 11) / 12);  // host mode: ~12 waves so copies overlap compute
+    // chunks ordered by transform size, so a wave holds few distinct plans (each pass launches once per
+    // plan in the wave, and fewer, larger launches fill the GPU better); in host mode the first wave
+    // is half size, so the compute starts after a shorter first upload
+    std::vector<int> order(n);
+    for (int i = 0; i < n; i++) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        const Plan& A = plans[a];
+        const Plan& Bp = plans[b];
+        if (A.dims[0] != Bp.dims[0]) return A.dims[0] < Bp.dims[0];
+        if (A.dims[1] != Bp.dims[1]) return A.dims[1] < Bp.dims[1];
+        return A.dims[2] < Bp.dims[2];
+    });
     std::vector<std::vector<int>> waves;
     {
         std::vector<int> cur;
         size_t cb = 0;
-        for (int i = 0; i < n; i++) {
-            if (!cur.empty() && (cb + plans[i].work_b > budget || (int)cur.size() >= max_per_wave)) {
+        for (int oi = 0; oi < n; oi++) {
+            const int i = order[oi];
+            const int cap = (!device && waves.empty()) ? std::max(1, max_per_wave / 2) : max_per_wave;
+            if (!cur.empty() && (cb + plans[i].work_b > budget || (int)cur.size() >= cap)) {
                 waves.push_back(cur);
                 cur.clear();
                 cb = 0;

@@ -6,27 +6,41 @@
 
 namespace pkfft {
 
-// Direct DFT butterfly for a compile-time radix (7, 9, 11, 13, 17): y_q = sum_m v_m W_R^{qm}, with
-// W_R^e = tw[e * wstep].
+// Direct DFT butterfly for a compile-time odd radix (7, 9, 11, 13, 17), in its symmetric form: with
+// a_m = v_m + v_{R-m}, b_m = v_m - v_{R-m} (m = 1..H, H = (R-1)/2) and W_R^e = c_e + i s_e (the
+// direction's sign in s), y_q = t1 + i t2 and y_{R-q} = t1 - i t2 for
+//   t1 = v_0 + sum_m a_m c_{qm},  t2 = sum_m b_m s_{qm}
+// which takes about a quarter of the multiply-adds of sum_m v_m W^{qm}.  W_R^e = tw[e * wstep] (forward
+// roots; the inverse negates their imaginary parts).
 template <int R, bool INV>
 __device__ __forceinline__ void bf_direct(float2* v, const float2* __restrict__ tw, int wstep) {
-    float2 w[R];
+    static_assert(R % 2 == 1, "symmetric direct DFT needs an odd radix");
+    constexpr int H = (R - 1) / 2;
+    float2 a[H + 1], b[H + 1];
+    float2 y0 = v[0];
 #pragma unroll
-    for (int e = 0; e < R; e++) {
-        w[e] = tw[e * wstep];
-        if (INV) w[e].y = -w[e].y;
+    for (int m = 1; m <= H; m++) {
+        a[m] = make_float2(v[m].x + v[R - m].x, v[m].y + v[R - m].y);
+        b[m] = make_float2(v[m].x - v[R - m].x, v[m].y - v[R - m].y);
+        y0.x += a[m].x;
+        y0.y += a[m].y;
     }
     float2 out[R];
+    out[0] = y0;
 #pragma unroll
-    for (int q = 0; q < R; q++) {
-        float2 acc = v[0];
+    for (int q = 1; q <= H; q++) {
+        float2 t1 = v[0], t2 = make_float2(0.f, 0.f);
 #pragma unroll
-        for (int m = 1; m < R; m++) {
-            const float2 ww = w[(q * m) % R];
-            acc.x += v[m].x * ww.x - v[m].y * ww.y;
-            acc.y += v[m].x * ww.y + v[m].y * ww.x;
+        for (int m = 1; m <= H; m++) {
+            const float2 ww = tw[((q * m) % R) * wstep];   // roots stay in shared memory, not registers
+            const float sw = INV ? -ww.y : ww.y;
+            t1.x += a[m].x * ww.x;
+            t1.y += a[m].y * ww.x;
+            t2.x += b[m].x * sw;
+            t2.y += b[m].y * sw;
         }
-        out[q] = acc;
+        out[q] = make_float2(t1.x - t2.y, t1.y + t2.x);
+        out[R - q] = make_float2(t1.x + t2.y, t1.y - t2.x);
     }
 #pragma unroll
     for (int q = 0; q < R; q++) v[q] = out[q];

@@ -5,7 +5,9 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 SIZES = [(16, 8, 4), (128, 128, 64), (64, 48, 40), (30, 22, 26), (31, 41, 17), (1, 1, 1), (2, 3, 5),
-         (224, 36, 28), (360, 12, 10), (352, 20, 8), (416, 14, 6), (21, 35, 49), (288, 160, 8)]
+         (224, 36, 28), (360, 12, 10), (352, 20, 8), (416, 14, 6), (21, 35, 49), (288, 160, 8),
+         # x and z lengths whose plans end in a direct odd radix (224 = 16*2*7, 288 = 16*2*9, ...)
+         (16, 224, 8), (8, 12, 288), (4, 352, 6), (6, 4, 416), (4, 272, 4), (2, 210, 420)]
 
 
 def _r2c(vol, cuda):
