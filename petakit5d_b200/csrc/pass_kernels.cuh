@@ -259,21 +259,21 @@ __device__ __forceinline__ float2 pre_pair(const VolDesc& d, bool raw_sync, bool
 }
 
 // Y_PRE value of a staged raw pair (even ny, raw in the volume's own layout): I and the raw-zero count.
-__device__ __forceinline__ float2 pre_value(const VolDesc& d, float2 a0, unsigned& zeros) {
+__device__ __forceinline__ float2 pre_value(bool u16, unsigned bg16, float bgf, float2 a0, unsigned& zeros) {
     float2 I;
     bool nz0, nz1;
-    if (d.raw_type == PK_U16) {
+    if (u16) {
         const ushort2 q = *reinterpret_cast<const ushort2*>(&a0);
         const unsigned r0 = q.x, r1 = q.y;
         nz0 = r0 != 0;
         nz1 = r1 != 0;
-        I.x = r0 > (unsigned)d.bg16 ? (float)(r0 - (unsigned)d.bg16) : 0.f;
-        I.y = r1 > (unsigned)d.bg16 ? (float)(r1 - (unsigned)d.bg16) : 0.f;
+        I.x = r0 > bg16 ? (float)(r0 - bg16) : 0.f;
+        I.y = r1 > bg16 ? (float)(r1 - bg16) : 0.f;
     } else {
         nz0 = a0.x != 0.f;
         nz1 = a0.y != 0.f;
-        I.x = fmaxf(__fsub_rn(a0.x, d.bg_f), 0.f);
-        I.y = fmaxf(__fsub_rn(a0.y, d.bg_f), 0.f);
+        I.x = fmaxf(__fsub_rn(a0.x, bgf), 0.f);
+        I.y = fmaxf(__fsub_rn(a0.y, bgf), 0.f);
     }
     zeros += (nz0 ? 0u : 1u) + (nz1 ? 0u : 1u);
     return I;
@@ -438,6 +438,11 @@ __global__ void __launch_bounds__(PK_THREADS, 3) k_y(const VolDesc* __restrict__
             // phase 1: every value of the thread's elements, no global stores (so the descriptor
             // fields stay in registers); phase 2: the stores of the mode's per-voxel outputs
             constexpr bool kPost = mode == Y_FINAL || mode == Y_RLFINAL;
+            // block-uniform settings read once (the common post-processing is just max(c*J, 0))
+            const bool plain_post = kPost && !(d.damp > 1.f) && d.scale_mode == 0;
+            const bool raw_u16 = d.raw_type == PK_U16;
+            const unsigned bg16 = (unsigned)d.bg16;
+            const float bgf = d.bg_f;
 #pragma unroll
             for (int i = 0; i < MAXB; i++) {
                 const int b = tid + i * NT;
@@ -457,7 +462,7 @@ __global__ void __launch_bounds__(PK_THREADS, 3) k_y(const VolDesc* __restrict__
                             const float2 a1 = pa1 ? aux1[idx] : make_float2(0.f, 0.f);
                             if constexpr (mode == Y_PRE) {
                                 if (raw_sync) out = pre_pair(d, true, false, a0, row, 2 * e, zeros);
-                                else out = pre_value(d, a0, zeros);
+                                else out = pre_value(raw_u16, bg16, bgf, a0, zeros);
                             } else if constexpr (mode == Y_R2C) {
                                 out = a0;
                             } else if constexpr (mode == Y_RATIO) {
@@ -467,9 +472,13 @@ __global__ void __launch_bounds__(PK_THREADS, 3) k_y(const VolDesc* __restrict__
                                 out.x = fmaxf(__fmul_rn(c.x, a0.x), 0.f);
                                 out.y = fmaxf(__fmul_rn(c.y, a0.y), 0.f);
                             } else if constexpr (kPost) {
-                                const long long vi = row * (long long)ny + 2 * e;
-                                out.x = post_value(d, fmaxf(__fmul_rn(c.x, a0.x), 0.f), vi, x, 2 * e, z);
-                                out.y = post_value(d, fmaxf(__fmul_rn(c.y, a0.y), 0.f), vi + 1, x, 2 * e + 1, z);
+                                out.x = fmaxf(__fmul_rn(c.x, a0.x), 0.f);
+                                out.y = fmaxf(__fmul_rn(c.y, a0.y), 0.f);
+                                if (!plain_post) {
+                                    const long long vi = row * (long long)ny + 2 * e;
+                                    out.x = post_value(d, out.x, vi, x, 2 * e, z);
+                                    out.y = post_value(d, out.y, vi + 1, x, 2 * e + 1, z);
+                                }
                             } else if constexpr (mode == Y_RLPRE) {
                                 out.x = fmaxf(__fadd_rn(a0.x, __fmul_rn(lam, __fsub_rn(a0.x, a1.x))), 0.f);
                                 out.y = fmaxf(__fadd_rn(a0.y, __fmul_rn(lam, __fsub_rn(a0.y, a1.y))), 0.f);
