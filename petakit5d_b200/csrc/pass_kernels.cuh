@@ -721,10 +721,10 @@ struct XZTile {
     }
 };
 
-// CTAs per SM the x/z kernel of plan P is compiled for: 4 (64 registers) for the lengths whose
-// stages fit that budget without spilling (512, 1024, 2048), else 3 (80 registers).
+// CTAs per SM the x/z kernel of plan P is compiled for: 4 (64 registers) for length 512, where that
+// measured faster, else 3 (80 registers; 1024 and 2048 measured slower at 4).
 constexpr int xz_min_blocks(int p) {
-    return p > 0 && (kPlans[p].n == 512 || kPlans[p].n == 1024 || kPlans[p].n == 2048) ? 4 : 3;
+    return p > 0 && kPlans[p].n == 512 ? 4 : 3;
 }
 
 template <int P>
