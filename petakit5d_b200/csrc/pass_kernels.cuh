@@ -423,7 +423,12 @@ __global__ void __launch_bounds__(PK_THREADS, 3) k_y(const VolDesc* __restrict__
 
     bool fused = false;
     if constexpr (same_end_radix(P)) {
-        if (!odd) {
+        // the common cases only: damping, scaling, masks, crops and the scalar raw path keep the rolled
+        // per-voxel loop below, so their code is not unrolled into this one
+        constexpr bool kPostMode = mode == Y_FINAL || mode == Y_RLFINAL;
+        const bool fuse_ok = !odd && !(mode == Y_PRE && raw_sync) &&
+                             !(kPostMode && (d.damp > 1.f || d.scale_mode != 0 || d.need_xz));
+        if (fuse_ok) {
             // The inverse transform's last stage and the forward transform's first stage have the
             // same radix, so each thread holds the same elements after the one and before the
             // other: the per-voxel phase runs on registers between them.
@@ -437,9 +442,8 @@ __global__ void __launch_bounds__(PK_THREADS, 3) k_y(const VolDesc* __restrict__
                 stage_s2r<R, plan_ns_before(P, NST - 1), N, LL, false, true, stage_tw_off(P, NST - 1)>(buf, tw, tid, v);
             // phase 1: every value of the thread's elements, no global stores (so the descriptor
             // fields stay in registers); phase 2: the stores of the mode's per-voxel outputs
-            constexpr bool kPost = mode == Y_FINAL || mode == Y_RLFINAL;
-            // block-uniform settings read once (the common post-processing is just max(c*J, 0))
-            const bool plain_post = kPost && !(d.damp > 1.f) && d.scale_mode == 0;
+            constexpr bool kPost = kPostMode;
+            // block-uniform settings read once
             const bool raw_u16 = d.raw_type == PK_U16;
             const unsigned bg16 = (unsigned)d.bg16;
             const float bgf = d.bg_f;
@@ -448,9 +452,6 @@ __global__ void __launch_bounds__(PK_THREADS, 3) k_y(const VolDesc* __restrict__
                 const int b = tid + i * NT;
                 if (MAXB * NT == LL * MS || b < LL * MS) {
                     const int l = b / MS, j = b - l * MS;
-                    const long long row = row0 + l;
-                    int x = 0, z = 0;
-                    if (kPost && d.need_xz) row_xz(d, row, x, z);
 #pragma unroll
                     for (int r = 0; r < R; r++) {
                         const int e = j + r * MS;
@@ -461,8 +462,7 @@ __global__ void __launch_bounds__(PK_THREADS, 3) k_y(const VolDesc* __restrict__
                             const float2 a0 = pa0 || mode == Y_PRE ? aux0[idx] : make_float2(0.f, 0.f);
                             const float2 a1 = pa1 ? aux1[idx] : make_float2(0.f, 0.f);
                             if constexpr (mode == Y_PRE) {
-                                if (raw_sync) out = pre_pair(d, true, false, a0, row, 2 * e, zeros);
-                                else out = pre_value(raw_u16, bg16, bgf, a0, zeros);
+                                out = pre_value(raw_u16, bg16, bgf, a0, zeros);
                             } else if constexpr (mode == Y_R2C) {
                                 out = a0;
                             } else if constexpr (mode == Y_RATIO) {
@@ -471,14 +471,9 @@ __global__ void __launch_bounds__(PK_THREADS, 3) k_y(const VolDesc* __restrict__
                             } else if constexpr (mode == Y_UPDATE) {
                                 out.x = fmaxf(__fmul_rn(c.x, a0.x), 0.f);
                                 out.y = fmaxf(__fmul_rn(c.y, a0.y), 0.f);
-                            } else if constexpr (kPost) {
+                            } else if constexpr (kPost) {   // no damping, scaling or mask here
                                 out.x = fmaxf(__fmul_rn(c.x, a0.x), 0.f);
                                 out.y = fmaxf(__fmul_rn(c.y, a0.y), 0.f);
-                                if (!plain_post) {
-                                    const long long vi = row * (long long)ny + 2 * e;
-                                    out.x = post_value(d, out.x, vi, x, 2 * e, z);
-                                    out.y = post_value(d, out.y, vi + 1, x, 2 * e + 1, z);
-                                }
                             } else if constexpr (mode == Y_RLPRE) {
                                 out.x = fmaxf(__fadd_rn(a0.x, __fmul_rn(lam, __fsub_rn(a0.x, a1.x))), 0.f);
                                 out.y = fmaxf(__fadd_rn(a0.y, __fmul_rn(lam, __fsub_rn(a0.y, a1.y))), 0.f);
@@ -503,14 +498,13 @@ __global__ void __launch_bounds__(PK_THREADS, 3) k_y(const VolDesc* __restrict__
                 float* p1 = nullptr;
                 float* p2 = nullptr;
                 uint8_t* mk = nullptr;
-                if constexpr (mode == Y_PRE) { p1 = raw_sync ? nullptr : d.I; mk = (raw_sync || !d.write_mask) ? nullptr : d.mask8; }
+                if constexpr (mode == Y_PRE) { p1 = d.I; mk = d.write_mask ? d.mask8 : nullptr; }
                 if constexpr (mode == Y_UPDATE) p1 = d.Jn;
                 if constexpr (mode == Y_RLPRE) p1 = d.Yb;
                 if constexpr (mode == Y_RLUPD) { p1 = d.J2n; p2 = d.J4; }
                 if constexpr (mode == Y_C2R) p1 = d.dst;
-                void* const o = kPost ? d.out : nullptr;
-                const bool vec_out = kPost && !d.crop &&
-                                     ((reinterpret_cast<uintptr_t>(o) & (d.save16 ? 3 : 7)) == 0);
+                void* const o = kPost ? d.out : nullptr;   // no crop here: the output has the volume's layout
+                const bool vec_out = kPost && ((reinterpret_cast<uintptr_t>(o) & (d.save16 ? 3 : 7)) == 0);
                 const bool s16 = kPost && d.save16;
 #pragma unroll
                 for (int i = 0; i < MAXB; i++) {
@@ -519,8 +513,6 @@ __global__ void __launch_bounds__(PK_THREADS, 3) k_y(const VolDesc* __restrict__
                         const int l = b / MS, j = b - l * MS;
                         if (l < Lc) {
                             const long long row = row0 + l;
-                            int x = 0, z = 0;
-                            if (kPost && !vec_out && d.need_xz) row_xz(d, row, x, z);
 #pragma unroll
                             for (int r = 0; r < R; r++) {
                                 const int e = j + r * MS;
@@ -534,9 +526,12 @@ __global__ void __launch_bounds__(PK_THREADS, 3) k_y(const VolDesc* __restrict__
                                         } else {
                                             *reinterpret_cast<float2*>((float*)o + vi) = val;
                                         }
+                                    } else if (s16) {
+                                        ((uint16_t*)o)[vi] = (uint16_t)u16_of(val.x);
+                                        ((uint16_t*)o)[vi + 1] = (uint16_t)u16_of(val.y);
                                     } else {
-                                        if (!d.need_xz || in_box(d, x, 2 * e, z)) out_store(d, val.x, vi, x, 2 * e, z);
-                                        if (!d.need_xz || in_box(d, x, 2 * e + 1, z)) out_store(d, val.y, vi + 1, x, 2 * e + 1, z);
+                                        ((float*)o)[vi] = val.x;
+                                        ((float*)o)[vi + 1] = val.y;
                                     }
                                 } else {
                                     if (p1) *reinterpret_cast<float2*>(p1 + vi) = val;
