@@ -28,6 +28,8 @@ __device__ __forceinline__ float2 mul_mi(float2 a) {
 }
 __device__ __forceinline__ int pad(int a) { return a + (a >> 4); }
 __host__ __device__ inline int padded_size(int n) { return n + (n >> 4) + 1; }
+// padded_size rounded up to even: what follows the tile starts on a 16-byte boundary
+__host__ __device__ inline int padded_size2(int n) { return (padded_size(n) + 1) & ~1; }
 
 template <bool INV>
 __device__ __forceinline__ void bf2(float2& a, float2& b) {

@@ -113,7 +113,7 @@ size_t smem_for(int kind, int mode, const VolDesc& v) {
                                  (size_t)pkpass::y_aux_arrays(mode) * v.Ly * v.M);
     const AxisDev& A = kind == PK_STEP_X ? v.ax : v.az;
     const int T = kind == PK_STEP_X ? v.Tx : v.Tz;
-    return sizeof(float2) * (tw_slots(A.n) + pkfft::padded_size(T * A.n) + (mode == XZ_CONV ? T * A.n : 0));
+    return sizeof(float2) * (tw_slots(A.n) + pkfft::padded_size2(T * A.n) + (mode == XZ_CONV ? T * A.n : 0));
 }
 
 pkpass::KernelTable g_kt;

@@ -691,10 +691,20 @@ struct XZTile {
     __device__ __forceinline__ void after_loads() const {
         const int tid = threadIdx.x;
         if (gh) {
+            if (T % 2 == 0 && n % 2 == 0) {   // column pairs, one 16-byte copy each: with even T, n, Pp and
+                                              // column offsets, source and shared tile are 16-byte aligned
 #pragma unroll 1
-            for (int idx = tid; idx < T * n; idx += PK_THREADS) {
-                const int e = idx / T, t = idx - e * T;
-                if (t < ncol) cp8(&h[idx], gh + e * es + t);
+                for (int idx = 2 * tid; idx < T * n; idx += 2 * PK_THREADS) {
+                    const int e = idx / T, t = idx - e * T;
+                    if (t + 1 < ncol) cp16(&h[idx], gh + e * es + t);
+                    else if (t < ncol) cp8(&h[idx], gh + e * es + t);
+                }
+            } else {
+#pragma unroll 1
+                for (int idx = tid; idx < T * n; idx += PK_THREADS) {
+                    const int e = idx / T, t = idx - e * T;
+                    if (t < ncol) cp8(&h[idx], gh + e * es + t);
+                }
             }
             cp_commit();
         }
@@ -744,7 +754,7 @@ __global__ void __launch_bounds__(PK_THREADS, xz_min_blocks(P)) k_xz(const VolDe
     // shared memory: tw[tw_slots(n)] | buf[padded T*n] | otf[T*n] (XZ_CONV)
     float2* tw = smem;
     float2* buf = smem + tw_slots(n);
-    float2* hbuf = buf + padded_size(T * n);
+    float2* hbuf = buf + padded_size2(T * n);   // 16-byte aligned: the OTF tile takes 16-byte copies
     const int P_ = T * n;
     const bool conv = mode == XZ_CONV;
     if constexpr (P > 0 && kPlans[P].nst >= 2) {

@@ -242,9 +242,9 @@ static size_t step_smem(int kind, int mode, const VolDesc& v) {
                                  (size_t)pkpass::y_aux_arrays(mode) * v.Ly * v.M);
     const bool conv = mode == XZ_CONV;
     if (kind == PK_STEP_X)
-        return sizeof(float2) * (tw_slots(v.ax.n) + padded_size(v.Tx * v.ax.n) + (conv ? v.Tx * v.ax.n : 0));
+        return sizeof(float2) * (tw_slots(v.ax.n) + padded_size2(v.Tx * v.ax.n) + (conv ? v.Tx * v.ax.n : 0));
     if (kind == PK_STEP_Z)
-        return sizeof(float2) * (tw_slots(v.az.n) + padded_size(v.Tz * v.az.n) + (conv ? v.Tz * v.az.n : 0));
+        return sizeof(float2) * (tw_slots(v.az.n) + padded_size2(v.Tz * v.az.n) + (conv ? v.Tz * v.az.n : 0));
     return 0;
 }
 
