@@ -355,13 +355,31 @@ __global__ void __launch_bounds__(PK_THREADS, 3) k_y(const VolDesc* __restrict__
     const int nvox = Lc * M;
     const long long v0 = row0 * (long long)ny;
     const bool raw_sync = mode == Y_PRE && (d.padded || d.raw_type == PK_F64 || (d.raw_type == PK_U16 && odd));
+    // 16-byte copies of two voxel pairs where rows, pairs and both buffers allow it (even ny divisible
+    // by 4, even M, 16-byte aligned bases), else one pair per copy
+    const bool wide_ok = !odd && M % 2 == 0 && ny % 4 == 0 && (reinterpret_cast<uintptr_t>(aux0) & 15) == 0 &&
+                         (reinterpret_cast<uintptr_t>(aux1) & 15) == 0;
     if (mode == Y_PRE && !raw_sync) {
-        for (int idx = tid; idx < nvox; idx += NT) {
+        if (d.raw_type == PK_F32 && wide_ok && (reinterpret_cast<uintptr_t>(d.raw) & 15) == 0) {
+            for (int idx = 2 * tid; idx < nvox; idx += 2 * NT) {
+                const int l = idx / M, k = idx - l * M;
+                cp16(&aux0[idx], (const float*)d.raw + v0 + (long long)l * ny + 2 * k);
+            }
+        } else {
+            for (int idx = tid; idx < nvox; idx += NT) {
+                const int l = idx / M, k = idx - l * M;
+                const long long vi = v0 + (long long)l * ny + (odd ? k : 2 * k);
+                if (d.raw_type == PK_U16) cp4(&aux0[idx], (const uint16_t*)d.raw + vi);
+                else if (!odd) cp8(&aux0[idx], (const float*)d.raw + vi);
+                else cp4(&aux0[idx], (const float*)d.raw + vi);
+            }
+        }
+    } else if (pa0 && wide_ok && ((reinterpret_cast<uintptr_t>(pa0) | reinterpret_cast<uintptr_t>(pa1)) & 15) == 0) {
+        for (int idx = 2 * tid; idx < nvox; idx += 2 * NT) {
             const int l = idx / M, k = idx - l * M;
-            const long long vi = v0 + (long long)l * ny + (odd ? k : 2 * k);
-            if (d.raw_type == PK_U16) cp4(&aux0[idx], (const uint16_t*)d.raw + vi);
-            else if (!odd) cp8(&aux0[idx], (const float*)d.raw + vi);
-            else cp4(&aux0[idx], (const float*)d.raw + vi);
+            const long long vi = v0 + (long long)l * ny + 2 * k;
+            cp16(&aux0[idx], pa0 + vi);
+            if (pa1) cp16(&aux1[idx], pa1 + vi);
         }
     } else if (pa0) {
         for (int idx = tid; idx < nvox; idx += NT) {
