@@ -618,14 +618,26 @@ __global__ void __launch_bounds__(PK_THREADS, 3) k_y(const VolDesc* __restrict__
         float2* S0 = d.S + row0 * (long long)Pp;
         if (P > 0 && !odd) {
             // X[k] = (Z[k] + Z*[M-k]) / 2 + W^k (Z[k] - Z*[M-k]) / 2i for k < M; X[M] from Z[0]
-            for (int idx = tid; idx < Lc * M; idx += NT) {
-                const int l = idx / M, k = idx - l * M;
-                const float2 zk = buf[pad(idx)];
+            auto split = [&](int l, int k) {
+                const float2 zk = buf[pad(l * M + k)];
                 const float2 zc = conjf2(buf[pad(l * M + (k == 0 ? 0 : M - k))]);
                 const float2 fe = make_float2(0.5f * (zk.x + zc.x), 0.5f * (zk.y + zc.y));
                 const float2 df = csub(zk, zc);
                 const float2 fo = make_float2(0.5f * df.y, -0.5f * df.x);
-                S0[l * Pp + k] = cadd(fe, cmul(twrc[k], fo));
+                return cadd(fe, cmul(twrc[k], fo));
+            };
+            if (M % 2 == 0 && (reinterpret_cast<uintptr_t>(S0) & 15) == 0) {
+                // two bins per thread, one 16-byte store (even M and row pitch keep the pairs aligned)
+                for (int idx = 2 * tid; idx < Lc * M; idx += 2 * NT) {
+                    const int l = idx / M, k = idx - l * M;
+                    const float2 x0 = split(l, k), x1 = split(l, k + 1);
+                    *reinterpret_cast<float4*>(S0 + l * Pp + k) = make_float4(x0.x, x0.y, x1.x, x1.y);
+                }
+            } else {
+                for (int idx = tid; idx < Lc * M; idx += NT) {
+                    const int l = idx / M, k = idx - l * M;
+                    S0[l * Pp + k] = split(l, k);
+                }
             }
             for (int l = tid; l < Lc; l += NT) {
                 const float2 zk = buf[pad(l * M)];
