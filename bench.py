@@ -198,7 +198,6 @@ def run_ours(args, rank, world, device):
         torch.distributed.barrier()
     torch.cuda.synchronize(device)
     l0 = ctx.kernel_launches
-    ctx.profile(True)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
@@ -206,10 +205,16 @@ def run_ours(args, rank, world, device):
         step()
     e1.record(stream)
     torch.cuda.synchronize(device)
-    ctx.profile(False)
     launches = ctx.kernel_launches - l0
     if world > 1:
         torch.distributed.barrier()
+    # per-pass times: the same K steps again with CUDA events around every kernel (these launch
+    # directly, without the call's CUDA graph, so they are timed apart from `value`)
+    ctx.profile(True)
+    for _ in range(args.steps):
+        step()
+    torch.cuda.synchronize(device)
+    ctx.profile(False)
     clk = clocks.stop()
     ms = e0.elapsed_time(e1) / args.steps
     prof = ctx.profile_read()
