@@ -17,17 +17,30 @@
 
 namespace {
 
-__global__ void k_psf_sum(const float* __restrict__ psf, long long n, double* out) {
+// Float64 sum of the PSF in a fixed order (deterministic): block b sums its contiguous slice
+// (thread-strided, then a tree), and k_psf_sum_final adds the block partials in block order.
+constexpr int kPsfSumBlocks = 64;
+__global__ void k_psf_sum(const float* __restrict__ psf, long long n, double* part) {
     __shared__ double s[256];
+    const long long per = (n + gridDim.x - 1) / gridDim.x;
+    const long long b0 = per * blockIdx.x, b1 = min(n, b0 + per);
     double a = 0.0;
-    for (long long i = threadIdx.x; i < n; i += blockDim.x) a += (double)psf[i];
+    for (long long i = b0 + threadIdx.x; i < b1; i += blockDim.x) a += (double)psf[i];
     s[threadIdx.x] = a;
     __syncthreads();
     for (int k = 128; k > 0; k >>= 1) {
         if ((int)threadIdx.x < k) s[threadIdx.x] += s[threadIdx.x + k];
         __syncthreads();
     }
-    if (threadIdx.x == 0) *out = s[0];
+    if (threadIdx.x == 0) part[blockIdx.x] = s[0];
+}
+
+__global__ void k_psf_sum_final(const double* __restrict__ part, int nb, double* out) {
+    if (threadIdx.x == 0) {
+        double a = 0.0;
+        for (int b = 0; b < nb; b++) a += part[b];
+        *out = a;
+    }
 }
 
 // Pad (post) to the volume, circshift by -floor(psz/2), normalise by the float64 sum
@@ -225,11 +238,12 @@ pk_status pk_make_otf(pk_ctx* ctx, const float* h_psf, const int64_t pd[3], int 
     void *d_psf, *d_sum, *d_vol;
     pk_status s;
     if ((s = pk_scratch(ctx, SL_PSF, sizeof(float) * pn, &d_psf)) != PK_OK) return s;
-    if ((s = pk_scratch(ctx, SL_SUM, sizeof(double) * 2, &d_sum)) != PK_OK) return s;
+    if ((s = pk_scratch(ctx, SL_SUM, sizeof(double) * (kPsfSumBlocks + 1), &d_sum)) != PK_OK) return s;
     if ((s = pk_scratch(ctx, SL_JB, sizeof(float) * (size_t)ny * nx * nz, &d_vol)) != PK_OK) return s;
     PK_CUDA(cudaMemcpyAsync(d_psf, h_psf, sizeof(float) * pn, cudaMemcpyHostToDevice, st));
     PK_CUDA(cudaMemsetAsync(d_vol, 0, sizeof(float) * (size_t)ny * nx * nz, st));
-    k_psf_sum<<<1, 256, 0, st>>>((const float*)d_psf, pn, (double*)d_sum);
+    k_psf_sum<<<kPsfSumBlocks, 256, 0, st>>>((const float*)d_psf, pn, (double*)d_sum + 1);
+    k_psf_sum_final<<<1, 32, 0, st>>>((const double*)d_sum + 1, kPsfSumBlocks, (double*)d_sum);
     k_psf_scatter<<<grid_for(pn), 256, 0, st>>>((const float*)d_psf, (int)pd[0], (int)pd[1], (int)pd[2],
                                                  (const double*)d_sum, (float*)d_vol, ny, nx, nz);
     PK_CUDA(cudaGetLastError());
