@@ -119,23 +119,23 @@ __device__ __forceinline__ void st2(float* p, long long vi, float2 v, bool odd) 
     else p[vi] = v.x;
 }
 
-template <int P, bool INV>
+template <int P, bool INV, int TP>
 __device__ __forceinline__ void fft_y(float2* buf, const AxisDev& A, const float2* tw, int L, int tid) {
     if constexpr (P == 0) {
         TileGeom g{L, A.n, A.n, 1, false};
         fft_lines<INV>(buf, A, tw, g, tid, PK_THREADS);
     } else {
-        run_plan<P, 0, 1, plan_lines_y(kPlans[P].n), false, INV>(buf, tw, tid);
+        run_plan<P, 0, 1, plan_lines_y(kPlans[P].n, TP), false, INV>(buf, tw, tid);
     }
 }
 
-template <int P, bool INV>
+template <int P, bool INV, int TP>
 __device__ __forceinline__ void fft_xz(float2* buf, const AxisDev& A, const float2* tw, int T, int tid) {
     if constexpr (P == 0) {
         TileGeom g{T, A.n, 1, T, true};
         fft_lines<INV>(buf, A, tw, g, tid, PK_THREADS);
     } else {
-        run_plan<P, 0, 1, plan_cols_xz(kPlans[P].n), true, INV>(buf, tw, tid);
+        run_plan<P, 0, 1, plan_cols_xz(kPlans[P].n, TP), true, INV>(buf, tw, tid);
     }
 }
 
@@ -294,7 +294,7 @@ __host__ __device__ inline int y_aux_arrays(int mode) {
     }
 }
 
-template <int P, int MODE>
+template <int P, int MODE, int TP = PK_TILE_POINTS>
 __global__ void __launch_bounds__(PK_THREADS, 3) k_y(const VolDesc* __restrict__ descs, const int* __restrict__ prefix,
                                                      int nvol, int) {
     constexpr int mode = MODE;   // one kernel per mode: only that mode's code is in the kernel
@@ -306,7 +306,7 @@ __global__ void __launch_bounds__(PK_THREADS, 3) k_y(const VolDesc* __restrict__
     const int tid = threadIdx.x;
     const AxisDev& A = d.ay;
     const int M = P == 0 ? d.M : kPlans[P].n;
-    const int L = P == 0 ? d.Ly : plan_lines_y(kPlans[P].n);
+    const int L = P == 0 ? d.Ly : plan_lines_y(kPlans[P].n, TP);
     const bool odd = d.odd;
     const int Py = d.Py, ny = d.ny;
     // shared memory: tw[tw_slots(M)] | twrc[M+1] (even ny) | buf[padded L*M] | nyq[L] | aux0[L*M] | aux1[L*M]
@@ -451,7 +451,7 @@ __global__ void __launch_bounds__(PK_THREADS, 3) k_y(const VolDesc* __restrict__
             // same radix, so each thread holds the same elements after the one and before the
             // other: the per-voxel phase runs on registers between them.
             constexpr int N = kPlans[P].n, NST = kPlans[P].nst, R = kPlans[P].rad[0];
-            constexpr int LL = plan_lines_y(N), MS = N / R, MAXB = (LL * MS + NT - 1) / NT;
+            constexpr int LL = plan_lines_y(N, TP), MS = N / R, MAXB = (LL * MS + NT - 1) / NT;
             float2 v[MAXB][R];
             if (spec_in) run_mid<P, 0, NST - 1, 1, LL, false, true>(buf, tw, tid);
             cp_wait<0>();
@@ -587,7 +587,7 @@ __global__ void __launch_bounds__(PK_THREADS, 3) k_y(const VolDesc* __restrict__
         }
     }
     if (!fused) {
-    if (spec_in) fft_y<P, true>(buf, A, tw, L, tid);
+    if (spec_in) fft_y<P, true, TP>(buf, A, tw, L, tid);
     cp_wait<0>();
     __syncthreads();
 
@@ -608,7 +608,7 @@ __global__ void __launch_bounds__(PK_THREADS, 3) k_y(const VolDesc* __restrict__
     }
     if (spec_out) {
         __syncthreads();
-        fft_y<P, false>(buf, A, tw, L, tid);
+        fft_y<P, false, TP>(buf, A, tw, L, tid);
     }
     }
 
@@ -762,7 +762,7 @@ constexpr int xz_min_blocks(int p) {
     return p > 0 && kPlans[p].n == 512 ? 4 : 3;
 }
 
-template <int P>
+template <int P, int TP = PK_TILE_POINTS>
 __global__ void __launch_bounds__(PK_THREADS, xz_min_blocks(P)) k_xz(const VolDesc* __restrict__ descs, const int* __restrict__ prefix,
                                                       int nvol, int axis, int mode) {
     extern __shared__ float2 smem[];
@@ -773,7 +773,7 @@ __global__ void __launch_bounds__(PK_THREADS, xz_min_blocks(P)) k_xz(const VolDe
     const int tid = threadIdx.x;
     const AxisDev& A = axis == 1 ? d.ax : d.az;
     const int n = P == 0 ? A.n : kPlans[P].n;
-    const int T = P == 0 ? (axis == 1 ? d.Tx : d.Tz) : plan_cols_xz(kPlans[P].n);
+    const int T = P == 0 ? (axis == 1 ? d.Tx : d.Tz) : plan_cols_xz(kPlans[P].n, TP);
     const int Py = d.Py;
     const int ctiles = (Py + T - 1) / T;
     const int outer = lb / ctiles;
@@ -790,7 +790,7 @@ __global__ void __launch_bounds__(PK_THREADS, xz_min_blocks(P)) k_xz(const VolDe
     if constexpr (P > 0 && kPlans[P].nst >= 2) {
         // first stage loads from HBM into registers, last stage stores from registers to HBM; the
         // OTF multiply runs inside the last forward stage
-        constexpr int TT = plan_cols_xz(kPlans[P].n);
+        constexpr int TT = plan_cols_xz(kPlans[P].n, TP);
         const XZTile g{d.S + base + k0, es, Py - k0, mode == XZ_FWD_SCALE ? d.xz_scale : 1.f, A.tw,
                        conv ? d.otf + base + k0 : nullptr, tw, hbuf, TT, kPlans[P].n, plan_tw_size(P), d.conj};
         if (mode == XZ_INV) fft_g<P, TT, true, true, false, true>(buf, tw, g, tid);
@@ -844,8 +844,8 @@ __global__ void __launch_bounds__(PK_THREADS, xz_min_blocks(P)) k_xz(const VolDe
         for (int i = tid; i < (P == 0 ? n : plan_tw_size(P)); i += NT) tw[i] = A.tw[i];
         cp_wait<1>();
         __syncthreads();
-        if (mode == XZ_INV) fft_xz<P, true>(buf, A, tw, T, tid);
-        else fft_xz<P, false>(buf, A, tw, T, tid);
+        if (mode == XZ_INV) fft_xz<P, true, TP>(buf, A, tw, T, tid);
+        else fft_xz<P, false, TP>(buf, A, tw, T, tid);
         if (conv) {
             cp_wait<0>();
             __syncthreads();
@@ -859,7 +859,7 @@ __global__ void __launch_bounds__(PK_THREADS, xz_min_blocks(P)) k_xz(const VolDe
                 }
             }
             __syncthreads();
-            fft_xz<P, true>(buf, A, tw, T, tid);
+            fft_xz<P, true, TP>(buf, A, tw, T, tid);
         }
         const float sc = mode == XZ_FWD_SCALE ? d.xz_scale : 1.f;
         for (int idx = tid; idx < P_; idx += NT) {
@@ -875,9 +875,11 @@ __global__ void __launch_bounds__(PK_THREADS, xz_min_blocks(P)) k_xz(const VolDe
 
 constexpr int kYModes = Y_C2R + 1;
 
+// Entries [0, kNumPlans) hold the 4096-point-tile kernels, [kNumPlans + p] the small-tile kernels
+// of plan p (small_tile_plan(p)); a program step's plan id carries that offset.
 struct KernelTable {
-    void (*y[kNumPlans][kYModes])(const VolDesc*, const int*, int, int);
-    void (*xz[kNumPlans])(const VolDesc*, const int*, int, int, int);
+    void (*y[2 * kNumPlans][kYModes])(const VolDesc*, const int*, int, int);
+    void (*xz[2 * kNumPlans])(const VolDesc*, const int*, int, int, int);
 };
 
 template <int P, int MD>
@@ -885,6 +887,10 @@ struct RegisterY {
     static void fill(KernelTable& t) {
         t.y[P][MD] = k_y<P, MD>;
         cudaFuncSetAttribute(k_y<P, MD>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        if constexpr (small_tile_plan(P)) {
+            t.y[kNumPlans + P][MD] = k_y<P, MD, PK_TILE_SMALL>;
+            cudaFuncSetAttribute(k_y<P, MD, PK_TILE_SMALL>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        }
         RegisterY<P, MD + 1>::fill(t);
     }
 };
@@ -899,6 +905,10 @@ struct Register {
         RegisterY<P, 0>::fill(t);
         t.xz[P] = k_xz<P>;
         cudaFuncSetAttribute(k_xz<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        if constexpr (small_tile_plan(P)) {
+            t.xz[kNumPlans + P] = k_xz<P, PK_TILE_SMALL>;
+            cudaFuncSetAttribute(k_xz<P, PK_TILE_SMALL>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        }
         Register<P + 1, HI>::fill(t);
     }
 };

@@ -1,5 +1,5 @@
 // Host side of the pass kernels: transform plans, twiddle tables, per-volume descriptors and the
-// launch programs (pass_kernels.cuh holds the kernels; kern_[a-d].cu instantiate them per plan).
+// launch programs (pass_kernels.cuh holds the kernels; kern_[a-i].cu instantiate them per plan).
 //
 // y pass   (k_y<plan>): one CTA = Ly consecutive rows (contiguous in HBM).  Forward: real row ->
 //          length-ny/2 complex FFT -> split into the ny/2+1 half-spectrum bins.  Inverse: the
@@ -35,6 +35,19 @@ void pk_fill_kernels_f(pkpass::KernelTable& t);
 void pk_fill_kernels_g(pkpass::KernelTable& t);
 void pk_fill_kernels_h(pkpass::KernelTable& t);
 void pk_fill_kernels_i(pkpass::KernelTable& t);
+
+static int sm_count() {
+    static int n = 0;
+    if (!n) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) {
+            cudaGetLastError();
+            n = 148;
+        }
+    }
+    return n;
+}
 
 // Every plan's kernels, with their shared-memory limits raised on the current device.
 void pk_fill_all_kernels(pkpass::KernelTable& t) {
@@ -219,10 +232,22 @@ pk_status pk_init_desc(pk_ctx* ctx, int ny, int nx, int nz, VolDesc* d) {
     if ((long long)d->Ly > d->nrows && d->ay.plan == 0) d->Ly = (int)d->nrows;
     d->Tx = d->ax.plan ? plan_cols_xz(nx) : std::max(1, std::min(P / nx, d->Py));
     d->Tz = d->az.plan ? plan_cols_xz(nz) : std::max(1, std::min(P / nz, d->Py));
-    const int ct_x = (d->Py + d->Tx - 1) / d->Tx, ct_z = (d->Py + d->Tz - 1) / d->Tz;
-    d->blocksY = (int)((d->nrows + d->Ly - 1) / d->Ly);
-    d->blocksX = nz * ct_x;
-    d->blocksZ = nx * ct_z;
+    auto set_blocks = [&]() {
+        const int ct_x = (d->Py + d->Tx - 1) / d->Tx, ct_z = (d->Py + d->Tz - 1) / d->Tz;
+        d->blocksY = (int)((d->nrows + d->Ly - 1) / d->Ly);
+        d->blocksX = nz * ct_x;
+        d->blocksZ = nx * ct_z;
+    };
+    set_blocks();
+    // a volume whose y pass would not give every SM two waves of 3 CTAs runs on 1024-point tiles
+    if (small_tile_plan(d->ay.plan) && small_tile_plan(d->ax.plan) && small_tile_plan(d->az.plan) &&
+        d->blocksY < 2 * 3 * sm_count()) {
+        d->Ly = plan_lines_y(d->M, PK_TILE_SMALL);
+        d->Tx = plan_cols_xz(nx, PK_TILE_SMALL);
+        d->Tz = plan_cols_xz(nz, PK_TILE_SMALL);
+        d->tiles_small = 1;
+        set_blocks();
+    }
     d->bb0[0] = d->bb0[1] = d->bb0[2] = 0;
     d->bb1[0] = ny - 1; d->bb1[1] = nx - 1; d->bb1[2] = nz - 1;
     d->scale = 1.f;
@@ -248,8 +273,10 @@ static size_t step_smem(int kind, int mode, const VolDesc& v) {
     return 0;
 }
 
+// Kernel-table index of a pass: the axis plan, offset by kNumPlans for the small-tile kernels.
 static int step_plan(int kind, const VolDesc& v) {
-    return kind == PK_STEP_Y ? v.ay.plan : kind == PK_STEP_X ? v.ax.plan : kind == PK_STEP_Z ? v.az.plan : 0;
+    const int p = kind == PK_STEP_Y ? v.ay.plan : kind == PK_STEP_X ? v.ax.plan : kind == PK_STEP_Z ? v.az.plan : 0;
+    return (v.tiles_small && kind != PK_STEP_LAMBDA) ? kNumPlans + p : p;
 }
 
 // One step per distinct transform plan among `vols` (a launch is instantiated for one plan).

@@ -89,6 +89,7 @@ struct VolDesc {
     int bb0[3], bb1[3];              // 0-based inclusive crop box (y, x, z)
     int crop;                        // crop box smaller than the volume
     int need_xz;                     // post needs x/z of a voxel (crop or border erosion)
+    int tiles_small;                 // passes use the 1024-point-tile kernels (small volumes)
 };
 
 // ------------------------------------------------------------------ host side

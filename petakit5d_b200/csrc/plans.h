@@ -98,12 +98,18 @@ constexpr int plan_tw_size(int p) { return stage_tw_off(p, kPlans[p].nst); }
 __host__ __device__ constexpr int tw_slots(int n) { return n + PK_TW_EXTRA; }
 
 // Lines (y pass, contiguous) and columns (x/z passes, a power of two for sector-aligned rows) per tile.
-constexpr int plan_lines_y(int n) { return n >= 1 ? (PK_TILE_POINTS / n > 0 ? PK_TILE_POINTS / n : 1) : 1; }
-constexpr int plan_cols_xz(int n) {
+constexpr int plan_lines_y(int n, int tp = PK_TILE_POINTS) { return n >= 1 ? (tp / n > 0 ? tp / n : 1) : 1; }
+constexpr int plan_cols_xz(int n, int tp = PK_TILE_POINTS) {
     int t = 1;
-    while (t * 2 * n <= PK_TILE_POINTS) t *= 2;
+    while (t * 2 * n <= tp) t *= 2;
     return t;
 }
+
+// Small tiles (1024 points, same 256 threads) for volumes too small to fill the GPU with 4096-point
+// tiles: four times the CTAs, at the cost of idle threads in the wide stages.  Instantiated for the
+// compile-time plans up to length 256.
+#define PK_TILE_SMALL 1024
+constexpr bool small_tile_plan(int p) { return p > 0 && kPlans[p].nst >= 2 && kPlans[p].n <= 256; }
 
 inline int pk_find_plan(int n) {
     for (int p = 1; p < kNumPlans; p++)
