@@ -122,9 +122,9 @@ __device__ __forceinline__ void run_plan(float2* buf, const float2* tw, int tid)
 }
 
 // ---- stages whose inputs come from / outputs go to HBM directly (registers <-> global), so a
-// transform makes two fewer passes over shared memory.  G is an accessor with
-//   bool ok(l, e); float2 ld(l, e); void st(l, e, v); float2 otf(l, e)
-// for element e of line l of the tile.
+// transform makes two fewer passes over shared memory.  G is an accessor of the tile with
+//   float2 ld(l, e); void st(l, e, v); float2 otf(l, e); void after_loads(); void before_last()
+// for element e of line l (ld reads zero and st skips outside the tile's valid columns).
 
 // first stage (Ns = 1, no twiddles): global -> registers -> butterfly -> shared.  g.after_loads()
 // runs once the loads are issued (the caller stages tables and side inputs there).

@@ -1,7 +1,9 @@
 // Pass kernels, templated on the transform plan of the axis they transform (plan 0 = runtime
-// engine).  The per-voxel mode of a y pass is a run-time argument.  Global loads are gathered
-// into registers in batches before any shared-memory store, so each thread keeps many loads in
-// flight.
+// engine), on the tile size (4096 points, or 1024 for small volumes) and, for the y pass, on the
+// per-voxel mode (one kernel per mode).  The x/z passes load their tiles from HBM straight into the
+// first radix stage's registers and store from the last stage's registers; the y pass stages rows
+// and per-voxel inputs with cp.async and, where the plan allows, runs the per-voxel arithmetic on
+// registers between the inverse and the forward transform.
 #pragma once
 #include "fft_ct.cuh"
 #include "pk_internal.h"
@@ -781,7 +783,7 @@ __global__ void __launch_bounds__(PK_THREADS, xz_min_blocks(P)) k_xz(const VolDe
     long long base, es;
     if (axis == 1) { base = (long long)outer * d.nx * d.Pp; es = d.Pp; }
     else { base = (long long)outer * d.Pp; es = (long long)d.nx * d.Pp; }
-    // shared memory: tw[tw_slots(n)] | buf[padded T*n] | otf[T*n] (XZ_CONV)
+    // shared memory: tw[tw_slots(n)] | buf[padded T*n, rounded up to even] | otf[T*n] (XZ_CONV)
     float2* tw = smem;
     float2* buf = smem + tw_slots(n);
     float2* hbuf = buf + padded_size2(T * n);   // 16-byte aligned: the OTF tile takes 16-byte copies
