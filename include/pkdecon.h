@@ -96,6 +96,21 @@ PK_API pk_status pk_decon_lucy_omw(pk_ctx* ctx, const void* in, pk_dtype in_type
                             const float* psf_b, const int64_t psf_b_dims[3], int32_t numit,
                             const pk_decon_params* params, void* out);
 
+/* debug = true form of the two calls: decon_lucy_omw_function.m:114-144 (method 1) and
+ * decon_lucy_function.m:144-175 (method 0).  Besides `out` (as above) it fills err_mat (column-major,
+ * *err_rows x 4 doubles, room for numit x 4): [k, mean((J - I).^2), that / its first value, the
+ * reference's stopping measure over every save_step-th iteration], trimmed as the reference trims it
+ * (OMW: floor(numit / save_step) rows; RL: the last step index, and RL with numit < 3 * save_step is
+ * refused as the reference's trim has no step index then).  If `snapshots` is not NULL, every
+ * save_step-th iteration's uint16(J) (full [ny nx nz] volume, before post-processing) is written to
+ * it, floor(numit / save_step) volumes one after another -- the reference writes these as
+ * Iter_%04d.tif; the caller writes the files. */
+PK_API pk_status pk_decon_debug(pk_ctx* ctx, int32_t method, const void* in, pk_dtype in_type, const int64_t dims[3],
+                                const float* psf_f, const int64_t psf_f_dims[3],
+                                const float* psf_b, const int64_t psf_b_dims[3], int32_t numit,
+                                const pk_decon_params* params, int32_t save_step, void* out, double* err_mat,
+                                int32_t* err_rows, uint16_t* snapshots);
+
 /* Device-pointer forms of the two calls (the gateway's mxGPUArray path): `in`/`out` are device
  * pointers, the work is queued on `stream` (a cudaStream_t, NULL = the context's stream) and the
  * call returns without synchronising. */

@@ -201,7 +201,7 @@ def postprocess(J, I, I_mask, damp=1.0, scale=1.0, offset=0.0, edge_erosion=0, s
 
 # ---------------------------------------------------------------- the iterations
 def decon_lucy_omw(I, psf_f, psf_b, numit, background=None, save16bit=True, damp=1.0, scale=1.0,
-                   offset=0.0, edge_erosion=0, bbox=None, dtype=np.float32, return_float=False):
+                   offset=0.0, edge_erosion=0, bbox=None, dtype=np.float32, return_float=False, iterates=None):
     """decon_lucy_omw_function.m:1-177 (GPU branch input handling, 2-iteration regime)."""
     need_mask = offset != 0 or edge_erosion > 0
     Ipre, I_mask = preprocess(I, background, need_mask, dtype)
@@ -215,13 +215,15 @@ def decon_lucy_omw(I, psf_f, psf_b, numit, background=None, save16bit=True, damp
         CX = np.fmax(CX, eps)
         J = conv_half(Ipre / CX, otf_b) * J
         J = np.fmax(J, dtype(0))
+        if iterates is not None:                               # the debug branch's J (:114)
+            iterates.append(J.copy())
     if return_float:
         return J
     return postprocess(J, Ipre, I_mask, damp, scale, offset, edge_erosion, save16bit, bbox)
 
 
 def decon_lucy(I, psf, numit, background=None, save16bit=True, damp=1.0, scale=1.0, offset=0.0,
-               edge_erosion=0, bbox=None, dtype=np.float32, return_float=False, lambdas=None):
+               edge_erosion=0, bbox=None, dtype=np.float32, return_float=False, lambdas=None, iterates=None):
     """decon_lucy_function.m:1-213: Biggs-Andrews accelerated RL ('simplified')."""
     need_mask = offset != 0 or edge_erosion > 0
     Ipre, I_mask = preprocess(I, background, need_mask, dtype)
@@ -250,9 +252,47 @@ def decon_lucy(I, psf, numit, background=None, save16bit=True, damp=1.0, scale=1
         J2 = np.fmax(Y * conv_half(RB, Hc), dtype(0))           # :142
         if lambdas is not None:
             lambdas.append(lam)
+        if iterates is not None:                               # the debug branch's J_2 (:144)
+            iterates.append(J2.copy())
     if return_float:
         return J2
     return postprocess(J2, Ipre, I_mask, damp, scale, offset, edge_erosion, save16bit, bbox)
+
+
+def err_mat_from_mse(mse, estep, method):
+    """err_mat of the debug branch from the per-iteration mean((J - I).^2): decon_lucy_omw_function.m
+    :115-127 with the trim at :142-144, decon_lucy_function.m:145-157 with the trim at :173-175.  The
+    reference indexes rows by the step index istp (not by k) in the stopping measure, and RL's trim
+    uses the last istp (an error in MATLAB when none was set); both are kept."""
+    numit = len(mse)
+    e = np.zeros((numit + 1, 4))                               # 1-based rows as in MATLAB
+    istp = None
+    for k in range(1, numit + 1):
+        e[k, 0] = k
+        e[k, 1] = mse[k - 1]
+        e[k, 2] = e[k, 1] / e[1, 1]
+        if k % estep == 0 and k > estep * 2:
+            istp = k // estep
+            e[k, 3] = min(abs(e[istp, 2] - e[istp - 1, 2]) / 10,
+                          abs(e[istp, 2] + e[istp - 2, 2] - 2 * e[istp - 1, 2]) / 2)
+        elif k < 3 * estep:
+            e[k, 3] = 1
+        else:
+            e[k, 3] = e[istp * estep, 3]
+    if method == "omw":
+        rows = numit // estep
+    else:
+        if istp is None:
+            raise ValueError("istp undefined: NUMIT < 3*saveStep (decon_lucy_function.m:174)")
+        rows = istp
+    return e[1:rows + 1]
+
+
+def debug_err_mat(iterates, Ipre, estep, method):
+    """err_mat of a debug run from its iterates (mean in float64 of the float64 difference, :115)."""
+    I64 = np.asarray(Ipre, np.float64)
+    mse = [float(np.mean((np.asarray(J, np.float64) - I64) ** 2)) for J in iterates]
+    return err_mat_from_mse(mse, estep, method)
 
 
 def rel_l2(a, b):

@@ -267,6 +267,98 @@ static pk_status decon_host(pk_ctx* ctx, int method, const void* in, pk_dtype in
     return PK_OK;
 }
 
+// err_mat of the reference's debug branch from the per-iteration MSEs (1-based rows as in MATLAB;
+// decon_lucy_omw_function.m:113-127 and decon_lucy_function.m:144-158, including their use of the
+// step index istp as a row index).  Returns the number of rows kept, or -1 where the reference's
+// trim would fail (RL without any step index).
+static int err_mat_rows(int method, int numit, int estep, const std::vector<double>& mse, std::vector<double>& e) {
+    e.assign((size_t)(numit + 1) * 4, 0.0);   // e[k * 4 + c], k = 1..numit, c = 0..3
+    auto E = [&](int k, int c) -> double& { return e[(size_t)k * 4 + c]; };
+    int istp = -1;
+    for (int k = 1; k <= numit; k++) {
+        E(k, 0) = k;
+        E(k, 1) = mse[k - 1];
+        E(k, 2) = E(k, 1) / E(1, 1);
+        if (k % estep == 0 && k > estep * 2) {
+            istp = k / estep;
+            E(k, 3) = std::min(std::fabs(E(istp, 2) - E(istp - 1, 2)) / 10,
+                               std::fabs(E(istp, 2) + E(istp - 2, 2) - 2 * E(istp - 1, 2)) / 2);
+        } else if (k < 3 * estep) {
+            E(k, 3) = 1;
+        } else {
+            E(k, 3) = E(istp * estep, 3);
+        }
+    }
+    if (method == 1) return numit / estep;
+    return istp;
+}
+
+pk_status pk_decon_debug(pk_ctx* ctx, int32_t method, const void* in, pk_dtype in_type, const int64_t dims[3],
+                         const float* psf_f, const int64_t psf_f_dims[3], const float* psf_b,
+                         const int64_t psf_b_dims[3], int32_t numit, const pk_decon_params* params,
+                         int32_t save_step, void* out, double* err_mat, int32_t* err_rows, uint16_t* snapshots) {
+    pk_status s;
+    if ((s = check_ctx(ctx)) != PK_OK) return s;
+    if ((s = check_dims(dims, "input volume")) != PK_OK) return s;
+    if ((s = check_psf(psf_f, psf_f_dims, "PSF")) != PK_OK) return s;
+    if (method != 0 && method != 1) return pk_fail(PK_ERR_INVALID, "method must be 0 (RL) or 1 (OMW)");
+    if (method == 1 && (s = check_psf(psf_b, psf_b_dims, "PSF_b")) != PK_OK) return s;
+    if (!in || !out || !err_mat || !err_rows) return pk_fail(PK_ERR_INVALID, "NULL buffer");
+    if (in_type != PK_U16 && in_type != PK_F32 && in_type != PK_F64) return pk_fail(PK_ERR_INVALID, "bad input dtype");
+    if (numit < 1) return pk_fail(PK_ERR_INVALID, "a debug run needs NUMIT >= 1");
+    if (save_step < 1) return pk_fail(PK_ERR_INVALID, "saveStep must be >= 1");
+    if (method == 0 && numit < 3 * save_step)
+        return pk_fail(PK_ERR_INVALID, "debug with NUMIT < 3*saveStep: the reference's err_mat trim has no step "
+                                       "index then (decon_lucy_function.m:173-175)");
+    pk_decon_params def;
+    if (!params) {
+        pk_params_default(&def);
+        params = &def;
+    }
+    std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+    DeviceGuard g(ctx->device);
+    const size_t N = (size_t)dims[0] * dims[1] * dims[2];
+    int64_t od[3];
+    pk_output_dims(dims, params, od);
+    const size_t outb = (size_t)od[0] * od[1] * od[2] * (params->save16bit ? 2 : 4);
+    void *d_in, *d_out, *d_err, *d_snap = nullptr;
+    if ((s = pk_scratch(ctx, 9, N * dtype_size(in_type), &d_in)) != PK_OK) return s;
+    if ((s = pk_scratch(ctx, 10, outb, &d_out)) != PK_OK) return s;
+    constexpr int kSq = 64;   // partial blocks of the error sum
+    if ((s = pk_scratch(ctx, 15, sizeof(double) * ((size_t)numit + kSq), &d_err)) != PK_OK) return s;
+    if (snapshots && (s = pk_scratch(ctx, 16, sizeof(uint16_t) * N, &d_snap)) != PK_OK) return s;
+    cudaStream_t st = ctx->stream;
+    PK_CUDA(cudaMemcpyAsync(d_in, in, N * dtype_size(in_type), cudaMemcpyHostToDevice, st));
+    DebugHook hook;
+    hook.after_iter = [&](int k, const float* J, const float* I) -> pk_status {
+        pk_status r;
+        if ((r = pk_debug_error(J, I, (long long)N, (double*)d_err + numit, kSq, (double*)d_err + (k - 1), st)) != PK_OK)
+            return r;
+        if (snapshots && k % save_step == 0) {
+            if ((r = pk_debug_u16(J, (long long)N, (uint16_t*)d_snap, st)) != PK_OK) return r;
+            PK_CUDA(cudaMemcpyAsync(snapshots + (size_t)(k / save_step - 1) * N, d_snap, sizeof(uint16_t) * N,
+                                    cudaMemcpyDeviceToHost, st));
+        }
+        return PK_OK;
+    };
+    s = pk_decon_run(ctx, method, d_in, in_type, dims, psf_f, psf_f_dims, psf_b, psf_b_dims, numit, params, d_out,
+                     st, nullptr, &hook);
+    if (s != PK_OK) {
+        cudaStreamSynchronize(st);
+        return s;
+    }
+    std::vector<double> mse(numit);
+    PK_CUDA(cudaMemcpyAsync(out, d_out, outb, cudaMemcpyDeviceToHost, st));
+    PK_CUDA(cudaMemcpyAsync(mse.data(), d_err, sizeof(double) * numit, cudaMemcpyDeviceToHost, st));
+    PK_CUDA(cudaStreamSynchronize(st));
+    std::vector<double> e;
+    const int rows = err_mat_rows(method, numit, save_step, mse, e);
+    for (int c = 0; c < 4; c++)
+        for (int r = 0; r < rows; r++) err_mat[(size_t)c * rows + r] = e[(size_t)(r + 1) * 4 + c];
+    *err_rows = rows;
+    return PK_OK;
+}
+
 pk_status pk_decon_lucy(pk_ctx* ctx, const void* in, pk_dtype in_type, const int64_t dims[3], const float* psf,
                         const int64_t psf_dims[3], int32_t numit, const pk_decon_params* params, void* out,
                         int32_t* iters_run) {

@@ -60,15 +60,16 @@ __global__ void k_psf_scatter(const float* __restrict__ psf, int py, int px, int
     }
 }
 
-// numit == 0: J = I, post-processing only.
-__global__ void k_post_identity(VolDesc d) {
+// Post-processing of a materialised estimate `src` into the output (numit == 0: src = I; debug
+// runs: the last iteration's J).
+__global__ void k_post_from(VolDesc d, const float* __restrict__ src) {
     const long long n = d.nrows * d.ny;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         const long long row = i / d.ny;
         const int y = (int)(i - row * d.ny);
         const int x = (int)(row % d.nx), z = (int)(row / d.nx);
         if (y < d.bb0[0] || y > d.bb1[0] || x < d.bb0[1] || x > d.bb1[1] || z < d.bb0[2] || z > d.bb1[2]) continue;
-        float J = d.I[i];
+        float J = src[i];
         if (d.damp > 1.f) {
             const float dI = __fmul_rn(d.damp, d.I[i]);
             J = __fadd_rn((J <= dI) ? J : 0.f, fminf(J, (J >= dI) ? dI : 0.f));
@@ -93,6 +94,43 @@ __global__ void k_post_identity(VolDesc d) {
         } else {
             ((float*)d.out)[oi] = J;
         }
+    }
+}
+
+// ---- debug runs: per-iteration float64 MSE of J against I and uint16 snapshots of J
+constexpr int kSqBlocks = 64;
+__global__ void k_sqdiff_part(const float* __restrict__ J, const float* __restrict__ I, long long n, double* part) {
+    __shared__ double s[256];
+    const long long per = (n + gridDim.x - 1) / gridDim.x;
+    const long long b0 = per * blockIdx.x, b1 = min(n, b0 + per);
+    double a = 0.0;
+    for (long long i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
+        const double d = (double)J[i] - (double)I[i];
+        a += d * d;
+    }
+    s[threadIdx.x] = a;
+    __syncthreads();
+    for (int k = 128; k > 0; k >>= 1) {
+        if ((int)threadIdx.x < k) s[threadIdx.x] += s[threadIdx.x + k];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = s[0];
+}
+
+__global__ void k_sqdiff_final(const double* __restrict__ part, int nb, long long n, double* out) {
+    if (threadIdx.x == 0) {
+        double a = 0.0;
+        for (int b = 0; b < nb; b++) a += part[b];
+        *out = a / (double)n;
+    }
+}
+
+__global__ void k_to_u16(const float* __restrict__ J, long long n, uint16_t* __restrict__ o) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        float r = roundf(J[i]);             // MATLAB uint16(): half away from zero, saturate, NaN -> 0
+        if (!(r >= 0.f)) r = 0.f;
+        if (r > 65535.f) r = 65535.f;
+        o[i] = (uint16_t)r;
     }
 }
 
@@ -169,6 +207,19 @@ int grid_for(long long n) {
 }
 
 }  // namespace
+
+pk_status pk_debug_error(const float* J, const float* I, long long n, double* part, int nb, double* out, cudaStream_t st) {
+    k_sqdiff_part<<<nb, 256, 0, st>>>(J, I, n, part);
+    k_sqdiff_final<<<1, 32, 0, st>>>(part, nb, n, out);
+    PK_CUDA(cudaGetLastError());
+    return PK_OK;
+}
+
+pk_status pk_debug_u16(const float* J, long long n, uint16_t* o, cudaStream_t st) {
+    k_to_u16<<<grid_for(n), 256, 0, st>>>(J, n, o);
+    PK_CUDA(cudaGetLastError());
+    return PK_OK;
+}
 
 // strel('disk', R) neighbourhood (default N = 4 approximation), as (dy, dx) offsets.
 std::vector<int2> pk_disk_offsets(int R) {
@@ -419,11 +470,12 @@ static pk_status get_io_event(pk_ctx* ctx, size_t i, cudaEvent_t* e) {
 }
 
 pk_status pk_decon_multi(pk_ctx* ctx, int method, std::vector<DeconJob>& jobs, pk_dtype in_type, int numit,
-                         const pk_decon_params* p, cudaStream_t st, HostStreamIO* io) {
+                         const pk_decon_params* p, cudaStream_t st, HostStreamIO* io, const DebugHook* dbg) {
     pk_status s;
     if (numit < 0) return pk_fail(PK_ERR_INVALID, "NUMIT must be non-negative");
     const size_t nj = jobs.size();
     if (nj == 0) return PK_OK;
+    if (dbg && (nj != 1 || io)) return pk_fail(PK_ERR_INVALID, "debug runs take one volume on device buffers");
     const bool need_mask = p->decon_offset != 0.0 || p->edge_erosion > 0;
     // a single-volume call with host buffers streams its copies by z-slab when its first and last
     // passes work plane by plane on the raw layout (no padding, crop, erosion or scalar raw path)
@@ -517,7 +569,7 @@ pk_status pk_decon_multi(pk_ctx* ctx, int method, std::vector<DeconJob>& jobs, p
         for (size_t i = 0; i < nj; i++) {
             VolDesc f = base[i];
             set_post_job(f, p, mask_mode[i], jobs[i]);
-            k_post_identity<<<grid_for((long long)f.nrows * f.ny), 256, 0, st>>>(f);
+            k_post_from<<<grid_for((long long)f.nrows * f.ny), 256, 0, st>>>(f, f.I);
             PK_CUDA(cudaGetLastError());
         }
         return PK_OK;
@@ -538,17 +590,29 @@ pk_status pk_decon_multi(pk_ctx* ctx, int method, std::vector<DeconJob>& jobs, p
         }));
         pk_program_add(prog, PK_STEP_X, XZ_INV, base);
     };
+    // debug runs launch each iteration's program on its own, then the caller's per-iteration work
+    auto flush = [&]() -> pk_status {
+        if (prog.steps.empty()) return PK_OK;
+        pk_status r = pk_program_upload(ctx, prog, st);
+        if (r == PK_OK) r = pk_program_launch(ctx, prog, st);
+        prog = PkProgram();
+        return r;
+    };
     if (method == 1) {
         for (int it = 1; it <= numit; it++) {
             conv(0);
             pk_program_add(prog, PK_STEP_Y, Y_RATIO, base);
             conv(1);
-            const bool last = it == numit;
+            const bool last = it == numit && !dbg;
             pk_program_add(prog, PK_STEP_Y, last ? Y_FINAL : Y_UPDATE, with([&](VolDesc& d, DeconJob& j, int i) {
                 d.Jo = it == 1 ? j.I : j.J;
                 d.Jn = j.J;
                 if (last) set_post_job(d, p, mask_mode[i], j);
             }));
+            if (dbg) {
+                if ((s = flush()) != PK_OK) return s;
+                if ((s = dbg->after_iter(it, jobs[0].J, jobs[0].I)) != PK_OK) return s;
+            }
         }
     } else {
         for (int k = 1; k <= numit; k++) {
@@ -564,7 +628,7 @@ pk_status pk_decon_multi(pk_ctx* ctx, int method, std::vector<DeconJob>& jobs, p
             conv(0);
             pk_program_add(prog, PK_STEP_Y, Y_RATIO, base);
             conv(1);
-            if (k < numit) {
+            if (k < numit || dbg) {
                 auto u = with([&](VolDesc& d, DeconJob& j, int) {
                     float* Jb[2] = {j.J, j.JB};
                     d.Yb = k == 1 ? j.I : j.Yb;
@@ -574,6 +638,10 @@ pk_status pk_decon_multi(pk_ctx* ctx, int method, std::vector<DeconJob>& jobs, p
                 });
                 pk_program_add(prog, PK_STEP_Y, Y_RLUPD, u);
                 pk_program_add(prog, PK_STEP_LAMBDA, 0, u);
+                if (dbg) {
+                    if ((s = flush()) != PK_OK) return s;
+                    if ((s = dbg->after_iter(k, (k + 1) % 2 ? jobs[0].JB : jobs[0].J, jobs[0].I)) != PK_OK) return s;
+                }
             } else {
                 pk_program_add(prog, PK_STEP_Y, Y_RLFINAL, with([&](VolDesc& d, DeconJob& j, int i) {
                     d.Yb = k == 1 ? j.I : j.Yb;
@@ -581,6 +649,15 @@ pk_status pk_decon_multi(pk_ctx* ctx, int method, std::vector<DeconJob>& jobs, p
                 }));
             }
         }
+    }
+    if (dbg) {   // the last estimate is materialised: post-process it into the output
+        if ((s = flush()) != PK_OK) return s;
+        VolDesc f = base[0];
+        set_post_job(f, p, mask_mode[0], jobs[0]);
+        const float* Jlast = method == 1 ? jobs[0].J : ((numit + 1) % 2 ? jobs[0].JB : jobs[0].J);
+        k_post_from<<<grid_for((long long)f.nrows * f.ny), 256, 0, st>>>(f, Jlast);
+        PK_CUDA(cudaGetLastError());
+        return PK_OK;
     }
     // streamed host call: the first two passes (y pre-pass, x forward) and the last two (x inverse,
     // final y pass) run slab by slab behind the slab copies
@@ -659,7 +736,7 @@ pk_status pk_decon_multi(pk_ctx* ctx, int method, std::vector<DeconJob>& jobs, p
 pk_status pk_decon_run(pk_ctx* ctx, int method, const void* d_in, pk_dtype in_type, const int64_t dims[3],
                        const float* psf_f, const int64_t psf_f_dims[3], const float* psf_b,
                        const int64_t psf_b_dims[3], int numit, const pk_decon_params* p, void* d_out,
-                       cudaStream_t st, HostStreamIO* io) {
+                       cudaStream_t st, HostStreamIO* io, const DebugHook* dbg) {
     pk_status s;
     if ((s = pk_check_params(dims, p)) != PK_OK) return s;
     if (numit < 0) return pk_fail(PK_ERR_INVALID, "NUMIT must be non-negative");
@@ -679,5 +756,5 @@ pk_status pk_decon_run(pk_ctx* ctx, int method, const void* d_in, pk_dtype in_ty
     j.has_bbox = p->has_bbox;
     for (int i = 0; i < 6; i++) j.bbox[i] = p->bbox[i];
     std::vector<DeconJob> jobs{j};
-    return pk_decon_multi(ctx, method, jobs, in_type, numit, p, st, io);
+    return pk_decon_multi(ctx, method, jobs, in_type, numit, p, st, io, dbg);
 }

@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <functional>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -223,11 +224,21 @@ struct HostStreamIO {
     size_t in_esize = 0, out_esize = 0;
     bool active = false;   // set by pk_decon_multi when the call could be streamed
 };
+// Debug run of one volume (decon_lucy_omw_function.m:114-144, decon_lucy_function.m:144-175): the
+// last iteration also writes J, and after the launches of iteration k, after_iter(k, J) queues the
+// caller's per-iteration work (error measure, snapshot) on the stream.
+struct DebugHook {
+    std::function<pk_status(int k, const float* J, const float* I)> after_iter;
+};
+// debug-run helpers (decon.cu): mean((J - I).^2) in float64 (fixed order) into *out, uint16(J) into o
+pk_status pk_debug_error(const float* J, const float* I, long long n, double* part, int nb, double* out, cudaStream_t st);
+pk_status pk_debug_u16(const float* J, long long n, uint16_t* o, cudaStream_t st);
 pk_status pk_decon_multi(pk_ctx* ctx, int method, std::vector<DeconJob>& jobs, pk_dtype in_type, int numit,
-                         const pk_decon_params* p, cudaStream_t st, HostStreamIO* io = nullptr);
+                         const pk_decon_params* p, cudaStream_t st, HostStreamIO* io = nullptr,
+                         const DebugHook* dbg = nullptr);
 pk_status pk_check_params(const int64_t dims[3], const pk_decon_params* p);
 
 pk_status pk_decon_run(pk_ctx* ctx, int method, const void* d_in, pk_dtype in_type, const int64_t dims[3],
                        const float* psf_f, const int64_t psf_f_dims[3], const float* psf_b,
                        const int64_t psf_b_dims[3], int numit, const pk_decon_params* p, void* d_out,
-                       cudaStream_t st, HostStreamIO* io = nullptr);
+                       cudaStream_t st, HostStreamIO* io = nullptr, const DebugHook* dbg = nullptr);

@@ -28,8 +28,6 @@ def _parse(kw):
         opts[key] = v
     if not opts["usegpu"]:
         raise ValueError("useGPU=false: this implementation runs on the GPU only (no CPU path)")
-    if opts["debug"]:
-        raise NotImplementedError("debug=true (err_mat and intermediate TIFFs) is not supported")
     return opts, ctx
 
 
@@ -85,6 +83,30 @@ def _out(dims, p):
     return np.empty(shape, dtype=np.uint16 if p.save16bit else np.float32, order="F")
 
 
+def _debug_run(method, vol, t, pf, pb, numit, p, opts, ctx, out):
+    """debug = true: err_mat from the library, uint16(J) of every saveStep-th iteration written to
+    debug_folder/Iter_%04d.tif (decon_lucy_omw_function.m:113-141, decon_lucy_function.m:144-171)."""
+    import os
+    from .tiff import write_tiff
+    estep = int(opts["savestep"])
+    numit = int(numit)
+    nsnap = numit // estep if estep >= 1 else 0
+    snaps = np.empty((max(nsnap, 1),) + vol.shape[::-1], np.uint16)      # C order of [nz nx ny] per volume
+    err = np.zeros((max(numit, 1), 4), np.float64)
+    rows = _lib.C.c_int32(0)
+    check(lib.pk_decon_debug(ctx.handle, int(method), ptr(vol), t, i64x3(vol.shape), ptr(pf), i64x3(pf.shape),
+                             ptr(pb) if pb is not None else None, i64x3(pb.shape if pb is not None else pf.shape),
+                             numit, p, estep, ptr(out), ptr(err), _lib.C.byref(rows),
+                             ptr(snaps) if nsnap > 0 else None))
+    n = int(rows.value)
+    err_mat = err.reshape(-1, order="C").view()[: 4 * n].reshape(4, n).T.copy()   # column-major n x 4
+    folder = opts["debug_folder"]
+    os.makedirs(folder, exist_ok=True)
+    for s in range(nsnap):
+        write_tiff(os.path.join(folder, f"Iter_{(s + 1) * estep:04d}.tif"), snaps[s].T)
+    return err_mat
+
+
 def decon_lucy_function(I, PSF, NUMIT, **kw):
     """[J_2, err_mat, k] = decon_lucy_function(I, PSF, NUMIT, ...) (Biggs-accelerated RL)."""
     opts, ctx = _parse(kw)
@@ -93,6 +115,9 @@ def decon_lucy_function(I, PSF, NUMIT, **kw):
     psf = _psf(PSF)
     p = _params(opts)
     out = _out(vol.shape, p)
+    if opts["debug"]:
+        err_mat = _debug_run(0, vol, t, psf, None, NUMIT, p, opts, ctx, out)
+        return _squeeze_like(out, I), err_mat, int(NUMIT)
     k = _lib.C.c_int32(0)
     check(lib.pk_decon_lucy(ctx.handle, ptr(vol), t, i64x3(vol.shape), ptr(psf), i64x3(psf.shape), int(NUMIT), p,
                             ptr(out), _lib.C.byref(k)))
@@ -108,6 +133,9 @@ def decon_lucy_omw_function(I, PSF_f, PSF_b, NUMIT, **kw):
     pb = _psf(PSF_b)
     p = _params(opts)
     out = _out(vol.shape, p)
+    if opts["debug"]:
+        err_mat = _debug_run(1, vol, t, pf, pb, NUMIT, p, opts, ctx, out)
+        return _squeeze_like(out, I), err_mat
     check(lib.pk_decon_lucy_omw(ctx.handle, ptr(vol), t, i64x3(vol.shape), ptr(pf), i64x3(pf.shape), ptr(pb),
                                 i64x3(pb.shape), int(NUMIT), p, ptr(out)))
     return _squeeze_like(out, I), np.zeros((int(NUMIT), 4))
