@@ -11,6 +11,7 @@
 // scaleFactor, deconOffset, EdgeErosion, bbox).  Errors are raised with mexErrMsgIdAndTxt using the
 // identifier "pkdecon:<status>" and pk_last_error() (the convention of crop3d_mex.c:36-63).
 #include <cstring>
+#include <vector>
 #include <string>
 
 #include "mex.h"
@@ -122,6 +123,41 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
                                 (int32_t)mxGetScalar(prhs[3]), &p, mxGetData(plhs[0]), &k));
             if (nlhs > 1) plhs[1] = mxCreateDoubleScalar(k);
         }
+        return;
+    }
+    if (!strcmp(cmd, "debug")) {
+        // [J, err_mat, snaps] = pkdecon_mex('debug', method, I, PSF_f, PSF_b, NUMIT, opts, saveStep)
+        // method 'omw' or 'rl' (PSF_b ignored); snaps = uint16 [ny nx nz nsnap], every saveStep-th J
+        if (nrhs < 8 || !mxIsChar(prhs[1])) mexErrMsgIdAndTxt("pkdecon:invalid", "debug: not enough arguments");
+        char m[8];
+        mxGetString(prhs[1], m, sizeof(m));
+        const int32_t method = !strcmp(m, "omw") ? 1 : 0;
+        const mxArray* I = prhs[2];
+        int64_t d[3], pf[3], pb[3], od[3];
+        dims3(I, d);
+        dims3(prhs[3], pf);
+        if (method == 1) dims3(prhs[4], pb);
+        else for (int i = 0; i < 3; i++) pb[i] = pf[i];
+        const int32_t numit = (int32_t)mxGetScalar(prhs[5]);
+        pk_decon_params p;
+        params(prhs[6], &p);
+        const int32_t step = (int32_t)mxGetScalar(prhs[7]);
+        pk_output_dims(d, &p, od);
+        plhs[0] = make_out(od, p.save16bit != 0);
+        const int32_t nsnap = step > 0 ? numit / step : 0;
+        const mwSize sd[4] = {(mwSize)d[0], (mwSize)d[1], (mwSize)d[2], (mwSize)(nsnap > 0 ? nsnap : 0)};
+        mxArray* snaps = mxCreateNumericArray(4, sd, mxUINT16_CLASS, mxREAL);
+        std::vector<double> err((size_t)(numit > 0 ? numit : 1) * 4);
+        int32_t rows = 0;
+        check(pk_decon_debug(ctx(), method, mxGetData(I), dtype_of(I), d, single_psf(prhs[3]), pf,
+                             method == 1 ? single_psf(prhs[4]) : nullptr, pb, numit, &p, step, mxGetData(plhs[0]),
+                             err.data(), &rows, nsnap > 0 ? (uint16_t*)mxGetData(snaps) : nullptr));
+        if (nlhs > 1) {
+            plhs[1] = mxCreateDoubleMatrix((mwSize)rows, 4, mxREAL);
+            memcpy(mxGetPr(plhs[1]), err.data(), sizeof(double) * (size_t)rows * 4);   // column-major rows x 4
+        }
+        if (nlhs > 2) plhs[2] = snaps;
+        else mxDestroyArray(snaps);
         return;
     }
     if (!strcmp(cmd, "omw_bp")) {
