@@ -167,6 +167,21 @@ PK_API pk_status pk_wb_backprojector(pk_ctx* ctx, const float* psf, const int64_
                               double beta, int32_t n, int32_t res_flag, const double ires[3],
                               double* psf_bp, double* otf_bp);
 
+/* ---------------------------------------------------------------- PSF preparation */
+/* psf = psf_gen_new(psf, dz_psf, dz_data, medFactor, PSFGenMethod)  (decon/psf_gen_new.m:1-140;
+ * called by RLdecon.m:247, RLdecon_large_in_memory.m:107, RLdecon_large_in_place.m:127 and
+ * XR_decon_data_wrapper.m:279 for every measured PSF).  psf: float32 [ny nx nz] column-major
+ * (nz == 1: a 2D PSF).  method: 0 = 'masked' (the reference default), 1 = 'median'.
+ * The output size depends on the PSF (z padding, axial resampling), so out_dims always receives it;
+ * with out == NULL nothing else is written, otherwise out (host, out_capacity floats) receives the
+ * PSF in float32.  ny * nx * (2 * nz + 8) floats always suffice (the two z paddings add at most
+ * nz + 7 slices), so one call with a buffer of that size is enough.  Errors: PK_ERR_INVALID where MATLAB would raise an indexing error (fewer than 5
+ * slices or 10 rows, an all-zero result), PK_ERR_UNSUPPORTED for the 2D 'median' method (its call
+ * to the undefined `medfilt`) and for 2D border rows with negative values (complex in MATLAB). */
+PK_API pk_status pk_psf_gen(pk_ctx* ctx, const float* psf, const int64_t dims[3], double dz_psf, double dz_data,
+                            double med_factor, int32_t method, float* out, int64_t out_capacity,
+                            int64_t out_dims[3]);
+
 /* ---------------------------------------------------------------- chunking helpers (host) */
 /* findGoodFactorNumber(n, direction, allowOddSeven)  -- utils/findGoodFactorNumber.m:1-26. */
 PK_API int64_t pk_find_good_factor_number(int64_t n, int32_t direction, int32_t allow_odd_seven);

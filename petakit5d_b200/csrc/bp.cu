@@ -4,9 +4,9 @@
 //
 // Device work: float64 PSF normalisation sum, float64 direct DFTs along each axis (any length),
 // |OTF|, the descending sort + sequential float64 cumulative sum of the OTF threshold search,
-// the K=2 nearest-edge search of the star distance, the Wiener / window products.  Host work
-// (a few hundred thousand voxels, once per PSF): binary morphology, connected components, the
-// per-slice convex hulls and the mask edge.
+// the K=2 nearest-edge search of the star distance, the Wiener / window products, and the binary
+// openings / closings / erosion of the OTF mask (psfvol.cu).  Host work (a few hundred thousand
+// voxels, once per PSF): connected components, the per-slice convex hulls and the mask edge list.
 #include <cub/device/device_radix_sort.cuh>
 
 #include <algorithm>
@@ -160,31 +160,13 @@ struct Dims {
     long long at(int y, int x, int z) const { return y + (long long)ny * (x + (long long)nx * z); }
 };
 
-std::vector<double2> twiddles(int n, int sign) {
-    std::vector<double2> t(n);
-    for (int m = 0; m < n; m++) {
-        double c, s;
-        if ((4LL * m) % n == 0) {
-            const int q = (int)((4LL * m) / n) & 3;
-            c = q == 0 ? 1 : q == 2 ? -1 : 0;
-            s = q == 1 ? 1 : q == 3 ? -1 : 0;
-        } else {
-            const double a = 2.0 * M_PI * (double)m / (double)n;
-            c = std::cos(a);
-            s = std::sin(a);
-        }
-        t[m] = make_double2(c, sign * s);
-    }
-    return t;
-}
-
 // 3D DFT in place (through a ping-pong buffer) on the device; sign -1 forward, +1 inverse (unnormalised)
 pk_status dft3(const Dims& D, double2* a, double2* tmp, int sign, cudaStream_t st) {
     const int ns[3] = {D.ny, D.nx, D.nz};
     double2* src = a;
     double2* dst = tmp;
     for (int ax = 0; ax < 3; ax++) {
-        std::vector<double2> tw = twiddles(ns[ax], sign);
+        std::vector<double2> tw = pk_twiddles64(ns[ax], sign);
         double2* dtw;
         PK_CUDA(cudaMallocAsync(&dtw, sizeof(double2) * tw.size(), st));
         PK_CUDA(cudaMemcpyAsync(dtw, tw.data(), sizeof(double2) * tw.size(), cudaMemcpyHostToDevice, st));
@@ -216,69 +198,9 @@ std::vector<T> shift3(const std::vector<T>& a, const Dims& D, bool inverse) {
     return o;
 }
 
-// ---- binary morphology (conventions of the MATLAB calls at omw_backprojector_generation.m:44-48,122)
-std::vector<int> sphere_offsets(int r, const Dims& D, std::vector<std::array<int, 3>>* out3) {
-    std::vector<int> o;
-    for (int a = -r; a <= r; a++)
-        for (int b = -r; b <= r; b++)
-            for (int c = -r; c <= r; c++)
-                if (a * a + b * b + c * c <= r * r) out3->push_back({a, b, c});
-    return o;
-}
-
-std::vector<uint8_t> morph(const std::vector<uint8_t>& m, const Dims& D, int r, bool erode) {
-    std::vector<std::array<int, 3>> offs;
-    sphere_offsets(r, D, &offs);
-    std::vector<uint8_t> o(m.size());
-    for (int z = 0; z < D.nz; z++)
-        for (int x = 0; x < D.nx; x++)
-            for (int y = 0; y < D.ny; y++) {
-                bool v = erode;
-                for (auto& f : offs) {
-                    const int yy = y + f[0], xx = x + f[1], zz = z + f[2];
-                    bool s;
-                    if (yy < 0 || yy >= D.ny || xx < 0 || xx >= D.nx || zz < 0 || zz >= D.nz) s = erode;  // erosion pads true
-                    else s = m[D.at(yy, xx, zz)] != 0;
-                    if (erode) { if (!s) { v = false; break; } }
-                    else if (s) { v = true; break; }
-                }
-                o[D.at(y, x, z)] = v;
-            }
-    return o;
-}
-
 // 26-connected components numbered by their first voxel in column-major order (1..n)
 int label26(const std::vector<uint8_t>& m, const Dims& D, std::vector<int>& lab, std::vector<long long>& sizes) {
-    lab.assign(m.size(), 0);
-    sizes.assign(1, 0);
-    int n = 0;
-    std::vector<long long> stack;
-    for (long long i = 0; i < D.n(); i++) {
-        if (!m[i] || lab[i]) continue;
-        n++;
-        long long cnt = 0;
-        lab[i] = n;
-        stack.push_back(i);
-        while (!stack.empty()) {
-            const long long v = stack.back();
-            stack.pop_back();
-            cnt++;
-            const int y = (int)(v % D.ny), x = (int)((v / D.ny) % D.nx), z = (int)(v / ((long long)D.ny * D.nx));
-            for (int c = -1; c <= 1; c++)
-                for (int b = -1; b <= 1; b++)
-                    for (int a = -1; a <= 1; a++) {
-                        const int yy = y + a, xx = x + b, zz = z + c;
-                        if (yy < 0 || yy >= D.ny || xx < 0 || xx >= D.nx || zz < 0 || zz >= D.nz) continue;
-                        const long long w = D.at(yy, xx, zz);
-                        if (m[w] && !lab[w]) {
-                            lab[w] = n;
-                            stack.push_back(w);
-                        }
-                    }
-        }
-        sizes.push_back(cnt);
-    }
-    return n;
+    return pk_label26(m.data(), D.ny, D.nx, D.nz, lab, sizes);
 }
 
 std::vector<uint8_t> bwareaopen(const std::vector<uint8_t>& m, const Dims& D, double P) {
@@ -361,15 +283,16 @@ void convhull_fill(std::vector<uint8_t>& img, int h, int w) {
 
 // Threshold .. convex hulls of omw_backprojector_generation.m:43-109 on the host.
 pk_status omw_mask_host(const std::vector<float>& abs_c, const Dims& D0, float abs0, double dc, int skewed_in,
-                        double area, std::vector<uint8_t>& mask, Dims& D, int& skewed) {
+                        double area, std::vector<uint8_t>& mask, Dims& D, int& skewed, cudaStream_t st) {
     D = D0;
     const float thr = abs0 * (float)dc;
     mask.assign(D.n(), 0);
     for (long long i = 0; i < D.n(); i++) mask[i] = abs_c[i] > thr;
-    mask = morph(morph(mask, D, 2, true), D, 2, false);    // imopen
+    const std::vector<int4> ball2 = pk_ball_offsets(2);
+    pk_status s;
+    if ((s = pk_morph_host(mask, D.ny, D.nx, D.nz, ball2, "ed", st)) != PK_OK) return s;     // imopen (GPU)
     mask = bwareaopen(mask, D, area);
-    mask = morph(morph(mask, D, 2, false), D, 2, true);    // imclose
-    mask = morph(morph(mask, D, 2, true), D, 2, false);    // imopen
+    if ((s = pk_morph_host(mask, D.ny, D.nx, D.nz, ball2, "deed", st)) != PK_OK) return s;   // imclose, imopen
     mask = bwareaopen(mask, D, area);
     if (std::find(mask.begin(), mask.end(), 1) == mask.end())
         return pk_fail(PK_ERR_EMPTY_OTF_MASK, "The OTF mask is empty, check the PSF and OTF-related parameters!");
@@ -524,9 +447,10 @@ pk_status pk_omw_backprojector(pk_ctx* ctx, const float* psf, const int64_t psf_
     std::vector<uint8_t> mask;
     Dims D;
     int sk = 0;
-    if ((s = omw_mask_host(abs_c, D0, absO[0], thr[0], skewed, otf_area_thresh, mask, D, sk)) != PK_OK) return s;
+    if ((s = omw_mask_host(abs_c, D0, absO[0], thr[0], skewed, otf_area_thresh, mask, D, sk, st)) != PK_OK) return s;
     // edge = mask & ~imerode(mask, sphere(1)) (:122) and the star geometry (:123-133)
-    const std::vector<uint8_t> er = morph(mask, D, 1, true);
+    std::vector<uint8_t> er = mask;
+    if ((s = pk_morph_host(er, D.ny, D.nx, D.nz, pk_ball_offsets(1), "e", st)) != PK_OK) return s;
     const long long nq = D.n();
     std::vector<double3> Q(nq), E;
     std::vector<double> rs(nq), Rn;

@@ -195,6 +195,18 @@ int pk_program_kernel_count(const PkProgram& prog);
 // scratch buffers
 pk_status pk_scratch(pk_ctx* ctx, int slot, size_t bytes, void** ptr);
 
+// PSF-size volume helpers (psfvol.cu, decon.cu)
+std::vector<int4> pk_ball_offsets(int r);           // strel('sphere', r): (dy, dx, dz, 0), dy^2+dx^2+dz^2 <= r^2
+std::vector<int2> pk_disk_offsets(int R);           // strel('disk', R): (dy, dx)
+// binary morphology on the GPU: ops is a string of 'd' (dilate) / 'e' (erode) applied in order;
+// d_a holds the mask in and out, d_tmp is a mask-sized work buffer
+pk_status pk_morph_ops(uint8_t* d_a, uint8_t* d_tmp, int ny, int nx, int nz, const int4* d_offs, int noff,
+                       const char* ops, cudaStream_t st);
+pk_status pk_morph_host(std::vector<uint8_t>& mask, int ny, int nx, int nz, const std::vector<int4>& offs,
+                        const char* ops, cudaStream_t st);
+int pk_label26(const uint8_t* m, int ny, int nx, int nz, std::vector<int>& lab, std::vector<long long>& sizes);
+std::vector<double2> pk_twiddles64(int n, int sign);   // exp(sign 2 pi i m / n), m < n
+
 // decon drivers (decon.cu)
 pk_status pk_get_otf(pk_ctx* ctx, const float* h_psf, const int64_t psf_dims[3], int ny, int nx, int nz,
                      const float2** d_otf, cudaStream_t st);

@@ -6,6 +6,7 @@
 //   [J, k]   = pkdecon_mex('rl', I, PSF, NUMIT, opts)             % decon_lucy_function
 //   [b, otf, absc, mask] = pkdecon_mex('omw_bp', psf, alpha, skewed, thresh, area, hann, minInt)
 //   [bp, otf] = pkdecon_mex('wb_bp', psf, alpha, beta, n, resFlag, iRes)
+//   psf      = pkdecon_mex('psf_gen', psf, dz_psf, dz_data, medFactor, PSFGenMethod)  % psf_gen_new
 //   pkdecon_mex('reset')                                           % reset(gpuDevice) analogue
 // opts: struct with the reference's name/value fields (Background, save16bit, dampFactor,
 // scaleFactor, deconOffset, EdgeErosion, bbox).  Errors are raised with mexErrMsgIdAndTxt using the
@@ -193,6 +194,24 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
                                   (int32_t)mxGetScalar(prhs[4]), (int32_t)mxGetScalar(prhs[5]), ires,
                                   mxGetPr(plhs[0]), (double*)mxGetComplexDoubles(otf)));
         if (nlhs > 1) plhs[1] = otf; else mxDestroyArray(otf);
+        return;
+    }
+    if (!strcmp(cmd, "psf_gen")) {
+        if (nrhs < 6 || !mxIsChar(prhs[5])) mexErrMsgIdAndTxt("pkdecon:invalid", "psf_gen: psf, dz_psf, dz_data, medFactor, PSFGenMethod");
+        int64_t pd[3], od[3];
+        dims3(prhs[1], pd);
+        char m[16];
+        mxGetString(prhs[5], m, sizeof(m));
+        int32_t method;
+        if (!strcmp(m, "masked")) method = 0;
+        else if (!strcmp(m, "median")) method = 1;
+        else mexErrMsgIdAndTxt("pkdecon:invalid", "PSFGenMethod must be 'masked' or 'median'");
+        const float* psf = single_psf(prhs[1]);
+        const double dzp = mxGetScalar(prhs[2]), dzd = mxGetScalar(prhs[3]), mf = mxGetScalar(prhs[4]);
+        check(pk_psf_gen(ctx(), psf, pd, dzp, dzd, mf, method, nullptr, 0, od));
+        const mwSize dd[3] = {(mwSize)od[0], (mwSize)od[1], (mwSize)od[2]};
+        plhs[0] = mxCreateNumericArray(3, dd, mxSINGLE_CLASS, mxREAL);
+        check(pk_psf_gen(ctx(), psf, pd, dzp, dzd, mf, method, (float*)mxGetData(plhs[0]), (int64_t)(od[0] * od[1] * od[2]), od));
         return;
     }
     mexErrMsgIdAndTxt("pkdecon:invalid", "unknown command '%s'", cmd);

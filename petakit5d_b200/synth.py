@@ -13,13 +13,15 @@ Workloads (sizes are x, y, z):
   * ``lobed_psf``            -- Gaussian PSF plus two side lobes at +-dz along z.
   * ``sinusoid_background``  -- smooth 3D sinusoid background (period, amplitude, offset).
   * ``chunk_workload``       -- uneven chunks with overlap borders and per-chunk PSF ids.
+  * ``measured_psf``         -- a bead image as a microscope records it (camera offset, read noise,
+                                hot pixels, peak anywhere): the input of psf_gen_new.
 """
 from __future__ import annotations
 
 import numpy as np
 
 __all__ = ["gaussian_psf", "lobed_psf", "puncta_volume", "sinusoid_background", "chunk_workload",
-           "single_volume_workload", "LLSM_PSF", "SMALL_PSF"]
+           "single_volume_workload", "measured_psf", "LLSM_PSF", "SMALL_PSF"]
 
 
 def _rng(seed):
@@ -43,6 +45,23 @@ def gaussian_psf(size_yxz=(31, 31, 41), sigma_xy=1.3, sigma_z=3.0, lobes=(), lob
 
 def lobed_psf(size_yxz=(64, 64, 101), sigma_xy=1.5, sigma_z=4.0, lobe_dz=12, lobe_amp=0.15):
     return gaussian_psf(size_yxz, sigma_xy, sigma_z, lobes=(-lobe_dz, lobe_dz), lobe_amp=lobe_amp)
+
+
+def measured_psf(size_yxz=(64, 64, 101), peak=None, sigma_xy=1.5, sigma_z=4.0, amplitude=5000.0, offset=100.0,
+                 read_noise=3.0, hot_pixels=6, seed=0):
+    """Bead image: offset + amplitude * Gaussian(peak) + Gaussian read noise + isolated hot pixels,
+    float32 in Fortran order.  ``peak`` is 0-based (y, x, z); default the array centre."""
+    ny, nx, nz = size_yxz
+    rng = _rng(seed)
+    py, px, pz = peak if peak is not None else (ny // 2, nx // 2, nz // 2)
+    y = (np.arange(ny) - py)[:, None, None].astype(np.float64)
+    x = (np.arange(nx) - px)[None, :, None].astype(np.float64)
+    z = (np.arange(nz) - pz)[None, None, :].astype(np.float64)
+    img = offset + amplitude * np.exp(-(y * y + x * x) / (2 * sigma_xy ** 2) - (z * z) / (2 * sigma_z ** 2))
+    img = img + rng.normal(0.0, read_noise, size=(ny, nx, nz))
+    for _ in range(hot_pixels):
+        img[rng.integers(ny), rng.integers(nx), rng.integers(nz)] += amplitude * 0.2
+    return np.asfortranarray(img.astype(np.float32))
 
 
 SMALL_PSF = dict(size_yxz=(31, 31, 41), sigma_xy=1.3, sigma_z=3.0)
