@@ -315,7 +315,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="omw_llsm", choices=["omw_llsm", "rl_small", "batched", "served", "large"])
+    ap.add_argument("--workload", default="omw_llsm",
+                    choices=["omw_llsm", "rl_small", "batched", "served", "large", "dsr"])
     ap.add_argument("--rate", type=float, default=200.0, help="served: Poisson arrival rate (requests/s)")
     ap.add_argument("--requests", type=int, default=240, help="served: number of requests")
     ap.add_argument("--ncu-case", action="store_true",
@@ -722,6 +723,80 @@ def wl_served(args):
            "peak_inflight_GB": round(st["peak_inflight_bytes"] / 1e9, 2)})
 
 
+DSR = dict(angle=32.45, dz=0.3, xy=0.108, reverse=True)   # the reference demo's deskew / rotate settings
+
+
+def wl_dsr(args):
+    """Deskew / rotate of the headline volume's deconvolution (deskewRotateFrame3D, the demo's light-
+    sheet geometry: 32.45 deg, dz 0.3 um, 0.108 um pixels, reverse; |dx| = 2.34 px > 2, so slices are
+    interpolated in the skewed space first), uint16 in and out, everything resident on the device.
+    The rate is output voxels per second; each kernel's algorithmic bytes read the input (and the
+    interpolated slices) once and write each output once."""
+    import torch
+    from petakit5d_b200 import _lib
+    from petakit5d_b200 import decon as D
+    from petakit5d_b200 import deskew as G
+    from oracle import deskew as OD
+    if args.impl == "reference":
+        vol, _, _ = make_workload(seed=1, reference=True)
+        sub = np.asfortranarray(vol[:, :, :24])
+        t0 = time.perf_counter()
+        out = OD.deskew_rotate_frame3d(sub, DSR["angle"], DSR["dz"], DSR["xy"], reverse=DSR["reverse"], save16bit=True)
+        v = out.size / (time.perf_counter() - t0) / 1e6
+        _emit({"impl": "reference", "metric": "deskew/rotate output Mvoxel/s", "value": round(v, 3), "unit": "Mvoxel/s",
+               "workload": "dsr", "cpu_baseline": {"value": round(v, 3), "unit": "Mvoxel/s", "cores": 1, "kind": "port",
+                                                   "sample": "the first 24 z slices of the volume"}})
+        return
+    device = torch.device("cuda", 0)
+    vol, psf, psf_b = make_workload(seed=1)
+    ctx = _lib.Context(0)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=device)
+    d_in = _u16_dev(vol, device)
+    d_j = torch.empty_like(d_in)
+    D.decon_device("omw", d_in, "uint16", vol.shape, psf, psf_b, ITERS, out=d_j, ctx=ctx, stream=ctx.stream,
+                   Background=BACKGROUND)
+    kw = dict(reverse=DSR["reverse"], save16bit=True, ctx=ctx, stream=ctx.stream)
+    dims = G.deskew_rotate_device(d_j, "uint16", vol.shape, DSR["angle"], DSR["dz"], DSR["xy"], **kw)
+    d_o = torch.empty(int(np.prod(dims)), dtype=torch.int16, device=device)
+    step = lambda: G.deskew_rotate_device(d_j, "uint16", vol.shape, DSR["angle"], DSR["dz"], DSR["xy"], d_out=d_o, **kw)
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    e0, e1 = _events(stream)
+    steps = max(1, args.steps)
+    e0.record(stream)
+    for _ in range(steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    ctx.profile(True)
+    step()
+    torch.cuda.synchronize()
+    prof = ctx.profile_read()
+    ctx.profile(False)
+    p = OD.plan(vol.shape, DSR["angle"], DSR["dz"], DSR["xy"], reverse=DSR["reverse"])
+    _, _, nint = OD.interp_indexing(p["nz_total"], p["stepsize"])
+    n_out = int(np.prod(dims))
+    peak = _peaks()[0]
+    kern = {}
+    for k, v in (prof or {}).items():
+        gbs = v["bytes"] / (v["ms"] * 1e-3) / 1e9
+        kern[k] = {"ms": round(v["ms"], 4), "algorithmic_MB": round(v["bytes"] / 1e6, 1), "GB/s": round(gbs, 1),
+                   "frac_of_measured_hbm": round(gbs / peak, 3)}
+    # CPU sample for scale: the oracle on the first 24 z slices
+    sub = np.asfortranarray(d_j.cpu().numpy().view(np.uint16).T[:, :, :24])
+    t0 = time.perf_counter()
+    osub = OD.deskew_rotate_frame3d(sub, DSR["angle"], DSR["dz"], DSR["xy"], reverse=DSR["reverse"], save16bit=True)
+    cpu = osub.size / (time.perf_counter() - t0) / 1e6
+    _emit({"metric": "deskew/rotate output Mvoxel/s", "workload": "dsr: OMW x2 result of the 512x512x256 volume, "
+           "angle 32.45, dz 0.3, 0.108 um, reverse, uint16 in/out, skewed-space interpolation (step 1/2)",
+           "value": round(n_out / (ms * 1e-3) / 1e6, 1), "unit": "Mvoxel/s", "ms_per_step": round(ms, 4),
+           "out_dims": list(dims), "interpolated_slices": nint, "kernels": kern,
+           "cpu_baseline": {"value": round(cpu, 3), "unit": "Mvoxel/s", "cores": 1, "kind": "port",
+                            "sample": "the first 24 z slices of the deconvolved volume"}})
+
+
 def D_params():
     from petakit5d_b200 import decon as D
     return D._params({"background": 100.0, "dampfactor": 1.0, "scalefactor": 1.0, "deconoffset": 0.0,
@@ -817,7 +892,7 @@ def wl_large(args):
            "reference_cpu": "not run (the float32 CPU restatement needs ~100 GB of host RAM for this volume)"})
 
 
-WORKLOADS = {"rl_small": wl_rl_small, "batched": wl_batched, "served": wl_served, "large": wl_large}
+WORKLOADS = {"rl_small": wl_rl_small, "batched": wl_batched, "served": wl_served, "large": wl_large, "dsr": wl_dsr}
 
 if __name__ == "__main__":
     main()

@@ -182,6 +182,26 @@ PK_API pk_status pk_psf_gen(pk_ctx* ctx, const float* psf, const int64_t dims[3]
                             double med_factor, int32_t method, float* out, int64_t out_capacity,
                             int64_t out_dims[3]);
 
+/* ---------------------------------------------------------------- deskew / rotate */
+/* volout = deskewRotateFrame3D(vol, angle, dz, xyPixelSize, 'reverse', reverse, 'bbox', bbox,
+ * 'objectiveScan', objective_scan, 'xStepThresh', xstep_thresh, 'save16bit', save16bit)
+ * (deskew_rotate/deskewRotateFrame3D.m:1-260 with linear interpolation and no resampling, the path
+ * RLdecon.m:487-491 takes after deconvolution; the work of volume_deskew_rotate_warp_mex.cpp and
+ * skewed_space_interp_volume_deskew_rotate_warp_mex.cpp).  in: uint16 or float32 [ny nx nz]
+ * column-major; out: uint16 when save16bit and the input is uint16, else float32.  bbox: NULL (the
+ * whole rotated box) or [y1 x1 z1 y2 x2 z2], 1-based inclusive, y2 <= ny.  out_dims always receives
+ * the output size; with out == NULL nothing else is done. */
+PK_API pk_status pk_deskew_rotate(pk_ctx* ctx, const void* in, pk_dtype in_type, const int64_t dims[3], double angle,
+                                  double dz, double xy_pixel_size, int32_t reverse, int32_t objective_scan,
+                                  double xstep_thresh, const int64_t* bbox, int32_t save16bit, void* out,
+                                  int64_t out_dims[3]);
+/* The same on device buffers (d_out holds out_dims voxels), ordered on `stream` (NULL: the context's);
+ * a deconvolved volume from pk_decon_*_device can be deskewed without leaving the GPU. */
+PK_API pk_status pk_deskew_rotate_device(pk_ctx* ctx, const void* d_in, pk_dtype in_type, const int64_t dims[3],
+                                         double angle, double dz, double xy_pixel_size, int32_t reverse,
+                                         int32_t objective_scan, double xstep_thresh, const int64_t* bbox,
+                                         int32_t save16bit, void* d_out, int64_t out_dims[3], void* stream);
+
 /* ---------------------------------------------------------------- chunking helpers (host) */
 /* findGoodFactorNumber(n, direction, allowOddSeven)  -- utils/findGoodFactorNumber.m:1-26. */
 PK_API int64_t pk_find_good_factor_number(int64_t n, int32_t direction, int32_t allow_odd_seven);

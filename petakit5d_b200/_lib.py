@@ -83,6 +83,10 @@ _SIGS = {
                                       C.POINTER(C.c_double), P, P]),
     "pk_psf_gen": (C.c_int, [P, P, I64x3, C.c_double, C.c_double, C.c_double, C.c_int32, P, C.c_int64,
                              C.POINTER(C.c_int64)]),
+    "pk_deskew_rotate": (C.c_int, [P, P, C.c_int, I64x3, C.c_double, C.c_double, C.c_double, C.c_int32, C.c_int32,
+                                   C.c_double, P, C.c_int32, P, C.POINTER(C.c_int64)]),
+    "pk_deskew_rotate_device": (C.c_int, [P, P, C.c_int, I64x3, C.c_double, C.c_double, C.c_double, C.c_int32,
+                                          C.c_int32, C.c_double, P, C.c_int32, P, C.POINTER(C.c_int64), P]),
     "pk_find_good_factor_number": (C.c_int64, [C.c_int64, C.c_int32, C.c_int32]),
     "pk_chunk_coordinates": (C.c_int64, [I64x3, I64x3, I64x3, P, C.c_int32, I64x3, P, P, P]),
     "pk_batch_decon": (C.c_int, [P, C.c_int32, C.c_int32, C.POINTER(Chunk), C.c_int, C.c_int32, P, P, P,
