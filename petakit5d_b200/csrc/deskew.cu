@@ -5,7 +5,7 @@
 //     interpolated in the skewed space first, then the same warp.
 // Both are HBM-bound gathers.  The warp keeps the first axis (MATLAB y, contiguous) and
 // interpolates bilinearly over (x, z): an output row is a weighted sum of four input rows, so one
-// CTA computes a whole row with coalesced loads of the four source rows and a coalesced store.
+// warp computes a whole row with 16-byte loads of the four source rows and 16-byte stores.
 //
 // The float arithmetic follows the x86-64 build of those MEX files (the reference's platform):
 //   float input:  ((a*wa + b*wb) + c*wc) + d*wd at every position;
@@ -24,7 +24,8 @@
 
 namespace {
 
-int grid_rows(long long rows) { return (int)std::max(1LL, std::min(rows, 148LL * 16)); }
+constexpr int kRowThreads = 256;   // 8 warps, one output row each
+int grid_rows(long long rows) { return (int)std::max(1LL, std::min((rows + 7) / 8, 148LL * 16)); }
 
 long long mround(double v) { return v >= 0 ? (long long)std::floor(v + 0.5) : (long long)std::ceil(v - 0.5); }
 
@@ -42,20 +43,70 @@ __device__ __forceinline__ float wsum(float a, float b, float c, float d, float 
     return pairs ? __fadd_rn(__fadd_rn(pa, pb), __fadd_rn(pc, pd)) : __fadd_rn(__fadd_rn(__fadd_rn(pa, pb), pc), pd);
 }
 
-__device__ __forceinline__ void store(float* o, long long i, float v, bool) { o[i] = v; }
-__device__ __forceinline__ void store(uint16_t* o, long long i, float v, bool body) {
+__device__ __forceinline__ uint16_t to_u16(float v, bool body) {
     const float h = __fadd_rn(v, 0.5f);
     float r = body ? rintf(h) : truncf(h);
     r = fminf(fmaxf(r, 0.f), 65535.f);
-    o[i] = (uint16_t)r;
+    return (uint16_t)r;
+}
+__device__ __forceinline__ void store(float* o, long long i, float v, bool) { o[i] = v; }
+__device__ __forceinline__ void store(uint16_t* o, long long i, float v, bool body) { o[i] = to_u16(v, body); }
+
+// 8 consecutive row elements (16-byte aligned) to / from registers
+__device__ __forceinline__ void ld8(const float* p, float (&v)[8]) {
+    const float4 x = __ldg((const float4*)p), y = __ldg((const float4*)p + 1);
+    v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w; v[4] = y.x; v[5] = y.y; v[6] = y.z; v[7] = y.w;
+}
+__device__ __forceinline__ void ld8(const uint16_t* p, float (&v)[8]) {
+    const uint4 x = __ldg((const uint4*)p);
+    const unsigned int w[4] = {x.x, x.y, x.z, x.w};
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        v[2 * k] = (float)(w[k] & 0xffffu);
+        v[2 * k + 1] = (float)(w[k] >> 16);
+    }
+}
+__device__ __forceinline__ void st8(float* o, const float (&v)[8], bool) {
+    ((float4*)o)[0] = make_float4(v[0], v[1], v[2], v[3]);
+    ((float4*)o)[1] = make_float4(v[4], v[5], v[6], v[7]);
+}
+__device__ __forceinline__ void st8(uint16_t* o, const float (&v)[8], bool body) {
+    unsigned int w[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) w[k] = (unsigned int)to_u16(v[2 * k], body) | ((unsigned int)to_u16(v[2 * k + 1], body) << 16);
+    *(uint4*)o = make_uint4(w[0], w[1], w[2], w[3]);
 }
 
-// one weighted row: out[i] = sum_k w_k * src_k[i], i < len; U16 selects the uint16-helper rules
+__device__ __forceinline__ bool al16(const void* p) { return ((uintptr_t)p & 15) == 0; }
+
+// One weighted row, computed by one warp: out[i] = sum_k w_k * src_k[i], i < len.  u16 selects the
+// uint16-helper rules.  When every row start is 16-byte aligned and len is a multiple of 8, each
+// lane moves 8 elements per source with 16-byte accesses (whole 16-element blocks and the tail
+// never share an 8-element group then); otherwise element by element.
 template <int NT, typename TA, typename TB, typename TO>
 __device__ __forceinline__ void row_blend(const TA* a, const TB* b, const TA* c, const TB* d, float wa, float wb,
-                                          float wc, float wd, TO* o, int len, bool u16) {
+                                          float wc, float wd, TO* o, int len, bool u16, int lane) {
     const int body = len - len % 16;
-    for (int i = threadIdx.x; i < len; i += blockDim.x) {
+    const bool vec = (len & 7) == 0 && al16(a) && al16(b) && al16(o) && (NT == 2 || (al16(c) && al16(d)));
+    if (vec) {
+#pragma unroll 2
+        for (int i = lane * 8; i < len; i += 256) {
+            float va[8], vb[8], vc[8], vd[8], r[8];
+            ld8(a + i, va);
+            ld8(b + i, vb);
+            if (NT == 4) {
+                ld8(c + i, vc);
+                ld8(d + i, vd);
+            }
+            const bool in_body = i < body;
+#pragma unroll
+            for (int k = 0; k < 8; k++)
+                r[k] = wsum<NT>(va[k], vb[k], NT == 4 ? vc[k] : 0.f, NT == 4 ? vd[k] : 0.f, wa, wb, wc, wd, u16 && in_body);
+            st8(o + i, r, in_body);
+        }
+        return;
+    }
+    for (int i = lane; i < len; i += 32) {
         const bool in_body = i < body;
         const float v = wsum<NT>(ld(a, i), ld(b, i), NT == 4 ? ld(c, i) : 0.f, NT == 4 ? ld(d, i) : 0.f, wa, wb, wc, wd,
                                  u16 && in_body);
@@ -64,8 +115,8 @@ __device__ __forceinline__ void row_blend(const TA* a, const TB* b, const TA* c,
 }
 
 template <typename TO>
-__device__ __forceinline__ void row_zero(TO* o, int len) {
-    for (int i = threadIdx.x; i < len; i += blockDim.x) o[i] = (TO)0;
+__device__ __forceinline__ void row_zero(TO* o, int len, int lane) {
+    for (int i = lane; i < len; i += 32) o[i] = (TO)0;
 }
 
 // per interpolated slice (skewed_space_interp_defined_stepsize, :430-584): source slice, row offsets
@@ -83,7 +134,9 @@ __global__ void k_skew_interp(const TI* __restrict__ im, TO* __restrict__ out, i
     const long long rows = (long long)nint * nx;
     const long long plane = (long long)ny * nx;
     const bool u16 = sizeof(TI) == 2;
-    for (long long r = blockIdx.x; r < rows; r += gridDim.x) {
+    const int lane = threadIdx.x & 31;
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long r = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < rows; r += nw) {
         const int y = (int)(r % nx), k = (int)(r / nx);
         const SkewSlice q = sl[k];
         TO* o = out + (long long)k * plane + (long long)y * ny;
@@ -115,7 +168,7 @@ __global__ void k_skew_interp(const TI* __restrict__ im, TO* __restrict__ out, i
         if (!a || !b || (nt == 4 && (!c || !d))) {
             // a source row outside the volume reads as zero (only for volumes narrower than ~2 shifts)
             const int body = ny - ny % 16;
-            for (int i = threadIdx.x; i < ny; i += blockDim.x) {
+            for (int i = lane; i < ny; i += 32) {
                 const float va = a ? ld(a, i) : 0.f, vb = b ? ld(b, i) : 0.f;
                 const float vc = c ? ld(c, i) : 0.f, vd = d ? ld(d, i) : 0.f;
                 const float v = nt == 4 ? wsum<4>(va, vb, vc, vd, wa, wb, wc, wd, u16 && i < body)
@@ -123,9 +176,9 @@ __global__ void k_skew_interp(const TI* __restrict__ im, TO* __restrict__ out, i
                 store(o, i, v, i < body);
             }
         } else if (nt == 4) {
-            row_blend<4>(a, b, c, d, wa, wb, wc, wd, o, ny, u16);
+            row_blend<4>(a, b, c, d, wa, wb, wc, wd, o, ny, u16, lane);
         } else {
-            row_blend<2>(a, b, a, b, wa, wb, 0.f, 0.f, o, ny, u16);
+            row_blend<2>(a, b, a, b, wa, wb, 0.f, 0.f, o, ny, u16, lane);
         }
     }
 }
@@ -153,19 +206,21 @@ __global__ void k_dsr_warp(const TI* __restrict__ im, const TN* __restrict__ imi
                            const uint8_t* __restrict__ zorig, TO* __restrict__ out, WarpArgs w) {
     const long long rows = (long long)w.oy * w.oz;
     const long long plane = (long long)w.ny * w.nx;
-    for (long long r = blockIdx.x; r < rows; r += gridDim.x) {
+    const int lane = threadIdx.x & 31;
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long r = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < rows; r += nw) {
         const int y = (int)(r % w.oy), z = (int)(r / w.oy);
         TO* o = out + r * w.ox;
         const float fz = __fadd_rn((float)z, w.sz), fy = __fadd_rn((float)y, w.sy);
         double ty = __dadd_rn(__dmul_rn(w.t12, (double)fz), w.t13);
         if (ty < 0 || ty + 1 >= w.nx) {
             if (ty + 1 == w.nx) ty = nudge(ty, w.nx);
-            else { row_zero(o, w.ox); continue; }
+            else { row_zero(o, w.ox, lane); continue; }
         }
         double tz = __dadd_rn(__dadd_rn(__dmul_rn(w.t21, (double)fy), __dmul_rn(w.t22, (double)fz)), w.t23);
         if (tz < 0 || tz + 1 >= w.nzt) {
             if (tz + 1 == w.nzt) tz = nudge(tz, w.nzt);
-            else { row_zero(o, w.ox); continue; }
+            else { row_zero(o, w.ox, lane); continue; }
         }
         const long long y0 = (long long)floor(ty), z0 = (long long)floor(tz);
         const float wy = (float)(ty - (double)y0), wz = (float)(tz - (double)z0);
@@ -176,15 +231,15 @@ __global__ void k_dsr_warp(const TI* __restrict__ im, const TN* __restrict__ imi
         const long long p0 = (imi ? zindex[z0] : z0) * plane + ind, p1 = (imi ? zindex[z0 + 1] : z0 + 1) * plane + ind;
         const bool uin = sizeof(TI) == 2, uint_ = sizeof(TN) == 2;
         if (o0 && o1) {
-            row_blend<4>(im + p0, im + p1, im + p0 + w.ny, im + p1 + w.ny, w00, w01, w10, w11, o, w.ox, uin);
+            row_blend<4>(im + p0, im + p1, im + p0 + w.ny, im + p1 + w.ny, w00, w01, w10, w11, o, w.ox, uin, lane);
         } else if (!o0 && !o1) {
-            row_blend<4>(imi + p0, imi + p1, imi + p0 + w.ny, imi + p1 + w.ny, w00, w01, w10, w11, o, w.ox, uint_);
+            row_blend<4>(imi + p0, imi + p1, imi + p0 + w.ny, imi + p1 + w.ny, w00, w01, w10, w11, o, w.ox, uint_, lane);
         } else if (o0) {          // source slice z0 original, z0 + 1 interpolated
-            row_blend<4>(im + p0, imi + p1, im + p0 + w.ny, imi + p1 + w.ny, w00, w01, w10, w11, o, w.ox, uin || uint_);
+            row_blend<4>(im + p0, imi + p1, im + p0 + w.ny, imi + p1 + w.ny, w00, w01, w10, w11, o, w.ox, uin || uint_, lane);
         } else if (uin == uint_) {  // same types: the helper keeps the slice order
-            row_blend<4>(imi + p0, im + p1, imi + p0 + w.ny, im + p1 + w.ny, w00, w01, w10, w11, o, w.ox, uin);
+            row_blend<4>(imi + p0, im + p1, imi + p0 + w.ny, im + p1 + w.ny, w00, w01, w10, w11, o, w.ox, uin, lane);
         } else {                  // uint16 original at z0 + 1, float interpolated at z0: operands swapped
-            row_blend<4>(im + p1, imi + p0, im + p1 + w.ny, imi + p0 + w.ny, w01, w00, w11, w10, o, w.ox, true);
+            row_blend<4>(im + p1, imi + p0, im + p1 + w.ny, imi + p0 + w.ny, w01, w00, w11, w10, o, w.ox, true, lane);
         }
     }
 }
@@ -429,11 +484,11 @@ pk_status dsr_run(pk_ctx* ctx, const void* d_in, pk_dtype t, const int64_t dims[
             const double ib = (double)esize(t) * ny * nx * nz + (double)ie * ny * nx * nint;
             KernelProf kp(ctx, "k_skew_interp", ib, st);
             if (t == PK_F32)
-                k_skew_interp<float, float><<<g, 128, 0, st>>>((const float*)d_in, (float*)dint, ny, nx, nz, dsl, nint, xa, reverse);
+                k_skew_interp<float, float><<<g, kRowThreads, 0, st>>>((const float*)d_in, (float*)dint, ny, nx, nz, dsl, nint, xa, reverse);
             else if (u16_out)
-                k_skew_interp<uint16_t, uint16_t><<<g, 128, 0, st>>>((const uint16_t*)d_in, (uint16_t*)dint, ny, nx, nz, dsl, nint, xa, reverse);
+                k_skew_interp<uint16_t, uint16_t><<<g, kRowThreads, 0, st>>>((const uint16_t*)d_in, (uint16_t*)dint, ny, nx, nz, dsl, nint, xa, reverse);
             else
-                k_skew_interp<uint16_t, float><<<g, 128, 0, st>>>((const uint16_t*)d_in, (float*)dint, ny, nx, nz, dsl, nint, xa, reverse);
+                k_skew_interp<uint16_t, float><<<g, kRowThreads, 0, st>>>((const uint16_t*)d_in, (float*)dint, ny, nx, nz, dsl, nint, xa, reverse);
             PK_CUDA(cudaGetLastError());
             kp.done(st);
         }
@@ -448,12 +503,12 @@ pk_status dsr_run(pk_ctx* ctx, const void* d_in, pk_dtype t, const int64_t dims[
     if (P.do_interp) wb += (double)oe * ny * nx * (P.ntotal - nz);
     KernelProf kp(ctx, "k_dsr_warp", wb, st);
     if (t == PK_F32)
-        k_dsr_warp<float, float, float><<<g, 128, 0, st>>>((const float*)d_in, (const float*)imi, dzi, dzo, (float*)d_out, w);
+        k_dsr_warp<float, float, float><<<g, kRowThreads, 0, st>>>((const float*)d_in, (const float*)imi, dzi, dzo, (float*)d_out, w);
     else if (u16_out)
-        k_dsr_warp<uint16_t, uint16_t, uint16_t><<<g, 128, 0, st>>>((const uint16_t*)d_in, (const uint16_t*)imi, dzi, dzo,
+        k_dsr_warp<uint16_t, uint16_t, uint16_t><<<g, kRowThreads, 0, st>>>((const uint16_t*)d_in, (const uint16_t*)imi, dzi, dzo,
                                                                    (uint16_t*)d_out, w);
     else
-        k_dsr_warp<uint16_t, float, float><<<g, 128, 0, st>>>((const uint16_t*)d_in, (const float*)imi, dzi, dzo,
+        k_dsr_warp<uint16_t, float, float><<<g, kRowThreads, 0, st>>>((const uint16_t*)d_in, (const float*)imi, dzi, dzo,
                                                              (float*)d_out, w);
     PK_CUDA(cudaGetLastError());
     kp.done(st);

@@ -7,6 +7,8 @@
 //   [b, otf, absc, mask] = pkdecon_mex('omw_bp', psf, alpha, skewed, thresh, area, hann, minInt)
 //   [bp, otf] = pkdecon_mex('wb_bp', psf, alpha, beta, n, resFlag, iRes)
 //   psf      = pkdecon_mex('psf_gen', psf, dz_psf, dz_data, medFactor, PSFGenMethod)  % psf_gen_new
+//   volout   = pkdecon_mex('dsr', vol, angle, dz, xyPixelSize, reverse, objectiveScan, xStepThresh, bbox, save16bit)
+//                                                                 % deskewRotateFrame3D
 //   pkdecon_mex('reset')                                           % reset(gpuDevice) analogue
 // opts: struct with the reference's name/value fields (Background, save16bit, dampFactor,
 // scaleFactor, deconOffset, EdgeErosion, bbox).  Errors are raised with mexErrMsgIdAndTxt using the
@@ -212,6 +214,30 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
         const mwSize dd[3] = {(mwSize)od[0], (mwSize)od[1], (mwSize)od[2]};
         plhs[0] = mxCreateNumericArray(3, dd, mxSINGLE_CLASS, mxREAL);
         check(pk_psf_gen(ctx(), psf, pd, dzp, dzd, mf, method, (float*)mxGetData(plhs[0]), (int64_t)(od[0] * od[1] * od[2]), od));
+        return;
+    }
+    if (!strcmp(cmd, "dsr")) {
+        if (nrhs < 10) mexErrMsgIdAndTxt("pkdecon:invalid", "dsr: vol, angle, dz, xyPixelSize, reverse, objectiveScan, xStepThresh, bbox, save16bit");
+        int64_t d[3], od[3], bb[6];
+        dims3(prhs[1], d);
+        pk_dtype t;
+        if (mxGetClassID(prhs[1]) == mxUINT16_CLASS) t = PK_U16;
+        else if (mxGetClassID(prhs[1]) == mxSINGLE_CLASS) t = PK_F32;
+        else mexErrMsgIdAndTxt("pkdecon:invalid", "vol must be uint16 or single");
+        const int64_t* pbb = nullptr;
+        if (!mxIsEmpty(prhs[8])) {
+            if (mxGetNumberOfElements(prhs[8]) != 6) mexErrMsgIdAndTxt("pkdecon:invalid", "bbox must have 6 elements");
+            for (int k = 0; k < 6; k++) bb[k] = (int64_t)mxGetPr(prhs[8])[k];
+            pbb = bb;
+        }
+        const double ang = mxGetScalar(prhs[2]), dz = mxGetScalar(prhs[3]), px = mxGetScalar(prhs[4]);
+        const int32_t rev = mxGetScalar(prhs[5]) != 0, obj = mxGetScalar(prhs[6]) != 0, s16 = mxGetScalar(prhs[9]) != 0;
+        const double thr = mxGetScalar(prhs[7]);
+        const void* in = mxGetData(prhs[1]);
+        check(pk_deskew_rotate(ctx(), in, t, d, ang, dz, px, rev, obj, thr, pbb, s16, nullptr, od));
+        const mwSize dd[3] = {(mwSize)od[0], (mwSize)od[1], (mwSize)od[2]};
+        plhs[0] = mxCreateNumericArray(3, dd, (s16 && t == PK_U16) ? mxUINT16_CLASS : mxSINGLE_CLASS, mxREAL);
+        check(pk_deskew_rotate(ctx(), in, t, d, ang, dz, px, rev, obj, thr, pbb, s16, mxGetData(plhs[0]), od));
         return;
     }
     mexErrMsgIdAndTxt("pkdecon:invalid", "unknown command '%s'", cmd);
