@@ -202,6 +202,26 @@ PK_API pk_status pk_deskew_rotate_device(pk_ctx* ctx, const void* d_in, pk_dtype
                                          int32_t objective_scan, double xstep_thresh, const int64_t* bbox,
                                          int32_t save16bit, void* d_out, int64_t out_dims[3], void* stream);
 
+/* ---------------------------------------------------------------- TIFF volumes (host) */
+/* getImageSizeMex(path) (io/cpp-tiff/mexSrc/getimagesizemex.cpp): [ny nx nz] of a TIFF (pages, or
+ * images=N of an ImageJ raw stack), bits per sample and whether samples are IEEE floats. */
+PK_API pk_status pk_tiff_info(const char* path, int64_t dims[3], int32_t* bits, int32_t* is_float);
+/* data = parallelReadTiff(path[, range]) (io/cpp-tiff/src/parallelreadtiff.cpp; io/readtiff.m):
+ * pages z_range[0]..z_range[1] (1-based inclusive; NULL = all) into out as a column-major
+ * [ny nx nz'] array of the file's sample type (out_bytes must hold it).  Classic TIFF or BigTIFF,
+ * strips, uncompressed / LZW / Deflate, horizontal predictor; strips decoded on `threads` host
+ * threads (0 = all cores).  Read into a pk_host_alloc buffer, the volume is ready for streamed
+ * (pinned) uploads. */
+PK_API pk_status pk_tiff_read(const char* path, const int64_t* z_range, void* out, int64_t out_bytes, int32_t threads);
+/* parallelWriteTiff(path, data) (io/cpp-tiff/src/parallelwritetiff.cpp; io/writetiff.m): a
+ * column-major [ny nx nz] array as BigTIFF, one page per z, 512-row strips, LZW (lzw = 1, the
+ * writetiff default) or none; bits 8/16/32/64, is_float for single/double. */
+PK_API pk_status pk_tiff_write(const char* path, const void* data, const int64_t dims[3], int32_t bits,
+                               int32_t is_float, int32_t lzw, int32_t threads);
+/* Page-locked host buffers (cudaHostAlloc) for file reads that feed the GPU. */
+PK_API pk_status pk_host_alloc(int64_t bytes, void** ptr);
+PK_API pk_status pk_host_free(void* ptr);
+
 /* ---------------------------------------------------------------- chunking helpers (host) */
 /* findGoodFactorNumber(n, direction, allowOddSeven)  -- utils/findGoodFactorNumber.m:1-26. */
 PK_API int64_t pk_find_good_factor_number(int64_t n, int32_t direction, int32_t allow_odd_seven);

@@ -87,7 +87,7 @@ def _debug_run(method, vol, t, pf, pb, numit, p, opts, ctx, out):
     """debug = true: err_mat from the library, uint16(J) of every saveStep-th iteration written to
     debug_folder/Iter_%04d.tif (decon_lucy_omw_function.m:113-141, decon_lucy_function.m:144-171)."""
     import os
-    from .tiff import write_tiff
+    from .tiff import writetiff
     estep = int(opts["savestep"])
     numit = int(numit)
     nsnap = numit // estep if estep >= 1 else 0
@@ -103,7 +103,7 @@ def _debug_run(method, vol, t, pf, pb, numit, p, opts, ctx, out):
     folder = opts["debug_folder"]
     os.makedirs(folder, exist_ok=True)
     for s in range(nsnap):
-        write_tiff(os.path.join(folder, f"Iter_{(s + 1) * estep:04d}.tif"), snaps[s].T)
+        writetiff(snaps[s].T, os.path.join(folder, f"Iter_{(s + 1) * estep:04d}.tif"))
     return err_mat
 
 

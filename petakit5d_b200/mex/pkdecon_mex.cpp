@@ -9,6 +9,9 @@
 //   psf      = pkdecon_mex('psf_gen', psf, dz_psf, dz_data, medFactor, PSFGenMethod)  % psf_gen_new
 //   volout   = pkdecon_mex('dsr', vol, angle, dz, xyPixelSize, reverse, objectiveScan, xStepThresh, bbox, save16bit)
 //                                                                 % deskewRotateFrame3D
+//   data     = pkdecon_mex('readtiff', path[, [z1 z2]])            % parallelReadTiff
+//   pkdecon_mex('writetiff', path, data, compression)             % parallelWriteTiff ('lzw' | 'none')
+//   sz       = pkdecon_mex('tiffsize', path)                      % getImageSizeMex
 //   pkdecon_mex('reset')                                           % reset(gpuDevice) analogue
 // opts: struct with the reference's name/value fields (Background, save16bit, dampFactor,
 // scaleFactor, deconOffset, EdgeErosion, bbox).  Errors are raised with mexErrMsgIdAndTxt using the
@@ -238,6 +241,55 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
         const mwSize dd[3] = {(mwSize)od[0], (mwSize)od[1], (mwSize)od[2]};
         plhs[0] = mxCreateNumericArray(3, dd, (s16 && t == PK_U16) ? mxUINT16_CLASS : mxSINGLE_CLASS, mxREAL);
         check(pk_deskew_rotate(ctx(), in, t, d, ang, dz, px, rev, obj, thr, pbb, s16, mxGetData(plhs[0]), od));
+        return;
+    }
+    if (!strcmp(cmd, "readtiff") || !strcmp(cmd, "tiffsize")) {
+        if (nrhs < 2 || !mxIsChar(prhs[1])) mexErrMsgIdAndTxt("pkdecon:invalid", "%s: file name", cmd);
+        std::vector<char> path(mxGetNumberOfElements(prhs[1]) + 1);
+        mxGetString(prhs[1], path.data(), (mwSize)path.size());
+        int64_t d[3];
+        int32_t bits = 0, isf = 0;
+        check(pk_tiff_info(path.data(), d, &bits, &isf));
+        if (!strcmp(cmd, "tiffsize")) {
+            plhs[0] = mxCreateDoubleMatrix(1, 3, mxREAL);
+            for (int k = 0; k < 3; k++) mxGetPr(plhs[0])[k] = (double)d[k];
+            return;
+        }
+        int64_t rng[2];
+        const int64_t* pr = nullptr;
+        if (nrhs > 2 && !mxIsEmpty(prhs[2])) {
+            if (mxGetNumberOfElements(prhs[2]) != 2) mexErrMsgIdAndTxt("pkdecon:invalid", "Input range is not 2");
+            rng[0] = (int64_t)mxGetPr(prhs[2])[0];
+            rng[1] = (int64_t)mxGetPr(prhs[2])[1];
+            d[2] = rng[1] - rng[0] + 1;
+            pr = rng;
+        }
+        mxClassID c;
+        if (isf) c = bits == 64 ? mxDOUBLE_CLASS : mxSINGLE_CLASS;
+        else c = bits == 8 ? mxUINT8_CLASS : bits == 16 ? mxUINT16_CLASS : mxUINT32_CLASS;
+        const mwSize dd[3] = {(mwSize)d[0], (mwSize)d[1], (mwSize)(d[2] > 0 ? d[2] : 0)};
+        plhs[0] = mxCreateNumericArray(3, dd, c, mxREAL);
+        check(pk_tiff_read(path.data(), pr, mxGetData(plhs[0]), (int64_t)(mxGetElementSize(plhs[0]) * mxGetNumberOfElements(plhs[0])), 0));
+        return;
+    }
+    if (!strcmp(cmd, "writetiff")) {
+        if (nrhs < 3 || !mxIsChar(prhs[1])) mexErrMsgIdAndTxt("pkdecon:invalid", "writetiff: file name, data[, compression]");
+        std::vector<char> path(mxGetNumberOfElements(prhs[1]) + 1);
+        mxGetString(prhs[1], path.data(), (mwSize)path.size());
+        int32_t bits, isf = 0;
+        switch (mxGetClassID(prhs[2])) {
+            case mxUINT8_CLASS: case mxLOGICAL_CLASS: bits = 8; break;
+            case mxUINT16_CLASS: bits = 16; break;
+            case mxUINT32_CLASS: bits = 32; break;
+            case mxSINGLE_CLASS: bits = 32; isf = 1; break;
+            case mxDOUBLE_CLASS: bits = 64; isf = 1; break;
+            default: mexErrMsgIdAndTxt("pkdecon:invalid", "Data type not suppported");
+        }
+        char comp[8] = "lzw";
+        if (nrhs > 3 && mxIsChar(prhs[3])) mxGetString(prhs[3], comp, sizeof(comp));
+        int64_t d[3];
+        dims3(prhs[2], d);
+        check(pk_tiff_write(path.data(), mxGetData(prhs[2]), d, bits, isf, strcmp(comp, "none") != 0, 0));
         return;
     }
     mexErrMsgIdAndTxt("pkdecon:invalid", "unknown command '%s'", cmd);

@@ -1,73 +1,89 @@
-"""Minimal uncompressed multi-page TIFF writer for uint16 volumes (the debug runs' Iter_%04d.tif).
+"""TIFF volumes (drop-ins for the reference's io/readtiff.m, io/writetiff.m and getImageSizeMex).
 
-A MATLAB [ny nx nz] volume is written as nz pages of ny rows by nx columns (the layout writetiff in
-the reference produces for its debug snapshots): little-endian, one strip per page, 16-bit
-unsigned, min-is-black.  No compression and no ImageJ metadata.
+The reference reads and writes every volume of the deconvolution pipeline with its parallel
+libtiff MEX files (io/cpp-tiff/src/parallelreadtiff.cpp, parallelwritetiff.cpp).  These functions
+call libpkdecon.so's own reader / writer (no libtiff): a MATLAB-ordered [ny nx nz] array is stored as
+nz pages of ny rows by nx columns; ``writetiff`` writes BigTIFF with LZW (the reference default) or
+no compression; ``readtiff`` decodes strips on all host cores and can place the volume in pinned
+(page-locked) memory, so the following host-buffer deconvolution call uploads it at full PCIe rate.
 """
 from __future__ import annotations
 
-import struct
+import ctypes as C
+import os
+import weakref
 
 import numpy as np
 
-_TAGS_PER_PAGE = 10
+from ._lib import check, i64x3, lib, ptr
+
+_W = {np.dtype(np.uint8): (8, 0), np.dtype(np.uint16): (16, 0), np.dtype(np.float32): (32, 1),
+      np.dtype(np.float64): (64, 1), np.dtype(np.uint32): (32, 0)}
 
 
-def write_tiff(path, vol):
-    """Write ``vol`` ([ny, nx, nz] or [ny, nx], uint16) to ``path``."""
-    v = np.asarray(vol)
-    if v.dtype != np.uint16:
-        raise TypeError("write_tiff takes uint16 volumes")
-    if v.ndim == 2:
-        v = v[:, :, None]
-    ny, nx, nz = v.shape
-    page_bytes = ny * nx * 2
-    ifd_bytes = 2 + 12 * _TAGS_PER_PAGE + 4
-    with open(path, "wb") as f:
-        f.write(b"II" + struct.pack("<HI", 42, 8))
-        pos = 8
-        for z in range(nz):
-            ifd_pos = pos
-            data_pos = ifd_pos + ifd_bytes
-            next_ifd = data_pos + page_bytes if z + 1 < nz else 0
-            tags = [                                    # (tag, type, count, value); 3 = SHORT, 4 = LONG
-                (256, 4, 1, nx),                        # ImageWidth (columns = x)
-                (257, 4, 1, ny),                        # ImageLength (rows = y)
-                (258, 3, 1, 16),                        # BitsPerSample
-                (259, 3, 1, 1),                         # Compression: none
-                (262, 3, 1, 1),                         # Photometric: min-is-black
-                (273, 4, 1, data_pos),                  # StripOffsets
-                (277, 3, 1, 1),                         # SamplesPerPixel
-                (278, 4, 1, ny),                        # RowsPerStrip
-                (279, 4, 1, page_bytes),                # StripByteCounts
-                (339, 3, 1, 1),                         # SampleFormat: unsigned
-            ]
-            f.write(struct.pack("<H", len(tags)))
-            for tag, typ, cnt, val in tags:
-                f.write(struct.pack("<HHI", tag, typ, cnt))
-                f.write(struct.pack("<HH", val, 0) if typ == 3 else struct.pack("<I", val))
-            f.write(struct.pack("<I", next_ifd))
-            f.write(np.ascontiguousarray(v[:, :, z]).astype("<u2").tobytes())   # row-major: rows = y
-            pos = data_pos + page_bytes
+def _dtype(bits, is_float):
+    for d, (b, f) in _W.items():
+        if b == bits and f == int(bool(is_float)):
+            return d
+    raise TypeError(f"unsupported TIFF sample type: {bits} bits, float={bool(is_float)}")
 
 
-def read_tiff(path):
-    """Read a file written by write_tiff back into a [ny, nx, nz] uint16 array (for tests)."""
-    with open(path, "rb") as f:
-        b = f.read()
-    if b[:4] != b"II*\x00":
-        raise ValueError("not a little-endian TIFF")
-    (off,) = struct.unpack_from("<I", b, 4)
-    pages = []
-    while off:
-        (n,) = struct.unpack_from("<H", b, off)
-        t = {}
-        for i in range(n):
-            tag, typ, cnt = struct.unpack_from("<HHI", b, off + 2 + 12 * i)
-            val = struct.unpack_from("<H" if typ == 3 else "<I", b, off + 2 + 12 * i + 8)[0]
-            t[tag] = val
-        nx, ny = t[256], t[257]
-        data = np.frombuffer(b, "<u2", ny * nx, t[273]).reshape(ny, nx)
-        pages.append(data)
-        (off,) = struct.unpack_from("<I", b, off + 2 + 12 * n)
-    return np.stack(pages, axis=2)
+def getImageSize(filepath):
+    """[ny, nx, nz] of a TIFF file (getImageSizeMex)."""
+    d = (C.c_int64 * 3)()
+    check(lib.pk_tiff_info(os.fsencode(str(filepath)), d, None, None))
+    return tuple(int(v) for v in d)
+
+
+def pinned_empty(shape, dtype):
+    """A Fortran-ordered numpy array in page-locked host memory (freed with the array)."""
+    dtype = np.dtype(dtype)
+    n = int(np.prod(shape)) * dtype.itemsize
+    p = C.c_void_p()
+    check(lib.pk_host_alloc(n, C.byref(p)))
+    buf = (C.c_char * max(n, 1)).from_address(p.value)
+    weakref.finalize(buf, lib.pk_host_free, C.c_void_p(p.value))
+    return np.frombuffer(buf, dtype=dtype, count=int(np.prod(shape))).reshape(shape, order="F")
+
+
+def readtiff(filepath, range=None, pinned=False, threads=0):
+    """data = readtiff(filepath[, range=[z1 z2]]) (io/readtiff.m -> parallelReadTiff).
+
+    A single page comes back 2D, as in MATLAB.  ``pinned=True`` reads into page-locked memory."""
+    path = os.fsencode(str(filepath))
+    d = (C.c_int64 * 3)()
+    bits = C.c_int32()
+    isf = C.c_int32()
+    check(lib.pk_tiff_info(path, d, C.byref(bits), C.byref(isf)))
+    dt = _dtype(bits.value, isf.value)
+    ny, nx, nz = (int(v) for v in d)
+    rng = None
+    if range is not None and len(range):
+        if len(range) != 2:
+            raise ValueError("Input range is not 2")
+        rng = (C.c_int64 * 2)(int(range[0]), int(range[1]))
+        nz = int(range[1]) - int(range[0]) + 1
+    shape = (ny, nx, max(nz, 0))
+    out = pinned_empty(shape, dt) if pinned else np.empty(shape, dt, order="F")
+    check(lib.pk_tiff_read(path, rng, ptr(out), out.nbytes, int(threads)))
+    return out[:, :, 0] if out.shape[2] == 1 else out
+
+
+def writetiff(img, filepath, Compression="lzw", threads=0):
+    """writetiff(img, filepath, Compression='lzw') (io/writetiff.m -> parallelWriteTiff)."""
+    a = np.asarray(img)
+    if a.dtype == np.bool_:
+        a = a.astype(np.uint8)
+    if a.dtype not in _W:
+        raise TypeError(f"writetiff: unsupported data type {a.dtype}")
+    comp = str(Compression).lower()
+    if comp not in ("lzw", "none"):
+        raise ValueError("Compression must be 'lzw' or 'none'")
+    while a.ndim < 3:
+        a = a[..., None]
+    a = np.asfortranarray(a)
+    bits, isf = _W[a.dtype]
+    d = os.path.dirname(os.path.abspath(str(filepath)))
+    os.makedirs(d, exist_ok=True)
+    check(lib.pk_tiff_write(os.fsencode(str(filepath)), ptr(a), i64x3(a.shape), bits, isf, int(comp == "lzw"),
+                            int(threads)))

@@ -5,7 +5,8 @@
 #include <stdint.h>
 typedef struct mxArray_tag mxArray;
 typedef size_t mwSize;
-typedef enum { mxUNKNOWN_CLASS, mxDOUBLE_CLASS, mxSINGLE_CLASS, mxUINT8_CLASS, mxUINT16_CLASS } mxClassID;
+typedef enum { mxUNKNOWN_CLASS, mxLOGICAL_CLASS, mxDOUBLE_CLASS, mxSINGLE_CLASS, mxUINT8_CLASS, mxUINT16_CLASS,
+               mxUINT32_CLASS } mxClassID;
 typedef enum { mxREAL, mxCOMPLEX } mxComplexity;
 typedef struct { double real, imag; } mxComplexDouble;
 typedef struct { float real, imag; } mxComplexSingle;
@@ -24,6 +25,7 @@ double* mxGetPr(const mxArray* a);
 const mwSize* mxGetDimensions(const mxArray* a);
 mwSize mxGetNumberOfDimensions(const mxArray* a);
 size_t mxGetNumberOfElements(const mxArray* a);
+size_t mxGetElementSize(const mxArray* a);
 mxArray* mxGetField(const mxArray* a, size_t i, const char* name);
 double mxGetScalar(const mxArray* a);
 int mxGetString(const mxArray* a, char* buf, mwSize n);

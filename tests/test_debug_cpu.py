@@ -4,7 +4,6 @@ import numpy as np
 import pytest
 
 from oracle import decon as O
-from petakit5d_b200.tiff import read_tiff, write_tiff
 
 
 def test_err_mat_every_iteration():
@@ -33,9 +32,3 @@ def test_err_mat_rl_without_step_index_fails_like_the_reference():
         O.err_mat_from_mse([4, 2, 1, 0.5, 0.25], 2, "rl")
 
 
-def test_tiff_roundtrip(tmp_path):
-    v = (np.arange(6 * 5 * 4) * 997 % 65536).astype(np.uint16).reshape(6, 5, 4, order="F")
-    write_tiff(tmp_path / "a.tif", v)
-    back = read_tiff(tmp_path / "a.tif")
-    assert back.shape == (6, 5, 4)
-    assert np.array_equal(back, v)

@@ -9,7 +9,7 @@ from oracle import decon as O
 from petakit5d_b200 import _lib
 from petakit5d_b200 import decon as D
 from petakit5d_b200 import synth
-from petakit5d_b200.tiff import read_tiff
+from petakit5d_b200.tiff import readtiff
 
 pytestmark = pytest.mark.gpu
 
@@ -38,7 +38,7 @@ def test_omw_debug(small, tmp_path):
     Ipre, _ = O.preprocess(vol, 100, False, np.float32)
     _check_err(err, O.debug_err_mat(its, Ipre, 2, "omw"))
     for k in (2, 4):
-        snap = read_tiff(os.path.join(folder, f"Iter_{k:04d}.tif"))
+        snap = readtiff(os.path.join(folder, f"Iter_{k:04d}.tif"))
         assert np.max(np.abs(snap.astype(np.int64) - O.to_uint16(its[k - 1]).astype(np.int64))) <= 1
     plain, _ = D.decon_lucy_omw_function(vol, psf, psf_b, 4, Background=100, save16bit=False)
     assert np.array_equal(J, plain)
