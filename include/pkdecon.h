@@ -111,6 +111,23 @@ PK_API pk_status pk_decon_debug(pk_ctx* ctx, int32_t method, const void* in, pk_
                                 const pk_decon_params* params, int32_t save_step, void* out, double* err_mat,
                                 int32_t* err_rows, uint16_t* snapshots);
 
+/* Asynchronous host-buffer call: uploads `in` on a copy stream, deconvolves (method 0 = Biggs RL,
+ * 1 = OMW, parameters as pk_decon_lucy / pk_decon_lucy_omw) and downloads into `out` on a second copy
+ * stream, then returns at once with a ticket.  Two staging slots are used in turn, so the upload of
+ * the next call and the download of the previous one overlap this call's compute (a stream of volumes
+ * runs at the slowest of upload, compute and download).  `in` and `out` must stay valid until
+ * pk_decon_wait returns; they must be page-locked (pk_host_alloc, cudaHostAlloc) for the copies to
+ * overlap.  No counterpart in the reference (its calls are synchronous). */
+PK_API pk_status pk_decon_submit(pk_ctx* ctx, int32_t method, const void* in, pk_dtype in_type, const int64_t dims[3],
+                                 const float* psf_f, const int64_t psf_f_dims[3], const float* psf_b,
+                                 const int64_t psf_b_dims[3], int32_t numit, const pk_decon_params* params, void* out,
+                                 int64_t* ticket);
+/* Waits for a submitted call (timeout_ms < 0: no limit; PK_ERR_TIMEOUT leaves the ticket valid). */
+PK_API pk_status pk_decon_wait(pk_ctx* ctx, int64_t ticket, int32_t timeout_ms);
+/* Orders the context's compute stream after everything queued so far on its copy streams (for
+ * device-side timing of submitted calls with events on pk_ctx_stream). */
+PK_API pk_status pk_ctx_join(pk_ctx* ctx);
+
 /* Device-pointer forms of the two calls (the gateway's mxGPUArray path): `in`/`out` are device
  * pointers, the work is queued on `stream` (a cudaStream_t, NULL = the context's stream) and the
  * call returns without synchronising. */

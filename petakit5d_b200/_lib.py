@@ -69,6 +69,10 @@ _SIGS = {
                                     C.POINTER(DeconParams), P]),
     "pk_decon_debug": (C.c_int, [P, C.c_int32, P, C.c_int, I64x3, P, I64x3, P, I64x3, C.c_int32,
                                  C.POINTER(DeconParams), C.c_int32, P, P, C.POINTER(C.c_int32), P]),
+    "pk_decon_submit": (C.c_int, [P, C.c_int32, P, C.c_int, I64x3, P, I64x3, P, I64x3, C.c_int32,
+                                  C.POINTER(DeconParams), P, C.POINTER(C.c_int64)]),
+    "pk_decon_wait": (C.c_int, [P, C.c_int64, C.c_int32]),
+    "pk_ctx_join": (C.c_int, [P]),
     "pk_decon_lucy_device": (C.c_int, [P, P, C.c_int, I64x3, P, I64x3, C.c_int32, C.POINTER(DeconParams), P, P]),
     "pk_decon_lucy_omw_device": (C.c_int, [P, P, C.c_int, I64x3, P, I64x3, P, I64x3, C.c_int32,
                                            C.POINTER(DeconParams), P, P]),

@@ -1,7 +1,9 @@
 // extern "C" entry points of libpkdecon.so (declared in include/pkdecon.h).
 #include <algorithm>
 #include <cmath>
+#include <chrono>
 #include <cstring>
+#include <thread>
 #include <string>
 #include <vector>
 
@@ -97,6 +99,15 @@ static void release_all(pk_ctx* ctx) {
     cudaStreamSynchronize(ctx->stream);
     if (ctx->h2d) { cudaStreamSynchronize(ctx->h2d); cudaStreamDestroy(ctx->h2d); ctx->h2d = nullptr; }
     if (ctx->d2h) { cudaStreamSynchronize(ctx->d2h); cudaStreamDestroy(ctx->d2h); ctx->d2h = nullptr; }
+    for (auto& a : ctx->aslot) {
+        if (a.d_in) cudaFree(a.d_in);
+        if (a.d_out) cudaFree(a.d_out);
+        for (cudaEvent_t e : {a.up, a.comp, a.down})
+            if (e) cudaEventDestroy(e);
+        a = pk_ctx::AsyncSlot();
+    }
+    for (auto& kv : ctx->tickets) cudaEventDestroy(kv.second);
+    ctx->tickets.clear();
     for (auto e : ctx->io_ev) cudaEventDestroy(e);
     ctx->io_ev.clear();
     pk_release_graphs(ctx);
@@ -263,6 +274,117 @@ static pk_status decon_host(pk_ctx* ctx, int method, const void* in, pk_dtype in
     } else {
         PK_CUDA(cudaMemcpyAsync(out, d_out, outb, cudaMemcpyDeviceToHost, st));
         PK_CUDA(cudaStreamSynchronize(st));
+    }
+    return PK_OK;
+}
+
+// ---- asynchronous host-buffer calls
+static pk_status grow(void** p, size_t* cap, size_t need, cudaEvent_t in_use) {
+    if (*cap >= need && *p) return PK_OK;
+    if (in_use) PK_CUDA(cudaEventSynchronize(in_use));
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+    *cap = 0;
+    if (cudaMalloc(p, std::max<size_t>(need, 256)) != cudaSuccess) {
+        cudaGetLastError();
+        *p = nullptr;
+        return pk_fail(PK_ERR_NOMEM, "staging buffer allocation failed");
+    }
+    *cap = need;
+    return PK_OK;
+}
+
+pk_status pk_decon_submit(pk_ctx* ctx, int32_t method, const void* in, pk_dtype in_type, const int64_t dims[3],
+                          const float* psf_f, const int64_t psf_f_dims[3], const float* psf_b,
+                          const int64_t psf_b_dims[3], int32_t numit, const pk_decon_params* params, void* out,
+                          int64_t* ticket) {
+    pk_status s;
+    if ((s = check_ctx(ctx)) != PK_OK) return s;
+    if (!ticket) return pk_fail(PK_ERR_INVALID, "NULL ticket");
+    if (method != 0 && method != 1) return pk_fail(PK_ERR_INVALID, "method must be 0 (RL) or 1 (OMW)");
+    if ((s = check_dims(dims, "input volume")) != PK_OK) return s;
+    if (!in || !out) return pk_fail(PK_ERR_INVALID, "NULL input/output buffer");
+    if (in_type != PK_U16 && in_type != PK_F32 && in_type != PK_F64) return pk_fail(PK_ERR_INVALID, "bad input dtype");
+    pk_decon_params def;
+    if (!params) {
+        pk_params_default(&def);
+        params = &def;
+    }
+    std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+    DeviceGuard g(ctx->device);
+    if (!ctx->h2d) PK_CUDA(cudaStreamCreateWithFlags(&ctx->h2d, cudaStreamNonBlocking));
+    if (!ctx->d2h) PK_CUDA(cudaStreamCreateWithFlags(&ctx->d2h, cudaStreamNonBlocking));
+    pk_ctx::AsyncSlot& a = ctx->aslot[ctx->next_ticket & 1];
+    for (cudaEvent_t* e : {&a.up, &a.comp, &a.down})
+        if (!*e) PK_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    const size_t inb = (size_t)dims[0] * dims[1] * dims[2] * dtype_size(in_type);
+    int64_t od[3];
+    pk_output_dims(dims, params, od);
+    const size_t outb = (size_t)od[0] * od[1] * od[2] * (params->save16bit ? 2 : 4);
+    if ((s = grow(&a.d_in, &a.in_cap, inb, a.used ? a.comp : nullptr)) != PK_OK) return s;
+    if ((s = grow(&a.d_out, &a.out_cap, outb, a.used ? a.down : nullptr)) != PK_OK) return s;
+    cudaStream_t st = ctx->stream;
+    // upload once the slot's previous call has read its input; compute once the upload has landed and
+    // the slot's previous result has been downloaded; download once the compute is done
+    if (a.used) PK_CUDA(cudaStreamWaitEvent(ctx->h2d, a.comp, 0));
+    PK_CUDA(cudaMemcpyAsync(a.d_in, in, inb, cudaMemcpyHostToDevice, ctx->h2d));
+    PK_CUDA(cudaEventRecord(a.up, ctx->h2d));
+    PK_CUDA(cudaStreamWaitEvent(st, a.up, 0));
+    if (a.used) PK_CUDA(cudaStreamWaitEvent(st, a.down, 0));
+    if ((s = decon_device(ctx, method, a.d_in, in_type, dims, psf_f, psf_f_dims, psf_b, psf_b_dims, numit, params,
+                          a.d_out, st)) != PK_OK)
+        return s;
+    PK_CUDA(cudaEventRecord(a.comp, st));
+    PK_CUDA(cudaStreamWaitEvent(ctx->d2h, a.comp, 0));
+    PK_CUDA(cudaMemcpyAsync(out, a.d_out, outb, cudaMemcpyDeviceToHost, ctx->d2h));
+    PK_CUDA(cudaEventRecord(a.down, ctx->d2h));
+    cudaEvent_t done;
+    PK_CUDA(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
+    PK_CUDA(cudaEventRecord(done, ctx->d2h));
+    a.used = true;
+    *ticket = ctx->next_ticket++;
+    ctx->tickets[*ticket] = done;
+    return PK_OK;
+}
+
+pk_status pk_decon_wait(pk_ctx* ctx, int64_t ticket, int32_t timeout_ms) {
+    pk_status s;
+    if ((s = check_ctx(ctx)) != PK_OK) return s;
+    cudaEvent_t ev;
+    {
+        std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+        auto it = ctx->tickets.find(ticket);
+        if (it == ctx->tickets.end()) return pk_fail(PK_ERR_INVALID, "unknown or already collected ticket");
+        ev = it->second;
+    }
+    DeviceGuard g(ctx->device);
+    const auto t0 = std::chrono::steady_clock::now();
+    cudaError_t e;
+    while ((e = cudaEventQuery(ev)) == cudaErrorNotReady) {
+        if (timeout_ms >= 0 &&
+            std::chrono::steady_clock::now() - t0 > std::chrono::milliseconds(timeout_ms))
+            return pk_fail(PK_ERR_TIMEOUT, "pk_decon_wait: the call has not finished");
+        std::this_thread::sleep_for(std::chrono::microseconds(20));
+    }
+    std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+    ctx->tickets.erase(ticket);
+    cudaEventDestroy(ev);
+    if (e != cudaSuccess) return pk_fail(PK_ERR_CUDA, std::string("pk_decon_wait: ") + cudaGetErrorString(e));
+    return PK_OK;
+}
+
+pk_status pk_ctx_join(pk_ctx* ctx) {
+    pk_status s;
+    if ((s = check_ctx(ctx)) != PK_OK) return s;
+    std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+    DeviceGuard g(ctx->device);
+    for (cudaStream_t c : {ctx->h2d, ctx->d2h}) {
+        if (!c) continue;
+        cudaEvent_t e;
+        PK_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        PK_CUDA(cudaEventRecord(e, c));
+        PK_CUDA(cudaStreamWaitEvent(ctx->stream, e, 0));
+        cudaEventDestroy(e);
     }
     return PK_OK;
 }

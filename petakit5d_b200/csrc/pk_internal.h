@@ -149,6 +149,17 @@ struct pk_ctx {
     // copy streams and per-slab events of streamed host calls
     cudaStream_t h2d = nullptr, d2h = nullptr;
     std::vector<cudaEvent_t> io_ev;
+    // asynchronous host-buffer calls (pk_decon_submit / pk_decon_wait): two staging slots used in
+    // turn, so the upload of call k+1 and the download of call k-1 overlap the compute of call k
+    struct AsyncSlot {
+        void* d_in = nullptr; size_t in_cap = 0;
+        void* d_out = nullptr; size_t out_cap = 0;
+        cudaEvent_t up = nullptr, comp = nullptr, down = nullptr;   // upload done, compute done, download done
+        bool used = false;
+    };
+    AsyncSlot aslot[2];
+    long long next_ticket = 1;
+    std::map<long long, cudaEvent_t> tickets;                  // ticket -> its download's event
 };
 
 // error helpers (capi.cpp)

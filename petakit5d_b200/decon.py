@@ -141,6 +141,41 @@ def decon_lucy_omw_function(I, PSF_f, PSF_b, NUMIT, **kw):
     return _squeeze_like(out, I), np.zeros((int(NUMIT), 4))
 
 
+_INFLIGHT = {}
+
+
+def decon_submit(method, I, PSF_f, PSF_b, NUMIT, out, ctx=None, **kw):
+    """Queue one host-buffer deconvolution ('omw' or 'rl') and return its ticket at once.
+
+    ``out`` receives the result (the shape and dtype ``decon_lucy_*_function`` would return, in
+    Fortran order); ``I`` and ``out`` should be page-locked (``tiff.pinned_empty``, torch
+    ``pin_memory``) for the copies to overlap other calls' compute.  Collect with ``decon_wait``."""
+    opts, _ = _parse(kw)
+    ctx = ctx or _lib.default_context()
+    vol, t = _volume(I)
+    pf = _psf(PSF_f)
+    pb = _psf(PSF_b) if method == "omw" else None
+    p = _params(opts)
+    od = i64x3([0, 0, 0])
+    check(lib.pk_output_dims(i64x3(vol.shape), p, od))
+    dt = np.dtype(np.uint16 if p.save16bit else np.float32)
+    if out.dtype != dt or out.size < int(np.prod([int(v) for v in od])):
+        raise ValueError(f"out must hold {tuple(int(v) for v in od)} {dt}")
+    tk = _lib.C.c_int64()
+    check(lib.pk_decon_submit(ctx.handle, 1 if method == "omw" else 0, ptr(vol), t, i64x3(vol.shape), ptr(pf),
+                              i64x3(pf.shape), ptr(pb), i64x3(pb.shape if pb is not None else pf.shape), int(NUMIT),
+                              p, ptr(out), _lib.C.byref(tk)))
+    _INFLIGHT[(ctx.handle, tk.value)] = (vol, out)       # keep the buffers alive until the wait
+    return tk.value
+
+
+def decon_wait(ticket, timeout_ms=-1, ctx=None):
+    """Wait for a ``decon_submit`` ticket (raises PkError PK_ERR_TIMEOUT when ``timeout_ms`` passes)."""
+    ctx = ctx or _lib.default_context()
+    check(lib.pk_decon_wait(ctx.handle, int(ticket), int(timeout_ms)))
+    _INFLIGHT.pop((ctx.handle, int(ticket)), None)
+
+
 def _squeeze_like(out, I):
     nd = np.asarray(I).ndim
     if nd < 3 and out.shape[2] == 1:
