@@ -1,0 +1,74 @@
+"""RLdecon drop-in (per-file driver): files in, files out, every step on the GPU, and the same
+numbers as calling the steps one by one."""
+import os
+
+import numpy as np
+import pytest
+
+from petakit5d_b200 import backprojector as B
+from petakit5d_b200 import decon as D
+from petakit5d_b200 import deskew as G
+from petakit5d_b200 import psfgen as P
+from petakit5d_b200 import synth
+from petakit5d_b200 import tiff as T
+from petakit5d_b200.rldecon import RLdecon
+
+pytestmark = pytest.mark.gpu
+
+
+def _files(tmp_path):
+    psf_true = synth.gaussian_psf((31, 31, 41))
+    vol = synth.puncta_volume((96, 80, 40), 60, psf_true, seed=5)
+    bead = synth.measured_psf((32, 32, 41), sigma_xy=1.3, sigma_z=3.0, seed=6)
+    raw = str(tmp_path / "data" / "frame_CamA.tif")
+    pfn = str(tmp_path / "psf" / "psf_CamA.tif")
+    T.writetiff(vol, raw)
+    T.writetiff(bead, pfn)
+    return vol, bead, raw, pfn
+
+
+def test_rldecon_omw_with_deskew_rotate(tmp_path):
+    vol, bead, raw, pfn = _files(tmp_path)
+    out = str(tmp_path / "data" / "matlab_decon" / "frame_CamA.tif")
+    J, ds, dsr = RLdecon(raw, out, pfn, 0.108, 0.3, 0.1, Background=100, DeconIter=2, RLMethod="omw",
+                         wienerAlpha=0.005, OTFCumThresh=0.6, Deskew=True, Rotate=True, Reverse=True)
+    dpath = os.path.dirname(out)
+    assert os.path.exists(out) and os.path.exists(os.path.join(dpath, "DSR", "frame_CamA.tif"))
+    assert os.path.exists(os.path.join(dpath, "MIPs", "frame_CamA_MIP_z.tif"))
+    assert os.path.exists(os.path.join(dpath, "DSR", "MIPs", "frame_CamA_MIP_z.tif"))
+    gen = os.path.join(dpath, "psfgen", "psf_CamA_omw.tif")
+    bpf = os.path.join(dpath, "psfgen", "psf_CamA_back_projector_alpha_0.005000_otf_cum_thresh_0.600000.tif")
+    assert os.path.exists(gen) and os.path.exists(bpf)
+    # the same steps one by one
+    psf = P.rldecon_psf_crop(P.psf_gen_new(bead, 0.1, 0.3 * np.sin(np.radians(32.45))), vol.shape, "omw")
+    np.testing.assert_array_equal(T.readtiff(gen), psf)
+    bp = B.omw_backprojector_generation(psf, 0.005, None, OTFCumThresh=0.6)[0]
+    np.testing.assert_array_equal(T.readtiff(bpf), bp)
+    p32 = psf / np.float32(psf.sum(dtype=np.float32))
+    ref, _ = D.decon_lucy_omw_function(vol, p32, bp, 2, Background=100)
+    np.testing.assert_array_equal(J, ref)
+    np.testing.assert_array_equal(T.readtiff(out), ref)
+    ref_dsr = G.deskewRotateFrame3D(ref, 32.45, 0.3, 0.108, reverse=True, save16bit=True)
+    np.testing.assert_array_equal(dsr, ref_dsr)
+    np.testing.assert_array_equal(T.readtiff(os.path.join(dpath, "DSR", "frame_CamA.tif")), ref_dsr)
+    np.testing.assert_array_equal(T.readtiff(os.path.join(dpath, "MIPs", "frame_CamA_MIP_z.tif")), ref.max(axis=2))
+    # a second call finds the outputs and the cached PSF files and does not redo the work
+    mtime = os.path.getmtime(out)
+    J2, _, _ = RLdecon(raw, out, pfn, 0.108, 0.3, 0.1, Background=100, DeconIter=2, OTFCumThresh=0.6)
+    assert os.path.getmtime(out) == mtime and J2 is None
+
+
+def test_rldecon_simplified_crops_the_psf_and_the_output(tmp_path):
+    vol, bead, raw, pfn = _files(tmp_path)
+    out = str(tmp_path / "o" / "frame_CamA.tif")
+    bbox = [5, 7, 3, 90, 70, 38]
+    J, _, _ = RLdecon(raw, out, pfn, 0.108, 0.3, 0.1, Background=100, DeconIter=3, RLMethod="simplified",
+                      deconBbox=bbox, save16bit=False, mipAxis=[1, 1, 1])
+    psf = P.psf_gen_new(bead, 0.1, 0.3 * np.sin(np.radians(32.45)))
+    psf = P.rldecon_psf_crop(psf, vol.shape, "simplified")
+    p32 = psf / np.float32(psf.sum(dtype=np.float32))
+    ref = D.decon_lucy_function(vol, p32, 3, Background=100, bbox=bbox, save16bit=False)[0]
+    assert J.shape == (86, 64, 36)
+    np.testing.assert_array_equal(J, ref)
+    for ax in "yxz":
+        assert os.path.exists(os.path.join(os.path.dirname(out), "MIPs", f"frame_CamA_MIP_{ax}.tif"))
