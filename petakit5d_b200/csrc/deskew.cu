@@ -29,8 +29,15 @@ int grid_rows(long long rows) { return (int)std::max(1LL, std::min((rows + 7) / 
 
 long long mround(double v) { return v >= 0 ? (long long)std::floor(v + 0.5) : (long long)std::ceil(v - 0.5); }
 
+// uint16 <-> float without the conversion unit: with 2^23 added, a float's low mantissa bits hold an
+// integer exactly, and a round-to-nearest-even add of 2^23 rounds a value in [0, 2^23) to an integer
+// the way rintf does.  (The conversion instructions run on a quarter-rate pipe and bounded these
+// kernels; these forms use only the integer and FMA pipes and give identical results.)
+constexpr float kMagic = 8388608.f;
+__device__ __forceinline__ float u16f(unsigned v) { return __fsub_rn(__uint_as_float(0x4B000000u | v), kMagic); }
+
 __device__ __forceinline__ float ld(const float* p, long long i) { return __ldg(p + i); }
-__device__ __forceinline__ float ld(const uint16_t* p, long long i) { return (float)__ldg(p + i); }
+__device__ __forceinline__ float ld(const uint16_t* p, long long i) { return u16f(__ldg(p + i)); }
 
 // 2- or 4-term weighted sum of one row position with the association of the MEX helper for the
 // operand types (pairs: uint16 helpers' whole blocks; otherwise left to right)
@@ -43,11 +50,12 @@ __device__ __forceinline__ float wsum(float a, float b, float c, float d, float 
     return pairs ? __fadd_rn(__fadd_rn(pa, pb), __fadd_rn(pc, pd)) : __fadd_rn(__fadd_rn(__fadd_rn(pa, pb), pc), pd);
 }
 
+// res + 0.5 rounded to nearest even (whole blocks) or truncated (tail), saturated to [0, 65535]
 __device__ __forceinline__ uint16_t to_u16(float v, bool body) {
-    const float h = __fadd_rn(v, 0.5f);
-    float r = body ? rintf(h) : truncf(h);
-    r = fminf(fmaxf(r, 0.f), 65535.f);
-    return (uint16_t)r;
+    const float h = fminf(fmaxf(__fadd_rn(v, 0.5f), 0.f), 65536.f);
+    unsigned r = __float_as_uint(__fadd_rn(h, kMagic)) & 0x7FFFFFu;                  // rintf(h)
+    if (!body && __fsub_rn(__uint_as_float(0x4B000000u | r), kMagic) > h) r -= 1;     // truncf(h), h >= 0
+    return (uint16_t)min(r, 65535u);
 }
 __device__ __forceinline__ void store(float* o, long long i, float v, bool) { o[i] = v; }
 __device__ __forceinline__ void store(uint16_t* o, long long i, float v, bool body) { o[i] = to_u16(v, body); }
@@ -62,8 +70,8 @@ __device__ __forceinline__ void ld8(const uint16_t* p, float (&v)[8]) {
     const unsigned int w[4] = {x.x, x.y, x.z, x.w};
 #pragma unroll
     for (int k = 0; k < 4; k++) {
-        v[2 * k] = (float)(w[k] & 0xffffu);
-        v[2 * k + 1] = (float)(w[k] >> 16);
+        v[2 * k] = u16f(w[k] & 0xffffu);
+        v[2 * k + 1] = u16f(w[k] >> 16);
     }
 }
 __device__ __forceinline__ void st8(float* o, const float (&v)[8], bool) {

@@ -18,7 +18,7 @@ pytestmark = pytest.mark.gpu
 
 def _files(tmp_path):
     psf_true = synth.gaussian_psf((31, 31, 41))
-    vol = synth.puncta_volume((96, 80, 40), 60, psf_true, seed=5)
+    vol = synth.puncta_volume((96, 80, 48), 60, psf_true, seed=5)
     bead = synth.measured_psf((32, 32, 41), sigma_xy=1.3, sigma_z=3.0, seed=6)
     raw = str(tmp_path / "data" / "frame_CamA.tif")
     pfn = str(tmp_path / "psf" / "psf_CamA.tif")
