@@ -239,6 +239,14 @@ PK_API pk_status pk_tiff_write(const char* path, const void* data, const int64_t
 PK_API pk_status pk_host_alloc(int64_t bytes, void** ptr);
 PK_API pk_status pk_host_free(void* ptr);
 
+/* ---------------------------------------------------------------- large-file edge erosion */
+/* The large-file runner's edge erosion (decon/RLdecon_large_in_memory.m:146-168, 267-270):
+ * mask = im > 0 with the six faces cleared, mask = bwdist(~mask) > erosion - 1 (Euclidean), then
+ * out = out .* mask.  im: host uint16/single [ny nx nz]; out (host, out_type, may be NULL) is
+ * multiplied in place; mask (host uint8, may be NULL) receives the mask. */
+PK_API pk_status pk_edge_erosion_edt(pk_ctx* ctx, const void* im, pk_dtype im_type, const int64_t dims[3],
+                                     int32_t erosion, void* out, pk_dtype out_type, uint8_t* mask);
+
 /* ---------------------------------------------------------------- chunking helpers (host) */
 /* findGoodFactorNumber(n, direction, allowOddSeven)  -- utils/findGoodFactorNumber.m:1-26. */
 PK_API int64_t pk_find_good_factor_number(int64_t n, int32_t direction, int32_t allow_odd_seven);

@@ -3,6 +3,7 @@
 * ``find_good_factor_number`` follows utils/findGoodFactorNumber.m:1-26.
 * ``zarr_chunk_coordinates`` follows microscopeDataProcessing/stitch/XR_zarrChunkCoordinatesExtraction.m:1-83.
 * ``border_size`` follows RLdecon_large_in_memory.m:177 / RLdecon_large_in_place.m:175.
+* ``edt_erosion_mask`` follows RLdecon_large_in_memory.m:153-157 (bwdist through scipy's exact EDT).
 """
 from __future__ import annotations
 
@@ -70,3 +71,16 @@ def zarr_chunk_coordinates(vol_size, batch_size=(1024, 1024, 1024), block_size=(
     local[:, 3:] = local[:, :3] + (region[:, 3:] - region[:, :3])
     region = region - np.concatenate([ws, ws]) + 1
     return batch, region, local
+
+
+def edt_erosion_mask(im, E):
+    """RLdecon_large_in_memory.m:153-157: mask = im > 0 with the six faces cleared, then
+    bwdist(~mask) > E - 1 (Euclidean distance to the nearest cleared voxel; scipy's exact EDT)."""
+    import scipy.ndimage as ndi
+    m = np.asarray(im) > 0
+    m[[0, -1], :, :] = False
+    m[:, [0, -1], :] = False
+    m[:, :, [0, -1]] = False
+    if not m.any():
+        return m
+    return ndi.distance_transform_edt(m) > (E - 1)

@@ -6,10 +6,14 @@
 * ``batch_decon``              -- many chunks in shared launches (pk_batch_decon)
 * ``decon_large_in_memory``    -- RLdecon_large_in_memory.m:177-260: chunk grid with borders, decon of
                                   every chunk cropped to its region (deconBbox), paste back
+* ``edge_erosion_mask``        -- the runner's bwdist edge erosion (RLdecon_large_in_memory.m:146-168)
+* ``RLdecon_large_in_memory``  -- the whole runner for TIFF files (RLdecon_large_in_memory.m:1-300)
 """
 from __future__ import annotations
 
 import ctypes as C
+import math
+import os
 
 import numpy as np
 
@@ -124,6 +128,132 @@ def decon_large_in_memory(volume, psf, numit=2, method="omw", psf_b=None, batch_
     out = np.empty(vol.shape, np.uint16 if save16 else np.float32, order="F")
     for r, o in zip(rb, outs):
         out[r[0] - 1:r[3], r[1] - 1:r[4], r[2] - 1:r[5]] = o
+    return out
+
+
+def edge_erosion_mask(im, erosion, out=None, ctx=None):
+    """RLdecon_large_in_memory.m:146-168, 267-270 on the GPU: the mask ``bwdist(~(im > 0, faces
+    cleared)) > erosion - 1``; ``out`` (uint16 / single, Fortran order) is multiplied by it in place."""
+    ctx = ctx or _lib.default_context()
+    a = np.asfortranarray(im)
+    if a.dtype not in (np.uint16, np.float32):
+        a = np.asfortranarray(a.astype(np.float32))
+    mask = np.empty(a.shape, np.uint8, order="F")
+    t = _lib.PK_U16 if a.dtype == np.uint16 else _lib.PK_F32
+    ot = 0
+    if out is not None:
+        if not out.flags.f_contiguous or out.shape != a.shape or out.dtype not in (np.uint16, np.float32):
+            raise ValueError("out must be a Fortran-ordered uint16/single array of the volume's shape")
+        ot = _lib.PK_U16 if out.dtype == np.uint16 else _lib.PK_F32
+    check(lib.pk_edge_erosion_edt(ctx.handle, ptr(a), t, i64x3(a.shape), int(erosion), ptr(out), ot, ptr(mask)))
+    return mask.astype(bool)
+
+
+def RLdecon_large_in_memory(frameFullpath, psfFullpath, deconFullpath, xyPixelSize, dz, **kw):
+    """RLdecon_large_in_memory(frameFullpath, psfFullpath, deconFullpath, xyPixelSize, dz, ...)
+    (decon/RLdecon_large_in_memory.m:1-300) for TIFF files: the PSF prepared with psf_gen_new and
+    saved under ``<deconPath>/psfgen/``, the volume read whole, cut into ``batchSize`` chunks with
+    ``round((size(psf) + 10) / 2)`` borders, every chunk deconvolved as RLdecon would (one batched
+    call), the regions pasted back, the edge-erosion mask applied, and the result and its z MIP
+    written.  Zarr files and ``maskFullpaths`` are not built (NotImplementedError)."""
+    from . import backprojector as B
+    from . import psfgen as P
+    from . import tiff as T
+    o = dict(save16bit=True, Rotate=False, Deskew=False, SkewAngle=-32.45, flipZstack=False, Background=None,
+             dzPSF=0.1, DeconIter=15, EdgeErosion=8, ErodeMaskfile="", SaveMaskfile=False, dampFactor=1.0,
+             scaleFactor=None, deconOffset=0.0, maskFullpaths=(), saveZarr=False, RLMethod="simplified",
+             wienerAlpha=0.005, OTFCumThresh=0.9, hannWinBounds=(0.8, 1.0), skewed=None, fixIter=True,
+             errThresh=None, batchSize=(1024, 1024, 1024), Overlap=200, CPUMaxMem=500, parseCluster=True, uuid="",
+             debug=False, psfGen=True, useGPU=True, ctx=None, EdgeSoften=5, zEdgeSoften=2, Crop=None, zFlip=False,
+             GenMaxZproj=(0, 0, 1))
+    low = {k.lower(): k for k in o}
+    for k, v in kw.items():
+        if k.lower() not in low:
+            raise TypeError(f"RLdecon_large_in_memory: unknown parameter {k!r}")
+        o[low[k.lower()]] = v
+    if o["saveZarr"] or not str(frameFullpath).endswith((".tif", ".tiff")):
+        raise NotImplementedError("Zarr input / output is not built")
+    if o["maskFullpaths"] and len(o["maskFullpaths"]) and o["maskFullpaths"][0]:
+        raise NotImplementedError("maskFullpaths (Zarr masks) is not built")
+    if o["Deskew"] or o["Rotate"]:
+        raise NotImplementedError("deskew / rotate of chunks is not built in the large-file runner")
+    method = str(o["RLMethod"])
+    if method not in ("simplified", "omw"):
+        raise NotImplementedError(f"RLMethod '{method}' is not built")
+    ctx = o["ctx"]
+    bg = 99.0 if o["Background"] is None or np.size(o["Background"]) == 0 else float(o["Background"])   # :81-83
+    erosion = int(o["EdgeErosion"])
+    if o["ErodeMaskfile"] and os.path.exists(o["ErodeMaskfile"]):
+        erosion = 0
+    decon_path = os.path.dirname(deconFullpath)
+    fsname = os.path.splitext(os.path.basename(frameFullpath))[0]
+    pp = T.readtiff(psfFullpath).astype(np.float32)
+    skew = float(o["SkewAngle"])
+    # the PSF that sets the chunk borders (:93-123)
+    if o["psfGen"]:
+        ratio = math.sin(math.radians(skew)) if o["Deskew"] else 1.0
+        g = P.psf_gen_new(pp, o["dzPSF"], dz * ratio, 1.5, "masked", ctx=ctx)
+        psf = P.rldecon_psf_crop(g, g.shape, "simplified")      # bounding box +-1 only (:108-114)
+        os.makedirs(os.path.join(decon_path, "psfgen"), exist_ok=True)
+        gen_fn = os.path.join(decon_path, "psfgen", os.path.splitext(os.path.basename(psfFullpath))[0] + ".tif")
+        if not os.path.exists(gen_fn):
+            T.writetiff(psf, gen_fn)
+    else:
+        psf = pp
+    im = T.readtiff(frameFullpath, pinned=True)
+    if im.ndim == 2:
+        im = im[:, :, None]
+    if o["flipZstack"]:
+        im = np.asfortranarray(im[:, :, ::-1])
+    # the PSF each chunk's RLdecon call prepares from the same file (RLdecon.m:241-265: its own
+    # dz ratio, sind(|SkewAngle|) outside objective scan), and the OMW backprojector of it
+    if o["psfGen"]:
+        cpsf = P.psf_gen_new(pp, o["dzPSF"], dz * math.sin(math.radians(abs(skew))), 1.5, "masked", ctx=ctx)
+        if method != "omw":
+            cpsf = P.rldecon_psf_crop(cpsf, cpsf.shape, "simplified")
+    else:
+        cpsf = pp
+    border = border_size(np.asarray(psf).shape[:3] + (1,) * (3 - np.asarray(psf).ndim))
+    bs = tuple(int(v) for v in o["batchSize"])
+    bb, rb, _ = zarr_chunk_coordinates(im.shape, batch_size=bs, block_size=bs, same_batch_size=False, border=border)
+    chunks, boxes, psfs, psfs_b, ids, key = [], [], [], [], [], {}
+    for b, r in zip(bb, rb):
+        c = np.asfortranarray(im[b[0] - 1:b[3], b[1] - 1:b[4], b[2] - 1:b[5]])
+        chunks.append(c)
+        boxes.append([*(r[:3] - b[:3] + 1), *(r[3:] - b[:3] + 1)])
+        cp = P.rldecon_psf_crop(cpsf, c.shape, "omw")          # crop a PSF larger than the chunk (:260-265)
+        k = cp.shape
+        if k not in key:
+            key[k] = len(psfs)
+            p32 = np.asarray(cp, np.float32)
+            psfs.append(p32 / np.float32(p32.sum(dtype=np.float32)))
+            if method == "omw":
+                bp = B.omw_backprojector_generation(cp, float(o["wienerAlpha"]), o["skewed"],
+                                                    OTFCumThresh=float(o["OTFCumThresh"]),
+                                                    hannWinBounds=o["hannWinBounds"], ctx=ctx)[0]
+                psfs_b.append(P.rldecon_psf_crop(bp, c.shape, "omw"))
+        ids.append(key[k])
+    scale = 1.0 if o["scaleFactor"] is None or np.size(o["scaleFactor"]) == 0 else float(o["scaleFactor"])
+    outs = batch_decon(chunks, psfs, ids, int(o["DeconIter"]), "omw" if method == "omw" else "rl",
+                       psfs_b if method == "omw" else None, boxes,
+                       False, ctx, Background=bg, save16bit=bool(o["save16bit"]), dampFactor=o["dampFactor"],
+                       scaleFactor=scale, deconOffset=o["deconOffset"])
+    out = np.zeros(im.shape, np.uint16 if o["save16bit"] else np.float32, order="F")
+    for r, ob in zip(rb, outs):
+        out[r[0] - 1:r[3], r[1] - 1:r[4], r[2] - 1:r[5]] = ob
+    if erosion > 0:                                                                     # :146-168, 267-270
+        mask = edge_erosion_mask(im, erosion, out=out, ctx=ctx)
+        if o["SaveMaskfile"]:
+            mp = os.path.join(decon_path, "Masks", f"{fsname}_eroded.tif")
+            os.makedirs(os.path.dirname(mp), exist_ok=True)
+            T.writetiff(mask.astype(np.uint8), mp)
+    if o["ErodeMaskfile"] and os.path.exists(o["ErodeMaskfile"]):
+        out *= (T.readtiff(o["ErodeMaskfile"]) > 0).reshape(out.shape, order="F").astype(out.dtype)
+    os.makedirs(decon_path or ".", exist_ok=True)
+    T.writetiff(out, deconFullpath)
+    mip_dir = os.path.join(decon_path, "MIPs")
+    os.makedirs(mip_dir, exist_ok=True)
+    T.writetiff(out.max(axis=2), os.path.join(mip_dir, f"{fsname}_MIP_z.tif"))
     return out
 
 
