@@ -312,7 +312,7 @@ pk_status pk_make_otf(pk_ctx* ctx, const float* h_psf, const int64_t pd[3], int 
 }
 
 pk_status pk_get_otf(pk_ctx* ctx, const float* h_psf, const int64_t pd[3], int ny, int nx, int nz,
-                     const float2** d_otf, cudaStream_t st) {
+                     const float2** d_otf, cudaStream_t st, std::shared_ptr<const std::vector<float>>* confirmed) {
     const long long pn = (long long)pd[0] * pd[1] * pd[2];
     // open addressing on the key: an entry with the same key but another PSF moves this one on
     uint64_t hk = psf_key(h_psf, pd);
@@ -320,15 +320,20 @@ pk_status pk_get_otf(pk_ctx* ctx, const float* h_psf, const int64_t pd[3], int n
         auto it = ctx->otf.find(std::make_tuple(hk, ny, nx, nz));
         if (it == ctx->otf.end()) break;
         const OtfEntry& c = it->second;
-        if (c.pd[0] == pd[0] && c.pd[1] == pd[1] && c.pd[2] == pd[2] && (long long)c.psf.size() == pn &&
-            memcmp(c.psf.data(), h_psf, sizeof(float) * pn) == 0) {
+        if (c.pd[0] != pd[0] || c.pd[1] != pd[1] || c.pd[2] != pd[2] || (long long)c.psf->size() != pn) continue;
+        const bool same = (confirmed && *confirmed && c.psf == *confirmed) ||
+                          memcmp(c.psf->data(), h_psf, sizeof(float) * pn) == 0;
+        if (same) {
+            if (confirmed && !*confirmed) *confirmed = c.psf;
             *d_otf = c.d;
             return PK_OK;
         }
     }
     const auto key = std::make_tuple(hk, ny, nx, nz);
     OtfEntry e;
-    e.psf.assign(h_psf, h_psf + pn);
+    if (confirmed && *confirmed && (long long)(*confirmed)->size() == pn) e.psf = *confirmed;
+    else e.psf = std::make_shared<const std::vector<float>>(h_psf, h_psf + pn);
+    if (confirmed) *confirmed = e.psf;
     for (int i = 0; i < 3; i++) e.pd[i] = pd[i];
     const int Py = ny / 2 + 1;
     e.bytes = sizeof(float2) * (size_t)(Py + (Py & 1)) * nx * nz;

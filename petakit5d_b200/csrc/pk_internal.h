@@ -106,7 +106,9 @@ struct TwTable { float2* d = nullptr; int n = 0; };
 struct OtfEntry {
     float2* d = nullptr;      // pre-scaled (1/N) half spectrum
     size_t bytes = 0;
-    std::vector<float> psf;   // the PSF it was made from (a cache hit compares the whole PSF)
+    // the PSF it was made from (a cache hit compares the whole PSF); entries of one PSF at several
+    // data sizes share this storage, so a PSF confirmed once needs no second comparison
+    std::shared_ptr<const std::vector<float>> psf;
     int64_t pd[3] = {0, 0, 0};
 };
 
@@ -219,8 +221,12 @@ int pk_label26(const uint8_t* m, int ny, int nx, int nz, std::vector<int>& lab, 
 std::vector<double2> pk_twiddles64(int n, int sign);   // exp(sign 2 pi i m / n), m < n
 
 // decon drivers (decon.cu)
+// OTF of a host PSF at a data size, from the context's cache or made on `st`.  `confirmed` (may be
+// null) carries, across the lookups of one call, the cached copy the host PSF has already been
+// compared equal to: entries sharing that copy are hits without another comparison.
 pk_status pk_get_otf(pk_ctx* ctx, const float* h_psf, const int64_t psf_dims[3], int ny, int nx, int nz,
-                     const float2** d_otf, cudaStream_t st);
+                     const float2** d_otf, cudaStream_t st,
+                     std::shared_ptr<const std::vector<float>>* confirmed = nullptr);
 // one volume of a multi-volume run: inputs, transform extent, OTFs, outputs and work buffers
 struct DeconJob {
     const void* d_raw = nullptr;
