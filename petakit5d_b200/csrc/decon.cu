@@ -331,8 +331,24 @@ pk_status pk_get_otf(pk_ctx* ctx, const float* h_psf, const int64_t pd[3], int n
     }
     const auto key = std::make_tuple(hk, ny, nx, nz);
     OtfEntry e;
-    if (confirmed && *confirmed && (long long)(*confirmed)->size() == pn) e.psf = *confirmed;
-    else e.psf = std::make_shared<const std::vector<float>>(h_psf, h_psf + pn);
+    if (confirmed && *confirmed && (long long)(*confirmed)->size() == pn) {
+        e.psf = *confirmed;
+    } else {
+        // share the copy of an entry of the same PSF at another data size (compared once, here), so a
+        // later call that confirms one of them hits the others by pointer
+        const uint64_t k0 = psf_key(h_psf, pd);
+        for (const auto& kv : ctx->otf) {
+            const OtfEntry& o = kv.second;
+            if (std::get<0>(kv.first) != k0 || o.pd[0] != pd[0] || o.pd[1] != pd[1] || o.pd[2] != pd[2] ||
+                (long long)o.psf->size() != pn)
+                continue;
+            if (memcmp(o.psf->data(), h_psf, sizeof(float) * pn) == 0) {
+                e.psf = o.psf;
+                break;
+            }
+        }
+        if (!e.psf) e.psf = std::make_shared<const std::vector<float>>(h_psf, h_psf + pn);
+    }
     if (confirmed) *confirmed = e.psf;
     for (int i = 0; i < 3; i++) e.pd[i] = pd[i];
     const int Py = ny / 2 + 1;

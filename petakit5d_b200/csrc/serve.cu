@@ -35,6 +35,9 @@ struct PsfEntry {
     std::vector<float> f, b;
     int64_t dims[3];
     bool has_b = false;
+    // the OTF cache's copies these (immutable) PSFs were found equal to: later lookups at other
+    // data sizes compare pointers instead of the whole PSF
+    std::shared_ptr<const std::vector<float>> seen_f, seen_b;
 };
 
 struct Step {
@@ -202,10 +205,12 @@ pk_status pk_server::admit(const std::shared_ptr<Request>& r) {
     VolDesc b;
     pk_status s = pk_init_desc(c, (int)r->dims[0], (int)r->dims[1], (int)r->dims[2], &b);
     if (s != PK_OK) return s;
-    const PsfEntry& pe = psfs[r->psf_id];
+    PsfEntry& pe = psfs[r->psf_id];
     const float2 *of = nullptr, *ob = nullptr;
-    if ((s = pk_get_otf(c, pe.f.data(), pe.dims, b.ny, b.nx, b.nz, &of, c->stream)) != PK_OK) return s;
-    if (r->method == 1 && (s = pk_get_otf(c, pe.b.data(), pe.dims, b.ny, b.nx, b.nz, &ob, c->stream)) != PK_OK) return s;
+    if ((s = pk_get_otf(c, pe.f.data(), pe.dims, b.ny, b.nx, b.nz, &of, c->stream, &pe.seen_f)) != PK_OK) return s;
+    if (r->method == 1 &&
+        (s = pk_get_otf(c, pe.b.data(), pe.dims, b.ny, b.nx, b.nz, &ob, c->stream, &pe.seen_b)) != PK_OK)
+        return s;
     const size_t raw_b = (size_t)b.nrows * b.ny * 2;
     int64_t od[3];
     pk_output_dims(r->dims, &r->params, od);
