@@ -54,9 +54,10 @@ void lzw_encode(const uint8_t* in, size_t len, std::vector<uint8_t>& out) {
     out.clear();
     out.reserve(len / 2 + 64);
     BitWriter bw(out);
-    // open-addressing table of (prefix code << 8 | byte) -> code, reset by generation
+    // open-addressing table of (prefix code << 8 | byte) -> code; a slot holds generation << 20 | key,
+    // so a Clear only bumps the generation (the table is wiped when the 12-bit generation wraps)
     constexpr int HS = 1 << 14;
-    std::vector<uint32_t> key(HS), gen(HS, 0);
+    std::vector<uint32_t> slot(HS, 0);
     std::vector<uint16_t> val(HS);
     uint32_t g = 1;
     int width = 9;
@@ -70,22 +71,22 @@ void lzw_encode(const uint8_t* in, size_t len, std::vector<uint8_t>& out) {
     unsigned w = in[0];
     for (size_t i = 1; i < len; i++) {
         const unsigned k = in[i];
-        const uint32_t kk = (w << 8) | k;
+        const uint32_t kk = (w << 8) | k, tag = (g << 20) | kk;
         uint32_t h = (kk * 2654435761u) >> 18;
         bool found = false;
-        while (gen[h] == g) {
-            if (key[h] == kk) { found = true; break; }
-            h = (h + 1) & (HS - 1);
-        }
+        for (uint32_t v; ((v = slot[h]) >> 20) == g; h = (h + 1) & (HS - 1))
+            if (v == tag) { found = true; break; }
         if (found) { w = val[h]; continue; }
         bw.put(w, width);
-        gen[h] = g;
-        key[h] = kk;
+        slot[h] = tag;
         val[h] = (uint16_t)next;
         next++;
         if (next == 4094) {
             bw.put(256, width);
-            g++;
+            if (++g == 4096) {
+                std::fill(slot.begin(), slot.end(), 0u);
+                g = 1;
+            }
             next = 258;
             width = 9;
         } else if (next > (1u << width) - 1) {
@@ -105,46 +106,45 @@ void lzw_encode(const uint8_t* in, size_t len, std::vector<uint8_t>& out) {
     bw.flush();
 }
 
-// decodes at most cap bytes into out; returns the bytes written or -1 for a corrupt stream
+// Decodes at most cap bytes into out; returns the bytes written or -1 for a corrupt stream.  Every
+// table string is a run of the output already written (the previous string plus the first byte
+// of the next), so a code is emitted by copying that run: each entry keeps its offset and length.
 long long lzw_decode(const uint8_t* in, size_t len, uint8_t* out, size_t cap) {
-    std::vector<uint16_t> prefix(4096);
-    std::vector<uint8_t> suffix(4096), first(4096);
-    std::vector<uint16_t> length(4096);
-    for (int i = 0; i < 256; i++) { prefix[i] = 0xffff; suffix[i] = (uint8_t)i; first[i] = (uint8_t)i; length[i] = 1; }
-    size_t pos = 0, o = 0;
-    const size_t nbits = len * 8;
+    uint32_t off[4096];
+    uint32_t length[4096];
+    size_t ip = 0, o = 0;
+    uint64_t bits = 0;
+    int nb = 0;
     int width = 9;
     unsigned next = 258;
     int prev = -1;
     auto get = [&](int w) -> unsigned {
-        if (pos + w > nbits) return 257;
-        unsigned v = 0;
-        size_t byte = pos >> 3;
-        const int sh = (int)(pos & 7);
-        // up to 12 + 7 bits: read 3 bytes
-        uint32_t chunk = (uint32_t)in[byte] << 16;
-        if (byte + 1 < len) chunk |= (uint32_t)in[byte + 1] << 8;
-        if (byte + 2 < len) chunk |= (uint32_t)in[byte + 2];
-        v = (chunk >> (24 - sh - w)) & ((1u << w) - 1);
-        pos += w;
-        return v;
-    };
-    auto emit = [&](unsigned code) -> bool {
-        const unsigned L = length[code];
-        if (o + L > cap) {
-            // write the part that fits (the strip is full)
-            std::vector<uint8_t> tmp(L);
-            unsigned c = code;
-            for (int i = (int)L - 1; i >= 0; i--) { tmp[i] = suffix[c]; c = prefix[c]; }
-            const size_t n = cap - o;
-            memcpy(out + o, tmp.data(), n);
-            o = cap;
-            return false;
+        if (nb < w) {
+            while (nb <= 56 && ip < len) {
+                bits = (bits << 8) | in[ip++];
+                nb += 8;
+            }
+            if (nb < w) return 257;                   // out of input: as EndOfInformation
         }
-        unsigned c = code;
-        for (int i = (int)L - 1; i >= 0; i--) { out[o + i] = suffix[c]; c = prefix[c]; }
-        o += L;
-        return true;
+        nb -= w;
+        return (unsigned)(bits >> nb) & ((1u << w) - 1);
+    };
+    // write string `code` at o (a literal, or a copy of its earlier run); false once the strip is full
+    auto emit = [&](unsigned code) -> bool {
+        if (code < 256) {
+            if (o >= cap) return false;
+            out[o++] = (uint8_t)code;
+            return o < cap;
+        }
+        const size_t L = length[code], n = std::min<size_t>(L, cap - o);
+        const uint8_t* src = out + off[code];    // the run ends at or before o: no overlap
+        if (n <= 16) {
+            for (size_t i = 0; i < n; i++) out[o + i] = src[i];
+        } else {
+            memcpy(out + o, src, n);
+        }
+        o += n;
+        return n == L && o < cap;
     };
     while (true) {
         unsigned code = get(width);
@@ -153,37 +153,37 @@ long long lzw_decode(const uint8_t* in, size_t len, uint8_t* out, size_t cap) {
             width = 9;
             next = 258;
             prev = -1;
-            code = get(width);
-            if (code == 257) break;
+            continue;
+        }
+        const size_t start = o;
+        if (prev < 0) {                            // the first code after Clear (or a stream without one)
             if (code >= 256) return -1;
             if (!emit(code)) break;
             prev = (int)code;
             continue;
         }
-        if (prev < 0) {                       // a stream that does not start with Clear
-            if (code >= 256) return -1;
-            if (!emit(code)) break;
-            prev = (int)code;
-            continue;
-        }
+        const size_t plen = prev < 256 ? 1 : length[prev];
         if (code < next) {
-            if (next < 4096) {
-                prefix[next] = (uint16_t)prev;
-                suffix[next] = first[code];
-                first[next] = first[prev];
-                length[next] = (uint16_t)(length[prev] + 1);
-                next++;
+            if (!emit(code)) {
+                o = std::min(o, cap);
+                break;
             }
-            if (!emit(code)) break;
         } else if (code == next && next < 4096) {
-            prefix[next] = (uint16_t)prev;
-            suffix[next] = first[prev];
-            first[next] = first[prev];
-            length[next] = (uint16_t)(length[prev] + 1);
-            next++;
-            if (!emit(code)) break;
+            // KwKwK: the previous string followed by its own first byte
+            const size_t pstart = start - plen;
+            const size_t n = std::min(plen, cap - o);
+            memcpy(out + o, out + pstart, n);
+            o += n;
+            if (o >= cap) break;
+            out[o++] = out[pstart];
+            if (o >= cap) break;
         } else {
             return -1;
+        }
+        if (next < 4096) {                         // previous string + first byte of this one
+            off[next] = (uint32_t)(start - plen);
+            length[next] = (uint32_t)(plen + 1);
+            next++;
         }
         prev = (int)code;
         if (next == (1u << width) - 1 && width < 12) width++;
@@ -344,15 +344,56 @@ void swap_bytes(uint8_t* p, size_t n, int es) {
 }
 
 // rows [r0, r0 + nr) of page z (row-major, row stride w) into the column-major output [h w nz]
-void scatter_rows(const uint8_t* rows, uint64_t r0, uint64_t nr, uint64_t w, uint64_t h, uint64_t z, int es, uint8_t* out) {
-    const uint64_t plane = w * h;
-    for (uint64_t x0 = 0; x0 < w; x0 += 64) {
-        const uint64_t x1 = std::min(w, x0 + 64);
-        for (uint64_t r = 0; r < nr; r++) {
-            const uint8_t* src = rows + (r * w + x0) * es;
-            uint8_t* dst = out + ((z * plane) + x0 * h + r0 + r) * es;
-            for (uint64_t x = x0; x < x1; x++, src += es, dst += h * es) memcpy(dst, src, es);
+// Transpose of an nr x w row-major block (row stride w) into a column-major array with column
+// stride h, in 32 x 32 tiles so that both sides stay in cache.
+template <typename T>
+void transpose_block(const T* src, uint64_t nr, uint64_t w, T* dst, uint64_t h) {
+    constexpr uint64_t B = 32;
+    for (uint64_t r0 = 0; r0 < nr; r0 += B) {
+        const uint64_t r1 = std::min(nr, r0 + B);
+        for (uint64_t x0 = 0; x0 < w; x0 += B) {
+            const uint64_t x1 = std::min(w, x0 + B);
+            for (uint64_t x = x0; x < x1; x++) {
+                const T* s = src + x;
+                T* d = dst + x * h;
+                for (uint64_t r = r0; r < r1; r++) d[r] = s[r * w];
+            }
         }
+    }
+}
+
+// rows [r0, r0 + nr) of page z (row-major, row stride w) into the column-major output [h w nz]
+void scatter_rows(const uint8_t* rows, uint64_t r0, uint64_t nr, uint64_t w, uint64_t h, uint64_t z, int es, uint8_t* out) {
+    const uint64_t base = z * w * h + r0;
+    switch (es) {
+        case 1: transpose_block((const uint8_t*)rows, nr, w, (uint8_t*)out + base, h); break;
+        case 2: transpose_block((const uint16_t*)rows, nr, w, (uint16_t*)out + base, h); break;
+        case 4: transpose_block((const uint32_t*)rows, nr, w, (uint32_t*)out + base, h); break;
+        default: transpose_block((const uint64_t*)rows, nr, w, (uint64_t*)out + base, h); break;
+    }
+}
+
+// column-major rows [r0, r0 + nr) of a plane (column stride h) into a row-major strip (row stride w)
+void gather_rows(const uint8_t* plane, uint64_t r0, uint64_t nr, uint64_t w, uint64_t h, int es, uint8_t* rows) {
+    auto go = [&](auto tag) {
+        using T = decltype(tag);
+        const T* src = (const T*)plane + r0;
+        T* dst = (T*)rows;
+        constexpr uint64_t B = 32;
+        for (uint64_t x0 = 0; x0 < w; x0 += B) {
+            const uint64_t x1 = std::min(w, x0 + B);
+            for (uint64_t q0 = 0; q0 < nr; q0 += B) {
+                const uint64_t q1 = std::min(nr, q0 + B);
+                for (uint64_t x = x0; x < x1; x++)
+                    for (uint64_t r = q0; r < q1; r++) dst[r * w + x] = src[x * h + r];
+            }
+        }
+    };
+    switch (es) {
+        case 1: go(uint8_t()); break;
+        case 2: go(uint16_t()); break;
+        case 4: go(uint32_t()); break;
+        default: go(uint64_t()); break;
     }
 }
 
@@ -498,12 +539,7 @@ extern "C" pk_status pk_tiff_write(const char* path, const void* data, const int
     parallel_for(nz * ns, n_threads(threads), [&](size_t t) {
         const uint64_t z = t / ns, k = t % ns, r0 = k * rps, nr = std::min(rps, h - r0);
         std::vector<uint8_t> rows(nr * w * es);
-        const uint8_t* src = (const uint8_t*)data + z * w * h * es;
-        for (uint64_t x0 = 0; x0 < w; x0 += 64) {
-            const uint64_t x1 = std::min(w, x0 + 64);
-            for (uint64_t r = 0; r < nr; r++)
-                for (uint64_t x = x0; x < x1; x++) memcpy(&rows[(r * w + x) * es], src + (x * h + r0 + r) * es, es);
-        }
+        gather_rows((const uint8_t*)data + z * w * h * es, r0, nr, w, h, es, rows.data());
         if (lzw) lzw_encode(rows.data(), rows.size(), strips[t]);
         else strips[t].swap(rows);
     });
