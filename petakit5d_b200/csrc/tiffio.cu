@@ -50,16 +50,31 @@ struct BitWriter {
     }
 };
 
-void lzw_encode(const uint8_t* in, size_t len, std::vector<uint8_t>& out) {
-    out.clear();
-    out.reserve(len / 2 + 64);
+// open-addressing table of (prefix code << 8 | byte) -> code, kept by each worker thread across
+// strips; a slot holds generation << 20 | key, so a new table (a Clear, a new strip) only bumps the
+// generation, and the slots are wiped when the 12-bit generation wraps
+struct LzwTable {
+    static constexpr int HS = 1 << 14;
+    std::vector<uint32_t> slot = std::vector<uint32_t>(HS, 0u);
+    std::vector<uint16_t> val = std::vector<uint16_t>(HS);
+    uint32_t g = 0;
+    void fresh() {
+        if (++g == 4096) {
+            std::fill(slot.begin(), slot.end(), 0u);
+            g = 1;
+        }
+    }
+};
+
+// appends the LZW stream of in[0, len) to out
+void lzw_encode(const uint8_t* in, size_t len, std::vector<uint8_t>& out, LzwTable& tb) {
+    out.reserve(out.size() + len / 2 + 64);
     BitWriter bw(out);
-    // open-addressing table of (prefix code << 8 | byte) -> code; a slot holds generation << 20 | key,
-    // so a Clear only bumps the generation (the table is wiped when the 12-bit generation wraps)
-    constexpr int HS = 1 << 14;
-    std::vector<uint32_t> slot(HS, 0);
-    std::vector<uint16_t> val(HS);
-    uint32_t g = 1;
+    constexpr int HS = LzwTable::HS;
+    uint32_t* slot = tb.slot.data();
+    uint16_t* val = tb.val.data();
+    tb.fresh();
+    uint32_t g = tb.g;
     int width = 9;
     unsigned next = 258;
     bw.put(256, width);
@@ -83,10 +98,8 @@ void lzw_encode(const uint8_t* in, size_t len, std::vector<uint8_t>& out) {
         next++;
         if (next == 4094) {
             bw.put(256, width);
-            if (++g == 4096) {
-                std::fill(slot.begin(), slot.end(), 0u);
-                g = 1;
-            }
+            tb.fresh();
+            g = tb.g;
             next = 258;
             width = 9;
         } else if (next > (1u << width) - 1) {
@@ -403,14 +416,16 @@ int n_threads(int req) {
     return (int)std::max(1u, std::min(hc, 64u));
 }
 
+// fn(task, worker): tasks handed out in order to `threads` workers (a worker index lets each keep
+// its buffers across tasks instead of allocating per strip)
 template <typename F>
 void parallel_for(size_t n, int threads, F&& fn) {
     std::atomic<size_t> next(0);
     std::vector<std::thread> pool;
     const int T = (int)std::min<size_t>(n, (size_t)threads);
     for (int t = 0; t < T; t++)
-        pool.emplace_back([&]() {
-            for (size_t i = next++; i < n; i = next++) fn(i);
+        pool.emplace_back([&, t]() {
+            for (size_t i = next++; i < n; i = next++) fn(i, t);
         });
     for (auto& th : pool) th.join();
 }
@@ -472,8 +487,10 @@ extern "C" pk_status pk_tiff_read(const char* path, const int64_t* z_range, void
     if (ij) {
         if ((s = check_page(p0, p0)) != PK_OK) return s;
         const uint64_t pb = w * h * es, base = p0.off[0];
-        parallel_for(z1 - z0, T, [&](size_t k) {
-            std::vector<uint8_t> page(pb);
+        std::vector<std::vector<uint8_t>> pages(T);
+        parallel_for(z1 - z0, T, [&](size_t k, int t) {
+            std::vector<uint8_t>& page = pages[t];
+            page.resize(pb);
             if (!f.rd(base + (z0 + k) * pb, page.data(), pb)) { err = 1; return; }
             if (f.swap && es > 1) swap_bytes(page.data(), pb, es);
             scatter_rows(page.data(), 0, h, w, h, k, es, (uint8_t*)out);
@@ -489,13 +506,17 @@ extern "C" pk_status pk_tiff_read(const char* path, const int64_t* z_range, void
         const uint64_t ns = (h + f.pages[z].rows - 1) / f.pages[z].rows;
         for (uint64_t k = 0; k < ns; k++) tasks.push_back({z, k});
     }
-    parallel_for(tasks.size(), T, [&](size_t t) {
+    std::vector<std::vector<uint8_t>> raws(T), rowss(T);
+    parallel_for(tasks.size(), T, [&](size_t t, int worker) {
         if (err) return;
         const uint64_t z = tasks[t].first, k = tasks[t].second;
         const Page& p = f.pages[z];
         const uint64_t r0 = k * p.rows, nr = std::min(p.rows, h - r0);
         const uint64_t want = nr * w * es;
-        std::vector<uint8_t> raw(p.cnt[k]), rows(want);
+        std::vector<uint8_t>& raw = raws[worker];
+        std::vector<uint8_t>& rows = rowss[worker];
+        raw.resize(p.cnt[k]);
+        rows.resize(want);
         if (!f.rd(p.off[k], raw.data(), raw.size())) { err = 2; return; }
         if (p.comp == 1) {
             if (raw.size() < want) { err = 2; return; }
@@ -535,13 +556,26 @@ extern "C" pk_status pk_tiff_write(const char* path, const void* data, const int
     const int es = bits / 8;
     const uint64_t rps = 512, ns = (h + rps - 1) / rps;
     // strips: transpose the column-major plane rows into row-major strips, compress in parallel
-    std::vector<std::vector<uint8_t>> strips(nz * ns);
-    parallel_for(nz * ns, n_threads(threads), [&](size_t t) {
+    // each worker appends its strips to an arena of its own (no allocation per strip)
+    const int T = (int)std::min<uint64_t>(nz * ns, (uint64_t)n_threads(threads));
+    std::vector<std::vector<uint8_t>> arena(T), rowss(T);
+    std::vector<LzwTable> tables(lzw ? T : 0);
+    struct StripRef { int worker; size_t off, size; };
+    std::vector<StripRef> strips(nz * ns);
+    parallel_for(nz * ns, T, [&](size_t t, int worker) {
         const uint64_t z = t / ns, k = t % ns, r0 = k * rps, nr = std::min(rps, h - r0);
-        std::vector<uint8_t> rows(nr * w * es);
-        gather_rows((const uint8_t*)data + z * w * h * es, r0, nr, w, h, es, rows.data());
-        if (lzw) lzw_encode(rows.data(), rows.size(), strips[t]);
-        else strips[t].swap(rows);
+        std::vector<uint8_t>& a = arena[worker];
+        const size_t at = a.size();
+        if (lzw) {
+            std::vector<uint8_t>& rows = rowss[worker];
+            rows.resize(nr * w * es);
+            gather_rows((const uint8_t*)data + z * w * h * es, r0, nr, w, h, es, rows.data());
+            lzw_encode(rows.data(), rows.size(), a, tables[worker]);
+        } else {
+            a.resize(at + nr * w * es);
+            gather_rows((const uint8_t*)data + z * w * h * es, r0, nr, w, h, es, a.data() + at);
+        }
+        strips[t] = {worker, at, a.size() - at};
     });
     const int fd = open(path, O_WRONLY | O_CREAT | O_TRUNC, 0644);
     if (fd < 0) return pk_fail(PK_ERR_INVALID, std::string("cannot create \"") + path + "\"");
@@ -550,8 +584,8 @@ extern "C" pk_status pk_tiff_write(const char* path, const void* data, const int
     std::vector<uint64_t> soff(nz * ns);
     for (size_t t = 0; t < strips.size(); t++) {
         soff[t] = pos;
-        o.put(pos, strips[t].data(), strips[t].size());
-        pos += strips[t].size();
+        o.put(pos, arena[strips[t].worker].data() + strips[t].off, strips[t].size);
+        pos += strips[t].size;
     }
     pos = (pos + 7) & ~7ull;
     const uint64_t first_ifd = pos;
@@ -579,7 +613,7 @@ extern "C" pk_status pk_tiff_write(const char* path, const void* data, const int
         ent(273, 16, ns, ns > 1 ? arr : soff[z * ns]);
         ent(277, 3, 1, 1);
         ent(278, 4, 1, rps);
-        ent(279, 16, ns, ns > 1 ? arr + 8 * ns : strips[z * ns].size());
+        ent(279, 16, ns, ns > 1 ? arr + 8 * ns : strips[z * ns].size);
         ent(284, 3, 1, 1);
         ent(339, 3, 1, is_float ? 3 : 1);
         memcpy(b.data() + 8 + NE * 20, &next, 8);
@@ -589,7 +623,7 @@ extern "C" pk_status pk_tiff_write(const char* path, const void* data, const int
             std::vector<uint64_t> a(2 * ns);
             for (uint64_t k = 0; k < ns; k++) {
                 a[k] = soff[z * ns + k];
-                a[ns + k] = strips[z * ns + k].size();
+                a[ns + k] = strips[z * ns + k].size;
             }
             o.put(pos, a.data(), 16 * ns);
             pos += 16 * ns;
