@@ -108,6 +108,8 @@ static void release_all(pk_ctx* ctx) {
     }
     for (auto& kv : ctx->tickets) cudaEventDestroy(kv.second);
     ctx->tickets.clear();
+    for (auto& kv : ctx->dev_tables) cudaFree(kv.second);
+    ctx->dev_tables.clear();
     for (auto e : ctx->io_ev) cudaEventDestroy(e);
     ctx->io_ev.clear();
     pk_release_graphs(ctx);

@@ -15,6 +15,7 @@
 //   the float64 coordinates and float32 weights as the MEX files form them; no fused multiply-adds.
 // Rows whose source falls outside the volume are zero.
 #include <algorithm>
+#include <cstdio>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -473,19 +474,30 @@ pk_status dsr_run(pk_ctx* ctx, const void* d_in, pk_dtype t, const int64_t dims[
         skew_tables(nz, P, reverse, zindex, zorig, sl);
         const int nint = (int)sl.size();
         const size_t ie = (t == PK_U16 && u16_out) ? 2 : 4;
-        void *dint, *dtab;
-        const size_t tb = sizeof(SkewSlice) * std::max<size_t>(1, sl.size()) + 4 * zindex.size() + zorig.size() + 64;
+        void* dint;
+        const size_t nsl = std::max<size_t>(1, sl.size());
         if ((s = pk_scratch(ctx, 25, ie * (size_t)ny * nx * std::max(1, nint), &dint)) != PK_OK) return s;
-        if ((s = pk_scratch(ctx, 26, tb, &dtab)) != PK_OK) return s;
+        // the slice tables depend only on the geometry: built and uploaded once per context
+        char key[160];
+        snprintf(key, sizeof(key), "dsr:%d:%a:%a:%d", nz, P.stepsize, P.xstep, reverse);
+        void*& dtab = ctx->dev_tables[key];
+        if (!dtab) {
+            const size_t tb = sizeof(SkewSlice) * nsl + 4 * zindex.size() + zorig.size();
+            std::vector<char> host(tb, 0);
+            memcpy(host.data(), sl.data(), sizeof(SkewSlice) * sl.size());
+            memcpy(host.data() + sizeof(SkewSlice) * nsl, zindex.data(), 4 * zindex.size());
+            memcpy(host.data() + sizeof(SkewSlice) * nsl + 4 * zindex.size(), zorig.data(), zorig.size());
+            if (cudaMalloc(&dtab, tb) != cudaSuccess) {
+                cudaGetLastError();
+                ctx->dev_tables.erase(key);
+                return pk_fail(PK_ERR_NOMEM, "deskew: table allocation failed");
+            }
+            PK_CUDA(cudaMemcpy(dtab, host.data(), tb, cudaMemcpyHostToDevice));
+        }
         char* tp = (char*)dtab;
         SkewSlice* dsl = (SkewSlice*)tp;
-        int* dzindex = (int*)(tp + sizeof(SkewSlice) * std::max<size_t>(1, sl.size()));
+        int* dzindex = (int*)(tp + sizeof(SkewSlice) * nsl);
         uint8_t* dzorig = (uint8_t*)(dzindex + zindex.size());
-        if (!sl.empty()) PK_CUDA(cudaMemcpyAsync(dsl, sl.data(), sizeof(SkewSlice) * sl.size(), cudaMemcpyHostToDevice, st));
-        PK_CUDA(cudaMemcpyAsync(dzindex, zindex.data(), 4 * zindex.size(), cudaMemcpyHostToDevice, st));
-        PK_CUDA(cudaMemcpyAsync(dzorig, zorig.data(), zorig.size(), cudaMemcpyHostToDevice, st));
-        // the host tables are temporaries: wait for their copies before they go out of scope
-        PK_CUDA(cudaStreamSynchronize(st));
         const int xa = (int)std::ceil(P.xstep);
         const int g = grid_rows((long long)nint * nx);
         if (nint > 0) {

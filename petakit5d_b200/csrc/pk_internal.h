@@ -160,6 +160,8 @@ struct pk_ctx {
         bool used = false;
     };
     AsyncSlot aslot[2];
+    // small read-only device tables built once per parameter set (e.g. the deskew's skewed-slice table)
+    std::map<std::string, void*> dev_tables;
     long long next_ticket = 1;
     std::map<long long, cudaEvent_t> tickets;                  // ticket -> its download's event
 };
