@@ -235,6 +235,21 @@ PK_API pk_status pk_tiff_read(const char* path, const int64_t* z_range, void* ou
  * writetiff default) or none; bits 8/16/32/64, is_float for single/double. */
 PK_API pk_status pk_tiff_write(const char* path, const void* data, const int64_t dims[3], int32_t bits,
                                int32_t is_float, int32_t lzw, int32_t threads);
+/* Zarr v2 volumes (io/readzarr.m, io/writezarr.m over io/cpp-zarr/src/parallelreadzarr.cpp,
+ * parallelwritezarr.cpp).  An array of shape [ny nx nz] is the MATLAB array [ny nx nz]; chunks in
+ * order "F" or "C", keys "i.j.k" or "i/j/k", compressor none, "zlib" or "gzip" (the reference's default
+ * "blosc" gives PK_ERR_UNSUPPORTED: no blosc library in this build).  pk_zarr_read: the whole array or
+ * bbox [y1 x1 z1 y2 x2 z2] (1-based inclusive; NULL = all) into out (column-major, the array's type);
+ * missing chunks read as fill_value.  pk_zarr_write: order "F", separator ".", chunks = min(chunks, dims),
+ * compressor 0 = none, 1 = zlib, 2 = gzip (level 1); chunks compressed on `threads` host threads. */
+PK_API pk_status pk_zarr_info(const char* path, int64_t dims[3], int64_t chunks[3], int32_t* bits, int32_t* is_float);
+PK_API pk_status pk_zarr_read(const char* path, const int64_t* bbox, void* out, int64_t out_bytes, int32_t threads);
+PK_API pk_status pk_zarr_write(const char* path, const void* data, const int64_t dims[3], int32_t bits,
+                               int32_t is_float, const int64_t chunks[3], int32_t compressor, int32_t threads);
+/* Writes a region [y1 x1 z1 y2 x2 z2] (1-based inclusive) of an existing order-F Zarr array from a
+ * column-major buffer of the region's size; the region must cover whole chunks (it may end at the
+ * array's edge) -- the chunk-aligned batches of the large-file runners. */
+PK_API pk_status pk_zarr_write_region(const char* path, const void* data, const int64_t bbox[6], int32_t threads);
 /* Page-locked host buffers (cudaHostAlloc) for file reads that feed the GPU. */
 PK_API pk_status pk_host_alloc(int64_t bytes, void** ptr);
 PK_API pk_status pk_host_free(void* ptr);

@@ -8,6 +8,10 @@ deconvolution path so that the CUDA library can be checked against them:
 * ``backprojector.py`` -- omw_backprojector_generation and the Wiener-Butterworth BackProjector.
 * ``chunking.py``      -- findGoodFactorNumber and XR_zarrChunkCoordinatesExtraction.
 * ``morph.py``         -- the binary morphology the OMW backprojector needs.
+* ``psfgen.py``        -- psf_gen_new and the PSF crops of RLdecon.
+* ``deskew.py``        -- deskewRotateFrame3D and its two MEX files.
+* ``tiff.py``          -- TIFF / BigTIFF with TIFF LZW.
+* ``zarrio.py``        -- Zarr v2 arrays (json, zlib, gzip).
 
 Parity status: **unpinned**.  The reference is pure MATLAB (no MATLAB/Octave here) and ships no
 test, golden vector or fixture for this path, so the restatement is pinned only by following the

@@ -94,6 +94,11 @@ _SIGS = {
     "pk_tiff_info": (C.c_int, [C.c_char_p, C.POINTER(C.c_int64), C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "pk_tiff_read": (C.c_int, [C.c_char_p, P, P, C.c_int64, C.c_int32]),
     "pk_tiff_write": (C.c_int, [C.c_char_p, P, I64x3, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
+    "pk_zarr_info": (C.c_int, [C.c_char_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int32),
+                               C.POINTER(C.c_int32)]),
+    "pk_zarr_read": (C.c_int, [C.c_char_p, P, P, C.c_int64, C.c_int32]),
+    "pk_zarr_write": (C.c_int, [C.c_char_p, P, I64x3, C.c_int32, C.c_int32, I64x3, C.c_int32, C.c_int32]),
+    "pk_zarr_write_region": (C.c_int, [C.c_char_p, P, P, C.c_int32]),
     "pk_host_alloc": (C.c_int, [C.c_int64, C.POINTER(C.c_void_p)]),
     "pk_host_free": (C.c_int, [P]),
     "pk_edge_erosion_edt": (C.c_int, [P, P, C.c_int, I64x3, C.c_int32, P, C.c_int, P]),

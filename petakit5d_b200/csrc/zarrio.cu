@@ -1,0 +1,453 @@
+// Zarr (v2) volumes either side of the deconvolution: the reference's readzarr / writezarr
+// (io/readzarr.m, io/writezarr.m over io/cpp-zarr/src/parallelreadzarr.cpp, parallelwritezarr.cpp),
+// re-implemented from the Zarr v2 storage specification.
+//
+//   * A MATLAB array [ny nx nz] is the Zarr array of shape [ny, nx, nz] (the reference writes order
+//     "F" with chunk keys "i.j.k" in the same axis order); chunks are read in either order ("F" or "C")
+//     and with either key separator ("." or "/").
+//   * Compressors: none, "zlib" and "gzip" (zlib is in this image).  The reference's default,
+//     "blosc" (with zstd or lz4 inside), is rejected with PK_ERR_UNSUPPORTED: no blosc library is here.
+//   * Reading: the chunks that meet the requested box are decoded in parallel (one task per chunk, a
+//     pool of host threads) and their intersection copied into the column-major output; a missing
+//     chunk file reads as fill_value.  Writing: full-size chunks (edges padded with 0), zlib level 1
+//     or none, compressed in parallel.
+#include <fcntl.h>
+#include <sys/stat.h>
+#include <unistd.h>
+#include <zlib.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cerrno>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "pk_internal.h"
+
+namespace {
+
+struct ZMeta {
+    int64_t shape[3] = {1, 1, 1}, chunks[3] = {1, 1, 1};
+    int ndim = 0;
+    int es = 0;                 // element bytes
+    char kind = 'u';            // 'u' unsigned, 'i' signed, 'f' float
+    bool big_endian = false;
+    bool order_c = false;
+    std::string compressor;     // "", "zlib", "gzip", or another id (unsupported)
+    std::string separator = ".";
+    double fill = 0.0;
+};
+
+// ---- a small reader for the .zarray JSON object (the keys this file needs)
+size_t skip_ws(const std::string& s, size_t i) {
+    while (i < s.size() && (s[i] == ' ' || s[i] == '\n' || s[i] == '\r' || s[i] == '\t')) i++;
+    return i;
+}
+
+// position just after the value of "key" at the top level of the object, or npos
+size_t find_key(const std::string& s, const std::string& key) {
+    int depth = 0;
+    bool in_str = false;
+    for (size_t i = 0; i < s.size(); i++) {
+        const char c = s[i];
+        if (in_str) {
+            if (c == '\\') { i++; continue; }
+            if (c == '"') in_str = false;
+            continue;
+        }
+        if (c == '{' || c == '[') depth++;
+        else if (c == '}' || c == ']') depth--;
+        else if (c == '"') {
+            if (depth == 1 && s.compare(i + 1, key.size(), key) == 0 && i + 1 + key.size() < s.size() &&
+                s[i + 1 + key.size()] == '"') {
+                size_t j = skip_ws(s, i + 2 + key.size());
+                if (j < s.size() && s[j] == ':') return skip_ws(s, j + 1);
+            }
+            in_str = true;
+        }
+    }
+    return std::string::npos;
+}
+
+bool read_ints(const std::string& s, size_t i, int64_t* out, int* n) {
+    if (i == std::string::npos || s[i] != '[') return false;
+    *n = 0;
+    i++;
+    while (i < s.size() && s[i] != ']') {
+        i = skip_ws(s, i);
+        if (s[i] == ']') break;
+        char* end;
+        const long long v = strtoll(s.c_str() + i, &end, 10);
+        if (end == s.c_str() + i || *n >= 3) return false;
+        out[(*n)++] = v;
+        i = skip_ws(s, (size_t)(end - s.c_str()));
+        if (s[i] == ',') i++;
+    }
+    return *n > 0;
+}
+
+std::string read_str(const std::string& s, size_t i) {
+    if (i == std::string::npos || s[i] != '"') return std::string();
+    const size_t j = s.find('"', i + 1);
+    return j == std::string::npos ? std::string() : s.substr(i + 1, j - i - 1);
+}
+
+bool read_file(const std::string& path, std::vector<uint8_t>& buf) {
+    const int fd = open(path.c_str(), O_RDONLY);
+    if (fd < 0) return false;
+    struct stat sb;
+    fstat(fd, &sb);
+    buf.resize((size_t)sb.st_size);
+    size_t got = 0;
+    while (got < buf.size()) {
+        const ssize_t r = read(fd, buf.data() + got, buf.size() - got);
+        if (r <= 0) break;
+        got += (size_t)r;
+    }
+    close(fd);
+    return got == buf.size();
+}
+
+bool write_file(const std::string& path, const void* p, size_t n) {
+    const int fd = open(path.c_str(), O_WRONLY | O_CREAT | O_TRUNC, 0644);
+    if (fd < 0) return false;
+    size_t done = 0;
+    while (done < n) {
+        const ssize_t r = write(fd, (const char*)p + done, n - done);
+        if (r <= 0) break;
+        done += (size_t)r;
+    }
+    close(fd);
+    return done == n;
+}
+
+pk_status parse_meta(const char* path, ZMeta& m) {
+    std::vector<uint8_t> raw;
+    if (!read_file(std::string(path) + "/.zarray", raw))
+        return pk_fail(PK_ERR_INVALID, std::string("zarr file ") + path + " does not exist (no .zarray)");
+    const std::string s(raw.begin(), raw.end());
+    int n = 0, nc = 0;
+    if (!read_ints(s, find_key(s, "shape"), m.shape, &n) || !read_ints(s, find_key(s, "chunks"), m.chunks, &nc) || n != nc)
+        return pk_fail(PK_ERR_INVALID, "zarr: bad shape / chunks in .zarray");
+    m.ndim = n;
+    for (int k = n; k < 3; k++) m.shape[k] = m.chunks[k] = 1;
+    const std::string dt = read_str(s, find_key(s, "dtype"));
+    if (dt.size() < 3) return pk_fail(PK_ERR_INVALID, "zarr: bad dtype");
+    m.big_endian = dt[0] == '>';
+    m.kind = dt[1];
+    m.es = atoi(dt.c_str() + 2);
+    if (!((m.kind == 'u' && (m.es == 1 || m.es == 2 || m.es == 4)) || (m.kind == 'f' && (m.es == 4 || m.es == 8))))
+        return pk_fail(PK_ERR_UNSUPPORTED, "zarr: dtype " + dt + " is not supported");
+    m.order_c = read_str(s, find_key(s, "order")) == "C";
+    const size_t sep = find_key(s, "dimension_separator");
+    if (sep != std::string::npos && s[sep] == '"') m.separator = read_str(s, sep);
+    const size_t ci = find_key(s, "compressor");
+    if (ci != std::string::npos && s[ci] == '{') {
+        const size_t ce = s.find('}', ci);
+        const std::string obj = s.substr(ci, ce - ci + 1);     // the compressor object: its "id"
+        m.compressor = read_str(obj, find_key(obj, "id"));
+    }
+    const size_t fi = find_key(s, "fill_value");
+    if (fi != std::string::npos && s[fi] != 'n' && s[fi] != '"') m.fill = strtod(s.c_str() + fi, nullptr);
+    if (!m.compressor.empty() && m.compressor != "zlib" && m.compressor != "gzip")
+        return pk_fail(PK_ERR_UNSUPPORTED, "zarr: compressor \"" + m.compressor +
+                                               "\" is not supported here (none, zlib and gzip are; blosc is not in this image)");
+    return PK_OK;
+}
+
+}  // namespace
+
+namespace {
+
+std::string chunk_key(const ZMeta& m, const int64_t c[3]) {
+    std::string k = std::to_string(c[0]);
+    for (int d = 1; d < m.ndim; d++) k += m.separator + std::to_string(c[d]);
+    return k;
+}
+
+// decompress one chunk file into `out` (chunk bytes); false for a corrupt file
+bool decode_chunk(const ZMeta& m, const std::vector<uint8_t>& raw, std::vector<uint8_t>& out) {
+    if (m.compressor.empty()) {
+        if (raw.size() < out.size()) return false;
+        memcpy(out.data(), raw.data(), out.size());
+        return true;
+    }
+    z_stream zs;
+    memset(&zs, 0, sizeof(zs));
+    if (inflateInit2(&zs, m.compressor == "gzip" ? 16 + MAX_WBITS : MAX_WBITS) != Z_OK) return false;
+    zs.next_in = const_cast<Bytef*>(raw.data());
+    zs.avail_in = (uInt)raw.size();
+    zs.next_out = out.data();
+    zs.avail_out = (uInt)out.size();
+    const int r = inflate(&zs, Z_FINISH);
+    inflateEnd(&zs);
+    return (r == Z_STREAM_END || r == Z_BUF_ERROR) && zs.avail_out == 0;
+}
+
+void byteswap(uint8_t* p, size_t n, int es) {
+    if (es == 1) return;
+    for (size_t i = 0; i < n; i += es) std::reverse(p + i, p + i + es);
+}
+
+template <typename T>
+void fill_value(T* p, size_t n, double v) {
+    const T t = (T)v;
+    for (size_t i = 0; i < n; i++) p[i] = t;
+}
+
+void fill_bytes(uint8_t* p, size_t n, const ZMeta& m) {
+    if (m.fill == 0.0) { memset(p, 0, n * m.es); return; }
+    if (m.kind == 'f') {
+        if (m.es == 4) fill_value((float*)p, n, m.fill);
+        else fill_value((double*)p, n, m.fill);
+    } else if (m.es == 1) fill_value((uint8_t*)p, n, m.fill);
+    else if (m.es == 2) fill_value((uint16_t*)p, n, m.fill);
+    else fill_value((uint32_t*)p, n, m.fill);
+}
+
+template <typename F>
+void pfor(size_t n, int threads, F&& fn) {
+    std::atomic<size_t> next(0);
+    std::vector<std::thread> pool;
+    const int T = (int)std::min<size_t>(n, (size_t)std::max(1, threads));
+    for (int t = 0; t < T; t++)
+        pool.emplace_back([&, t]() {
+            for (size_t i = next++; i < n; i = next++) fn(i, t);
+        });
+    for (auto& th : pool) th.join();
+}
+
+int nthreads(int req) {
+    if (req > 0) return req;
+    return (int)std::max(1u, std::min(std::thread::hardware_concurrency(), 64u));
+}
+
+bool make_dir(const std::string& p) { return mkdir(p.c_str(), 0755) == 0 || errno == EEXIST; }
+
+}  // namespace
+
+extern "C" pk_status pk_zarr_info(const char* path, int64_t dims[3], int64_t chunks[3], int32_t* bits, int32_t* is_float) {
+    if (!path || !dims) return pk_fail(PK_ERR_INVALID, "NULL path/dims");
+    ZMeta m;
+    pk_status s = parse_meta(path, m);
+    if (s != PK_OK) return s;
+    for (int k = 0; k < 3; k++) {
+        dims[k] = m.shape[k];
+        if (chunks) chunks[k] = m.chunks[k];
+    }
+    if (bits) *bits = m.es * 8;
+    if (is_float) *is_float = m.kind == 'f';
+    return PK_OK;
+}
+
+extern "C" pk_status pk_zarr_read(const char* path, const int64_t* bbox, void* out, int64_t out_bytes, int32_t threads) {
+    if (!path || !out) return pk_fail(PK_ERR_INVALID, "NULL path/out");
+    ZMeta m;
+    pk_status s = parse_meta(path, m);
+    if (s != PK_OK) return s;
+    int64_t lo[3] = {0, 0, 0}, hi[3] = {m.shape[0], m.shape[1], m.shape[2]};   // [lo, hi) 0-based
+    if (bbox) {
+        for (int d = 0; d < 3; d++) {
+            if (bbox[d] < 1 || bbox[d + 3] > m.shape[d] || bbox[d + 3] < bbox[d])
+                return pk_fail(PK_ERR_INVALID, "zarr: the bounding box is outside the array");
+            lo[d] = bbox[d] - 1;
+            hi[d] = bbox[d + 3];
+        }
+    }
+    const int64_t oy = hi[0] - lo[0], ox = hi[1] - lo[1], oz = hi[2] - lo[2];
+    if ((uint64_t)out_bytes < (uint64_t)(oy * ox * oz) * m.es) return pk_fail(PK_ERR_INVALID, "output buffer too small");
+    int64_t c0[3], c1[3], nc[3];
+    for (int d = 0; d < 3; d++) {
+        c0[d] = lo[d] / m.chunks[d];
+        c1[d] = (hi[d] - 1) / m.chunks[d];
+        nc[d] = c1[d] - c0[d] + 1;
+    }
+    const size_t ntask = (size_t)(nc[0] * nc[1] * nc[2]);
+    const int T = nthreads(threads);
+    const size_t cn = (size_t)(m.chunks[0] * m.chunks[1] * m.chunks[2]);
+    std::vector<std::vector<uint8_t>> raws(T), bufs(T);
+    std::atomic<int> err(0);
+    uint8_t* o = (uint8_t*)out;
+    const int es = m.es;
+    pfor(ntask, T, [&](size_t t, int w) {
+        if (err) return;
+        const int64_t c[3] = {c0[0] + (int64_t)(t % nc[0]), c0[1] + (int64_t)((t / nc[0]) % nc[1]),
+                              c0[2] + (int64_t)(t / (nc[0] * nc[1]))};
+        std::vector<uint8_t>& buf = bufs[w];
+        buf.resize(cn * es);
+        if (read_file(std::string(path) + "/" + chunk_key(m, c), raws[w])) {
+            if (!decode_chunk(m, raws[w], buf)) { err = 1; return; }
+            if (m.big_endian) byteswap(buf.data(), buf.size(), es);
+        } else {
+            fill_bytes(buf.data(), cn, m);                       // a chunk never written: fill_value
+        }
+        // intersection of the chunk with the box, copied run by run along y
+        int64_t a[3], b[3];
+        for (int d = 0; d < 3; d++) {
+            a[d] = std::max(lo[d], c[d] * m.chunks[d]);
+            b[d] = std::min(hi[d], (c[d] + 1) * m.chunks[d]);
+        }
+        const int64_t cy = m.chunks[0], cx = m.chunks[1], cz = m.chunks[2];
+        for (int64_t z = a[2]; z < b[2]; z++)
+            for (int64_t x = a[1]; x < b[1]; x++) {
+                const int64_t lz = z - c[2] * cz, lx = x - c[1] * cx;
+                uint8_t* dst = o + (((z - lo[2]) * ox + (x - lo[1])) * oy + (a[0] - lo[0])) * es;
+                if (!m.order_c) {
+                    const uint8_t* src = buf.data() + (((lz * cx) + lx) * cy + (a[0] - c[0] * cy)) * es;
+                    memcpy(dst, src, (size_t)(b[0] - a[0]) * es);
+                } else {
+                    for (int64_t y = a[0]; y < b[0]; y++) {                // C order: z fastest
+                        const int64_t ly = y - c[0] * cy;
+                        memcpy(dst + (y - a[0]) * es, buf.data() + (((ly * cx) + lx) * cz + lz) * es, es);
+                    }
+                }
+            }
+    });
+    if (err) return pk_fail(PK_ERR_INVALID, "zarr: a chunk file is corrupt or truncated");
+    return PK_OK;
+}
+
+extern "C" pk_status pk_zarr_write(const char* path, const void* data, const int64_t dims[3], int32_t bits,
+                                   int32_t is_float, const int64_t chunks[3], int32_t compressor, int32_t threads) {
+    if (!path || !data || !dims || !chunks) return pk_fail(PK_ERR_INVALID, "NULL path/data/dims/chunks");
+    if (!((!is_float && (bits == 8 || bits == 16 || bits == 32)) || (is_float && (bits == 32 || bits == 64))))
+        return pk_fail(PK_ERR_INVALID, "zarr: data must be uint8/16/32, single or double");
+    if (compressor < 0 || compressor > 2) return pk_fail(PK_ERR_INVALID, "zarr: compressor must be 0 (none), 1 (zlib) or 2 (gzip)");
+    int64_t ch[3];
+    for (int d = 0; d < 3; d++) {
+        if (dims[d] < 1 || chunks[d] < 1) return pk_fail(PK_ERR_INVALID, "zarr: sizes must be positive");
+        ch[d] = std::min(chunks[d], dims[d]);                           // blockSize = min(sz, blockSize)
+    }
+    const std::string root(path);
+    if (!make_dir(root)) return pk_fail(PK_ERR_INVALID, "zarr: cannot create " + root);
+    const int es = bits / 8;
+    char meta[1024];
+    const char* comp = compressor == 1 ? "{\"id\": \"zlib\", \"level\": 1}" : compressor == 2 ? "{\"id\": \"gzip\", \"level\": 1}" : "null";
+    snprintf(meta, sizeof(meta),
+             "{\n    \"chunks\": [%lld, %lld, %lld],\n    \"compressor\": %s,\n    \"dimension_separator\": \".\",\n"
+             "    \"dtype\": \"<%c%d\",\n    \"fill_value\": 0,\n    \"filters\": null,\n    \"order\": \"F\",\n"
+             "    \"shape\": [%lld, %lld, %lld],\n    \"zarr_format\": 2\n}\n",
+             (long long)ch[0], (long long)ch[1], (long long)ch[2], comp, is_float ? 'f' : 'u', es, (long long)dims[0],
+             (long long)dims[1], (long long)dims[2]);
+    if (!write_file(root + "/.zarray", meta, strlen(meta))) return pk_fail(PK_ERR_INVALID, "zarr: cannot write .zarray");
+    int64_t nc[3];
+    for (int d = 0; d < 3; d++) nc[d] = (dims[d] + ch[d] - 1) / ch[d];
+    const size_t ntask = (size_t)(nc[0] * nc[1] * nc[2]);
+    const size_t cn = (size_t)(ch[0] * ch[1] * ch[2]);
+    const int T = nthreads(threads);
+    std::vector<std::vector<uint8_t>> bufs(T), zbufs(T);
+    std::atomic<int> err(0);
+    ZMeta m;
+    m.ndim = 3;
+    const uint8_t* in = (const uint8_t*)data;
+    pfor(ntask, T, [&](size_t t, int w) {
+        if (err) return;
+        const int64_t c[3] = {(int64_t)(t % nc[0]), (int64_t)((t / nc[0]) % nc[1]), (int64_t)(t / (nc[0] * nc[1]))};
+        std::vector<uint8_t>& buf = bufs[w];
+        buf.assign(cn * es, 0);                                   // edge chunks padded with the fill value
+        int64_t a[3], b[3];
+        for (int d = 0; d < 3; d++) {
+            a[d] = c[d] * ch[d];
+            b[d] = std::min(dims[d], a[d] + ch[d]);
+        }
+        for (int64_t z = a[2]; z < b[2]; z++)
+            for (int64_t x = a[1]; x < b[1]; x++)
+                memcpy(buf.data() + (((z - a[2]) * ch[1] + (x - a[1])) * ch[0]) * es,
+                       in + ((z * dims[1] + x) * dims[0] + a[0]) * es, (size_t)(b[0] - a[0]) * es);
+        const std::string fn = root + "/" + chunk_key(m, c);
+        bool ok;
+        if (compressor == 0) {
+            ok = write_file(fn, buf.data(), buf.size());
+        } else {
+            std::vector<uint8_t>& zb = zbufs[w];
+            z_stream zs;
+            memset(&zs, 0, sizeof(zs));
+            ok = deflateInit2(&zs, 1, Z_DEFLATED, compressor == 2 ? 16 + MAX_WBITS : MAX_WBITS, 8, Z_DEFAULT_STRATEGY) == Z_OK;
+            if (ok) {
+                zb.resize(deflateBound(&zs, (uLong)buf.size()));
+                zs.next_in = buf.data();
+                zs.avail_in = (uInt)buf.size();
+                zs.next_out = zb.data();
+                zs.avail_out = (uInt)zb.size();
+                ok = deflate(&zs, Z_FINISH) == Z_STREAM_END;
+                const size_t n = zb.size() - zs.avail_out;
+                deflateEnd(&zs);
+                ok = ok && write_file(fn, zb.data(), n);
+            }
+        }
+        if (!ok) err = 1;
+    });
+    if (err) return pk_fail(PK_ERR_INVALID, "zarr: writing a chunk of " + root + " failed");
+    return PK_OK;
+}
+
+extern "C" pk_status pk_zarr_write_region(const char* path, const void* data, const int64_t bbox[6], int32_t threads) {
+    if (!path || !data || !bbox) return pk_fail(PK_ERR_INVALID, "NULL path/data/bbox");
+    ZMeta m;
+    pk_status s = parse_meta(path, m);
+    if (s != PK_OK) return s;
+    if (m.order_c || m.separator != "." || m.big_endian) return pk_fail(PK_ERR_UNSUPPORTED, "zarr: region writes need order F, '.' keys, little endian");
+    int64_t lo[3], hi[3], c0[3], nc[3];
+    for (int d = 0; d < 3; d++) {
+        lo[d] = bbox[d] - 1;
+        hi[d] = bbox[d + 3];
+        if (lo[d] < 0 || hi[d] > m.shape[d] || hi[d] <= lo[d]) return pk_fail(PK_ERR_INVALID, "zarr: the region is outside the array");
+        if (lo[d] % m.chunks[d] != 0 || (hi[d] % m.chunks[d] != 0 && hi[d] != m.shape[d]))
+            return pk_fail(PK_ERR_INVALID, "zarr: a region write must cover whole chunks");
+        c0[d] = lo[d] / m.chunks[d];
+        nc[d] = (hi[d] - lo[d] + m.chunks[d] - 1) / m.chunks[d];
+    }
+    const int es = m.es;
+    const int64_t ry = hi[0] - lo[0], rx = hi[1] - lo[1];
+    const size_t cn = (size_t)(m.chunks[0] * m.chunks[1] * m.chunks[2]);
+    const int T = nthreads(threads);
+    std::vector<std::vector<uint8_t>> bufs(T), zbufs(T);
+    std::atomic<int> err(0);
+    const uint8_t* in = (const uint8_t*)data;
+    pfor((size_t)(nc[0] * nc[1] * nc[2]), T, [&](size_t t, int w) {
+        if (err) return;
+        const int64_t c[3] = {c0[0] + (int64_t)(t % nc[0]), c0[1] + (int64_t)((t / nc[0]) % nc[1]),
+                              c0[2] + (int64_t)(t / (nc[0] * nc[1]))};
+        std::vector<uint8_t>& buf = bufs[w];
+        buf.assign(cn * es, 0);
+        int64_t a[3], b[3];
+        for (int d = 0; d < 3; d++) {
+            a[d] = c[d] * m.chunks[d];
+            b[d] = std::min(hi[d], a[d] + m.chunks[d]);
+        }
+        for (int64_t z = a[2]; z < b[2]; z++)
+            for (int64_t x = a[1]; x < b[1]; x++)
+                memcpy(buf.data() + (((z - a[2]) * m.chunks[1] + (x - a[1])) * m.chunks[0]) * es,
+                       in + (((z - lo[2]) * rx + (x - lo[1])) * ry + (a[0] - lo[0])) * es, (size_t)(b[0] - a[0]) * es);
+        const std::string fn = std::string(path) + "/" + chunk_key(m, c);
+        bool ok;
+        if (m.compressor.empty()) {
+            ok = write_file(fn, buf.data(), buf.size());
+        } else {
+            std::vector<uint8_t>& zb = zbufs[w];
+            z_stream zs;
+            memset(&zs, 0, sizeof(zs));
+            ok = deflateInit2(&zs, 1, Z_DEFLATED, m.compressor == "gzip" ? 16 + MAX_WBITS : MAX_WBITS, 8,
+                              Z_DEFAULT_STRATEGY) == Z_OK;
+            if (ok) {
+                zb.resize(deflateBound(&zs, (uLong)buf.size()));
+                zs.next_in = buf.data();
+                zs.avail_in = (uInt)buf.size();
+                zs.next_out = zb.data();
+                zs.avail_out = (uInt)zb.size();
+                ok = deflate(&zs, Z_FINISH) == Z_STREAM_END;
+                const size_t n = zb.size() - zs.avail_out;
+                deflateEnd(&zs);
+                ok = ok && write_file(fn, zb.data(), n);
+            }
+        }
+        if (!ok) err = 1;
+    });
+    if (err) return pk_fail(PK_ERR_INVALID, "zarr: writing a chunk failed");
+    return PK_OK;
+}

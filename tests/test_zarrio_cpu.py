@@ -1,0 +1,80 @@
+"""Zarr v2 reader / writer of libpkdecon.so against the format restatement in oracle/zarrio.py
+(no GPU)."""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import zarrio as OZ
+from petakit5d_b200 import zarrio as Z
+from petakit5d_b200._lib import PkError
+
+
+def _vol(dtype, shape, seed=0):
+    rng = np.random.default_rng(seed)
+    a = rng.random(shape) * 1000 if np.dtype(dtype).kind == "f" else rng.integers(0, 60000, shape)
+    return np.asfortranarray(a.astype(dtype))
+
+
+@pytest.mark.parametrize("dtype", [np.uint16, np.float32, np.uint8, np.float64])
+@pytest.mark.parametrize("comp", ["zlib", "gzip", None])
+def test_written_arrays_read_back_by_the_restatement(tmp_path, dtype, comp):
+    v = _vol(dtype, (70, 53, 29))
+    p = str(tmp_path / "a.zarr")
+    Z.writezarr(v, p, blockSize=(32, 20, 16), compressor=comp)     # ragged edge chunks on every axis
+    np.testing.assert_array_equal(OZ.read(p), v)
+    np.testing.assert_array_equal(Z.readzarr(p), v)
+    shape, chunks, dt = Z.getZarrInfo(p)
+    assert shape == v.shape and chunks == (32, 20, 16) and dt == v.dtype
+
+
+@pytest.mark.parametrize("order,sep,comp", [("F", ".", "zlib"), ("C", ".", "gzip"), ("F", "/", None),
+                                            ("C", "/", "zlib")])
+def test_reads_restatement_arrays_and_regions(tmp_path, order, sep, comp):
+    v = _vol(np.uint16, (45, 38, 21), seed=1)
+    p = str(tmp_path / "b.zarr")
+    OZ.write(p, v, (16, 16, 8), order=order, compressor=comp, separator=sep)
+    np.testing.assert_array_equal(Z.readzarr(p), v)
+    bb = [3, 10, 2, 40, 33, 19]
+    np.testing.assert_array_equal(Z.readzarr(p, inputBbox=bb), v[2:40, 9:33, 1:19])
+
+
+def test_missing_chunks_read_as_fill_value(tmp_path):
+    v = _vol(np.uint16, (20, 20, 20), seed=2)
+    p = str(tmp_path / "c.zarr")
+    OZ.write(p, v, (10, 10, 10), fill_value=7)
+    os.remove(os.path.join(p, "1.0.1"))
+    ref = v.copy()
+    ref[10:20, 0:10, 10:20] = 7
+    np.testing.assert_array_equal(Z.readzarr(p), ref)
+
+
+def test_2d_arrays_and_errors(tmp_path):
+    im = _vol(np.uint16, (33, 17), seed=3)
+    p = str(tmp_path / "d.zarr")
+    Z.writezarr(im, p, blockSize=(16, 16, 16))
+    assert Z.getZarrInfo(p)[0] == (33, 17, 1)
+    np.testing.assert_array_equal(Z.readzarr(p)[:, :, 0], im)
+    with pytest.raises(PkError):
+        Z.readzarr(str(tmp_path / "missing.zarr"))
+    with pytest.raises(PkError):
+        Z.readzarr(p, inputBbox=[1, 1, 1, 40, 17, 1])
+    q = str(tmp_path / "e.zarr")
+    OZ.write(q, im[:, :, None], (16, 16, 1), compressor="zlib")
+    meta = open(os.path.join(q, ".zarray")).read().replace('"zlib"', '"blosc"')
+    open(os.path.join(q, ".zarray"), "w").write(meta)
+    with pytest.raises(PkError):                      # the reference's default codec: not in this build
+        Z.readzarr(q)
+
+
+def test_region_writes_cover_whole_chunks(tmp_path):
+    v = _vol(np.uint16, (50, 40, 30), seed=4)
+    p = str(tmp_path / "r.zarr")
+    Z.writezarr(np.zeros_like(v), p, blockSize=(16, 16, 8))
+    for bb in ([1, 1, 1, 32, 32, 16], [33, 1, 1, 50, 40, 30], [1, 33, 17, 32, 40, 30], [1, 1, 17, 32, 32, 30],
+               [1, 33, 1, 32, 40, 16], [33, 1, 1, 50, 40, 30]):
+        Z.writezarr_region(np.asfortranarray(v[bb[0] - 1:bb[3], bb[1] - 1:bb[4], bb[2] - 1:bb[5]]), p, bb)
+    np.testing.assert_array_equal(Z.readzarr(p), v)
+    np.testing.assert_array_equal(OZ.read(p), v)
+    with pytest.raises(PkError):                       # not chunk aligned
+        Z.writezarr_region(np.zeros((10, 10, 10), np.uint16), p, [2, 1, 1, 11, 10, 10])
