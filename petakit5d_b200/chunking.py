@@ -8,6 +8,7 @@
                                   every chunk cropped to its region (deconBbox), paste back
 * ``edge_erosion_mask``        -- the runner's bwdist edge erosion (RLdecon_large_in_memory.m:146-168)
 * ``RLdecon_large_in_memory``  -- the whole runner for TIFF files (RLdecon_large_in_memory.m:1-300)
+* ``RLdecon_large_in_place``   -- the Zarr runner, region by region (RLdecon_large_in_place.m:1-277)
 """
 from __future__ import annotations
 
@@ -149,79 +150,55 @@ def edge_erosion_mask(im, erosion, out=None, ctx=None):
     return mask.astype(bool)
 
 
-def RLdecon_large_in_memory(frameFullpath, psfFullpath, deconFullpath, xyPixelSize, dz, **kw):
-    """RLdecon_large_in_memory(frameFullpath, psfFullpath, deconFullpath, xyPixelSize, dz, ...)
-    (decon/RLdecon_large_in_memory.m:1-300) for TIFF files: the PSF prepared with psf_gen_new and
-    saved under ``<deconPath>/psfgen/``, the volume read whole, cut into ``batchSize`` chunks with
-    ``round((size(psf) + 10) / 2)`` borders, every chunk deconvolved as RLdecon would (one batched
-    call), the regions pasted back, the edge-erosion mask applied, and the result and its z MIP
-    written.  Zarr files and ``maskFullpaths`` are not built (NotImplementedError)."""
-    from . import backprojector as B
-    from . import psfgen as P
-    from . import tiff as T
-    o = dict(save16bit=True, Rotate=False, Deskew=False, SkewAngle=-32.45, flipZstack=False, Background=None,
-             dzPSF=0.1, DeconIter=15, EdgeErosion=8, ErodeMaskfile="", SaveMaskfile=False, dampFactor=1.0,
-             scaleFactor=None, deconOffset=0.0, maskFullpaths=(), saveZarr=False, RLMethod="simplified",
-             wienerAlpha=0.005, OTFCumThresh=0.9, hannWinBounds=(0.8, 1.0), skewed=None, fixIter=True,
-             errThresh=None, batchSize=(1024, 1024, 1024), Overlap=200, CPUMaxMem=500, parseCluster=True, uuid="",
-             debug=False, psfGen=True, useGPU=True, ctx=None, EdgeSoften=5, zEdgeSoften=2, Crop=None, zFlip=False,
-             GenMaxZproj=(0, 0, 1))
-    low = {k.lower(): k for k in o}
+def _runner_options(name, defaults, kw):
+    low = {k.lower(): k for k in defaults}
+    o = dict(defaults)
     for k, v in kw.items():
         if k.lower() not in low:
-            raise TypeError(f"RLdecon_large_in_memory: unknown parameter {k!r}")
+            raise TypeError(f"{name}: unknown parameter {k!r}")
         o[low[k.lower()]] = v
-    if o["saveZarr"] or not str(frameFullpath).endswith((".tif", ".tiff")):
-        raise NotImplementedError("Zarr input / output is not built")
     if o["maskFullpaths"] and len(o["maskFullpaths"]) and o["maskFullpaths"][0]:
         raise NotImplementedError("maskFullpaths (Zarr masks) is not built")
     if o["Deskew"] or o["Rotate"]:
-        raise NotImplementedError("deskew / rotate of chunks is not built in the large-file runner")
-    method = str(o["RLMethod"])
-    if method not in ("simplified", "omw"):
-        raise NotImplementedError(f"RLMethod '{method}' is not built")
-    ctx = o["ctx"]
-    bg = 99.0 if o["Background"] is None or np.size(o["Background"]) == 0 else float(o["Background"])   # :81-83
-    erosion = int(o["EdgeErosion"])
-    if o["ErodeMaskfile"] and os.path.exists(o["ErodeMaskfile"]):
-        erosion = 0
-    decon_path = os.path.dirname(deconFullpath)
-    fsname = os.path.splitext(os.path.basename(frameFullpath))[0]
+        raise NotImplementedError("deskew / rotate of chunks is not built in the large-file runners")
+    if str(o["RLMethod"]) not in ("simplified", "omw"):
+        raise NotImplementedError(f"RLMethod '{o['RLMethod']}' is not built")
+    return o
+
+
+def _runner_psfs(psfFullpath, decon_path, dz, o, ctx):
+    """The PSF that sets the chunk borders (RLdecon_large_in_memory.m:93-123,
+    RLdecon_large_in_place.m:112-141; written to <deconPath>/psfgen/) and the PSF each chunk's RLdecon
+    call prepares from the same file (RLdecon.m:241-265: its own dz ratio, sind(|SkewAngle|))."""
+    from . import psfgen as P
+    from . import tiff as T
     pp = T.readtiff(psfFullpath).astype(np.float32)
     skew = float(o["SkewAngle"])
-    # the PSF that sets the chunk borders (:93-123)
-    if o["psfGen"]:
-        ratio = math.sin(math.radians(skew)) if o["Deskew"] else 1.0
-        g = P.psf_gen_new(pp, o["dzPSF"], dz * ratio, 1.5, "masked", ctx=ctx)
-        psf = P.rldecon_psf_crop(g, g.shape, "simplified")      # bounding box +-1 only (:108-114)
-        os.makedirs(os.path.join(decon_path, "psfgen"), exist_ok=True)
-        gen_fn = os.path.join(decon_path, "psfgen", os.path.splitext(os.path.basename(psfFullpath))[0] + ".tif")
-        if not os.path.exists(gen_fn):
-            T.writetiff(psf, gen_fn)
-    else:
-        psf = pp
-    im = T.readtiff(frameFullpath, pinned=True)
-    if im.ndim == 2:
-        im = im[:, :, None]
-    if o["flipZstack"]:
-        im = np.asfortranarray(im[:, :, ::-1])
-    # the PSF each chunk's RLdecon call prepares from the same file (RLdecon.m:241-265: its own
-    # dz ratio, sind(|SkewAngle|) outside objective scan), and the OMW backprojector of it
-    if o["psfGen"]:
-        cpsf = P.psf_gen_new(pp, o["dzPSF"], dz * math.sin(math.radians(abs(skew))), 1.5, "masked", ctx=ctx)
-        if method != "omw":
-            cpsf = P.rldecon_psf_crop(cpsf, cpsf.shape, "simplified")
-    else:
-        cpsf = pp
-    border = border_size(np.asarray(psf).shape[:3] + (1,) * (3 - np.asarray(psf).ndim))
-    bs = tuple(int(v) for v in o["batchSize"])
-    bb, rb, _ = zarr_chunk_coordinates(im.shape, batch_size=bs, block_size=bs, same_batch_size=False, border=border)
-    chunks, boxes, psfs, psfs_b, ids, key = [], [], [], [], [], {}
-    for b, r in zip(bb, rb):
-        c = np.asfortranarray(im[b[0] - 1:b[3], b[1] - 1:b[4], b[2] - 1:b[5]])
-        chunks.append(c)
-        boxes.append([*(r[:3] - b[:3] + 1), *(r[3:] - b[:3] + 1)])
-        cp = P.rldecon_psf_crop(cpsf, c.shape, "omw")          # crop a PSF larger than the chunk (:260-265)
+    method = str(o["RLMethod"])
+    if not o["psfGen"]:
+        return pp, pp
+    ratio = math.sin(math.radians(skew)) if o["Deskew"] else 1.0
+    g = P.psf_gen_new(pp, o["dzPSF"], dz * ratio, 1.5, "masked", ctx=ctx)
+    psf = P.rldecon_psf_crop(g, g.shape, "simplified")          # bounding box +-1 only
+    os.makedirs(os.path.join(decon_path, "psfgen"), exist_ok=True)
+    gen_fn = os.path.join(decon_path, "psfgen", os.path.splitext(os.path.basename(psfFullpath))[0] + ".tif")
+    if not os.path.exists(gen_fn):
+        T.writetiff(psf, gen_fn)
+    cpsf = P.psf_gen_new(pp, o["dzPSF"], dz * math.sin(math.radians(abs(skew))), 1.5, "masked", ctx=ctx)
+    if method != "omw":
+        cpsf = P.rldecon_psf_crop(cpsf, cpsf.shape, "simplified")
+    return psf, cpsf
+
+
+def _decon_chunks(chunks, boxes, cpsf, o, ctx, bg, edge_erosion=0):
+    """Every chunk deconvolved as RLdecon would (PSF cropped to the chunk when larger, :260-265; OMW
+    backprojector of that PSF), cropped to its region; one batched call."""
+    from . import backprojector as B
+    from . import psfgen as P
+    method = str(o["RLMethod"])
+    psfs, psfs_b, ids, key = [], [], [], {}
+    for c in chunks:
+        cp = P.rldecon_psf_crop(cpsf, c.shape, "omw")
         k = cp.shape
         if k not in key:
             key[k] = len(psfs)
@@ -234,10 +211,51 @@ def RLdecon_large_in_memory(frameFullpath, psfFullpath, deconFullpath, xyPixelSi
                 psfs_b.append(P.rldecon_psf_crop(bp, c.shape, "omw"))
         ids.append(key[k])
     scale = 1.0 if o["scaleFactor"] is None or np.size(o["scaleFactor"]) == 0 else float(o["scaleFactor"])
-    outs = batch_decon(chunks, psfs, ids, int(o["DeconIter"]), "omw" if method == "omw" else "rl",
-                       psfs_b if method == "omw" else None, boxes,
-                       False, ctx, Background=bg, save16bit=bool(o["save16bit"]), dampFactor=o["dampFactor"],
-                       scaleFactor=scale, deconOffset=o["deconOffset"])
+    return batch_decon(chunks, psfs, ids, int(o["DeconIter"]), "omw" if method == "omw" else "rl",
+                       psfs_b if method == "omw" else None, boxes, False, ctx, Background=bg,
+                       save16bit=bool(o["save16bit"]), dampFactor=o["dampFactor"], scaleFactor=scale,
+                       deconOffset=o["deconOffset"], EdgeErosion=int(edge_erosion))
+
+
+def RLdecon_large_in_memory(frameFullpath, psfFullpath, deconFullpath, xyPixelSize, dz, **kw):
+    """RLdecon_large_in_memory(frameFullpath, psfFullpath, deconFullpath, xyPixelSize, dz, ...)
+    (decon/RLdecon_large_in_memory.m:1-300) for TIFF files: the PSF prepared with psf_gen_new and
+    saved under ``<deconPath>/psfgen/``, the volume read whole, cut into ``batchSize`` chunks with
+    ``round((size(psf) + 10) / 2)`` borders, every chunk deconvolved as RLdecon would (one batched
+    call), the regions pasted back, the edge-erosion mask applied, and the result and its z MIP
+    written.  Zarr files and ``maskFullpaths`` are not built (NotImplementedError)."""
+    from . import tiff as T
+    o = _runner_options("RLdecon_large_in_memory", dict(
+        save16bit=True, Rotate=False, Deskew=False, SkewAngle=-32.45, flipZstack=False, Background=None,
+        dzPSF=0.1, DeconIter=15, EdgeErosion=8, ErodeMaskfile="", SaveMaskfile=False, dampFactor=1.0,
+        scaleFactor=None, deconOffset=0.0, maskFullpaths=(), saveZarr=False, RLMethod="simplified",
+        wienerAlpha=0.005, OTFCumThresh=0.9, hannWinBounds=(0.8, 1.0), skewed=None, fixIter=True,
+        errThresh=None, batchSize=(1024, 1024, 1024), Overlap=200, CPUMaxMem=500, parseCluster=True, uuid="",
+        debug=False, psfGen=True, useGPU=True, ctx=None, EdgeSoften=5, zEdgeSoften=2, Crop=None, zFlip=False,
+        GenMaxZproj=(0, 0, 1)), kw)
+    if o["saveZarr"] or not str(frameFullpath).endswith((".tif", ".tiff")):
+        raise NotImplementedError("Zarr input / output: use RLdecon_large_in_place")
+    ctx = o["ctx"]
+    bg = 99.0 if o["Background"] is None or np.size(o["Background"]) == 0 else float(o["Background"])   # :81-83
+    erosion = int(o["EdgeErosion"])
+    if o["ErodeMaskfile"] and os.path.exists(o["ErodeMaskfile"]):
+        erosion = 0
+    decon_path = os.path.dirname(deconFullpath)
+    fsname = os.path.splitext(os.path.basename(frameFullpath))[0]
+    psf, cpsf = _runner_psfs(psfFullpath, decon_path, dz, o, ctx)
+    im = T.readtiff(frameFullpath, pinned=True)
+    if im.ndim == 2:
+        im = im[:, :, None]
+    if o["flipZstack"]:
+        im = np.asfortranarray(im[:, :, ::-1])
+    border = border_size(np.asarray(psf).shape[:3] + (1,) * (3 - np.asarray(psf).ndim))
+    bs = tuple(int(v) for v in o["batchSize"])
+    bb, rb, _ = zarr_chunk_coordinates(im.shape, batch_size=bs, block_size=bs, same_batch_size=False, border=border)
+    chunks, boxes = [], []
+    for b, r in zip(bb, rb):
+        chunks.append(np.asfortranarray(im[b[0] - 1:b[3], b[1] - 1:b[4], b[2] - 1:b[5]]))
+        boxes.append([*(r[:3] - b[:3] + 1), *(r[3:] - b[:3] + 1)])
+    outs = _decon_chunks(chunks, boxes, cpsf, o, ctx, bg)
     out = np.zeros(im.shape, np.uint16 if o["save16bit"] else np.float32, order="F")
     for r, ob in zip(rb, outs):
         out[r[0] - 1:r[3], r[1] - 1:r[4], r[2] - 1:r[5]] = ob
@@ -255,6 +273,73 @@ def RLdecon_large_in_memory(frameFullpath, psfFullpath, deconFullpath, xyPixelSi
     os.makedirs(mip_dir, exist_ok=True)
     T.writetiff(out.max(axis=2), os.path.join(mip_dir, f"{fsname}_MIP_z.tif"))
     return out
+
+
+def RLdecon_large_in_place(frameFullpath, psfFullpath, deconPath, xyPixelSize, dz, **kw):
+    """RLdecon_large_in_place(frameFullpath, xyPixelSize, dz, deconPath, PSF, ...)
+    (decon/RLdecon_large_in_place.m:1-277 with RLdecon_for_zarr_block.m:101-171) for Zarr input: the
+    output ``<deconPath>/<name>.zarr`` is skipped when it exists, else built in a temporary array and
+    renamed; batches of the same size (``sameBatchSize``) with ``round((size(psf) + 10) / 2)`` borders
+    are read from the input region by region, deconvolved as RLdecon would (EdgeErosion per batch, as
+    RLdecon applies it) ``groupSize`` batches per batched call, and their regions written into the
+    output chunk by chunk.  The job distribution over a cluster is replaced by one process per GPU.
+    Returns the output path."""
+    from . import zarrio as Z
+    o = _runner_options("RLdecon_large_in_place", dict(
+        save16bit=True, Rotate=False, Deskew=False, SkewAngle=-32.45, flipZstack=False, Background=None,
+        dzPSF=0.1, DeconIter=15, EdgeErosion=0, dampFactor=1.0, scaleFactor=None, deconOffset=0.0,
+        maskFullpaths=(), RLMethod="simplified", wienerAlpha=0.005, OTFCumThresh=0.9, hannWinBounds=(0.8, 1.0),
+        skewed=None, fixIter=True, errThresh=None, batchSize=(1024, 1024, 1024), blockSize=(256, 256, 256),
+        largeFile=False, largeMethod="inplace", parseCluster=False, parseParfor=False, jobLogDir="",
+        cpusPerTask=8, uuid="", maxTrialNum=3, unitWaitTime=1, debug=False, psfGen=True, useGPU=True,
+        GPUJob=False, ctx=None, groupSize=8), kw)
+    if o["flipZstack"]:
+        raise NotImplementedError("flipZstack is not built in the in-place runner")
+    ctx = o["ctx"]
+    bg = 0.0 if o["Background"] is None or np.size(o["Background"]) == 0 else float(o["Background"])
+    fsname = os.path.splitext(os.path.basename(str(frameFullpath).rstrip("/")))[0]
+    out_path = os.path.join(deconPath, f"{fsname}.zarr")
+    if os.path.isdir(out_path):                                                   # :102-105
+        return out_path
+    os.makedirs(deconPath, exist_ok=True)
+    tmp_path = f"{out_path}_{o['uuid'] or os.getpid()}"
+    psf, cpsf = _runner_psfs(psfFullpath, deconPath, dz, o, ctx)
+    im_size, _, in_dt = Z.getZarrInfo(frameFullpath)
+    border = border_size(np.asarray(psf).shape[:3] + (1,) * (3 - np.asarray(psf).ndim))
+    bb, rb, _ = zarr_chunk_coordinates(im_size, batch_size=tuple(int(v) for v in o["batchSize"]),
+                                       block_size=tuple(int(v) for v in o["blockSize"]), same_batch_size=True,
+                                       border=border)
+    order = np.lexsort(tuple(np.asarray(bb)[:, ::-1].T) + (np.prod(bb[:, 3:] - bb[:, :3] + 1, axis=1),))
+    bb, rb = bb[order], rb[order]                                                 # sortrows by size, then box
+    out_dt = np.uint16 if o["save16bit"] else np.float32
+    bs = tuple(int(min(a, b)) for a, b in zip(o["blockSize"], im_size))
+    if not os.path.isdir(tmp_path):
+        _create_empty_zarr(tmp_path, im_size, bs, out_dt)
+    g = max(1, int(o["groupSize"]))
+    for s0 in range(0, len(bb), g):
+        chunks, boxes = [], []
+        for b, r in zip(bb[s0:s0 + g], rb[s0:s0 + g]):
+            chunks.append(Z.readzarr(frameFullpath, inputBbox=list(b), pinned=True))
+            boxes.append([*(r[:3] - b[:3] + 1), *(r[3:] - b[:3] + 1)])
+        outs = _decon_chunks(chunks, boxes, cpsf, o, ctx, bg, o["EdgeErosion"])
+        for r, ob in zip(rb[s0:s0 + g], outs):
+            Z.writezarr_region(ob, tmp_path, list(r))
+    os.replace(tmp_path, out_path)
+    return out_path
+
+
+def _create_empty_zarr(path, shape, chunks, dtype):
+    """An order-F, zlib, fill-value-0 array with no chunk files yet (createzarr's role)."""
+    import json
+    import shutil
+    if os.path.isdir(path):
+        shutil.rmtree(path)
+    os.makedirs(path)
+    meta = {"chunks": [int(c) for c in chunks], "compressor": {"id": "zlib", "level": 1},
+            "dimension_separator": ".", "dtype": np.dtype(dtype).newbyteorder("<").str, "fill_value": 0,
+            "filters": None, "order": "F", "shape": [int(v) for v in shape], "zarr_format": 2}
+    with open(os.path.join(path, ".zarray"), "w") as f:
+        json.dump(meta, f)
 
 
 def shard(n_items, rank, world):
