@@ -12,6 +12,8 @@
 //   data     = pkdecon_mex('readtiff', path[, [z1 z2]])            % parallelReadTiff
 //   pkdecon_mex('writetiff', path, data, compression)             % parallelWriteTiff ('lzw' | 'none')
 //   sz       = pkdecon_mex('tiffsize', path)                      % getImageSizeMex
+//   data     = pkdecon_mex('readzarr', path[, bbox])               % parallelReadZarr (none / zlib / gzip)
+//   pkdecon_mex('writezarr', path, data, blockSize)               % writezarr (order F, zlib)
 //   pkdecon_mex('reset')                                           % reset(gpuDevice) analogue
 // opts: struct with the reference's name/value fields (Background, save16bit, dampFactor,
 // scaleFactor, deconOffset, EdgeErosion, bbox).  Errors are raised with mexErrMsgIdAndTxt using the
@@ -290,6 +292,48 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
         int64_t d[3];
         dims3(prhs[2], d);
         check(pk_tiff_write(path.data(), mxGetData(prhs[2]), d, bits, isf, strcmp(comp, "none") != 0, 0));
+        return;
+    }
+    if (!strcmp(cmd, "readzarr")) {
+        if (nrhs < 2 || !mxIsChar(prhs[1])) mexErrMsgIdAndTxt("pkdecon:invalid", "readzarr: file name[, bbox]");
+        std::vector<char> path(mxGetNumberOfElements(prhs[1]) + 1);
+        mxGetString(prhs[1], path.data(), (mwSize)path.size());
+        int64_t d[3], ch[3], bb[6];
+        int32_t bits = 0, isf = 0;
+        check(pk_zarr_info(path.data(), d, ch, &bits, &isf));
+        const int64_t* pb = nullptr;
+        if (nrhs > 2 && !mxIsEmpty(prhs[2])) {
+            if (mxGetNumberOfElements(prhs[2]) != 6) mexErrMsgIdAndTxt("pkdecon:invalid", "bbox must have 6 elements");
+            for (int k = 0; k < 6; k++) bb[k] = (int64_t)mxGetPr(prhs[2])[k];
+            for (int k = 0; k < 3; k++) d[k] = bb[k + 3] - bb[k] + 1;
+            pb = bb;
+        }
+        mxClassID c;
+        if (isf) c = bits == 64 ? mxDOUBLE_CLASS : mxSINGLE_CLASS;
+        else c = bits == 8 ? mxUINT8_CLASS : bits == 16 ? mxUINT16_CLASS : mxUINT32_CLASS;
+        const mwSize dd[3] = {(mwSize)d[0], (mwSize)d[1], (mwSize)d[2]};
+        plhs[0] = mxCreateNumericArray(3, dd, c, mxREAL);
+        check(pk_zarr_read(path.data(), pb, mxGetData(plhs[0]), (int64_t)(mxGetElementSize(plhs[0]) * mxGetNumberOfElements(plhs[0])), 0));
+        return;
+    }
+    if (!strcmp(cmd, "writezarr")) {
+        if (nrhs < 3 || !mxIsChar(prhs[1])) mexErrMsgIdAndTxt("pkdecon:invalid", "writezarr: file name, data[, blockSize]");
+        std::vector<char> path(mxGetNumberOfElements(prhs[1]) + 1);
+        mxGetString(prhs[1], path.data(), (mwSize)path.size());
+        int32_t bits, isf = 0;
+        switch (mxGetClassID(prhs[2])) {
+            case mxUINT8_CLASS: case mxLOGICAL_CLASS: bits = 8; break;
+            case mxUINT16_CLASS: bits = 16; break;
+            case mxUINT32_CLASS: bits = 32; break;
+            case mxSINGLE_CLASS: bits = 32; isf = 1; break;
+            case mxDOUBLE_CLASS: bits = 64; isf = 1; break;
+            default: mexErrMsgIdAndTxt("pkdecon:invalid", "Data type not suppported");
+        }
+        int64_t d[3], bs[3] = {500, 500, 500};
+        dims3(prhs[2], d);
+        if (nrhs > 3 && mxGetNumberOfElements(prhs[3]) >= 3)
+            for (int k = 0; k < 3; k++) bs[k] = (int64_t)mxGetPr(prhs[3])[k];
+        check(pk_zarr_write(path.data(), mxGetData(prhs[2]), d, bits, isf, bs, 1, 0));
         return;
     }
     mexErrMsgIdAndTxt("pkdecon:invalid", "unknown command '%s'", cmd);
