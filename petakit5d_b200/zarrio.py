@@ -67,6 +67,7 @@ def writezarr(data, filepath, blockSize=(500, 500, 500), compressor="zlib", over
         bs[2] = 1
     if overwrite and os.path.isdir(str(filepath)):
         shutil.rmtree(str(filepath))
+    os.makedirs(os.path.dirname(os.path.abspath(str(filepath))), exist_ok=True)
     bits, isf = _W[a.dtype]
     check(lib.pk_zarr_write(os.fsencode(str(filepath)), ptr(a), i64x3(a.shape), bits, isf, i64x3(bs),
                             _COMP[compressor if compressor is None else str(compressor).lower()], int(threads)))

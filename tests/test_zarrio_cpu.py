@@ -20,7 +20,7 @@ def _vol(dtype, shape, seed=0):
 @pytest.mark.parametrize("comp", ["zlib", "gzip", None])
 def test_written_arrays_read_back_by_the_restatement(tmp_path, dtype, comp):
     v = _vol(dtype, (70, 53, 29))
-    p = str(tmp_path / "a.zarr")
+    p = str(tmp_path / "nested" / "dir" / "a.zarr")
     Z.writezarr(v, p, blockSize=(32, 20, 16), compressor=comp)     # ragged edge chunks on every axis
     np.testing.assert_array_equal(OZ.read(p), v)
     np.testing.assert_array_equal(Z.readzarr(p), v)
