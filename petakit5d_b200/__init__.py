@@ -3,7 +3,12 @@
 Modules:
   decon          -- decon_lucy_function / decon_lucy_omw_function drop-ins (and device-pointer forms)
   backprojector  -- omw_backprojector_generation / BackProjector('wiener-butterworth')
-  chunking       -- findGoodFactorNumber, XR_zarrChunkCoordinatesExtraction, batched chunk decon
+  chunking       -- findGoodFactorNumber, XR_zarrChunkCoordinatesExtraction, batched chunk decon,
+                    RLdecon_large_in_memory / RLdecon_large_in_place (large-file runners)
+  psfgen         -- psf_gen_new (PSF preparation) and RLdecon's PSF crops
+  deskew         -- deskewRotateFrame3D (combined deskew / rotate after deconvolution)
+  rldecon        -- RLdecon (per-file driver: files in, files out)
+  tiff, zarrio   -- readtiff / writetiff / getImageSize, readzarr / writezarr
   serve          -- device-resident serving loop with continuous batching
   synth          -- seeded synthetic volumes and PSFs
 """
