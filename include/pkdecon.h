@@ -262,6 +262,16 @@ PK_API pk_status pk_host_free(void* ptr);
 PK_API pk_status pk_edge_erosion_edt(pk_ctx* ctx, const void* im, pk_dtype im_type, const int64_t dims[3],
                                      int32_t erosion, void* out, pk_dtype out_type, uint8_t* mask);
 
+/* ---------------------------------------------------------------- edge taper */
+/* RLdecon.m:351-357: edgetaper(I(:,:,iz), PSF) for every z slice of a host uint16/single [ny nx nz]
+ * volume (MATLAB Image Processing Toolbox edgetaper; the reference passes
+ * PSF = fspecial('gaussian', nTapering + 30, nTapering)).  psf: host float64, column-major
+ * [psf_dims[0] psf_dims[1]], each smaller than the image's y/x size.  out (host, same type and size
+ * as in; may equal in) receives J = alpha .* I + (1 - alpha) .* circular blur of I by PSF, alpha from
+ * the PSF's autocorrelation (1 inside, 0 at the borders); uint16 by round-half-away, saturated. */
+PK_API pk_status pk_edgetaper(pk_ctx* ctx, const void* in, pk_dtype type, const int64_t dims[3], const double* psf,
+                              const int64_t psf_dims[2], void* out);
+
 /* ---------------------------------------------------------------- chunking helpers (host) */
 /* findGoodFactorNumber(n, direction, allowOddSeven)  -- utils/findGoodFactorNumber.m:1-26. */
 PK_API int64_t pk_find_good_factor_number(int64_t n, int32_t direction, int32_t allow_odd_seven);

@@ -7,6 +7,7 @@ Modules:
                     RLdecon_large_in_memory / RLdecon_large_in_place (large-file runners)
   psfgen         -- psf_gen_new (PSF preparation) and RLdecon's PSF crops
   deskew         -- deskewRotateFrame3D (combined deskew / rotate after deconvolution)
+  taper          -- edgetaper of every z slice and fspecial('gaussian') (RLdecon's nTapering)
   rldecon        -- RLdecon (per-file driver: files in, files out)
   tiff, zarrio   -- readtiff / writetiff / getImageSize, readzarr / writezarr
   serve          -- device-resident serving loop with continuous batching

@@ -9,6 +9,7 @@
 //   psf      = pkdecon_mex('psf_gen', psf, dz_psf, dz_data, medFactor, PSFGenMethod)  % psf_gen_new
 //   volout   = pkdecon_mex('dsr', vol, angle, dz, xyPixelSize, reverse, objectiveScan, xStepThresh, bbox, save16bit)
 //                                                                 % deskewRotateFrame3D
+//   J        = pkdecon_mex('edgetaper', vol, PSF)                 % edgetaper of every z slice (RLdecon.m:352-357)
 //   data     = pkdecon_mex('readtiff', path[, [z1 z2]])            % parallelReadTiff
 //   pkdecon_mex('writetiff', path, data, compression)             % parallelWriteTiff ('lzw' | 'none')
 //   sz       = pkdecon_mex('tiffsize', path)                      % getImageSizeMex
@@ -243,6 +244,21 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
         const mwSize dd[3] = {(mwSize)od[0], (mwSize)od[1], (mwSize)od[2]};
         plhs[0] = mxCreateNumericArray(3, dd, (s16 && t == PK_U16) ? mxUINT16_CLASS : mxSINGLE_CLASS, mxREAL);
         check(pk_deskew_rotate(ctx(), in, t, d, ang, dz, px, rev, obj, thr, pbb, s16, mxGetData(plhs[0]), od));
+        return;
+    }
+    if (!strcmp(cmd, "edgetaper")) {
+        if (nrhs < 3) mexErrMsgIdAndTxt("pkdecon:invalid", "edgetaper: vol, PSF");
+        int64_t d[3], pd[3];
+        dims3(prhs[1], d);
+        dims3(prhs[2], pd);
+        pk_dtype t;
+        if (mxGetClassID(prhs[1]) == mxUINT16_CLASS) t = PK_U16;
+        else if (mxGetClassID(prhs[1]) == mxSINGLE_CLASS) t = PK_F32;
+        else mexErrMsgIdAndTxt("pkdecon:invalid", "vol must be uint16 or single");
+        if (mxGetClassID(prhs[2]) != mxDOUBLE_CLASS || pd[2] != 1) mexErrMsgIdAndTxt("pkdecon:invalid", "PSF must be a 2-D double array");
+        const mwSize dd[3] = {(mwSize)d[0], (mwSize)d[1], (mwSize)d[2]};
+        plhs[0] = mxCreateNumericArray(3, dd, t == PK_U16 ? mxUINT16_CLASS : mxSINGLE_CLASS, mxREAL);
+        check(pk_edgetaper(ctx(), mxGetData(prhs[1]), t, d, mxGetPr(prhs[2]), pd, mxGetData(plhs[0])));
         return;
     }
     if (!strcmp(cmd, "readtiff") || !strcmp(cmd, "tiffsize")) {

@@ -3,14 +3,15 @@
 ``RLdecon(inputFn, outputFn, PSFfn, xyPixelSize, dz, dzPSF, **options)`` follows RLdecon.m:1-571 for
 TIFF files: the PSF is prepared with psf_gen_new and cached under ``<deconPath>/psfgen/`` (:207-281),
 the OMW backprojector is generated or loaded from its cache file (:283-333), the volume is read
-(:335-344), deconvolved with ``decon_lucy_omw_function`` / ``decon_lucy_function`` (:366-412),
-optionally deskewed and rotated in one step (``deskewRotateFrame3D``, :487-491), and the results and
-their maximum projections are written (:494-571).  Every step runs on the GPU through libpkdecon.so;
-the files are read and written by its TIFF reader / writer.
+(:335-344), edge-tapered slice by slice when ``nTapering > 0`` (:351-357), deconvolved with
+``decon_lucy_omw_function`` / ``decon_lucy_function`` (:366-412), optionally deskewed and rotated
+in one step (``deskewRotateFrame3D``, :487-491), and the results and their maximum projections are
+written (:494-571).  Every step runs on the GPU through libpkdecon.so; the files are read and
+written by its TIFF reader / writer.
 
 Not built (each raises NotImplementedError): Zarr input/output (``saveZarr``), the 'original'
-(MATLAB's deconvlucy) and 'cudagen' methods, edge tapering (``nTapering``), an existing erosion mask
-file (``ErodeMaskfile``), the separate deskew and rotate steps (``DSRCombined=false``, objective-scan
+(MATLAB's deconvlucy) and 'cudagen' methods, an existing erosion mask file (``ErodeMaskfile``), the
+separate deskew and rotate steps (``DSRCombined=false``, objective-scan
 rotation) and resampling / cubic interpolation in the deskew.
 """
 from __future__ import annotations
@@ -25,6 +26,7 @@ from . import backprojector as B
 from . import decon as D
 from . import deskew as G
 from . import psfgen as P
+from . import taper as TP
 from . import tiff as T
 
 _DEFAULTS = dict(rawdata=None, nTapering=0, save16bit=True, objectiveScan=False, Deskew=False, Rotate=False,
@@ -97,8 +99,6 @@ def RLdecon(inputFn, outputFn, PSFfn, xyPixelSize, dz, dzPSF, **kw):
                                   f"{'deconvlucy' if method == 'original' else 'the undefined decon_lucy_cuda_function'})")
     if method not in ("omw", "simplified"):
         raise ValueError(f"unknown RLMethod {method!r}")
-    if o["nTapering"] > 0:
-        raise NotImplementedError("nTapering > 0 (edgetaper) is not built")
     if o["EdgeErosion"] > 0 and o["ErodeMaskfile"]:
         raise NotImplementedError("ErodeMaskfile: existing Zarr erosion masks are not built")
     skew = abs(float(o["SkewAngle"]))
@@ -183,6 +183,9 @@ def RLdecon(inputFn, outputFn, PSFfn, xyPixelSize, dz, dzPSF, **kw):
             rawdata = T.readtiff(inputFn, pinned=True)
         if o["flipZstack"]:
             rawdata = np.asfortranarray(np.asarray(rawdata)[:, :, ::-1])
+        if o["nTapering"] > 0:                   # soften the x-y borders (:351-357)
+            nt = o["nTapering"]
+            rawdata = TP.edgetaper_slices(rawdata, TP.fspecial_gaussian(int(nt) + 30, float(nt)), ctx=ctx)
         if n_iter > 0 and np.any(rawdata):
             scale = 1.0 if o["scaleFactor"] is None or np.size(o["scaleFactor"]) == 0 else float(o["scaleFactor"])
             p32 = np.asarray(psf, np.float32)

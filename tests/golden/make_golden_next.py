@@ -2,10 +2,10 @@
 
 Fixtures for the rows on either side of the deconvolution (the reference ships no golden vectors for
 them either): psf_gen_new on a seeded bead image (both methods, with and without axial resampling),
-deskewRotateFrame3D on a seeded volume (direct warp and skewed-space interpolation, uint16 and single)
-and the large-file runner's bwdist edge erosion.  They pin the oracle against regressions
-(tests/test_golden_next_oracle.py) and give the GPU tests fixed expected values
-(tests/test_golden_next_gpu.py).
+deskewRotateFrame3D on a seeded volume (direct warp and skewed-space interpolation, uint16 and single),
+RLdecon's edge taper (edgetaper with fspecial('gaussian', 35, 5)) and the large-file runner's bwdist
+edge erosion.  They pin the oracle against regressions (tests/test_golden_next_oracle.py) and give
+the GPU tests fixed expected values (tests/test_golden_next_gpu.py).
 """
 import os
 import sys
@@ -17,6 +17,7 @@ sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 
 from oracle import chunking as OC  # noqa: E402
 from oracle import deskew as OD  # noqa: E402
+from oracle import edgetaper as OE  # noqa: E402
 from oracle import psfgen as OP  # noqa: E402
 from petakit5d_b200 import synth  # noqa: E402
 
@@ -37,6 +38,9 @@ def make():
     im = (rng.random((30, 28, 20)) > 0.05).astype(np.uint16) * 7
     g["edt_im"] = im
     g["edt_mask_e4"] = OC.edt_erosion_mask(im, 4).astype(np.uint8)
+    tv = np.asfortranarray((rng.random((44, 40, 3)) * 3000 + 100).astype(np.uint16))
+    g["taper_vol"] = tv
+    g["taper_u16_nt5"] = OE.edgetaper_slices(tv, OE.fspecial_gaussian(35, 5.0))
     return g
 
 

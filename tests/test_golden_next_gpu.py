@@ -1,5 +1,5 @@
 """The library against the committed fixtures of the rows next to the path (psf_gen_new,
-deskewRotateFrame3D, the large-file runner's edge erosion)."""
+deskewRotateFrame3D, RLdecon's edge taper, the large-file runner's edge erosion)."""
 import os
 
 import numpy as np
@@ -8,6 +8,7 @@ import pytest
 from petakit5d_b200 import chunking as K
 from petakit5d_b200 import deskew as G
 from petakit5d_b200 import psfgen as P
+from petakit5d_b200 import taper as TP
 
 pytestmark = pytest.mark.gpu
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -42,3 +43,9 @@ def test_deskew_fixtures(golden, key, dz, rev, s16, f32):
 def test_edge_erosion_fixture(golden):
     m = K.edge_erosion_mask(golden["edt_im"], 4)
     np.testing.assert_array_equal(m.astype(np.uint8), golden["edt_mask_e4"])
+
+
+def test_edge_taper_fixture(golden):
+    got = TP.edgetaper_slices(golden["taper_vol"], TP.fspecial_gaussian(35, 5.0))
+    d = np.abs(got.astype(np.int64) - golden["taper_u16_nt5"].astype(np.int64))
+    assert d.max() <= 1 and (d == 0).mean() >= 0.999

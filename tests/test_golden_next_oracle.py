@@ -22,7 +22,8 @@ def fresh():
 
 
 @pytest.mark.parametrize("key", ["bead", "psfgen_masked", "psfgen_median", "dsr_vol", "dsr_direct_u16",
-                                 "dsr_skewed_u16", "dsr_skewed_f32", "edt_im", "edt_mask_e4"])
+                                 "dsr_skewed_u16", "dsr_skewed_f32", "edt_im", "edt_mask_e4", "taper_vol",
+                                 "taper_u16_nt5"])
 def test_exact_fixtures(golden, fresh, key):
     assert np.array_equal(np.asarray(fresh[key]), golden[key])
 

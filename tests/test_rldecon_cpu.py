@@ -7,7 +7,6 @@ from petakit5d_b200.rldecon import RLdecon
 @pytest.mark.parametrize("kw,err", [({"saveZarr": True}, NotImplementedError),
                                     ({"RLMethod": "original"}, NotImplementedError),
                                     ({"RLMethod": "cudagen"}, NotImplementedError),
-                                    ({"nTapering": 5}, NotImplementedError),
                                     ({"Deskew": True, "DSRCombined": False, "Rotate": True}, NotImplementedError),
                                     ({"notAnOption": 1}, TypeError),
                                     ({"RLMethod": "fancy"}, ValueError)])
