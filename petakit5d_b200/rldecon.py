@@ -11,8 +11,11 @@ written by its TIFF reader / writer.
 
 Not built (each raises NotImplementedError): Zarr input/output (``saveZarr``), the 'original'
 (MATLAB's deconvlucy) and 'cudagen' methods, an existing erosion mask file (``ErodeMaskfile``), the
-separate deskew and rotate steps (``DSRCombined=false``, objective-scan
-rotation) and resampling / cubic interpolation in the deskew.
+separate deskew and rotate steps (``DSRCombined=false``, deskew without rotation, objective-scan
+rotation: RLdecon.m:448-449, :485-486 and :499-500 pass 'interpMethod' to deskewFrame3D /
+rotateFrame3D, whose inputParsers accept only 'Interp' (pointDetection/src/deskewFrame3D.m:28-37,
+pointDetection/src/rotateFrame3D.m:26-35), so those reference branches stop with MATLAB's
+unmatched-parameter error as written) and resampling / cubic interpolation in the deskew.
 """
 from __future__ import annotations
 
@@ -28,6 +31,9 @@ from . import deskew as G
 from . import psfgen as P
 from . import taper as TP
 from . import tiff as T
+
+_NO_IMWARP = ("%s is not built: RLdecon.m passes it 'interpMethod', which its inputParser does not "
+              "accept (only 'Interp'), so the reference branch errors as written")
 
 _DEFAULTS = dict(rawdata=None, nTapering=0, save16bit=True, objectiveScan=False, Deskew=False, Rotate=False,
                  DSRCombined=True, Reverse=False, SkewAngle=32.45, flipZstack=False, interpMethod="linear",
@@ -119,13 +125,13 @@ def RLdecon(inputFn, outputFn, PSFfn, xyPixelSize, dz, dzPSF, **kw):
     if objective:
         deskew = False
         if rotate:
-            raise NotImplementedError("objective-scan rotation (rotateFrame3D) is not built")
+            raise NotImplementedError(_NO_IMWARP % "rotateFrame3D")
     if not deskew and rotate:
         deskew, combined = True, True
     if deskew and not combined:
-        raise NotImplementedError("separate deskew / rotate (DSRCombined=false) is not built")
+        raise NotImplementedError(_NO_IMWARP % "deskewFrame3D")
     if deskew and not rotate:
-        raise NotImplementedError("deskew without rotation (deskewFrame3D) is not built")
+        raise NotImplementedError(_NO_IMWARP % "deskewFrame3D")
     dsr_fn = os.path.join(decon_path, "DSR", f"{out_fsn}.tif") if rotate else None
     if not rotate:
         save3d[2] = False
