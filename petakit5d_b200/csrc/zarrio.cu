@@ -141,6 +141,7 @@ pk_status parse_meta(const char* path, ZMeta& m) {
     m.big_endian = dt[0] == '>';
     m.kind = dt[1];
     m.es = atoi(dt.c_str() + 2);
+    if (m.kind == 'b' && m.es == 1) m.kind = 'u';   // "|b1" (logical masks): one byte, 0 or 1, read as uint8
     if (!((m.kind == 'u' && (m.es == 1 || m.es == 2 || m.es == 4)) || (m.kind == 'f' && (m.es == 4 || m.es == 8))))
         return pk_fail(PK_ERR_UNSUPPORTED, "zarr: dtype " + dt + " is not supported");
     m.order_c = read_str(s, find_key(s, "order")) == "C";
@@ -153,7 +154,8 @@ pk_status parse_meta(const char* path, ZMeta& m) {
         m.compressor = read_str(obj, find_key(obj, "id"));
     }
     const size_t fi = find_key(s, "fill_value");
-    if (fi != std::string::npos && s[fi] != 'n' && s[fi] != '"') m.fill = strtod(s.c_str() + fi, nullptr);
+    if (fi != std::string::npos && s[fi] == 't') m.fill = 1.0;                     // JSON true (bool arrays)
+    else if (fi != std::string::npos && s[fi] != 'n' && s[fi] != '"' && s[fi] != 'f') m.fill = strtod(s.c_str() + fi, nullptr);
     if (!m.compressor.empty() && m.compressor != "zlib" && m.compressor != "gzip")
         return pk_fail(PK_ERR_UNSUPPORTED, "zarr: compressor \"" + m.compressor +
                                                "\" is not supported here (none, zlib and gzip are; blosc is not in this image)");

@@ -4,18 +4,20 @@
 TIFF files: the PSF is prepared with psf_gen_new and cached under ``<deconPath>/psfgen/`` (:207-281),
 the OMW backprojector is generated or loaded from its cache file (:283-333), the volume is read
 (:335-344), edge-tapered slice by slice when ``nTapering > 0`` (:351-357), deconvolved with
-``decon_lucy_omw_function`` / ``decon_lucy_function`` (:366-412), optionally deskewed and rotated
+``decon_lucy_omw_function`` / ``decon_lucy_function`` and masked by an existing Zarr erosion mask
+(``ErodeMaskfile``, :409-413) when one is given (:366-412), optionally deskewed and rotated
 in one step (``deskewRotateFrame3D``, :487-491), and the results and their maximum projections are
-written (:494-571).  Every step runs on the GPU through libpkdecon.so; the files are read and
-written by its TIFF reader / writer.
+written (:494-571).  Every compute step runs on the GPU through libpkdecon.so (the erosion-mask
+multiply of the returned host result is one host pass, as in the reference); the files are read and
+written by its TIFF / Zarr readers and writer.
 
 Not built (each raises NotImplementedError): Zarr input/output (``saveZarr``), the 'original'
-(MATLAB's deconvlucy) and 'cudagen' methods, an existing erosion mask file (``ErodeMaskfile``), the
-separate deskew and rotate steps (``DSRCombined=false``, deskew without rotation, objective-scan
-rotation: RLdecon.m:448-449, :485-486 and :499-500 pass 'interpMethod' to deskewFrame3D /
-rotateFrame3D, whose inputParsers accept only 'Interp' (pointDetection/src/deskewFrame3D.m:28-37,
-pointDetection/src/rotateFrame3D.m:26-35), so those reference branches stop with MATLAB's
-unmatched-parameter error as written) and resampling / cubic interpolation in the deskew.
+(MATLAB's deconvlucy) and 'cudagen' methods, the separate deskew and rotate steps
+(``DSRCombined=false``, deskew without rotation, objective-scan rotation: RLdecon.m:448-449,
+:485-486 and :499-500 pass 'interpMethod' to deskewFrame3D / rotateFrame3D, whose inputParsers
+accept only 'Interp' (pointDetection/src/deskewFrame3D.m:28-37, pointDetection/src/rotateFrame3D.m:26-35),
+so those reference branches stop with MATLAB's unmatched-parameter error as written) and
+resampling / cubic interpolation in the deskew.
 """
 from __future__ import annotations
 
@@ -31,6 +33,7 @@ from . import deskew as G
 from . import psfgen as P
 from . import taper as TP
 from . import tiff as T
+from . import zarrio as Z
 
 _NO_IMWARP = ("%s is not built: RLdecon.m passes it 'interpMethod', which its inputParser does not "
               "accept (only 'Interp'), so the reference branch errors as written")
@@ -105,8 +108,8 @@ def RLdecon(inputFn, outputFn, PSFfn, xyPixelSize, dz, dzPSF, **kw):
                                   f"{'deconvlucy' if method == 'original' else 'the undefined decon_lucy_cuda_function'})")
     if method not in ("omw", "simplified"):
         raise ValueError(f"unknown RLMethod {method!r}")
-    if o["EdgeErosion"] > 0 and o["ErodeMaskfile"]:
-        raise NotImplementedError("ErodeMaskfile: existing Zarr erosion masks are not built")
+    # an existing erosion mask replaces the decon functions' own edge erosion (:364, :382-385, :409-413)
+    use_exist_mask = o["EdgeErosion"] > 0 and bool(o["ErodeMaskfile"]) and os.path.exists(o["ErodeMaskfile"])
     skew = abs(float(o["SkewAngle"]))
     objective = bool(o["objectiveScan"])
     deskew, rotate, combined = bool(o["Deskew"]), bool(o["Rotate"]), bool(o["DSRCombined"])
@@ -204,12 +207,18 @@ def RLdecon(inputFn, outputFn, PSFfn, xyPixelSize, dz, dzPSF, **kw):
                 save_step = min(save_step, n_iter)
             common = dict(Background=o["Background"], useGPU=True, save16bit=save16, dampFactor=o["dampFactor"],
                           scaleFactor=scale, deconOffset=o["deconOffset"], bbox=o["deconBbox"],
-                          EdgeErosion=o["EdgeErosion"], debug=o["debug"], debug_folder=debug_folder,
+                          EdgeErosion=0 if use_exist_mask else o["EdgeErosion"], debug=o["debug"], debug_folder=debug_folder,
                           saveStep=save_step, ctx=ctx)
             if method == "omw":
                 deconvolved = D.decon_lucy_omw_function(rawdata, p32, psf_b, n_iter, **common)[0]
             else:
                 deconvolved = D.decon_lucy_function(rawdata, p32, n_iter, **common)[0]
+            if use_exist_mask:
+                mask = Z.readzarr(o["ErodeMaskfile"])
+                if mask.shape != deconvolved.shape:
+                    raise ValueError(f"ErodeMaskfile: mask size {mask.shape} differs from the result's "
+                                     f"{deconvolved.shape}")
+                deconvolved *= mask > 0
         else:
             deconvolved = np.asarray(rawdata)
             bb = o["deconBbox"]

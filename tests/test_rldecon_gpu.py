@@ -11,6 +11,7 @@ from petakit5d_b200 import deskew as G
 from petakit5d_b200 import psfgen as P
 from petakit5d_b200 import synth
 from petakit5d_b200 import tiff as T
+from petakit5d_b200 import zarrio as Z
 from petakit5d_b200.rldecon import RLdecon
 
 pytestmark = pytest.mark.gpu
@@ -72,3 +73,23 @@ def test_rldecon_simplified_crops_the_psf_and_the_output(tmp_path):
     np.testing.assert_array_equal(J, ref)
     for ax in "yxz":
         assert os.path.exists(os.path.join(os.path.dirname(out), "MIPs", f"frame_CamA_MIP_{ax}.tif"))
+
+
+def test_rldecon_existing_erosion_mask(tmp_path):
+    vol, bead, raw, pfn = _files(tmp_path)
+    mask = np.ones(vol.shape, np.uint8)
+    mask[:10] = 0
+    mask[:, -7:] = 0
+    mfn = str(tmp_path / "mask.zarr")
+    Z.writezarr(mask, mfn, blockSize=(64, 64, 32))
+    kw = dict(Background=100, DeconIter=3, RLMethod="simplified", EdgeErosion=6, save16bit=False)
+    J, _, _ = RLdecon(raw, str(tmp_path / "a" / "frame_CamA.tif"), pfn, 0.108, 0.3, 0.1, ErodeMaskfile=mfn, **kw)
+    psf = P.rldecon_psf_crop(P.psf_gen_new(bead, 0.1, 0.3 * np.sin(np.radians(32.45))), vol.shape, "simplified")
+    p32 = psf / np.float32(psf.sum(dtype=np.float32))
+    ref = D.decon_lucy_function(vol, p32, 3, Background=100, save16bit=False, EdgeErosion=0)[0]
+    np.testing.assert_array_equal(J, ref * (mask > 0))               # RLdecon.m:382-385, 409-413
+    # a mask file that does not exist: the decon function erodes the edges itself (:364)
+    J2, _, _ = RLdecon(raw, str(tmp_path / "b" / "frame_CamA.tif"), pfn, 0.108, 0.3, 0.1,
+                       ErodeMaskfile=str(tmp_path / "absent.zarr"), **kw)
+    ref2 = D.decon_lucy_function(vol, p32, 3, Background=100, save16bit=False, EdgeErosion=6)[0]
+    np.testing.assert_array_equal(J2, ref2)

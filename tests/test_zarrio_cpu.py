@@ -78,3 +78,16 @@ def test_region_writes_cover_whole_chunks(tmp_path):
     np.testing.assert_array_equal(OZ.read(p), v)
     with pytest.raises(PkError):                       # not chunk aligned
         Z.writezarr_region(np.zeros((10, 10, 10), np.uint16), p, [2, 1, 1, 11, 10, 10])
+
+
+@pytest.mark.parametrize("fill", [False, True])
+def test_bool_masks_read_as_uint8(tmp_path, fill):
+    m = np.asfortranarray(np.random.default_rng(5).random((30, 22, 9)) > 0.4)
+    p = str(tmp_path / "m.zarr")
+    OZ.write(p, m, (16, 16, 4), fill_value=fill)                   # dtype "|b1", fill_value false / true
+    os.remove(os.path.join(p, "1.0.1"))
+    ref = m.copy()
+    ref[16:30, 0:16, 4:8] = fill
+    got = Z.readzarr(p)
+    assert got.dtype == np.uint8
+    np.testing.assert_array_equal(got, ref.astype(np.uint8))
