@@ -11,8 +11,10 @@ written (:494-571).  Every compute step runs on the GPU through libpkdecon.so (t
 multiply of the returned host result is one host pass, as in the reference); the files are read and
 written by its TIFF / Zarr readers and writer.
 
-Not built (each raises NotImplementedError): Zarr input/output (``saveZarr``), the 'original'
-(MATLAB's deconvlucy) and 'cudagen' methods, the separate deskew and rotate steps
+Zarr input (``.zarr`` inputFn) and output (``saveZarr``, chunked by ``blockSize``) go through the
+Zarr reader / writer; maximum projections stay TIFF, as in the reference.
+
+Not built (each raises NotImplementedError): the 'original' (MATLAB's deconvlucy) and 'cudagen' methods, the separate deskew and rotate steps
 (``DSRCombined=false``, deskew without rotation, objective-scan rotation: RLdecon.m:448-449,
 :485-486 and :499-500 pass 'interpMethod' to deskewFrame3D / rotateFrame3D, whose inputParsers
 accept only 'Interp' (pointDetection/src/deskewFrame3D.m:28-37, pointDetection/src/rotateFrame3D.m:26-35),
@@ -23,6 +25,7 @@ from __future__ import annotations
 
 import math
 import os
+import shutil
 import uuid as _uuid
 
 import numpy as np
@@ -59,9 +62,31 @@ def _opts(kw):
 
 def _move_into_place(write, final):
     """Write to a temporary name beside the target, then rename (the reference's tmp + movefile)."""
-    tmp = f"{final[:-4]}_{_uuid.uuid4().hex[:8]}.tif"
+    root, ext = os.path.splitext(final)
+    tmp = f"{root}_{_uuid.uuid4().hex[:8]}{ext or '.tif'}"
     write(tmp)
+    if os.path.isdir(final):                         # movefile replaces an existing Zarr folder
+        shutil.rmtree(final)
     os.replace(tmp, final)
+
+
+def _read(fn, pinned=False):
+    """readtiff / readzarr by extension (RLdecon.m:337-343, :423-428)."""
+    if str(fn).endswith(".zarr"):
+        return Z.readzarr(fn, pinned=pinned)
+    return T.readtiff(fn, pinned=pinned)
+
+
+def _size(fn):
+    return Z.getZarrInfo(fn)[0] if str(fn).endswith(".zarr") else T.getImageSize(fn)
+
+
+def _writer(o):
+    """writezarr with the run's blockSize when saveZarr is set (:455-461, :514-517, :560-562), else writetiff."""
+    if o["saveZarr"]:
+        bs = tuple(int(v) for v in o["blockSize"])
+        return lambda a, f: Z.writezarr(a, f, blockSize=bs)
+    return lambda a, f: T.writetiff(a, f)
 
 
 def _u16(a):
@@ -101,8 +126,6 @@ def RLdecon(inputFn, outputFn, PSFfn, xyPixelSize, dz, dzPSF, **kw):
     o = _opts(kw)
     ctx = o["ctx"]
     method = str(o["RLMethod"])
-    if o["saveZarr"]:
-        raise NotImplementedError("saveZarr: Zarr output is not built")
     if method in ("original", "cudagen"):
         raise NotImplementedError(f"RLMethod '{method}' is not built (the reference calls "
                                   f"{'deconvlucy' if method == 'original' else 'the undefined decon_lucy_cuda_function'})")
@@ -135,7 +158,9 @@ def RLdecon(inputFn, outputFn, PSFfn, xyPixelSize, dz, dzPSF, **kw):
         raise NotImplementedError(_NO_IMWARP % "deskewFrame3D")
     if deskew and not rotate:
         raise NotImplementedError(_NO_IMWARP % "deskewFrame3D")
-    dsr_fn = os.path.join(decon_path, "DSR", f"{out_fsn}.tif") if rotate else None
+    ext = ".zarr" if o["saveZarr"] else ".tif"                    # :126-130
+    write = _writer(o)
+    dsr_fn = os.path.join(decon_path, "DSR", f"{out_fsn}{ext}") if rotate else None
     if not rotate:
         save3d[2] = False
     save3d[1] = False
@@ -143,7 +168,7 @@ def RLdecon(inputFn, outputFn, PSFfn, xyPixelSize, dz, dzPSF, **kw):
               bool(not rotate or (save3d[2] and os.path.exists(dsr_fn)))]
 
     rawdata = o["rawdata"]
-    im_size = T.getImageSize(inputFn) if rawdata is None else tuple(np.shape(rawdata)) + (1,) * (3 - np.ndim(rawdata))
+    im_size = _size(inputFn) if rawdata is None else tuple(np.shape(rawdata)) + (1,) * (3 - np.ndim(rawdata))
 
     # ---- PSF (RLdecon.m:207-281) and backprojector (:283-333)
     psf = psf_b = None
@@ -189,7 +214,7 @@ def RLdecon(inputFn, outputFn, PSFfn, xyPixelSize, dz, dzPSF, **kw):
     n_iter = int(o["DeconIter"])
     if not exists[0]:
         if rawdata is None:
-            rawdata = T.readtiff(inputFn, pinned=True)
+            rawdata = _read(inputFn, pinned=True)
         if o["flipZstack"]:
             rawdata = np.asfortranarray(np.asarray(rawdata)[:, :, ::-1])
         if o["nTapering"] > 0:                   # soften the x-y borders (:351-357)
@@ -225,7 +250,7 @@ def RLdecon(inputFn, outputFn, PSFfn, xyPixelSize, dz, dzPSF, **kw):
             if bb is not None and len(bb):
                 deconvolved = deconvolved[bb[0] - 1:bb[3], bb[1] - 1:bb[4], bb[2] - 1:bb[5]]
     elif deskew or rotate:
-        deconvolved = T.readtiff(outputFn)
+        deconvolved = _read(outputFn)
     rawdata = None
 
     # ---- deskew / rotate in one step (:487-491) and its output (:499-520)
@@ -241,7 +266,7 @@ def RLdecon(inputFn, outputFn, PSFfn, xyPixelSize, dz, dzPSF, **kw):
         save_mip_frame(dsr, os.path.join(dsr_path, "MIPs", f"{fsname}_MIP_z.tif"), o["mipAxis"])
         if save3d[2]:
             os.makedirs(dsr_path, exist_ok=True)
-            _move_into_place(lambda f: T.writetiff(dsr, f), dsr_fn)
+            _move_into_place(lambda f: write(dsr, f), dsr_fn)
 
     # ---- the deconvolved volume (:528-571)
     if not outputFn or not any(save3d) or exists[0]:
@@ -252,5 +277,5 @@ def RLdecon(inputFn, outputFn, PSFfn, xyPixelSize, dz, dzPSF, **kw):
         save_mip_frame(deconvolved, os.path.join(decon_path, "MIPs", f"{fsname}_MIP_z.tif"), o["mipAxis"])
     if save3d[0]:
         os.makedirs(decon_path, exist_ok=True)
-        _move_into_place(lambda f: T.writetiff(deconvolved, f), outputFn)
+        _move_into_place(lambda f: write(deconvolved, f), outputFn)
     return deconvolved, None, dsr

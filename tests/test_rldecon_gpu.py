@@ -93,3 +93,27 @@ def test_rldecon_existing_erosion_mask(tmp_path):
                        ErodeMaskfile=str(tmp_path / "absent.zarr"), **kw)
     ref2 = D.decon_lucy_function(vol, p32, 3, Background=100, save16bit=False, EdgeErosion=6)[0]
     np.testing.assert_array_equal(J2, ref2)
+
+
+def test_rldecon_zarr_input_and_output(tmp_path):
+    vol, bead, raw, pfn = _files(tmp_path)
+    zin = str(tmp_path / "data" / "frame_CamA.zarr")
+    Z.writezarr(vol, zin, blockSize=(64, 64, 32))
+    kw = dict(Background=100, DeconIter=2, RLMethod="omw", wienerAlpha=0.005, OTFCumThresh=0.6, Deskew=True,
+              Rotate=True, Reverse=True)
+    Jt, _, dt = RLdecon(raw, str(tmp_path / "t" / "frame_CamA.tif"), pfn, 0.108, 0.3, 0.1, **kw)
+    out = str(tmp_path / "z" / "frame_CamA.zarr")
+    Jz, _, dz = RLdecon(zin, out, pfn, 0.108, 0.3, 0.1, saveZarr=True, blockSize=[64, 64, 64], **kw)
+    np.testing.assert_array_equal(Jz, Jt)
+    np.testing.assert_array_equal(dz, dt)
+    np.testing.assert_array_equal(Z.readzarr(out), Jt)
+    dsr_fn = str(tmp_path / "z" / "DSR" / "frame_CamA.zarr")
+    np.testing.assert_array_equal(Z.readzarr(dsr_fn), dt)
+    assert os.path.exists(str(tmp_path / "z" / "DSR" / "MIPs" / "frame_CamA_MIP_z.tif"))
+    # the deconvolved Zarr exists and the rotated one does not: it is read back and rotated (:420-428)
+    import shutil
+    shutil.rmtree(dsr_fn)
+    J3, _, d3 = RLdecon(zin, out, pfn, 0.108, 0.3, 0.1, saveZarr=True, blockSize=[64, 64, 64], **kw)
+    np.testing.assert_array_equal(J3, Jt)
+    np.testing.assert_array_equal(d3, dt)
+    np.testing.assert_array_equal(Z.readzarr(dsr_fn), dt)
