@@ -15,6 +15,7 @@ from __future__ import annotations
 import ctypes as C
 import math
 import os
+import shutil
 
 import numpy as np
 
@@ -157,13 +158,31 @@ def _runner_options(name, defaults, kw):
         if k.lower() not in low:
             raise TypeError(f"{name}: unknown parameter {k!r}")
         o[low[k.lower()]] = v
-    if o["maskFullpaths"] and len(o["maskFullpaths"]) and o["maskFullpaths"][0]:
-        raise NotImplementedError("maskFullpaths (Zarr masks) is not built")
+    if o["maskFullpaths"] and len(o["maskFullpaths"]) and o["maskFullpaths"][0] and len(o["maskFullpaths"]) != 3:
+        raise ValueError("maskFullpaths: three 2-D Zarr masks (xy, xz, yz) are needed")
     if o["Deskew"] or o["Rotate"]:
         raise NotImplementedError("deskew / rotate of chunks is not built in the large-file runners")
     if str(o["RLMethod"]) not in ("simplified", "omw"):
         raise NotImplementedError(f"RLMethod '{o['RLMethod']}' is not built")
     return o
+
+
+_MASK_AXES = ((0, 1), (1, 2), (0, 2))          # finds = [1, 2; 2, 3; 1, 3]: xy, xz, yz
+
+
+def region_masked_out(mask_paths, region):
+    """True when a region need not be deconvolved (RLdecon_large_in_memory.m:201-216,
+    RLdecon_for_zarr_block.m:111-128): one of the three 2-D Zarr masks (xy, xz, yz maximum-projection
+    masks, in that order) is all zero over the region's window ``[start(a) 1 end(a) 1]``."""
+    from . import zarrio as Z
+    if not mask_paths or not len(mask_paths) or not mask_paths[0]:
+        return False
+    r = [int(v) for v in region]
+    for f, (a, b) in enumerate(_MASK_AXES):
+        win = Z.readzarr(mask_paths[f], inputBbox=[r[a], r[b], 1, r[a + 3], r[b + 3], 1])
+        if not np.any(win):
+            return True
+    return False
 
 
 def _runner_psfs(psfFullpath, decon_path, dz, o, ctx):
@@ -223,8 +242,11 @@ def RLdecon_large_in_memory(frameFullpath, psfFullpath, deconFullpath, xyPixelSi
     saved under ``<deconPath>/psfgen/``, the volume read whole, cut into ``batchSize`` chunks with
     ``round((size(psf) + 10) / 2)`` borders, every chunk deconvolved as RLdecon would (one batched
     call), the regions pasted back, the edge-erosion mask applied, and the result and its z MIP
-    written.  Zarr files and ``maskFullpaths`` are not built (NotImplementedError)."""
+    written.  The input may be TIFF or Zarr (:129-135); ``saveZarr`` writes the result as Zarr
+    (:288-293); regions that ``maskFullpaths`` masks out are left zero without deconvolution
+    (:201-216)."""
     from . import tiff as T
+    from . import zarrio as Z
     o = _runner_options("RLdecon_large_in_memory", dict(
         save16bit=True, Rotate=False, Deskew=False, SkewAngle=-32.45, flipZstack=False, Background=None,
         dzPSF=0.1, DeconIter=15, EdgeErosion=8, ErodeMaskfile="", SaveMaskfile=False, dampFactor=1.0,
@@ -233,8 +255,6 @@ def RLdecon_large_in_memory(frameFullpath, psfFullpath, deconFullpath, xyPixelSi
         errThresh=None, batchSize=(1024, 1024, 1024), Overlap=200, CPUMaxMem=500, parseCluster=True, uuid="",
         debug=False, psfGen=True, useGPU=True, ctx=None, EdgeSoften=5, zEdgeSoften=2, Crop=None, zFlip=False,
         GenMaxZproj=(0, 0, 1)), kw)
-    if o["saveZarr"] or not str(frameFullpath).endswith((".tif", ".tiff")):
-        raise NotImplementedError("Zarr input / output: use RLdecon_large_in_place")
     ctx = o["ctx"]
     bg = 99.0 if o["Background"] is None or np.size(o["Background"]) == 0 else float(o["Background"])   # :81-83
     erosion = int(o["EdgeErosion"])
@@ -243,7 +263,10 @@ def RLdecon_large_in_memory(frameFullpath, psfFullpath, deconFullpath, xyPixelSi
     decon_path = os.path.dirname(deconFullpath)
     fsname = os.path.splitext(os.path.basename(frameFullpath))[0]
     psf, cpsf = _runner_psfs(psfFullpath, decon_path, dz, o, ctx)
-    im = T.readtiff(frameFullpath, pinned=True)
+    if str(frameFullpath).rstrip("/").endswith(".zarr"):
+        im = Z.readzarr(frameFullpath, pinned=True)
+    else:
+        im = T.readtiff(frameFullpath, pinned=True)
     if im.ndim == 2:
         im = im[:, :, None]
     if o["flipZstack"]:
@@ -251,11 +274,13 @@ def RLdecon_large_in_memory(frameFullpath, psfFullpath, deconFullpath, xyPixelSi
     border = border_size(np.asarray(psf).shape[:3] + (1,) * (3 - np.asarray(psf).ndim))
     bs = tuple(int(v) for v in o["batchSize"])
     bb, rb, _ = zarr_chunk_coordinates(im.shape, batch_size=bs, block_size=bs, same_batch_size=False, border=border)
+    keep = [not region_masked_out(o["maskFullpaths"], r) for r in rb]
+    bb, rb = bb[keep], rb[keep]
     chunks, boxes = [], []
     for b, r in zip(bb, rb):
         chunks.append(np.asfortranarray(im[b[0] - 1:b[3], b[1] - 1:b[4], b[2] - 1:b[5]]))
         boxes.append([*(r[:3] - b[:3] + 1), *(r[3:] - b[:3] + 1)])
-    outs = _decon_chunks(chunks, boxes, cpsf, o, ctx, bg)
+    outs = _decon_chunks(chunks, boxes, cpsf, o, ctx, bg) if chunks else []
     out = np.zeros(im.shape, np.uint16 if o["save16bit"] else np.float32, order="F")
     for r, ob in zip(rb, outs):
         out[r[0] - 1:r[3], r[1] - 1:r[4], r[2] - 1:r[5]] = ob
@@ -268,7 +293,14 @@ def RLdecon_large_in_memory(frameFullpath, psfFullpath, deconFullpath, xyPixelSi
     if o["ErodeMaskfile"] and os.path.exists(o["ErodeMaskfile"]):
         out *= (T.readtiff(o["ErodeMaskfile"]) > 0).reshape(out.shape, order="F").astype(out.dtype)
     os.makedirs(decon_path or ".", exist_ok=True)
-    T.writetiff(out, deconFullpath)
+    if o["saveZarr"]:
+        tmp = f"{os.path.splitext(deconFullpath)[0]}_{o['uuid'] or os.getpid()}.zarr"
+        Z.writezarr(out, tmp, overwrite=True)
+        if os.path.isdir(deconFullpath):
+            shutil.rmtree(deconFullpath)
+        os.replace(tmp, deconFullpath)
+    else:
+        T.writetiff(out, deconFullpath)
     mip_dir = os.path.join(decon_path, "MIPs")
     os.makedirs(mip_dir, exist_ok=True)
     T.writetiff(out.max(axis=2), os.path.join(mip_dir, f"{fsname}_MIP_z.tif"))
@@ -282,7 +314,8 @@ def RLdecon_large_in_place(frameFullpath, psfFullpath, deconPath, xyPixelSize, d
     renamed; batches of the same size (``sameBatchSize``) with ``round((size(psf) + 10) / 2)`` borders
     are read from the input region by region, deconvolved as RLdecon would (EdgeErosion per batch, as
     RLdecon applies it) ``groupSize`` batches per batched call, and their regions written into the
-    output chunk by chunk.  The job distribution over a cluster is replaced by one process per GPU.
+    output chunk by chunk; regions that ``maskFullpaths`` masks out are written as zeros without
+    deconvolution.  The job distribution over a cluster is replaced by one process per GPU.
     Returns the output path."""
     from . import zarrio as Z
     o = _runner_options("RLdecon_large_in_place", dict(
@@ -293,8 +326,7 @@ def RLdecon_large_in_place(frameFullpath, psfFullpath, deconPath, xyPixelSize, d
         largeFile=False, largeMethod="inplace", parseCluster=False, parseParfor=False, jobLogDir="",
         cpusPerTask=8, uuid="", maxTrialNum=3, unitWaitTime=1, debug=False, psfGen=True, useGPU=True,
         GPUJob=False, ctx=None, groupSize=8), kw)
-    if o["flipZstack"]:
-        raise NotImplementedError("flipZstack is not built in the in-place runner")
+    # flipZstack is passed on to RLdecon_for_zarr_block, which parses it and never uses it (:27, :54)
     ctx = o["ctx"]
     bg = 0.0 if o["Background"] is None or np.size(o["Background"]) == 0 else float(o["Background"])
     fsname = os.path.splitext(os.path.basename(str(frameFullpath).rstrip("/")))[0]
@@ -317,12 +349,16 @@ def RLdecon_large_in_place(frameFullpath, psfFullpath, deconPath, xyPixelSize, d
         _create_empty_zarr(tmp_path, im_size, bs, out_dt)
     g = max(1, int(o["groupSize"]))
     for s0 in range(0, len(bb), g):
-        chunks, boxes = [], []
+        chunks, boxes, regions = [], [], []
         for b, r in zip(bb[s0:s0 + g], rb[s0:s0 + g]):
+            if region_masked_out(o["maskFullpaths"], r):                  # RLdecon_for_zarr_block.m:111-128
+                Z.writezarr_region(np.zeros(tuple(r[3:] - r[:3] + 1), out_dt, order="F"), tmp_path, list(r))
+                continue
             chunks.append(Z.readzarr(frameFullpath, inputBbox=list(b), pinned=True))
             boxes.append([*(r[:3] - b[:3] + 1), *(r[3:] - b[:3] + 1)])
-        outs = _decon_chunks(chunks, boxes, cpsf, o, ctx, bg, o["EdgeErosion"])
-        for r, ob in zip(rb[s0:s0 + g], outs):
+            regions.append(r)
+        outs = _decon_chunks(chunks, boxes, cpsf, o, ctx, bg, o["EdgeErosion"]) if chunks else []
+        for r, ob in zip(regions, outs):
             Z.writezarr_region(ob, tmp_path, list(r))
     os.replace(tmp_path, out_path)
     return out_path
@@ -331,7 +367,6 @@ def RLdecon_large_in_place(frameFullpath, psfFullpath, deconPath, xyPixelSize, d
 def _create_empty_zarr(path, shape, chunks, dtype):
     """An order-F, zlib, fill-value-0 array with no chunk files yet (createzarr's role)."""
     import json
-    import shutil
     if os.path.isdir(path):
         shutil.rmtree(path)
     os.makedirs(path)

@@ -65,3 +65,47 @@ def test_large_runner_tiff_matches_chunked_composition(tmp_path, method):
     ref = ref * OC.edt_erosion_mask(vol, 4).astype(np.uint16)
     assert len(bb) > 4
     np.testing.assert_array_equal(out, ref)
+
+
+def _proj_masks(tmp_path, shape, x_cut):
+    """xy / xz / yz masks (RLdecon_large_in_memory.m:31) that empty every x >= x_cut."""
+    from petakit5d_b200 import zarrio as Z
+    ny, nx, nz = shape
+    xy = np.ones((ny, nx), np.uint8)
+    xy[:, x_cut:] = 0
+    xz = np.ones((nx, nz), np.uint8)
+    xz[x_cut:, :] = 0
+    paths = []
+    for name, m in (("xy", xy), ("xz", xz), ("yz", np.ones((ny, nz), np.uint8))):
+        paths.append(str(tmp_path / f"m_{name}.zarr"))
+        Z.writezarr(m, paths[-1], blockSize=(64, 64, 1))
+    return paths
+
+
+def test_large_runner_zarr_io_and_masks(tmp_path):
+    from petakit5d_b200 import zarrio as Z
+    psf_true = synth.gaussian_psf((31, 31, 41))
+    vol = synth.puncta_volume((150, 130, 64), 150, psf_true, seed=13)
+    bead = synth.measured_psf((32, 32, 41), sigma_xy=1.3, sigma_z=3.0, seed=14)
+    fin, zin, pfn = str(tmp_path / "raw.tif"), str(tmp_path / "raw.zarr"), str(tmp_path / "psf.tif")
+    T.writetiff(vol, fin)
+    Z.writezarr(vol, zin, blockSize=(64, 64, 32))
+    T.writetiff(bead, pfn)
+    kw = dict(DeconIter=2, batchSize=(64, 64, 64), EdgeErosion=4)
+    full = K.RLdecon_large_in_memory(fin, pfn, str(tmp_path / "a" / "raw.tif"), 0.108, 0.3, **kw)
+    paths = _proj_masks(tmp_path, vol.shape, 70)
+    zout = str(tmp_path / "b" / "raw.zarr")
+    got = K.RLdecon_large_in_memory(zin, pfn, zout, 0.108, 0.3, saveZarr=True, maskFullpaths=paths, **kw)
+    np.testing.assert_array_equal(Z.readzarr(zout), got)
+    g = P.psf_gen_new(bead, 0.1, 0.3)
+    border = K.border_size(P.rldecon_psf_crop(g, g.shape, "simplified").shape)
+    _, rb, _ = K.zarr_chunk_coordinates(vol.shape, batch_size=(64, 64, 64), block_size=(64, 64, 64),
+                                        same_batch_size=False, border=border)
+    ref = full.copy(order="F")
+    skipped = 0
+    for r in rb:
+        if K.region_masked_out(paths, r):
+            ref[r[0] - 1:r[3], r[1] - 1:r[4], r[2] - 1:r[5]] = 0
+            skipped += 1
+    assert 0 < skipped < len(rb)
+    np.testing.assert_array_equal(got, ref)

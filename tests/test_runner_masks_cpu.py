@@ -1,0 +1,61 @@
+"""Region skipping by 2-D Zarr masks in the large-file runners (RLdecon_large_in_memory.m:201-216,
+RLdecon_for_zarr_block.m:111-128), on the host."""
+import os
+
+import numpy as np
+import pytest
+
+from petakit5d_b200 import chunking as K
+from petakit5d_b200 import tiff as T
+from petakit5d_b200 import zarrio as Z
+
+
+def _masks(tmp_path, ny, nx, nz, xy=None, xz=None, yz=None):
+    paths = []
+    for name, shape, m in (("xy", (ny, nx), xy), ("xz", (nx, nz), xz), ("yz", (ny, nz), yz)):
+        a = np.ones(shape, np.uint8) if m is None else m.astype(np.uint8)
+        p = str(tmp_path / f"mask_{name}.zarr")
+        Z.writezarr(a, p, blockSize=(16, 16, 1))
+        paths.append(p)
+    return paths
+
+
+def test_region_is_skipped_when_any_projection_window_is_empty(tmp_path):
+    ny, nx, nz = 40, 36, 20
+    xy = np.zeros((ny, nx), bool)
+    xy[5:15, 20:30] = True
+    yz = np.ones((ny, nz), bool)
+    yz[:, 12:] = False
+    paths = _masks(tmp_path, ny, nx, nz, xy=xy, yz=yz)
+    rng = np.random.default_rng(0)
+    for _ in range(60):
+        lo = rng.integers(1, [ny, nx, nz], endpoint=True)
+        hi = np.array([rng.integers(l, n, endpoint=True) for l, n in zip(lo, (ny, nx, nz))])
+        r = [*lo, *hi]
+        want = not (xy[lo[0] - 1:hi[0], lo[1] - 1:hi[1]].any() and yz[lo[0] - 1:hi[0], lo[2] - 1:hi[2]].any())
+        assert K.region_masked_out(paths, r) == want, r
+    assert not K.region_masked_out((), [1, 1, 1, 4, 4, 4])
+    assert not K.region_masked_out([""], [1, 1, 1, 4, 4, 4])
+
+
+def test_in_place_runner_writes_zeros_for_masked_regions_without_deconvolving(tmp_path):
+    vol = np.asfortranarray(np.random.default_rng(1).integers(100, 3000, (70, 60, 40)).astype(np.uint16))
+    zin = str(tmp_path / "raw.zarr")
+    Z.writezarr(vol, zin, blockSize=(32, 32, 32))
+    pfn = str(tmp_path / "psf.tif")
+    T.writetiff(np.ones((9, 9, 11), np.float32), pfn)
+    paths = _masks(tmp_path, 70, 60, 40, xy=np.zeros((70, 60), bool))
+    dpath = str(tmp_path / "decon")
+    os.makedirs(dpath)
+    stale = str(tmp_path / "decon" / "raw.zarr_7")              # an interrupted run's temporary array
+    Z.writezarr(np.full(vol.shape, 9, np.uint16), stale, blockSize=(32, 32, 32))
+    out = K.RLdecon_large_in_place(zin, pfn, dpath, 0.108, 0.3, batchSize=(64, 64, 64), blockSize=(32, 32, 32),
+                                   maskFullpaths=paths, psfGen=False, flipZstack=True, uuid="7")
+    got = Z.readzarr(out)
+    assert got.shape == vol.shape and got.dtype == np.uint16 and not got.any()
+    assert not os.path.exists(stale)
+
+
+def test_mask_list_must_have_three_paths():
+    with pytest.raises(ValueError):
+        K.RLdecon_large_in_place("a.zarr", "p.tif", "d", 0.108, 0.3, maskFullpaths=["a.zarr", "b.zarr"])
