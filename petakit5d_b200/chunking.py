@@ -160,8 +160,6 @@ def _runner_options(name, defaults, kw):
         o[low[k.lower()]] = v
     if o["maskFullpaths"] and len(o["maskFullpaths"]) and o["maskFullpaths"][0] and len(o["maskFullpaths"]) != 3:
         raise ValueError("maskFullpaths: three 2-D Zarr masks (xy, xz, yz) are needed")
-    if o["Deskew"] or o["Rotate"]:
-        raise NotImplementedError("deskew / rotate of chunks is not built in the large-file runners")
     if str(o["RLMethod"]) not in ("simplified", "omw"):
         raise NotImplementedError(f"RLMethod '{o['RLMethod']}' is not built")
     return o
@@ -255,6 +253,12 @@ def RLdecon_large_in_memory(frameFullpath, psfFullpath, deconFullpath, xyPixelSi
         errThresh=None, batchSize=(1024, 1024, 1024), Overlap=200, CPUMaxMem=500, parseCluster=True, uuid="",
         debug=False, psfGen=True, useGPU=True, ctx=None, EdgeSoften=5, zEdgeSoften=2, Crop=None, zFlip=False,
         GenMaxZproj=(0, 0, 1)), kw)
+    # Deskew sets the dz ratio of the border PSF (:102-106); each chunk's RLdecon call would also
+    # deskew / rotate it (:240-247), but only its first output, the deconvolved chunk, is kept
+    if o["Deskew"] and not o["Rotate"]:
+        raise NotImplementedError("Deskew without Rotate: each chunk's RLdecon call would run deskewFrame3D "
+                                  "with 'interpMethod', which its inputParser does not accept (the reference "
+                                  "errors as written)")
     ctx = o["ctx"]
     bg = 99.0 if o["Background"] is None or np.size(o["Background"]) == 0 else float(o["Background"])   # :81-83
     erosion = int(o["EdgeErosion"])
@@ -326,7 +330,8 @@ def RLdecon_large_in_place(frameFullpath, psfFullpath, deconPath, xyPixelSize, d
         largeFile=False, largeMethod="inplace", parseCluster=False, parseParfor=False, jobLogDir="",
         cpusPerTask=8, uuid="", maxTrialNum=3, unitWaitTime=1, debug=False, psfGen=True, useGPU=True,
         GPUJob=False, ctx=None, groupSize=8), kw)
-    # flipZstack is passed on to RLdecon_for_zarr_block, which parses it and never uses it (:27, :54)
+    # flipZstack is passed on to RLdecon_for_zarr_block, which parses it and never uses it (:27, :54);
+    # Deskew only sets the dz ratio of the border PSF (:122-126): the blocks run without it (:137-138)
     ctx = o["ctx"]
     bg = 0.0 if o["Background"] is None or np.size(o["Background"]) == 0 else float(o["Background"])
     fsname = os.path.splitext(os.path.basename(str(frameFullpath).rstrip("/")))[0]

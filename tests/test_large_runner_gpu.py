@@ -109,3 +109,28 @@ def test_large_runner_zarr_io_and_masks(tmp_path):
             skipped += 1
     assert 0 < skipped < len(rb)
     np.testing.assert_array_equal(got, ref)
+
+
+def test_large_runner_deskew_rotate_sets_the_border_psf_only(tmp_path):
+    psf_true = synth.gaussian_psf((31, 31, 41))
+    vol = synth.puncta_volume((150, 130, 64), 150, psf_true, seed=15)
+    bead = synth.measured_psf((32, 32, 41), sigma_xy=1.3, sigma_z=3.0, seed=16)
+    fin, pfn = str(tmp_path / "raw.tif"), str(tmp_path / "psf.tif")
+    T.writetiff(vol, fin)
+    T.writetiff(bead, pfn)
+    out = K.RLdecon_large_in_memory(fin, pfn, str(tmp_path / "d" / "raw.tif"), 0.108, 0.3, DeconIter=2,
+                                    batchSize=(64, 64, 64), EdgeErosion=0, Deskew=True, Rotate=True)
+    cpsf = P.psf_gen_new(bead, 0.1, 0.3 * np.sin(np.radians(32.45)))
+    cpsf = P.rldecon_psf_crop(cpsf, cpsf.shape, "simplified")
+    g = P.psf_gen_new(bead, 0.1, 0.3 * np.sin(np.radians(-32.45)))        # sind(SkewAngle), :102-106
+    border = K.border_size(P.rldecon_psf_crop(g, g.shape, "simplified").shape)
+    bb, rb, _ = K.zarr_chunk_coordinates(vol.shape, batch_size=(64, 64, 64), block_size=(64, 64, 64),
+                                         same_batch_size=False, border=border)
+    ref = np.zeros(vol.shape, np.uint16, order="F")
+    for b, r in zip(bb, rb):
+        c = np.asfortranarray(vol[b[0] - 1:b[3], b[1] - 1:b[4], b[2] - 1:b[5]])
+        cp = P.rldecon_psf_crop(cpsf, c.shape, "omw")
+        p32 = cp / np.float32(cp.sum(dtype=np.float32))
+        box = [*(r[:3] - b[:3] + 1), *(r[3:] - b[:3] + 1)]
+        ref[r[0] - 1:r[3], r[1] - 1:r[4], r[2] - 1:r[5]] = D.decon_lucy_function(c, p32, 2, Background=99, bbox=box)[0]
+    np.testing.assert_array_equal(out, ref)

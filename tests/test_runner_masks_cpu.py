@@ -59,3 +59,20 @@ def test_in_place_runner_writes_zeros_for_masked_regions_without_deconvolving(tm
 def test_mask_list_must_have_three_paths():
     with pytest.raises(ValueError):
         K.RLdecon_large_in_place("a.zarr", "p.tif", "d", 0.108, 0.3, maskFullpaths=["a.zarr", "b.zarr"])
+
+
+def test_in_memory_runner_refuses_deskew_without_rotate():
+    with pytest.raises(NotImplementedError):
+        K.RLdecon_large_in_memory("a.tif", "p.tif", "d/a.tif", 0.108, 0.3, Deskew=True, Rotate=False)
+
+
+def test_in_place_runner_accepts_deskew(tmp_path):
+    vol = np.zeros((40, 40, 20), np.uint16)
+    zin = str(tmp_path / "raw.zarr")
+    Z.writezarr(vol, zin, blockSize=(32, 32, 32))
+    pfn = str(tmp_path / "psf.tif")
+    T.writetiff(np.ones((9, 9, 11), np.float32), pfn)
+    paths = _masks(tmp_path, 40, 40, 20, xy=np.zeros((40, 40), bool))
+    out = K.RLdecon_large_in_place(zin, pfn, str(tmp_path / "d"), 0.108, 0.3, batchSize=(32, 32, 32),
+                                   blockSize=(32, 32, 32), maskFullpaths=paths, psfGen=False, Deskew=True)
+    assert not Z.readzarr(out).any()
