@@ -19,6 +19,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <thread>
@@ -29,94 +30,119 @@
 namespace {
 
 // ------------------------------------------------------------------ LZW
-struct BitWriter {
-    std::vector<uint8_t>& out;
-    uint64_t acc = 0;
-    int n = 0;
-    explicit BitWriter(std::vector<uint8_t>& o) : out(o) {}
-    void put(unsigned code, int w) {
-        acc = (acc << w) | code;
-        n += w;
-        while (n >= 8) {
-            n -= 8;
-            out.push_back((uint8_t)(acc >> n));
-        }
-        acc &= (n ? ((1ull << n) - 1) : 0);
-    }
-    void flush() {
-        if (n) out.push_back((uint8_t)(acc << (8 - n)));
-        n = 0;
-        acc = 0;
+// a worker's output arena: grows geometrically and is never zero-filled (strips are appended)
+struct Arena {
+    uint8_t* p = nullptr;
+    size_t n = 0, cap = 0;
+    Arena() = default;
+    Arena(const Arena&) = delete;
+    Arena& operator=(const Arena&) = delete;
+    Arena(Arena&& o) noexcept : p(o.p), n(o.n), cap(o.cap) { o.p = nullptr; o.n = o.cap = 0; }
+    ~Arena() { std::free(p); }
+    bool ensure(size_t extra) {                       // room for n + extra bytes
+        if (n + extra <= cap) return true;
+        const size_t c = std::max(n + extra, cap * 2 + 4096);
+        uint8_t* q = (uint8_t*)std::realloc(p, c);
+        if (!q) return false;
+        p = q;
+        cap = c;
+        return true;
     }
 };
 
 // open-addressing table of (prefix code << 8 | byte) -> code, kept by each worker thread across
-// strips; a slot holds generation << 20 | key, so a new table (a Clear, a new strip) only bumps the
-// generation, and the slots are wiped when the 12-bit generation wraps
+// strips.  A slot is one 64-bit word, generation << 32 | key << 12 | code, so a probe is one load
+// and a new table (a Clear, a new strip) only bumps the generation; the slots are wiped when the
+// 12-bit generation wraps.  16384 slots for at most 3836 entries: a load factor under 1/4.
 struct LzwTable {
     static constexpr int HS = 1 << 14;
-    std::vector<uint32_t> slot = std::vector<uint32_t>(HS, 0u);
-    std::vector<uint16_t> val = std::vector<uint16_t>(HS);
-    uint32_t g = 0;
+    std::vector<uint64_t> slot = std::vector<uint64_t>(HS, 0ull);
+    uint64_t g = 0;
     void fresh() {
         if (++g == 4096) {
-            std::fill(slot.begin(), slot.end(), 0u);
+            std::fill(slot.begin(), slot.end(), 0ull);
             g = 1;
         }
     }
 };
 
-// appends the LZW stream of in[0, len) to out
-void lzw_encode(const uint8_t* in, size_t len, std::vector<uint8_t>& out, LzwTable& tb) {
-    out.reserve(out.size() + len / 2 + 64);
-    BitWriter bw(out);
+// largest LZW stream of len bytes: at most one 12-bit code per input byte, a Clear every 3836 codes,
+// the first Clear and EndOfInformation
+size_t lzw_bound(size_t len) { return len + len / 2 + len / 1024 + 16; }
+
+// appends the LZW stream of in[0, len) to the arena (false when it cannot grow)
+bool lzw_encode(const uint8_t* in, size_t len, Arena& out, LzwTable& tb) {
+    if (!out.ensure(lzw_bound(len))) return false;
+    uint8_t* dst = out.p + out.n;
+    uint64_t acc = 0;                                  // pending bits are its low nb bits (nb < 32)
+    int nb = 0;
+    auto put = [&](unsigned code, int w) {
+        acc = (acc << w) | code;
+        nb += w;
+        if (nb >= 32) {                                // four bytes at a time, most significant first
+            nb -= 32;
+            const uint32_t x = (uint32_t)(acc >> nb);
+            dst[0] = (uint8_t)(x >> 24);
+            dst[1] = (uint8_t)(x >> 16);
+            dst[2] = (uint8_t)(x >> 8);
+            dst[3] = (uint8_t)x;
+            dst += 4;
+        }
+    };
     constexpr int HS = LzwTable::HS;
-    uint32_t* slot = tb.slot.data();
-    uint16_t* val = tb.val.data();
+    uint64_t* slot = tb.slot.data();
     tb.fresh();
-    uint32_t g = tb.g;
+    uint64_t g = tb.g;
     int width = 9;
     unsigned next = 258;
-    bw.put(256, width);
-    if (len == 0) {
-        bw.put(257, width);
-        bw.flush();
-        return;
-    }
-    unsigned w = in[0];
-    for (size_t i = 1; i < len; i++) {
-        const unsigned k = in[i];
-        const uint32_t kk = (w << 8) | k, tag = (g << 20) | kk;
-        uint32_t h = (kk * 2654435761u) >> 18;
-        bool found = false;
-        for (uint32_t v; ((v = slot[h]) >> 20) == g; h = (h + 1) & (HS - 1))
-            if (v == tag) { found = true; break; }
-        if (found) { w = val[h]; continue; }
-        bw.put(w, width);
-        slot[h] = tag;
-        val[h] = (uint16_t)next;
+    put(256, width);
+    if (len > 0) {
+        unsigned w = in[0];
+        for (size_t i = 1; i < len; i++) {
+            const unsigned k = in[i];
+            const uint32_t kk = (w << 8) | k;
+            const uint64_t tag = (g << 20) | kk;         // the slot's value without its code
+            uint32_t h = (kk * 2654435761u) >> 18;
+            uint64_t v = slot[h];
+            if ((v >> 12) == tag) { w = (unsigned)(v & 4095u); continue; }   // the usual hit: first slot
+            bool found = false;
+            while ((v >> 32) == g) {
+                h = (h + 1) & (HS - 1);
+                v = slot[h];
+                if ((v >> 12) == tag) { found = true; break; }
+            }
+            if (found) { w = (unsigned)(v & 4095u); continue; }
+            put(w, width);
+            slot[h] = (tag << 12) | next;
+            next++;
+            if (next == 4094) {
+                put(256, width);
+                tb.fresh();
+                g = tb.g;
+                next = 258;
+                width = 9;
+            } else if (next > (1u << width) - 1) {
+                width++;
+            }
+            w = k;
+        }
+        put(w, width);
         next++;
         if (next == 4094) {
-            bw.put(256, width);
-            tb.fresh();
-            g = tb.g;
-            next = 258;
+            put(256, width);
             width = 9;
         } else if (next > (1u << width) - 1) {
             width++;
         }
-        w = k;
     }
-    bw.put(w, width);
-    next++;
-    if (next == 4094) {
-        bw.put(256, width);
-        width = 9;
-    } else if (next > (1u << width) - 1) {
-        width++;
+    put(257, width);
+    while (nb >= 8) {
+        nb -= 8;
+        *dst++ = (uint8_t)(acc >> nb);
     }
-    bw.put(257, width);
-    bw.flush();
+    if (nb) *dst++ = (uint8_t)(acc << (8 - nb));
+    out.n = (size_t)(dst - out.p);
+    return true;
 }
 
 // Decodes at most cap bytes into out; returns the bytes written or -1 for a corrupt stream.  Every
@@ -133,11 +159,21 @@ long long lzw_decode(const uint8_t* in, size_t len, uint8_t* out, size_t cap) {
     int prev = -1;
     auto get = [&](int w) -> unsigned {
         if (nb < w) {
-            while (nb <= 56 && ip < len) {
-                bits = (bits << 8) | in[ip++];
-                nb += 8;
+            if (ip + 8 <= len) {                      // 6 or 7 whole bytes from one big-endian load
+                uint64_t x;
+                memcpy(&x, in + ip, 8);
+                x = __builtin_bswap64(x);
+                const int take = (63 - nb) >> 3;
+                bits = (bits << (8 * take)) | (x >> (64 - 8 * take));
+                ip += take;
+                nb += 8 * take;
+            } else {
+                while (nb <= 56 && ip < len) {
+                    bits = (bits << 8) | in[ip++];
+                    nb += 8;
+                }
+                if (nb < w) return 257;               // out of input: as EndOfInformation
             }
-            if (nb < w) return 257;                   // out of input: as EndOfInformation
         }
         nb -= w;
         return (unsigned)(bits >> nb) & ((1u << w) - 1);
@@ -149,8 +185,18 @@ long long lzw_decode(const uint8_t* in, size_t len, uint8_t* out, size_t cap) {
             out[o++] = (uint8_t)code;
             return o < cap;
         }
-        const size_t L = length[code], n = std::min<size_t>(L, cap - o);
-        const uint8_t* src = out + off[code];    // the run ends at or before o: no overlap
+        const size_t L = length[code];
+        const uint8_t* src = out + off[code];    // the run ends at or before o
+        if (L <= 16 && o + 16 <= cap) {          // one 16-byte load then store: the bytes past L lie
+            uint64_t lo, hi;                     // inside the strip and later codes overwrite them
+            memcpy(&lo, src, 8);
+            memcpy(&hi, src + 8, 8);
+            memcpy(out + o, &lo, 8);
+            memcpy(out + o + 8, &hi, 8);
+            o += L;
+            return o < cap;
+        }
+        const size_t n = std::min<size_t>(L, cap - o);
         if (n <= 16) {
             for (size_t i = 0; i < n; i++) out[o + i] = src[i];
         } else {
@@ -433,10 +479,10 @@ void parallel_for(size_t n, int threads, F&& fn) {
 // ------------------------------------------------------------------ writing
 struct Out {
     int fd;
-    bool ok = true;
+    std::atomic<bool> ok{true};
     void put(uint64_t off, const void* p, size_t n) {
         size_t done = 0;
-        while (ok && done < n) {
+        while (ok.load(std::memory_order_relaxed) && done < n) {
             const ssize_t r = pwrite(fd, (const char*)p + done, n - done, (off_t)(off + done));
             if (r <= 0) ok = false;
             else done += (size_t)r;
@@ -558,46 +604,58 @@ extern "C" pk_status pk_tiff_write(const char* path, const void* data, const int
     // strips: transpose the column-major plane rows into row-major strips, compress in parallel
     // each worker appends its strips to an arena of its own (no allocation per strip)
     const int T = (int)std::min<uint64_t>(nz * ns, (uint64_t)n_threads(threads));
-    std::vector<std::vector<uint8_t>> arena(T), rowss(T);
+    std::vector<Arena> arena(T);
+    std::vector<std::vector<uint8_t>> rowss(T);
     std::vector<LzwTable> tables(lzw ? T : 0);
     struct StripRef { int worker; size_t off, size; };
     std::vector<StripRef> strips(nz * ns);
+    std::atomic<bool> grown(true);
     parallel_for(nz * ns, T, [&](size_t t, int worker) {
         const uint64_t z = t / ns, k = t % ns, r0 = k * rps, nr = std::min(rps, h - r0);
-        std::vector<uint8_t>& a = arena[worker];
-        const size_t at = a.size();
+        Arena& a = arena[worker];
+        const size_t at = a.n;
+        const uint8_t* plane = (const uint8_t*)data + z * w * h * es;
         if (lzw) {
             std::vector<uint8_t>& rows = rowss[worker];
             rows.resize(nr * w * es);
-            gather_rows((const uint8_t*)data + z * w * h * es, r0, nr, w, h, es, rows.data());
-            lzw_encode(rows.data(), rows.size(), a, tables[worker]);
+            gather_rows(plane, r0, nr, w, h, es, rows.data());
+            if (!lzw_encode(rows.data(), rows.size(), a, tables[worker])) grown = false;
+        } else if (a.ensure(nr * w * es)) {
+            gather_rows(plane, r0, nr, w, h, es, a.p + at);
+            a.n += nr * w * es;
         } else {
-            a.resize(at + nr * w * es);
-            gather_rows((const uint8_t*)data + z * w * h * es, r0, nr, w, h, es, a.data() + at);
+            grown = false;
         }
-        strips[t] = {worker, at, a.size() - at};
+        strips[t] = {worker, at, a.n - at};
     });
+    if (!grown) return pk_fail(PK_ERR_NOMEM, "out of host memory for the compressed strips");
     const int fd = open(path, O_WRONLY | O_CREAT | O_TRUNC, 0644);
     if (fd < 0) return pk_fail(PK_ERR_INVALID, std::string("cannot create \"") + path + "\"");
     Out o{fd};
-    uint64_t pos = 16;
+    // strip offsets by a prefix sum, then the strips written in parallel at their offsets
     std::vector<uint64_t> soff(nz * ns);
+    uint64_t pos = 16;
     for (size_t t = 0; t < strips.size(); t++) {
         soff[t] = pos;
-        o.put(pos, arena[strips[t].worker].data() + strips[t].off, strips[t].size);
         pos += strips[t].size;
     }
+    parallel_for(strips.size(), T, [&](size_t t, int) {
+        o.put(soff[t], arena[strips[t].worker].p + strips[t].off, strips[t].size);
+    });
     pos = (pos + 7) & ~7ull;
     const uint64_t first_ifd = pos;
-    // IFDs: 11 entries; strip offsets / byte counts out of line when more than one strip
+    // IFDs: 11 entries; strip offsets / byte counts out of line when more than one strip; all of
+    // them assembled in one buffer and written at once
     const int NE = 11;
+    const uint64_t ifd_bytes = 8 + NE * 20 + 8 + (ns > 1 ? 16 * ns : 0);
+    std::vector<uint8_t> ifds(nz * ifd_bytes, 0);
     for (uint64_t z = 0; z < nz; z++) {
-        const uint64_t ifd = pos, arr = ifd + 8 + NE * 20 + 8;
-        const uint64_t next = z + 1 < nz ? arr + (ns > 1 ? 16 * ns : 0) : 0;
-        std::vector<uint8_t> b(8 + NE * 20 + 8, 0);
+        const uint64_t ifd = first_ifd + z * ifd_bytes, arr = ifd + 8 + NE * 20 + 8;
+        const uint64_t next = z + 1 < nz ? ifd + ifd_bytes : 0;
+        uint8_t* b = ifds.data() + z * ifd_bytes;
         uint64_t n = NE;
-        memcpy(b.data(), &n, 8);
-        uint8_t* e = b.data() + 8;
+        memcpy(b, &n, 8);
+        uint8_t* e = b + 8;
         auto ent = [&](uint16_t tag, uint16_t typ, uint64_t cnt, uint64_t val) {
             memcpy(e, &tag, 2);
             memcpy(e + 2, &typ, 2);
@@ -616,19 +674,17 @@ extern "C" pk_status pk_tiff_write(const char* path, const void* data, const int
         ent(279, 16, ns, ns > 1 ? arr + 8 * ns : strips[z * ns].size);
         ent(284, 3, 1, 1);
         ent(339, 3, 1, is_float ? 3 : 1);
-        memcpy(b.data() + 8 + NE * 20, &next, 8);
-        o.put(ifd, b.data(), b.size());
-        pos = arr;
+        memcpy(b + 8 + NE * 20, &next, 8);
         if (ns > 1) {
-            std::vector<uint64_t> a(2 * ns);
+            uint8_t* a = b + 8 + NE * 20 + 8;
             for (uint64_t k = 0; k < ns; k++) {
-                a[k] = soff[z * ns + k];
-                a[ns + k] = strips[z * ns + k].size;
+                const uint64_t off = soff[z * ns + k], cnt = strips[z * ns + k].size;
+                memcpy(a + 8 * k, &off, 8);
+                memcpy(a + 8 * (ns + k), &cnt, 8);
             }
-            o.put(pos, a.data(), 16 * ns);
-            pos += 16 * ns;
         }
     }
+    o.put(first_ifd, ifds.data(), ifds.size());
     const uint8_t hd[8] = {'I', 'I', 43, 0, 8, 0, 0, 0};
     o.put(0, hd, 8);
     o.put(8, &first_ifd, 8);
