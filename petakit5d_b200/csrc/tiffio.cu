@@ -16,6 +16,9 @@
 #include <sys/stat.h>
 #include <unistd.h>
 #include <zlib.h>
+#if defined(__SSE2__)
+#include <emmintrin.h>
+#endif
 
 #include <algorithm>
 #include <atomic>
@@ -402,9 +405,34 @@ void swap_bytes(uint8_t* p, size_t n, int es) {
     else if (es == 8) for (size_t i = 0; i < n; i += 8) for (int k = 0; k < 4; k++) std::swap(p[i + k], p[i + 7 - k]);
 }
 
-// rows [r0, r0 + nr) of page z (row-major, row stride w) into the column-major output [h w nz]
+// d[j * ds + i] = s[i * ss + j] for an 8 x 8 block of 16-bit values: three rounds of interleaves
+// (SSE2, part of every x86-64 CPU), or plain loads and stores elsewhere
+inline void transpose8x8_u16(const uint16_t* s, uint64_t ss, uint16_t* d, uint64_t ds) {
+#if defined(__SSE2__)
+    __m128i a[8], b[8], c[8];
+    for (int i = 0; i < 8; i++) a[i] = _mm_loadu_si128((const __m128i*)(s + i * ss));
+    for (int i = 0; i < 4; i++) {
+        b[2 * i] = _mm_unpacklo_epi16(a[2 * i], a[2 * i + 1]);      // rows 2i, 2i+1: columns 0-3
+        b[2 * i + 1] = _mm_unpackhi_epi16(a[2 * i], a[2 * i + 1]);  // columns 4-7
+    }
+    for (int i = 0; i < 2; i++) {
+        c[4 * i + 0] = _mm_unpacklo_epi32(b[4 * i + 0], b[4 * i + 2]);   // rows 4i..4i+3: columns 0, 1
+        c[4 * i + 1] = _mm_unpackhi_epi32(b[4 * i + 0], b[4 * i + 2]);   // columns 2, 3
+        c[4 * i + 2] = _mm_unpacklo_epi32(b[4 * i + 1], b[4 * i + 3]);   // columns 4, 5
+        c[4 * i + 3] = _mm_unpackhi_epi32(b[4 * i + 1], b[4 * i + 3]);   // columns 6, 7
+    }
+    for (int j = 0; j < 4; j++) {
+        _mm_storeu_si128((__m128i*)(d + (2 * j) * ds), _mm_unpacklo_epi64(c[j], c[4 + j]));
+        _mm_storeu_si128((__m128i*)(d + (2 * j + 1) * ds), _mm_unpackhi_epi64(c[j], c[4 + j]));
+    }
+#else
+    for (int i = 0; i < 8; i++)
+        for (int j = 0; j < 8; j++) d[j * ds + i] = s[i * ss + j];
+#endif
+}
+
 // Transpose of an nr x w row-major block (row stride w) into a column-major array with column
-// stride h, in 32 x 32 tiles so that both sides stay in cache.
+// stride h, in 32 x 32 tiles so that both sides stay in cache (whole 16-bit tiles by 8 x 8 blocks).
 template <typename T>
 void transpose_block(const T* src, uint64_t nr, uint64_t w, T* dst, uint64_t h) {
     constexpr uint64_t B = 32;
@@ -412,6 +440,12 @@ void transpose_block(const T* src, uint64_t nr, uint64_t w, T* dst, uint64_t h) 
         const uint64_t r1 = std::min(nr, r0 + B);
         for (uint64_t x0 = 0; x0 < w; x0 += B) {
             const uint64_t x1 = std::min(w, x0 + B);
+            if (sizeof(T) == 2 && r1 - r0 == B && x1 - x0 == B) {   // whole tile: 8 x 8 blocks
+                for (uint64_t x = x0; x < x1; x += 8)
+                    for (uint64_t r = r0; r < r1; r += 8)
+                        transpose8x8_u16((const uint16_t*)src + r * w + x, w, (uint16_t*)dst + x * h + r, h);
+                continue;
+            }
             for (uint64_t x = x0; x < x1; x++) {
                 const T* s = src + x;
                 T* d = dst + x * h;
@@ -443,6 +477,12 @@ void gather_rows(const uint8_t* plane, uint64_t r0, uint64_t nr, uint64_t w, uin
             const uint64_t x1 = std::min(w, x0 + B);
             for (uint64_t q0 = 0; q0 < nr; q0 += B) {
                 const uint64_t q1 = std::min(nr, q0 + B);
+                if (sizeof(T) == 2 && x1 - x0 == B && q1 - q0 == B) {  // whole tile: 8 x 8 blocks
+                    for (uint64_t x = x0; x < x1; x += 8)
+                        for (uint64_t r = q0; r < q1; r += 8)
+                            transpose8x8_u16((const uint16_t*)src + x * h + r, h, (uint16_t*)dst + r * w + x, w);
+                    continue;
+                }
                 for (uint64_t x = x0; x < x1; x++)
                     for (uint64_t r = q0; r < q1; r++) dst[r * w + x] = src[x * h + r];
             }
