@@ -231,7 +231,111 @@ int nthreads(int req) {
 
 bool make_dir(const std::string& p) { return mkdir(p.c_str(), 0755) == 0 || errno == EEXIST; }
 
+// one chunk as a single zlib / gzip stream (level 1)
+bool deflate_whole(const std::vector<uint8_t>& buf, bool gz, std::vector<uint8_t>& zb) {
+    z_stream zs;
+    memset(&zs, 0, sizeof(zs));
+    if (deflateInit2(&zs, 1, Z_DEFLATED, gz ? 16 + MAX_WBITS : MAX_WBITS, 8, Z_DEFAULT_STRATEGY) != Z_OK) return false;
+    zb.resize(deflateBound(&zs, (uLong)buf.size()));
+    zs.next_in = (Bytef*)buf.data();
+    zs.avail_in = (uInt)buf.size();
+    zs.next_out = zb.data();
+    zs.avail_out = (uInt)zb.size();
+    const bool ok = deflate(&zs, Z_FINISH) == Z_STREAM_END;
+    zb.resize(zb.size() - zs.avail_out);
+    deflateEnd(&zs);
+    return ok;
+}
+
+// raw deflate of one piece of a chunk: the last piece ends the stream (Z_FINISH); the others end
+// byte-aligned by a sync flush without the final-block bit, so the pieces, each compressed without
+// the others' history, concatenate into one valid deflate stream
+bool deflate_piece(const uint8_t* p, size_t n, bool last, std::vector<uint8_t>& out) {
+    z_stream zs;
+    memset(&zs, 0, sizeof(zs));
+    if (deflateInit2(&zs, 1, Z_DEFLATED, -MAX_WBITS, 8, Z_DEFAULT_STRATEGY) != Z_OK) return false;
+    out.resize(deflateBound(&zs, (uLong)n) + 16);
+    zs.next_in = (Bytef*)p;
+    zs.avail_in = (uInt)n;
+    zs.next_out = out.data();
+    zs.avail_out = (uInt)out.size();
+    const int r = deflate(&zs, last ? Z_FINISH : Z_SYNC_FLUSH);
+    const bool ok = last ? r == Z_STREAM_END : (r == Z_OK && zs.avail_in == 0 && zs.avail_out > 0);
+    out.resize(out.size() - zs.avail_out);
+    deflateEnd(&zs);
+    return ok;
+}
+
+// Writes chunks 0..ntask-1: prep(t, buf) fills chunk t's cb bytes and returns its file name.
+// comp: 0 none, 1 zlib, 2 gzip (level 1).  With at least as many chunks as threads, one task per
+// chunk.  With fewer (a few large chunks), each chunk's deflate is cut into 1 MB pieces compressed
+// in parallel and joined behind one zlib / gzip header, the Adler-32 / CRC-32 of the pieces joined
+// with zlib's adler32_combine / crc32_combine: a standard stream that every reader decodes.
+template <typename Prep>
+bool write_chunks(size_t ntask, size_t cb, int comp, int T, Prep&& prep) {
+    std::atomic<int> err(0);
+    constexpr size_t PIECE = size_t(1) << 20;
+    const size_t np = comp ? std::max<size_t>(1, (cb + PIECE - 1) / PIECE) : 1;
+    if (comp == 0 || np == 1 || ntask >= (size_t)T) {
+        std::vector<std::vector<uint8_t>> bufs(T), zbufs(T);
+        pfor(ntask, T, [&](size_t t, int w) {
+            if (err) return;
+            std::vector<uint8_t>& buf = bufs[w];
+            const std::string fn = prep(t, buf);
+            bool ok;
+            if (comp == 0) ok = write_file(fn, buf.data(), buf.size());
+            else ok = deflate_whole(buf, comp == 2, zbufs[w]) && write_file(fn, zbufs[w].data(), zbufs[w].size());
+            if (!ok) err = 1;
+        });
+        return !err;
+    }
+    std::vector<std::vector<uint8_t>> bufs(ntask), zp(ntask * np);
+    std::vector<std::string> names(ntask);
+    std::vector<uLong> sums(ntask * np);
+    pfor(ntask, T, [&](size_t t, int) { names[t] = prep(t, bufs[t]); });
+    pfor(ntask * np, T, [&](size_t q, int) {
+        if (err) return;
+        const size_t t = q / np, k = q % np, off = k * PIECE, n = std::min(PIECE, cb - off);
+        const uint8_t* p = bufs[t].data() + off;
+        sums[q] = comp == 2 ? crc32(0L, p, (uInt)n) : adler32(1L, p, (uInt)n);
+        if (!deflate_piece(p, n, k + 1 == np, zp[q])) err = 1;
+    });
+    if (err) return false;
+    pfor(ntask, T, [&](size_t t, int) {
+        if (err) return;
+        uLong sum = sums[t * np];
+        size_t tot = 18;
+        for (size_t k = 0; k < np; k++) {
+            tot += zp[t * np + k].size();
+            if (k) {
+                const z_off_t n = (z_off_t)std::min(PIECE, cb - k * PIECE);
+                sum = comp == 2 ? crc32_combine(sum, sums[t * np + k], n) : adler32_combine(sum, sums[t * np + k], n);
+            }
+        }
+        std::vector<uint8_t> out;
+        out.reserve(tot);
+        if (comp == 2) {
+            const uint8_t h[10] = {0x1f, 0x8b, 8, 0, 0, 0, 0, 0, 4, 3};   // deflate, no name, fastest, Unix
+            out.insert(out.end(), h, h + 10);
+        } else {
+            out.push_back(0x78);                                            // deflate, 32 KB window
+            out.push_back(0x01);                                            // fastest; header % 31 == 0
+        }
+        for (size_t k = 0; k < np; k++) out.insert(out.end(), zp[t * np + k].begin(), zp[t * np + k].end());
+        const uint32_t s32 = (uint32_t)sum, len32 = (uint32_t)cb;
+        if (comp == 2) {
+            for (int i = 0; i < 4; i++) out.push_back((uint8_t)(s32 >> (8 * i)));      // CRC-32, little-endian
+            for (int i = 0; i < 4; i++) out.push_back((uint8_t)(len32 >> (8 * i)));    // size mod 2^32
+        } else {
+            for (int i = 3; i >= 0; i--) out.push_back((uint8_t)(s32 >> (8 * i)));     // Adler-32, big-endian
+        }
+        if (!write_file(names[t], out.data(), out.size())) err = 1;
+    });
+    return !err;
+}
+
 }  // namespace
+
 
 extern "C" pk_status pk_zarr_info(const char* path, int64_t dims[3], int64_t chunks[3], int32_t* bits, int32_t* is_float) {
     if (!path || !dims) return pk_fail(PK_ERR_INVALID, "NULL path/dims");
@@ -342,15 +446,11 @@ extern "C" pk_status pk_zarr_write(const char* path, const void* data, const int
     const size_t ntask = (size_t)(nc[0] * nc[1] * nc[2]);
     const size_t cn = (size_t)(ch[0] * ch[1] * ch[2]);
     const int T = nthreads(threads);
-    std::vector<std::vector<uint8_t>> bufs(T), zbufs(T);
-    std::atomic<int> err(0);
     ZMeta m;
     m.ndim = 3;
     const uint8_t* in = (const uint8_t*)data;
-    pfor(ntask, T, [&](size_t t, int w) {
-        if (err) return;
+    const bool ok = write_chunks(ntask, cn * es, compressor, T, [&](size_t t, std::vector<uint8_t>& buf) {
         const int64_t c[3] = {(int64_t)(t % nc[0]), (int64_t)((t / nc[0]) % nc[1]), (int64_t)(t / (nc[0] * nc[1]))};
-        std::vector<uint8_t>& buf = bufs[w];
         buf.assign(cn * es, 0);                                   // edge chunks padded with the fill value
         int64_t a[3], b[3];
         for (int d = 0; d < 3; d++) {
@@ -361,30 +461,9 @@ extern "C" pk_status pk_zarr_write(const char* path, const void* data, const int
             for (int64_t x = a[1]; x < b[1]; x++)
                 memcpy(buf.data() + (((z - a[2]) * ch[1] + (x - a[1])) * ch[0]) * es,
                        in + ((z * dims[1] + x) * dims[0] + a[0]) * es, (size_t)(b[0] - a[0]) * es);
-        const std::string fn = root + "/" + chunk_key(m, c);
-        bool ok;
-        if (compressor == 0) {
-            ok = write_file(fn, buf.data(), buf.size());
-        } else {
-            std::vector<uint8_t>& zb = zbufs[w];
-            z_stream zs;
-            memset(&zs, 0, sizeof(zs));
-            ok = deflateInit2(&zs, 1, Z_DEFLATED, compressor == 2 ? 16 + MAX_WBITS : MAX_WBITS, 8, Z_DEFAULT_STRATEGY) == Z_OK;
-            if (ok) {
-                zb.resize(deflateBound(&zs, (uLong)buf.size()));
-                zs.next_in = buf.data();
-                zs.avail_in = (uInt)buf.size();
-                zs.next_out = zb.data();
-                zs.avail_out = (uInt)zb.size();
-                ok = deflate(&zs, Z_FINISH) == Z_STREAM_END;
-                const size_t n = zb.size() - zs.avail_out;
-                deflateEnd(&zs);
-                ok = ok && write_file(fn, zb.data(), n);
-            }
-        }
-        if (!ok) err = 1;
+        return root + "/" + chunk_key(m, c);
     });
-    if (err) return pk_fail(PK_ERR_INVALID, "zarr: writing a chunk of " + root + " failed");
+    if (!ok) return pk_fail(PK_ERR_INVALID, "zarr: writing a chunk of " + root + " failed");
     return PK_OK;
 }
 
@@ -408,14 +487,11 @@ extern "C" pk_status pk_zarr_write_region(const char* path, const void* data, co
     const int64_t ry = hi[0] - lo[0], rx = hi[1] - lo[1];
     const size_t cn = (size_t)(m.chunks[0] * m.chunks[1] * m.chunks[2]);
     const int T = nthreads(threads);
-    std::vector<std::vector<uint8_t>> bufs(T), zbufs(T);
-    std::atomic<int> err(0);
     const uint8_t* in = (const uint8_t*)data;
-    pfor((size_t)(nc[0] * nc[1] * nc[2]), T, [&](size_t t, int w) {
-        if (err) return;
+    const int comp = m.compressor.empty() ? 0 : m.compressor == "gzip" ? 2 : 1;
+    const bool ok = write_chunks((size_t)(nc[0] * nc[1] * nc[2]), cn * es, comp, T, [&](size_t t, std::vector<uint8_t>& buf) {
         const int64_t c[3] = {c0[0] + (int64_t)(t % nc[0]), c0[1] + (int64_t)((t / nc[0]) % nc[1]),
                               c0[2] + (int64_t)(t / (nc[0] * nc[1]))};
-        std::vector<uint8_t>& buf = bufs[w];
         buf.assign(cn * es, 0);
         int64_t a[3], b[3];
         for (int d = 0; d < 3; d++) {
@@ -426,30 +502,8 @@ extern "C" pk_status pk_zarr_write_region(const char* path, const void* data, co
             for (int64_t x = a[1]; x < b[1]; x++)
                 memcpy(buf.data() + (((z - a[2]) * m.chunks[1] + (x - a[1])) * m.chunks[0]) * es,
                        in + (((z - lo[2]) * rx + (x - lo[1])) * ry + (a[0] - lo[0])) * es, (size_t)(b[0] - a[0]) * es);
-        const std::string fn = std::string(path) + "/" + chunk_key(m, c);
-        bool ok;
-        if (m.compressor.empty()) {
-            ok = write_file(fn, buf.data(), buf.size());
-        } else {
-            std::vector<uint8_t>& zb = zbufs[w];
-            z_stream zs;
-            memset(&zs, 0, sizeof(zs));
-            ok = deflateInit2(&zs, 1, Z_DEFLATED, m.compressor == "gzip" ? 16 + MAX_WBITS : MAX_WBITS, 8,
-                              Z_DEFAULT_STRATEGY) == Z_OK;
-            if (ok) {
-                zb.resize(deflateBound(&zs, (uLong)buf.size()));
-                zs.next_in = buf.data();
-                zs.avail_in = (uInt)buf.size();
-                zs.next_out = zb.data();
-                zs.avail_out = (uInt)zb.size();
-                ok = deflate(&zs, Z_FINISH) == Z_STREAM_END;
-                const size_t n = zb.size() - zs.avail_out;
-                deflateEnd(&zs);
-                ok = ok && write_file(fn, zb.data(), n);
-            }
-        }
-        if (!ok) err = 1;
+        return std::string(path) + "/" + chunk_key(m, c);
     });
-    if (err) return pk_fail(PK_ERR_INVALID, "zarr: writing a chunk failed");
+    if (!ok) return pk_fail(PK_ERR_INVALID, "zarr: writing a chunk failed");
     return PK_OK;
 }

@@ -91,3 +91,19 @@ def test_bool_masks_read_as_uint8(tmp_path, fill):
     got = Z.readzarr(p)
     assert got.dtype == np.uint8
     np.testing.assert_array_equal(got, ref.astype(np.uint8))
+
+
+@pytest.mark.parametrize("comp", ["zlib", "gzip"])
+def test_large_chunks_compressed_in_pieces_are_standard_streams(tmp_path, comp):
+    """Fewer chunks than threads: each 2.6 MB chunk is deflated as parallel 1 MB pieces joined behind
+    one header; Python's zlib / gzip decode every chunk file to the same bytes."""
+    v = _vol(np.uint16, (300, 280, 20), seed=6)
+    p = str(tmp_path / "big.zarr")
+    Z.writezarr(v, p, blockSize=(300, 280, 16), compressor=comp, threads=8)
+    np.testing.assert_array_equal(OZ.read(p), v)
+    np.testing.assert_array_equal(Z.readzarr(p), v)
+    import gzip
+    import zlib
+    raw = open(os.path.join(p, "0.0.0"), "rb").read()
+    body = gzip.decompress(raw) if comp == "gzip" else zlib.decompress(raw)
+    assert len(body) == 300 * 280 * 16 * 2
