@@ -380,6 +380,55 @@ extern "C" pk_status pk_zarr_read(const char* path, const int64_t* bbox, void* o
     std::atomic<int> err(0);
     uint8_t* o = (uint8_t*)out;
     const int es = m.es;
+    if (m.compressor.empty() && !m.order_c) {
+        // uncompressed, order F: a z-slab of a chunk is one byte range of its file, so each chunk's
+        // part of the box is cut into z-pieces (enough for every thread to have work), each read by
+        // its own pread straight into a worker buffer and copied run by run along y
+        const int64_t cy = m.chunks[0], cx = m.chunks[1], cz = m.chunks[2];
+        const size_t S = ntask >= (size_t)T ? 1 : ((size_t)T + ntask - 1) / ntask;
+        pfor(ntask * S, T, [&](size_t q, int w) {
+            if (err) return;
+            const size_t t = q / S, k = q % S;
+            const int64_t c[3] = {c0[0] + (int64_t)(t % nc[0]), c0[1] + (int64_t)((t / nc[0]) % nc[1]),
+                                  c0[2] + (int64_t)(t / (nc[0] * nc[1]))};
+            int64_t a[3], b[3];
+            for (int d = 0; d < 3; d++) {
+                a[d] = std::max(lo[d], c[d] * m.chunks[d]);
+                b[d] = std::min(hi[d], (c[d] + 1) * m.chunks[d]);
+            }
+            const int64_t span = (b[2] - a[2] + (int64_t)S - 1) / (int64_t)S;
+            const int64_t zs = a[2] + (int64_t)k * span, ze = std::min(b[2], zs + span);
+            if (zs >= ze) return;
+            const size_t slab = (size_t)(cx * cy) * es, nbytes = (size_t)(ze - zs) * slab;
+            std::vector<uint8_t>& buf = bufs[w];
+            buf.resize(nbytes);
+            const int fd = open((std::string(path) + "/" + chunk_key(m, c)).c_str(), O_RDONLY);
+            if (fd >= 0) {
+                struct stat sb;
+                const bool whole = fstat(fd, &sb) == 0 && (uint64_t)sb.st_size >= (uint64_t)cn * es;
+                size_t got = 0;
+                const off_t off = (off_t)((zs - c[2] * cz) * (int64_t)slab);
+                while (whole && got < nbytes) {
+                    const ssize_t r = pread(fd, buf.data() + got, nbytes - got, off + (off_t)got);
+                    if (r <= 0) break;
+                    got += (size_t)r;
+                }
+                close(fd);
+                if (!whole || got != nbytes) { err = 1; return; }
+                if (m.big_endian) byteswap(buf.data(), nbytes, es);
+            } else {
+                fill_bytes(buf.data(), nbytes / es, m);                // a chunk never written: fill_value
+            }
+            for (int64_t z = zs; z < ze; z++)
+                for (int64_t x = a[1]; x < b[1]; x++) {
+                    uint8_t* dst = o + (((z - lo[2]) * ox + (x - lo[1])) * oy + (a[0] - lo[0])) * es;
+                    const uint8_t* src = buf.data() + (((z - zs) * cx + (x - c[1] * cx)) * cy + (a[0] - c[0] * cy)) * es;
+                    memcpy(dst, src, (size_t)(b[0] - a[0]) * es);
+                }
+        });
+        if (err) return pk_fail(PK_ERR_INVALID, "zarr: a chunk file is corrupt or truncated");
+        return PK_OK;
+    }
     pfor(ntask, T, [&](size_t t, int w) {
         if (err) return;
         const int64_t c[3] = {c0[0] + (int64_t)(t % nc[0]), c0[1] + (int64_t)((t / nc[0]) % nc[1]),

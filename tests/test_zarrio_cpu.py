@@ -107,3 +107,23 @@ def test_large_chunks_compressed_in_pieces_are_standard_streams(tmp_path, comp):
     raw = open(os.path.join(p, "0.0.0"), "rb").read()
     body = gzip.decompress(raw) if comp == "gzip" else zlib.decompress(raw)
     assert len(body) == 300 * 280 * 16 * 2
+
+
+def test_uncompressed_reads_by_pieces_fill_swap_and_truncation(tmp_path):
+    v = _vol(np.uint16, (50, 40, 30), seed=7)
+    p = str(tmp_path / "u.zarr")
+    OZ.write(p, v, (32, 32, 16), compressor=None, fill_value=7)
+    os.remove(os.path.join(p, "1.0.1"))
+    ref = v.copy()
+    ref[32:50, 0:32, 16:30] = 7
+    np.testing.assert_array_equal(Z.readzarr(p, threads=8), ref)               # 8 chunks, 8 threads
+    np.testing.assert_array_equal(Z.readzarr(p, threads=32), ref)              # 4 z-pieces per chunk
+    bb = [5, 3, 2, 47, 38, 29]
+    np.testing.assert_array_equal(Z.readzarr(p, inputBbox=bb, threads=16), ref[4:47, 2:38, 1:29])
+    pb = str(tmp_path / "be.zarr")
+    OZ.write(pb, v.astype(">u2"), (32, 32, 16), compressor=None)
+    np.testing.assert_array_equal(Z.readzarr(pb, threads=16), v)
+    with open(os.path.join(p, "0.0.0"), "r+b") as f:                            # a truncated chunk
+        f.truncate(100)
+    with pytest.raises(PkError):
+        Z.readzarr(p, threads=16)
