@@ -168,6 +168,10 @@ def _runner_options(name, defaults, kw):
 _MASK_AXES = ((0, 1), (1, 2), (0, 2))          # finds = [1, 2; 2, 3; 1, 3]: xy, xz, yz
 
 
+def _round_half_away(v):
+    return math.floor(v + 0.5) if v >= 0 else math.ceil(v - 0.5)
+
+
 def region_masked_out(mask_paths, region):
     """True when a region need not be deconvolved (RLdecon_large_in_memory.m:201-216,
     RLdecon_for_zarr_block.m:111-128): one of the three 2-D Zarr masks (xy, xz, yz maximum-projection
@@ -319,8 +323,11 @@ def RLdecon_large_in_place(frameFullpath, psfFullpath, deconPath, xyPixelSize, d
     are read from the input region by region, deconvolved as RLdecon would (EdgeErosion per batch, as
     RLdecon applies it) ``groupSize`` batches per batched call, and their regions written into the
     output chunk by chunk; regions that ``maskFullpaths`` masks out are written as zeros without
-    deconvolution.  The job distribution over a cluster is replaced by one process per GPU.
-    Returns the output path."""
+    deconvolution.  Batches run in tasks of ``taskSize`` (:192-197) whose completion is flagged under
+    ``<deconPath>/zarr_flag/<name>_<uuid>/`` (:164-167, :217-221), so a second call with the same
+    ``uuid`` resumes at the first unfinished task; at the end the temporary array is renamed, the
+    flags removed (:272-280) and the y/x/z MIPs written (XR_MIP_zarr, :283-289).  The job
+    distribution over a cluster is replaced by one process per GPU.  Returns the output path."""
     from . import zarrio as Z
     o = _runner_options("RLdecon_large_in_place", dict(
         save16bit=True, Rotate=False, Deskew=False, SkewAngle=-32.45, flipZstack=False, Background=None,
@@ -339,7 +346,8 @@ def RLdecon_large_in_place(frameFullpath, psfFullpath, deconPath, xyPixelSize, d
     if os.path.isdir(out_path):                                                   # :102-105
         return out_path
     os.makedirs(deconPath, exist_ok=True)
-    tmp_path = f"{out_path}_{o['uuid'] or os.getpid()}"
+    uid = str(o["uuid"] or os.getpid())
+    tmp_path = f"{out_path}_{uid}"
     psf, cpsf = _runner_psfs(psfFullpath, deconPath, dz, o, ctx)
     im_size, _, in_dt = Z.getZarrInfo(frameFullpath)
     border = border_size(np.asarray(psf).shape[:3] + (1,) * (3 - np.asarray(psf).ndim))
@@ -352,21 +360,67 @@ def RLdecon_large_in_place(frameFullpath, psfFullpath, deconPath, xyPixelSize, d
     bs = tuple(int(min(a, b)) for a, b in zip(o["blockSize"], im_size))
     if not os.path.isdir(tmp_path):
         _create_empty_zarr(tmp_path, im_size, bs, out_dt)
+    # tasks of taskSize batches (:192-197), each flagged when its regions are written (:217-221), so that
+    # a second call with the same uuid resumes at the first unflagged task
+    n = len(bb)
+    task = 20
+    if (o["parseCluster"] or o["GPUJob"] or str(o["RLMethod"]) == "omw") and n > 200:
+        task = max(100, int(_round_half_away(n / 5000)))
+    flag_dir = os.path.join(deconPath, "zarr_flag", f"{fsname}_{uid}")
+    os.makedirs(flag_dir, exist_ok=True)
     g = max(1, int(o["groupSize"]))
-    for s0 in range(0, len(bb), g):
-        chunks, boxes, regions = [], [], []
-        for b, r in zip(bb[s0:s0 + g], rb[s0:s0 + g]):
-            if region_masked_out(o["maskFullpaths"], r):                  # RLdecon_for_zarr_block.m:111-128
-                Z.writezarr_region(np.zeros(tuple(r[3:] - r[:3] + 1), out_dt, order="F"), tmp_path, list(r))
-                continue
-            chunks.append(Z.readzarr(frameFullpath, inputBbox=list(b), pinned=True))
-            boxes.append([*(r[:3] - b[:3] + 1), *(r[3:] - b[:3] + 1)])
-            regions.append(r)
-        outs = _decon_chunks(chunks, boxes, cpsf, o, ctx, bg, o["EdgeErosion"]) if chunks else []
-        for r, ob in zip(regions, outs):
-            Z.writezarr_region(ob, tmp_path, list(r))
+    for t0 in range(0, n, task):
+        t1 = min(n, t0 + task)
+        flag = os.path.join(flag_dir, f"blocks_{t0 + 1}_{t1}.mat")
+        if os.path.exists(flag):
+            continue
+        for s0 in range(t0, t1, g):
+            s1 = min(t1, s0 + g)
+            chunks, boxes, regions = [], [], []
+            for b, r in zip(bb[s0:s1], rb[s0:s1]):
+                if region_masked_out(o["maskFullpaths"], r):              # RLdecon_for_zarr_block.m:111-128
+                    Z.writezarr_region(np.zeros(tuple(r[3:] - r[:3] + 1), out_dt, order="F"), tmp_path, list(r))
+                    continue
+                chunks.append(Z.readzarr(frameFullpath, inputBbox=list(b), pinned=True))
+                boxes.append([*(r[:3] - b[:3] + 1), *(r[3:] - b[:3] + 1)])
+                regions.append(r)
+            outs = _decon_chunks(chunks, boxes, cpsf, o, ctx, bg, o["EdgeErosion"]) if chunks else []
+            for r, ob in zip(regions, outs):
+                Z.writezarr_region(ob, tmp_path, list(r))
+        open(flag, "wb").close()
+    if os.path.isdir(out_path):                                                   # :272-280
+        shutil.rmtree(out_path)
     os.replace(tmp_path, out_path)
+    shutil.rmtree(flag_dir, ignore_errors=True)
+    zarr_mips(out_path, os.path.join(deconPath, "MIPs"), bs[2])                   # XR_MIP_zarr, axis [1 1 1]
     return out_path
+
+
+def zarr_mips(path, mip_dir, slab_z=256):
+    """XR_MIP_zarr(path, 'axis', [1 1 1]) (io/XR_MIP_zarr.m:56-67): the y, x and z maximum projections
+    of a Zarr array written as ``<mip_dir>/<name>_MIP_{y,x,z}.tif`` (each skipped when it exists),
+    reading the array in z-slabs of ``slab_z`` planes."""
+    from . import tiff as T
+    from . import zarrio as Z
+    fsname = os.path.splitext(os.path.basename(str(path).rstrip("/")))[0]
+    names = [os.path.join(mip_dir, f"{fsname}_MIP_{a}.tif") for a in "yxz"]
+    if all(os.path.exists(f) for f in names):
+        return names
+    (ny, nx, nz), _, dt = Z.getZarrInfo(path)
+    my = np.empty((nx, nz), dt, order="F")
+    mx = np.empty((ny, nz), dt, order="F")
+    mz = None
+    for z0 in range(0, nz, max(1, int(slab_z))):
+        z1 = min(nz, z0 + max(1, int(slab_z)))
+        v = Z.readzarr(path, inputBbox=[1, 1, z0 + 1, ny, nx, z1])
+        my[:, z0:z1] = v.max(axis=0)
+        mx[:, z0:z1] = v.max(axis=1)
+        mz = v.max(axis=2) if mz is None else np.maximum(mz, v.max(axis=2))
+    os.makedirs(mip_dir, exist_ok=True)
+    for f, m in zip(names, (my, mx, mz)):
+        if not os.path.exists(f):
+            T.writetiff(np.asfortranarray(m), f)
+    return names
 
 
 def _create_empty_zarr(path, shape, chunks, dtype):

@@ -54,6 +54,34 @@ def test_in_place_runner_writes_zeros_for_masked_regions_without_deconvolving(tm
     got = Z.readzarr(out)
     assert got.shape == vol.shape and got.dtype == np.uint16 and not got.any()
     assert not os.path.exists(stale)
+    assert not os.path.exists(os.path.join(dpath, "zarr_flag", "raw_7"))       # flags removed at the end
+    for ax, shape in (("y", (60, 40)), ("x", (70, 40)), ("z", (70, 60))):       # XR_MIP_zarr, axis [1 1 1]
+        mip = T.readtiff(os.path.join(dpath, "MIPs", f"raw_MIP_{ax}.tif"))
+        assert mip.shape == shape and not mip.any()
+
+
+def test_in_place_runner_resumes_flagged_tasks(tmp_path):
+    """A second call with the same uuid skips the tasks whose flag exists (RLdecon_large_in_place.m:217-221):
+    here the only task, so the temporary array is moved into place as it stands."""
+    vol = np.asfortranarray(np.random.default_rng(2).integers(100, 3000, (70, 60, 40)).astype(np.uint16))
+    zin = str(tmp_path / "raw.zarr")
+    Z.writezarr(vol, zin, blockSize=(32, 32, 32))
+    pfn = str(tmp_path / "psf.tif")
+    T.writetiff(np.ones((9, 9, 11), np.float32), pfn)
+    dpath = str(tmp_path / "decon")
+    os.makedirs(dpath)
+    part = np.asfortranarray(np.arange(70 * 60 * 40, dtype=np.uint32).reshape(70, 60, 40) % 5000).astype(np.uint16)
+    Z.writezarr(part, os.path.join(dpath, "raw.zarr_9"), blockSize=(32, 32, 32))
+    _, rb, _ = K.zarr_chunk_coordinates((70, 60, 40), batch_size=(64, 64, 64), block_size=(32, 32, 32),
+                                        same_batch_size=True, border=K.border_size((9, 9, 11)))
+    flags = os.path.join(dpath, "zarr_flag", "raw_9")
+    os.makedirs(flags)
+    open(os.path.join(flags, f"blocks_1_{len(rb)}.mat"), "wb").close()
+    out = K.RLdecon_large_in_place(zin, pfn, dpath, 0.108, 0.3, batchSize=(64, 64, 64), blockSize=(32, 32, 32),
+                                   psfGen=False, uuid="9")
+    np.testing.assert_array_equal(Z.readzarr(out), part)
+    np.testing.assert_array_equal(T.readtiff(os.path.join(dpath, "MIPs", "raw_MIP_z.tif")), part.max(axis=2))
+    assert not os.path.exists(flags)
 
 
 def test_mask_list_must_have_three_paths():
