@@ -152,12 +152,20 @@ def _erode_offsets(mask, offsets):
 
 
 def mask_edge_erosion(mask, E):
-    """decon_mask_edge_erosion.m:1-30."""
+    """decon_mask_edge_erosion.m:1-30.  MATLAB's ndims of an [ny nx 1] array is 2, so a single plane
+    takes the 2-D steps: no z faces (:11-13) and no z erosion (:23-28)."""
     mask = np.asarray(mask) > 0
-    E = int(E)
+    shape = mask.shape
+    if mask.ndim == 2:
+        mask = mask[:, :, None]
+    two_d = mask.shape[2] == 1
+    return _mask_edge_erosion3(mask, int(E), two_d).reshape(shape)
+
+
+def _mask_edge_erosion3(mask, E, two_d):
     if mask.all():                                             # :8-15 full rectangular mask
         m = mask.copy()
-        for ax in range(3):
+        for ax in range(2 if two_d else 3):
             idx = [slice(None)] * 3
             idx[ax] = slice(0, min(E, m.shape[ax]))
             m[tuple(idx)] = False
@@ -167,13 +175,15 @@ def mask_edge_erosion(mask, E):
     m = mask.copy()                                            # :18-29 irregular mask
     m[[0, -1], :, :] = False
     m[:, [0, -1], :] = False
-    m[:, :, [0, -1]] = False
+    if not two_d:
+        m[:, :, [0, -1]] = False
     d = disk_nhood(E - 1)
     r = d.shape[0] // 2
     offs = [(a - r, b - r, 0) for a, b in zip(*np.nonzero(d))]
     m = _erode_offsets(m, offs)
-    h = E - 1                                                  # true(2E-1, 1) along z
-    m = _erode_offsets(m, [(0, 0, o) for o in range(-h, h + 1)])
+    if not two_d:
+        h = E - 1                                              # true(2E-1, 1) along z
+        m = _erode_offsets(m, [(0, 0, o) for o in range(-h, h + 1)])
     return m
 
 

@@ -80,7 +80,8 @@ __global__ void k_post_from(VolDesc d, const float* __restrict__ src) {
             if (d.mask_mode == 1 || d.mask_mode == 3) m = d.mask8[i] != 0;
             else if (d.mask_mode == 2) {
                 const int E = d.erosion;
-                m = d.mask8[i] != 0 && y >= E && y < d.ny - E && x >= E && x < d.nx - E && z >= E && z < d.nz - E;
+                m = d.mask8[i] != 0 && y >= E && y < d.ny - E && x >= E && x < d.nx - E &&
+                    (d.nz == 1 || (z >= E && z < d.nz - E));      // one plane: MATLAB's 2-D case
             }
             J = __fmul_rn(__fadd_rn(__fmul_rn(J, d.scale), d.offset), (float)m);
         }
@@ -141,7 +142,8 @@ __global__ void k_mask_faces(uint8_t* m, int ny, int nx, int nz) {
         const int y = (int)(i % ny);
         const int x = (int)((i / ny) % nx);
         const int z = (int)(i / ((long long)ny * nx));
-        if (y == 0 || y == ny - 1 || x == 0 || x == nx - 1 || z == 0 || z == nz - 1) m[i] = 0;
+        // one plane is MATLAB's 2-D case (ndims 2): no z faces
+        if (y == 0 || y == ny - 1 || x == 0 || x == nx - 1 || (nz > 1 && (z == 0 || z == nz - 1))) m[i] = 0;
     }
 }
 

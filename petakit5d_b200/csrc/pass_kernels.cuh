@@ -64,7 +64,8 @@ __device__ __forceinline__ float post_value(const VolDesc& d, float J, long long
         if (d.mask_mode == 1 || d.mask_mode == 3) m = d.mask8[vi] != 0;
         else if (d.mask_mode == 2) {
             const int E = d.erosion;
-            m = d.mask8[vi] != 0 && y >= E && y < d.ny - E && x >= E && x < d.nx - E && z >= E && z < d.nz - E;
+            m = d.mask8[vi] != 0 && y >= E && y < d.ny - E && x >= E && x < d.nx - E &&
+                (d.nz == 1 || (z >= E && z < d.nz - E));          // one plane: MATLAB's 2-D case
         }
         J = __fmul_rn(__fadd_rn(__fmul_rn(J, d.scale), d.offset), (float)m);
     }

@@ -148,3 +148,20 @@ def test_damp_factor_tie_doubles():
     I = np.array([1.0, 1.0, 1.0], np.float32).reshape(3, 1, 1)
     out = O.postprocess(J, I, None, damp=2.0, save16bit=False)
     assert out.ravel().tolist() == [1.0, 4.0, 2.0]
+
+
+def test_single_plane_edge_erosion_takes_the_2d_steps():
+    """decon_mask_edge_erosion.m on an [ny nx 1] array: ndims is 2, so no z faces and no z erosion."""
+    from oracle.decon import mask_edge_erosion
+    full = np.ones((20, 17, 1), bool)
+    m = mask_edge_erosion(full, 3)
+    ref = np.zeros((20, 17), bool)
+    ref[3:17, 3:14] = True
+    np.testing.assert_array_equal(m[:, :, 0], ref)
+    np.testing.assert_array_equal(mask_edge_erosion(full[:, :, 0], 3), ref)
+    irr = np.ones((20, 17), bool)
+    irr[8, 8] = False
+    m2 = mask_edge_erosion(irr, 2)                              # disk(1): the 4-neighbourhood
+    assert m2.shape == (20, 17) and not m2[0].any() and not m2[:, -1].any()
+    assert not m2[8, 8] and not m2[7, 8] and not m2[8, 9] and m2[7, 7] and m2[5, 5]
+    np.testing.assert_array_equal(mask_edge_erosion(irr[:, :, None], 2)[:, :, 0], m2)
