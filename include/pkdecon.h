@@ -262,6 +262,15 @@ PK_API pk_status pk_host_free(void* ptr);
 PK_API pk_status pk_edge_erosion_edt(pk_ctx* ctx, const void* im, pk_dtype im_type, const int64_t dims[3],
                                      int32_t erosion, void* out, pk_dtype out_type, uint8_t* mask);
 
+/* ---------------------------------------------------------------- eroded mask */
+/* decon_mask_edge_erosion(im > 0, erosion) (decon/decon_mask_edge_erosion.m:1-30) on its own: the
+ * eroded-mask file of XR_RLdeconFrame3D.m:205-231.  im: host uint16/single [ny nx nz]; mask (host
+ * uint8, ny*nx*nz) receives 0/1.  A full mask loses `erosion` voxels at each face; otherwise the faces
+ * are cleared and the mask eroded by strel('disk', erosion-1) per plane and a (2*erosion-1)-long
+ * line in z.  A single plane (nz = 1) takes MATLAB's 2-D steps (no z faces, no z erosion). */
+PK_API pk_status pk_mask_edge_erosion(pk_ctx* ctx, const void* im, pk_dtype type, const int64_t dims[3],
+                                      int32_t erosion, uint8_t* mask);
+
 /* ---------------------------------------------------------------- edge taper */
 /* RLdecon.m:351-357: edgetaper(I(:,:,iz), PSF) for every z slice of a host uint16/single [ny nx nz]
  * volume (MATLAB Image Processing Toolbox edgetaper; the reference passes

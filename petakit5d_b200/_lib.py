@@ -103,6 +103,7 @@ _SIGS = {
     "pk_host_free": (C.c_int, [P]),
     "pk_edge_erosion_edt": (C.c_int, [P, P, C.c_int, I64x3, C.c_int32, P, C.c_int, P]),
     "pk_edgetaper": (C.c_int, [P, P, C.c_int, I64x3, P, P, P]),
+    "pk_mask_edge_erosion": (C.c_int, [P, P, C.c_int, I64x3, C.c_int32, P]),
     "pk_find_good_factor_number": (C.c_int64, [C.c_int64, C.c_int32, C.c_int32]),
     "pk_chunk_coordinates": (C.c_int64, [I64x3, I64x3, I64x3, P, C.c_int32, I64x3, P, P, P]),
     "pk_batch_decon": (C.c_int, [P, C.c_int32, C.c_int32, C.POINTER(Chunk), C.c_int, C.c_int32, P, P, P,

@@ -781,3 +781,78 @@ pk_status pk_decon_run(pk_ctx* ctx, int method, const void* d_in, pk_dtype in_ty
     std::vector<DeconJob> jobs{j};
     return pk_decon_multi(ctx, method, jobs, in_type, numit, p, st, io, dbg);
 }
+
+// ---- decon_mask_edge_erosion(im > 0, E) on its own (decon/decon_mask_edge_erosion.m:1-30), for the
+// eroded-mask files that XR_RLdeconFrame3D saves; the irregular branch runs the kernels above
+namespace {
+
+template <typename T>
+__global__ void k_positive(const T* __restrict__ im, long long n, uint8_t* __restrict__ m,
+                           unsigned long long* __restrict__ zeros) {
+    unsigned long long z = 0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const bool p = im[i] > (T)0;
+        m[i] = p;
+        z += !p;
+    }
+    if (z) atomicAdd(zeros, z);
+}
+
+// full mask: E voxels cleared at each face (:8-15), z only for more than one plane
+__global__ void k_full_faces(uint8_t* m, int ny, int nx, int nz, int E) {
+    const long long n = (long long)ny * nx * nz;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int y = (int)(i % ny);
+        const int x = (int)((i / ny) % nx);
+        const int z = (int)(i / ((long long)ny * nx));
+        if (y < E || y >= ny - E || x < E || x >= nx - E || (nz > 1 && (z < E || z >= nz - E))) m[i] = 0;
+    }
+}
+
+}  // namespace
+
+extern "C" pk_status pk_mask_edge_erosion(pk_ctx* ctx, const void* im, pk_dtype type, const int64_t dims[3],
+                                          int32_t erosion, uint8_t* mask) {
+    if (!ctx) return pk_fail(PK_ERR_INVALID, "null pk_ctx");
+    if (!im || !dims || !mask) return pk_fail(PK_ERR_INVALID, "NULL volume/dims/mask");
+    if (type != PK_U16 && type != PK_F32) return pk_fail(PK_ERR_INVALID, "volume must be uint16 or single");
+    if (dims[0] < 1 || dims[1] < 1 || dims[2] < 1 || dims[0] > INT32_MAX || dims[1] > INT32_MAX || dims[2] > INT32_MAX)
+        return pk_fail(PK_ERR_INVALID, "bad volume size");
+    if (erosion < 1 || erosion > 180) return pk_fail(PK_ERR_INVALID, "EdgeErosion must be in [1, 180]");
+    const int ny = (int)dims[0], nx = (int)dims[1], nz = (int)dims[2];
+    const long long n = (long long)ny * nx * nz;
+    const size_t es = type == PK_U16 ? 2 : 4;
+    std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+    cudaSetDevice(ctx->device);
+    cudaStream_t st = ctx->stream;
+    pk_status s;
+    void *din, *dm, *dm2, *dz, *doffs;
+    const std::vector<int2> disk = pk_disk_offsets(erosion - 1);
+    if ((s = pk_scratch(ctx, 37, es * n, &din)) != PK_OK) return s;
+    if ((s = pk_scratch(ctx, 38, n, &dm)) != PK_OK) return s;
+    if ((s = pk_scratch(ctx, 39, n, &dm2)) != PK_OK) return s;
+    if ((s = pk_scratch(ctx, 40, sizeof(unsigned long long), &dz)) != PK_OK) return s;
+    if ((s = pk_scratch(ctx, 41, sizeof(int2) * disk.size(), &doffs)) != PK_OK) return s;
+    PK_CUDA(cudaMemcpyAsync(din, im, es * n, cudaMemcpyHostToDevice, st));
+    PK_CUDA(cudaMemsetAsync(dz, 0, sizeof(unsigned long long), st));
+    if (type == PK_U16) k_positive<<<grid_for(n), 256, 0, st>>>((const uint16_t*)din, n, (uint8_t*)dm, (unsigned long long*)dz);
+    else k_positive<<<grid_for(n), 256, 0, st>>>((const float*)din, n, (uint8_t*)dm, (unsigned long long*)dz);
+    unsigned long long zeros = 0;
+    PK_CUDA(cudaMemcpyAsync(&zeros, dz, sizeof(zeros), cudaMemcpyDeviceToHost, st));
+    PK_CUDA(cudaStreamSynchronize(st));
+    if (zeros == 0) {
+        k_full_faces<<<grid_for(n), 256, 0, st>>>((uint8_t*)dm, ny, nx, nz, erosion);
+        ctx->launches += 2;
+    } else {                                                     // :18-29; k_erode_z is a copy for one plane
+        PK_CUDA(cudaMemcpyAsync(doffs, disk.data(), sizeof(int2) * disk.size(), cudaMemcpyHostToDevice, st));
+        k_mask_faces<<<grid_for(n), 256, 0, st>>>((uint8_t*)dm, ny, nx, nz);
+        k_erode_xy<<<grid_for(n), 256, 0, st>>>((const uint8_t*)dm, (uint8_t*)dm2, ny, nx, nz, (const int2*)doffs,
+                                                (int)disk.size());
+        k_erode_z<<<grid_for(n), 256, 0, st>>>((const uint8_t*)dm2, (uint8_t*)dm, ny, nx, nz, erosion - 1);
+        ctx->launches += 4;
+    }
+    PK_CUDA(cudaGetLastError());
+    PK_CUDA(cudaMemcpyAsync(mask, dm, n, cudaMemcpyDeviceToHost, st));
+    PK_CUDA(cudaStreamSynchronize(st));
+    return PK_OK;
+}

@@ -225,3 +225,22 @@ def fft3_r2c(d_in, dims, d_spec, ctx=None, stream=None):
 def fft3_c2r(d_spec, dims, d_out, ctx=None, stream=None):
     ctx = ctx or _lib.default_context()
     check(lib.pk_fft3_c2r_device(ctx.handle, ptr(d_spec), i64x3(dims), ptr(d_out), ptr(stream) if stream else None))
+
+
+def decon_mask_edge_erosion(mask, EdgeErosion, ctx=None):
+    """mask = decon_mask_edge_erosion(mask, EdgeErosion) (decon/decon_mask_edge_erosion.m:1-30) on the
+    GPU: ``mask > 0`` eroded at the volume's edges (full mask: EdgeErosion voxels off each face;
+    otherwise faces cleared, then strel('disk', EdgeErosion - 1) per plane and a line of
+    2 * EdgeErosion - 1 in z).  ``mask`` may be logical, uint8, uint16 or single; returns logical."""
+    ctx = ctx or _lib.default_context()
+    a = np.asarray(mask)
+    shape = a.shape
+    if a.dtype not in (np.uint16, np.float32):
+        a = (a > 0).astype(np.uint16)
+    while a.ndim < 3:
+        a = a[..., None]
+    a = np.asfortranarray(a)
+    out = np.empty(a.shape, np.uint8, order="F")
+    check(lib.pk_mask_edge_erosion(ctx.handle, ptr(a), _lib.PK_U16 if a.dtype == np.uint16 else _lib.PK_F32,
+                                   i64x3(a.shape), int(EdgeErosion), ptr(out)))
+    return out.astype(bool).reshape(shape, order="F")

@@ -279,3 +279,101 @@ def RLdecon(inputFn, outputFn, PSFfn, xyPixelSize, dz, dzPSF, **kw):
         os.makedirs(decon_path, exist_ok=True)
         _move_into_place(lambda f: write(deconvolved, f), outputFn)
     return deconvolved, None, dsr
+
+
+_FRAME3D_DEFAULTS = dict(
+    PSFfile="", Overwrite=False, save16bit=True, Rotate=False, Deskew=False, SkewAngle=-32.45, flipZstack=False,
+    Reverse=True, Background=None, EdgeSoften=5, zEdgeSoften=2, dzPSF=0.1, DeconIter=15, EdgeErosion=8,
+    ErodeMaskfile="", SaveMaskfile=False, RLMethod="simplified", wienerAlpha=0.005, OTFCumThresh=0.9,
+    hannWinBounds=(0.8, 1.0), skewed=None, fixIter=False, errThresh=None, CPUMaxMem=500,
+    batchSize=(1024, 1024, 1024), blockSize=(256, 256, 256), largeFile=False, largeMethod="inmemory",
+    saveZarr=False, save3Dstack=(True, True, True), mipAxis=(0, 0, 1), dampFactor=1.0, scaleFactor=None,
+    deconOffset=0.0, maskFullpaths=(), parseCluster=True, parseParfor=False, masterCompute=True, masterCPU=False,
+    GPUJob=False, jobLogDir="../job_logs", cpusPerTask=4, uuid="", maxTrialNum=3, unitWaitTime=2, debug=False,
+    saveStep=5, psfGen=True, mccMode=False, configFile="", GPUConfigFile="", ctx=None)
+
+
+def XR_RLdeconFrame3D(frameFullpaths, xyPixelSize, dz, deconPath="", **kw):
+    """XR_RLdeconFrame3D(frameFullpaths, xyPixelSize, dz, deconPath, ...)
+    (decon/XR_RLdeconFrame3D.m:1-316): for each frame, skip a missing input or an existing result
+    (unless ``Overwrite``); frames whose ``prod(size) * 4 B * 10`` exceeds ``CPUMaxMem`` GB (and every
+    frame after one, as the reference keeps ``largeFile`` set) go to the large-file runner of
+    ``largeMethod`` ('inplace' or 'inmemory', after which the call returns, as in the reference);
+    the others to RLdecon, with the eroded mask of the raw data saved as
+    ``<deconPath>/Masks/<name>_eroded.zarr`` and used as ``ErodeMaskfile`` when ``SaveMaskfile``
+    (:205-231).  The Slurm / parfor job options are accepted; the work runs in this process."""
+    import warnings
+    from . import chunking as K
+    from . import decon as D
+    low = {k.lower(): k for k in _FRAME3D_DEFAULTS}
+    o = dict(_FRAME3D_DEFAULTS)
+    for k, v in kw.items():
+        if k.lower() not in low:
+            raise TypeError(f"XR_RLdeconFrame3D: unknown parameter {k!r}")
+        o[low[k.lower()]] = v
+    if isinstance(frameFullpaths, str):
+        frameFullpaths = [frameFullpaths]
+    uid = o["uuid"] or _uuid.uuid4().hex[:8]
+    s3 = o["save3Dstack"]
+    save3d = [bool(s3)] * 3 if np.ndim(s3) == 0 or len(s3) == 1 else [bool(v) for v in s3]
+    save3d[1] = save3d[1] and bool(o["Deskew"])
+    save3d[2] = save3d[2] and bool(o["Rotate"])
+    large = bool(o["largeFile"])
+    if not large and not any(save3d) and not any(np.asarray(o["mipAxis"]) > 0):
+        raise ValueError("Either the 3D stack or the MIP for at least one axis needs to be saved!")
+    ext_out = ".zarr" if o["saveZarr"] else ".tif"
+    for frame in frameFullpaths:
+        if not os.path.exists(frame):
+            warnings.warn(f"{frame} does not exist! Skip it!")
+            continue
+        pathstr, name = os.path.split(str(frame).rstrip("/"))
+        fsname = os.path.splitext(name)[0]
+        dpath = deconPath or os.path.join(pathstr, "matlab_decon")
+        os.makedirs(dpath, exist_ok=True)
+        im_size = _size(frame)
+        if np.prod(im_size) * 4 / 2 ** 30 * 10 > float(o["CPUMaxMem"]):
+            large = True
+        decon_fn = os.path.join(dpath, fsname + ext_out)
+        dsr_fn = os.path.join(dpath, "DSR", fsname + ext_out)
+        if os.path.exists(decon_fn) and not o["Overwrite"]:
+            continue
+        common = dict(save16bit=o["save16bit"], Deskew=o["Deskew"], SkewAngle=o["SkewAngle"],
+                      Background=o["Background"], dzPSF=o["dzPSF"], DeconIter=o["DeconIter"], RLMethod=o["RLMethod"],
+                      skewed=o["skewed"], wienerAlpha=o["wienerAlpha"], OTFCumThresh=o["OTFCumThresh"],
+                      hannWinBounds=o["hannWinBounds"], fixIter=o["fixIter"], dampFactor=o["dampFactor"],
+                      scaleFactor=o["scaleFactor"], deconOffset=o["deconOffset"], debug=o["debug"],
+                      psfGen=o["psfGen"], ctx=o["ctx"])
+        if not large:
+            erode_fn = o["ErodeMaskfile"]
+            if o["EdgeErosion"] > 0 and o["SaveMaskfile"]:                        # :205-231
+                raw = _read(frame)
+                if o["flipZstack"]:
+                    raw = np.asfortranarray(np.asarray(raw)[:, :, ::-1])
+                m = D.decon_mask_edge_erosion(raw, o["EdgeErosion"], ctx=o["ctx"])
+                raw = None
+                erode_fn = os.path.join(dpath, "Masks", f"{fsname}_eroded.zarr")
+                tmp = os.path.join(dpath, "Masks", f"{fsname}_eroded_{uid}.zarr")
+                Z.writezarr(m.astype(np.uint8), tmp, blockSize=tuple(int(v) for v in o["blockSize"]), overwrite=True)
+                if os.path.isdir(erode_fn):
+                    shutil.rmtree(erode_fn)
+                os.replace(tmp, erode_fn)
+            RLdecon(frame, decon_fn, o["PSFfile"], xyPixelSize, dz, o["dzPSF"], Rotate=o["Rotate"], DSRCombined=True,
+                    Reverse=o["Reverse"], saveZarr=o["saveZarr"], blockSize=o["blockSize"], flipZstack=o["flipZstack"],
+                    EdgeErosion=o["EdgeErosion"], ErodeMaskfile=erode_fn, errThresh=o["errThresh"],
+                    saveStep=o["saveStep"], useGPU=o["GPUJob"], save3Dstack=save3d, mipAxis=o["mipAxis"],
+                    **{k: v for k, v in common.items() if k != "dzPSF"})
+            if (save3d[0] and os.path.exists(decon_fn)) or (save3d[2] and os.path.exists(dsr_fn)):
+                continue
+        method = str(o["largeMethod"]).lower()
+        if method == "inplace":
+            K.RLdecon_large_in_place(frame, o["PSFfile"], dpath, xyPixelSize, dz, flipZstack=o["flipZstack"],
+                                     batchSize=o["batchSize"], blockSize=o["blockSize"], EdgeErosion=o["EdgeErosion"],
+                                     maskFullpaths=o["maskFullpaths"], parseCluster=o["parseCluster"],
+                                     parseParfor=o["parseParfor"], cpusPerTask=o["cpusPerTask"], GPUJob=o["GPUJob"],
+                                     uuid=uid, **common)
+            return
+        if method == "inmemory":
+            K.RLdecon_large_in_memory(frame, o["PSFfile"], decon_fn, xyPixelSize, dz, flipZstack=o["flipZstack"],
+                                      EdgeErosion=o["EdgeErosion"], batchSize=o["batchSize"], saveZarr=o["saveZarr"],
+                                      maskFullpaths=o["maskFullpaths"], useGPU=o["GPUJob"], uuid=uid, **common)
+            return

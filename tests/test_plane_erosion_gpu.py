@@ -23,3 +23,15 @@ def test_single_plane_edge_erosion_matches_oracle(irregular):
     assert np.array_equal(J == 0, ref == 0)                     # the mask is bit-exact
     assert J[40:54, 30:46, 0].all()                              # a plane is not cleared as a z face
     assert O.rel_l2(J, ref) <= 1e-3
+
+
+@pytest.mark.parametrize("shape,hole", [((40, 36, 20), False), ((40, 36, 20), True), ((40, 36, 1), True),
+                                        ((40, 36, 1), False)])
+def test_mask_edge_erosion_entry_matches_oracle(shape, hole):
+    """pk_mask_edge_erosion (decon_mask_edge_erosion(im > 0, E) on its own) against the oracle."""
+    vol = np.asfortranarray((np.random.default_rng(5).random(shape) * 1000 + 1).astype(np.float32))
+    if hole:
+        vol[10:20, 5:15, :] = 0
+    for E in (1, 3, 4):
+        got = D.decon_mask_edge_erosion(vol, E)
+        np.testing.assert_array_equal(got, O.mask_edge_erosion(vol > 0, E))

@@ -38,3 +38,24 @@ def test_zero_iterations_write_the_input_through_the_chosen_writer(tmp_path, sav
         np.testing.assert_array_equal(T.readtiff(out), ref)
     np.testing.assert_array_equal(T.readtiff(str(tmp_path / "d" / "MIPs" / "frame_MIP_z.tif")), ref.max(axis=2))
     assert sorted(os.listdir(tmp_path / "d")) == ["MIPs", os.path.basename(out)]   # no temporaries left
+
+
+def test_frame3d_options_and_skips(tmp_path):
+    """XR_RLdeconFrame3D.m:145-193: nothing to save is an error; missing frames and frames whose
+    result exists (without Overwrite) are skipped before any GPU work."""
+    import warnings
+    from petakit5d_b200.rldecon import XR_RLdeconFrame3D
+    with pytest.raises(ValueError):
+        XR_RLdeconFrame3D(["a.tif"], 0.108, 0.3, str(tmp_path), save3Dstack=[False, False, False], mipAxis=[0, 0, 0])
+    with pytest.raises(TypeError):
+        XR_RLdeconFrame3D(["a.tif"], 0.108, 0.3, str(tmp_path), notAnOption=1)
+    with warnings.catch_warnings(record=True) as w:
+        warnings.simplefilter("always")
+        XR_RLdeconFrame3D([str(tmp_path / "missing.tif")], 0.108, 0.3, str(tmp_path))
+    assert any("does not exist" in str(x.message) for x in w)
+    raw = str(tmp_path / "frame.tif")
+    T.writetiff(np.ones((8, 8, 4), np.uint16), raw)
+    os.makedirs(tmp_path / "matlab_decon")
+    T.writetiff(np.full((8, 8, 4), 3, np.uint16), str(tmp_path / "matlab_decon" / "frame.tif"))
+    XR_RLdeconFrame3D([raw], 0.108, 0.3, "", PSFfile="psf.tif")       # the result exists: skipped
+    assert T.readtiff(str(tmp_path / "matlab_decon" / "frame.tif")).max() == 3

@@ -117,3 +117,19 @@ def test_rldecon_zarr_input_and_output(tmp_path):
     np.testing.assert_array_equal(J3, Jt)
     np.testing.assert_array_equal(d3, dt)
     np.testing.assert_array_equal(Z.readzarr(dsr_fn), dt)
+
+
+def test_frame3d_saves_the_eroded_mask_and_uses_it(tmp_path):
+    """XR_RLdeconFrame3D.m:205-231: the eroded mask of the raw data saved as Masks/<name>_eroded.zarr and
+    used as ErodeMaskfile gives the result of RLdecon's own erosion."""
+    from oracle.decon import mask_edge_erosion
+    from petakit5d_b200.rldecon import XR_RLdeconFrame3D
+    vol, bead, raw, pfn = _files(tmp_path)
+    dpath = str(tmp_path / "out")
+    kw = dict(Background=100, DeconIter=2, RLMethod="simplified", EdgeErosion=4, save16bit=False)
+    XR_RLdeconFrame3D([raw], 0.108, 0.3, dpath, PSFfile=pfn, SaveMaskfile=True, **kw)
+    m = Z.readzarr(os.path.join(dpath, "Masks", "frame_CamA_eroded.zarr"))
+    np.testing.assert_array_equal(m.astype(bool), mask_edge_erosion(vol > 0, 4))
+    J = T.readtiff(os.path.join(dpath, "frame_CamA.tif"))
+    ref, _, _ = RLdecon(raw, str(tmp_path / "ref" / "frame_CamA.tif"), pfn, 0.108, 0.3, 0.1, **kw)
+    np.testing.assert_array_equal(J, ref)
