@@ -8,8 +8,6 @@ device-pointer entry point's (pk_decon_lucy_omw_device) within the tolerance of 
 tests; that a call leaves the device's free memory unchanged; and that a volume larger than the
 array's 1,048,576-voxel limit is refused.  The file is named so pytest collects it last.
 """
-import ctypes as C
-
 import numpy as np
 import pytest
 
