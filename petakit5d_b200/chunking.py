@@ -424,13 +424,15 @@ def zarr_mips(path, mip_dir, slab_z=256):
 
 
 def _create_empty_zarr(path, shape, chunks, dtype):
-    """An order-F, zlib, fill-value-0 array with no chunk files yet (createzarr's role)."""
+    """An order-F, zlib, fill-value-0 array with no chunk files yet (createzarr's role); "/" chunk keys
+    when it has more than 10000 chunks, else "." (RLdecon_large_in_place.m:186-191)."""
     import json
     if os.path.isdir(path):
         shutil.rmtree(path)
     os.makedirs(path)
     meta = {"chunks": [int(c) for c in chunks], "compressor": {"id": "zlib", "level": 1},
-            "dimension_separator": ".", "dtype": np.dtype(dtype).newbyteorder("<").str, "fill_value": 0,
+            "dimension_separator": "/" if np.prod(-(-np.asarray(shape) // np.asarray(chunks))) > 10000 else ".",
+            "dtype": np.dtype(dtype).newbyteorder("<").str, "fill_value": 0,
             "filters": None, "order": "F", "shape": [int(v) for v in shape], "zarr_format": 2}
     with open(os.path.join(path, ".zarray"), "w") as f:
         json.dump(meta, f)

@@ -114,7 +114,12 @@ bool read_file(const std::string& path, std::vector<uint8_t>& buf) {
 }
 
 bool write_file(const std::string& path, const void* p, size_t n) {
-    const int fd = open(path.c_str(), O_WRONLY | O_CREAT | O_TRUNC, 0644);
+    int fd = open(path.c_str(), O_WRONLY | O_CREAT | O_TRUNC, 0644);
+    if (fd < 0 && errno == ENOENT) {              // "/" keys: the chunk's parent folders first
+        for (size_t i = path.find('/', 1); i != std::string::npos; i = path.find('/', i + 1))
+            mkdir(path.substr(0, i).c_str(), 0755);
+        fd = open(path.c_str(), O_WRONLY | O_CREAT | O_TRUNC, 0644);
+    }
     if (fd < 0) return false;
     size_t done = 0;
     while (done < n) {
@@ -521,7 +526,7 @@ extern "C" pk_status pk_zarr_write_region(const char* path, const void* data, co
     ZMeta m;
     pk_status s = parse_meta(path, m);
     if (s != PK_OK) return s;
-    if (m.order_c || m.separator != "." || m.big_endian) return pk_fail(PK_ERR_UNSUPPORTED, "zarr: region writes need order F, '.' keys, little endian");
+    if (m.order_c || m.big_endian) return pk_fail(PK_ERR_UNSUPPORTED, "zarr: region writes need order F, little endian");
     int64_t lo[3], hi[3], c0[3], nc[3];
     for (int d = 0; d < 3; d++) {
         lo[d] = bbox[d] - 1;

@@ -127,3 +127,29 @@ def test_uncompressed_reads_by_pieces_fill_swap_and_truncation(tmp_path):
         f.truncate(100)
     with pytest.raises(PkError):
         Z.readzarr(p, threads=16)
+
+
+def test_region_writes_with_nested_keys(tmp_path):
+    """'/' chunk keys (the in-place runner's arrays of more than 10000 chunks): region writes create
+    the chunk folders; Python's reading of the format agrees."""
+    v = _vol(np.uint16, (40, 36, 20), seed=8)
+    p = str(tmp_path / "n.zarr")
+    OZ.write(p, np.zeros_like(v), (16, 16, 8), separator="/")
+    import shutil
+    for d in os.listdir(p):
+        if not d.startswith("."):
+            shutil.rmtree(os.path.join(p, d))                       # no chunk folders yet
+    Z.writezarr_region(v[16:40, 0:32, 8:20], p, [17, 1, 9, 40, 32, 20])
+    ref = np.zeros_like(v)
+    ref[16:40, 0:32, 8:20] = v[16:40, 0:32, 8:20]
+    np.testing.assert_array_equal(OZ.read(p), ref)
+    assert os.path.isfile(os.path.join(p, "1", "0", "1"))
+
+
+def test_runner_arrays_use_nested_keys_past_10000_chunks(tmp_path):
+    import json
+    from petakit5d_b200.chunking import _create_empty_zarr
+    _create_empty_zarr(str(tmp_path / "a.zarr"), (200, 100, 10), (2, 2, 2), np.uint16)      # 25000 chunks
+    _create_empty_zarr(str(tmp_path / "b.zarr"), (200, 100, 10), (20, 20, 10), np.uint16)
+    sep = [json.load(open(str(tmp_path / f / ".zarray")))["dimension_separator"] for f in ("a.zarr", "b.zarr")]
+    assert sep == ["/", "."]
