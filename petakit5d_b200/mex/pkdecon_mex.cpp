@@ -10,6 +10,7 @@
 //   volout   = pkdecon_mex('dsr', vol, angle, dz, xyPixelSize, reverse, objectiveScan, xStepThresh, bbox, save16bit)
 //                                                                 % deskewRotateFrame3D
 //   J        = pkdecon_mex('edgetaper', vol, PSF)                 % edgetaper of every z slice (RLdecon.m:352-357)
+//   mask     = pkdecon_mex('mask_erosion', im, EdgeErosion)       % decon_mask_edge_erosion(im > 0, E)
 //   data     = pkdecon_mex('readtiff', path[, [z1 z2]])            % parallelReadTiff
 //   pkdecon_mex('writetiff', path, data, compression)             % parallelWriteTiff ('lzw' | 'none')
 //   sz       = pkdecon_mex('tiffsize', path)                      % getImageSizeMex
@@ -259,6 +260,20 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
         const mwSize dd[3] = {(mwSize)d[0], (mwSize)d[1], (mwSize)d[2]};
         plhs[0] = mxCreateNumericArray(3, dd, t == PK_U16 ? mxUINT16_CLASS : mxSINGLE_CLASS, mxREAL);
         check(pk_edgetaper(ctx(), mxGetData(prhs[1]), t, d, mxGetPr(prhs[2]), pd, mxGetData(plhs[0])));
+        return;
+    }
+    if (!strcmp(cmd, "mask_erosion")) {
+        if (nrhs < 3) mexErrMsgIdAndTxt("pkdecon:invalid", "mask_erosion: im, EdgeErosion");
+        int64_t d[3];
+        dims3(prhs[1], d);
+        pk_dtype t;
+        if (mxGetClassID(prhs[1]) == mxUINT16_CLASS) t = PK_U16;
+        else if (mxGetClassID(prhs[1]) == mxSINGLE_CLASS) t = PK_F32;
+        else mexErrMsgIdAndTxt("pkdecon:invalid", "im must be uint16 or single");
+        const mwSize dd[3] = {(mwSize)d[0], (mwSize)d[1], (mwSize)d[2]};
+        plhs[0] = mxCreateLogicalArray(3, dd);                                // logical: one byte, 0 or 1
+        check(pk_mask_edge_erosion(ctx(), mxGetData(prhs[1]), t, d, (int32_t)mxGetScalar(prhs[2]),
+                                   (uint8_t*)mxGetData(plhs[0])));
         return;
     }
     if (!strcmp(cmd, "readtiff") || !strcmp(cmd, "tiffsize")) {

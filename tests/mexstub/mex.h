@@ -14,6 +14,7 @@ extern "C" {
 void mexErrMsgIdAndTxt(const char* id, const char* fmt, ...);
 int mexAtExit(void (*fn)(void));
 mxArray* mxCreateNumericArray(mwSize ndim, const mwSize* dims, mxClassID c, mxComplexity flag);
+mxArray* mxCreateLogicalArray(mwSize ndim, const mwSize* dims);
 mxArray* mxCreateDoubleMatrix(mwSize m, mwSize n, mxComplexity flag);
 mxArray* mxCreateDoubleScalar(double v);
 void mxDestroyArray(mxArray* a);
