@@ -293,11 +293,16 @@ def RLdecon_large_in_memory(frameFullpath, psfFullpath, deconFullpath, xyPixelSi
     for r, ob in zip(rb, outs):
         out[r[0] - 1:r[3], r[1] - 1:r[4], r[2] - 1:r[5]] = ob
     if erosion > 0:                                                                     # :146-168, 267-270
-        mask = edge_erosion_mask(im, erosion, out=out, ctx=ctx)
-        if o["SaveMaskfile"]:
-            mp = os.path.join(decon_path, "Masks", f"{fsname}_eroded.tif")
-            os.makedirs(os.path.dirname(mp), exist_ok=True)
-            T.writetiff(mask.astype(np.uint8), mp)
+        mp = os.path.join(decon_path, "Masks", f"{fsname}_eroded.tif")
+        if o["SaveMaskfile"] and os.path.exists(mp):       # the common mask saved for this name (:149-157)
+            out *= (T.readtiff(mp) > 0).reshape(out.shape, order="F")
+        else:
+            mask = edge_erosion_mask(im, erosion, out=out, ctx=ctx)
+            if o["SaveMaskfile"]:                                                       # :160-164
+                os.makedirs(os.path.dirname(mp), exist_ok=True)
+                tmp = os.path.join(os.path.dirname(mp), f"{fsname}_eroded_{o['uuid'] or os.getpid()}.tif")
+                T.writetiff(mask.astype(np.uint8), tmp)
+                os.replace(tmp, mp)
     if o["ErodeMaskfile"] and os.path.exists(o["ErodeMaskfile"]):
         out *= (T.readtiff(o["ErodeMaskfile"]) > 0).reshape(out.shape, order="F").astype(out.dtype)
     os.makedirs(decon_path or ".", exist_ok=True)

@@ -134,3 +134,23 @@ def test_large_runner_deskew_rotate_sets_the_border_psf_only(tmp_path):
         box = [*(r[:3] - b[:3] + 1), *(r[3:] - b[:3] + 1)]
         ref[r[0] - 1:r[3], r[1] - 1:r[4], r[2] - 1:r[5]] = D.decon_lucy_function(c, p32, 2, Background=99, bbox=box)[0]
     np.testing.assert_array_equal(out, ref)
+
+
+def test_large_runner_reuses_a_saved_common_mask(tmp_path):
+    """RLdecon_large_in_memory.m:149-164: with SaveMaskfile, an existing Masks/<name>_eroded.tif (saved
+    for another channel or time point) is applied instead of a mask computed from this frame."""
+    psf_true = synth.gaussian_psf((31, 31, 41))
+    vol = synth.puncta_volume((150, 130, 64), 150, psf_true, seed=17)
+    bead = synth.measured_psf((32, 32, 41), sigma_xy=1.3, sigma_z=3.0, seed=18)
+    fin, pfn = str(tmp_path / "raw.tif"), str(tmp_path / "psf.tif")
+    T.writetiff(vol, fin)
+    T.writetiff(bead, pfn)
+    plain = K.RLdecon_large_in_memory(fin, pfn, str(tmp_path / "a" / "raw.tif"), 0.108, 0.3, DeconIter=2,
+                                      batchSize=(64, 64, 64), EdgeErosion=0)
+    common = np.zeros(vol.shape, np.uint8, order="F")
+    common[20:120, 10:100, 5:60] = 1
+    os.makedirs(tmp_path / "b" / "Masks")
+    T.writetiff(common, str(tmp_path / "b" / "Masks" / "raw_eroded.tif"))
+    out = K.RLdecon_large_in_memory(fin, pfn, str(tmp_path / "b" / "raw.tif"), 0.108, 0.3, DeconIter=2,
+                                    batchSize=(64, 64, 64), EdgeErosion=4, SaveMaskfile=True)
+    np.testing.assert_array_equal(out, plain * common.astype(bool))
