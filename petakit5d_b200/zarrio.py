@@ -52,8 +52,12 @@ def readzarr(filepath, inputBbox=None, pinned=False, threads=0):
     return out
 
 
-def writezarr(data, filepath, blockSize=(500, 500, 500), compressor="zlib", overwrite=False, threads=0):
-    """writezarr(data, filepath, 'blockSize', [...]) (io/writezarr.m): order F, separator '.'."""
+def writezarr(data, filepath, blockSize=(500, 500, 500), compressor="zlib", overwrite=False, threads=0,
+              dimSeparator="."):
+    """writezarr(data, filepath, 'blockSize', [...], 'dimSeparator', ...) (io/writezarr.m): order F;
+    chunk keys joined by '.' (the default) or '/' (nested folders)."""
+    if dimSeparator not in (".", "/"):
+        raise ValueError("dimSeparator must be '.' or '/'")
     a = np.asarray(data)
     if a.dtype == np.bool_:
         a = a.astype(np.uint8)
@@ -69,8 +73,20 @@ def writezarr(data, filepath, blockSize=(500, 500, 500), compressor="zlib", over
         shutil.rmtree(str(filepath))
     os.makedirs(os.path.dirname(os.path.abspath(str(filepath))), exist_ok=True)
     bits, isf = _W[a.dtype]
-    check(lib.pk_zarr_write(os.fsencode(str(filepath)), ptr(a), i64x3(a.shape), bits, isf, i64x3(bs),
-                            _COMP[compressor if compressor is None else str(compressor).lower()], int(threads)))
+    comp = _COMP[compressor if compressor is None else str(compressor).lower()]
+    if dimSeparator == "/":                 # the metadata, then the whole array as one region write
+        import json
+        os.makedirs(str(filepath), exist_ok=True)
+        meta = {"chunks": [int(min(b, n)) for b, n in zip(bs, a.shape)],
+                "compressor": None if comp == 0 else {"id": "zlib" if comp == 1 else "gzip", "level": 1},
+                "dimension_separator": "/", "dtype": f"<{'f' if isf else 'u'}{bits // 8}", "fill_value": 0,
+                "filters": None, "order": "F", "shape": [int(n) for n in a.shape], "zarr_format": 2}
+        with open(os.path.join(str(filepath), ".zarray"), "w") as f:
+            json.dump(meta, f, indent=4)
+        writezarr_region(a, filepath, [1, 1, 1, *a.shape], threads=threads)
+        return
+    check(lib.pk_zarr_write(os.fsencode(str(filepath)), ptr(a), i64x3(a.shape), bits, isf, i64x3(bs), comp,
+                            int(threads)))
 
 
 def writezarr_region(data, filepath, bbox, threads=0):

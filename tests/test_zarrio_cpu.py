@@ -153,3 +153,17 @@ def test_runner_arrays_use_nested_keys_past_10000_chunks(tmp_path):
     _create_empty_zarr(str(tmp_path / "b.zarr"), (200, 100, 10), (20, 20, 10), np.uint16)
     sep = [json.load(open(str(tmp_path / f / ".zarray")))["dimension_separator"] for f in ("a.zarr", "b.zarr")]
     assert sep == ["/", "."]
+
+
+@pytest.mark.parametrize("comp", ["zlib", None])
+def test_writezarr_nested_keys(tmp_path, comp):
+    """writezarr(..., 'dimSeparator', '/') (io/writezarr.m:21): nested chunk folders, read back by the
+    format restatement and by the reader."""
+    v = _vol(np.uint16, (50, 40, 30), seed=9)
+    p = str(tmp_path / "s.zarr")
+    Z.writezarr(v, p, blockSize=(32, 32, 16), compressor=comp, dimSeparator="/")
+    assert os.path.isdir(os.path.join(p, "1", "1"))
+    np.testing.assert_array_equal(OZ.read(p), v)
+    np.testing.assert_array_equal(Z.readzarr(p), v)
+    with pytest.raises(ValueError):
+        Z.writezarr(v, p, dimSeparator="_")
