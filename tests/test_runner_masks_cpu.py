@@ -104,3 +104,22 @@ def test_in_place_runner_accepts_deskew(tmp_path):
     out = K.RLdecon_large_in_place(zin, pfn, str(tmp_path / "d"), 0.108, 0.3, batchSize=(32, 32, 32),
                                    blockSize=(32, 32, 32), maskFullpaths=paths, psfGen=False, Deskew=True)
     assert not Z.readzarr(out).any()
+
+
+def test_frame3d_sends_large_frames_to_the_in_place_runner_and_returns(tmp_path):
+    """XR_RLdeconFrame3D.m:164-168, 245-262: a frame over CPUMaxMem goes to RLdecon_large_in_place, after
+    which the call returns (the next frame is not processed), as in the reference."""
+    from petakit5d_b200.rldecon import XR_RLdeconFrame3D
+    vol = np.asfortranarray(np.random.default_rng(3).integers(100, 3000, (40, 36, 20)).astype(np.uint16))
+    frames = [str(tmp_path / "f1.zarr"), str(tmp_path / "f2.zarr")]
+    for f in frames:
+        Z.writezarr(vol, f, blockSize=(32, 32, 32))
+    pfn = str(tmp_path / "psf.tif")
+    T.writetiff(np.ones((9, 9, 11), np.float32), pfn)
+    paths = _masks(tmp_path, 40, 36, 20, xy=np.zeros((40, 36), bool))
+    dpath = str(tmp_path / "decon")
+    XR_RLdeconFrame3D(frames, 0.108, 0.3, dpath, PSFfile=pfn, CPUMaxMem=0, largeMethod="inplace",
+                      batchSize=[32, 32, 32], blockSize=[32, 32, 32], maskFullpaths=paths, psfGen=False, uuid="5")
+    assert os.path.isdir(os.path.join(dpath, "f1.zarr")) and not Z.readzarr(os.path.join(dpath, "f1.zarr")).any()
+    assert not os.path.exists(os.path.join(dpath, "f2.zarr"))
+    assert os.path.exists(os.path.join(dpath, "MIPs", "f1_MIP_z.tif"))
