@@ -79,6 +79,14 @@ PK_API int64_t pk_ctx_kernel_launches(pk_ctx* ctx);
 PK_API pk_status pk_ctx_profile(pk_ctx* ctx, int32_t enable);
 PK_API int32_t pk_ctx_profile_read(pk_ctx* ctx, char* buf, int32_t cap);
 
+/* Failure-detection self-test (no counterpart in the reference).  Every wait inside the pass
+ * kernels is bounded: a wait that runs out records it in the context's device-wait status word
+ * and the kernel returns, and the next call on the context (or the synchronous call itself)
+ * returns PK_ERR_TIMEOUT.  This call runs one CTA that waits on a barrier nothing completes,
+ * bounded by limit_ns (1e3 .. 1e9), and returns what such a call returns (PK_ERR_TIMEOUT); the
+ * context stays usable afterwards. */
+PK_API pk_status pk_selftest_device_wait(pk_ctx* ctx, int64_t limit_ns);
+
 /* Output extent for dims/params: the bbox size when has_bbox, else dims. */
 PK_API pk_status pk_output_dims(const int64_t dims[3], const pk_decon_params* p, int64_t out_dims[3]);
 
@@ -147,10 +155,11 @@ PK_API pk_status pk_decon_lucy_omw_device(pk_ctx* ctx, const void* d_in, pk_dtyp
  * 32.4 MB, held on each GPU that loads the library until exit).  d_in/d_out are device pointers,
  * the PSFs host arrays; the work is queued on `stream` (a cudaStream_t, NULL = default stream) of
  * the calling thread's current device.  Limit: 1,048,576 voxels per volume (larger ones return
- * PK_ERR_UNSUPPORTED); deconOffset and EdgeErosion are not supported.  Every call shares the array
- * and leaves its contents behind, so calls that overlap on the GPU race: issue them one after
- * another on one stream.  The first call on a device looks up the array's address and should come
- * before any stream capture. */
+ * PK_ERR_UNSUPPORTED); deconOffset, EdgeErosion and NUMIT = 0 return PK_ERR_UNSUPPORTED.  Every
+ * call shares the array and leaves its contents behind, so calls that overlap on the GPU race:
+ * issue them one after another on one stream.  The first call on a device looks up the array's
+ * address and should come before any stream capture; that address is kept for the process, so do
+ * not call this entry point on a device after cudaDeviceReset. */
 PK_API pk_status pk_decon_lucy_omw_noalloc(const void* d_in, pk_dtype in_type, const int64_t dims[3],
                                            const float* psf_f, const int64_t psf_f_dims[3],
                                            const float* psf_b, const int64_t psf_b_dims[3], int32_t numit,

@@ -62,6 +62,7 @@ _SIGS = {
     "pk_ctx_kernel_launches": (C.c_int64, [P]),
     "pk_ctx_profile": (C.c_int, [P, C.c_int32]),
     "pk_ctx_profile_read": (C.c_int32, [P, C.c_char_p, C.c_int32]),
+    "pk_selftest_device_wait": (C.c_int, [P, C.c_int64]),
     "pk_output_dims": (C.c_int, [I64x3, C.POINTER(DeconParams), I64x3]),
     "pk_decon_lucy": (C.c_int, [P, P, C.c_int, I64x3, P, I64x3, C.c_int32, C.POINTER(DeconParams), P,
                                 C.POINTER(C.c_int32)]),

@@ -92,6 +92,17 @@ pk_ctx* pk_ctx_create(int device) {
         delete ctx;
         return nullptr;
     }
+    // the device-wait status word: page-locked, written by the kernels only when a wait runs out
+    if (cudaHostAlloc((void**)&ctx->h_err, 64, cudaHostAllocMapped) != cudaSuccess ||
+        cudaHostGetDevicePointer((void**)&ctx->d_err, ctx->h_err, 0) != cudaSuccess) {
+        cudaGetLastError();
+        if (ctx->h_err) cudaFreeHost(ctx->h_err);
+        cudaStreamDestroy(ctx->stream);
+        pk_set_error("page-locked status word: cudaHostAlloc failed");
+        delete ctx;
+        return nullptr;
+    }
+    *(volatile int*)ctx->h_err = 0;
     return ctx;
 }
 
@@ -142,6 +153,7 @@ void pk_ctx_destroy(pk_ctx* ctx) {
     for (auto e : ctx->ev_pool) cudaEventDestroy(e);
         ctx->host_pinned.clear();
         cudaStreamDestroy(ctx->stream);
+        if (ctx->h_err) cudaFreeHost(ctx->h_err);
     }
     delete ctx;
 }
@@ -277,7 +289,7 @@ static pk_status decon_host(pk_ctx* ctx, int method, const void* in, pk_dtype in
         PK_CUDA(cudaMemcpyAsync(out, d_out, outb, cudaMemcpyDeviceToHost, st));
         PK_CUDA(cudaStreamSynchronize(st));
     }
-    return PK_OK;
+    return pk_check_device_waits(ctx);   // a device wait of this call that ran out
 }
 
 // ---- asynchronous host-buffer calls

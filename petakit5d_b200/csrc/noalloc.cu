@@ -14,8 +14,8 @@
 //   * at most PK_NOALLOC_MAX_VOXELS voxels per volume (1,048,576, e.g. 128 x 128 x 64); larger
 //     volumes are rejected with PK_ERR_UNSUPPORTED.  The array (about 32.4 MB) is held on every
 //     GPU that loads the library until the process exits;
-//   * deconOffset and EdgeErosion (which need a mask volume) are rejected; dampFactor,
-//     scaleFactor, save16bit and bbox are supported;
+//   * deconOffset and EdgeErosion (which need a mask volume) and NUMIT = 0 are rejected with
+//     PK_ERR_UNSUPPORTED; dampFactor, scaleFactor, save16bit and bbox are supported;
 //   * every call uses the same array and the array keeps the last call's contents: the call
 //     clears what must start at zero (the OTF scatter volume) itself.  Calls whose work overlaps
 //     on the GPU (two host threads, or two streams) race on the array and corrupt each other's
@@ -23,7 +23,8 @@
 //   * the call runs on the calling thread's current device.  The first call on a device looks up
 //     the array's device address (cudaGetSymbolAddress, once per device, with that device
 //     current) and sets the kernels' shared-memory limits; make that first call before any
-//     stream capture.
+//     stream capture.  Both are kept for the life of the process: a program that resets a device
+//     (cudaDeviceReset) must not call this entry point on that device afterwards.
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -128,7 +129,9 @@ extern "C" pk_status pk_decon_lucy_omw_noalloc(const void* d_in, pk_dtype in_typ
     if (!d_in || !d_out || !dims || !psf_f || !psf_f_dims || !psf_b || !psf_b_dims)
         return pk_fail(PK_ERR_INVALID, "NULL argument");
     if (in_type != PK_U16 && in_type != PK_F32 && in_type != PK_F64) return pk_fail(PK_ERR_INVALID, "bad input dtype");
-    if (numit < 1) return pk_fail(PK_ERR_INVALID, "NUMIT must be >= 1");
+    if (numit < 0) return pk_fail(PK_ERR_INVALID, "NUMIT must be non-negative");
+    if (numit == 0)
+        return pk_fail(PK_ERR_UNSUPPORTED, "the no-allocation call needs NUMIT >= 1 (use pk_decon_lucy_omw_device for 0)");
     pk_decon_params def;
     if (!params) {
         pk_params_default(&def);
@@ -138,6 +141,11 @@ extern "C" pk_status pk_decon_lucy_omw_noalloc(const void* d_in, pk_dtype in_typ
     if (s != PK_OK) return s;
     if (params->decon_offset != 0.0 || params->edge_erosion > 0)
         return pk_fail(PK_ERR_UNSUPPORTED, "the no-allocation call does not support deconOffset or EdgeErosion");
+    // every axis of a volume that fits the array is below 2^20; checked before the int conversion,
+    // so a huge extent cannot wrap to a small one
+    for (int i = 0; i < 3; i++)
+        if (dims[i] > (int64_t)PK_NOALLOC_MAX_VOXELS)
+            return pk_fail(PK_ERR_UNSUPPORTED, "volume has more voxels than the no-allocation scratch holds (1048576)");
     const int ny = (int)dims[0], nx = (int)dims[1], nz = (int)dims[2];
     const long long N = (long long)ny * nx * nz;
     if (N > (long long)PK_NOALLOC_MAX_VOXELS)

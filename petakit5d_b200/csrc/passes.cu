@@ -21,6 +21,8 @@
 
 #include "fft_engine.cuh"
 #include "pass_kernels.cuh"
+#include "pass_tma.cuh"
+#include "pass_yreg.cuh"
 #include "pk_internal.h"
 #include "plans.h"
 
@@ -35,6 +37,11 @@ void pk_fill_kernels_f(pkpass::KernelTable& t);
 void pk_fill_kernels_g(pkpass::KernelTable& t);
 void pk_fill_kernels_h(pkpass::KernelTable& t);
 void pk_fill_kernels_i(pkpass::KernelTable& t);
+void pk_fill_tma_0(pkpass::TmaTable& t);
+void pk_fill_tma_1(pkpass::TmaTable& t);
+void pk_fill_tma_2(pkpass::TmaTable& t);
+void pk_fill_tma_3(pkpass::TmaTable& t);
+void pk_fill_yreg(pkpass::YregTable& t);
 
 static int sm_count() {
     static int n = 0;
@@ -72,6 +79,185 @@ const pkpass::KernelTable& kernels() {
     return t;
 }
 
+// The persistent TMA x / z kernels (pass_tma.cuh); PK_NO_TMA=1 keeps every x / z pass on the
+// register-IO kernels (diagnostics and A/B timing).
+const pkpass::TmaTable* tma_kernels() {
+    static pkpass::TmaTable t;
+    static bool on = false;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        memset(&t, 0, sizeof(t));
+        const char* e = getenv("PK_NO_TMA");
+        if (e && e[0] == '1') return;
+        pk_fill_tma_0(t);
+        pk_fill_tma_1(t);
+        pk_fill_tma_2(t);
+        pk_fill_tma_3(t);
+        on = true;
+    });
+    return on ? &t : nullptr;
+}
+
+// The register-packing y kernels (pass_yreg.cuh); PK_NO_YREG=1 keeps every y pass on the rolled
+// kernels (diagnostics and A/B timing).
+const pkpass::YregTable* yreg_kernels() {
+    static pkpass::YregTable t;
+    static bool on = false;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        memset(&t, 0, sizeof(t));
+        const char* e = getenv("PK_NO_YREG");
+        if (e && e[0] == '1') return;
+        pk_fill_yreg(t);
+        on = true;
+    });
+    return on ? &t : nullptr;
+}
+
+// A y step's descriptor the register-packing kernel can take: 512-voxel rows on the 4096-point
+// tiles, per-voxel inputs 16-byte aligned (bulk copies), the rolled kernel's fused-path conditions
+// (no padded / float64 raw input, no damping, scaling, mask or crop in the final pass).
+bool yreg_ok(const VolDesc& d, int mode) {
+    auto al = [](const void* p) { return p && (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
+    if (d.odd || d.ny != 512 || d.M != 256 || d.tiles_small || !d.tw_rc) return false;
+    switch (mode) {
+        case Y_PRE: return !d.padded && (d.raw_type == PK_U16 || d.raw_type == PK_F32) && al(d.raw);
+        case Y_R2C: return al(d.src);
+        case Y_RATIO: return al(d.I);
+        case Y_UPDATE: return al(d.Jo);
+        case Y_FINAL: return al(d.Jo) && !(d.damp > 1.f || d.scale_mode != 0 || d.need_xz);
+        case Y_RLPRE: return al(d.J2) && al(d.J3);
+        case Y_RLUPD: return al(d.Yb) && (d.rl_first || al(d.J4));
+        case Y_RLFINAL: return al(d.Yb) && !(d.damp > 1.f || d.scale_mode != 0 || d.need_xz);
+        case Y_C2R: return true;
+        default: return false;
+    }
+}
+
+// cuTensorMapEncodeTiled from the driver, found through the runtime (no link against libcuda)
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled() {
+    static EncodeTiledFn f = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            f = (EncodeTiledFn)p;
+        else
+            cudaGetLastError();
+    });
+    return f;
+}
+
+// Tensor map of a half spectrum (S or an OTF) laid out [z][x][k] with row pitch Pp, as
+// {2 Py floats, nx, nz}, with the column-tile box of an x (axis 1) or z (axis 2) pass of plan p.
+bool encode_spec_map(CUtensorMap* m, const void* base, const VolDesc& d, int axis, int p, int T) {
+    EncodeTiledFn enc = encode_tiled();
+    if (!enc || !base || (reinterpret_cast<uintptr_t>(base) & 15)) return false;
+    const int n = kPlans[p].n;
+    const int rows = pkpass::tma_box_rows(n);
+    const cuuint64_t dims[3] = {(cuuint64_t)2 * d.Py, (cuuint64_t)d.nx, (cuuint64_t)d.nz};
+    const cuuint64_t strides[2] = {(cuuint64_t)d.Pp * 8, (cuuint64_t)d.Pp * 8 * (cuuint64_t)d.nx};
+    const cuuint32_t box[3] = {(cuuint32_t)(2 * T), (cuuint32_t)(axis == 1 ? rows : 1), (cuuint32_t)(axis == 2 ? rows : 1)};
+    const cuuint32_t es[3] = {1, 1, 1};
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<void*>(base), dims, strides, box, es,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// Index of a step's TMA kernel in the table, or -1 when the step keeps the register-IO kernels.
+int tma_index(const PkStep& s) {
+    const pkpass::TmaTable* t = tma_kernels();
+    if (!t || s.plan <= 0 || s.plan >= kNumPlans || !pkpass::tma_plan(s.plan)) return -1;
+    int idx = -1;
+    if (s.kind == PK_STEP_X && s.mode == XZ_FWD) idx = pkpass::TMA_X_FWD;
+    else if (s.kind == PK_STEP_X && s.mode == XZ_INV) idx = pkpass::TMA_X_INV;
+    else if (s.kind == PK_STEP_Z && s.mode == XZ_CONV) idx = pkpass::TMA_Z_CONV;
+    if (idx < 0 || !t->k[s.plan][idx]) return -1;
+    return idx;
+}
+
+// Decides which x / z steps run on the TMA kernels (every descriptor's maps encode and its rows
+// are at least one tile wide) and encodes their maps into prog.maps.
+void assign_tma(PkProgram& prog) {
+    prog.maps.assign(prog.descs.size(), XZMaps());
+    const pkpass::YregTable* yt = yreg_kernels();
+    for (PkStep& s : prog.steps) {
+        s.tma = -1;
+        s.yreg = 0;
+        if (s.kind == PK_STEP_Y && yt && s.plan == pkpass::kYregPlan && s.grid > 0 && s.mode >= 0 &&
+            s.mode <= Y_C2R && yt->k[s.mode]) {
+            bool ok = true;
+            for (int i = 0; i < s.nvol && ok; i++) ok = yreg_ok(prog.descs[s.desc_off + i], s.mode);
+            if (ok) {
+                s.yreg = 1;
+                s.yreg_smem = yt->smem[s.mode];
+            }
+            continue;
+        }
+        const int idx = tma_index(s);
+        if (idx < 0 || s.grid == 0) continue;
+        const int axis = s.kind == PK_STEP_X ? 1 : 2;
+        const pkpass::TmaTable* t = tma_kernels();
+        const int T = t->cols[s.plan][idx];
+        bool ok = true;
+        for (int i = 0; i < s.nvol && ok; i++) {
+            const VolDesc& d = prog.descs[s.desc_off + i];
+            XZMaps& m = prog.maps[s.desc_off + i];
+            ok = d.Py >= T && encode_spec_map(&m.s, d.S, d, axis, s.plan, T);
+            if (ok && s.mode == XZ_CONV) ok = encode_spec_map(&m.otf, d.otf, d, axis, s.plan, T);
+        }
+        if (!ok) continue;
+        // the kernel's tiles are T columns wide: the step's tile prefix follows them
+        int* pf = prog.prefix.data() + s.prefix_off;
+        for (int i = 0; i < s.nvol; i++) {
+            const VolDesc& d = prog.descs[s.desc_off + i];
+            pf[i + 1] = pf[i] + (axis == 1 ? d.nz : d.nx) * ((d.Py + T - 1) / T);
+        }
+        s.grid = pf[s.nvol];
+        s.tma = idx;
+        s.tma_smem = t->smem[s.plan][idx];
+        s.tma_grid = std::min(s.grid, t->per_sm[s.plan][idx] * sm_count());
+    }
+}
+
+// Queues the copy of a page-locked host blob (a multiple of 16 bytes) to device memory on `st`.
+pk_status blob_upload(pk_ctx* ctx, void* d, const void* h, size_t bytes, cudaStream_t st) {
+    const long long n16 = (long long)((bytes + 15) / 16);
+    if (n16 == 0) return PK_OK;
+    const void* hd = nullptr;
+    if (cudaHostGetDevicePointer((void**)&hd, const_cast<void*>(h), 0) != cudaSuccess || !hd) {
+        cudaGetLastError();   // not mapped: fall back to a copy-engine copy
+        PK_CUDA(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, st));
+        return PK_OK;
+    }
+    const int grid = (int)std::min<long long>(64, std::max<long long>(1, n16 / 1024));
+    k_blob_copy<<<grid, 256, 0, st>>>((uint4*)d, (const uint4*)hd, n16);
+    PK_CUDA(cudaGetLastError());
+    if (ctx) ctx->launches++;
+    return PK_OK;
+}
+
+// Layout of an uploaded program: descriptors | block prefixes | (64-byte aligned) tensor maps.
+void blob_layout(const PkProgram& prog, size_t* dbytes, size_t* moff, size_t* total) {
+    *dbytes = sizeof(VolDesc) * prog.descs.size();
+    const size_t pend = *dbytes + sizeof(int) * prog.prefix.size();
+    *moff = (pend + 63) & ~(size_t)63;
+    *total = *moff + sizeof(XZMaps) * prog.maps.size();
+}
+
+void blob_fill(const PkProgram& prog, void* h) {
+    size_t dbytes, moff, total;
+    blob_layout(prog, &dbytes, &moff, &total);
+    memcpy(h, prog.descs.data(), dbytes);
+    memcpy((char*)h + dbytes, prog.prefix.data(), sizeof(int) * prog.prefix.size());
+    if (!prog.maps.empty()) memcpy((char*)h + moff, prog.maps.data(), sizeof(XZMaps) * prog.maps.size());
+}
+
 // lambda = clamp(sum((J2-Y).*J4) / (sum(J4.*J4) + eps), 0, 1)  (decon_lucy_function.m:126-127),
 // one CTA per volume, fixed summation order; the result goes to partials[0].
 __global__ void k_lambda(const VolDesc* __restrict__ descs, int nvol) {
@@ -101,6 +287,27 @@ __global__ void k_lambda(const VolDesc* __restrict__ descs, int nvol) {
 }
 
 }  // namespace
+
+// Descriptor blobs reach the device through this kernel, which reads the page-locked host copy
+// directly (zero-copy): a cudaMemcpyAsync would go through a copy engine, where it can queue behind
+// a large volume upload of another stream and hold back the compute stream for the whole upload.
+__global__ void k_blob_copy(uint4* __restrict__ dst, const uint4* __restrict__ src, long long n16) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n16; i += (long long)gridDim.x * blockDim.x)
+        dst[i] = src[i];
+}
+
+// One CTA waits on an mbarrier that nothing arrives on: the bounded wait runs out after limit_ns
+// and the failure goes to the context's status word (the self-test of the device waits).
+__global__ void k_wait_selftest(int* err, unsigned long long limit_ns) {
+    __shared__ uint64_t bar;
+    if (threadIdx.x == 0) {
+        pktma::mbar_init(&bar, 1);
+        pktma::fence_mbar_init();
+    }
+    __syncthreads();
+    const bool ok = pktma::mbar_wait(&bar, 0, limit_ns);
+    if (!__syncthreads_and(ok) && threadIdx.x == 0) pktma::report_wait_failure(err, 1);
+}
 
 // ------------------------------------------------------------------ host: plans and tables
 bool pk_make_axis_plan(int n, AxisPlan* p) {
@@ -312,9 +519,9 @@ void pk_program_add(PkProgram& prog, int kind, int mode, const std::vector<VolDe
 }
 
 pk_status pk_program_upload(pk_ctx* ctx, PkProgram& prog, cudaStream_t st) {
-    const size_t dbytes = sizeof(VolDesc) * prog.descs.size();
-    const size_t pbytes = sizeof(int) * prog.prefix.size();
-    const size_t need = dbytes + pbytes;
+    assign_tma(prog);
+    size_t dbytes, moff, need;
+    blob_layout(prog, &dbytes, &moff, &need);
     const int si = ctx->next_slot;
     ctx->next_slot = (ctx->next_slot + 1) % 4;
     pk_ctx::ProgSlot& sl = ctx->slots[si];
@@ -331,11 +538,14 @@ pk_status pk_program_upload(pk_ctx* ctx, PkProgram& prog, cudaStream_t st) {
         PK_CUDA(cudaMallocHost(&sl.h, cap));
         sl.cap = cap;
     }
-    memcpy(sl.h, prog.descs.data(), dbytes);
-    memcpy((char*)sl.h + dbytes, prog.prefix.data(), pbytes);
-    PK_CUDA(cudaMemcpyAsync(sl.d, sl.h, need, cudaMemcpyHostToDevice, st));
+    blob_fill(prog, sl.h);
+    {
+        const pk_status bs = blob_upload(ctx, sl.d, sl.h, need, st);
+        if (bs != PK_OK) return bs;
+    }
     prog.d_desc = (VolDesc*)sl.d;
     prog.d_prefix = (int*)((char*)sl.d + dbytes);
+    prog.d_maps = (XZMaps*)((char*)sl.d + moff);
     prog.slot = si;
     return PK_OK;
 }
@@ -401,7 +611,12 @@ static pk_status launch_steps(pk_ctx* ctx, const PkProgram& prog, cudaStream_t s
             rec.b = take();
             cudaEventRecord(rec.a, st);
         }
-        if (s.kind == PK_STEP_Y) {
+        if (s.tma >= 0) {
+            tma_kernels()->k[s.plan][s.tma]<<<s.tma_grid, PK_XZT_THREADS, s.tma_smem, st>>>(
+                dd, prog.d_maps + s.desc_off, dp, s.nvol, ctx ? ctx->d_err : nullptr);
+        } else if (s.yreg) {
+            yreg_kernels()->k[s.mode]<<<s.grid, kThreads, s.yreg_smem, st>>>(dd, dp, s.nvol, ctx ? ctx->d_err : nullptr);
+        } else if (s.kind == PK_STEP_Y) {
             kt.y[s.plan][s.mode]<<<s.grid, kThreads, s.smem, st>>>(dd, dp, s.nvol, s.mode);
         } else if (s.kind == PK_STEP_X || s.kind == PK_STEP_Z) {
             kt.xz[s.plan]<<<s.grid, kThreads, s.smem, st>>>(dd, dp, s.nvol, s.kind == PK_STEP_X ? 1 : 2, s.mode);
@@ -423,7 +638,8 @@ static pk_status launch_steps(pk_ctx* ctx, const PkProgram& prog, cudaStream_t s
 
 // The program's launches as a graph of kernel nodes in launch order, built node by node (no stream
 // capture, so other threads' CUDA calls cannot disturb it).
-static bool build_graph(const PkProgram& prog, const VolDesc* d_desc, const int* d_prefix, cudaGraphExec_t* out) {
+static bool build_graph(const PkProgram& prog, const VolDesc* d_desc, const int* d_prefix, const XZMaps* d_maps,
+                        int* d_err, cudaGraphExec_t* out) {
     const pkpass::KernelTable& kt = kernels();
     cudaGraph_t g = nullptr;
     if (cudaGraphCreate(&g, 0) != cudaSuccess) { cudaGetLastError(); return false; }
@@ -433,15 +649,29 @@ static bool build_graph(const PkProgram& prog, const VolDesc* d_desc, const int*
         if (s.grid == 0) continue;
         const VolDesc* dd = d_desc + s.desc_off;
         const int* dp = d_prefix + s.prefix_off;
+        const XZMaps* dm = d_maps + s.desc_off;
+        int* de = d_err;
         int nvol = s.nvol, mode = s.mode, axis = s.kind == PK_STEP_X ? 1 : 2;
         void* args5[] = {(void*)&dd, (void*)&dp, (void*)&nvol, (void*)&axis, (void*)&mode};
         void* args4[] = {(void*)&dd, (void*)&dp, (void*)&nvol, (void*)&mode};
         void* args2[] = {(void*)&dd, (void*)&nvol};
+        void* argst[] = {(void*)&dd, (void*)&dm, (void*)&dp, (void*)&nvol, (void*)&de};
+        void* argsy[] = {(void*)&dd, (void*)&dp, (void*)&nvol, (void*)&de};
         cudaKernelNodeParams p = {};
         p.blockDim = dim3(kThreads);
         p.gridDim = dim3(s.grid);
         p.sharedMemBytes = (unsigned)s.smem;
-        if (s.kind == PK_STEP_Y) {
+        if (s.tma >= 0) {
+            p.func = (void*)tma_kernels()->k[s.plan][s.tma];
+            p.gridDim = dim3(s.tma_grid);
+            p.blockDim = dim3(PK_XZT_THREADS);
+            p.sharedMemBytes = (unsigned)s.tma_smem;
+            p.kernelParams = argst;
+        } else if (s.yreg) {
+            p.func = (void*)yreg_kernels()->k[s.mode];
+            p.sharedMemBytes = (unsigned)s.yreg_smem;
+            p.kernelParams = argsy;
+        } else if (s.kind == PK_STEP_Y) {
             p.func = (void*)kt.y[s.plan][s.mode];
             p.kernelParams = args4;
         } else if (s.kind == PK_STEP_X || s.kind == PK_STEP_Z) {
@@ -488,7 +718,20 @@ static bool graphs_enabled() {
 // Launches a program's kernels.  A program seen before with the same launch shapes and descriptor
 // layout replays a CUDA graph of its launches, whose descriptor buffer is refreshed on the stream
 // before each replay; per-kernel profiling and a stream the caller is capturing take the direct path.
+pk_status pk_check_device_waits(pk_ctx* ctx) {
+    if (ctx && ctx->h_err && *(volatile int*)ctx->h_err != 0) {
+        *(volatile int*)ctx->h_err = 0;
+        return pk_fail(PK_ERR_TIMEOUT, "a bounded wait on the device ran out in an earlier call of this context "
+                                       "(its results are not valid)");
+    }
+    return PK_OK;
+}
+
 pk_status pk_program_launch(pk_ctx* ctx, PkProgram& prog, cudaStream_t st) {
+    {
+        const pk_status w = pk_check_device_waits(ctx);
+        if (w != PK_OK) return w;
+    }
     const int nk = pk_program_kernel_count(prog);
     bool direct = !ctx || ctx->prof_on || prog.slot < 0 || prog.no_graph || !graphs_enabled() || nk < 2;
     if (!direct) {
@@ -509,8 +752,9 @@ pk_status pk_program_launch(pk_ctx* ctx, PkProgram& prog, cudaStream_t st) {
         key.push_back((long long)prog.descs.size());
         key.push_back((long long)prog.prefix.size());
         for (const PkStep& s : prog.steps) {
-            const long long v[] = {s.kind, s.mode, s.plan, s.nvol, s.grid, (long long)s.smem, s.desc_off, s.prefix_off};
-            key.insert(key.end(), v, v + 8);
+            const long long v[] = {s.kind, s.mode, s.plan, s.nvol, s.grid, (long long)s.smem, s.desc_off, s.prefix_off,
+                                   s.tma, s.tma_grid, s.yreg};
+            key.insert(key.end(), v, v + 11);
         }
         auto it = ctx->graphs.find(key);
         if (it == ctx->graphs.end() && ctx->graph_seen.size() >= 4096) ctx->graph_seen.clear();  // bounded
@@ -520,12 +764,14 @@ pk_status pk_program_launch(pk_ctx* ctx, PkProgram& prog, cudaStream_t st) {
         } else {
             if (it == ctx->graphs.end()) {
                 if (ctx->graphs.size() >= 64) pk_release_graphs(ctx);   // bounded cache: start over
-                const size_t dbytes = sizeof(VolDesc) * prog.descs.size();
+                size_t dbytes, moff, total;
+                blob_layout(prog, &dbytes, &moff, &total);
                 pk_ctx::GraphEntry e;
-                e.bytes = dbytes + sizeof(int) * prog.prefix.size();
+                e.bytes = total;
                 bool ok = cudaMalloc(&e.d, e.bytes) == cudaSuccess && cudaMallocHost(&e.h, e.bytes) == cudaSuccess &&
                           cudaEventCreateWithFlags(&e.ev, cudaEventDisableTiming) == cudaSuccess;
-                ok = ok && build_graph(prog, (const VolDesc*)e.d, (const int*)((char*)e.d + dbytes), &e.exec);
+                ok = ok && build_graph(prog, (const VolDesc*)e.d, (const int*)((char*)e.d + dbytes),
+                                       (const XZMaps*)((char*)e.d + moff), ctx->d_err, &e.exec);
                 if (!ok) {
                     cudaGetLastError();
                     if (e.d) cudaFree(e.d);
@@ -540,10 +786,11 @@ pk_status pk_program_launch(pk_ctx* ctx, PkProgram& prog, cudaStream_t st) {
             if (it != ctx->graphs.end()) {
                 pk_ctx::GraphEntry& e = it->second;
                 if (e.used) PK_CUDA(cudaEventSynchronize(e.ev));   // the previous refresh has been read
-                const size_t dbytes = sizeof(VolDesc) * prog.descs.size();
-                memcpy(e.h, prog.descs.data(), dbytes);
-                memcpy((char*)e.h + dbytes, prog.prefix.data(), sizeof(int) * prog.prefix.size());
-                PK_CUDA(cudaMemcpyAsync(e.d, e.h, e.bytes, cudaMemcpyHostToDevice, st));
+                blob_fill(prog, e.h);
+                {
+                    const pk_status bs = blob_upload(ctx, e.d, e.h, e.bytes, st);
+                    if (bs != PK_OK) return bs;
+                }
                 PK_CUDA(cudaGraphLaunch(e.exec, st));
                 PK_CUDA(cudaEventRecord(e.ev, st));
                 e.used = true;
@@ -564,7 +811,9 @@ pk_status pk_program_launch(pk_ctx* ctx, PkProgram& prog, cudaStream_t st) {
 // streams between ranges); the last range of a program passes last = true, which marks its
 // descriptor slot busy until the work queued so far has run.
 pk_status pk_program_launch_range(pk_ctx* ctx, PkProgram& prog, cudaStream_t st, size_t b, size_t e, bool last) {
-    pk_status rs = launch_steps(ctx, prog, st, b, e);
+    pk_status rs = pk_check_device_waits(ctx);
+    if (rs != PK_OK) return rs;
+    rs = launch_steps(ctx, prog, st, b, e);
     if (rs != PK_OK) return rs;
     for (size_t i = b; i < std::min(e, prog.steps.size()); i++) ctx->launches += prog.steps[i].grid > 0 ? 1 : 0;
     if (last && prog.slot >= 0) {
@@ -594,3 +843,18 @@ int pk_program_kernel_count(const PkProgram& prog) {
     return n;
 }
 
+
+extern "C" pk_status pk_selftest_device_wait(pk_ctx* ctx, int64_t limit_ns) {
+    if (!ctx) return pk_fail(PK_ERR_INVALID, "NULL context");
+    if (limit_ns < 1000 || limit_ns > 1000000000) return pk_fail(PK_ERR_INVALID, "limit_ns must be in [1e3, 1e9]");
+    std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+    int prev = 0;
+    cudaGetDevice(&prev);
+    PK_CUDA(cudaSetDevice(ctx->device));
+    k_wait_selftest<<<1, 32, 0, ctx->stream>>>(ctx->d_err, (unsigned long long)limit_ns);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    cudaSetDevice(prev);
+    if (e != cudaSuccess) return pk_fail(PK_ERR_CUDA, std::string("wait self-test: ") + cudaGetErrorString(e));
+    return pk_check_device_waits(ctx);
+}

@@ -8,6 +8,7 @@
 // complex passes over x and z on tiles of T adjacent k-columns.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -93,6 +94,14 @@ struct VolDesc {
     int tiles_small;                 // passes use the 1024-point-tile kernels (small volumes)
 };
 
+// TMA tensor maps of one descriptor of an x or z step run by the persistent TMA kernel: the
+// spectrum S as a 3-D tensor {2 Py floats, nx, nz} (row pitch Pp) with the step's column-tile box,
+// and the OTF (same layout) for XZ_CONV.  Encoded on the host when the program is uploaded.
+struct alignas(64) XZMaps {
+    CUtensorMap s;
+    CUtensorMap otf;
+};
+
 // ------------------------------------------------------------------ host side
 struct AxisPlan {
     int n = 0, nst = 0;
@@ -164,6 +173,10 @@ struct pk_ctx {
     std::map<std::string, void*> dev_tables;
     long long next_ticket = 1;
     std::map<long long, cudaEvent_t> tickets;                  // ticket -> its download's event
+    // device-wait status: page-locked word the kernels write when a bounded wait on the device ran
+    // out (0 = none); h_err is the host view, d_err the device pointer passed to the kernels
+    int* h_err = nullptr;
+    int* d_err = nullptr;
 };
 
 // error helpers (capi.cpp)
@@ -189,12 +202,21 @@ enum { PK_STEP_Y = 0, PK_STEP_X = 1, PK_STEP_Z = 2, PK_STEP_LAMBDA = 3 };
 struct PkStep {
     int kind = 0, mode = 0, plan = 0, nvol = 0, desc_off = 0, prefix_off = 0, grid = 0;
     size_t smem = 0;
+    // set at upload: index of the persistent TMA kernel that runs this x / z step (-1: none), its
+    // grid (resident CTAs, each walking tiles) and dynamic shared memory
+    int tma = -1, tma_grid = 0;
+    size_t tma_smem = 0;
+    // set at upload: this y step runs the register-packing kernel (512-voxel rows), with its smem
+    int yreg = 0;
+    size_t yreg_smem = 0;
 };
 struct PkProgram {
     std::vector<VolDesc> descs;
     std::vector<int> prefix;
     std::vector<PkStep> steps;
+    std::vector<XZMaps> maps;   // parallel to descs: tensor maps of the steps run by the TMA kernels
     VolDesc* d_desc = nullptr; int* d_prefix = nullptr;   // inside one of the context's program slots
+    XZMaps* d_maps = nullptr;
     int slot = -1;
     bool no_graph = false;   // launch directly (e.g. per-slab programs of a streamed call)
 };
@@ -202,6 +224,9 @@ void pk_program_add(PkProgram& prog, int kind, int mode, const std::vector<VolDe
 pk_status pk_program_upload(pk_ctx* ctx, PkProgram& prog, cudaStream_t st);
 pk_status pk_program_launch(pk_ctx* ctx, PkProgram& prog, cudaStream_t st);
 void pk_release_graphs(pk_ctx* ctx);
+// PK_ERR_TIMEOUT (and the status cleared) when a kernel of this context reported that one of its
+// bounded device waits ran out since the last check; PK_OK otherwise
+pk_status pk_check_device_waits(pk_ctx* ctx);
 pk_status pk_program_launch_range(pk_ctx* ctx, PkProgram& prog, cudaStream_t st, size_t b, size_t e, bool last);
 double pk_step_bytes(const PkStep& s, const VolDesc* descs);
 const char* pk_step_name(const PkStep& s);
