@@ -350,6 +350,7 @@ def run_ours(args, rank, world, device):
                    "share": round(v["ms"] / sum(x["ms"] for x in prof.values()), 4)} for k, v in prof.items()}
     return {
         "ms": ms, "N": N, "launches": launches, "clocks": clk, "roofline": roof, "kernels": kernels,
+        "autotune": ctx.tune_read(),
         "e2e_ms": e2e_ms, "e2e_sync_ms": e2e_sync_ms, "same": same, "cufft_ms": cufft_ms, "call_bytes": call_bytes, "vol": vol, "psf": psf,
         "psf_b": psf_b, "peak": peak, "peak_kind": peak_kind, "copy_ms": copy_ms, "J32": J32, "J16": J16,
     }
@@ -376,6 +377,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="leave the batched (96 chunks) and served (Poisson requests) sub-objects off the line")
     ap.add_argument("--workload", default="omw_llsm",
                     choices=["omw_llsm", "rl_small", "batched", "served", "large", "dsr"])
     ap.add_argument("--rate", type=float, default=200.0, help="served: Poisson arrival rate (requests/s)")
@@ -395,7 +398,9 @@ def main():
         return
 
     if args.workload != "omw_llsm":
-        WORKLOADS[args.workload](args)
+        out = WORKLOADS[args.workload](args)
+        if out is not None:
+            _emit(out)
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -459,6 +464,7 @@ def main():
                           "peak": r["peak"], "frac": round(r["call_bytes"] / (r["ms"] * 1e-3) / 1e9 / r["peak"], 4),
                           "unit": "GB/s", "note": "N*(64*iters+12) bytes per call"},
         "kernels": r["kernels"],
+        "autotune": r["autotune"],
         "cufft_comparator": {"value": round(N / (r["cufft_ms"] * 1e-3) / 1e6, 1), "unit": "Mvoxel/s",
                              "ms_per_step": round(r["cufft_ms"], 3)},
         "clocks": r["clocks"],
@@ -483,6 +489,18 @@ def main():
                       "checked": "a float32-output device call on rank 0's volume after the timed loops, and the "
                                  "timed calls' uint16 output, against the oracle restatement of "
                                  "decon_lucy_omw_function.m:105-113 with the same backprojector"}
+    if world == 1 and not args.no_extras:
+        # the batched and served patterns of the same library, on their own workloads (compact)
+        for name, fn, keys in (("batched", wl_batched, ("value", "unit", "plain_per_chunk", "speedup_vs_plain",
+                                                         "batched_equals_plain", "ms_batched", "ms_plain",
+                                                         "device_resident", "workload")),
+                               ("served", wl_served, ("value", "unit", "latency_ms", "plain_sequential",
+                                                      "speedup_vs_plain", "wall_s", "workload"))):
+            try:
+                sub = fn(args)
+                line[name] = {k: sub[k] for k in keys if k in sub}
+            except Exception as e:   # reported, not fatal: the headline line still prints
+                line[name] = {"error": repr(e)[:300]}
     line["e2e"]["copy_floor"] = {
         "ms_per_step": round(r["copy_ms"], 4), "value": round(N * world / (r["copy_ms"] * 1e-3) / 1e6, 1),
         "GBps_each_way": round(2 * N / (r["copy_ms"] * 1e-3) / 1e9, 1),
@@ -678,7 +696,7 @@ def wl_batched(args):
     ref_out = [o.copy() for o in outs]
     batched()
     same = all(np.array_equal(a, b) for a, b in zip(ref_out, outs))
-    _emit({"metric": "batched OMW Mvoxel/s (output core voxels, host buffers, copies included)",
+    return ({"metric": "batched OMW Mvoxel/s (output core voxels, host buffers, copies included)",
            "workload": "96 uneven chunks (core x,y in {192..384}, z in {96..256}, +16 borders), 3 PSFs, OMW x2",
            "value": round(core / (res["batched"] * 1e-3) / 1e6, 1), "unit": "Mvoxel/s",
            "plain_per_chunk": round(core / (res["plain"] * 1e-3) / 1e6, 1),
@@ -796,7 +814,7 @@ def wl_served(args):
                                               pf.ctypes.data, _lib.i64x3(pf.shape), it, p, o.ctypes.data, None))
     plain = time.perf_counter() - t1
     L = np.array(lat)
-    _emit({"metric": "served Mvoxel/s and request latency", "workload":
+    return ({"metric": "served Mvoxel/s and request latency", "workload":
            f"{len(reqs)} open-loop Poisson requests at {args.rate} req/s (90% chunk sizes, 10% 768x768x384; 80% OMW x2, "
            "20% RL x10; 3 PSFs; 150 GB budget)",
            "value": round(nvox / wall / 1e6, 1), "unit": "Mvoxel/s",

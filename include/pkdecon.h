@@ -79,6 +79,14 @@ PK_API int64_t pk_ctx_kernel_launches(pk_ctx* ctx);
 PK_API pk_status pk_ctx_profile(pk_ctx* ctx, int32_t enable);
 PK_API int32_t pk_ctx_profile_read(pk_ctx* ctx, char* buf, int32_t cap);
 
+/* Autotuner record (no counterpart in the reference).  The first time an x / z pass of a given
+ * transform plan and volume geometry runs on a context, each kernel variant that can run it (the
+ * register-IO kernel and the TMA kernels' tile widths / buffer counts) is timed three times on
+ * scratch buffers of that geometry and the fastest is kept; choices persist in an on-disk cache
+ * (PK_TUNE_FILE, else ~/.cache/pkdecon/tune-v1.txt; PK_TUNE=0 disables the timing).  This writes
+ * the context's decisions as a JSON list and returns its length (truncated to cap-1). */
+PK_API int32_t pk_ctx_tune_read(pk_ctx* ctx, char* buf, int32_t cap);
+
 /* Failure-detection self-test (no counterpart in the reference).  Every wait inside the pass
  * kernels is bounded: a wait that runs out records it in the context's device-wait status word
  * and the kernel returns, and the next call on the context (or the synchronous call itself)

@@ -63,6 +63,7 @@ _SIGS = {
     "pk_ctx_profile": (C.c_int, [P, C.c_int32]),
     "pk_ctx_profile_read": (C.c_int32, [P, C.c_char_p, C.c_int32]),
     "pk_selftest_device_wait": (C.c_int, [P, C.c_int64]),
+    "pk_ctx_tune_read": (C.c_int32, [P, C.c_char_p, C.c_int32]),
     "pk_output_dims": (C.c_int, [I64x3, C.POINTER(DeconParams), I64x3]),
     "pk_decon_lucy": (C.c_int, [P, P, C.c_int, I64x3, P, I64x3, C.c_int32, C.POINTER(DeconParams), P,
                                 C.POINTER(C.c_int32)]),
@@ -196,6 +197,16 @@ class Context:
         n = lib.pk_ctx_profile_read(self.handle, buf, cap)
         if n >= cap:
             raise PkError(PK_ERR_INVALID, "profile record larger than the read buffer")
+        return json.loads(buf.value.decode())
+
+    def tune_read(self):
+        """The autotuner's decisions on this context (a list of dicts)."""
+        import json
+        cap = 1 << 20
+        buf = C.create_string_buffer(cap)
+        n = lib.pk_ctx_tune_read(self.handle, buf, cap)
+        if n >= cap:
+            raise PkError(PK_ERR_INVALID, "tune record larger than the read buffer")
         return json.loads(buf.value.decode())
 
     def reset(self):

@@ -45,10 +45,11 @@ struct XztLayout {
     static constexpr size_t bytes(bool conv) { return 1024 + NBUF * BUF + (conv ? BUF : 0) + TW + 64; }
 };
 
-// CTAs per SM a variant is compiled for (register budget): 3 for one 4096-point tile in flight per
-// buffer, 2 for the convolution (three buffers) or 8192-point tiles, 1 for two 8192-point buffers
+// CTAs per SM a variant is compiled for (register budget): 3 for 4096-point tiles, 2 for the
+// two-buffer convolution (three tile-sized buffers) or one 8192-point buffer, 1 for two 8192-point buffers
 constexpr int xzt_min_blocks(int P, int TC, int NBUF, bool conv) {
-    return (TC > 0 ? TC : plan_cols_xz(kPlans[P].n)) * kPlans[P].n > 4096 ? (NBUF == 2 ? 1 : 2) : (conv ? 2 : 3);
+    return (TC > 0 ? TC : plan_cols_xz(kPlans[P].n)) * kPlans[P].n > 4096 ? (NBUF == 2 ? 1 : 2)
+                                                                           : ((conv && NBUF == 2) ? 2 : 3);
 }
 
 // The TMA kernels run PK_THREADS compute threads (warps 0-7) and one producer warp (warp 8) that
@@ -374,51 +375,55 @@ __global__ void __launch_bounds__(PK_XZT_THREADS, xzt_min_blocks(P, TC, NBUF, MO
     }
 }
 
-// The TMA kernels by plan: [p][0] x forward, [p][1] x inverse, [p][2] z convolution; with each
-// one's dynamic shared memory and resident CTAs per SM (the persistent grid is that times the SMs).
+// The TMA kernels by plan, pass and variant: [p][0] x forward, [p][1] x inverse, [p][2] z convolution;
+// variant 0 is the plan's 4096-point tile with two buffers, variants 1 and 2 (where built) are the
+// alternatives the autotuner times against it.  With each one's dynamic shared memory, resident CTAs
+// per SM (the persistent grid is that times the SMs) and tile width.
 enum { TMA_X_FWD = 0, TMA_X_INV = 1, TMA_Z_CONV = 2 };
+constexpr int kTmaVariants = 3;
 struct TmaTable {
-    void (*k[kNumPlans][3])(const VolDesc*, const XZMaps*, const int*, int, int*);
-    size_t smem[kNumPlans][3];
-    int per_sm[kNumPlans][3];
-    int cols[kNumPlans][3];   // columns per tile (the tile prefix and the TMA box follow it)
+    void (*k[kNumPlans][3][kTmaVariants])(const VolDesc*, const XZMaps*, const int*, int, int*);
+    size_t smem[kNumPlans][3][kTmaVariants];
+    int per_sm[kNumPlans][3][kTmaVariants];
+    int cols[kNumPlans][3][kTmaVariants];    // columns per tile (the tile prefix and the TMA box follow it)
+    int nbuf[kNumPlans][3][kTmaVariants];
 };
 
-template <int P, int IDX, int AXIS, int MODE, int TC = 0, int NBUF = 2>
+template <int P, int IDX, int VAR, int AXIS, int MODE, int TC = 0, int NBUF = 2>
 inline void register_tma_one(TmaTable& t) {
     auto fn = k_xzt<P, AXIS, MODE, TC, NBUF>;
     const size_t smem = XztLayout<P, TC, NBUF>::bytes(MODE == XZ_CONV);
-    t.k[P][IDX] = fn;
-    t.smem[P][IDX] = smem;
-    t.cols[P][IDX] = XztLayout<P, TC, NBUF>::T;
+    t.k[P][IDX][VAR] = fn;
+    t.smem[P][IDX][VAR] = smem;
+    t.cols[P][IDX][VAR] = XztLayout<P, TC, NBUF>::T;
+    t.nbuf[P][IDX][VAR] = NBUF;
     int n = 0;
     if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, PK_XZT_THREADS, smem) != cudaSuccess || n < 1) {
         cudaGetLastError();
-        t.k[P][IDX] = nullptr;   // this plan falls back to the register-IO kernels
+        t.k[P][IDX][VAR] = nullptr;   // this variant is not offered
         n = 0;
     }
-    t.per_sm[P][IDX] = n;
+    t.per_sm[P][IDX][VAR] = n;
 }
 
 template <int P, int HI>
 struct RegisterTma {
     static void fill(TmaTable& t) {
         if constexpr (tma_plan(P)) {
-            register_tma_one<P, TMA_X_FWD, 1, XZ_FWD>(t);
-            register_tma_one<P, TMA_X_INV, 1, XZ_INV>(t);
-            register_tma_one<P, TMA_Z_CONV, 2, XZ_CONV>(t);
+            register_tma_one<P, TMA_X_FWD, 0, 1, XZ_FWD>(t);
+            register_tma_one<P, TMA_X_INV, 0, 1, XZ_INV>(t);
+            register_tma_one<P, TMA_Z_CONV, 0, 2, XZ_CONV>(t);
             if constexpr (kPlans[P].n == 512) {
-                // 64-byte rows (8 columns) against 128-byte rows (16 columns) for the x pass of 512-long
-                // lines: PK_XWIDE=1 -> 16 columns, one buffer; 2 -> 16 columns, two buffers
-                const char* e = getenv("PK_XWIDE");
-                if (e && e[0] == '1') {
-                    register_tma_one<P, TMA_X_FWD, 1, XZ_FWD, 16, 1>(t);
-                    register_tma_one<P, TMA_X_INV, 1, XZ_INV, 16, 1>(t);
-                } else if (e && e[0] == '2') {
-                    register_tma_one<P, TMA_X_FWD, 1, XZ_FWD, 16, 2>(t);
-                    register_tma_one<P, TMA_X_INV, 1, XZ_INV, 16, 2>(t);
-                }
+                // 8-column tiles (64-byte rows) against 16-column tiles (128-byte rows) with one or two buffers
+                register_tma_one<P, TMA_X_FWD, 1, 1, XZ_FWD, 16, 1>(t);
+                register_tma_one<P, TMA_X_INV, 1, 1, XZ_INV, 16, 1>(t);
+                register_tma_one<P, TMA_X_FWD, 2, 1, XZ_FWD, 16, 2>(t);
+                register_tma_one<P, TMA_X_INV, 2, 1, XZ_INV, 16, 2>(t);
+            }
+            if constexpr (kPlans[P].n == 256) {
+                // the convolution with one tile buffer (three CTAs per SM instead of two)
+                register_tma_one<P, TMA_Z_CONV, 1, 2, XZ_CONV, 0, 1>(t);
             }
         }
         RegisterTma<P + 1, HI>::fill(t);

@@ -15,7 +15,10 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <filesystem>
+#include <fstream>
 #include <mutex>
+#include <sstream>
 #include <string>
 #include <vector>
 
@@ -68,6 +71,26 @@ void pk_fill_all_kernels(pkpass::KernelTable& t) {
     pk_fill_kernels_g(t);
     pk_fill_kernels_h(t);
     pk_fill_kernels_i(t);
+}
+
+static size_t step_smem(int kind, int mode, const VolDesc& v) {
+    if (kind == PK_STEP_Y)
+        return sizeof(float2) * (tw_slots(v.M) + (v.odd ? 0 : v.M + 1) + padded_size(v.Ly * v.M) + v.Ly +
+                                 (size_t)pkpass::y_aux_arrays(mode) * v.Ly * v.M);
+    const bool conv = mode == XZ_CONV;
+    if (kind == PK_STEP_X)
+        return sizeof(float2) * (tw_slots(v.ax.n) + padded_size2(v.Tx * v.ax.n) + (conv ? v.Tx * v.ax.n : 0));
+    if (kind == PK_STEP_Z)
+        return sizeof(float2) * (tw_slots(v.az.n) + padded_size2(v.Tz * v.az.n) + (conv ? v.Tz * v.az.n : 0));
+    return 0;
+}
+
+// Descriptor blobs reach the device through this kernel, which reads the page-locked host copy
+// directly (zero-copy): a cudaMemcpyAsync would go through a copy engine, where it can queue behind
+// a large volume upload of another stream and hold back the compute stream for the whole upload.
+__global__ void k_blob_copy(uint4* __restrict__ dst, const uint4* __restrict__ src, long long n16) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n16; i += (long long)gridDim.x * blockDim.x)
+        dst[i] = src[i];
 }
 
 namespace {
@@ -177,13 +200,226 @@ int tma_index(const PkStep& s) {
     if (s.kind == PK_STEP_X && s.mode == XZ_FWD) idx = pkpass::TMA_X_FWD;
     else if (s.kind == PK_STEP_X && s.mode == XZ_INV) idx = pkpass::TMA_X_INV;
     else if (s.kind == PK_STEP_Z && s.mode == XZ_CONV) idx = pkpass::TMA_Z_CONV;
-    if (idx < 0 || !t->k[s.plan][idx]) return -1;
+    if (idx < 0 || !t->k[s.plan][idx][0]) return -1;
     return idx;
+}
+
+// ------------------------------------------------------------------ autotuner of the x / z passes
+// An x / z step can run on the register-IO kernel (k_xz, variant -1) or on a TMA variant (k_xzt:
+// 0 = the plan's 4096-point tile with two buffers; 1, 2 = the alternatives built for the plan).
+// The first time a (pass, plan, volume geometry) is seen, every candidate runs three times on
+// scratch buffers of that geometry (zeroed spectrum and OTF; no live data is touched) and the
+// fastest is kept for the context and appended to an on-disk cache (PK_TUNE_FILE, else
+// ~/.cache/pkdecon/tune-v1.txt), keyed by the device name, so later processes skip the timing.
+// PK_TUNE=0 turns the timing off (variant 0 everywhere).
+
+std::mutex g_tf_mu;
+std::map<std::string, int> g_tf;   // "<device>|<key>" -> variant
+bool g_tf_loaded = false;
+
+std::string tune_path() {
+    const char* e = getenv("PK_TUNE_FILE");
+    if (e && *e) return e;
+    const char* h = getenv("HOME");
+    if (!h || !*h) return "";
+    return std::string(h) + "/.cache/pkdecon/tune-v1.txt";
+}
+
+std::string device_tag(int dev) {
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) {
+        cudaGetLastError();
+        return "unknown";
+    }
+    std::string n = prop.name;
+    for (char& c : n)
+        if (c == ' ' || c == '|') c = '_';
+    return n + "_sm" + std::to_string(prop.multiProcessorCount);
+}
+
+void tf_load() {
+    if (g_tf_loaded) return;
+    g_tf_loaded = true;
+    const std::string path = tune_path();
+    if (path.empty()) return;
+    std::ifstream f(path);
+    std::string line;
+    while (std::getline(f, line)) {
+        std::istringstream ls(line);
+        std::string key;
+        int v = 0;
+        if (ls >> key >> v) g_tf[key] = v;
+    }
+}
+
+void tf_store(const std::string& key, int v, float ms) {
+    const std::string path = tune_path();
+    if (path.empty()) return;
+    std::error_code ec;
+    std::filesystem::create_directories(std::filesystem::path(path).parent_path(), ec);
+    std::ofstream f(path, std::ios::app);
+    if (f) f << key << " " << v << " " << ms << "\n";
+}
+
+const char* variant_name(int idx, int v) {
+    static const char* names[] = {"register-IO", "tma", "tma-16col-1buf", "tma-16col-2buf", "tma-1buf"};
+    if (v < 0) return names[0];
+    if (v == 0) return names[1];
+    if (idx == pkpass::TMA_Z_CONV) return names[4];
+    return v == 1 ? names[2] : names[3];
+}
+
+// Times each candidate of step `s` (first descriptor's geometry) on scratch buffers; returns the
+// fastest, or -2 when nothing could be timed.  ms[i] receives candidate i's time.
+int time_candidates(pk_ctx* ctx, const PkStep& s, const VolDesc& d0, int idx, const std::vector<int>& cands,
+                    cudaStream_t st, std::vector<float>& ms) {
+    const pkpass::TmaTable* t = tma_kernels();
+    const pkpass::KernelTable& kt = kernels();
+    const int axis = s.kind == PK_STEP_X ? 1 : 2;
+    const bool conv = s.mode == XZ_CONV;
+    const size_t Sb = (size_t)8 * d0.Pp * d0.nx * d0.nz;
+    if (Sb > ((size_t)3 << 29)) return -2;   // above 1.5 GB of scratch: keep the default
+    const size_t moff = (sizeof(VolDesc) + 63) & ~(size_t)63;
+    const size_t poff = moff + sizeof(XZMaps);
+    const size_t blob = poff + 64;
+    char* d = nullptr;
+    if (cudaMalloc(&d, blob + (conv ? 2 : 1) * Sb + 256) != cudaSuccess) {
+        cudaGetLastError();
+        return -2;
+    }
+    float2* S = (float2*)(d + ((blob + 255) & ~(size_t)255));
+    float2* O = conv ? S + Sb / 8 : nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    int best = -2;
+    float best_ms = 1e30f;
+    bool ok = cudaMemsetAsync(S, 0, (conv ? 2 : 1) * Sb, st) == cudaSuccess &&
+              cudaEventCreate(&e0) == cudaSuccess && cudaEventCreate(&e1) == cudaSuccess;
+    VolDesc dt = d0;
+    dt.S = S;
+    dt.otf = O;
+    std::vector<unsigned char> h(blob, 0);
+    memcpy(h.data(), &dt, sizeof(VolDesc));
+    ms.assign(cands.size(), -1.f);
+    for (size_t ci = 0; ok && ci < cands.size(); ci++) {
+        const int v = cands[ci];
+        int tiles, grid;
+        size_t smem;
+        XZMaps m;
+        memset(&m, 0, sizeof(m));
+        if (v < 0) {
+            tiles = axis == 1 ? d0.blocksX : d0.blocksZ;
+            grid = tiles;
+            smem = step_smem(s.kind, s.mode, dt);
+        } else {
+            const int T = t->cols[s.plan][idx][v];
+            if (d0.Py < T || !encode_spec_map(&m.s, S, dt, axis, s.plan, T) ||
+                (conv && !encode_spec_map(&m.otf, O, dt, axis, s.plan, T)))
+                continue;
+            tiles = (axis == 1 ? d0.nz : d0.nx) * ((d0.Py + T - 1) / T);
+            grid = std::min(tiles, t->per_sm[s.plan][idx][v] * sm_count());
+            smem = t->smem[s.plan][idx][v];
+        }
+        const int pf[2] = {0, tiles};
+        memcpy(h.data() + moff, &m, sizeof(m));
+        memcpy(h.data() + poff, pf, sizeof(pf));
+        ok = cudaMemcpyAsync(d, h.data(), blob, cudaMemcpyHostToDevice, st) == cudaSuccess &&
+             cudaStreamSynchronize(st) == cudaSuccess;
+        const VolDesc* dd = (const VolDesc*)d;
+        const XZMaps* dm = (const XZMaps*)(d + moff);
+        const int* dp = (const int*)(d + poff);
+        auto launch = [&]() {
+            if (v < 0) kt.xz[s.plan]<<<grid, PK_THREADS, smem, st>>>(dd, dp, 1, axis, s.mode);
+            else t->k[s.plan][idx][v]<<<grid, PK_XZT_THREADS, smem, st>>>(dd, dm, dp, 1, ctx->d_err);
+        };
+        for (int r = 0; ok && r < 1; r++) launch();
+        ok = ok && cudaEventRecord(e0, st) == cudaSuccess;
+        for (int r = 0; ok && r < 3; r++) launch();
+        ok = ok && cudaEventRecord(e1, st) == cudaSuccess && cudaEventSynchronize(e1) == cudaSuccess;
+        float el = 0.f;
+        ok = ok && cudaEventElapsedTime(&el, e0, e1) == cudaSuccess;
+        if (!ok) break;
+        ms[ci] = el / 3.f;
+        if (ms[ci] < best_ms) {
+            best_ms = ms[ci];
+            best = v;
+        }
+    }
+    if (!ok) {
+        cudaGetLastError();
+        best = -2;
+    }
+    cudaStreamSynchronize(st);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaFree(d);
+    cudaGetLastError();
+    return best;
+}
+
+// The variant an x / z step runs: the context's earlier choice, the on-disk cache's, or a timing.
+int choose_variant(pk_ctx* ctx, const PkProgram& prog, const PkStep& s, int idx, cudaStream_t st) {
+    const pkpass::TmaTable* t = tma_kernels();
+    std::vector<int> cands;
+    if (kernels().xz[s.plan]) cands.push_back(-1);
+    for (int v = 0; v < pkpass::kTmaVariants; v++)
+        if (t->k[s.plan][idx][v]) cands.push_back(v);
+    const VolDesc& d0 = prog.descs[s.desc_off];
+    if (!ctx || cands.size() < 2) return 0;
+    const std::vector<long long> key = {s.kind, s.mode, s.plan, d0.ny, d0.nx, d0.nz, s.nvol};
+    auto it = ctx->tune.find(key);
+    if (it != ctx->tune.end()) return it->second;
+    const char* off = getenv("PK_TUNE");
+    if (off && off[0] == '0') return 0;
+    std::string fkey = device_tag(ctx->device) + "|";
+    for (size_t i = 0; i < key.size(); i++) fkey += (i ? "," : "") + std::to_string(key[i]);
+    {
+        std::lock_guard<std::mutex> lk(g_tf_mu);
+        tf_load();
+        auto f = g_tf.find(fkey);
+        if (f != g_tf.end() && std::find(cands.begin(), cands.end(), f->second) != cands.end()) {
+            ctx->tune[key] = f->second;
+            ctx->tune_log.push_back("{\"pass\": \"" + std::string(pk_step_name(s)) + "\", \"n\": " +
+                                    std::to_string(kPlans[s.plan].n) + ", \"volume\": [" + std::to_string(d0.ny) + ", " +
+                                    std::to_string(d0.nx) + ", " + std::to_string(d0.nz) + "], \"nvol\": " +
+                                    std::to_string(s.nvol) + ", \"chosen\": \"" + variant_name(idx, f->second) +
+                                    "\", \"source\": \"cache\"}");
+            return f->second;
+        }
+    }
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+        cudaGetLastError();
+        return 0;   // no timing inside a capture
+    }
+    std::vector<float> ms;
+    int best = time_candidates(ctx, s, d0, idx, cands, st, ms);
+    if (best == -2) best = 0;
+    ctx->tune[key] = best;
+    std::string rec = "{\"pass\": \"" + std::string(pk_step_name(s)) + "\", \"n\": " + std::to_string(kPlans[s.plan].n) +
+                      ", \"volume\": [" + std::to_string(d0.ny) + ", " + std::to_string(d0.nx) + ", " +
+                      std::to_string(d0.nz) + "], \"nvol\": " + std::to_string(s.nvol) + ", \"chosen\": \"" +
+                      variant_name(idx, best) + "\", \"source\": \"timed\", \"ms\": {";
+    for (size_t i = 0; i < cands.size(); i++) {
+        char tmp[96];
+        snprintf(tmp, sizeof(tmp), "%s\"%s\": %.5f", i ? ", " : "", variant_name(idx, cands[i]), ms.size() > i ? ms[i] : -1.f);
+        rec += tmp;
+    }
+    rec += "}}";
+    ctx->tune_log.push_back(rec);
+    {
+        std::lock_guard<std::mutex> lk(g_tf_mu);
+        g_tf[fkey] = best;
+        float bms = 0.f;
+        for (size_t i = 0; i < cands.size(); i++)
+            if (cands[i] == best && i < ms.size()) bms = ms[i];
+        tf_store(fkey, best, bms);
+    }
+    return best;
 }
 
 // Decides which x / z steps run on the TMA kernels (every descriptor's maps encode and its rows
 // are at least one tile wide) and encodes their maps into prog.maps.
-void assign_tma(PkProgram& prog) {
+void assign_tma(pk_ctx* ctx, PkProgram& prog, cudaStream_t st) {
     prog.maps.assign(prog.descs.size(), XZMaps());
     const pkpass::YregTable* yt = yreg_kernels();
     for (PkStep& s : prog.steps) {
@@ -203,7 +439,17 @@ void assign_tma(PkProgram& prog) {
         if (idx < 0 || s.grid == 0) continue;
         const int axis = s.kind == PK_STEP_X ? 1 : 2;
         const pkpass::TmaTable* t = tma_kernels();
-        const int T = t->cols[s.plan][idx];
+        int* pf = prog.prefix.data() + s.prefix_off;
+        const int var = choose_variant(ctx, prog, s, idx, st);
+        if (var < 0) {   // the register-IO kernel: its own tile prefix
+            for (int i = 0; i < s.nvol; i++) {
+                const VolDesc& d = prog.descs[s.desc_off + i];
+                pf[i + 1] = pf[i] + (axis == 1 ? d.blocksX : d.blocksZ);
+            }
+            s.grid = pf[s.nvol];
+            continue;
+        }
+        const int T = t->cols[s.plan][idx][var];
         bool ok = true;
         for (int i = 0; i < s.nvol && ok; i++) {
             const VolDesc& d = prog.descs[s.desc_off + i];
@@ -213,15 +459,15 @@ void assign_tma(PkProgram& prog) {
         }
         if (!ok) continue;
         // the kernel's tiles are T columns wide: the step's tile prefix follows them
-        int* pf = prog.prefix.data() + s.prefix_off;
         for (int i = 0; i < s.nvol; i++) {
             const VolDesc& d = prog.descs[s.desc_off + i];
             pf[i + 1] = pf[i] + (axis == 1 ? d.nz : d.nx) * ((d.Py + T - 1) / T);
         }
         s.grid = pf[s.nvol];
         s.tma = idx;
-        s.tma_smem = t->smem[s.plan][idx];
-        s.tma_grid = std::min(s.grid, t->per_sm[s.plan][idx] * sm_count());
+        s.tma_var = var;
+        s.tma_smem = t->smem[s.plan][idx][var];
+        s.tma_grid = std::min(s.grid, t->per_sm[s.plan][idx][var] * sm_count());
     }
 }
 
@@ -287,14 +533,6 @@ __global__ void k_lambda(const VolDesc* __restrict__ descs, int nvol) {
 }
 
 }  // namespace
-
-// Descriptor blobs reach the device through this kernel, which reads the page-locked host copy
-// directly (zero-copy): a cudaMemcpyAsync would go through a copy engine, where it can queue behind
-// a large volume upload of another stream and hold back the compute stream for the whole upload.
-__global__ void k_blob_copy(uint4* __restrict__ dst, const uint4* __restrict__ src, long long n16) {
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n16; i += (long long)gridDim.x * blockDim.x)
-        dst[i] = src[i];
-}
 
 // One CTA waits on an mbarrier that nothing arrives on: the bounded wait runs out after limit_ns
 // and the failure goes to the context's status word (the self-test of the device waits).
@@ -468,18 +706,6 @@ size_t pk_spec_elems(const VolDesc& d) { return (size_t)d.Pp * (size_t)d.nrows; 
 // A program is the full launch sequence of a call (or of a batch / serving round): every step's
 // descriptors and block prefix live in one device buffer uploaded once, so the launches run
 // back to back without host synchronisation and can be captured into a CUDA graph.
-static size_t step_smem(int kind, int mode, const VolDesc& v) {
-    if (kind == PK_STEP_Y)
-        return sizeof(float2) * (tw_slots(v.M) + (v.odd ? 0 : v.M + 1) + padded_size(v.Ly * v.M) + v.Ly +
-                                 (size_t)pkpass::y_aux_arrays(mode) * v.Ly * v.M);
-    const bool conv = mode == XZ_CONV;
-    if (kind == PK_STEP_X)
-        return sizeof(float2) * (tw_slots(v.ax.n) + padded_size2(v.Tx * v.ax.n) + (conv ? v.Tx * v.ax.n : 0));
-    if (kind == PK_STEP_Z)
-        return sizeof(float2) * (tw_slots(v.az.n) + padded_size2(v.Tz * v.az.n) + (conv ? v.Tz * v.az.n : 0));
-    return 0;
-}
-
 // Kernel-table index of a pass: the axis plan, offset by kNumPlans for the small-tile kernels.
 static int step_plan(int kind, const VolDesc& v) {
     const int p = kind == PK_STEP_Y ? v.ay.plan : kind == PK_STEP_X ? v.ax.plan : kind == PK_STEP_Z ? v.az.plan : 0;
@@ -519,7 +745,7 @@ void pk_program_add(PkProgram& prog, int kind, int mode, const std::vector<VolDe
 }
 
 pk_status pk_program_upload(pk_ctx* ctx, PkProgram& prog, cudaStream_t st) {
-    assign_tma(prog);
+    assign_tma(ctx, prog, st);
     size_t dbytes, moff, need;
     blob_layout(prog, &dbytes, &moff, &need);
     const int si = ctx->next_slot;
@@ -612,7 +838,7 @@ static pk_status launch_steps(pk_ctx* ctx, const PkProgram& prog, cudaStream_t s
             cudaEventRecord(rec.a, st);
         }
         if (s.tma >= 0) {
-            tma_kernels()->k[s.plan][s.tma]<<<s.tma_grid, PK_XZT_THREADS, s.tma_smem, st>>>(
+            tma_kernels()->k[s.plan][s.tma][s.tma_var]<<<s.tma_grid, PK_XZT_THREADS, s.tma_smem, st>>>(
                 dd, prog.d_maps + s.desc_off, dp, s.nvol, ctx ? ctx->d_err : nullptr);
         } else if (s.yreg) {
             yreg_kernels()->k[s.mode]<<<s.grid, kThreads, s.yreg_smem, st>>>(dd, dp, s.nvol, ctx ? ctx->d_err : nullptr);
@@ -662,7 +888,7 @@ static bool build_graph(const PkProgram& prog, const VolDesc* d_desc, const int*
         p.gridDim = dim3(s.grid);
         p.sharedMemBytes = (unsigned)s.smem;
         if (s.tma >= 0) {
-            p.func = (void*)tma_kernels()->k[s.plan][s.tma];
+            p.func = (void*)tma_kernels()->k[s.plan][s.tma][s.tma_var];
             p.gridDim = dim3(s.tma_grid);
             p.blockDim = dim3(PK_XZT_THREADS);
             p.sharedMemBytes = (unsigned)s.tma_smem;
@@ -753,8 +979,8 @@ pk_status pk_program_launch(pk_ctx* ctx, PkProgram& prog, cudaStream_t st) {
         key.push_back((long long)prog.prefix.size());
         for (const PkStep& s : prog.steps) {
             const long long v[] = {s.kind, s.mode, s.plan, s.nvol, s.grid, (long long)s.smem, s.desc_off, s.prefix_off,
-                                   s.tma, s.tma_grid, s.yreg};
-            key.insert(key.end(), v, v + 11);
+                                   s.tma, s.tma_var, s.tma_grid, s.yreg};
+            key.insert(key.end(), v, v + 12);
         }
         auto it = ctx->graphs.find(key);
         if (it == ctx->graphs.end() && ctx->graph_seen.size() >= 4096) ctx->graph_seen.clear();  // bounded
@@ -857,4 +1083,18 @@ extern "C" pk_status pk_selftest_device_wait(pk_ctx* ctx, int64_t limit_ns) {
     cudaSetDevice(prev);
     if (e != cudaSuccess) return pk_fail(PK_ERR_CUDA, std::string("wait self-test: ") + cudaGetErrorString(e));
     return pk_check_device_waits(ctx);
+}
+
+extern "C" int32_t pk_ctx_tune_read(pk_ctx* ctx, char* buf, int32_t cap) {
+    if (!ctx) return -1;
+    std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+    std::string js = "[";
+    for (size_t i = 0; i < ctx->tune_log.size(); i++) js += (i ? ", " : "") + ctx->tune_log[i];
+    js += "]";
+    if (buf && cap > 0) {
+        const int n = std::min((int)js.size(), cap - 1);
+        memcpy(buf, js.data(), n);
+        buf[n] = 0;
+    }
+    return (int32_t)js.size();
 }

@@ -177,6 +177,10 @@ struct pk_ctx {
     // out (0 = none); h_err is the host view, d_err the device pointer passed to the kernels
     int* h_err = nullptr;
     int* d_err = nullptr;
+    // autotuner of the x / z passes: chosen variant per (pass, plan, geometry) key (-1 = register-IO
+    // kernel, 0.. = TMA variant), and a JSON record of each decision (pk_ctx_tune_read)
+    std::map<std::vector<long long>, int> tune;
+    std::vector<std::string> tune_log;
 };
 
 // error helpers (capi.cpp)
@@ -204,7 +208,7 @@ struct PkStep {
     size_t smem = 0;
     // set at upload: index of the persistent TMA kernel that runs this x / z step (-1: none), its
     // grid (resident CTAs, each walking tiles) and dynamic shared memory
-    int tma = -1, tma_grid = 0;
+    int tma = -1, tma_var = 0, tma_grid = 0;
     size_t tma_smem = 0;
     // set at upload: this y step runs the register-packing kernel (512-voxel rows), with its smem
     int yreg = 0;
