@@ -79,12 +79,13 @@ PK_API int64_t pk_ctx_kernel_launches(pk_ctx* ctx);
 PK_API pk_status pk_ctx_profile(pk_ctx* ctx, int32_t enable);
 PK_API int32_t pk_ctx_profile_read(pk_ctx* ctx, char* buf, int32_t cap);
 
-/* Autotuner record (no counterpart in the reference).  The first time an x / z pass of a given
- * transform plan and volume geometry runs on a context, each kernel variant that can run it (the
- * register-IO kernel and the TMA kernels' tile widths / buffer counts) is timed three times on
- * scratch buffers of that geometry and the fastest is kept; choices persist in an on-disk cache
- * (PK_TUNE_FILE, else ~/.cache/pkdecon/tune-v1.txt; PK_TUNE=0 disables the timing).  This writes
- * the context's decisions as a JSON list and returns its length (truncated to cap-1). */
+/* Autotuner record (no counterpart in the reference).  The first time a single-volume x / z pass of
+ * a given transform plan and size class (waves of resident CTAs its tiles make) runs on a context,
+ * each kernel variant that can run it (the register-IO kernel and the TMA kernels' tile widths /
+ * buffer counts) is timed on scratch buffers of that geometry and the fastest is kept for every
+ * later pass of that plan and class, batched and served ones included; choices persist in an
+ * on-disk cache (PK_TUNE_FILE, else ~/.cache/pkdecon/tune-v3.txt; PK_TUNE=0 disables the timing).
+ * This writes the context's decisions as a JSON list and returns its length (truncated to cap-1). */
 PK_API int32_t pk_ctx_tune_read(pk_ctx* ctx, char* buf, int32_t cap);
 
 /* Failure-detection self-test (no counterpart in the reference).  Every wait inside the pass
@@ -254,11 +255,13 @@ PK_API pk_status pk_tiff_write(const char* path, const void* data, const int64_t
                                int32_t is_float, int32_t lzw, int32_t threads);
 /* Zarr v2 volumes (io/readzarr.m, io/writezarr.m over io/cpp-zarr/src/parallelreadzarr.cpp,
  * parallelwritezarr.cpp).  An array of shape [ny nx nz] is the MATLAB array [ny nx nz]; chunks in
- * order "F" or "C", keys "i.j.k" or "i/j/k", compressor none, "zlib" or "gzip" (the reference's default
- * "blosc" gives PK_ERR_UNSUPPORTED: no blosc library in this build).  pk_zarr_read: the whole array or
+ * order "F" or "C", keys "i.j.k" or "i/j/k", compressor none, "zlib", "gzip" or "blosc" (the reference's
+ * default; lz4, zlib or zstd inside, byte shuffle or none; blosclz, snappy and bit shuffle give
+ * PK_ERR_INVALID on the chunk).  pk_zarr_read: the whole array or
  * bbox [y1 x1 z1 y2 x2 z2] (1-based inclusive; NULL = all) into out (column-major, the array's type);
  * missing chunks read as fill_value.  pk_zarr_write: order "F", separator ".", chunks = min(chunks, dims),
- * compressor 0 = none, 1 = zlib, 2 = gzip (level 1); chunks compressed on `threads` host threads. */
+ * compressor 0 = none, 1 = zlib, 2 = gzip (level 1), 3 = blosc lz4, 4 = blosc zstd, 5 = blosc zlib (clevel 5,
+ * byte shuffle, as zarr.cpp:17 sets); chunks compressed on `threads` host threads. */
 PK_API pk_status pk_zarr_info(const char* path, int64_t dims[3], int64_t chunks[3], int32_t* bits, int32_t* is_float);
 PK_API pk_status pk_zarr_read(const char* path, const int64_t* bbox, void* out, int64_t out_bytes, int32_t threads);
 PK_API pk_status pk_zarr_write(const char* path, const void* data, const int64_t dims[3], int32_t bits,

@@ -1,7 +1,8 @@
 """Zarr v2 restatement (oracle; test infrastructure).
 
-Reads and writes Zarr v2 arrays from the published storage specification with json, zlib, gzip
-and numpy, to check libpkdecon.so's reader / writer (tests/test_zarrio_cpu.py): ``.zarray`` with
+Reads and writes Zarr v2 arrays from the published storage specification with json, zlib, gzip,
+numpy and the blosc chunk restatement of oracle/blosc.py, to check libpkdecon.so's reader / writer
+(tests/test_zarrio_cpu.py, tests/test_blosc_cpu.py): ``.zarray`` with
 shape, chunks, dtype, order, compressor, fill_value and dimension_separator; one file per chunk named
 by its chunk indices; every chunk stored at full chunk size, in order "F" or "C".
 """
@@ -14,11 +15,16 @@ import zlib
 
 import numpy as np
 
+from . import blosc
 
-def write(path, a, chunks, order="F", compressor="zlib", separator=".", fill_value=0):
+
+def write(path, a, chunks, order="F", compressor="zlib", separator=".", fill_value=0, cname="lz4", split=True):
     a = np.asarray(a)
     os.makedirs(path, exist_ok=True)
-    comp = None if compressor is None else {"id": compressor, "level": 1}
+    if compressor == "blosc":
+        comp = {"blocksize": 0, "clevel": 5, "cname": cname, "id": "blosc", "shuffle": 1}
+    else:
+        comp = None if compressor is None else {"id": compressor, "level": 1}
     meta = {"chunks": list(chunks), "compressor": comp, "dimension_separator": separator,
             "dtype": a.dtype.str, "fill_value": fill_value, "filters": None, "order": order,
             "shape": list(a.shape), "zarr_format": 2}
@@ -35,6 +41,8 @@ def write(path, a, chunks, order="F", compressor="zlib", separator=".", fill_val
             raw = zlib.compress(raw, 1)
         elif compressor == "gzip":
             raw = gzip.compress(raw, 1)
+        elif compressor == "blosc":
+            raw = blosc.compress(raw, a.dtype.itemsize, cname=cname, split=split)
         key = separator.join(str(i) for i in idx)
         fn = os.path.join(path, *key.split("/")) if separator == "/" else os.path.join(path, key)
         os.makedirs(os.path.dirname(fn), exist_ok=True)
@@ -62,6 +70,8 @@ def read(path):
                 raw = zlib.decompress(raw)
             elif comp == "gzip":
                 raw = gzip.decompress(raw)
+            elif comp == "blosc":
+                raw = blosc.decompress(raw)
             blk = np.frombuffer(raw, dt).reshape(chunks, order=order)
         else:
             blk = np.full(chunks, fill, dt)

@@ -43,6 +43,7 @@ struct XztLayout {
     static constexpr size_t BUF = ((size_t)PTS * 8 + 1023) & ~(size_t)1023;
     static constexpr size_t TW = ((size_t)(plan_tw_size(P) > 0 ? plan_tw_size(P) : 1) * 8 + 15) & ~(size_t)15;
     static constexpr size_t bytes(bool conv) { return 1024 + NBUF * BUF + (conv ? BUF : 0) + TW + 64; }
+    static_assert(1024 + NBUF * BUF + BUF + TW + 64 <= 227 * 1024 || NBUF == 1, "tile buffers exceed shared memory");
 };
 
 // CTAs per SM a variant is compiled for (register budget): 3 for 4096-point tiles, 2 for the
@@ -52,18 +53,19 @@ constexpr int xzt_min_blocks(int P, int TC, int NBUF, bool conv) {
                                                                            : ((conv && NBUF == 2) ? 2 : 3);
 }
 
-// The TMA kernels run PK_THREADS compute threads (warps 0-7) and one producer warp (warp 8) that
+// The TMA kernels run NTH compute threads (NTH / 32 warps) and one producer warp after them that
 // issues the TMA loads and stores.  The compute warps synchronise among themselves on named
 // barrier 1, so the producer never holds them up and they never wait on a copy they do not need.
-#define PK_XZT_THREADS (PK_THREADS + 32)
-__device__ __forceinline__ void compute_bar() { asm volatile("bar.sync 1, %0;\n" ::"n"(PK_THREADS) : "memory"); }
+template <int NTH>
+__device__ __forceinline__ void compute_bar() { asm volatile("bar.sync 1, %0;\n" ::"n"(NTH) : "memory"); }
 // every compute thread's `ok`, and-reduced over the compute warps (named barrier 1)
+template <int NTH>
 __device__ __forceinline__ bool compute_bar_and(bool ok) {
     int r;
     asm volatile(
         "{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n bar.red.and.pred q, 1, %2, p;\n selp.u32 %0, 1, 0, q;\n}\n"
         : "=r"(r)
-        : "r"((unsigned)ok), "n"(PK_THREADS)
+        : "r"((unsigned)ok), "n"(NTH)
         : "memory");
     return r != 0;
 }
@@ -73,11 +75,11 @@ __device__ __forceinline__ void mbar_arrive_cta(uint64_t* bar) {
 }
 
 // ---- dense column-tile stages (element (l, e) at e*L + l, L = T columns)
-template <int R, int NS, int N, int L, bool INV, int OFF>
+template <int R, int NS, int N, int L, bool INV, int OFF, int NTH>
 __device__ __forceinline__ void dstage(float2* __restrict__ buf, const float2* __restrict__ tw, int tid) {
     constexpr int M = N / R;
     constexpr int B = L * M;
-    constexpr int NT = PK_THREADS;
+    constexpr int NT = NTH;
     constexpr int MAXB = (B + NT - 1) / NT;
     float2 v[MAXB][R];
 #pragma unroll
@@ -89,7 +91,7 @@ __device__ __forceinline__ void dstage(float2* __restrict__ buf, const float2* _
             for (int r = 0; r < R; r++) v[i][r] = buf[(j + r * M) * L + l];
         }
     }
-    compute_bar();
+    compute_bar<NTH>();
 #pragma unroll
     for (int i = 0; i < MAXB; i++) {
         const int b = tid + i * NT;
@@ -111,16 +113,16 @@ __device__ __forceinline__ void dstage(float2* __restrict__ buf, const float2* _
             for (int r = 0; r < R; r++) buf[a0 + r * NS * L] = v[i][r];
         }
     }
-    compute_bar();
+    compute_bar<NTH>();
 }
 
 // last stage into registers: v[i][r] = element (j - k) R + k + r NS of column l (b = tid + i NT)
-template <int R, int NS, int N, int L, bool INV, int OFF>
+template <int R, int NS, int N, int L, bool INV, int OFF, int NTH>
 __device__ __forceinline__ void dstage_s2r(const float2* __restrict__ buf, const float2* __restrict__ tw, int tid,
-                                           float2 (&v)[(L * (N / R) + PK_THREADS - 1) / PK_THREADS][R]) {
+                                           float2 (&v)[(L * (N / R) + NTH - 1) / NTH][R]) {
     constexpr int M = N / R;
     constexpr int B = L * M;
-    constexpr int NT = PK_THREADS;
+    constexpr int NT = NTH;
     constexpr int MAXB = (B + NT - 1) / NT;
 #pragma unroll
     for (int i = 0; i < MAXB; i++) {
@@ -131,7 +133,7 @@ __device__ __forceinline__ void dstage_s2r(const float2* __restrict__ buf, const
             for (int r = 0; r < R; r++) v[i][r] = buf[(j + r * M) * L + l];
         }
     }
-    compute_bar();
+    compute_bar<NTH>();
 #pragma unroll
     for (int i = 0; i < MAXB; i++) {
         const int b = tid + i * NT;
@@ -153,13 +155,13 @@ __device__ __forceinline__ void dstage_s2r(const float2* __restrict__ buf, const
 }
 
 // first stage from registers: v[i][r] is element j + r (N / R) of column l; butterfly, store
-template <int R, int N, int L, bool INV>
+template <int R, int N, int L, bool INV, int NTH>
 __device__ __forceinline__ void dstage_r2s(float2* __restrict__ buf, int tid,
-                                           float2 (&v)[(L * (N / R) + PK_THREADS - 1) / PK_THREADS][R]) {
+                                           float2 (&v)[(L * (N / R) + NTH - 1) / NTH][R]) {
     static_assert(!direct_radix(R), "first stage needs a register butterfly");
     constexpr int M = N / R;
     constexpr int B = L * M;
-    constexpr int NT = PK_THREADS;
+    constexpr int NT = NTH;
     constexpr int MAXB = (B + NT - 1) / NT;
 #pragma unroll
     for (int i = 0; i < MAXB; i++) {
@@ -172,15 +174,15 @@ __device__ __forceinline__ void dstage_r2s(float2* __restrict__ buf, int tid,
             for (int r = 0; r < R; r++) buf[a0 + r * L] = v[i][r];
         }
     }
-    compute_bar();
+    compute_bar<NTH>();
 }
 
-template <int P, int S, int S1, int NS, int L, bool INV>
+template <int P, int S, int S1, int NS, int L, bool INV, int NTH>
 __device__ __forceinline__ void run_dense(float2* buf, const float2* tw, int tid) {
     if constexpr (S < S1) {
         constexpr int R = kPlans[P].rad[S];
-        dstage<R, NS, kPlans[P].n, L, INV, stage_tw_off(P, S)>(buf, tw, tid);
-        run_dense<P, S + 1, S1, NS * R, L, INV>(buf, tw, tid);
+        dstage<R, NS, kPlans[P].n, L, INV, stage_tw_off(P, S), NTH>(buf, tw, tid);
+        run_dense<P, S + 1, S1, NS * R, L, INV, NTH>(buf, tw, tid);
     }
 }
 
@@ -196,8 +198,8 @@ __device__ __forceinline__ void run_dense(float2* buf, const float2* tw, int tid
 //     transforms, then release the OTF buffer), then release buffer s (empty[s]).
 // With NBUF = 2 the next tile's load is in flight while the current one is transformed.  Every wait
 // is bounded; a wait that runs out is recorded in *err and the role that saw it stops.
-template <int P, int AXIS, int MODE, int TC = 0, int NBUF = 2>
-__global__ void __launch_bounds__(PK_XZT_THREADS, xzt_min_blocks(P, TC, NBUF, MODE == XZ_CONV))
+template <int P, int AXIS, int MODE, int TC = 0, int NBUF = 2, int NTH = PK_THREADS>
+__global__ void __launch_bounds__(NTH + 32, xzt_min_blocks(P, TC, NBUF, MODE == XZ_CONV))
     k_xzt(const VolDesc* __restrict__ descs, const XZMaps* __restrict__ maps, const int* __restrict__ prefix, int nvol,
           int* err) {
     static_assert(NBUF == 1 || NBUF == 2, "one or two tile buffers");
@@ -206,7 +208,7 @@ __global__ void __launch_bounds__(PK_XZT_THREADS, xzt_min_blocks(P, TC, NBUF, MO
     constexpr int NST = kPlans[P].nst;
     constexpr bool CONV = MODE == XZ_CONV;
     constexpr uint32_t TILE_BYTES = (uint32_t)PTS * 8u;
-    constexpr int NT = PK_THREADS;
+    constexpr int NT = NTH;
     extern __shared__ unsigned char smraw[];
     unsigned char* sm = smraw + ((1024 - (pktma::smem_u32(smraw) & 1023)) & 1023);
     float2* bufs[2] = {(float2*)sm, (float2*)(sm + (NBUF - 1) * Lay::BUF)};
@@ -256,7 +258,7 @@ __global__ void __launch_bounds__(PK_XZT_THREADS, xzt_min_blocks(P, TC, NBUF, MO
     // the plan's twiddles, once per CTA (every volume of the launch has this plan)
     {
         const float2* gtw = AXIS == 1 ? descs[0].ax.tw : descs[0].az.tw;
-        for (int i = tid; i < plan_tw_size(P); i += PK_XZT_THREADS) tw[i] = gtw[i];
+        for (int i = tid; i < plan_tw_size(P); i += NTH + 32) tw[i] = gtw[i];
     }
     __syncthreads();
 
@@ -308,28 +310,28 @@ __global__ void __launch_bounds__(PK_XZT_THREADS, xzt_min_blocks(P, TC, NBUF, MO
         return;
     }
 
-    // ---------------- compute (warps 0-7)
+    // ---------------- compute (warps 0 .. NTH/32 - 1)
     int it = 0;
     for (int g = blockIdx.x; g < total; g += gridDim.x, it++) {
         const int s = NBUF == 2 ? (it & 1) : 0;
         float2* cur = bufs[s];
         const int vol = find_vol(prefix, nvol, g);
         bool ok = pktma::mbar_wait(&full[s], (uint32_t)((it / NBUF) & 1));
-        if (!compute_bar_and(ok)) {
+        if (!compute_bar_and<NTH>(ok)) {
             if (tid == 0) pktma::report_wait_failure(err, 1);
             return;
         }
         if constexpr (!CONV) {
-            run_dense<P, 0, NST, 1, T, MODE == XZ_INV>(cur, tw, tid);
+            run_dense<P, 0, NST, 1, T, MODE == XZ_INV, NTH>(cur, tw, tid);
         } else {
             const bool cj = descs[vol].conj != 0;
             if constexpr (pkpass::same_end_radix(P)) {
                 constexpr int R = kPlans[P].rad[0], MS = N / R, MAXB = (T * MS + NT - 1) / NT;
                 float2 v[MAXB][R];
-                run_dense<P, 0, NST - 1, 1, T, false>(cur, tw, tid);
-                dstage_s2r<R, plan_ns_before(P, NST - 1), N, T, false, stage_tw_off(P, NST - 1)>(cur, tw, tid, v);
+                run_dense<P, 0, NST - 1, 1, T, false, NTH>(cur, tw, tid);
+                dstage_s2r<R, plan_ns_before(P, NST - 1), N, T, false, stage_tw_off(P, NST - 1), NTH>(cur, tw, tid, v);
                 ok = pktma::mbar_wait(otf_full, (uint32_t)(it & 1));
-                if (!compute_bar_and(ok)) {
+                if (!compute_bar_and<NTH>(ok)) {
                     if (tid == 0) pktma::report_wait_failure(err, 1);
                     return;
                 }
@@ -346,14 +348,14 @@ __global__ void __launch_bounds__(PK_XZT_THREADS, xzt_min_blocks(P, TC, NBUF, MO
                         }
                     }
                 }
-                compute_bar();   // every OTF read done: the producer may refill it
+                compute_bar<NTH>();   // every OTF read done: the producer may refill it
                 if (tid == 0) mbar_arrive_cta(otf_empty);
-                dstage_r2s<R, N, T, true>(cur, tid, v);
-                run_dense<P, 1, NST, R, T, true>(cur, tw, tid);
+                dstage_r2s<R, N, T, true, NTH>(cur, tid, v);
+                run_dense<P, 1, NST, R, T, true, NTH>(cur, tw, tid);
             } else {
-                run_dense<P, 0, NST, 1, T, false>(cur, tw, tid);
+                run_dense<P, 0, NST, 1, T, false, NTH>(cur, tw, tid);
                 ok = pktma::mbar_wait(otf_full, (uint32_t)(it & 1));
-                if (!compute_bar_and(ok)) {
+                if (!compute_bar_and<NTH>(ok)) {
                     if (tid == 0) pktma::report_wait_failure(err, 1);
                     return;
                 }
@@ -362,15 +364,15 @@ __global__ void __launch_bounds__(PK_XZT_THREADS, xzt_min_blocks(P, TC, NBUF, MO
                     if (cj) h.y = -h.y;
                     cur[i] = cmul(cur[i], h);
                 }
-                compute_bar();
+                compute_bar<NTH>();
                 if (tid == 0) mbar_arrive_cta(otf_empty);
-                run_dense<P, 0, NST, 1, T, true>(cur, tw, tid);
+                run_dense<P, 0, NST, 1, T, true, NTH>(cur, tw, tid);
             }
         }
         // the tile leaves by TMA: each thread's writes are ordered before the async proxy's reads,
         // then the buffer is handed to the producer
         pktma::fence_async_smem();
-        compute_bar();
+        compute_bar<NTH>();
         if (tid == 0) mbar_arrive_cta(&empty[s]);
     }
 }
@@ -387,11 +389,13 @@ struct TmaTable {
     int per_sm[kNumPlans][3][kTmaVariants];
     int cols[kNumPlans][3][kTmaVariants];    // columns per tile (the tile prefix and the TMA box follow it)
     int nbuf[kNumPlans][3][kTmaVariants];
+    int threads[kNumPlans][3][kTmaVariants];   // compute threads + the producer warp
 };
 
-template <int P, int IDX, int VAR, int AXIS, int MODE, int TC = 0, int NBUF = 2>
+template <int P, int IDX, int VAR, int AXIS, int MODE, int TC = 0, int NBUF = 2, int NTH = PK_THREADS>
 inline void register_tma_one(TmaTable& t) {
-    auto fn = k_xzt<P, AXIS, MODE, TC, NBUF>;
+    auto fn = k_xzt<P, AXIS, MODE, TC, NBUF, NTH>;
+    t.threads[P][IDX][VAR] = NTH + 32;
     const size_t smem = XztLayout<P, TC, NBUF>::bytes(MODE == XZ_CONV);
     t.k[P][IDX][VAR] = fn;
     t.smem[P][IDX][VAR] = smem;
@@ -399,7 +403,7 @@ inline void register_tma_one(TmaTable& t) {
     t.nbuf[P][IDX][VAR] = NBUF;
     int n = 0;
     if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, PK_XZT_THREADS, smem) != cudaSuccess || n < 1) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, NTH + 32, smem) != cudaSuccess || n < 1) {
         cudaGetLastError();
         t.k[P][IDX][VAR] = nullptr;   // this variant is not offered
         n = 0;
@@ -415,15 +419,18 @@ struct RegisterTma {
             register_tma_one<P, TMA_X_INV, 0, 1, XZ_INV>(t);
             register_tma_one<P, TMA_Z_CONV, 0, 2, XZ_CONV>(t);
             if constexpr (kPlans[P].n == 512) {
-                // 8-column tiles (64-byte rows) against 16-column tiles (128-byte rows) with one or two buffers
-                register_tma_one<P, TMA_X_FWD, 1, 1, XZ_FWD, 16, 1>(t);
-                register_tma_one<P, TMA_X_INV, 1, 1, XZ_INV, 16, 1>(t);
+                // 8-column tiles (64-byte rows, 3 CTAs per SM) against 16-column tiles (128-byte rows,
+                // two buffers, one CTA per SM) with 8 or 16 compute warps
+                register_tma_one<P, TMA_X_FWD, 1, 1, XZ_FWD, 16, 2, 512>(t);
+                register_tma_one<P, TMA_X_INV, 1, 1, XZ_INV, 16, 2, 512>(t);
                 register_tma_one<P, TMA_X_FWD, 2, 1, XZ_FWD, 16, 2>(t);
                 register_tma_one<P, TMA_X_INV, 2, 1, XZ_INV, 16, 2>(t);
             }
             if constexpr (kPlans[P].n == 256) {
-                // the convolution with one tile buffer (three CTAs per SM instead of two)
-                register_tma_one<P, TMA_Z_CONV, 1, 2, XZ_CONV, 0, 1>(t);
+                // the convolution with 32-column tiles (256-byte rows, one CTA per SM) and 16 or 8
+                // compute warps
+                register_tma_one<P, TMA_Z_CONV, 1, 2, XZ_CONV, 32, 2, 512>(t);
+                register_tma_one<P, TMA_Z_CONV, 2, 2, XZ_CONV, 32, 2>(t);
             }
         }
         RegisterTma<P + 1, HI>::fill(t);

@@ -207,11 +207,11 @@ int tma_index(const PkStep& s) {
 // ------------------------------------------------------------------ autotuner of the x / z passes
 // An x / z step can run on the register-IO kernel (k_xz, variant -1) or on a TMA variant (k_xzt:
 // 0 = the plan's 4096-point tile with two buffers; 1, 2 = the alternatives built for the plan).
-// The first time a (pass, plan, volume geometry) is seen, every candidate runs three times on
-// scratch buffers of that geometry (zeroed spectrum and OTF; no live data is touched) and the
-// fastest is kept for the context and appended to an on-disk cache (PK_TUNE_FILE, else
-// ~/.cache/pkdecon/tune-v1.txt), keyed by the device name, so later processes skip the timing.
-// PK_TUNE=0 turns the timing off (variant 0 everywhere).
+// The first time a single-volume step of a (pass, plan, size class) is seen, every candidate runs
+// once to warm up and twice timed on scratch buffers of that step's geometry (zeroed spectrum and
+// OTF; no live data is touched); the fastest is kept for the context and appended to an on-disk
+// cache (PK_TUNE_FILE, else ~/.cache/pkdecon/tune-v3.txt), keyed by the device name, so later
+// processes skip the timing.  PK_TUNE=0 turns the timing off (the fallback choice everywhere).
 
 std::mutex g_tf_mu;
 std::map<std::string, int> g_tf;   // "<device>|<key>" -> variant
@@ -222,7 +222,7 @@ std::string tune_path() {
     if (e && *e) return e;
     const char* h = getenv("HOME");
     if (!h || !*h) return "";
-    return std::string(h) + "/.cache/pkdecon/tune-v1.txt";
+    return std::string(h) + "/.cache/pkdecon/tune-v3.txt";
 }
 
 std::string device_tag(int dev) {
@@ -262,10 +262,11 @@ void tf_store(const std::string& key, int v, float ms) {
 }
 
 const char* variant_name(int idx, int v) {
-    static const char* names[] = {"register-IO", "tma", "tma-16col-1buf", "tma-16col-2buf", "tma-1buf"};
+    static const char* names[] = {"register-IO", "tma", "tma-16col-16warps", "tma-16col-8warps", "tma-32col-16warps",
+                                  "tma-32col-8warps"};
     if (v < 0) return names[0];
     if (v == 0) return names[1];
-    if (idx == pkpass::TMA_Z_CONV) return names[4];
+    if (idx == pkpass::TMA_Z_CONV) return v == 1 ? names[4] : names[5];
     return v == 1 ? names[2] : names[3];
 }
 
@@ -273,6 +274,7 @@ const char* variant_name(int idx, int v) {
 // fastest, or -2 when nothing could be timed.  ms[i] receives candidate i's time.
 int time_candidates(pk_ctx* ctx, const PkStep& s, const VolDesc& d0, int idx, const std::vector<int>& cands,
                     cudaStream_t st, std::vector<float>& ms) {
+    // (d0 is the geometry timed: the step's first volume, its outer extent scaled to the step's tiles)
     const pkpass::TmaTable* t = tma_kernels();
     const pkpass::KernelTable& kt = kernels();
     const int axis = s.kind == PK_STEP_X ? 1 : 2;
@@ -329,16 +331,16 @@ int time_candidates(pk_ctx* ctx, const PkStep& s, const VolDesc& d0, int idx, co
         const int* dp = (const int*)(d + poff);
         auto launch = [&]() {
             if (v < 0) kt.xz[s.plan]<<<grid, PK_THREADS, smem, st>>>(dd, dp, 1, axis, s.mode);
-            else t->k[s.plan][idx][v]<<<grid, PK_XZT_THREADS, smem, st>>>(dd, dm, dp, 1, ctx->d_err);
+            else t->k[s.plan][idx][v]<<<grid, t->threads[s.plan][idx][v], smem, st>>>(dd, dm, dp, 1, ctx->d_err);
         };
         for (int r = 0; ok && r < 1; r++) launch();
         ok = ok && cudaEventRecord(e0, st) == cudaSuccess;
-        for (int r = 0; ok && r < 3; r++) launch();
+        for (int r = 0; ok && r < 2; r++) launch();
         ok = ok && cudaEventRecord(e1, st) == cudaSuccess && cudaEventSynchronize(e1) == cudaSuccess;
         float el = 0.f;
         ok = ok && cudaEventElapsedTime(&el, e0, e1) == cudaSuccess;
         if (!ok) break;
-        ms[ci] = el / 3.f;
+        ms[ci] = el / 2.f;
         if (ms[ci] < best_ms) {
             best_ms = ms[ci];
             best = v;
@@ -356,7 +358,26 @@ int time_candidates(pk_ctx* ctx, const PkStep& s, const VolDesc& d0, int idx, co
     return best;
 }
 
+// Size class of an x / z step: how many waves of variant 0's resident CTAs its tiles make (0: under
+// one wave, 1: one to three, 2: more).  Variants are chosen per (pass, plan, size class).
+int size_class(const PkProgram& prog, const PkStep& s, int idx) {
+    const pkpass::TmaTable* t = tma_kernels();
+    const int T = t->cols[s.plan][idx][0];
+    long long tiles = 0;
+    for (int i = 0; i < s.nvol; i++) {
+        const VolDesc& d = prog.descs[s.desc_off + i];
+        tiles += (long long)(s.kind == PK_STEP_X ? d.nz : d.nx) * ((d.Py + T - 1) / T);
+    }
+    const long long wave = (long long)std::max(1, t->per_sm[s.plan][idx][0]) * sm_count();
+    return tiles < wave ? 0 : tiles < 3 * wave ? 1 : 2;
+}
+
 // The variant an x / z step runs: the context's earlier choice, the on-disk cache's, or a timing.
+// A step times its candidates once per (pass, plan, size class): on its own volume, or for a
+// multi-volume step of a batch or a serving round on its first volume stretched to the step's
+// tile count; without a timing (inside a stream capture, PK_TUNE=0) it takes the fallback:
+// register-IO under one wave of tiles, where the persistent kernel's set-up does not pay, else TMA
+// variant 0.
 int choose_variant(pk_ctx* ctx, const PkProgram& prog, const PkStep& s, int idx, cudaStream_t st) {
     const pkpass::TmaTable* t = tma_kernels();
     std::vector<int> cands;
@@ -364,48 +385,70 @@ int choose_variant(pk_ctx* ctx, const PkProgram& prog, const PkStep& s, int idx,
     for (int v = 0; v < pkpass::kTmaVariants; v++)
         if (t->k[s.plan][idx][v]) cands.push_back(v);
     const VolDesc& d0 = prog.descs[s.desc_off];
-    if (!ctx || cands.size() < 2) return 0;
-    const std::vector<long long> key = {s.kind, s.mode, s.plan, d0.ny, d0.nx, d0.nz, s.nvol};
+    const int cls = size_class(prog, s, idx);
+    const int fallback = (cls == 0 && kernels().xz[s.plan]) ? -1 : 0;
+    if (!ctx || cands.size() < 2) return cands.empty() ? 0 : (cands.size() == 1 ? cands[0] : fallback);
+    const std::vector<long long> key = {s.kind, s.mode, s.plan, cls};
     auto it = ctx->tune.find(key);
     if (it != ctx->tune.end()) return it->second;
-    const char* off = getenv("PK_TUNE");
-    if (off && off[0] == '0') return 0;
     std::string fkey = device_tag(ctx->device) + "|";
     for (size_t i = 0; i < key.size(); i++) fkey += (i ? "," : "") + std::to_string(key[i]);
+    auto record = [&](int v, const char* source, const std::vector<float>* ms) {
+        std::string rec = "{\"pass\": \"" + std::string(pk_step_name(s)) + "\", \"n\": " + std::to_string(kPlans[s.plan].n) +
+                          ", \"size_class\": " + std::to_string(cls) + ", \"timed_on\": [" + std::to_string(d0.ny) + ", " +
+                          std::to_string(d0.nx) + ", " + std::to_string(d0.nz) + "], \"chosen\": \"" +
+                          variant_name(idx, v) + "\", \"source\": \"" + source + "\"";
+        if (ms) {
+            rec += ", \"ms\": {";
+            for (size_t i = 0; i < cands.size(); i++) {
+                char tmp[96];
+                snprintf(tmp, sizeof(tmp), "%s\"%s\": %.5f", i ? ", " : "", variant_name(idx, cands[i]),
+                         ms->size() > i ? (*ms)[i] : -1.f);
+                rec += tmp;
+            }
+            rec += "}";
+        }
+        rec += "}";
+        ctx->tune_log.push_back(rec);
+    };
     {
         std::lock_guard<std::mutex> lk(g_tf_mu);
         tf_load();
         auto f = g_tf.find(fkey);
         if (f != g_tf.end() && std::find(cands.begin(), cands.end(), f->second) != cands.end()) {
             ctx->tune[key] = f->second;
-            ctx->tune_log.push_back("{\"pass\": \"" + std::string(pk_step_name(s)) + "\", \"n\": " +
-                                    std::to_string(kPlans[s.plan].n) + ", \"volume\": [" + std::to_string(d0.ny) + ", " +
-                                    std::to_string(d0.nx) + ", " + std::to_string(d0.nz) + "], \"nvol\": " +
-                                    std::to_string(s.nvol) + ", \"chosen\": \"" + variant_name(idx, f->second) +
-                                    "\", \"source\": \"cache\"}");
+            record(f->second, "cache", nullptr);
             return f->second;
         }
     }
+    const char* off = getenv("PK_TUNE");
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-    if (cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
-        cudaGetLastError();
-        return 0;   // no timing inside a capture
+    const bool capturing = cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone;
+    if (capturing) cudaGetLastError();
+    if ((off && off[0] == '0') || capturing) return fallback;   // no timing here
+    // the timed geometry: the first volume, with its outer extent (z for an x pass, x for a z pass)
+    // scaled so that it has as many tiles as the whole step (a batch's or a round's volumes together)
+    VolDesc dt = d0;
+    if (s.nvol > 1) {
+        const int T0 = t->cols[s.plan][idx][0];
+        long long tiles = 0;
+        for (int i = 0; i < s.nvol; i++) {
+            const VolDesc& d = prog.descs[s.desc_off + i];
+            tiles += (long long)(s.kind == PK_STEP_X ? d.nz : d.nx) * ((d.Py + T0 - 1) / T0);
+        }
+        const long long per_outer = (d0.Py + T0 - 1) / T0;
+        const int outer = (int)std::min<long long>(4096, std::max<long long>(1, (tiles + per_outer - 1) / per_outer));
+        if (s.kind == PK_STEP_X) dt.nz = outer;
+        else dt.nx = outer;
+        dt.nrows = (long long)dt.nx * dt.nz;
+        dt.blocksX = dt.nz * ((dt.Py + dt.Tx - 1) / dt.Tx);
+        dt.blocksZ = dt.nx * ((dt.Py + dt.Tz - 1) / dt.Tz);
     }
     std::vector<float> ms;
-    int best = time_candidates(ctx, s, d0, idx, cands, st, ms);
-    if (best == -2) best = 0;
+    int best = time_candidates(ctx, s, dt, idx, cands, st, ms);
+    if (best == -2) return fallback;
     ctx->tune[key] = best;
-    std::string rec = "{\"pass\": \"" + std::string(pk_step_name(s)) + "\", \"n\": " + std::to_string(kPlans[s.plan].n) +
-                      ", \"volume\": [" + std::to_string(d0.ny) + ", " + std::to_string(d0.nx) + ", " +
-                      std::to_string(d0.nz) + "], \"nvol\": " + std::to_string(s.nvol) + ", \"chosen\": \"" +
-                      variant_name(idx, best) + "\", \"source\": \"timed\", \"ms\": {";
-    for (size_t i = 0; i < cands.size(); i++) {
-        char tmp[96];
-        snprintf(tmp, sizeof(tmp), "%s\"%s\": %.5f", i ? ", " : "", variant_name(idx, cands[i]), ms.size() > i ? ms[i] : -1.f);
-        rec += tmp;
-    }
-    rec += "}}";
-    ctx->tune_log.push_back(rec);
+    record(best, "timed", &ms);
     {
         std::lock_guard<std::mutex> lk(g_tf_mu);
         g_tf[fkey] = best;
@@ -417,8 +460,6 @@ int choose_variant(pk_ctx* ctx, const PkProgram& prog, const PkStep& s, int idx,
     return best;
 }
 
-// Decides which x / z steps run on the TMA kernels (every descriptor's maps encode and its rows
-// are at least one tile wide) and encodes their maps into prog.maps.
 void assign_tma(pk_ctx* ctx, PkProgram& prog, cudaStream_t st) {
     prog.maps.assign(prog.descs.size(), XZMaps());
     const pkpass::YregTable* yt = yreg_kernels();
@@ -838,7 +879,8 @@ static pk_status launch_steps(pk_ctx* ctx, const PkProgram& prog, cudaStream_t s
             cudaEventRecord(rec.a, st);
         }
         if (s.tma >= 0) {
-            tma_kernels()->k[s.plan][s.tma][s.tma_var]<<<s.tma_grid, PK_XZT_THREADS, s.tma_smem, st>>>(
+            tma_kernels()->k[s.plan][s.tma][s.tma_var]<<<s.tma_grid, tma_kernels()->threads[s.plan][s.tma][s.tma_var],
+                                                         s.tma_smem, st>>>(
                 dd, prog.d_maps + s.desc_off, dp, s.nvol, ctx ? ctx->d_err : nullptr);
         } else if (s.yreg) {
             yreg_kernels()->k[s.mode]<<<s.grid, kThreads, s.yreg_smem, st>>>(dd, dp, s.nvol, ctx ? ctx->d_err : nullptr);
@@ -890,7 +932,7 @@ static bool build_graph(const PkProgram& prog, const VolDesc* d_desc, const int*
         if (s.tma >= 0) {
             p.func = (void*)tma_kernels()->k[s.plan][s.tma][s.tma_var];
             p.gridDim = dim3(s.tma_grid);
-            p.blockDim = dim3(PK_XZT_THREADS);
+            p.blockDim = dim3(tma_kernels()->threads[s.plan][s.tma][s.tma_var]);
             p.sharedMemBytes = (unsigned)s.tma_smem;
             p.kernelParams = argst;
         } else if (s.yreg) {

@@ -5,8 +5,8 @@
 //   * A MATLAB array [ny nx nz] is the Zarr array of shape [ny, nx, nz] (the reference writes order
 //     "F" with chunk keys "i.j.k" in the same axis order); chunks are read in either order ("F" or "C")
 //     and with either key separator ("." or "/").
-//   * Compressors: none, "zlib" and "gzip" (zlib is in this image).  The reference's default,
-//     "blosc" (with zstd or lz4 inside), is rejected with PK_ERR_UNSUPPORTED: no blosc library is here.
+//   * Compressors: none, "zlib", "gzip" and "blosc" (the reference's default, cname "lz4", clevel 5,
+//     shuffle 1: io/cpp-zarr/src/zarr.cpp:17) with lz4, zlib or zstd inside (csrc/blosc.cu).
 //   * Reading: the chunks that meet the requested box are decoded in parallel (one task per chunk, a
 //     pool of host threads) and their intersection copied into the column-major output; a missing
 //     chunk file reads as fill_value.  Writing: full-size chunks (edges padded with 0), zlib level 1
@@ -29,6 +29,10 @@
 
 #include "pk_internal.h"
 
+bool pk_blosc_decompress(const uint8_t* src, size_t slen, uint8_t* dst, size_t dst_len, std::string* err);
+bool pk_blosc_compress(const uint8_t* src, size_t n, int typesize, const std::string& cname, int clevel, bool shuffle,
+                       std::vector<uint8_t>& out, std::string* err);
+
 namespace {
 
 struct ZMeta {
@@ -38,7 +42,9 @@ struct ZMeta {
     char kind = 'u';            // 'u' unsigned, 'i' signed, 'f' float
     bool big_endian = false;
     bool order_c = false;
-    std::string compressor;     // "", "zlib", "gzip", or another id (unsupported)
+    std::string compressor;     // "", "zlib", "gzip", "blosc", or another id (unsupported)
+    std::string cname = "lz4";  // blosc: the codec inside, its level and shuffle (for writes)
+    int clevel = 5, shuffle = 1;
     std::string separator = ".";
     double fill = 0.0;
 };
@@ -157,13 +163,21 @@ pk_status parse_meta(const char* path, ZMeta& m) {
         const size_t ce = s.find('}', ci);
         const std::string obj = s.substr(ci, ce - ci + 1);     // the compressor object: its "id"
         m.compressor = read_str(obj, find_key(obj, "id"));
+        if (m.compressor == "blosc") {
+            const size_t cn = find_key(obj, "cname");
+            if (cn != std::string::npos) m.cname = read_str(obj, cn);
+            const size_t cl = find_key(obj, "clevel");
+            if (cl != std::string::npos) m.clevel = atoi(obj.c_str() + cl);
+            const size_t sh = find_key(obj, "shuffle");
+            if (sh != std::string::npos) m.shuffle = atoi(obj.c_str() + sh);
+        }
     }
     const size_t fi = find_key(s, "fill_value");
     if (fi != std::string::npos && s[fi] == 't') m.fill = 1.0;                     // JSON true (bool arrays)
     else if (fi != std::string::npos && s[fi] != 'n' && s[fi] != '"' && s[fi] != 'f') m.fill = strtod(s.c_str() + fi, nullptr);
-    if (!m.compressor.empty() && m.compressor != "zlib" && m.compressor != "gzip")
+    if (!m.compressor.empty() && m.compressor != "zlib" && m.compressor != "gzip" && m.compressor != "blosc")
         return pk_fail(PK_ERR_UNSUPPORTED, "zarr: compressor \"" + m.compressor +
-                                               "\" is not supported here (none, zlib and gzip are; blosc is not in this image)");
+                                               "\" is not supported here (none, zlib, gzip and blosc are)");
     return PK_OK;
 }
 
@@ -183,6 +197,10 @@ bool decode_chunk(const ZMeta& m, const std::vector<uint8_t>& raw, std::vector<u
         if (raw.size() < out.size()) return false;
         memcpy(out.data(), raw.data(), out.size());
         return true;
+    }
+    if (m.compressor == "blosc") {
+        std::string err;
+        return pk_blosc_decompress(raw.data(), raw.size(), out.data(), out.size(), &err);
     }
     z_stream zs;
     memset(&zs, 0, sizeof(zs));
@@ -276,12 +294,13 @@ bool deflate_piece(const uint8_t* p, size_t n, bool last, std::vector<uint8_t>& 
 // chunk.  With fewer (a few large chunks), each chunk's deflate is cut into 1 MB pieces compressed
 // in parallel and joined behind one zlib / gzip header, the Adler-32 / CRC-32 of the pieces joined
 // with zlib's adler32_combine / crc32_combine: a standard stream that every reader decodes.
+// comp 3: blosc with the codec, level, shuffle and element size of `bm`, one task per chunk.
 template <typename Prep>
-bool write_chunks(size_t ntask, size_t cb, int comp, int T, Prep&& prep) {
+bool write_chunks(size_t ntask, size_t cb, int comp, int T, Prep&& prep, const ZMeta* bm = nullptr) {
     std::atomic<int> err(0);
     constexpr size_t PIECE = size_t(1) << 20;
     const size_t np = comp ? std::max<size_t>(1, (cb + PIECE - 1) / PIECE) : 1;
-    if (comp == 0 || np == 1 || ntask >= (size_t)T) {
+    if (comp == 0 || comp == 3 || np == 1 || ntask >= (size_t)T) {
         std::vector<std::vector<uint8_t>> bufs(T), zbufs(T);
         pfor(ntask, T, [&](size_t t, int w) {
             if (err) return;
@@ -289,7 +308,12 @@ bool write_chunks(size_t ntask, size_t cb, int comp, int T, Prep&& prep) {
             const std::string fn = prep(t, buf);
             bool ok;
             if (comp == 0) ok = write_file(fn, buf.data(), buf.size());
-            else ok = deflate_whole(buf, comp == 2, zbufs[w]) && write_file(fn, zbufs[w].data(), zbufs[w].size());
+            else if (comp == 3) {
+                std::string e;
+                ok = bm && pk_blosc_compress(buf.data(), buf.size(), bm->es, bm->cname, bm->clevel, bm->shuffle != 0,
+                                             zbufs[w], &e) &&
+                     write_file(fn, zbufs[w].data(), zbufs[w].size());
+            } else ok = deflate_whole(buf, comp == 2, zbufs[w]) && write_file(fn, zbufs[w].data(), zbufs[w].size());
             if (!ok) err = 1;
         });
         return !err;
@@ -477,7 +501,9 @@ extern "C" pk_status pk_zarr_write(const char* path, const void* data, const int
     if (!path || !data || !dims || !chunks) return pk_fail(PK_ERR_INVALID, "NULL path/data/dims/chunks");
     if (!((!is_float && (bits == 8 || bits == 16 || bits == 32)) || (is_float && (bits == 32 || bits == 64))))
         return pk_fail(PK_ERR_INVALID, "zarr: data must be uint8/16/32, single or double");
-    if (compressor < 0 || compressor > 2) return pk_fail(PK_ERR_INVALID, "zarr: compressor must be 0 (none), 1 (zlib) or 2 (gzip)");
+    if (compressor < 0 || compressor > 5)
+        return pk_fail(PK_ERR_INVALID, "zarr: compressor must be 0 (none), 1 (zlib), 2 (gzip), 3 (blosc lz4), 4 (blosc zstd) "
+                                       "or 5 (blosc zlib)");
     int64_t ch[3];
     for (int d = 0; d < 3; d++) {
         if (dims[d] < 1 || chunks[d] < 1) return pk_fail(PK_ERR_INVALID, "zarr: sizes must be positive");
@@ -487,7 +513,17 @@ extern "C" pk_status pk_zarr_write(const char* path, const void* data, const int
     if (!make_dir(root)) return pk_fail(PK_ERR_INVALID, "zarr: cannot create " + root);
     const int es = bits / 8;
     char meta[1024];
-    const char* comp = compressor == 1 ? "{\"id\": \"zlib\", \"level\": 1}" : compressor == 2 ? "{\"id\": \"gzip\", \"level\": 1}" : "null";
+    // blosc: the reference's defaults (clevel 5, byte shuffle) with lz4, zstd or zlib inside
+    static const char* kBlosc[3] = {"lz4", "zstd", "zlib"};
+    char bcomp[160];
+    if (compressor >= 3)
+        snprintf(bcomp, sizeof(bcomp),
+                 "{\"blocksize\": 0, \"clevel\": 5, \"cname\": \"%s\", \"id\": \"blosc\", \"shuffle\": 1}",
+                 kBlosc[compressor - 3]);
+    const char* comp = compressor == 1 ? "{\"id\": \"zlib\", \"level\": 1}"
+                       : compressor == 2 ? "{\"id\": \"gzip\", \"level\": 1}"
+                       : compressor >= 3 ? bcomp
+                                         : "null";
     snprintf(meta, sizeof(meta),
              "{\n    \"chunks\": [%lld, %lld, %lld],\n    \"compressor\": %s,\n    \"dimension_separator\": \".\",\n"
              "    \"dtype\": \"<%c%d\",\n    \"fill_value\": 0,\n    \"filters\": null,\n    \"order\": \"F\",\n"
@@ -502,8 +538,15 @@ extern "C" pk_status pk_zarr_write(const char* path, const void* data, const int
     const int T = nthreads(threads);
     ZMeta m;
     m.ndim = 3;
+    m.es = es;
+    if (compressor >= 3) {
+        static const char* kB[3] = {"lz4", "zstd", "zlib"};
+        m.cname = kB[compressor - 3];
+        m.clevel = 5;
+        m.shuffle = 1;
+    }
     const uint8_t* in = (const uint8_t*)data;
-    const bool ok = write_chunks(ntask, cn * es, compressor, T, [&](size_t t, std::vector<uint8_t>& buf) {
+    const bool ok = write_chunks(ntask, cn * es, compressor >= 3 ? 3 : compressor, T, [&](size_t t, std::vector<uint8_t>& buf) {
         const int64_t c[3] = {(int64_t)(t % nc[0]), (int64_t)((t / nc[0]) % nc[1]), (int64_t)(t / (nc[0] * nc[1]))};
         buf.assign(cn * es, 0);                                   // edge chunks padded with the fill value
         int64_t a[3], b[3];
@@ -516,7 +559,7 @@ extern "C" pk_status pk_zarr_write(const char* path, const void* data, const int
                 memcpy(buf.data() + (((z - a[2]) * ch[1] + (x - a[1])) * ch[0]) * es,
                        in + ((z * dims[1] + x) * dims[0] + a[0]) * es, (size_t)(b[0] - a[0]) * es);
         return root + "/" + chunk_key(m, c);
-    });
+    }, &m);
     if (!ok) return pk_fail(PK_ERR_INVALID, "zarr: writing a chunk of " + root + " failed");
     return PK_OK;
 }
@@ -542,7 +585,7 @@ extern "C" pk_status pk_zarr_write_region(const char* path, const void* data, co
     const size_t cn = (size_t)(m.chunks[0] * m.chunks[1] * m.chunks[2]);
     const int T = nthreads(threads);
     const uint8_t* in = (const uint8_t*)data;
-    const int comp = m.compressor.empty() ? 0 : m.compressor == "gzip" ? 2 : 1;
+    const int comp = m.compressor.empty() ? 0 : m.compressor == "gzip" ? 2 : m.compressor == "blosc" ? 3 : 1;
     const bool ok = write_chunks((size_t)(nc[0] * nc[1] * nc[2]), cn * es, comp, T, [&](size_t t, std::vector<uint8_t>& buf) {
         const int64_t c[3] = {c0[0] + (int64_t)(t % nc[0]), c0[1] + (int64_t)((t / nc[0]) % nc[1]),
                               c0[2] + (int64_t)(t / (nc[0] * nc[1]))};
@@ -557,7 +600,7 @@ extern "C" pk_status pk_zarr_write_region(const char* path, const void* data, co
                 memcpy(buf.data() + (((z - a[2]) * m.chunks[1] + (x - a[1])) * m.chunks[0]) * es,
                        in + (((z - lo[2]) * rx + (x - lo[1])) * ry + (a[0] - lo[0])) * es, (size_t)(b[0] - a[0]) * es);
         return std::string(path) + "/" + chunk_key(m, c);
-    });
+    }, &m);
     if (!ok) return pk_fail(PK_ERR_INVALID, "zarr: writing a chunk failed");
     return PK_OK;
 }

@@ -4,8 +4,9 @@ The reference reads and writes Zarr through its cpp-zarr MEX files (io/cpp-zarr/
 parallelreadzarr.cpp, parallelwritezarr.cpp).  These functions call libpkdecon.so's own reader /
 writer: a MATLAB-ordered [ny nx nz] array is the Zarr array of that shape, chunks are decoded and
 encoded on all host cores, and a region read (``inputBbox``) touches only the chunks that meet it.
-Compressors: none, zlib and gzip; the reference's default (blosc with zstd) is not available in this
-build and raises PkError (PK_ERR_UNSUPPORTED).
+Compressors: none, zlib, gzip and blosc (the reference's default: cname lz4, clevel 5, byte shuffle;
+lz4, zstd or zlib inside).  ``compressor="blosc"`` writes blosc-lz4; "blosc-zstd" and "blosc-zlib"
+choose the codec inside.
 """
 from __future__ import annotations
 
@@ -20,7 +21,8 @@ from .tiff import pinned_empty
 
 _W = {np.dtype(np.uint8): (8, 0), np.dtype(np.uint16): (16, 0), np.dtype(np.uint32): (32, 0),
       np.dtype(np.float32): (32, 1), np.dtype(np.float64): (64, 1)}
-_COMP = {"none": 0, None: 0, "zlib": 1, "gzip": 2}
+_COMP = {"none": 0, None: 0, "zlib": 1, "gzip": 2, "blosc": 3, "blosc-lz4": 3, "blosc-zstd": 4, "blosc-zlib": 5}
+_BLOSC = {3: "lz4", 4: "zstd", 5: "zlib"}
 
 
 def _dtype(bits, is_float):
@@ -77,8 +79,12 @@ def writezarr(data, filepath, blockSize=(500, 500, 500), compressor="zlib", over
     if dimSeparator == "/":                 # the metadata, then the whole array as one region write
         import json
         os.makedirs(str(filepath), exist_ok=True)
+        if comp >= 3:
+            cmeta = {"blocksize": 0, "clevel": 5, "cname": _BLOSC[comp], "id": "blosc", "shuffle": 1}
+        else:
+            cmeta = None if comp == 0 else {"id": "zlib" if comp == 1 else "gzip", "level": 1}
         meta = {"chunks": [int(min(b, n)) for b, n in zip(bs, a.shape)],
-                "compressor": None if comp == 0 else {"id": "zlib" if comp == 1 else "gzip", "level": 1},
+                "compressor": cmeta,
                 "dimension_separator": "/", "dtype": f"<{'f' if isf else 'u'}{bits // 8}", "fill_value": 0,
                 "filters": None, "order": "F", "shape": [int(n) for n in a.shape], "zarr_format": 2}
         with open(os.path.join(str(filepath), ".zarray"), "w") as f:
