@@ -36,7 +36,8 @@ typedef enum {
     PK_ERR_BUSY = 5,         /* server queue full */
     PK_ERR_TIMEOUT = 6,      /* bounded wait expired */
     PK_ERR_CANCELLED = 7,    /* request cancelled */
-    PK_ERR_EMPTY_OTF_MASK = 8 /* omw_backprojector_generation.m:50-52 */
+    PK_ERR_EMPTY_OTF_MASK = 8, /* omw_backprojector_generation.m:50-52 */
+    PK_ERR_INTERNAL = 9       /* an index check of the bounds-checked build (-DPK_CHECK) failed */
 } pk_status;
 
 typedef enum { PK_U16 = 0, PK_F32 = 1, PK_F64 = 2 } pk_dtype;
@@ -95,6 +96,10 @@ PK_API int32_t pk_ctx_tune_read(pk_ctx* ctx, char* buf, int32_t cap);
  * bounded by limit_ns (1e3 .. 1e9), and returns what such a call returns (PK_ERR_TIMEOUT); the
  * context stays usable afterwards. */
 PK_API pk_status pk_selftest_device_wait(pk_ctx* ctx, int64_t limit_ns);
+/* 1 in the bounds-checked build (built with -DPK_CHECK: index checks in the pass kernels that record a
+ * failure and skip the access, the call returning PK_ERR_INTERNAL), else 0 (no counterpart in the
+ * reference; a substitute for compute-sanitizer runs). */
+PK_API int32_t pk_checked_build(void);
 
 /* Output extent for dims/params: the bbox size when has_bbox, else dims. */
 PK_API pk_status pk_output_dims(const int64_t dims[3], const pk_decon_params* p, int64_t out_dims[3]);

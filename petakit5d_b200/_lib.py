@@ -12,14 +12,15 @@ import threading
 
 import numpy as np
 
-LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib", "libpkdecon.so")
+# PK_LIB names another build of the library (the bounds-checked lib/libpkdecon_check.so, for one)
+LIB_PATH = os.environ.get("PK_LIB") or os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib", "libpkdecon.so")
 
 PK_OK, PK_ERR_INVALID, PK_ERR_UNSUPPORTED, PK_ERR_CUDA, PK_ERR_NOMEM, PK_ERR_BUSY, PK_ERR_TIMEOUT, \
-    PK_ERR_CANCELLED, PK_ERR_EMPTY_OTF_MASK = range(9)
+    PK_ERR_CANCELLED, PK_ERR_EMPTY_OTF_MASK, PK_ERR_INTERNAL = range(10)
 PK_U16, PK_F32, PK_F64 = 0, 1, 2
 
 STATUS_NAMES = {0: "ok", 1: "invalid", 2: "unsupported", 3: "cuda", 4: "nomem", 5: "busy", 6: "timeout",
-                7: "cancelled", 8: "emptyOTFMask"}
+                7: "cancelled", 8: "emptyOTFMask", 9: "internal"}
 
 
 class PkError(RuntimeError):
@@ -63,6 +64,7 @@ _SIGS = {
     "pk_ctx_profile": (C.c_int, [P, C.c_int32]),
     "pk_ctx_profile_read": (C.c_int32, [P, C.c_char_p, C.c_int32]),
     "pk_selftest_device_wait": (C.c_int, [P, C.c_int64]),
+    "pk_checked_build": (C.c_int32, []),
     "pk_ctx_tune_read": (C.c_int32, [P, C.c_char_p, C.c_int32]),
     "pk_output_dims": (C.c_int, [I64x3, C.POINTER(DeconParams), I64x3]),
     "pk_decon_lucy": (C.c_int, [P, P, C.c_int, I64x3, P, I64x3, C.c_int32, C.POINTER(DeconParams), P,

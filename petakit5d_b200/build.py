@@ -2,7 +2,10 @@
 
 ``python -m petakit5d_b200.build`` compiles every ``csrc/*.cu`` into ``petakit5d_b200/lib/libpkdecon.so``
 (``-gencode arch=compute_100a,code=sm_100a -lineinfo -O3``).  Objects are cached in ``_build/`` by
-source hash so a rebuild only recompiles what changed.
+source hash so a rebuild only recompiles what changed.  ``--check`` builds the bounds-checked library
+``lib/libpkdecon_check.so`` (``-DPK_CHECK``: the pass kernels test the indices of their global-memory
+accesses and their shared-memory layout, record a failure and skip the access; the call returns
+PK_ERR_INTERNAL); load it with ``PK_LIB=.../libpkdecon_check.so``.
 """
 from __future__ import annotations
 
@@ -18,6 +21,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libpkdecon.so")
+CHECK_LIB = os.path.join(LIBDIR, "libpkdecon_check.so")
 OBJDIR = os.path.join(ROOT, "_build")
 
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-gencode", "arch=compute_100a,code=sm_100a",
@@ -46,11 +50,12 @@ def _digest(path, extra):
     return h.hexdigest()[:16]
 
 
-def build(verbose=False, extra_flags=()):
+def build(verbose=False, extra_flags=(), checked=False):
     nvcc = _nvcc()
     os.makedirs(OBJDIR, exist_ok=True)
     os.makedirs(LIBDIR, exist_ok=True)
-    flags = NVCC_FLAGS + list(extra_flags)
+    flags = NVCC_FLAGS + list(extra_flags) + (["-DPK_CHECK"] if checked else [])
+    lib_path = CHECK_LIB if checked else LIB
     srcs = sorted(f for f in os.listdir(CSRC) if f.endswith(".cu"))
 
     def compile_one(src):
@@ -69,14 +74,14 @@ def build(verbose=False, extra_flags=()):
 
     with ThreadPoolExecutor(max_workers=min(8, len(srcs))) as ex:
         objs = list(ex.map(compile_one, srcs))
-    tmp = LIB + ".tmp"
+    tmp = lib_path + ".tmp"
     cmd = [nvcc, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-cudart", "static", "-o", tmp, *objs, "-lz"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
-    os.replace(tmp, LIB)
-    return LIB
+    os.replace(tmp, lib_path)
+    return lib_path
 
 
 if __name__ == "__main__":
-    print(build(verbose="-v" in sys.argv))
+    print(build(verbose="-v" in sys.argv, checked="--check" in sys.argv))

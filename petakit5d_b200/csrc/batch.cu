@@ -42,6 +42,7 @@ extern "C" pk_status pk_batch_decon(pk_ctx* ctx, int32_t method, int32_t n, cons
         params = &def;
     }
     if (n == 0) return PK_OK;
+    PkRange range("pk_batch_decon");
     std::lock_guard<std::recursive_mutex> lk(ctx->mu);
     cudaSetDevice(ctx->device);
     cudaStream_t st = ctx->stream;

@@ -760,6 +760,7 @@ pk_status pk_decon_run(pk_ctx* ctx, int method, const void* d_in, pk_dtype in_ty
                        const float* psf_f, const int64_t psf_f_dims[3], const float* psf_b,
                        const int64_t psf_b_dims[3], int numit, const pk_decon_params* p, void* d_out,
                        cudaStream_t st, HostStreamIO* io, const DebugHook* dbg) {
+    PkRange range(method == 1 ? "pk_decon omw" : "pk_decon rl");
     pk_status s;
     if ((s = pk_check_params(dims, p)) != PK_OK) return s;
     if (numit < 0) return pk_fail(PK_ERR_INVALID, "NUMIT must be non-negative");

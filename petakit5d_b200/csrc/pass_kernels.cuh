@@ -89,6 +89,8 @@ __device__ __forceinline__ void out_store(const VolDesc& d, float J, long long v
         const long long oy = d.bb1[0] - d.bb0[0] + 1, ox = d.bb1[1] - d.bb0[1] + 1;
         oi = (long long)(y - d.bb0[0]) + oy * ((long long)(x - d.bb0[1]) + ox * (long long)(z - d.bb0[2]));
     }
+    if (!PK_IN(d, oi >= 0 && oi < (long long)(d.bb1[0] - d.bb0[0] + 1) * (d.bb1[1] - d.bb0[1] + 1) * (d.bb1[2] - d.bb0[2] + 1), 20))
+        return;
     if (d.save16) ((uint16_t*)d.out)[oi] = (uint16_t)u16_of(J);
     else ((float*)d.out)[oi] = J;
 }
@@ -322,6 +324,10 @@ __global__ void __launch_bounds__(PK_THREADS, 3) k_y(const VolDesc* __restrict__
     const long long row0 = (long long)lb * L;
     const int Lc = (int)min((long long)L, d.nrows - row0);
     const bool spec_in = mode_from_spec(mode), spec_out = mode_to_spec(mode);
+    if (!PK_SMEM_OK(d, sizeof(float2) * (tw_slots(M) + (odd ? 0 : M + 1) + padded_size(L * M) + L +
+                                         (size_t)y_aux_arrays(mode) * L * M), 1) ||
+        !PK_IN(d, row0 < d.nrows && Lc >= 1, 2))
+        return;   // uniform over the CTA, before any barrier
 
     // ---- issue the asynchronous loads: group A = spectrum rows, group B = per-voxel inputs
     if (spec_in) {
@@ -331,9 +337,10 @@ __global__ void __launch_bounds__(PK_THREADS, 3) k_y(const VolDesc* __restrict__
             // Py = M + 1: bins 0..M-1 of each row into the tile, bin M (Nyquist) aside
             for (int idx = tid; idx < Lc * M; idx += NT) {
                 const int l = idx / M, k = idx - l * M;
-                cp8(&buf[pad(idx)], S0 + l * Pp + k);
+                if (PK_IN(d, k < Pp, 11)) cp8(&buf[pad(idx)], S0 + l * Pp + k);
             }
-            for (int l = tid; l < Lc; l += NT) cp8(&nyq[l], S0 + l * Pp + M);
+            for (int l = tid; l < Lc; l += NT)
+                if (PK_IN(d, M < Pp, 11)) cp8(&nyq[l], S0 + l * Pp + M);
         } else {
             const int nin = Lc * Py;
             for (int idx = tid; idx < nin; idx += NT) {
@@ -381,6 +388,7 @@ __global__ void __launch_bounds__(PK_THREADS, 3) k_y(const VolDesc* __restrict__
         for (int idx = 2 * tid; idx < nvox; idx += 2 * NT) {
             const int l = idx / M, k = idx - l * M;
             const long long vi = v0 + (long long)l * ny + 2 * k;
+            if (!PK_IN(d, vi + 3 < d.nrows * (long long)ny, 12)) continue;
             cp16(&aux0[idx], pa0 + vi);
             if (pa1) cp16(&aux1[idx], pa1 + vi);
         }
@@ -539,6 +547,7 @@ __global__ void __launch_bounds__(PK_THREADS, 3) k_y(const VolDesc* __restrict__
                                 const int e = j + r * MS;
                                 const long long vi = row * (long long)ny + 2 * e;
                                 const float2 val = v[i][r];
+                                if (!PK_IN(d, vi + 1 < d.nrows * (long long)ny, 13)) continue;
                                 if constexpr (kPost) {
                                     if (vec_out) {
                                         if (s16) {
@@ -634,7 +643,8 @@ __global__ void __launch_bounds__(PK_THREADS, 3) k_y(const VolDesc* __restrict__
                 for (int idx = 2 * tid; idx < Lc * M; idx += 2 * NT) {
                     const int l = idx / M, k = idx - l * M;
                     const float2 x0 = split(l, k), x1 = split(l, k + 1);
-                    *reinterpret_cast<float4*>(S0 + l * Pp + k) = make_float4(x0.x, x0.y, x1.x, x1.y);
+                    if (PK_IN(d, k + 1 < Pp, 14))
+                        *reinterpret_cast<float4*>(S0 + l * Pp + k) = make_float4(x0.x, x0.y, x1.x, x1.y);
                 }
             } else {
                 for (int idx = tid; idx < Lc * M; idx += NT) {
@@ -704,6 +714,10 @@ struct XZTile {
     float2* p;             // S + tile origin
     long long es;          // element stride along the transformed axis
     int ncol;              // valid columns of the tile
+#ifdef PK_CHECK
+    long long lim;         // elements of S from p on (the checked build tests every access against it)
+    int* chk;
+#endif
     float sc;              // output scale (XZ_FWD_SCALE), else 1
     const float2* gtw;     // twiddle table (global)
     const float2* gh;      // OTF at the tile origin (XZ_CONV), else null
@@ -711,9 +725,15 @@ struct XZTile {
     float2* h;             // shared OTF tile
     int T, n, ntw, conj;
     __device__ __forceinline__ float2 ld(int l, int e) const {
+#ifdef PK_CHECK
+        if (l < ncol && !pk_check_in(chk, e * es + l < lim, 30)) return make_float2(0.f, 0.f);
+#endif
         return l < ncol ? p[e * es + l] : make_float2(0.f, 0.f);
     }
     __device__ __forceinline__ void st(int l, int e, float2 v) const {
+#ifdef PK_CHECK
+        if (l < ncol && !pk_check_in(chk, e * es + l < lim, 31)) return;
+#endif
         if (l < ncol) p[e * es + l] = make_float2(v.x * sc, v.y * sc);
     }
     __device__ __forceinline__ float2 otf(int l, int e) const {
@@ -794,8 +814,15 @@ __global__ void __launch_bounds__(PK_THREADS, xz_min_blocks(P)) k_xz(const VolDe
         // first stage loads from HBM into registers, last stage stores from registers to HBM; the
         // OTF multiply runs inside the last forward stage
         constexpr int TT = plan_cols_xz(kPlans[P].n, TP);
+#ifdef PK_CHECK
+        if (!PK_SMEM_OK(d, sizeof(float2) * (tw_slots(n) + padded_size2(TT * n) + (conv ? TT * n : 0)), 3)) return;
+        const XZTile g{d.S + base + k0, es, Py - k0, d.Pp * d.nrows - (base + k0), d.chk,
+                       mode == XZ_FWD_SCALE ? d.xz_scale : 1.f, A.tw, conv ? d.otf + base + k0 : nullptr, tw, hbuf, TT,
+                       kPlans[P].n, plan_tw_size(P), d.conj};
+#else
         const XZTile g{d.S + base + k0, es, Py - k0, mode == XZ_FWD_SCALE ? d.xz_scale : 1.f, A.tw,
                        conv ? d.otf + base + k0 : nullptr, tw, hbuf, TT, kPlans[P].n, plan_tw_size(P), d.conj};
+#endif
         if (mode == XZ_INV) fft_g<P, TT, true, true, false, true>(buf, tw, g, tid);
         else if (!conv) fft_g<P, TT, true, false, false, true>(buf, tw, g, tid);
         else if constexpr (same_end_radix(P)) {

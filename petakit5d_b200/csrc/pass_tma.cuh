@@ -223,6 +223,7 @@ __global__ void __launch_bounds__(NTH + 32, xzt_min_blocks(P, TC, NBUF, MODE == 
     const int tid = threadIdx.x;
     const int total = prefix[nvol];
     if ((int)blockIdx.x >= total) return;
+    if (!PK_SMEM_OK(descs[0], Lay::bytes(CONV), 6)) return;   // uniform over the CTA, before any barrier
 
     // tile g -> volume and TMA coordinates of its first box (box r adds r*ROWS on the line's axis)
     auto locate = [&](int g, int& vol, int& c0, int& c1, int& c2) {

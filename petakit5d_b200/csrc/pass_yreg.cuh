@@ -78,6 +78,8 @@ __global__ void __launch_bounds__(PK_THREADS, y_naux(MODE) == 2 ? 2 : 3)
     const long long row = row0 + l;
     const int ny = d.ny;
     const long long v0 = row0 * (long long)ny;
+    if (!PK_SMEM_OK(d, yreg_smem_bytes(MODE), 4) || !PK_IN(d, row0 < d.nrows && Lc >= 1 && d.Pp >= M + 1, 5))
+        return;   // uniform over the CTA, before any barrier
 
     // ---- the tile's per-voxel inputs: one bulk copy per array (contiguous rows row0 .. row0+Lc-1)
     const void* src0 = nullptr;
@@ -93,10 +95,13 @@ __global__ void __launch_bounds__(PK_THREADS, y_naux(MODE) == 2 ? 2 : 3)
     if (tid == 0 && NAUX > 0) {
         pktma::mbar_init(bar, 1);
         pktma::fence_mbar_init();
-        const uint32_t bytes = (uint32_t)Lc * (uint32_t)ny * esz;
+        uint32_t bytes = (uint32_t)Lc * (uint32_t)ny * esz;
+        if (!PK_IN(d, (row0 + Lc) * (long long)ny <= d.nrows * (long long)ny && bytes <= LL * M * 8u, 15)) bytes = 0;
         pktma::mbar_expect_tx(bar, src1 ? 2 * bytes : bytes);
-        pktma::bulk_load(aux0, (const char*)src0 + (size_t)v0 * esz, bytes, bar);
-        if (src1) pktma::bulk_load(aux1, (const char*)src1 + (size_t)v0 * esz, bytes, bar);
+        if (bytes) {
+            pktma::bulk_load(aux0, (const char*)src0 + (size_t)v0 * esz, bytes, bar);
+            if (src1) pktma::bulk_load(aux1, (const char*)src1 + (size_t)v0 * esz, bytes, bar);
+        }
     }
 
     float2 v[1][R];

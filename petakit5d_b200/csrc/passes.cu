@@ -445,6 +445,7 @@ int choose_variant(pk_ctx* ctx, const PkProgram& prog, const PkStep& s, int idx,
         dt.blocksZ = dt.nx * ((dt.Py + dt.Tz - 1) / dt.Tz);
     }
     std::vector<float> ms;
+    PkRange range("pk autotune");
     int best = time_candidates(ctx, s, dt, idx, cands, st, ms);
     if (best == -2) return fallback;
     ctx->tune[key] = best;
@@ -786,6 +787,7 @@ void pk_program_add(PkProgram& prog, int kind, int mode, const std::vector<VolDe
 }
 
 pk_status pk_program_upload(pk_ctx* ctx, PkProgram& prog, cudaStream_t st) {
+    for (VolDesc& d : prog.descs) d.chk = ctx && ctx->d_err ? ctx->d_err + 1 : nullptr;
     assign_tma(ctx, prog, st);
     size_t dbytes, moff, need;
     blob_layout(prog, &dbytes, &moff, &need);
@@ -864,6 +866,7 @@ static pk_status launch_steps(pk_ctx* ctx, const PkProgram& prog, cudaStream_t s
         const VolDesc* dd = prog.d_desc + s.desc_off;
         const int* dp = prog.d_prefix + s.prefix_off;
         if (s.grid == 0) continue;
+        PkRange range(pk_step_name(s));
         pk_ctx::ProfRec rec;
         if (ctx && ctx->prof_on) {
             auto take = [&]() {
@@ -992,10 +995,25 @@ pk_status pk_check_device_waits(pk_ctx* ctx) {
         return pk_fail(PK_ERR_TIMEOUT, "a bounded wait on the device ran out in an earlier call of this context "
                                        "(its results are not valid)");
     }
+    if (ctx && ctx->h_err && *(volatile int*)(ctx->h_err + 1) != 0) {
+        const int code = *(volatile int*)(ctx->h_err + 1);
+        *(volatile int*)(ctx->h_err + 1) = 0;
+        return pk_fail(PK_ERR_INTERNAL, "index check " + std::to_string(code) +
+                                            " of the bounds-checked build failed (the access was skipped)");
+    }
     return PK_OK;
 }
 
+extern "C" int32_t pk_checked_build(void) {
+#ifdef PK_CHECK
+    return 1;
+#else
+    return 0;
+#endif
+}
+
 pk_status pk_program_launch(pk_ctx* ctx, PkProgram& prog, cudaStream_t st) {
+    PkRange range("pk program launch");
     {
         const pk_status w = pk_check_device_waits(ctx);
         if (w != PK_OK) return w;

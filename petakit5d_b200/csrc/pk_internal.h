@@ -22,6 +22,17 @@
 
 #include "../../include/pkdecon.h"
 
+#include <nvtx3/nvToolsExt.h>
+
+// NVTX range over a scope (header-only NVTX 3: inert unless a profiler attaches): API calls,
+// program launches and each pass launch are named, so a timeline shows where the host time goes.
+struct PkRange {
+    explicit PkRange(const char* name) { nvtxRangePushA(name); }
+    ~PkRange() { nvtxRangePop(); }
+    PkRange(const PkRange&) = delete;
+    PkRange& operator=(const PkRange&) = delete;
+};
+
 #define PK_MAXST 16   // max radix stages per axis
 #ifndef PK_PPT
 #define PK_PPT 16     // max complex points per thread per stage
@@ -92,7 +103,29 @@ struct VolDesc {
     int crop;                        // crop box smaller than the volume
     int need_xz;                     // post needs x/z of a voxel (crop or border erosion)
     int tiles_small;                 // passes use the 1024-point-tile kernels (small volumes)
+    int* chk;                        // bounds-checked build (-DPK_CHECK): where a failed index check is recorded
 };
+
+// Bounds-checked build.  With -DPK_CHECK the pass kernels test the indices of their global-memory
+// accesses (and their shared-memory layout against the launch's dynamic shared memory); a failed
+// test records its check code in the context's status word (VolDesc::chk) and skips the access,
+// and the call returns PK_ERR_INTERNAL.  Without it the tests compile to nothing.
+#ifdef PK_CHECK
+#define PK_IN(d, cond, code) pk_check_in((d).chk, (cond), (code))
+__device__ __forceinline__ bool pk_check_in(int* chk, bool ok, int code) {
+    if (!ok && chk) *(volatile int*)chk = code;
+    return ok;
+}
+__device__ __forceinline__ unsigned pk_dyn_smem() {
+    unsigned v;
+    asm volatile("mov.u32 %0, %%dynamic_smem_size;" : "=r"(v));
+    return v;
+}
+#define PK_SMEM_OK(d, need, code) pk_check_in((d).chk, pk_dyn_smem() >= (unsigned)(need), (code))
+#else
+#define PK_IN(d, cond, code) true
+#define PK_SMEM_OK(d, need, code) true
+#endif
 
 // TMA tensor maps of one descriptor of an x or z step run by the persistent TMA kernel: the
 // spectrum S as a 3-D tensor {2 Py floats, nx, nz} (row pitch Pp) with the step's column-tile box,
