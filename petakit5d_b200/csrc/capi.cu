@@ -102,7 +102,7 @@ pk_ctx* pk_ctx_create(int device) {
         delete ctx;
         return nullptr;
     }
-    *(volatile int*)ctx->h_err = 0;
+    for (int i = 0; i < 16; i++) ((volatile int*)ctx->h_err)[i] = 0;   // page-locked memory is not zeroed
     return ctx;
 }
 
