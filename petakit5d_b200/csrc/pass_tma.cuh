@@ -43,14 +43,14 @@ struct XztLayout {
     static constexpr size_t BUF = ((size_t)PTS * 8 + 1023) & ~(size_t)1023;
     static constexpr size_t TW = ((size_t)(plan_tw_size(P) > 0 ? plan_tw_size(P) : 1) * 8 + 15) & ~(size_t)15;
     static constexpr size_t bytes(bool conv) { return 1024 + NBUF * BUF + (conv ? BUF : 0) + TW + 64; }
-    static_assert(1024 + NBUF * BUF + BUF + TW + 64 <= 227 * 1024 || NBUF == 1, "tile buffers exceed shared memory");
+    static_assert(1024 + NBUF * BUF + TW + 64 <= 227 * 1024, "tile buffers exceed shared memory");
 };
 
 // CTAs per SM a variant is compiled for (register budget): 3 for 4096-point tiles, 2 for the
 // two-buffer convolution (three tile-sized buffers) or one 8192-point buffer, 1 for two 8192-point buffers
 constexpr int xzt_min_blocks(int P, int TC, int NBUF, bool conv) {
-    return (TC > 0 ? TC : plan_cols_xz(kPlans[P].n)) * kPlans[P].n > 4096 ? (NBUF == 2 ? 1 : 2)
-                                                                           : ((conv && NBUF == 2) ? 2 : 3);
+    return (TC > 0 ? TC : plan_cols_xz(kPlans[P].n)) * kPlans[P].n > 4096 ? (NBUF >= 2 ? 1 : 2)
+                                                                           : ((conv && NBUF >= 2) ? 2 : 3);
 }
 
 // The TMA kernels run NTH compute threads (NTH / 32 warps) and one producer warp after them that
@@ -196,13 +196,13 @@ __device__ __forceinline__ void run_dense(float2* buf, const float2* tw, int tid
 //     for XZ_CONV, once compute has used the previous OTF tile (otf_empty), load tile it's OTF tile;
 //   compute (warps 0-7): wait full[s], transform in place (multiply by the OTF tile between the
 //     transforms, then release the OTF buffer), then release buffer s (empty[s]).
-// With NBUF = 2 the next tile's load is in flight while the current one is transformed.  Every wait
+// With NBUF = 2 (3) the next one (two) tiles' loads are in flight while the current one is transformed.  Every wait
 // is bounded; a wait that runs out is recorded in *err and the role that saw it stops.
 template <int P, int AXIS, int MODE, int TC = 0, int NBUF = 2, int NTH = PK_THREADS>
 __global__ void __launch_bounds__(NTH + 32, xzt_min_blocks(P, TC, NBUF, MODE == XZ_CONV))
     k_xzt(const VolDesc* __restrict__ descs, const XZMaps* __restrict__ maps, const int* __restrict__ prefix, int nvol,
           int* err) {
-    static_assert(NBUF == 1 || NBUF == 2, "one or two tile buffers");
+    static_assert(NBUF >= 1 && NBUF <= 3, "one to three tile buffers (the barrier area holds eight barriers)");
     using Lay = XztLayout<P, TC, NBUF>;
     constexpr int N = Lay::N, T = Lay::T, PTS = Lay::PTS, ROWS = Lay::ROWS, NBOX = Lay::NBOX;
     constexpr int NST = kPlans[P].nst;
@@ -211,15 +211,16 @@ __global__ void __launch_bounds__(NTH + 32, xzt_min_blocks(P, TC, NBUF, MODE == 
     constexpr int NT = NTH;
     extern __shared__ unsigned char smraw[];
     unsigned char* sm = smraw + ((1024 - (pktma::smem_u32(smraw) & 1023)) & 1023);
-    float2* bufs[2] = {(float2*)sm, (float2*)(sm + (NBUF - 1) * Lay::BUF)};
+    float2* bufs[NBUF];
+    for (int i = 0; i < NBUF; i++) bufs[i] = (float2*)(sm + i * Lay::BUF);
     float2* hb = (float2*)(sm + NBUF * Lay::BUF);
     float2* tw = (float2*)(sm + NBUF * Lay::BUF + (CONV ? Lay::BUF : 0));
     // barriers: full[0..1] (tile landed), empty[0..1] (compute done with the buffer), otf_full, otf_empty
     uint64_t* bars = (uint64_t*)((unsigned char*)tw + Lay::TW);
     uint64_t* full = bars;
-    uint64_t* empty = bars + 2;
-    uint64_t* otf_full = bars + 4;
-    uint64_t* otf_empty = bars + 5;
+    uint64_t* empty = bars + NBUF;
+    uint64_t* otf_full = bars + 2 * NBUF;
+    uint64_t* otf_empty = bars + 2 * NBUF + 1;
     const int tid = threadIdx.x;
     const int total = prefix[nvol];
     if ((int)blockIdx.x >= total) return;
@@ -253,7 +254,7 @@ __global__ void __launch_bounds__(NTH + 32, xzt_min_blocks(P, TC, NBUF, MODE == 
     };
 
     if (tid == 0) {
-        for (int i = 0; i < 6; i++) pktma::mbar_init(&bars[i], 1);
+        for (int i = 0; i < 2 * NBUF + 2; i++) pktma::mbar_init(&bars[i], 1);
         pktma::fence_mbar_init();
     }
     // the plan's twiddles, once per CTA (every volume of the launch has this plan)
@@ -271,9 +272,9 @@ __global__ void __launch_bounds__(NTH + 32, xzt_min_blocks(P, TC, NBUF, MODE == 
             if (CONV) pktma::tmap_acquire(&maps[v].otf);
         }
         int it = 0;
-        int pv[2] = {0, 0}, pc[2][3] = {{0, 0, 0}, {0, 0, 0}};   // volume and coordinates of each buffer's tile
+        int pv[NBUF], pc[NBUF][3];   // volume and coordinates of each buffer's tile
         for (int g = blockIdx.x; g < total; g += gridDim.x, it++) {
-            const int s = NBUF == 2 ? (it & 1) : 0;
+            const int s = it % NBUF;
             int vol, c0, c1, c2;
             locate(g, vol, c0, c1, c2);
             if (it >= NBUF) {
@@ -300,7 +301,7 @@ __global__ void __launch_bounds__(NTH + 32, xzt_min_blocks(P, TC, NBUF, MODE == 
         // the last tiles: store each once compute has released its buffer
         const int n_it = it;
         for (int k = n_it - NBUF < 0 ? 0 : n_it - NBUF; k < n_it; k++) {
-            const int s = NBUF == 2 ? (k & 1) : 0;
+            const int s = k % NBUF;
             if (!pktma::mbar_wait(&empty[s], (uint32_t)((k / NBUF) & 1))) {
                 pktma::report_wait_failure(err, 1);
                 break;
@@ -314,7 +315,7 @@ __global__ void __launch_bounds__(NTH + 32, xzt_min_blocks(P, TC, NBUF, MODE == 
     // ---------------- compute (warps 0 .. NTH/32 - 1)
     int it = 0;
     for (int g = blockIdx.x; g < total; g += gridDim.x, it++) {
-        const int s = NBUF == 2 ? (it & 1) : 0;
+        const int s = it % NBUF;
         float2* cur = bufs[s];
         const int vol = find_vol(prefix, nvol, g);
         bool ok = pktma::mbar_wait(&full[s], (uint32_t)((it / NBUF) & 1));
@@ -421,17 +422,17 @@ struct RegisterTma {
             register_tma_one<P, TMA_Z_CONV, 0, 2, XZ_CONV>(t);
             if constexpr (kPlans[P].n == 512) {
                 // 8-column tiles (64-byte rows, 3 CTAs per SM) against 16-column tiles (128-byte rows,
-                // two buffers, one CTA per SM) with 8 or 16 compute warps
+                // one CTA per SM, 16 compute warps) with two or three buffers
                 register_tma_one<P, TMA_X_FWD, 1, 1, XZ_FWD, 16, 2, 512>(t);
                 register_tma_one<P, TMA_X_INV, 1, 1, XZ_INV, 16, 2, 512>(t);
-                register_tma_one<P, TMA_X_FWD, 2, 1, XZ_FWD, 16, 2>(t);
-                register_tma_one<P, TMA_X_INV, 2, 1, XZ_INV, 16, 2>(t);
+                register_tma_one<P, TMA_X_FWD, 2, 1, XZ_FWD, 16, 3, 512>(t);
+                register_tma_one<P, TMA_X_INV, 2, 1, XZ_INV, 16, 3, 512>(t);
             }
             if constexpr (kPlans[P].n == 256) {
-                // the convolution with 32-column tiles (256-byte rows, one CTA per SM) and 16 or 8
-                // compute warps
+                // the convolution with 32-column tiles (256-byte rows, two buffers, 16 compute warps) and
+                // with 24-column tiles (three buffers, 12 compute warps), one CTA per SM
                 register_tma_one<P, TMA_Z_CONV, 1, 2, XZ_CONV, 32, 2, 512>(t);
-                register_tma_one<P, TMA_Z_CONV, 2, 2, XZ_CONV, 32, 2>(t);
+                register_tma_one<P, TMA_Z_CONV, 2, 2, XZ_CONV, 24, 3, 384>(t);
             }
         }
         RegisterTma<P + 1, HI>::fill(t);

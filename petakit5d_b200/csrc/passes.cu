@@ -187,8 +187,15 @@ bool encode_spec_map(CUtensorMap* m, const void* base, const VolDesc& d, int axi
     const cuuint64_t strides[2] = {(cuuint64_t)d.Pp * 8, (cuuint64_t)d.Pp * 8 * (cuuint64_t)d.nx};
     const cuuint32_t box[3] = {(cuuint32_t)(2 * T), (cuuint32_t)(axis == 1 ? rows : 1), (cuuint32_t)(axis == 2 ? rows : 1)};
     const cuuint32_t es[3] = {1, 1, 1};
+    // L2 promotion of the TMA's DRAM fetches (PK_TMA_L2 = 0 none, 1 64 B, 2 128 B, 3 256 B: diagnostics)
+    static const CUtensorMapL2promotion promo = [] {
+        const char* e = getenv("PK_TMA_L2");
+        const int v = e ? atoi(e) : 3;
+        return v == 0 ? CU_TENSOR_MAP_L2_PROMOTION_NONE : v == 1 ? CU_TENSOR_MAP_L2_PROMOTION_L2_64B
+               : v == 2 ? CU_TENSOR_MAP_L2_PROMOTION_L2_128B : CU_TENSOR_MAP_L2_PROMOTION_L2_256B;
+    }();
     return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<void*>(base), dims, strides, box, es,
-               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, promo,
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
@@ -262,8 +269,8 @@ void tf_store(const std::string& key, int v, float ms) {
 }
 
 const char* variant_name(int idx, int v) {
-    static const char* names[] = {"register-IO", "tma", "tma-16col-16warps", "tma-16col-8warps", "tma-32col-16warps",
-                                  "tma-32col-8warps"};
+    static const char* names[] = {"register-IO", "tma", "tma-16col-16warps", "tma-16col-16warps-3buf",
+                                  "tma-32col-16warps", "tma-24col-12warps-3buf"};
     if (v < 0) return names[0];
     if (v == 0) return names[1];
     if (idx == pkpass::TMA_Z_CONV) return v == 1 ? names[4] : names[5];
