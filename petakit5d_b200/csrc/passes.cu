@@ -883,6 +883,13 @@ static pk_status launch_steps(pk_ctx* ctx, const PkProgram& prog, cudaStream_t s
                 return e;
             };
             rec.kind = pk_step_name(s);
+            static const bool detail = getenv("PK_PROF_DETAIL") && getenv("PK_PROF_DETAIL")[0] == '1';
+            if (detail) {   // diagnostics: the transform length and the kernel family in the kind
+                const int pl = s.plan % kNumPlans;
+                rec.kind += "@" + std::to_string(kPlans[pl].n) +
+                            (s.tma >= 0 ? ":tma" : s.yreg ? ":yreg" : s.kind == PK_STEP_Y ? ":rolled" : ":rio") +
+                            (s.plan >= kNumPlans ? "-1k" : "");
+            }
             rec.bytes = pk_step_bytes(s, prog.descs.data() + s.desc_off);
             rec.a = take();
             rec.b = take();
