@@ -85,7 +85,7 @@ PK_API int32_t pk_ctx_profile_read(pk_ctx* ctx, char* buf, int32_t cap);
  * each kernel variant that can run it (the register-IO kernel and the TMA kernels' tile widths /
  * buffer counts) is timed on scratch buffers of that geometry and the fastest is kept for every
  * later pass of that plan and class, batched and served ones included; choices persist in an
- * on-disk cache (PK_TUNE_FILE, else ~/.cache/pkdecon/tune-v3.txt; PK_TUNE=0 disables the timing).
+ * on-disk cache (PK_TUNE_FILE, else ~/.cache/pkdecon/tune-v4.txt; PK_TUNE=0 disables the timing).
  * This writes the context's decisions as a JSON list and returns its length (truncated to cap-1). */
 PK_API int32_t pk_ctx_tune_read(pk_ctx* ctx, char* buf, int32_t cap);
 

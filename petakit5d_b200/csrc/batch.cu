@@ -5,6 +5,8 @@
 // wave w computes, wave w+1 uploads and wave w-1 downloads on separate streams (host chunks
 // should be in pinned memory for the copies to overlap).
 #include <algorithm>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -127,6 +129,9 @@ extern "C" pk_status pk_batch_decon(pk_ctx* ctx, int32_t method, int32_t n, cons
         for (int i : waves[w]) b += plans[i].work_b;
         slot_b[w % 2] = std::max(slot_b[w % 2], b);
     }
+    if (getenv("PK_BATCH_LOG") && getenv("PK_BATCH_LOG")[0] == '1')
+        fprintf(stderr, "pk_batch_decon: %d chunks, %zu waves, budget %.1f GB of %.1f GB free, slots %.1f / %.1f GB\n", n,
+                waves.size(), budget / 1e9, freeb / 1e9, slot_b[0] / 1e9, slot_b[1] / 1e9);
     void* arena[2] = {nullptr, nullptr};
     for (int k = 0; k < 2 && k < (int)waves.size(); k++)
         if ((s = pk_scratch(ctx, 20 + k, slot_b[k], &arena[k])) != PK_OK) return s;

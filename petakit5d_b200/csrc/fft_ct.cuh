@@ -11,15 +11,19 @@ namespace pkfft {
 // direction's sign in s), y_q = t1 + i t2 and y_{R-q} = t1 - i t2 for
 //   t1 = v_0 + sum_m a_m c_{qm},  t2 = sum_m b_m s_{qm}
 // which takes about a quarter of the multiply-adds of sum_m v_m W^{qm}.  W_R^e = tw[e * wstep] (forward
-// roots; the inverse negates their imaginary parts).
+// roots; the inverse negates their imaginary parts).  Only the H roots W_R^1 .. W_R^H are read: the
+// table's W_R^{R-e} is the conjugate of its W_R^e, bit for bit (both come from the same angle), so
+// c_{R-e} = c_e and s_{R-e} = -s_e select, at compile time, among H loads instead of H^2.
 template <int R, bool INV>
 __device__ __forceinline__ void bf_direct(float2* v, const float2* __restrict__ tw, int wstep) {
     static_assert(R % 2 == 1, "symmetric direct DFT needs an odd radix");
     constexpr int H = (R - 1) / 2;
-    float2 a[H + 1], b[H + 1];
+    float2 a[H + 1], b[H + 1], w[H + 1];
+    w[0] = make_float2(1.f, 0.f);   // W_R^0, as the table holds it (q m = 0 mod R for a composite R)
     float2 y0 = v[0];
 #pragma unroll
     for (int m = 1; m <= H; m++) {
+        w[m] = tw[m * wstep];   // roots stay in shared memory until here
         a[m] = make_float2(v[m].x + v[R - m].x, v[m].y + v[R - m].y);
         b[m] = make_float2(v[m].x - v[R - m].x, v[m].y - v[R - m].y);
         y0.x += a[m].x;
@@ -32,10 +36,12 @@ __device__ __forceinline__ void bf_direct(float2* v, const float2* __restrict__ 
         float2 t1 = v[0], t2 = make_float2(0.f, 0.f);
 #pragma unroll
         for (int m = 1; m <= H; m++) {
-            const float2 ww = tw[((q * m) % R) * wstep];   // roots stay in shared memory, not registers
-            const float sw = INV ? -ww.y : ww.y;
-            t1.x += a[m].x * ww.x;
-            t1.y += a[m].y * ww.x;
+            const int e = (q * m) % R;
+            const float c = e <= H ? w[e].x : w[R - e].x;
+            const float sn = e <= H ? w[e].y : -w[R - e].y;
+            const float sw = INV ? -sn : sn;
+            t1.x += a[m].x * c;
+            t1.y += a[m].y * c;
             t2.x += b[m].x * sw;
             t2.y += b[m].y * sw;
         }

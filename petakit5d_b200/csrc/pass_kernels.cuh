@@ -48,9 +48,41 @@ __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_grou
 template <int N>
 __device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
+// The descriptor fields the per-voxel helpers below read, copied into registers once per CTA.  Read
+// through the descriptor itself, every store to one of the volume's arrays would make the compiler
+// load them again from memory (the store might alias the descriptor) before the next voxel.
+struct VoxFields {
+    int ny, nx, nz;
+    long long nrows;
+    int rdims[3];
+    const void* raw;
+    int raw_type, bg16;
+    float bg_f;
+    float *I, *Jn, *Yb, *J4, *J2n, *dst;
+    uint8_t* mask8;
+    int write_mask, rl_first, mask_mode, erosion, scale_mode, save16, crop, need_xz;
+    float damp, scale, offset;
+    void* out;
+    int bb0[3], bb1[3];
+    int* chk;
+    __device__ __forceinline__ explicit VoxFields(const VolDesc& d)
+        : ny(d.ny), nx(d.nx), nz(d.nz), nrows(d.nrows), raw(d.raw), raw_type(d.raw_type), bg16(d.bg16),
+          bg_f(d.bg_f), I(d.I), Jn(d.Jn), Yb(d.Yb), J4(d.J4), J2n(d.J2n), dst(d.dst), mask8(d.mask8),
+          write_mask(d.write_mask), rl_first(d.rl_first), mask_mode(d.mask_mode), erosion(d.erosion),
+          scale_mode(d.scale_mode), save16(d.save16), crop(d.crop), need_xz(d.need_xz), damp(d.damp),
+          scale(d.scale), offset(d.offset), out(d.out), chk(d.chk) {
+        for (int i = 0; i < 3; i++) {
+            rdims[i] = d.rdims[i];
+            bb0[i] = d.bb0[i];
+            bb1[i] = d.bb1[i];
+        }
+    }
+};
+
 // Value of one voxel after the post-processing of decon_lucy_omw_function.m:146-177 (damping, then
 // scaling with offset and mask); x/z only matter to the border-erosion mask.
-__device__ __forceinline__ float post_value(const VolDesc& d, float J, long long vi, int x, int y, int z) {
+template <class D>
+__device__ __forceinline__ float post_value(const D& d, float J, long long vi, int x, int y, int z) {
     if (d.damp > 1.f) {
         const float dI = __fmul_rn(d.damp, d.I[vi]);
         const float a = (J <= dI) ? J : 0.f;
@@ -72,18 +104,21 @@ __device__ __forceinline__ float post_value(const VolDesc& d, float J, long long
     return J;
 }
 
-__device__ __forceinline__ void row_xz(const VolDesc& d, long long row, int& x, int& z) {
+template <class D>
+__device__ __forceinline__ void row_xz(const D& d, long long row, int& x, int& z) {
     const unsigned r = (unsigned)row;
     z = (int)(r / (unsigned)d.nx);
     x = (int)(r - (unsigned)z * (unsigned)d.nx);
 }
 
-__device__ __forceinline__ bool in_box(const VolDesc& d, int x, int y, int z) {
+template <class D>
+__device__ __forceinline__ bool in_box(const D& d, int x, int y, int z) {
     return !(y < d.bb0[0] || y > d.bb1[0] || x < d.bb0[1] || x > d.bb1[1] || z < d.bb0[2] || z > d.bb1[2]);
 }
 
 // Store of one post-processed voxel into the (cropped) output.
-__device__ __forceinline__ void out_store(const VolDesc& d, float J, long long vi, int x, int y, int z) {
+template <class D>
+__device__ __forceinline__ void out_store(const D& d, float J, long long vi, int x, int y, int z) {
     long long oi = vi;
     if (d.crop) {
         const long long oy = d.bb1[0] - d.bb0[0] + 1, ox = d.bb1[1] - d.bb0[1] + 1;
@@ -95,9 +130,21 @@ __device__ __forceinline__ void out_store(const VolDesc& d, float J, long long v
     else ((float*)d.out)[oi] = J;
 }
 
+// Whether rows row0 .. row0 + n - 1 (row = x + nx z) hold a voxel of the crop box: the rows of a
+// y-pass tile are consecutive, so they cover one x range of one z plane or reach over whole planes.
+__device__ __forceinline__ bool rows_meet_box(const VolDesc& d, long long row0, int n) {
+    const unsigned nx = (unsigned)d.nx;
+    const int z0 = (int)((unsigned)row0 / nx), z1 = (int)((unsigned)(row0 + n - 1) / nx);
+    if (z1 < d.bb0[2] || z0 > d.bb1[2]) return false;
+    if (z0 != z1) return true;
+    const int x0 = (int)((unsigned)row0 - (unsigned)z0 * nx), x1 = x0 + n - 1;
+    return !(x1 < d.bb0[1] || x0 > d.bb1[1]);
+}
+
 // post-processing of one voxel and the cropped store.  x/z of the row are only derived when a crop
 // box or the border-erosion mask needs them.
-__device__ __forceinline__ void post_store(const VolDesc& d, float J, long long row, int y) {
+template <class D>
+__device__ __forceinline__ void post_store(const D& d, float J, long long row, int y) {
     const long long vi = row * d.ny + y;
     int x = 0, z = 0;
     if (d.need_xz) {
@@ -146,7 +193,8 @@ __device__ __forceinline__ void fft_xz(float2* buf, const AxisDev& A, const floa
 
 // Per-voxel operation of a y-pass mode on a pair of reals (x = element y, y = element y+1; for odd
 // ny only .x is live).  a0/a1 are the mode's gathered inputs for the same voxels.
-__device__ __forceinline__ float2 voxel_pair(const VolDesc& d, int mode, float2 c, float2 a0, float2 a1, long long row,
+template <class D>
+__device__ __forceinline__ float2 voxel_pair(const D& d, int mode, float2 c, float2 a0, float2 a1, long long row,
                                              int y, bool two, float lam, double& acc0, double& acc1) {
     float2 r = make_float2(0.f, 0.f);
     const long long vi = row * d.ny + y;
@@ -203,7 +251,8 @@ __device__ __forceinline__ float2 voxel_pair(const VolDesc& d, int mode, float2 
 
 // Y_PRE on a pair of voxels: raw -> I = sat(raw - bg) (uint16) or max(raw - bg, 0) (written), mask =
 // raw ~= 0 (decon_lucy_omw_function.m:79-98).  a0 is the staged raw pair.
-__device__ __forceinline__ float2 pre_pair(const VolDesc& d, bool raw_sync, bool odd, float2 a0, long long row, int y,
+template <class D>
+__device__ __forceinline__ float2 pre_pair(const D& d, bool raw_sync, bool odd, float2 a0, long long row, int y,
                                            unsigned& zeros) {
     // raw -> I = sat(raw - bg) (uint16) or max(raw - bg, 0); mask = raw ~= 0
     const long long vi = row * (long long)d.ny + y;
@@ -328,6 +377,9 @@ __global__ void __launch_bounds__(PK_THREADS, 3) k_y(const VolDesc* __restrict__
                                          (size_t)y_aux_arrays(mode) * L * M), 1) ||
         !PK_IN(d, row0 < d.nrows && Lc >= 1, 2))
         return;   // uniform over the CTA, before any barrier
+    if constexpr (mode == Y_FINAL || mode == Y_RLFINAL) {
+        if (d.crop && !rows_meet_box(d, row0, Lc)) return;   // none of these rows has a stored voxel
+    }
 
     // ---- issue the asynchronous loads: group A = spectrum rows, group B = per-voxel inputs
     if (spec_in) {
@@ -603,17 +655,18 @@ __global__ void __launch_bounds__(PK_THREADS, 3) k_y(const VolDesc* __restrict__
     cp_wait<0>();
     __syncthreads();
 
-    // ---- per-voxel phase
+    // ---- per-voxel phase (descriptor fields in registers: the loop stores to the volume's arrays)
+    const VoxFields f(d);
     for (int idx = tid; idx < nvox; idx += NT) {
         const int l = idx / M, k = idx - l * M;
         const long long row = row0 + l;
         const int y = odd ? k : 2 * k;
         float2 out;
         if (mode == Y_PRE) {
-            out = pre_pair(d, raw_sync, odd, aux0[idx], row, y, zeros);
+            out = pre_pair(f, raw_sync, odd, aux0[idx], row, y, zeros);
         } else {
             const float2 cval = spec_in ? buf[pad(idx)] : make_float2(0.f, 0.f);
-            out = voxel_pair(d, mode, cval, pa0 ? aux0[idx] : make_float2(0.f, 0.f), pa1 ? aux1[idx] : make_float2(0.f, 0.f),
+            out = voxel_pair(f, mode, cval, pa0 ? aux0[idx] : make_float2(0.f, 0.f), pa1 ? aux1[idx] : make_float2(0.f, 0.f),
                              row, y, !odd, lam, acc0, acc1);
         }
         if (spec_out) buf[pad(idx)] = odd ? make_float2(out.x, 0.f) : out;

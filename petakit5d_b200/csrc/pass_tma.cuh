@@ -434,6 +434,24 @@ struct RegisterTma {
                 register_tma_one<P, TMA_Z_CONV, 1, 2, XZ_CONV, 32, 2, 512>(t);
                 register_tma_one<P, TMA_Z_CONV, 2, 2, XZ_CONV, 24, 3, 384>(t);
             }
+            if constexpr (kPlans[P].n > 256 && kPlans[P].n < 512) {
+                // lines longer than 256: the 4096-point tile is 8 columns (64-byte rows) or fewer wide;
+                // 16-column tiles (128-byte rows), 16 compute warps, three or two buffers, one CTA per SM
+                register_tma_one<P, TMA_X_FWD, 1, 1, XZ_FWD, 16, 3, 512>(t);
+                register_tma_one<P, TMA_X_INV, 1, 1, XZ_INV, 16, 3, 512>(t);
+                register_tma_one<P, TMA_X_FWD, 2, 1, XZ_FWD, 16, 2, 512>(t);
+                register_tma_one<P, TMA_X_INV, 2, 1, XZ_INV, 16, 2, 512>(t);
+                if constexpr (XztLayout<P, 16, 3>::bytes(true) <= 227 * 1024)
+                    register_tma_one<P, TMA_Z_CONV, 1, 2, XZ_CONV, 16, 3, 384>(t);
+                register_tma_one<P, TMA_Z_CONV, 2, 2, XZ_CONV, 16, 2, 512>(t);
+            }
+            if constexpr (kPlans[P].n >= 128 && kPlans[P].n < 256) {
+                // 16- or 32-column tiles already: three buffers (x), and the convolution with three
+                // buffers and 12 compute warps, one CTA per SM
+                register_tma_one<P, TMA_X_FWD, 1, 1, XZ_FWD, 0, 3>(t);
+                register_tma_one<P, TMA_X_INV, 1, 1, XZ_INV, 0, 3>(t);
+                register_tma_one<P, TMA_Z_CONV, 1, 2, XZ_CONV, 0, 3, 384>(t);
+            }
         }
         RegisterTma<P + 1, HI>::fill(t);
     }

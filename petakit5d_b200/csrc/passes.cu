@@ -217,7 +217,7 @@ int tma_index(const PkStep& s) {
 // The first time a single-volume step of a (pass, plan, size class) is seen, every candidate runs
 // once to warm up and twice timed on scratch buffers of that step's geometry (zeroed spectrum and
 // OTF; no live data is touched); the fastest is kept for the context and appended to an on-disk
-// cache (PK_TUNE_FILE, else ~/.cache/pkdecon/tune-v3.txt), keyed by the device name, so later
+// cache (PK_TUNE_FILE, else ~/.cache/pkdecon/tune-v4.txt), keyed by the device name, so later
 // processes skip the timing.  PK_TUNE=0 turns the timing off (the fallback choice everywhere).
 
 std::mutex g_tf_mu;
@@ -229,7 +229,7 @@ std::string tune_path() {
     if (e && *e) return e;
     const char* h = getenv("HOME");
     if (!h || !*h) return "";
-    return std::string(h) + "/.cache/pkdecon/tune-v3.txt";
+    return std::string(h) + "/.cache/pkdecon/tune-v4.txt";
 }
 
 std::string device_tag(int dev) {
@@ -268,13 +268,12 @@ void tf_store(const std::string& key, int v, float ms) {
     if (f) f << key << " " << v << " " << ms << "\n";
 }
 
-const char* variant_name(int idx, int v) {
-    static const char* names[] = {"register-IO", "tma", "tma-16col-16warps", "tma-16col-16warps-3buf",
-                                  "tma-32col-16warps", "tma-24col-12warps-3buf"};
-    if (v < 0) return names[0];
-    if (v == 0) return names[1];
-    if (idx == pkpass::TMA_Z_CONV) return v == 1 ? names[4] : names[5];
-    return v == 1 ? names[2] : names[3];
+// A candidate's name: "register-IO", or the TMA variant's tile width, compute warps and buffers.
+std::string variant_name(int plan, int idx, int v) {
+    if (v < 0) return "register-IO";
+    const pkpass::TmaTable* t = tma_kernels();
+    return "tma-" + std::to_string(t->cols[plan][idx][v]) + "col-" + std::to_string((t->threads[plan][idx][v] - 32) / 32) +
+           "warps-" + std::to_string(t->nbuf[plan][idx][v]) + "buf";
 }
 
 // Times each candidate of step `s` (first descriptor's geometry) on scratch buffers; returns the
@@ -343,10 +342,15 @@ int time_candidates(pk_ctx* ctx, const PkStep& s, const VolDesc& d0, int idx, co
         for (int r = 0; ok && r < 1; r++) launch();
         ok = ok && cudaEventRecord(e0, st) == cudaSuccess;
         for (int r = 0; ok && r < 2; r++) launch();
+        const cudaError_t le = cudaGetLastError();   // a launch that failed did no work: not a candidate
         ok = ok && cudaEventRecord(e1, st) == cudaSuccess && cudaEventSynchronize(e1) == cudaSuccess;
         float el = 0.f;
         ok = ok && cudaEventElapsedTime(&el, e0, e1) == cudaSuccess;
         if (!ok) break;
+        // a time below the pass's bytes at 10 TB/s (above any B200's HBM) means the launch did not do
+        // the work either
+        const double floor_ms = (double)(conv ? 3 : 2) * (double)Sb / 10e12 * 1e3;
+        if (le != cudaSuccess || el / 2.f < floor_ms) continue;
         ms[ci] = el / 2.f;
         if (ms[ci] < best_ms) {
             best_ms = ms[ci];
@@ -366,7 +370,8 @@ int time_candidates(pk_ctx* ctx, const PkStep& s, const VolDesc& d0, int idx, co
 }
 
 // Size class of an x / z step: how many waves of variant 0's resident CTAs its tiles make (0: under
-// one wave, 1: one to three, 2: more).  Variants are chosen per (pass, plan, size class).
+// one wave, 1: one to three, 2: three to twelve, 3: more -- a batch's or a serving round's steps).
+// Variants are chosen per (pass, plan, size class).
 int size_class(const PkProgram& prog, const PkStep& s, int idx) {
     const pkpass::TmaTable* t = tma_kernels();
     const int T = t->cols[s.plan][idx][0];
@@ -376,7 +381,7 @@ int size_class(const PkProgram& prog, const PkStep& s, int idx) {
         tiles += (long long)(s.kind == PK_STEP_X ? d.nz : d.nx) * ((d.Py + T - 1) / T);
     }
     const long long wave = (long long)std::max(1, t->per_sm[s.plan][idx][0]) * sm_count();
-    return tiles < wave ? 0 : tiles < 3 * wave ? 1 : 2;
+    return tiles < wave ? 0 : tiles < 3 * wave ? 1 : tiles < 12 * wave ? 2 : 3;
 }
 
 // The variant an x / z step runs: the context's earlier choice, the on-disk cache's, or a timing.
@@ -392,6 +397,10 @@ int choose_variant(pk_ctx* ctx, const PkProgram& prog, const PkStep& s, int idx,
     for (int v = 0; v < pkpass::kTmaVariants; v++)
         if (t->k[s.plan][idx][v]) cands.push_back(v);
     const VolDesc& d0 = prog.descs[s.desc_off];
+    if (const char* fv = getenv("PK_TMA_VARIANT")) {   // diagnostics: this candidate wherever it exists
+        const int v = atoi(fv);
+        if (fv[0] && std::find(cands.begin(), cands.end(), v) != cands.end()) return v;
+    }
     const int cls = size_class(prog, s, idx);
     const int fallback = (cls == 0 && kernels().xz[s.plan]) ? -1 : 0;
     if (!ctx || cands.size() < 2) return cands.empty() ? 0 : (cands.size() == 1 ? cands[0] : fallback);
@@ -400,16 +409,16 @@ int choose_variant(pk_ctx* ctx, const PkProgram& prog, const PkStep& s, int idx,
     if (it != ctx->tune.end()) return it->second;
     std::string fkey = device_tag(ctx->device) + "|";
     for (size_t i = 0; i < key.size(); i++) fkey += (i ? "," : "") + std::to_string(key[i]);
-    auto record = [&](int v, const char* source, const std::vector<float>* ms) {
+    auto record = [&](int v, const char* source, const std::vector<float>* ms, const VolDesc& g) {
         std::string rec = "{\"pass\": \"" + std::string(pk_step_name(s)) + "\", \"n\": " + std::to_string(kPlans[s.plan].n) +
-                          ", \"size_class\": " + std::to_string(cls) + ", \"timed_on\": [" + std::to_string(d0.ny) + ", " +
-                          std::to_string(d0.nx) + ", " + std::to_string(d0.nz) + "], \"chosen\": \"" +
-                          variant_name(idx, v) + "\", \"source\": \"" + source + "\"";
+                          ", \"size_class\": " + std::to_string(cls) + ", \"timed_on\": [" + std::to_string(g.ny) + ", " +
+                          std::to_string(g.nx) + ", " + std::to_string(g.nz) + "], \"chosen\": \"" +
+                          variant_name(s.plan, idx, v) + "\", \"source\": \"" + source + "\"";
         if (ms) {
             rec += ", \"ms\": {";
             for (size_t i = 0; i < cands.size(); i++) {
                 char tmp[96];
-                snprintf(tmp, sizeof(tmp), "%s\"%s\": %.5f", i ? ", " : "", variant_name(idx, cands[i]),
+                snprintf(tmp, sizeof(tmp), "%s\"%s\": %.5f", i ? ", " : "", variant_name(s.plan, idx, cands[i]).c_str(),
                          ms->size() > i ? (*ms)[i] : -1.f);
                 rec += tmp;
             }
@@ -424,7 +433,7 @@ int choose_variant(pk_ctx* ctx, const PkProgram& prog, const PkStep& s, int idx,
         auto f = g_tf.find(fkey);
         if (f != g_tf.end() && std::find(cands.begin(), cands.end(), f->second) != cands.end()) {
             ctx->tune[key] = f->second;
-            record(f->second, "cache", nullptr);
+            record(f->second, "cache", nullptr, d0);
             return f->second;
         }
     }
@@ -456,7 +465,7 @@ int choose_variant(pk_ctx* ctx, const PkProgram& prog, const PkStep& s, int idx,
     int best = time_candidates(ctx, s, dt, idx, cands, st, ms);
     if (best == -2) return fallback;
     ctx->tune[key] = best;
-    record(best, "timed", &ms);
+    record(best, "timed", &ms, dt);
     {
         std::lock_guard<std::mutex> lk(g_tf_mu);
         g_tf[fkey] = best;
