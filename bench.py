@@ -495,7 +495,7 @@ def main():
                                                          "batched_equals_plain", "ms_batched", "ms_plain",
                                                          "device_resident", "workload")),
                                ("served", wl_served, ("value", "unit", "latency_ms", "plain_sequential",
-                                                      "speedup_vs_plain", "wall_s", "workload"))):
+                                                      "speedup_vs_plain", "wall_s", "saturated", "workload"))):
             try:
                 sub = fn(args)
                 line[name] = {k: sub[k] for k in keys if k in sub}
@@ -765,39 +765,41 @@ def wl_served(args):
             t = torch.empty(v.shape[::-1], dtype=torch.int16).pin_memory()
             keep.append(t)
             outs[v.shape] = t.numpy().view(np.uint16).T
-    lat = [None] * len(reqs)
-    ids = [None] * len(reqs)
-    done = threading.Semaphore(0)
-
-    def waiter(q):
-        while True:
-            i = q.get()
-            if i is None:
-                return
-            _, ms = srv.wait(ids[i], out=outs[reqs[i][0].shape])
-            lat[i] = ms
-            done.release()
-
     import queue
-    q = queue.Queue()
-    ws = [threading.Thread(target=waiter, args=(q,), daemon=True) for _ in range(8)]
-    for w in ws:
-        w.start()
-    t0 = time.perf_counter()
-    for i, (v, pid, m, it) in enumerate(reqs):
-        now = time.perf_counter() - t0
-        if arrivals[i] > now:
-            time.sleep(arrivals[i] - now)
-        ids[i] = srv.submit(v, pid, m, it, Background=100)
-        q.put(i)
-    for _ in reqs:
-        done.acquire()
-    wall = time.perf_counter() - t0
-    _log(f"served: {len(reqs)} requests done in {wall:.2f} s")
-    for _ in ws:
-        q.put(None)
-    st = srv.stats()
-    srv.close()
+
+    def phase(arr):
+        """Submit request i at arrival time arr[i] (seconds from the start); returns (wall s, latencies)."""
+        lat = [None] * len(reqs)
+        ids = [None] * len(reqs)
+        done = threading.Semaphore(0)
+        q = queue.Queue()
+
+        def waiter():
+            while True:
+                i = q.get()
+                if i is None:
+                    return
+                _, ms = srv.wait(ids[i], out=outs[reqs[i][0].shape])
+                lat[i] = ms
+                done.release()
+
+        ws = [threading.Thread(target=waiter, daemon=True) for _ in range(8)]
+        for w in ws:
+            w.start()
+        t0 = time.perf_counter()
+        for i, (v, pid, m, it) in enumerate(reqs):
+            now = time.perf_counter() - t0
+            if arr[i] > now:
+                time.sleep(arr[i] - now)
+            ids[i] = srv.submit(v, pid, m, it, Background=100)
+            q.put(i)
+        for _ in reqs:
+            done.acquire()
+        wall = time.perf_counter() - t0
+        for _ in ws:
+            q.put(None)
+        return wall, lat
+
     # the same requests, one plain host call after another (each (size, PSF, method) warmed up first,
     # as the server's were: OTFs cached, kernels loaded, variants tuned)
     def plain_call(v, pid, m, it):
@@ -813,12 +815,27 @@ def wl_served(args):
             _lib.check(_lib.lib.pk_decon_lucy(ctx.handle, v.ctypes.data, _lib.PK_U16, _lib.i64x3(v.shape),
                                               pf.ctypes.data, _lib.i64x3(pf.shape), it, p, o.ctypes.data, None))
 
+    def plain_all():
+        t1 = time.perf_counter()
+        for v, pid, m, it in reqs:
+            plain_call(v, pid, m, it)
+        return time.perf_counter() - t1
+
     for (shp, pid, m), v in seen.items():
         plain_call(v, pid, m, 1)
-    t1 = time.perf_counter()
-    for v, pid, m, it in reqs:
-        plain_call(v, pid, m, it)
-    plain = time.perf_counter() - t1
+    plain = plain_all()
+    _log(f"served: the plain calls one after another took {plain:.2f} s")
+    timed0 = sum(1 for r in ctx.tune_read() if r.get("source") == "timed")
+    wall, lat = phase(arrivals)
+    _log(f"served: {len(reqs)} requests done in {wall:.2f} s")
+    # the same requests all at once: the server's throughput when arrivals do not limit it
+    wall_sat, lat_sat = phase(np.zeros(len(reqs)))
+    _log(f"served: {len(reqs)} requests submitted at once done in {wall_sat:.2f} s")
+    tuned_in_phases = sum(1 for r in ctx.tune_read() if r.get("source") == "timed") - timed0
+    st = srv.stats()
+    srv.close()
+    plain_after = plain_all()
+    _log(f"served: the plain calls again after serving took {plain_after:.2f} s")
     L = np.array(lat)
     return ({"metric": "served Mvoxel/s and request latency", "workload":
            f"{len(reqs)} open-loop Poisson requests at {args.rate} req/s (90% chunk sizes, 10% 768x768x384; 80% OMW x2, "
@@ -828,7 +845,13 @@ def wl_served(args):
                           "p99": round(float(np.percentile(L, 99)), 2), "max": round(float(L.max()), 2)},
            "plain_sequential": round(nvox / plain / 1e6, 1), "speedup_vs_plain": round(plain / wall, 3),
            "wall_s": round(wall, 3), "plain_s": round(plain, 3), "rounds": st["rounds"],
-           "peak_inflight_GB": round(st["peak_inflight_bytes"] / 1e9, 2)})
+           "peak_inflight_GB": round(st["peak_inflight_bytes"] / 1e9, 2), "plain_s_after_serving": round(plain_after, 3),
+           "autotune_timings_while_serving": tuned_in_phases,
+           "saturated": {"value": round(nvox / wall_sat / 1e6, 1), "unit": "Mvoxel/s",
+                         "speedup_vs_plain": round(plain / wall_sat, 3), "wall_s": round(wall_sat, 3),
+                         "latency_ms": {"p50": round(float(np.percentile(lat_sat, 50)), 2),
+                                        "p99": round(float(np.percentile(lat_sat, 99)), 2)},
+                         "note": "the same requests submitted at once (throughput not limited by arrivals)"}})
 
 
 DSR = dict(angle=32.45, dz=0.3, xy=0.108, reverse=True)   # the reference demo's deskew / rotate settings

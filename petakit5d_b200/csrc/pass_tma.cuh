@@ -446,11 +446,9 @@ struct RegisterTma {
                 register_tma_one<P, TMA_Z_CONV, 2, 2, XZ_CONV, 16, 2, 512>(t);
             }
             if constexpr (kPlans[P].n >= 128 && kPlans[P].n < 256) {
-                // 16- or 32-column tiles already: three buffers (x), and the convolution with three
-                // buffers and 12 compute warps, one CTA per SM
+                // 16- or 32-column tiles already: three buffers (x)
                 register_tma_one<P, TMA_X_FWD, 1, 1, XZ_FWD, 0, 3>(t);
                 register_tma_one<P, TMA_X_INV, 1, 1, XZ_INV, 0, 3>(t);
-                register_tma_one<P, TMA_Z_CONV, 1, 2, XZ_CONV, 0, 3, 384>(t);
             }
         }
         RegisterTma<P + 1, HI>::fill(t);

@@ -276,68 +276,74 @@ std::string variant_name(int plan, int idx, int v) {
            "warps-" + std::to_string(t->nbuf[plan][idx][v]) + "buf";
 }
 
-// Times each candidate of step `s` (first descriptor's geometry) on scratch buffers; returns the
-// fastest, or -2 when nothing could be timed.  ms[i] receives candidate i's time.
-int time_candidates(pk_ctx* ctx, const PkStep& s, const VolDesc& d0, int idx, const std::vector<int>& cands,
+// Times each candidate of step `s` on scratch buffers: nrep volumes of geometry d0 (one, or for a
+// multi-volume step of a batch or a serving round, copies of its first volume, each with its own
+// buffers, descriptor and tensor maps); returns the fastest, or -2 when nothing could be timed.
+// ms[i] receives candidate i's time.
+int time_candidates(pk_ctx* ctx, const PkStep& s, const VolDesc& d0, int nrep, int idx, const std::vector<int>& cands,
                     cudaStream_t st, std::vector<float>& ms) {
-    // (d0 is the geometry timed: the step's first volume, its outer extent scaled to the step's tiles)
     const pkpass::TmaTable* t = tma_kernels();
     const pkpass::KernelTable& kt = kernels();
     const int axis = s.kind == PK_STEP_X ? 1 : 2;
     const bool conv = s.mode == XZ_CONV;
     const size_t Sb = (size_t)8 * d0.Pp * d0.nx * d0.nz;
-    if (Sb > ((size_t)3 << 29)) return -2;   // above 1.5 GB of scratch: keep the default
-    const size_t moff = (sizeof(VolDesc) + 63) & ~(size_t)63;
-    const size_t poff = moff + sizeof(XZMaps);
-    const size_t blob = poff + 64;
+    const size_t per = (conv ? 2 : 1) * ((Sb + 255) & ~(size_t)255);
+    if (nrep < 1 || per * nrep > ((size_t)3 << 29)) return -2;   // above 1.5 GB of scratch: keep the default
+    const size_t moff = ((size_t)nrep * sizeof(VolDesc) + 63) & ~(size_t)63;
+    const size_t poff = moff + (size_t)nrep * sizeof(XZMaps);
+    const size_t blob = poff + sizeof(int) * (nrep + 1);
+    const size_t soff = (blob + 255) & ~(size_t)255;
     char* d = nullptr;
-    if (cudaMalloc(&d, blob + (conv ? 2 : 1) * Sb + 256) != cudaSuccess) {
+    if (cudaMalloc(&d, soff + per * nrep) != cudaSuccess) {
         cudaGetLastError();
         return -2;
     }
-    float2* S = (float2*)(d + ((blob + 255) & ~(size_t)255));
-    float2* O = conv ? S + Sb / 8 : nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     int best = -2;
     float best_ms = 1e30f;
-    bool ok = cudaMemsetAsync(S, 0, (conv ? 2 : 1) * Sb, st) == cudaSuccess &&
+    bool ok = cudaMemsetAsync(d + soff, 0, per * nrep, st) == cudaSuccess &&
               cudaEventCreate(&e0) == cudaSuccess && cudaEventCreate(&e1) == cudaSuccess;
-    VolDesc dt = d0;
-    dt.S = S;
-    dt.otf = O;
+    std::vector<VolDesc> dv(nrep, d0);
+    for (int r = 0; r < nrep; r++) {
+        dv[r].S = (float2*)(d + soff + per * r);
+        dv[r].otf = conv ? (float2*)(d + soff + per * r + per / 2) : nullptr;
+    }
     std::vector<unsigned char> h(blob, 0);
-    memcpy(h.data(), &dt, sizeof(VolDesc));
+    memcpy(h.data(), dv.data(), sizeof(VolDesc) * nrep);
     ms.assign(cands.size(), -1.f);
     for (size_t ci = 0; ok && ci < cands.size(); ci++) {
         const int v = cands[ci];
-        int tiles, grid;
+        int per_vol, grid;
         size_t smem;
-        XZMaps m;
-        memset(&m, 0, sizeof(m));
+        std::vector<XZMaps> m(nrep);
+        memset(m.data(), 0, sizeof(XZMaps) * nrep);
         if (v < 0) {
-            tiles = axis == 1 ? d0.blocksX : d0.blocksZ;
-            grid = tiles;
-            smem = step_smem(s.kind, s.mode, dt);
+            per_vol = axis == 1 ? d0.blocksX : d0.blocksZ;
+            grid = per_vol * nrep;
+            smem = step_smem(s.kind, s.mode, d0);
         } else {
             const int T = t->cols[s.plan][idx][v];
-            if (d0.Py < T || !encode_spec_map(&m.s, S, dt, axis, s.plan, T) ||
-                (conv && !encode_spec_map(&m.otf, O, dt, axis, s.plan, T)))
-                continue;
-            tiles = (axis == 1 ? d0.nz : d0.nx) * ((d0.Py + T - 1) / T);
-            grid = std::min(tiles, t->per_sm[s.plan][idx][v] * sm_count());
+            bool enc = d0.Py >= T;
+            for (int r = 0; r < nrep && enc; r++)
+                enc = encode_spec_map(&m[r].s, dv[r].S, dv[r], axis, s.plan, T) &&
+                      (!conv || encode_spec_map(&m[r].otf, dv[r].otf, dv[r], axis, s.plan, T));
+            if (!enc) continue;
+            per_vol = (axis == 1 ? d0.nz : d0.nx) * ((d0.Py + T - 1) / T);
+            grid = std::min(per_vol * nrep, t->per_sm[s.plan][idx][v] * sm_count());
             smem = t->smem[s.plan][idx][v];
         }
-        const int pf[2] = {0, tiles};
-        memcpy(h.data() + moff, &m, sizeof(m));
-        memcpy(h.data() + poff, pf, sizeof(pf));
+        std::vector<int> pf(nrep + 1);
+        for (int r = 0; r <= nrep; r++) pf[r] = per_vol * r;
+        memcpy(h.data() + moff, m.data(), sizeof(XZMaps) * nrep);
+        memcpy(h.data() + poff, pf.data(), sizeof(int) * (nrep + 1));
         ok = cudaMemcpyAsync(d, h.data(), blob, cudaMemcpyHostToDevice, st) == cudaSuccess &&
              cudaStreamSynchronize(st) == cudaSuccess;
         const VolDesc* dd = (const VolDesc*)d;
         const XZMaps* dm = (const XZMaps*)(d + moff);
         const int* dp = (const int*)(d + poff);
         auto launch = [&]() {
-            if (v < 0) kt.xz[s.plan]<<<grid, PK_THREADS, smem, st>>>(dd, dp, 1, axis, s.mode);
-            else t->k[s.plan][idx][v]<<<grid, t->threads[s.plan][idx][v], smem, st>>>(dd, dm, dp, 1, ctx->d_err);
+            if (v < 0) kt.xz[s.plan]<<<grid, PK_THREADS, smem, st>>>(dd, dp, nrep, axis, s.mode);
+            else t->k[s.plan][idx][v]<<<grid, t->threads[s.plan][idx][v], smem, st>>>(dd, dm, dp, nrep, ctx->d_err);
         };
         for (int r = 0; ok && r < 1; r++) launch();
         ok = ok && cudaEventRecord(e0, st) == cudaSuccess;
@@ -349,7 +355,7 @@ int time_candidates(pk_ctx* ctx, const PkStep& s, const VolDesc& d0, int idx, co
         if (!ok) break;
         // a time below the pass's bytes at 10 TB/s (above any B200's HBM) means the launch did not do
         // the work either
-        const double floor_ms = (double)(conv ? 3 : 2) * (double)Sb / 10e12 * 1e3;
+        const double floor_ms = (double)(conv ? 3 : 2) * (double)Sb * nrep / 10e12 * 1e3;
         if (le != cudaSuccess || el / 2.f < floor_ms) continue;
         ms[ci] = el / 2.f;
         if (ms[ci] < best_ms) {
@@ -404,7 +410,8 @@ int choose_variant(pk_ctx* ctx, const PkProgram& prog, const PkStep& s, int idx,
     const int cls = size_class(prog, s, idx);
     const int fallback = (cls == 0 && kernels().xz[s.plan]) ? -1 : 0;
     if (!ctx || cands.size() < 2) return cands.empty() ? 0 : (cands.size() == 1 ? cands[0] : fallback);
-    const std::vector<long long> key = {s.kind, s.mode, s.plan, cls};
+    const int multi = s.nvol > 1 ? 1 : 0;   // steps over many volumes (batches, serving rounds) time apart
+    const std::vector<long long> key = {s.kind, s.mode, s.plan, cls, multi};
     auto it = ctx->tune.find(key);
     if (it != ctx->tune.end()) return it->second;
     std::string fkey = device_tag(ctx->device) + "|";
@@ -442,27 +449,25 @@ int choose_variant(pk_ctx* ctx, const PkProgram& prog, const PkStep& s, int idx,
     const bool capturing = cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone;
     if (capturing) cudaGetLastError();
     if ((off && off[0] == '0') || capturing) return fallback;   // no timing here
-    // the timed geometry: the first volume, with its outer extent (z for an x pass, x for a z pass)
-    // scaled so that it has as many tiles as the whole step (a batch's or a round's volumes together)
-    VolDesc dt = d0;
-    if (s.nvol > 1) {
+    // the timed geometry: the step's first volume; for a multi-volume step, as many copies of it (each
+    // with its own buffers) as make the step's tile count, 2 to 16 of them within the scratch limit
+    int nrep = 1;
+    if (multi) {
         const int T0 = t->cols[s.plan][idx][0];
         long long tiles = 0;
         for (int i = 0; i < s.nvol; i++) {
             const VolDesc& d = prog.descs[s.desc_off + i];
             tiles += (long long)(s.kind == PK_STEP_X ? d.nz : d.nx) * ((d.Py + T0 - 1) / T0);
         }
-        const long long per_outer = (d0.Py + T0 - 1) / T0;
-        const int outer = (int)std::min<long long>(4096, std::max<long long>(1, (tiles + per_outer - 1) / per_outer));
-        if (s.kind == PK_STEP_X) dt.nz = outer;
-        else dt.nx = outer;
-        dt.nrows = (long long)dt.nx * dt.nz;
-        dt.blocksX = dt.nz * ((dt.Py + dt.Tx - 1) / dt.Tx);
-        dt.blocksZ = dt.nx * ((dt.Py + dt.Tz - 1) / dt.Tz);
+        const long long one = (long long)(s.kind == PK_STEP_X ? d0.nz : d0.nx) * ((d0.Py + T0 - 1) / T0);
+        const size_t Sb = (size_t)8 * d0.Pp * d0.nx * d0.nz * (s.mode == XZ_CONV ? 2 : 1);
+        const long long fit = std::max<long long>(1, (long long)(((size_t)3 << 29) / std::max<size_t>(Sb, 1)));
+        nrep = (int)std::max<long long>(2, std::min<long long>({16, fit, (tiles + one - 1) / one}));
     }
+    VolDesc dt = d0;
     std::vector<float> ms;
     PkRange range("pk autotune");
-    int best = time_candidates(ctx, s, dt, idx, cands, st, ms);
+    int best = time_candidates(ctx, s, dt, nrep, idx, cands, st, ms);
     if (best == -2) return fallback;
     ctx->tune[key] = best;
     record(best, "timed", &ms, dt);
