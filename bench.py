@@ -380,7 +380,7 @@ def main():
     ap.add_argument("--no-extras", action="store_true",
                     help="leave the batched (96 chunks) and served (Poisson requests) sub-objects off the line")
     ap.add_argument("--workload", default="omw_llsm",
-                    choices=["omw_llsm", "rl_small", "batched", "served", "large", "dsr"])
+                    choices=["omw_llsm", "rl_small", "batched", "batched_passes", "served", "large", "dsr"])
     ap.add_argument("--rate", type=float, default=200.0, help="served: Poisson arrival rate (requests/s)")
     ap.add_argument("--requests", type=int, default=240, help="served: number of requests")
     ap.add_argument("--ncu-case", action="store_true",
@@ -495,7 +495,8 @@ def main():
                                                          "batched_equals_plain", "ms_batched", "ms_plain",
                                                          "device_resident", "workload")),
                                ("served", wl_served, ("value", "unit", "latency_ms", "plain_sequential",
-                                                      "speedup_vs_plain", "wall_s", "saturated", "workload"))):
+                                                      "speedup_vs_plain", "wall_s", "saturated", "device_loop",
+                                                      "workload"))):
             try:
                 sub = fn(args)
                 line[name] = {k: sub[k] for k in keys if k in sub}
@@ -707,6 +708,72 @@ def wl_batched(args):
                                "note": "same batch with chunks and outputs already in HBM (compute bound)"}})
 
 
+def wl_batched_passes(args):
+    """Config 3's batch, chunks and outputs resident in HBM, with every x / z kernel candidate forced
+    in turn (PK_TMA_VARIANT; "tuned" = the autotuner's choices): per-pass kernel time by transform
+    length and kernel family, one profiled call after two warm-ups per candidate."""
+    import torch
+    from petakit5d_b200 import _lib
+    from petakit5d_b200 import backprojector as B
+    from petakit5d_b200 import decon as D
+    if args.impl == "reference":
+        _emit({"impl": "reference", "unavailable": "per-pass kernel profile of the GPU path (no CPU counterpart)"})
+        return None
+    os.environ["PK_PROF_DETAIL"] = "1"
+    device = torch.device("cuda", 0)
+    chunks, pinned, psfs, ids, boxes = _chunk_set(device)
+    bps = [B.omw_backprojector_generation(p, 0.005, False, OTFCumThresh=0.6)[0] for p in psfs]
+    d_chunks = [pc.to(device) for pc in pinned]
+    d_outs = [torch.empty(((b[5] - b[2] + 1), (b[4] - b[1] + 1), (b[3] - b[0] + 1)), dtype=torch.int16, device=device)
+              for b in boxes]
+    arr = (_lib.Chunk * len(chunks))()
+    for i, (c, bb) in enumerate(zip(chunks, boxes)):
+        arr[i].in_ = d_chunks[i].data_ptr()
+        arr[i].dims = _lib.i64x3(c.shape)
+        arr[i].psf_id = int(ids[i])
+        arr[i].has_bbox = 1
+        for k in range(6):
+            arr[i].bbox[k] = int(bb[k])
+        arr[i].out = d_outs[i].data_ptr()
+    pfs = [np.asfortranarray(q, np.float32) for q in psfs]
+    pbs = [np.asfortranarray(q, np.float32) for q in bps]
+    fptrs = (_lib.C.c_void_p * 3)(*[a.ctypes.data for a in pfs])
+    bptrs = (_lib.C.c_void_p * 3)(*[a.ctypes.data for a in pbs])
+    pdims = np.array([list(a.shape) for a in pfs], dtype=np.int64).ravel()
+    p = D._params({"background": 100.0, "dampfactor": 1.0, "scalefactor": 1.0, "deconoffset": 0.0,
+                   "edgeerosion": 0, "save16bit": True, "bbox": None})
+    res = {}
+    for v in ("tuned", "-1", "0", "1", "2"):
+        if v == "tuned":
+            os.environ.pop("PK_TMA_VARIANT", None)
+        else:
+            os.environ["PK_TMA_VARIANT"] = v
+        ctx = _lib.Context(0)
+
+        def run():
+            _lib.check(_lib.lib.pk_batch_decon(ctx.handle, 1, len(chunks), arr, _lib.PK_U16, 3, fptrs, bptrs,
+                                               pdims.ctypes.data, 2, p, 0, 1))
+
+        run()
+        run()
+        torch.cuda.synchronize()
+        ctx.profile(True)
+        run()
+        torch.cuda.synchronize()
+        ctx.profile(False)
+        prof = ctx.profile_read()
+        res[v] = {"total_ms": round(sum(x["ms"] for x in prof.values()), 3),
+                  "passes": {k: round(x["ms"], 3) for k, x in sorted(prof.items())}}
+        if v == "tuned":
+            res[v]["autotune"] = ctx.tune_read()
+        del ctx
+    os.environ.pop("PK_TMA_VARIANT", None)
+    return {"metric": "batched per-pass kernel ms by forced x / z candidate", "workload": "batched_passes",
+            "unit": "ms", "candidates": res,
+            "note": "kinds are pass@transform-length:family (tma, rio = register-IO, rolled / yreg y kernels, "
+                    "-1k = 1024-point tiles); -1 = register-IO forced, 0-2 = TMA variant where the plan has it"}
+
+
 def wl_served(args):
     """Config 4: open-loop Poisson requests (90% chunk sizes, 10% 768x768x384; 80% OMW x2, 20% RL x10;
     3 PSFs; 150 GB budget) through the continuous-batching server, against the same requests run one
@@ -767,7 +834,7 @@ def wl_served(args):
             outs[v.shape] = t.numpy().view(np.uint16).T
     import queue
 
-    def phase(arr):
+    def phase(arr, srv):
         """Submit request i at arrival time arr[i] (seconds from the start); returns (wall s, latencies)."""
         lat = [None] * len(reqs)
         ids = [None] * len(reqs)
@@ -826,14 +893,26 @@ def wl_served(args):
     plain = plain_all()
     _log(f"served: the plain calls one after another took {plain:.2f} s")
     timed0 = sum(1 for r in ctx.tune_read() if r.get("source") == "timed")
-    wall, lat = phase(arrivals)
+    wall, lat = phase(arrivals, srv)
     _log(f"served: {len(reqs)} requests done in {wall:.2f} s")
     # the same requests all at once: the server's throughput when arrivals do not limit it
-    wall_sat, lat_sat = phase(np.zeros(len(reqs)))
+    wall_sat, lat_sat = phase(np.zeros(len(reqs)), srv)
     _log(f"served: {len(reqs)} requests submitted at once done in {wall_sat:.2f} s")
     tuned_in_phases = sum(1 for r in ctx.tune_read() if r.get("source") == "timed") - timed0
     st = srv.stats()
     srv.close()
+    # the same two phases through the device-resident request loop (a dispatcher kernel launches
+    # each admitted request's pass graph from the device)
+    dsrv = SV.Server(ctx, budget_bytes=150e9, max_batch=64, borrow_inputs=True, device_loop=True)
+    for i in range(3):
+        dsrv.add_psf(i, psfs[i], bps[i])
+    for w in [dsrv.submit(v, pid, m, 1, Background=100) for (shp, pid, m), v in seen.items()]:
+        dsrv.wait(w)
+    dwall, dlat = phase(arrivals, dsrv)
+    dwall_sat, dlat_sat = phase(np.zeros(len(reqs)), dsrv)
+    dloop = dsrv.loop_status()
+    dsrv.close()
+    _log(f"served (device loop): {dwall:.2f} s open loop, {dwall_sat:.2f} s all at once")
     plain_after = plain_all()
     _log(f"served: the plain calls again after serving took {plain_after:.2f} s")
     L = np.array(lat)
@@ -851,7 +930,17 @@ def wl_served(args):
                          "speedup_vs_plain": round(plain / wall_sat, 3), "wall_s": round(wall_sat, 3),
                          "latency_ms": {"p50": round(float(np.percentile(lat_sat, 50)), 2),
                                         "p99": round(float(np.percentile(lat_sat, 99)), 2)},
-                         "note": "the same requests submitted at once (throughput not limited by arrivals)"}})
+                         "note": "the same requests submitted at once (throughput not limited by arrivals)"},
+           "device_loop": {"value": round(nvox / dwall / 1e6, 1), "unit": "Mvoxel/s",
+                           "speedup_vs_plain": round(plain / dwall, 3), "wall_s": round(dwall, 3),
+                           "latency_ms": {"p50": round(float(np.percentile(dlat, 50)), 2),
+                                          "p95": round(float(np.percentile(dlat, 95)), 2),
+                                          "p99": round(float(np.percentile(dlat, 99)), 2)},
+                           "saturated": {"value": round(nvox / dwall_sat / 1e6, 1),
+                                         "speedup_vs_plain": round(plain / dwall_sat, 3)},
+                           "dispatcher_instances": dloop["instances"],
+                           "note": "the same requests through the device-resident loop: a dispatcher kernel "
+                                   "launches each admitted request's pass graph from the device"}})
 
 
 DSR = dict(angle=32.45, dz=0.3, xy=0.108, reverse=True)   # the reference demo's deskew / rotate settings
@@ -1046,7 +1135,8 @@ def wl_large(args):
            "reference_cpu": "not run (the float32 CPU restatement needs ~100 GB of host RAM for this volume)"})
 
 
-WORKLOADS = {"rl_small": wl_rl_small, "batched": wl_batched, "served": wl_served, "large": wl_large, "dsr": wl_dsr}
+WORKLOADS = {"rl_small": wl_rl_small, "batched": wl_batched, "batched_passes": wl_batched_passes, "served": wl_served,
+             "large": wl_large, "dsr": wl_dsr}
 
 if __name__ == "__main__":
     main()

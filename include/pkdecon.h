@@ -349,6 +349,14 @@ typedef struct {
     int32_t queue_capacity;    /* max queued (not yet admitted) requests */
     int32_t borrow_inputs;     /* 0: copy each volume at submit; 1: read the caller's buffer (keep it
                                   valid, ideally pinned, until pk_server_wait returns) */
+    int32_t device_loop;       /* 0: a host scheduler thread runs rounds of shared pass launches;
+                                  1: device-resident loop: a dispatcher kernel takes each admitted
+                                  request's whole pass program (a device-launchable graph) from a ring
+                                  in page-locked memory and launches it from the device */
+    int32_t heartbeat_ms;      /* device loop: a dispatcher returns when the host's heartbeat has
+                                  stalled this long (default 2000; the host restarts it with work) */
+    int32_t idle_us;           /* device loop: a dispatcher returns after this long without a new
+                                  request (default 2000) */
 } pk_server_config;
 
 /* Register a PSF pair (psf_b NULL for RL-only) under psf_id; OTFs are cached per (psf_id, size). */
@@ -366,6 +374,13 @@ PK_API pk_status pk_server_cancel(pk_server* s, int64_t id);
 /* stats[0..3] = completed, rejected, peak in-flight bytes, rounds run. */
 PK_API pk_status pk_server_stats(pk_server* s, int64_t stats[4]);
 PK_API void pk_server_destroy(pk_server* s);
+/* Device loop: *running = 1 while a dispatcher instance runs, *exit_code = why the last one returned
+ * (0 none yet, 1 stopped, 2 launch budget used up, 3 host heartbeat stalled, 4 idle), *instances = dispatcher
+ * instances started.  PK_ERR_UNSUPPORTED for a host-scheduler server. */
+PK_API pk_status pk_server_loop_status(pk_server* s, int32_t* running, int32_t* exit_code, int64_t* instances);
+/* Test hook of the device loop's bounded wait: pause = 1 stops the scheduler's heartbeat (a running
+ * dispatcher returns with exit code 3 within heartbeat_ms), 0 resumes it. */
+PK_API pk_status pk_server_pause_heartbeat(pk_server* s, int32_t pause);
 
 #ifdef __cplusplus
 }

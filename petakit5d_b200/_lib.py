@@ -46,7 +46,8 @@ class Chunk(C.Structure):
 
 class ServerConfig(C.Structure):
     _fields_ = [("budget_bytes", C.c_int64), ("max_batch", C.c_int32), ("queue_capacity", C.c_int32),
-                ("borrow_inputs", C.c_int32)]
+                ("borrow_inputs", C.c_int32), ("device_loop", C.c_int32), ("heartbeat_ms", C.c_int32),
+                ("idle_us", C.c_int32)]
 
 
 I64x3 = C.c_int64 * 3
@@ -119,6 +120,8 @@ _SIGS = {
     "pk_server_cancel": (C.c_int, [P, C.c_int64]),
     "pk_server_stats": (C.c_int, [P, C.c_int64 * 4]),
     "pk_server_destroy": (None, [P]),
+    "pk_server_loop_status": (C.c_int, [P, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int64)]),
+    "pk_server_pause_heartbeat": (C.c_int, [P, C.c_int32]),
 }
 
 EXPORTED = tuple(_SIGS)

@@ -60,9 +60,11 @@ def build(verbose=False, extra_flags=(), checked=False):
 
     def compile_one(src):
         path = os.path.join(CSRC, src)
-        obj = os.path.join(OBJDIR, f"{src}.{_digest(path, flags)}.o")
+        # *_rdc.cu launch graphs from the device: relocatable device code, device-linked below
+        fl = flags + (["-rdc=true"] if src.endswith("_rdc.cu") else [])
+        obj = os.path.join(OBJDIR, f"{src}.{_digest(path, fl)}.o")
         if not os.path.exists(obj):
-            cmd = [nvcc, *flags, "-I", os.path.join(ROOT, "include"), "-c", path, "-o", obj]
+            cmd = [nvcc, *fl, "-I", os.path.join(ROOT, "include"), "-c", path, "-o", obj]
             if verbose:
                 print(" ".join(cmd), flush=True)
             r = subprocess.run(cmd, capture_output=True, text=True)
@@ -74,8 +76,18 @@ def build(verbose=False, extra_flags=(), checked=False):
 
     with ThreadPoolExecutor(max_workers=min(8, len(srcs))) as ex:
         objs = list(ex.map(compile_one, srcs))
+    rdc = [o for o, src in zip(objs, srcs) if src.endswith("_rdc.cu")]
+    if rdc:
+        dlink = os.path.join(OBJDIR, "dlink." + hashlib.sha256("".join(rdc).encode()).hexdigest()[:16] + ".o")
+        cmd = [nvcc, "-dlink", "-gencode", "arch=compute_100a,code=sm_100a", "-Xcompiler", "-fPIC", "-o", dlink,
+               *rdc, "-lcudadevrt"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"device link failed:\n{r.stdout}\n{r.stderr}")
+        objs = objs + [dlink]
     tmp = lib_path + ".tmp"
-    cmd = [nvcc, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-cudart", "static", "-o", tmp, *objs, "-lz"]
+    cmd = [nvcc, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-cudart", "static", "-o", tmp, *objs,
+           "-lcudadevrt", "-lz"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")

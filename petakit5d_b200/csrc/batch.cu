@@ -106,13 +106,29 @@ extern "C" pk_status pk_batch_decon(pk_ctx* ctx, int32_t method, int32_t n, cons
         if (A.dims[1] != Bp.dims[1]) return A.dims[1] < Bp.dims[1];
         return A.dims[2] < Bp.dims[2];
     });
+    if (!device && n >= 4 * max_per_wave) {
+        // host mode: the first wave's upload and the last wave's download are not hidden behind any
+        // compute, so both waves take the smallest chunks (the smallest half-wave first, the next
+        // smallest half-wave last); the waves between stay ordered by size
+        const int h = std::max(1, max_per_wave / 2);
+        std::vector<int> o2(order.begin(), order.begin() + h);
+        o2.insert(o2.end(), order.begin() + 2 * h, order.end());
+        o2.insert(o2.end(), order.begin() + h, order.begin() + 2 * h);
+        order.swap(o2);
+    }
     std::vector<std::vector<int>> waves;
     {
         std::vector<int> cur;
         size_t cb = 0;
         for (int oi = 0; oi < n; oi++) {
             const int i = order[oi];
+            const bool last_h = !device && n >= 4 * max_per_wave && oi == n - std::max(1, max_per_wave / 2);
             const int cap = (!device && waves.empty()) ? std::max(1, max_per_wave / 2) : max_per_wave;
+            if (last_h && !cur.empty()) {   // the smallest chunks' second half-wave is a wave of its own
+                waves.push_back(cur);
+                cur.clear();
+                cb = 0;
+            }
             if (!cur.empty() && (cb + plans[i].work_b > budget || (int)cur.size() >= cap)) {
                 waves.push_back(cur);
                 cur.clear();

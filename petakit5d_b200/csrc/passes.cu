@@ -293,8 +293,8 @@ int time_candidates(pk_ctx* ctx, const PkStep& s, const VolDesc& d0, int nrep, i
     const size_t poff = moff + (size_t)nrep * sizeof(XZMaps);
     const size_t blob = poff + sizeof(int) * (nrep + 1);
     const size_t soff = (blob + 255) & ~(size_t)255;
-    char* d = nullptr;
-    if (cudaMalloc(&d, soff + per * nrep) != cudaSuccess) {
+    char* d = nullptr;   // stream-ordered: a device-wide synchronisation here would wait on a serving dispatcher
+    if (cudaMallocAsync((void**)&d, soff + per * nrep, st) != cudaSuccess) {
         cudaGetLastError();
         return -2;
     }
@@ -367,10 +367,10 @@ int time_candidates(pk_ctx* ctx, const PkStep& s, const VolDesc& d0, int nrep, i
         cudaGetLastError();
         best = -2;
     }
+    cudaFreeAsync(d, st);
     cudaStreamSynchronize(st);
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
-    cudaFree(d);
     cudaGetLastError();
     return best;
 }
@@ -937,8 +937,16 @@ static pk_status launch_steps(pk_ctx* ctx, const PkProgram& prog, cudaStream_t s
 
 // The program's launches as a graph of kernel nodes in launch order, built node by node (no stream
 // capture, so other threads' CUDA calls cannot disturb it).
+// A device-launched request graph's last node: every pass before it is done.
+__global__ void k_req_done(int* done) {
+    if (threadIdx.x == 0) {
+        __threadfence_system();
+        *(volatile int*)done = 1;
+    }
+}
+
 static bool build_graph(const PkProgram& prog, const VolDesc* d_desc, const int* d_prefix, const XZMaps* d_maps,
-                        int* d_err, cudaGraphExec_t* out) {
+                        int* d_err, cudaGraphExec_t* out, unsigned long long flags = 0, int* d_done = nullptr) {
     const pkpass::KernelTable& kt = kernels();
     cudaGraph_t g = nullptr;
     if (cudaGraphCreate(&g, 0) != cudaSuccess) { cudaGetLastError(); return false; }
@@ -992,8 +1000,18 @@ static bool build_graph(const PkProgram& prog, const VolDesc* d_desc, const int*
         }
         prev = node;
     }
+    if (ok && d_done) {
+        cudaKernelNodeParams p = {};
+        void* args[] = {(void*)&d_done};
+        p.func = (void*)k_req_done;
+        p.gridDim = dim3(1);
+        p.blockDim = dim3(32);
+        p.kernelParams = args;
+        cudaGraphNode_t node = nullptr;
+        ok = cudaGraphAddKernelNode(&node, g, prev ? &prev : nullptr, prev ? 1 : 0, &p) == cudaSuccess;
+    }
     if (ok) {
-        const cudaError_t ei = cudaGraphInstantiate(out, g, 0);
+        const cudaError_t ei = cudaGraphInstantiate(out, g, flags);
         if (ei != cudaSuccess) {
             if (getenv("PK_DEBUG_GRAPHS")) fprintf(stderr, "graph instantiate: %s\n", cudaGetErrorString(ei));
             ok = false;
@@ -1118,6 +1136,40 @@ pk_status pk_program_launch(pk_ctx* ctx, PkProgram& prog, cudaStream_t st) {
         PK_CUDA(cudaEventRecord(sl.ev, st));
         sl.used = true;
     }
+    return PK_OK;
+}
+
+pk_status pk_program_device_graph(pk_ctx* ctx, PkProgram& prog, cudaStream_t st, int* d_done,
+                                  const std::function<void*(size_t)>& host_blob, void** d_blob, cudaGraphExec_t* out) {
+    *d_blob = nullptr;
+    for (VolDesc& d : prog.descs) d.chk = ctx && ctx->d_err ? ctx->d_err + 1 : nullptr;
+    assign_tma(ctx, prog, st);
+    size_t dbytes, moff, need;
+    blob_layout(prog, &dbytes, &moff, &need);
+    void* h = host_blob(need);
+    void* d = nullptr;
+    if (!h || cudaMallocAsync(&d, need, st) != cudaSuccess) {
+        cudaGetLastError();
+        return pk_fail(PK_ERR_NOMEM, "request graph descriptors: allocation failed");
+    }
+    blob_fill(prog, h);
+    cudaError_t e = cudaMemcpyAsync(d, h, need, cudaMemcpyHostToDevice, st);
+    bool ok = e == cudaSuccess && build_graph(prog, (const VolDesc*)d, (const int*)((char*)d + dbytes),
+                                              (const XZMaps*)((char*)d + moff), ctx->d_err, out,
+                                              cudaGraphInstantiateFlagDeviceLaunch, d_done);
+    if (ok) {
+        e = cudaGraphUpload(*out, st);
+        if (e != cudaSuccess) {
+            cudaGraphExecDestroy(*out);
+            ok = false;
+        }
+    }
+    if (!ok) {
+        cudaGetLastError();
+        cudaFreeAsync(d, st);
+        return pk_fail(PK_ERR_CUDA, "request graph: device-launch instantiation failed");
+    }
+    *d_blob = d;
     return PK_OK;
 }
 

@@ -268,6 +268,36 @@ pk_status pk_program_launch_range(pk_ctx* ctx, PkProgram& prog, cudaStream_t st,
 double pk_step_bytes(const PkStep& s, const VolDesc* descs);
 const char* pk_step_name(const PkStep& s);
 int pk_program_kernel_count(const PkProgram& prog);
+// The program as a graph that a kernel can launch (the server's device loop): its descriptors in a
+// device blob of its own (*d_blob, stream-ordered allocation on st, copied there from a page-locked
+// buffer of host_blob(bytes); both must outlive the graph's run), then a node that sets
+// *d_done = 1 (page-locked host memory) when every pass is done; instantiated for device launch and
+// uploaded on st.
+pk_status pk_program_device_graph(pk_ctx* ctx, PkProgram& prog, cudaStream_t st, int* d_done,
+                                  const std::function<void*(size_t)>& host_blob, void** d_blob, cudaGraphExec_t* out);
+
+// Device-resident request loop (serve.cu host side, dloop_rdc.cu dispatcher).  The ring lives in
+// page-locked host memory: the host appends ready requests' graphs at `tail`; a dispatcher kernel
+// takes them at `head` and launches each fire-and-forget from the device.
+constexpr int kDlRingCap = 1024;
+constexpr int kDlLaunchBudget = 112;   // graphs one dispatcher launches (the device runtime allows 120)
+enum DlExit : int { DL_NONE = 0, DL_STOPPED = 1, DL_BUDGET = 2, DL_HEARTBEAT = 3, DL_IDLE = 4 };
+struct DlRing {
+    volatile long long tail;             // host: entries appended
+    volatile long long head;             // dispatcher: entries launched
+    volatile long long heartbeat;        // host: bumped by the scheduler thread while it runs
+    volatile long long heartbeat_ns;     // host: a dispatcher returns when the heartbeat stalls this long
+    volatile long long idle_ns;          // host: a dispatcher returns after this long without an entry
+    volatile long long epoch_launched;   // host: dispatcher instances started
+    volatile long long epoch_ended;      // dispatcher: instances that have returned
+    volatile int stop;                   // host: dispatchers return
+    volatile int exit_code;              // dispatcher: why the last instance returned (DlExit)
+    cudaGraphExec_t graph[kDlRingCap];
+    volatile int status[kDlRingCap];     // dispatcher: 1 + cudaError of the entry's launch
+    volatile int epoch[kDlRingCap];      // dispatcher: the instance that launched the entry
+};
+// One dispatcher instance as a (host-launched) graph of one kernel on ring d_ring.
+pk_status pk_dloop_instance(DlRing* d_ring, cudaStream_t st, cudaGraphExec_t* out);
 
 // scratch buffers
 pk_status pk_scratch(pk_ctx* ctx, int slot, size_t bytes, void** ptr);

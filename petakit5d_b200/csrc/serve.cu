@@ -10,6 +10,17 @@
 // Request volumes are staged in pinned memory at submit and uploaded on a copy stream; the client
 // that waits for a request copies its result out and releases the request's device memory.
 // All waits are host-side with timeouts; no kernel waits on another.
+//
+// With device_loop set the request loop is device-resident instead: admission, allocation and the
+// uploads stay on the host, but each admitted request's whole pass program becomes a graph that a
+// dispatcher kernel (dloop_rdc.cu) takes from a ring in page-locked memory and launches from the
+// device as soon as its input is on the GPU; requests then overlap as independent graphs rather
+// than sharing launches.  The last node of a request's graph sets its done flag in page-locked
+// memory, which the scheduler thread polls.  The dispatcher's waits are bounded (stop flag, launch
+// budget, idle time, the scheduler's heartbeat); the host starts a new dispatcher instance when the
+// last one has returned and requests are pending.  Nothing on the scheduler's path synchronises the
+// whole device (page-locked staging buffers are pooled, not freed, and device memory is freed
+// stream-ordered), so the host side never waits on a running dispatcher.
 #include <algorithm>
 #include <atomic>
 #include <chrono>
@@ -50,6 +61,7 @@ enum ReqState { RQ_QUEUED, RQ_ACTIVE, RQ_DONE, RQ_FAILED, RQ_CANCELLED };
 struct Request {
     int64_t id;
     uint16_t* vol = nullptr;         // pinned staging copy of the input (copy mode)
+    size_t vol_cap = 0;              // its capacity (pooled buffers can be larger)
     const uint16_t* src = nullptr;   // the bytes the upload reads (staging copy or the caller's buffer)
     size_t vol_bytes = 0;
     int64_t dims[3];
@@ -70,6 +82,13 @@ struct Request {
     bool last_queued = false;
     bool uploading = false;          // input still on its way to the device
     bool collected = false;          // the waiter took the result
+    // device loop: the request's graph, its descriptor blob and done flag, its ring entry
+    cudaGraphExec_t gexec = nullptr;
+    void* gblob_d = nullptr;
+    void* gblob_h = nullptr;
+    size_t gblob_cap = 0;
+    int done_slot = -1;
+    long long ring_idx = -1;
 };
 
 size_t al256(size_t b) { return (b + 255) & ~(size_t)255; }
@@ -91,13 +110,44 @@ struct pk_server {
     int64_t completed = 0, rejected = 0, rounds = 0;
     size_t inflight = 0, peak_inflight = 0;
     cudaStream_t up = nullptr, down = nullptr;
+    // device loop
+    static constexpr int kInstances = 16;
+    static constexpr int kDoneSlots = 4096;
+    DlRing* ring = nullptr;           // page-locked, mapped
+    DlRing* d_ring = nullptr;
+    int* done_h = nullptr;            // page-locked, mapped: one flag per slot
+    int* done_d = nullptr;
+    std::vector<int> free_done;
+    cudaStream_t dl_st[kInstances] = {};
+    cudaGraphExec_t dl_exec[kInstances] = {};
+    cudaEvent_t dl_ev[kInstances] = {};
+    long long dl_epoch_of[kInstances] = {};   // the instance each stream ran last (0: none)
+    int dl_next = 0;
+    std::atomic<bool> hb_paused{false};
+    // graphs and blobs of finished requests, freed once the dispatcher instance that launched them
+    // has completed (its completion includes every graph it launched)
+    struct Retired { long long epoch; cudaGraphExec_t g; void* d; void* h; size_t cap; };
+    std::vector<Retired> retired;
+    std::multimap<size_t, void*> blob_pool;   // page-locked descriptor staging buffers by capacity
+    std::multimap<size_t, void*> stage_pool;  // page-locked input staging buffers (copy mode) by capacity
+    int64_t instances = 0;
 
     void loop();
+    void loop_device();
+    pk_status setup_device_loop();
+    void retire(const std::shared_ptr<Request>& r);
+    void free_retired(bool all);
     pk_status admit(const std::shared_ptr<Request>& r);
     void build_steps(Request& r, const VolDesc& base, const float2* otf_f, const float2* otf_b);
     void finish(const std::shared_ptr<Request>& r, pk_status st, const std::string& msg);
     void release(const std::shared_ptr<Request>& r);
+    void stage_return(void* p, size_t cap);
 };
+
+void pk_server::stage_return(void* p, size_t cap) {
+    if (stage_pool.size() < 256) stage_pool.emplace(cap, p);
+    else cudaFreeHost(p);   // pool full (rare: hundreds of distinct sizes in flight)
+}
 
 void pk_server::release(const std::shared_ptr<Request>& r) {
     if (r->dev) {
@@ -105,8 +155,8 @@ void pk_server::release(const std::shared_ptr<Request>& r) {
         inflight -= r->dev_bytes;
         r->dev = nullptr;
     }
-    if (r->vol) {
-        cudaFreeHost(r->vol);
+    if (r->vol) {   // back to the staging pool: freeing page-locked memory would synchronise the device
+        stage_return(r->vol, r->vol_cap);
         r->vol = nullptr;
     }
     if (r->ev_up) { cudaEventDestroy(r->ev_up); r->ev_up = nullptr; }
@@ -119,7 +169,7 @@ void pk_server::finish(const std::shared_ptr<Request>& r, pk_status st, const st
     r->msg = msg;
     if (st != PK_OK) release(r);
     else if (r->vol) {
-        cudaFreeHost(r->vol);
+        stage_return(r->vol, r->vol_cap);
         r->vol = nullptr;
     }
     if (r->state != RQ_CANCELLED) r->state = st == PK_OK ? RQ_DONE : RQ_FAILED;
@@ -236,8 +286,211 @@ pk_status pk_server::admit(const std::shared_ptr<Request>& r) {
     PK_CUDA(cudaEventRecord(r->ev_up, up));
     r->uploading = true;
     build_steps(*r, b, of, ob);
+    if (cfg.device_loop) {
+        // the whole pass program as one device-launchable graph, ready once its input has landed
+        if (free_done.empty()) return pk_fail(PK_ERR_BUSY, "no free completion flag");
+        PkProgram prog;
+        for (const Step& st : r->steps) pk_program_add(prog, st.kind, st.mode, {st.d});
+        r->steps.clear();
+        r->done_slot = free_done.back();
+        free_done.pop_back();
+        done_h[r->done_slot] = 0;
+        auto host_blob = [&](size_t need) -> void* {
+            auto it = blob_pool.lower_bound(need);
+            if (it != blob_pool.end()) {
+                r->gblob_h = it->second;
+                r->gblob_cap = it->first;
+                blob_pool.erase(it);
+                return r->gblob_h;
+            }
+            const size_t cap = std::max<size_t>(4096, need);
+            if (cudaMallocHost(&r->gblob_h, cap) != cudaSuccess) {
+                cudaGetLastError();
+                r->gblob_h = nullptr;
+                return nullptr;
+            }
+            r->gblob_cap = cap;
+            return r->gblob_h;
+        };
+        s = pk_program_device_graph(c, prog, up, done_d + r->done_slot, host_blob, &r->gblob_d, &r->gexec);
+        if (s != PK_OK) {
+            retire(r);
+            return s;
+        }
+        PK_CUDA(cudaEventRecord(r->ev_up, up));   // input, descriptors and graph are on the device
+    }
     r->state = RQ_ACTIVE;
     return PK_OK;
+}
+
+void pk_server::retire(const std::shared_ptr<Request>& r) {
+    if (r->done_slot >= 0) {
+        free_done.push_back(r->done_slot);
+        r->done_slot = -1;
+    }
+    if (r->gexec || r->gblob_d || r->gblob_h) {
+        long long ep = 0;   // never launched: free at once
+        if (r->ring_idx >= 0 && ring->head > r->ring_idx) ep = ring->epoch[r->ring_idx % kDlRingCap];
+        retired.push_back(Retired{ep, r->gexec, r->gblob_d, r->gblob_h, r->gblob_cap});
+        r->gexec = nullptr;
+        r->gblob_d = r->gblob_h = nullptr;
+    }
+}
+
+// Frees retired request graphs whose dispatcher instance has completed (an instance's execution
+// completes only after every graph it launched); `all` after the dispatcher streams are drained.
+void pk_server::free_retired(bool all) {
+    for (auto it = retired.begin(); it != retired.end();) {
+        bool ok = all || it->epoch == 0;
+        if (!ok) {
+            ok = true;   // a stream that has moved on to a later instance finished this one first
+            for (int j = 0; j < kInstances; j++)
+                if (dl_epoch_of[j] == it->epoch) {
+                    ok = cudaEventQuery(dl_ev[j]) == cudaSuccess;
+                    if (!ok) cudaGetLastError();
+                    break;
+                }
+        }
+        if (!ok) {
+            ++it;
+            continue;
+        }
+        if (it->g) cudaGraphExecDestroy(it->g);
+        if (it->d) cudaFreeAsync(it->d, up);
+        if (it->h) blob_pool.emplace(it->cap, it->h);
+        it = retired.erase(it);
+    }
+}
+
+pk_status pk_server::setup_device_loop() {
+    PK_CUDA(cudaHostAlloc((void**)&ring, sizeof(DlRing), cudaHostAllocMapped));
+    memset((void*)ring, 0, sizeof(DlRing));
+    ring->heartbeat_ns = (long long)cfg.heartbeat_ms * 1000000LL;
+    ring->idle_ns = (long long)cfg.idle_us * 1000LL;
+    PK_CUDA(cudaHostGetDevicePointer((void**)&d_ring, (void*)ring, 0));
+    PK_CUDA(cudaHostAlloc((void**)&done_h, sizeof(int) * kDoneSlots, cudaHostAllocMapped));
+    memset(done_h, 0, sizeof(int) * kDoneSlots);
+    PK_CUDA(cudaHostGetDevicePointer((void**)&done_d, done_h, 0));
+    for (int i = kDoneSlots - 1; i >= 0; i--) free_done.push_back(i);
+    for (int k = 0; k < kInstances; k++) {
+        PK_CUDA(cudaStreamCreateWithFlags(&dl_st[k], cudaStreamNonBlocking));
+        PK_CUDA(cudaEventCreateWithFlags(&dl_ev[k], cudaEventDisableTiming));
+        pk_status s = pk_dloop_instance(d_ring, dl_st[k], &dl_exec[k]);
+        if (s != PK_OK) return s;
+    }
+    return PK_OK;
+}
+
+// The device-resident loop's host side: admission and uploads as in loop(), then ready requests go
+// to the ring, a dispatcher instance is started when the last one has returned and entries wait,
+// and finished requests are found by their done flags.
+void pk_server::loop_device() {
+    cudaSetDevice(ctx->device);
+    while (!stop.load()) {
+        std::unique_lock<std::mutex> lk(mu);
+        if (!hb_paused.load()) ring->heartbeat = ring->heartbeat + 1;
+        const long long head = ring->head;
+        for (auto it = active.begin(); it != active.end();) {
+            auto& r = *it;
+            bool gone = false;
+            if (r->ring_idx >= 0) {
+                const int i = (int)(r->ring_idx % kDlRingCap);
+                const int launch = head > r->ring_idx ? ring->status[i] : 0;
+                if (launch > 1) {
+                    finish(r, PK_ERR_CUDA, std::string("device launch of the request's graph failed: ") +
+                                               cudaGetErrorString((cudaError_t)(launch - 1)));
+                    gone = true;
+                } else if (launch == 1 && done_h[r->done_slot]) {
+                    // a bounded device wait that ran out (context status word) fails the request
+                    const pk_status ws = pk_check_device_waits(ctx);
+                    if (r->state == RQ_CANCELLED) finish(r, PK_ERR_CANCELLED, "cancelled");
+                    else finish(r, ws, ws == PK_OK ? "" : pk_last_error());
+                    gone = true;
+                }
+            } else if (r->state == RQ_CANCELLED) {   // not handed to the device yet
+                cudaStreamSynchronize(up);
+                finish(r, PK_ERR_CANCELLED, "cancelled");
+                gone = true;
+            }
+            if (gone) {
+                retire(r);
+                it = active.erase(it);
+            } else {
+                ++it;
+            }
+        }
+        while (!queue.empty() && (int)active.size() < cfg.max_batch) {
+            auto r = queue.front();
+            if (r->state == RQ_CANCELLED) {
+                queue.pop_front();
+                finish(r, PK_ERR_CANCELLED, "cancelled");
+                continue;
+            }
+            VolDesc tmp;
+            size_t need = 0;
+            {
+                std::lock_guard<std::recursive_mutex> cl(ctx->mu);
+                if (pk_init_desc(ctx, (int)r->dims[0], (int)r->dims[1], (int)r->dims[2], &tmp) == PK_OK) {
+                    const int dims[3] = {tmp.ny, tmp.nx, tmp.nz};
+                    need = pk_job_bytes(r->method, dims, false, tmp.blocksY) + 4 * (size_t)tmp.nrows * tmp.ny;
+                }
+            }
+            if (inflight + need > (size_t)cfg.budget_bytes && !active.empty()) break;   // wait for memory
+            queue.pop_front();
+            pk_status s;
+            {
+                std::lock_guard<std::recursive_mutex> cl(ctx->mu);
+                s = admit(r);
+            }
+            if (s != PK_OK) {
+                finish(r, s, pk_last_error());
+                retire(r);
+                continue;
+            }
+            active.push_back(r);
+        }
+        // requests whose input, descriptors and graph are on the device join the ring
+        for (auto& r : active) {
+            if (r->ring_idx >= 0 || r->state == RQ_CANCELLED) continue;
+            const cudaError_t q = cudaEventQuery(r->ev_up);
+            if (q == cudaErrorNotReady) {
+                cudaGetLastError();
+                continue;
+            }
+            if (ring->tail - ring->head >= kDlRingCap) break;
+            const long long t = ring->tail;
+            ring->graph[t % kDlRingCap] = r->gexec;
+            ring->status[t % kDlRingCap] = 0;
+            std::atomic_thread_fence(std::memory_order_seq_cst);
+            ring->tail = t + 1;
+            r->ring_idx = t;
+        }
+        // a dispatcher instance for waiting entries, once the previous one has returned
+        if (ring->tail > ring->head && ring->epoch_ended == ring->epoch_launched) {
+            for (int k = 0; k < kInstances; k++) {
+                const int j = (dl_next + k) % kInstances;
+                if (dl_epoch_of[j] && cudaEventQuery(dl_ev[j]) != cudaSuccess) {
+                    cudaGetLastError();
+                    continue;
+                }
+                const long long ep = ring->epoch_launched + 1;
+                ring->epoch_launched = ep;
+                std::atomic_thread_fence(std::memory_order_seq_cst);
+                if (cudaGraphLaunch(dl_exec[j], dl_st[j]) != cudaSuccess || cudaEventRecord(dl_ev[j], dl_st[j]) != cudaSuccess) {
+                    cudaGetLastError();
+                    ring->epoch_launched = ep - 1;
+                    break;
+                }
+                dl_epoch_of[j] = ep;
+                dl_next = (j + 1) % kInstances;
+                instances++;
+                rounds++;
+                break;
+            }
+        }
+        free_retired(false);
+        cv_work.wait_for(lk, std::chrono::microseconds(200));
+    }
 }
 
 void pk_server::loop() {
@@ -355,6 +608,9 @@ pk_server* pk_server_create(pk_ctx* ctx, const pk_server_config* cfg) {
     s->cfg.max_batch = cfg && cfg->max_batch > 0 ? cfg->max_batch : 64;
     s->cfg.queue_capacity = cfg && cfg->queue_capacity > 0 ? cfg->queue_capacity : 1024;
     s->cfg.borrow_inputs = cfg ? cfg->borrow_inputs : 0;
+    s->cfg.device_loop = cfg ? cfg->device_loop : 0;
+    s->cfg.heartbeat_ms = cfg && cfg->heartbeat_ms > 0 ? cfg->heartbeat_ms : 2000;
+    s->cfg.idle_us = cfg && cfg->idle_us > 0 ? cfg->idle_us : 2000;
     cudaSetDevice(ctx->device);
     {
         // request buffers come from the device's stream-ordered pool; keep freed blocks in the pool
@@ -372,7 +628,14 @@ pk_server* pk_server_create(pk_ctx* ctx, const pk_server_config* cfg) {
         delete s;
         return nullptr;
     }
-    s->th = std::thread([s] { s->loop(); });
+    if (s->cfg.device_loop && s->setup_device_loop() != PK_OK) {
+        const std::string m = pk_last_error();
+        pk_server_destroy(s);
+        pk_set_error(m);
+        return nullptr;
+    }
+    if (s->cfg.device_loop) s->th = std::thread([s] { s->loop_device(); });
+    else s->th = std::thread([s] { s->loop(); });
     return s;
 }
 
@@ -420,10 +683,23 @@ int64_t pk_server_submit(pk_server* s, const uint16_t* vol, const int64_t dims[3
     if (s->cfg.borrow_inputs) {
         r->src = vol;
     } else {
-        cudaSetDevice(s->ctx->device);
-        if (cudaMallocHost(&r->vol, r->vol_bytes) != cudaSuccess) {
-            cudaGetLastError();
-            return -(int64_t)pk_fail(PK_ERR_NOMEM, "pinned staging allocation failed");
+        {   // a pooled page-locked staging buffer, else a new one
+            std::lock_guard<std::mutex> pl(s->mu);
+            auto it = s->stage_pool.lower_bound(r->vol_bytes);
+            if (it != s->stage_pool.end() && it->first <= 2 * r->vol_bytes) {
+                r->vol = (uint16_t*)it->second;
+                r->vol_cap = it->first;
+                s->stage_pool.erase(it);
+            }
+        }
+        if (!r->vol) {
+            cudaSetDevice(s->ctx->device);
+            if (cudaMallocHost(&r->vol, r->vol_bytes) != cudaSuccess) {
+                cudaGetLastError();
+                r->vol = nullptr;
+                return -(int64_t)pk_fail(PK_ERR_NOMEM, "pinned staging allocation failed");
+            }
+            r->vol_cap = r->vol_bytes;
         }
         memcpy(r->vol, vol, r->vol_bytes);
         r->src = r->vol;
@@ -498,11 +774,54 @@ pk_status pk_server_stats(pk_server* s, int64_t stats[4]) {
     return PK_OK;
 }
 
+pk_status pk_server_loop_status(pk_server* s, int32_t* running, int32_t* exit_code, int64_t* instances) {
+    if (!s) return pk_fail(PK_ERR_INVALID, "null server");
+    if (!s->ring) return pk_fail(PK_ERR_UNSUPPORTED, "the server runs the host scheduler (device_loop = 0)");
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (running) *running = s->ring->epoch_ended != s->ring->epoch_launched ? 1 : 0;
+    if (exit_code) *exit_code = s->ring->exit_code;
+    if (instances) *instances = s->instances;
+    return PK_OK;
+}
+
+pk_status pk_server_pause_heartbeat(pk_server* s, int32_t pause) {
+    if (!s) return pk_fail(PK_ERR_INVALID, "null server");
+    if (!s->ring) return pk_fail(PK_ERR_UNSUPPORTED, "the server runs the host scheduler (device_loop = 0)");
+    s->hb_paused.store(pause != 0);
+    return PK_OK;
+}
+
 void pk_server_destroy(pk_server* s) {
     if (!s) return;
     s->stop.store(true);
     s->cv_work.notify_all();
     if (s->th.joinable()) s->th.join();
+    if (s->ring) {
+        // dispatchers return at their next poll; then their streams drain every graph they launched
+        cudaSetDevice(s->ctx->device);
+        s->ring->stop = 1;
+        const auto t0 = clk::now();
+        while (s->ring->epoch_ended != s->ring->epoch_launched &&
+               clk::now() - t0 < std::chrono::milliseconds(s->cfg.heartbeat_ms + 2000))
+            std::this_thread::sleep_for(std::chrono::microseconds(200));
+        for (int k = 0; k < pk_server::kInstances; k++)
+            if (s->dl_st[k]) cudaStreamSynchronize(s->dl_st[k]);
+        std::lock_guard<std::mutex> lk(s->mu);
+        for (auto& r : s->active) s->retire(r);
+        s->free_retired(true);
+        if (s->up) cudaStreamSynchronize(s->up);
+        for (auto& kv : s->blob_pool) cudaFreeHost(kv.second);
+        s->blob_pool.clear();
+        for (int k = 0; k < pk_server::kInstances; k++) {
+            if (s->dl_exec[k]) cudaGraphExecDestroy(s->dl_exec[k]);
+            if (s->dl_ev[k]) cudaEventDestroy(s->dl_ev[k]);
+            if (s->dl_st[k]) cudaStreamDestroy(s->dl_st[k]);
+        }
+        cudaFreeHost((void*)s->ring);
+        s->ring = nullptr;
+        if (s->done_h) cudaFreeHost(s->done_h);
+        s->done_h = nullptr;
+    }
     {
         std::lock_guard<std::recursive_mutex> cl(s->ctx->mu);
         cudaSetDevice(s->ctx->device);
@@ -512,6 +831,8 @@ void pk_server_destroy(pk_server* s) {
         for (auto& r : s->queue) s->release(r);
         for (auto& r : s->active) s->release(r);
         cudaStreamSynchronize(s->ctx->stream);
+        for (auto& kv : s->stage_pool) cudaFreeHost(kv.second);
+        s->stage_pool.clear();
         cudaStreamDestroy(s->up);
         cudaStreamDestroy(s->down);
     }

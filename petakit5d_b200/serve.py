@@ -6,8 +6,10 @@
     out, latency_ms = srv.wait(rid)
 
 Requests that arrive while others are on the GPU are admitted at the next round as memory frees
-up; their passes share launches with the running requests.  A result is bitwise the same as the
-plain drop-in call's on the same inputs.
+up; their passes share launches with the running requests.  With device_loop=True the request loop
+is device-resident: a dispatcher kernel launches each admitted request's whole pass program (a
+device-launchable graph) from the device as soon as its input is on the GPU.  A result is bitwise
+the same as the plain drop-in call's on the same inputs.
 """
 from __future__ import annotations
 
@@ -21,11 +23,16 @@ from .decon import _params, _parse
 
 
 class Server:
-    def __init__(self, ctx=None, budget_bytes=150e9, max_batch=64, queue_capacity=1024, borrow_inputs=False):
+    def __init__(self, ctx=None, budget_bytes=150e9, max_batch=64, queue_capacity=1024, borrow_inputs=False,
+                 device_loop=False, heartbeat_ms=2000, idle_us=2000):
         """borrow_inputs: read each submitted array in place (keep it alive and unchanged, ideally in
-        pinned memory, until wait() returns) instead of copying it at submit."""
+        pinned memory, until wait() returns) instead of copying it at submit.  device_loop: run the
+        device-resident request loop (a dispatcher kernel launches each admitted request's pass graph
+        from the device) instead of the host scheduler's rounds; heartbeat_ms and idle_us bound the
+        dispatcher's waits on the host."""
         self.ctx = ctx or _lib.default_context()
-        cfg = ServerConfig(int(budget_bytes), int(max_batch), int(queue_capacity), 1 if borrow_inputs else 0)
+        cfg = ServerConfig(int(budget_bytes), int(max_batch), int(queue_capacity), 1 if borrow_inputs else 0,
+                           1 if device_loop else 0, int(heartbeat_ms), int(idle_us))
         self._borrowed = {}
         h = lib.pk_server_create(self.ctx.handle, cfg)
         if not h:
@@ -75,6 +82,17 @@ class Server:
 
     def cancel(self, rid):
         check(lib.pk_server_cancel(self.handle, int(rid)))
+
+    def loop_status(self):
+        """Device loop: {"running", "exit_code" (0 none, 1 stopped, 2 launch budget, 3 heartbeat
+        stalled, 4 idle), "instances"}."""
+        run, code, inst = C.c_int32(0), C.c_int32(0), C.c_int64(0)
+        check(lib.pk_server_loop_status(self.handle, C.byref(run), C.byref(code), C.byref(inst)))
+        return {"running": run.value, "exit_code": code.value, "instances": inst.value}
+
+    def pause_heartbeat(self, pause=True):
+        """Test hook: stop (or resume) the scheduler's heartbeat that bounds the dispatcher's wait."""
+        check(lib.pk_server_pause_heartbeat(self.handle, 1 if pause else 0))
 
     def stats(self):
         s = (C.c_int64 * 4)()

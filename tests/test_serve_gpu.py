@@ -1,5 +1,10 @@
-"""Serving with continuous batching: each result equals the plain drop-in call's, alone and mixed."""
+"""Serving with continuous batching: each result equals the plain drop-in call's, alone and mixed.
+
+Every scenario runs on both request loops: the host scheduler's rounds of shared pass launches and
+the device-resident loop (a dispatcher kernel launching each request's pass graph from the device).
+"""
 import threading
+import time
 
 import numpy as np
 import pytest
@@ -35,9 +40,13 @@ def _alone(psfs, psfs_b, vol, pid, method, numit):
     return D.decon_lucy_function(vol, psfs[pid], numit, Background=100)[0]
 
 
-def test_served_results_equal_alone_in_the_mix(setup):
+LOOPS = [pytest.param(False, id="host-loop"), pytest.param(True, id="device-loop")]
+
+
+@pytest.mark.parametrize("device_loop", LOOPS)
+def test_served_results_equal_alone_in_the_mix(setup, device_loop):
     psfs, psfs_b, reqs = setup
-    with SV.Server(budget_bytes=4e9, max_batch=8) as srv:
+    with SV.Server(budget_bytes=4e9, max_batch=8, device_loop=device_loop) as srv:
         for i in range(3):
             srv.add_psf(i, psfs[i], psfs_b[i])
         ids = []
@@ -59,9 +68,10 @@ def test_served_results_equal_alone_in_the_mix(setup):
         assert all(v > 0 for v in lat)
 
 
-def test_served_tiny_budget_still_completes(setup):
+@pytest.mark.parametrize("device_loop", LOOPS)
+def test_served_tiny_budget_still_completes(setup, device_loop):
     psfs, psfs_b, reqs = setup
-    with SV.Server(budget_bytes=1, max_batch=4) as srv:
+    with SV.Server(budget_bytes=1, max_batch=4, device_loop=device_loop) as srv:
         srv.add_psf(0, psfs[0], psfs_b[0])
         ids = [srv.submit(v, 0, "omw", 2, Background=100) for v, _, _, _ in reqs[:4]]
         outs = [srv.wait(r)[0] for r in ids]
@@ -71,9 +81,10 @@ def test_served_tiny_budget_still_completes(setup):
         assert srv.stats()["peak_inflight_bytes"] < 64 * 1024 * 1024
 
 
-def test_served_cancel_and_timeout(setup):
+@pytest.mark.parametrize("device_loop", LOOPS)
+def test_served_cancel_and_timeout(setup, device_loop):
     psfs, psfs_b, reqs = setup
-    with SV.Server(budget_bytes=4e9, max_batch=2) as srv:
+    with SV.Server(budget_bytes=4e9, max_batch=2, device_loop=device_loop) as srv:
         srv.add_psf(0, psfs[0], psfs_b[0])
         vol = reqs[6][0]
         r1 = srv.submit(vol, 0, "rl", 20, Background=100)
@@ -97,3 +108,61 @@ def test_served_rejects_bad_requests(setup):
             srv.submit(reqs[0][0], 0, "omw", 2)        # no backprojector registered for OMW
         with pytest.raises(PkError):
             srv.submit(reqs[0][0], 7, "rl", 2)         # unknown PSF id
+
+
+def test_device_loop_wait_is_bounded(setup):
+    """The dispatcher's waits are bounded.  Idle, it returns after idle_us (exit code 4).  With the
+    idle bound out of the way and the scheduler's heartbeat stopped, it returns within heartbeat_ms
+    (exit code 3); with the heartbeat back a new instance serves the next request."""
+    psfs, psfs_b, reqs = setup
+    vol = reqs[0][0]
+    ref = _alone(psfs, psfs_b, vol, 0, "omw", 2)       # plain calls before any dispatcher runs
+    with SV.Server(budget_bytes=4e9, max_batch=4, device_loop=True, idle_us=2000) as srv:
+        srv.add_psf(0, psfs[0], psfs_b[0])
+        out, _ = srv.wait(srv.submit(vol, 0, "omw", 2, Background=100))
+        assert np.array_equal(out, ref)
+        t0 = time.time()
+        while srv.loop_status()["running"] and time.time() - t0 < 5.0:
+            time.sleep(0.001)
+        st = srv.loop_status()
+        assert st["running"] == 0 and st["exit_code"] == 4, st
+    with SV.Server(budget_bytes=4e9, max_batch=4, device_loop=True, heartbeat_ms=200, idle_us=60_000_000) as srv:
+        srv.add_psf(0, psfs[0], psfs_b[0])
+        out, _ = srv.wait(srv.submit(vol, 0, "omw", 2, Background=100))
+        assert np.array_equal(out, ref)
+        st = srv.loop_status()
+        assert st["instances"] >= 1 and st["running"] == 1     # waiting for the next request
+        srv.pause_heartbeat(True)
+        t0 = time.time()
+        while srv.loop_status()["running"] and time.time() - t0 < 5.0:
+            time.sleep(0.01)
+        st = srv.loop_status()
+        assert st["running"] == 0 and st["exit_code"] == 3, st
+        assert time.time() - t0 < 2.0
+        srv.pause_heartbeat(False)
+        out, _ = srv.wait(srv.submit(vol, 0, "omw", 2, Background=100))
+        assert np.array_equal(out, ref)
+        assert srv.loop_status()["instances"] >= 2
+
+
+def test_device_loop_hands_over_after_its_launch_budget(setup):
+    """A dispatcher launches at most 112 request graphs (the device runtime allows 120 fire-and-forget
+    launches per launching graph); 130 requests need a second instance, and every one completes."""
+    psfs, psfs_b, reqs = setup
+    vol = reqs[3][0]                                            # 36 x 36 x 30
+    ref = _alone(psfs, psfs_b, vol, 0, "omw", 2)
+    with SV.Server(budget_bytes=4e9, max_batch=16, device_loop=True) as srv:
+        srv.add_psf(0, psfs[0], psfs_b[0])
+        ids = [srv.submit(vol, 0, "omw", 2, Background=100) for _ in range(130)]
+        for rid in ids:
+            out, _ = srv.wait(rid)
+            assert np.array_equal(out, ref)
+        st = srv.loop_status()
+        assert st["instances"] >= 2
+        assert srv.stats()["completed"] == 130
+
+
+def test_host_loop_has_no_loop_status(setup):
+    with SV.Server() as srv:
+        with pytest.raises(PkError):
+            srv.loop_status()
