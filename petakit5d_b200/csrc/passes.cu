@@ -410,7 +410,10 @@ int choose_variant(pk_ctx* ctx, const PkProgram& prog, const PkStep& s, int idx,
     const int cls = size_class(prog, s, idx);
     const int fallback = (cls == 0 && kernels().xz[s.plan]) ? -1 : 0;
     if (!ctx || cands.size() < 2) return cands.empty() ? 0 : (cands.size() == 1 ? cands[0] : fallback);
-    const int multi = s.nvol > 1 ? 1 : 0;   // steps over many volumes (batches, serving rounds) time apart
+    // steps over several volumes (batches, serving rounds) time apart from single volumes, and steps
+    // over 8 or more apart again: on the 96-chunk batch the 8-column x kernel of 352- and 416-long
+    // lines ran 1.4-2x slower with 20 volumes per launch than the 16-column one, with 2-3 volumes not
+    const int multi = s.nvol == 1 ? 0 : s.nvol < 8 ? 1 : 2;
     const std::vector<long long> key = {s.kind, s.mode, s.plan, cls, multi};
     auto it = ctx->tune.find(key);
     if (it != ctx->tune.end()) return it->second;
@@ -463,6 +466,7 @@ int choose_variant(pk_ctx* ctx, const PkProgram& prog, const PkStep& s, int idx,
         const size_t Sb = (size_t)8 * d0.Pp * d0.nx * d0.nz * (s.mode == XZ_CONV ? 2 : 1);
         const long long fit = std::max<long long>(1, (long long)(((size_t)3 << 29) / std::max<size_t>(Sb, 1)));
         nrep = (int)std::max<long long>(2, std::min<long long>({16, fit, (tiles + one - 1) / one}));
+        if (multi == 2) nrep = (int)std::min<long long>(std::max(nrep, 8), std::max<long long>(fit, 2));
     }
     VolDesc dt = d0;
     std::vector<float> ms;

@@ -111,7 +111,7 @@ struct pk_server {
     size_t inflight = 0, peak_inflight = 0;
     cudaStream_t up = nullptr, down = nullptr;
     // device loop
-    static constexpr int kInstances = 16;
+    static constexpr int kInstances = 64;
     static constexpr int kDoneSlots = 4096;
     DlRing* ring = nullptr;           // page-locked, mapped
     DlRing* d_ring = nullptr;
