@@ -25,6 +25,7 @@
 #include "fft_engine.cuh"
 #include "pass_kernels.cuh"
 #include "pass_tma.cuh"
+#include "pass_conv3.cuh"
 #include "pass_yreg.cuh"
 #include "pk_internal.h"
 #include "plans.h"
@@ -44,6 +45,7 @@ void pk_fill_tma_0(pkpass::TmaTable& t);
 void pk_fill_tma_1(pkpass::TmaTable& t);
 void pk_fill_tma_2(pkpass::TmaTable& t);
 void pk_fill_tma_3(pkpass::TmaTable& t);
+void pk_fill_conv3(std::vector<pkpass::Conv3Entry>& v);
 void pk_fill_yreg(pkpass::YregTable& t);
 
 static int sm_count() {
@@ -119,6 +121,19 @@ const pkpass::TmaTable* tma_kernels() {
         on = true;
     });
     return on ? &t : nullptr;
+}
+
+// The fused x-z-x convolution kernels (pass_conv3.cuh), by (x plan, z plan); used with PK_CONV3=1
+// (otherwise the three separate passes run).
+const std::vector<pkpass::Conv3Entry>& conv3_kernels() {
+    static std::vector<pkpass::Conv3Entry> v;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        const char* e = getenv("PK_CONV3");
+        if (!(e && e[0] == '1')) return;
+        pk_fill_conv3(v);
+    });
+    return v;
 }
 
 // The register-packing y kernels (pass_yreg.cuh); PK_NO_YREG=1 keeps every y pass on the rolled
@@ -486,12 +501,79 @@ int choose_variant(pk_ctx* ctx, const PkProgram& prog, const PkStep& s, int idx,
     return best;
 }
 
+// Replaces each x forward / z convolution / x inverse triple of one volume by one fused step when a
+// fused kernel is built for its plans and the volume's column tiles fit it.
+static void fuse_conv3(pk_ctx* ctx, PkProgram& prog) {
+    const auto& c3 = conv3_kernels();
+    if (c3.empty() || !ctx || !tma_kernels()) return;
+    std::vector<PkStep> out;
+    out.reserve(prog.steps.size());
+    for (size_t i = 0; i < prog.steps.size(); i++) {
+        const PkStep& a = prog.steps[i];
+        if (i + 2 < prog.steps.size()) {
+            const PkStep& z = prog.steps[i + 1];
+            const PkStep& c = prog.steps[i + 2];
+            const bool shape = a.kind == PK_STEP_X && a.mode == XZ_FWD && z.kind == PK_STEP_Z && z.mode == XZ_CONV &&
+                               c.kind == PK_STEP_X && c.mode == XZ_INV && a.nvol == 1 && z.nvol == 1 && c.nvol == 1 &&
+                               a.grid > 0 && z.grid > 0 && c.grid > 0 && a.plan == c.plan;
+            int k = -1;
+            if (shape) {
+                const VolDesc& da = prog.descs[a.desc_off];
+                const VolDesc& dz = prog.descs[z.desc_off];
+                const VolDesc& dc = prog.descs[c.desc_off];
+                if (da.S == dz.S && dc.S == dz.S && dz.otf)
+                    for (size_t e = 0; e < c3.size(); e++)
+                        if (c3[e].k && c3[e].px == a.plan && c3[e].pz == z.plan && dz.Py >= c3[e].cols) k = (int)e;
+                XZMaps m;
+                if (k >= 0 && !(encode_spec_map(&m.s, dz.S, dz, 2, z.plan, c3[k].cols) &&
+                                encode_spec_map(&m.otf, dz.otf, dz, 2, z.plan, c3[k].cols) &&
+                                encode_spec_map(&m.s2, dz.S, dz, 1, a.plan, c3[k].cols)))
+                    k = -1;   // the tensor maps cannot describe this volume: keep the separate passes
+            }
+            if (k >= 0) {
+                // the column-tile counters live in the program's prefix array: every upload of the
+                // program's blob (before each launch or graph replay) brings them in as zeros, and
+                // programs that run at the same time (streams, graphs, device-launched requests)
+                // each have their own blob
+                const VolDesc& dz = prog.descs[z.desc_off];
+                const int K = (dz.Py + c3[k].cols - 1) / c3[k].cols;
+                PkStep f = z;
+                f.kind = PK_STEP_CONV3;
+                f.mode = 0;
+                f.plan = a.plan;
+                f.plan2 = z.plan;
+                f.conv3 = k;
+                f.prefix_off = (int)prog.prefix.size();
+                prog.prefix.insert(prog.prefix.end(), 2 * (size_t)K + 1, 0);   // claim counter, X and Z counters
+                static const int grid_cap = getenv("PK_CONV3_GRID") ? atoi(getenv("PK_CONV3_GRID")) : 0;   // diagnostics
+                f.grid = grid_cap > 0 ? std::min(grid_cap, sm_count()) : sm_count();
+                out.push_back(f);
+                i += 2;
+                continue;
+            }
+        }
+        out.push_back(a);
+    }
+    prog.steps.swap(out);
+}
+
 void assign_tma(pk_ctx* ctx, PkProgram& prog, cudaStream_t st) {
+    fuse_conv3(ctx, prog);
     prog.maps.assign(prog.descs.size(), XZMaps());
     const pkpass::YregTable* yt = yreg_kernels();
     for (PkStep& s : prog.steps) {
         s.tma = -1;
         s.yreg = 0;
+        if (s.kind == PK_STEP_CONV3) {
+            // z-box map of S, z-box map of the OTF, x-box map of S (fuse_conv3 checked that they encode)
+            const pkpass::Conv3Entry& e = conv3_kernels()[s.conv3];
+            const VolDesc& d = prog.descs[s.desc_off];
+            XZMaps& m = prog.maps[s.desc_off];
+            encode_spec_map(&m.s, d.S, d, 2, s.plan2, e.cols);
+            encode_spec_map(&m.otf, d.otf, d, 2, s.plan2, e.cols);
+            encode_spec_map(&m.s2, d.S, d, 1, s.plan, e.cols);
+            continue;
+        }
         if (s.kind == PK_STEP_Y && yt && s.plan == pkpass::kYregPlan && s.grid > 0 && s.mode >= 0 &&
             s.mode <= Y_C2R && yt->k[s.mode]) {
             bool ok = true;
@@ -851,6 +933,7 @@ const char* pk_step_name(const PkStep& s) {
     if (s.kind == PK_STEP_Y) return yn[s.mode];
     if (s.kind == PK_STEP_X) return xn[s.mode];
     if (s.kind == PK_STEP_Z) return zn[s.mode];
+    if (s.kind == PK_STEP_CONV3) return "xzx_conv";
     return "lambda";
 }
 
@@ -875,11 +958,21 @@ double pk_step_bytes(const PkStep& s, const VolDesc* descs) {
             }
         } else if (s.kind == PK_STEP_X || s.kind == PK_STEP_Z) {
             b += (s.mode == XZ_CONV ? 3 : 2) * Sb;
+        } else if (s.kind == PK_STEP_CONV3) {
+            b += 3 * Sb;   // S in, the OTF in, S out: the convolution's ruler
         } else {
             b += 16.0 * d.blocksY;
         }
     }
     return b;
+}
+
+// A device-launched request graph's last node: every pass before it is done.
+__global__ void k_req_done(int* done) {
+    if (threadIdx.x == 0) {
+        __threadfence_system();
+        *(volatile int*)done = 1;
+    }
 }
 
 static pk_status launch_steps(pk_ctx* ctx, const PkProgram& prog, cudaStream_t st, size_t b = 0,
@@ -913,7 +1006,11 @@ static pk_status launch_steps(pk_ctx* ctx, const PkProgram& prog, cudaStream_t s
             rec.b = take();
             cudaEventRecord(rec.a, st);
         }
-        if (s.tma >= 0) {
+        if (s.kind == PK_STEP_CONV3) {
+            const pkpass::Conv3Entry& c3 = conv3_kernels()[s.conv3];
+            c3.k<<<s.grid, c3.threads, c3.smem, st>>>(dd, prog.d_maps + s.desc_off, const_cast<int*>(dp),
+                                                     ctx ? ctx->d_err : nullptr);
+        } else if (s.tma >= 0) {
             tma_kernels()->k[s.plan][s.tma][s.tma_var]<<<s.tma_grid, tma_kernels()->threads[s.plan][s.tma][s.tma_var],
                                                          s.tma_smem, st>>>(
                 dd, prog.d_maps + s.desc_off, dp, s.nvol, ctx ? ctx->d_err : nullptr);
@@ -941,13 +1038,6 @@ static pk_status launch_steps(pk_ctx* ctx, const PkProgram& prog, cudaStream_t s
 
 // The program's launches as a graph of kernel nodes in launch order, built node by node (no stream
 // capture, so other threads' CUDA calls cannot disturb it).
-// A device-launched request graph's last node: every pass before it is done.
-__global__ void k_req_done(int* done) {
-    if (threadIdx.x == 0) {
-        __threadfence_system();
-        *(volatile int*)done = 1;
-    }
-}
 
 static bool build_graph(const PkProgram& prog, const VolDesc* d_desc, const int* d_prefix, const XZMaps* d_maps,
                         int* d_err, cudaGraphExec_t* out, unsigned long long flags = 0, int* d_done = nullptr) {
@@ -972,7 +1062,15 @@ static bool build_graph(const PkProgram& prog, const VolDesc* d_desc, const int*
         p.blockDim = dim3(kThreads);
         p.gridDim = dim3(s.grid);
         p.sharedMemBytes = (unsigned)s.smem;
-        if (s.tma >= 0) {
+        int* cnt = const_cast<int*>(dp);
+        void* argsc[] = {(void*)&dd, (void*)&dm, (void*)&cnt, (void*)&de};
+        if (s.kind == PK_STEP_CONV3) {
+            const pkpass::Conv3Entry& c3 = conv3_kernels()[s.conv3];
+            p.func = (void*)c3.k;
+            p.blockDim = dim3(c3.threads);
+            p.sharedMemBytes = (unsigned)c3.smem;
+            p.kernelParams = argsc;
+        } else if (s.tma >= 0) {
             p.func = (void*)tma_kernels()->k[s.plan][s.tma][s.tma_var];
             p.gridDim = dim3(s.tma_grid);
             p.blockDim = dim3(tma_kernels()->threads[s.plan][s.tma][s.tma_var]);
@@ -1089,8 +1187,8 @@ pk_status pk_program_launch(pk_ctx* ctx, PkProgram& prog, cudaStream_t st) {
         key.push_back((long long)prog.prefix.size());
         for (const PkStep& s : prog.steps) {
             const long long v[] = {s.kind, s.mode, s.plan, s.nvol, s.grid, (long long)s.smem, s.desc_off, s.prefix_off,
-                                   s.tma, s.tma_var, s.tma_grid, s.yreg};
-            key.insert(key.end(), v, v + 12);
+                                   s.tma, s.tma_var, s.tma_grid, s.yreg, s.conv3};
+            key.insert(key.end(), v, v + 13);
         }
         auto it = ctx->graphs.find(key);
         if (it == ctx->graphs.end() && ctx->graph_seen.size() >= 4096) ctx->graph_seen.clear();  // bounded

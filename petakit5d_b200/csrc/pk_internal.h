@@ -133,6 +133,7 @@ __device__ __forceinline__ unsigned pk_dyn_smem() {
 struct alignas(64) XZMaps {
     CUtensorMap s;
     CUtensorMap otf;
+    CUtensorMap s2;   // the fused convolution pass: S with the x pass's box (s has the z pass's)
 };
 
 // ------------------------------------------------------------------ host side
@@ -235,13 +236,17 @@ pk_status pk_init_desc(pk_ctx* ctx, int ny, int nx, int nz, VolDesc* d);
 size_t pk_spec_elems(const VolDesc& d);   // complex elements of the half spectrum
 
 // launch programs (passes.cu)
-enum { PK_STEP_Y = 0, PK_STEP_X = 1, PK_STEP_Z = 2, PK_STEP_LAMBDA = 3 };
+// PK_STEP_CONV3: x forward, z convolution and x inverse of one volume in one launch (pass_conv3.cuh)
+enum { PK_STEP_Y = 0, PK_STEP_X = 1, PK_STEP_Z = 2, PK_STEP_LAMBDA = 3, PK_STEP_CONV3 = 4 };
 struct PkStep {
     int kind = 0, mode = 0, plan = 0, nvol = 0, desc_off = 0, prefix_off = 0, grid = 0;
     size_t smem = 0;
     // set at upload: index of the persistent TMA kernel that runs this x / z step (-1: none), its
     // grid (resident CTAs, each walking tiles) and dynamic shared memory
     int tma = -1, tma_var = 0, tma_grid = 0;
+    // PK_STEP_CONV3: the fused kernel's table index and its z plan (its column-tile counters are the
+    // 2K ints of the prefix array at prefix_off)
+    int conv3 = -1, plan2 = 0;
     size_t tma_smem = 0;
     // set at upload: this y step runs the register-packing kernel (512-voxel rows), with its smem
     int yreg = 0;

@@ -94,6 +94,19 @@ __device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bu
 // every committed store has completed
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory"); }
 
+// orders this thread's generic-proxy global accesses with its async-proxy (bulk copy) ones
+__device__ __forceinline__ void fence_async_global() { asm volatile("fence.proxy.async.global;\n" ::: "memory"); }
+
+// an int in global memory read with gpu-scope acquire / raised with gpu-scope release
+__device__ __forceinline__ int ld_acquire_gpu(const int* p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void red_release_gpu_add(int* p, int v) {
+    asm volatile("red.release.gpu.global.add.s32 [%0], %1;\n" ::"l"(p), "r"(v) : "memory");
+}
+
 // a tensor map that the host wrote to global memory before the launch, made visible to the TMA unit
 __device__ __forceinline__ void tmap_acquire(const CUtensorMap* map) {
     asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;\n" ::"l"(map) : "memory");
