@@ -730,6 +730,9 @@ pk_status pk_decon_multi(pk_ctx* ctx, int method, std::vector<DeconJob>& jobs, p
     if (all.steps.size() != tail0 + 2 * (size_t)nslab || mid0 != 2 * (size_t)nslab)
         return pk_fail(PK_ERR_UNSUPPORTED, "streamed program layout");
     if ((s = pk_program_upload(ctx, all, st)) != PK_OK) return s;
+    // the upload may fuse convolution triples of the middle part (not the per-slab head or tail):
+    // the tail starts 2 nslab steps from the end
+    const size_t tail0u = all.steps.size() - 2 * (size_t)nslab;
     cudaEvent_t ev;
     for (int sl = 0; sl < nslab; sl++) {   // every slab upload is queued before any wait on the host
         if ((s = get_io_event(ctx, sl, &ev)) != PK_OK) return s;
@@ -742,9 +745,9 @@ pk_status pk_decon_multi(pk_ctx* ctx, int method, std::vector<DeconJob>& jobs, p
         PK_CUDA(cudaStreamWaitEvent(st, ctx->io_ev[sl], 0));
         if ((s = pk_program_launch_range(ctx, all, st, 2 * sl, 2 * sl + 2, false)) != PK_OK) return s;
     }
-    if ((s = pk_program_launch_range(ctx, all, st, mid0, tail0, false)) != PK_OK) return s;
+    if ((s = pk_program_launch_range(ctx, all, st, mid0, tail0u, false)) != PK_OK) return s;
     for (int sl = 0; sl < nslab; sl++) {
-        if ((s = pk_program_launch_range(ctx, all, st, tail0 + 2 * sl, tail0 + 2 * sl + 2, sl == nslab - 1)) != PK_OK)
+        if ((s = pk_program_launch_range(ctx, all, st, tail0u + 2 * sl, tail0u + 2 * sl + 2, sl == nslab - 1)) != PK_OK)
             return s;
         if ((s = get_io_event(ctx, nslab + sl, &ev)) != PK_OK) return s;
         PK_CUDA(cudaEventRecord(ev, st));

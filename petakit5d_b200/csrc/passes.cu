@@ -521,8 +521,12 @@ static void fuse_conv3(pk_ctx* ctx, PkProgram& prog) {
                 const VolDesc& da = prog.descs[a.desc_off];
                 const VolDesc& dz = prog.descs[z.desc_off];
                 const VolDesc& dc = prog.descs[c.desc_off];
-                if (da.S == dz.S && dc.S == dz.S && dz.otf)
-                    for (size_t e = 0; e < c3.size(); e++)
+                // the three steps cover the same whole volume (not the z-slab views of a streamed call)
+                const auto same = [&](const VolDesc& u) {
+                    return u.S == dz.S && u.nx == dz.nx && u.nz == dz.nz && u.Py == dz.Py && u.Pp == dz.Pp;
+                };
+                if (same(da) && same(dc) && dz.otf)
+                    for (size_t e = 0; e < c3.size() && k < 0; e++)
                         if (c3[e].k && c3[e].px == a.plan && c3[e].pz == z.plan && dz.Py >= c3[e].cols) k = (int)e;
                 XZMaps m;
                 if (k >= 0 && !(encode_spec_map(&m.s, dz.S, dz, 2, z.plan, c3[k].cols) &&
@@ -543,8 +547,12 @@ static void fuse_conv3(pk_ctx* ctx, PkProgram& prog) {
                 f.plan = a.plan;
                 f.plan2 = z.plan;
                 f.conv3 = k;
+                // claim counter, X and Z counters, one 128-byte line each (from the blob's start,
+                // which is 256-byte aligned in device memory)
+                const size_t dbytes = sizeof(VolDesc) * prog.descs.size();
+                while ((dbytes + sizeof(int) * prog.prefix.size()) % (sizeof(int) * pkpass::kC3Line)) prog.prefix.push_back(0);
                 f.prefix_off = (int)prog.prefix.size();
-                prog.prefix.insert(prog.prefix.end(), 2 * (size_t)K + 1, 0);   // claim counter, X and Z counters
+                prog.prefix.insert(prog.prefix.end(), (size_t)pkpass::c3_counter_ints(K), 0);
                 static const int grid_cap = getenv("PK_CONV3_GRID") ? atoi(getenv("PK_CONV3_GRID")) : 0;   // diagnostics
                 f.grid = grid_cap > 0 ? std::min(grid_cap, sm_count()) : sm_count();
                 out.push_back(f);

@@ -72,6 +72,35 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, i
         : "memory");
 }
 
+// L2 eviction priorities for the cache-hinted copies below (applied to every line a copy touches)
+__device__ __forceinline__ uint64_t l2_evict_first() {
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;\n" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ uint64_t l2_evict_last() {
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;\n" : "=l"(p));
+    return p;
+}
+
+// tma_load_3d with an L2 eviction priority
+__device__ __forceinline__ void tma_load_3d_hint(void* dst, const CUtensorMap* map, int c0, int c1, int c2, uint64_t* bar,
+                                                 uint64_t pol) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1, {%2, %3, "
+        "%4}], [%5], %6;\n" ::"r"(smem_u32(dst)),
+        "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar)), "l"(pol)
+        : "memory");
+}
+
+// Prefetch of the box at (c0, c1, c2) into L2 (no shared memory, no completion to wait for)
+__device__ __forceinline__ void tma_prefetch_3d(const CUtensorMap* map, int c0, int c1, int c2) {
+    asm volatile("cp.async.bulk.prefetch.tensor.3d.L2.global.tile [%0, {%1, %2, %3}];\n" ::"l"(map), "r"(c0), "r"(c1),
+                 "r"(c2)
+                 : "memory");
+}
+
 // Untiled bulk copy of `bytes` contiguous bytes (both addresses 16-byte aligned, bytes a multiple
 // of 16) from global to shared memory, completing on `bar`.
 __device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
@@ -85,6 +114,15 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t b
 __device__ __forceinline__ void tma_store_3d(const CUtensorMap* map, int c0, int c1, int c2, const void* src) {
     asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%1, %2, %3}], [%4];\n" ::"l"(map), "r"(c0),
                  "r"(c1), "r"(c2), "r"(smem_u32(src))
+                 : "memory");
+}
+
+// tma_store_3d with an L2 eviction priority
+__device__ __forceinline__ void tma_store_3d_hint(const CUtensorMap* map, int c0, int c1, int c2, const void* src,
+                                                  uint64_t pol) {
+    asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.bulk_group.L2::cache_hint [%0, {%1, %2, %3}], [%4], %5;\n" ::"l"(
+                     map),
+                 "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(src)), "l"(pol)
                  : "memory");
 }
 
