@@ -95,6 +95,47 @@ struct Conv3Layout {
     static_assert(1024 + NBUF * BUF + OTF + TWX + TWZ + BARS <= 227 * 1024, "tiles exceed shared memory");
 };
 
+// z convolution of a z tile whose OTF tile is in shared memory already: the forward stages but the
+// last in shared memory; the last forward stage, the OTF multiply and the first inverse stage in
+// registers, one butterfly column per thread for the first B = T NZ / R threads (whole warps; the
+// others only keep the barriers); the remaining inverse stages in shared memory.  The same element
+// order, twiddles and operations as dstage_s2r / dstage_r2s with the multiply between them.
+template <int PZ, int T, int NTH>
+__device__ __forceinline__ void c3_zconv(float2* __restrict__ cur, const float2* __restrict__ twz,
+                                         const float2* __restrict__ hb, bool cj, int tid) {
+    constexpr int NZ = kPlans[PZ].n, NST = kPlans[PZ].nst, R = kPlans[PZ].rad[0], MS = NZ / R, B = T * MS;
+    constexpr int NS = plan_ns_before(PZ, NST - 1), OFF = stage_tw_off(PZ, NST - 1);
+    static_assert(same_end_radix(PZ) && !direct_radix(R) && NS == MS, "first and last radix equal, register butterfly");
+    static_assert(B <= NTH && B % 32 == 0, "one butterfly column per thread, whole warps");
+    run_dense<PZ, 0, NST - 1, 1, T, false, NTH>(cur, twz, tid);
+    float2 v[R];
+    const int l = tid % T, j = tid / T;
+    if (tid < B) {
+#pragma unroll
+        for (int r = 0; r < R; r++) v[r] = cur[(j + r * MS) * T + l];
+    }
+    compute_bar<NTH>();   // every element read before the first inverse stage overwrites the tile
+    if (tid < B) {
+        if constexpr (NS > 1) {
+#pragma unroll
+            for (int r = 1; r < R; r++) v[r] = cmul(v[r], twz[OFF + (r - 1) * NS + j]);
+        }
+        bfly<R, false>(v);
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            float2 h = hb[(j + r * MS) * T + l];
+            if (cj) h.y = -h.y;
+            v[r] = cmul(v[r], h);
+        }
+        bfly<R, true>(v);
+        const int a0 = j * R * T + l;
+#pragma unroll
+        for (int r = 0; r < R; r++) cur[a0 + r * T] = v[r];
+    }
+    compute_bar<NTH>();
+    run_dense<PZ, 1, NST, R, T, true, NTH>(cur, twz, tid);
+}
+
 template <int PX, int PZ, int T, int NBUF, int NTH>
 __global__ void __launch_bounds__(NTH + 64, 1)
     k_conv3(const VolDesc* __restrict__ descs, const XZMaps* __restrict__ maps, int* cnt, int* err) {
@@ -117,6 +158,7 @@ __global__ void __launch_bounds__(NTH + 64, 1)
     uint64_t* otf_full = bars + 3 * NBUF;
     uint64_t* otf_empty = bars + 3 * NBUF + 1;
     __shared__ int slot_item[NBUF];   // the item each buffer holds (-1: no more items)
+    __shared__ int slot_type[NBUF];   // its type (C3_X / C3_Z / C3_I) for the compute warps
     __shared__ int n_items;           // items this CTA loaded, once the loader has no more (-1 before)
     const int tid = threadIdx.x;
     const VolDesc& d = descs[0];
@@ -198,6 +240,7 @@ __global__ void __launch_bounds__(NTH + 64, 1)
                     (k_load < NBUF || pktma::mbar_try(&freed[s], (uint32_t)(((k_load / NBUF) - 1) & 1)))) {
                     if (claimed < 0) {   // an arrival without bytes: no more items
                         slot_item[s] = -1;
+                        slot_type[s] = -1;
                         *(volatile int*)&n_items = k_load;
                         mbar_arrive_cta(&full[s]);
                         break;
@@ -206,6 +249,7 @@ __global__ void __launch_bounds__(NTH + 64, 1)
                     if (OIB || type != C3_Z || z_loaded == 0 || pktma::mbar_try(otf_empty, (uint32_t)((z_loaded - 1) & 1))) {
                         pktma::fence_async_global();
                         slot_item[s] = claimed;
+                        slot_type[s] = type;
                         const int c0 = 2 * c * T;
                         if (type == C3_Z) {
                             uint64_t* ob = OIB ? &full[s] : otf_full;
@@ -245,7 +289,7 @@ __global__ void __launch_bounds__(NTH + 64, 1)
         } else {
             pktma::tmap_acquire(&m.s);
             pktma::tmap_acquire(&m.s2);
-            int ring[8];   // items stored and not yet published (at most two)
+            int ring[8];   // items stored and not yet published (at most three)
             int k_store = 0, k_pub = 0;
             // raise the counters of stored items [k_pub, upto): their stores have completed
             auto publish = [&](int upto) {
@@ -284,11 +328,11 @@ __global__ void __launch_bounds__(NTH + 64, 1)
                     mbar_arrive_cta(&freed[s]);
                     prog = true;
                 }
-                // stores older than the newest are complete by now: publish; with nothing else to
-                // do, wait for all of them
-                if (k_pub < k_store - 1) {
-                    asm volatile("cp.async.bulk.wait_group 1;\n" ::: "memory");
-                    publish(k_store - 1);
+                // stores older than the two newest are complete by now: publish; with nothing else
+                // to do, wait for all of them
+                if (k_pub < k_store - 2) {
+                    asm volatile("cp.async.bulk.wait_group 2;\n" ::: "memory");
+                    publish(k_store - 2);
                     prog = true;
                 } else if (!prog && k_pub < k_store) {
                     pktma::bulk_wait_all();
@@ -319,10 +363,8 @@ __global__ void __launch_bounds__(NTH + 64, 1)
             if (tid == 0) pktma::report_wait_failure(err, 1);
             return;
         }
-        const int item = slot_item[s];
-        if (item < 0) break;   // no more items
-        int type, c, o;
-        c3_locate(item, K, nx, nz, type, c, o);
+        const int type = slot_type[s];
+        if (type < 0) break;   // no more items
         if (type == C3_X) {
             run_dense<PX, 0, NSTX, 1, T, false, NTH>(cur, twx, tid);
         } else if (type == C3_I) {
@@ -330,7 +372,10 @@ __global__ void __launch_bounds__(NTH + 64, 1)
         } else {
             const bool cj = d.conj != 0;
             const float2* hb = otf_of(s);
-            if constexpr (same_end_radix(PZ)) {
+            if constexpr (OIB && same_end_radix(PZ) && T * (NZ / kPlans[PZ].rad[0]) <= NTH &&
+                          T * (NZ / kPlans[PZ].rad[0]) % 32 == 0) {
+                c3_zconv<PZ, T, NTH>(cur, twz, hb, cj, tid);
+            } else if constexpr (same_end_radix(PZ)) {
                 constexpr int R = kPlans[PZ].rad[0], MS = NZ / R, MAXB = (T * MS + NTH - 1) / NTH;
                 float2 v[MAXB][R];
                 run_dense<PZ, 0, NSTZ - 1, 1, T, false, NTH>(cur, twz, tid);

@@ -82,14 +82,15 @@ __device__ __forceinline__ void dstage(float2* __restrict__ buf, const float2* _
     constexpr int NT = NTH;
     constexpr int MAXB = (B + NT - 1) / NT;
     float2 v[MAXB][R];
+    // a thread past the last butterfly reads butterfly 0's elements (in the tile, never used): an
+    // unconditional load keeps v's registers out of a predicated region that spills under tight caps
 #pragma unroll
     for (int i = 0; i < MAXB; i++) {
         const int b = tid + i * NT;
-        if (B % NT == 0 || b < B) {
-            const int l = b % L, j = b / L;
+        const int bb = (B % NT == 0 || b < B) ? b : 0;
+        const int l = bb % L, j = bb / L;
 #pragma unroll
-            for (int r = 0; r < R; r++) v[i][r] = buf[(j + r * M) * L + l];
-        }
+        for (int r = 0; r < R; r++) v[i][r] = buf[(j + r * M) * L + l];
     }
     compute_bar<NTH>();
 #pragma unroll

@@ -232,7 +232,7 @@ int tma_index(const PkStep& s) {
 // The first time a single-volume step of a (pass, plan, size class) is seen, every candidate runs
 // once to warm up and twice timed on scratch buffers of that step's geometry (zeroed spectrum and
 // OTF; no live data is touched); the fastest is kept for the context and appended to an on-disk
-// cache (PK_TUNE_FILE, else ~/.cache/pkdecon/tune-v4.txt), keyed by the device name, so later
+// cache (PK_TUNE_FILE, else ~/.cache/pkdecon/tune-v5.txt), keyed by the device name, so later
 // processes skip the timing.  PK_TUNE=0 turns the timing off (the fallback choice everywhere).
 
 std::mutex g_tf_mu;
@@ -244,7 +244,7 @@ std::string tune_path() {
     if (e && *e) return e;
     const char* h = getenv("HOME");
     if (!h || !*h) return "";
-    return std::string(h) + "/.cache/pkdecon/tune-v4.txt";
+    return std::string(h) + "/.cache/pkdecon/tune-v5.txt";
 }
 
 std::string device_tag(int dev) {
@@ -291,64 +291,74 @@ std::string variant_name(int plan, int idx, int v) {
            "warps-" + std::to_string(t->nbuf[plan][idx][v]) + "buf";
 }
 
-// Times each candidate of step `s` on scratch buffers: nrep volumes of geometry d0 (one, or for a
-// multi-volume step of a batch or a serving round, copies of its first volume, each with its own
-// buffers, descriptor and tensor maps); returns the fastest, or -2 when nothing could be timed.
-// ms[i] receives candidate i's time.
-int time_candidates(pk_ctx* ctx, const PkStep& s, const VolDesc& d0, int nrep, int idx, const std::vector<int>& cands,
+// Times each candidate of step `s` on scratch buffers: one volume per entry of `geo` (the step's
+// own volume, or for a multi-volume step of a batch or a serving round the geometries of its first
+// volumes), each with its own zeroed buffers, descriptor and tensor maps; returns the fastest, or -2
+// when nothing could be timed. ms[i] receives candidate i's time.
+int time_candidates(pk_ctx* ctx, const PkStep& s, const std::vector<VolDesc>& geo, int idx, const std::vector<int>& cands,
                     cudaStream_t st, std::vector<float>& ms) {
     const pkpass::TmaTable* t = tma_kernels();
     const pkpass::KernelTable& kt = kernels();
     const int axis = s.kind == PK_STEP_X ? 1 : 2;
     const bool conv = s.mode == XZ_CONV;
-    const size_t Sb = (size_t)8 * d0.Pp * d0.nx * d0.nz;
-    const size_t per = (conv ? 2 : 1) * ((Sb + 255) & ~(size_t)255);
-    if (nrep < 1 || per * nrep > ((size_t)3 << 29)) return -2;   // above 1.5 GB of scratch: keep the default
+    const int nrep = (int)geo.size();
+    if (nrep < 1) return -2;
+    std::vector<size_t> off(nrep + 1, 0);
+    size_t Sb_all = 0;
+    for (int r = 0; r < nrep; r++) {
+        const size_t Sb = (size_t)8 * geo[r].Pp * geo[r].nx * geo[r].nz;
+        Sb_all += Sb;
+        off[r + 1] = off[r] + (conv ? 2 : 1) * ((Sb + 255) & ~(size_t)255);
+    }
+    if (off[nrep] > ((size_t)3 << 29)) return -2;   // above 1.5 GB of scratch: keep the default
     const size_t moff = ((size_t)nrep * sizeof(VolDesc) + 63) & ~(size_t)63;
     const size_t poff = moff + (size_t)nrep * sizeof(XZMaps);
     const size_t blob = poff + sizeof(int) * (nrep + 1);
     const size_t soff = (blob + 255) & ~(size_t)255;
     char* d = nullptr;   // stream-ordered: a device-wide synchronisation here would wait on a serving dispatcher
-    if (cudaMallocAsync((void**)&d, soff + per * nrep, st) != cudaSuccess) {
+    if (cudaMallocAsync((void**)&d, soff + off[nrep], st) != cudaSuccess) {
         cudaGetLastError();
         return -2;
     }
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     int best = -2;
     float best_ms = 1e30f;
-    bool ok = cudaMemsetAsync(d + soff, 0, per * nrep, st) == cudaSuccess &&
+    bool ok = cudaMemsetAsync(d + soff, 0, off[nrep], st) == cudaSuccess &&
               cudaEventCreate(&e0) == cudaSuccess && cudaEventCreate(&e1) == cudaSuccess;
-    std::vector<VolDesc> dv(nrep, d0);
+    std::vector<VolDesc> dv(geo);
     for (int r = 0; r < nrep; r++) {
-        dv[r].S = (float2*)(d + soff + per * r);
-        dv[r].otf = conv ? (float2*)(d + soff + per * r + per / 2) : nullptr;
+        const size_t per = off[r + 1] - off[r];
+        dv[r].S = (float2*)(d + soff + off[r]);
+        dv[r].otf = conv ? (float2*)(d + soff + off[r] + per / 2) : nullptr;
     }
     std::vector<unsigned char> h(blob, 0);
     memcpy(h.data(), dv.data(), sizeof(VolDesc) * nrep);
     ms.assign(cands.size(), -1.f);
     for (size_t ci = 0; ok && ci < cands.size(); ci++) {
         const int v = cands[ci];
-        int per_vol, grid;
-        size_t smem;
+        std::vector<int> pf(nrep + 1, 0);
+        int grid;
+        size_t smem = 0;
         std::vector<XZMaps> m(nrep);
         memset(m.data(), 0, sizeof(XZMaps) * nrep);
         if (v < 0) {
-            per_vol = axis == 1 ? d0.blocksX : d0.blocksZ;
-            grid = per_vol * nrep;
-            smem = step_smem(s.kind, s.mode, d0);
+            for (int r = 0; r < nrep; r++) {
+                pf[r + 1] = pf[r] + (axis == 1 ? dv[r].blocksX : dv[r].blocksZ);
+                smem = std::max(smem, step_smem(s.kind, s.mode, dv[r]));
+            }
+            grid = pf[nrep];
         } else {
             const int T = t->cols[s.plan][idx][v];
-            bool enc = d0.Py >= T;
+            bool enc = true;
             for (int r = 0; r < nrep && enc; r++)
-                enc = encode_spec_map(&m[r].s, dv[r].S, dv[r], axis, s.plan, T) &&
+                enc = dv[r].Py >= T && encode_spec_map(&m[r].s, dv[r].S, dv[r], axis, s.plan, T) &&
                       (!conv || encode_spec_map(&m[r].otf, dv[r].otf, dv[r], axis, s.plan, T));
             if (!enc) continue;
-            per_vol = (axis == 1 ? d0.nz : d0.nx) * ((d0.Py + T - 1) / T);
-            grid = std::min(per_vol * nrep, t->per_sm[s.plan][idx][v] * sm_count());
+            for (int r = 0; r < nrep; r++)
+                pf[r + 1] = pf[r] + (axis == 1 ? dv[r].nz : dv[r].nx) * ((dv[r].Py + T - 1) / T);
+            grid = std::min(pf[nrep], t->per_sm[s.plan][idx][v] * sm_count());
             smem = t->smem[s.plan][idx][v];
         }
-        std::vector<int> pf(nrep + 1);
-        for (int r = 0; r <= nrep; r++) pf[r] = per_vol * r;
         memcpy(h.data() + moff, m.data(), sizeof(XZMaps) * nrep);
         memcpy(h.data() + poff, pf.data(), sizeof(int) * (nrep + 1));
         ok = cudaMemcpyAsync(d, h.data(), blob, cudaMemcpyHostToDevice, st) == cudaSuccess &&
@@ -370,7 +380,7 @@ int time_candidates(pk_ctx* ctx, const PkStep& s, const VolDesc& d0, int nrep, i
         if (!ok) break;
         // a time below the pass's bytes at 10 TB/s (above any B200's HBM) means the launch did not do
         // the work either
-        const double floor_ms = (double)(conv ? 3 : 2) * (double)Sb * nrep / 10e12 * 1e3;
+        const double floor_ms = (double)(conv ? 3 : 2) * (double)Sb_all / 10e12 * 1e3;
         if (le != cudaSuccess || el / 2.f < floor_ms) continue;
         ms[ci] = el / 2.f;
         if (ms[ci] < best_ms) {
@@ -467,26 +477,28 @@ int choose_variant(pk_ctx* ctx, const PkProgram& prog, const PkStep& s, int idx,
     const bool capturing = cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone;
     if (capturing) cudaGetLastError();
     if ((off && off[0] == '0') || capturing) return fallback;   // no timing here
-    // the timed geometry: the step's first volume; for a multi-volume step, as many copies of it (each
-    // with its own buffers) as make the step's tile count, 2 to 16 of them within the scratch limit
-    int nrep = 1;
+    // the timed geometry: the step's volume; for a multi-volume step, its volumes in order (each with
+    // its own scratch buffers), up to 16 of them within the scratch limit, so that a batch of mixed
+    // shapes is timed on its own mix (copies of one volume ranked the x tiles of a 96-chunk batch the
+    // other way round from the batch itself)
+    std::vector<VolDesc> geo{d0};
     if (multi) {
-        const int T0 = t->cols[s.plan][idx][0];
-        long long tiles = 0;
-        for (int i = 0; i < s.nvol; i++) {
+        const bool conv = s.mode == XZ_CONV;
+        size_t used = 0;
+        geo.clear();
+        for (int i = 0; i < s.nvol && geo.size() < 16; i++) {
             const VolDesc& d = prog.descs[s.desc_off + i];
-            tiles += (long long)(s.kind == PK_STEP_X ? d.nz : d.nx) * ((d.Py + T0 - 1) / T0);
+            const size_t Sb = (size_t)8 * d.Pp * d.nx * d.nz;
+            const size_t need = (conv ? 2 : 1) * ((Sb + 255) & ~(size_t)255);
+            if (!geo.empty() && used + need > ((size_t)3 << 29)) break;
+            geo.push_back(d);
+            used += need;
         }
-        const long long one = (long long)(s.kind == PK_STEP_X ? d0.nz : d0.nx) * ((d0.Py + T0 - 1) / T0);
-        const size_t Sb = (size_t)8 * d0.Pp * d0.nx * d0.nz * (s.mode == XZ_CONV ? 2 : 1);
-        const long long fit = std::max<long long>(1, (long long)(((size_t)3 << 29) / std::max<size_t>(Sb, 1)));
-        nrep = (int)std::max<long long>(2, std::min<long long>({16, fit, (tiles + one - 1) / one}));
-        if (multi == 2) nrep = (int)std::min<long long>(std::max(nrep, 8), std::max<long long>(fit, 2));
     }
-    VolDesc dt = d0;
+    const VolDesc& dt = d0;
     std::vector<float> ms;
     PkRange range("pk autotune");
-    int best = time_candidates(ctx, s, dt, nrep, idx, cands, st, ms);
+    int best = time_candidates(ctx, s, geo, idx, cands, st, ms);
     if (best == -2) return fallback;
     ctx->tune[key] = best;
     record(best, "timed", &ms, dt);
