@@ -416,9 +416,8 @@ int size_class(const PkProgram& prog, const PkStep& s, int idx) {
 }
 
 // The variant an x / z step runs: the context's earlier choice, the on-disk cache's, or a timing.
-// A step times its candidates once per (pass, plan, size class): on its own volume, or for a
-// multi-volume step of a batch or a serving round on its first volume stretched to the step's
-// tile count; without a timing (inside a stream capture, PK_TUNE=0) it takes the fallback:
+// A step times its candidates once per (pass, plan, size class, volume count): on its own volume,
+// or for a multi-volume step of a batch or a serving round on its own first volumes; without a timing (inside a stream capture, PK_TUNE=0) it takes the fallback:
 // register-IO under one wave of tiles, where the persistent kernel's set-up does not pay, else TMA
 // variant 0.
 int choose_variant(pk_ctx* ctx, const PkProgram& prog, const PkStep& s, int idx, cudaStream_t st) {
