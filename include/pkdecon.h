@@ -200,9 +200,26 @@ PK_API pk_status pk_omw_backprojector(pk_ctx* ctx, const float* psf, const int64
                                double hann_lo, double hann_hi, double min_int_thresh,
                                float* b_omw, float* otf_bp_omw, float* abs_otf_c, uint8_t* otf_mask);
 
-/* [PSF_bp, OTF_bp] = BackProjector(PSF_fp, 'wiener-butterworth', alpha, beta, n, resFlag, iRes)
- * (third_parties/WBDeconvolution/BackProjector.m:67-233).  psf_bp: float64 of psf_dims;
- * otf_bp (NULL to skip): complex128 interleaved. */
+/* BackProjector's bp_type (third_parties/WBDeconvolution/BackProjector.m:163-231). */
+typedef enum {
+    PK_BP_TRADITIONAL = 0,        /* 'traditional': the flipped PSF */
+    PK_BP_GAUSSIAN = 1,           /* 'gaussian': a Gaussian of the PSF's FWHMs */
+    PK_BP_BUTTERWORTH = 2,        /* 'butterworth': the Butterworth filter alone */
+    PK_BP_WIENER = 3,             /* 'wiener': Wiener filter of the flipped OTF */
+    PK_BP_WIENER_BUTTERWORTH = 4  /* 'wiener-butterworth' */
+} pk_bp_type;
+
+/* [PSF_bp, OTF_bp] = BackProjector(PSF_fp, bp_type, alpha, beta, n, resFlag, iRes)
+ * (third_parties/WBDeconvolution/BackProjector.m:67-233; called by decon/RLdecon.m for
+ * wiener-butterworth back projection).  psf_bp: float64 of psf_dims; otf_bp (NULL to skip):
+ * complex128 interleaved.  A bp_type outside pk_bp_type is PK_ERR_INVALID (the reference's
+ * "bp_type does not match any back-projector type"). */
+PK_API pk_status pk_backprojector(pk_ctx* ctx, const float* psf, const int64_t psf_dims[3], int32_t bp_type,
+                                  double alpha, double beta, int32_t n, int32_t res_flag, const double ires[3],
+                                  double* psf_bp, double* otf_bp);
+
+/* pk_backprojector with bp_type PK_BP_WIENER_BUTTERWORTH
+ * (third_parties/WBDeconvolution/BackProjector.m:67-233, the 'wiener-butterworth' branch). */
 PK_API pk_status pk_wb_backprojector(pk_ctx* ctx, const float* psf, const int64_t psf_dims[3], double alpha,
                               double beta, int32_t n, int32_t res_flag, const double ires[3],
                               double* psf_bp, double* otf_bp);

@@ -1,7 +1,8 @@
 """CPU restatement of the OMW and Wiener-Butterworth backprojector generators (oracle; test infra).
 
 * ``omw_backprojector_generation`` follows microscopeDataProcessing/decon/omw_backprojector_generation.m
-* ``wb_backprojector`` follows third_parties/WBDeconvolution/BackProjector.m ('wiener-butterworth')
+* ``back_projector`` follows third_parties/WBDeconvolution/BackProjector.m (every bp_type;
+  ``wb_backprojector`` is its 'wiener-butterworth' form)
 
 Arithmetic choices shared with the CUDA library (the reference leaves them to MATLAB):
   * the PSF-size transforms are computed in float64 and, where the reference works in single,
@@ -217,6 +218,28 @@ def fwhm_psf(psf32):
 
 def wb_backprojector(psf_fp, alpha=1e-4, beta=1e-3, n=10, res_flag=1, ires=(0.0, 0.0, 0.0)):
     """BackProjector(PSF_fp, 'wiener-butterworth', alpha, beta, n, resFlag, iRes) -> (PSF_bp, OTF_bp)."""
+    return back_projector(psf_fp, "wiener-butterworth", alpha, beta, n, res_flag, ires)
+
+
+def _gaussian_psf_3d(Sx, Sy, Sz, Fx, Fy, Fz):
+    """gen_gaussianPSF_3D / gen_gaussian3D (BackProjector.m:485-514) with single-precision FWHMs: every
+    product with a sigma is single, so the PSF is single."""
+    sx, sy, sz = Fx / np.float32(2.3548), Fy / np.float32(2.3548), Fz / np.float32(2.3548)
+    qx, qy, qz = sx * sx * np.float32(2), sy * sy * np.float32(2), sz * sz * np.float32(2)
+    coef = np.float32(1) / (((np.float32((2 * np.pi) ** 1.5) * sx) * sy) * sz)
+    i = np.arange(1, Sx + 1, dtype=np.float64)[:, None, None] - (Sx + 1) / 2.0
+    j = np.arange(1, Sy + 1, dtype=np.float64)[None, :, None] - (Sy + 1) / 2.0
+    k = np.arange(1, Sz + 1, dtype=np.float64)[None, None, :] - (Sz + 1) / 2.0
+    d = ((i * i).astype(np.float32) / qx + (j * j).astype(np.float32) / qy) + (k * k).astype(np.float32) / qz
+    return (coef * np.exp(-d.astype(np.float32))).astype(np.float32)
+
+
+def back_projector(psf_fp, bp_type="wiener-butterworth", alpha=1e-4, beta=1e-3, n=10, res_flag=1,
+                   ires=(0.0, 0.0, 0.0)):
+    """BackProjector(PSF_fp, bp_type, alpha, beta, n, resFlag, iRes) -> (PSF_bp, OTF_bp)
+    (BackProjector.m:67-233, every bp_type of :163-231)."""
+    if bp_type not in ("traditional", "gaussian", "butterworth", "wiener", "wiener-butterworth"):
+        raise ValueError("bp_type does not match any back-projector type")
     P = _to3(np.asarray(psf_fp)).astype(np.float32)
     Sx, Sy, Sz = P.shape
     Scx, Scy, Scz = (Sx + 1) / 2.0, (Sy + 1) / 2.0, (Sz + 1) / 2.0
@@ -250,25 +273,39 @@ def wb_backprojector(psf_fp, alpha=1e-4, beta=1e-3, n=10, res_flag=1, ires=(0.0,
             alpha = bfp
         if beta == 1:
             beta = bfp
+    i = np.arange(1, Sx + 1, dtype=np.float32)[:, None, None]
+    j = np.arange(1, Sy + 1, dtype=np.float32)[None, :, None]
+    k = np.arange(1, Sz + 1, dtype=np.float32)[None, None, :]
+
+    def butterworth(ee):                                              # :178-186, :214-227
+        a = (i - np.float32(Scx)) / tx
+        b = (j - np.float32(Scy)) / ty
+        c = (k - np.float32(Scz)) / tz
+        w = (a * a + b * b) + c * c
+        wn = np.power(w.astype(np.float64), float(n)).astype(np.float32)
+        mask = (np.float32(1) / np.sqrt(np.float32(1) + np.float32(ee) * wn)).astype(np.float64)
+        return np.fft.ifftshift(mask)
+
+    if bp_type == "traditional":                                      # :164-166
+        return flipped, OTF_flip
+    if bp_type == "gaussian":                                         # :168-171
+        G = _gaussian_psf_3d(Sx, Sy, Sz, Fx, Fy, Fz)
+        OTF = np.fft.fftn(np.fft.ifftshift(G.astype(np.float64)))
+        return G.astype(np.float64), OTF.astype(np.complex64).astype(np.complex128)
+    if bp_type == "butterworth":                                      # :173-187
+        OTF_bp = butterworth(1 / beta ** 2 - 1).astype(np.complex128)
+        return np.fft.fftshift(np.real(np.fft.ifftn(OTF_bp))), OTF_bp
     OTF_flip_norm = OTF_flip / M
     OTF_W = OTF_flip_norm / (np.abs(OTF_flip_norm) ** 2 + alpha)
+    if bp_type == "wiener":                                           # :189-191
+        return np.fft.fftshift(np.real(np.fft.ifftn(OTF_W))), OTF_W
     W_abs = np.fft.fftshift(np.abs(OTF_W))
     tplane = np.abs(W_abs[:, :, Soz - 1])
     tline = tplane.max(axis=1)
     to1 = max(_mround(np.float32(Scx) - tx), 1)
     to2 = min(_mround(np.float32(Scx) + tx), Sx)
     beta_wx = (tline[to1 - 1] + tline[to2 - 1]) / 2
-    ee = beta_wx / beta ** 2 - 1
-    i = np.arange(1, Sx + 1, dtype=np.float32)[:, None, None]
-    j = np.arange(1, Sy + 1, dtype=np.float32)[None, :, None]
-    k = np.arange(1, Sz + 1, dtype=np.float32)[None, None, :]
-    a = (i - np.float32(Scx)) / tx
-    b = (j - np.float32(Scy)) / ty
-    c = (k - np.float32(Scz)) / tz
-    w = (a * a + b * b) + c * c
-    wn = np.power(w.astype(np.float64), float(n)).astype(np.float32)
-    mask = (np.float32(1) / np.sqrt(np.float32(1) + np.float32(ee) * wn)).astype(np.float64)
-    mask = np.fft.ifftshift(mask)
+    mask = butterworth(beta_wx / beta ** 2 - 1)
     OTF_bp = mask * OTF_W
     PSF_bp = np.fft.fftshift(np.real(np.fft.ifftn(OTF_bp)))
     return PSF_bp, OTF_bp

@@ -2,7 +2,7 @@
 
 Modules:
   decon          -- decon_lucy_function / decon_lucy_omw_function drop-ins (and device-pointer forms)
-  backprojector  -- omw_backprojector_generation / BackProjector('wiener-butterworth')
+  backprojector  -- omw_backprojector_generation / BackProjector (every bp_type)
   chunking       -- findGoodFactorNumber, XR_zarrChunkCoordinatesExtraction, batched chunk decon,
                     RLdecon_large_in_memory / RLdecon_large_in_place (large-file runners)
   psfgen         -- psf_gen_new (PSF preparation) and RLdecon's PSF crops

@@ -90,6 +90,8 @@ _SIGS = {
                                        C.c_double, C.c_double, P, P, P, P]),
     "pk_wb_backprojector": (C.c_int, [P, P, I64x3, C.c_double, C.c_double, C.c_int32, C.c_int32,
                                       C.POINTER(C.c_double), P, P]),
+    "pk_backprojector": (C.c_int, [P, P, I64x3, C.c_int32, C.c_double, C.c_double, C.c_int32, C.c_int32,
+                                   C.POINTER(C.c_double), P, P]),
     "pk_psf_gen": (C.c_int, [P, P, I64x3, C.c_double, C.c_double, C.c_double, C.c_int32, P, C.c_int64,
                              C.POINTER(C.c_int64)]),
     "pk_deskew_rotate": (C.c_int, [P, P, C.c_int, I64x3, C.c_double, C.c_double, C.c_double, C.c_int32, C.c_int32,

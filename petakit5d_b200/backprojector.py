@@ -3,8 +3,9 @@
 * ``omw_backprojector_generation(psf, alpha, skewed, ...)`` mirrors
   microscopeDataProcessing/decon/omw_backprojector_generation.m:1-166 and returns
   ``(b_omw, OTF_bp_omw, abs_OTF_c, OTF_mask)``.
-* ``BackProjector(PSF_fp, 'wiener-butterworth', alpha, beta, n, resFlag, iRes)`` mirrors
-  third_parties/WBDeconvolution/BackProjector.m:1-233 and returns ``(PSF_bp, OTF_bp)``.
+* ``BackProjector(PSF_fp, bp_type, alpha, beta, n, resFlag, iRes)`` mirrors
+  third_parties/WBDeconvolution/BackProjector.m:1-233 (all five bp_types) and returns
+  ``(PSF_bp, OTF_bp)``.
 
 Both run on the GPU through libpkdecon.so (float64 transforms at PSF size).
 """
@@ -47,16 +48,23 @@ def omw_backprojector_generation(psf, alpha, skewed, OTFCumThresh=0.9, OTFAreaTh
     return b, omw, absc, mask.astype(bool) if mask.max(initial=0) <= 1 else mask
 
 
-def BackProjector(PSF_fp, bp_type="wiener-butterworth", alpha=0.001, beta=1, n=10, resFlag=1, iRes=(0, 0, 0),
+BP_TYPES = {"traditional": 0, "gaussian": 1, "butterworth": 2, "wiener": 3, "wiener-butterworth": 4}
+
+
+def BackProjector(PSF_fp, bp_type="traditional", alpha=0.001, beta=1, n=10, resFlag=1, iRes=(0, 0, 0),
                   verboseFlag=0, ctx=None):
-    """[PSF_bp, OTF_bp] = BackProjector(PSF_fp, 'wiener-butterworth', alpha, beta, n, resFlag, iRes, verboseFlag)."""
-    if bp_type != "wiener-butterworth":
-        raise NotImplementedError(f"bp_type '{bp_type}': only 'wiener-butterworth' is implemented")
+    """[PSF_bp, OTF_bp] = BackProjector(PSF_fp, bp_type, alpha, beta, n, resFlag, iRes, verboseFlag).
+
+    bp_type: 'traditional', 'gaussian', 'butterworth', 'wiener' or 'wiener-butterworth'
+    (BackProjector.m:163-231); anything else raises ValueError as the reference errors.
+    """
+    if bp_type not in BP_TYPES:
+        raise ValueError("bp_type does not match any back-projector type")
     ctx = ctx or _lib.default_context()
     p = _psf3(PSF_fp)
     out = np.empty(p.shape, np.float64, order="F")
     otf = np.empty(p.shape, np.complex128, order="F")
     ires = (C.c_double * 3)(*[float(v) for v in (list(iRes) + [0, 0, 0])[:3]])
-    check(lib.pk_wb_backprojector(ctx.handle, ptr(p), i64x3(p.shape), float(alpha), float(beta), int(n), int(resFlag),
-                                  ires, ptr(out), ptr(otf)))
+    check(lib.pk_backprojector(ctx.handle, ptr(p), i64x3(p.shape), BP_TYPES[bp_type], float(alpha), float(beta), int(n),
+                               int(resFlag), ires, ptr(out), ptr(otf)))
     return out, otf

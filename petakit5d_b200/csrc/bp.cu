@@ -1,6 +1,7 @@
 // Backprojector generation at PSF size:
 //   pk_omw_backprojector  -- omw_backprojector_generation.m:1-166 (OTF-masked Wiener)
-//   pk_wb_backprojector   -- third_parties/WBDeconvolution/BackProjector.m:67-233 ('wiener-butterworth')
+//   pk_backprojector      -- third_parties/WBDeconvolution/BackProjector.m:67-233 (every bp_type;
+//                            pk_wb_backprojector is its 'wiener-butterworth' form)
 //
 // Device work: float64 PSF normalisation sum, float64 direct DFTs along each axis (any length),
 // |OTF|, the descending sort + sequential float64 cumulative sum of the OTF threshold search,
@@ -569,10 +570,13 @@ bool fwhm_line(std::vector<float> y, float* out) {
 
 extern "C" {
 
-pk_status pk_wb_backprojector(pk_ctx* ctx, const float* psf, const int64_t psf_dims[3], double alpha, double beta,
-                              int32_t nord, int32_t res_flag, const double ires[3], double* psf_bp, double* otf_bp) {
+pk_status pk_backprojector(pk_ctx* ctx, const float* psf, const int64_t psf_dims[3], int32_t bp_type, double alpha,
+                           double beta, int32_t nord, int32_t res_flag, const double ires[3], double* psf_bp,
+                           double* otf_bp) {
     if (!ctx) return pk_fail(PK_ERR_INVALID, "null pk_ctx");
     if (!psf || !psf_dims || !psf_bp) return pk_fail(PK_ERR_INVALID, "NULL psf/output");
+    if (bp_type < PK_BP_TRADITIONAL || bp_type > PK_BP_WIENER_BUTTERWORTH)
+        return pk_fail(PK_ERR_INVALID, "bp_type does not match any back-projector type");
     if (psf_dims[0] < 2 || psf_dims[1] < 2 || psf_dims[2] < 2) return pk_fail(PK_ERR_INVALID, "PSF must be 3D");
     if (res_flag < 0 || res_flag > 2) return pk_fail(PK_ERR_INVALID, "Processing terminated, please set resFlag as 0, 1, or 2");
     const Dims D{(int)psf_dims[0], (int)psf_dims[1], (int)psf_dims[2]};
@@ -646,7 +650,77 @@ pk_status pk_wb_backprojector(pk_ctx* ctx, const float* psf, const int64_t psf_d
         if (alpha == 1) alpha = bfp;
         if (beta == 1) beta = bfp;
     }
-    // Wiener filter of the normalised flipped OTF and its cutoff gain (:202-209)
+    // PSF_bp = fftshift(real(ifftn(OTF_bp))) of the OTF in `a` (:174, 187, 191, 230)
+    auto psf_of_otf = [&]() -> pk_status {
+        PK_CUDA(cudaMemcpyAsync(dA.p, a.data(), 16 * n, cudaMemcpyHostToDevice, st));
+        pk_status r = dft3(D, dA.as<double2>(), dT.as<double2>(), +1, st);
+        if (r != PK_OK) return r;
+        PK_CUDA(cudaMemcpyAsync(F.data(), dA.p, 16 * n, cudaMemcpyDeviceToHost, st));
+        PK_CUDA(cudaStreamSynchronize(st));
+        std::vector<double> re(n);
+        for (long long i = 0; i < n; i++) re[i] = F[i].x / (double)n;
+        const std::vector<double> out = shift3(re, D, false);
+        memcpy(psf_bp, out.data(), 8 * n);
+        return PK_OK;
+    };
+    // Butterworth mask 1/sqrt(1 + ee w^n), w = ((i-Scx)/kcx)^2 + ... in single precision (ee meets the
+    // single-precision w, so the product is single) (:178-186, :214-227), as ifftshift(mask)
+    auto butterworth = [&](double ee) {
+        std::vector<double> mask(n);
+        const float eef = (float)ee;
+        for (int k = 0; k < Sz; k++)
+            for (int j = 0; j < Sy; j++)
+                for (int i = 0; i < Sx; i++) {
+                    const float aa = ((float)(i + 1) - (float)Scx) / tx;
+                    const float bb = ((float)(j + 1) - (float)Scy) / ty;
+                    const float cc = ((float)(k + 1) - (float)Scz) / tz;
+                    const float w = (aa * aa + bb * bb) + cc * cc;
+                    const float wn = (float)std::pow((double)w, (double)nord);
+                    mask[D.at(i, j, k)] = (double)(1.0f / std::sqrt(1.0f + eef * wn));
+                }
+        return shift3(mask, D, true);
+    };
+    if (bp_type == PK_BP_TRADITIONAL) {   // PSF_bp = flipPSF(PSF_fp), OTF_bp = fftn(ifftshift(PSF_bp)) (:164-166)
+        if (otf_bp) memcpy(otf_bp, F.data(), 16 * n);
+        memcpy(psf_bp, flipped.data(), 8 * n);
+        return PK_OK;
+    }
+    if (bp_type == PK_BP_GAUSSIAN) {
+        // gen_gaussianPSF_3D(Sx, Sy, Sz, FWHMx, FWHMy, FWHMz) (:168-171, :485-514): the FWHMs are single,
+        // so sigma, the exponent and the normalisation are single-precision arithmetic and the PSF
+        // is single; its OTF is a single-precision transform (here float64, rounded to single)
+        const float sgx = Fx / 2.3548f, sgy = Fy / 2.3548f, sgz = Fz / 2.3548f;
+        const float qx = sgx * sgx * 2.0f, qy = sgy * sgy * 2.0f, qz = sgz * sgz * 2.0f;
+        const float c2pi = (float)std::pow(6.283185307179586, 1.5);   // (2 pi)^(3/2) meets single sigmas
+        const float coef = 1.0f / (((c2pi * sgx) * sgy) * sgz);
+        std::vector<double> g(n);
+        for (int k = 0; k < Sz; k++)
+            for (int j = 0; j < Sy; j++)
+                for (int i = 0; i < Sx; i++) {
+                    const double di = (i + 1) - Scx, dj = (j + 1) - Scy, dk = (k + 1) - Scz;
+                    const float d = ((float)(di * di) / qx + (float)(dj * dj) / qy) + (float)(dk * dk) / qz;
+                    g[D.at(i, j, k)] = (double)(coef * std::exp(-d));
+                }
+        const std::vector<double> gs = shift3(g, D, true);
+        for (long long i = 0; i < n; i++) a[i] = make_double2(gs[i], 0.0);
+        PK_CUDA(cudaMemcpyAsync(dA.p, a.data(), 16 * n, cudaMemcpyHostToDevice, st));
+        if ((s = dft3(D, dA.as<double2>(), dT.as<double2>(), -1, st)) != PK_OK) return s;
+        PK_CUDA(cudaMemcpyAsync(F.data(), dA.p, 16 * n, cudaMemcpyDeviceToHost, st));
+        PK_CUDA(cudaStreamSynchronize(st));
+        if (otf_bp) {
+            for (long long i = 0; i < n; i++) F[i] = make_double2((double)(float)F[i].x, (double)(float)F[i].y);
+            memcpy(otf_bp, F.data(), 16 * n);
+        }
+        memcpy(psf_bp, g.data(), 8 * n);
+        return PK_OK;
+    }
+    if (bp_type == PK_BP_BUTTERWORTH) {   // ee = 1/beta^2 - 1; OTF_bp = ifftshift(mask) (:173-187)
+        const std::vector<double> mk = butterworth(1 / (beta * beta) - 1);
+        for (long long i = 0; i < n; i++) a[i] = make_double2(mk[i], 0.0);
+        if (otf_bp) memcpy(otf_bp, a.data(), 16 * n);
+        return psf_of_otf();
+    }
+    // Wiener filter of the normalised flipped OTF (:190, :202-203)
     std::vector<double2> W(n);
     std::vector<double> absW(n);
     for (long long i = 0; i < n; i++) {
@@ -656,6 +730,12 @@ pk_status pk_wb_backprojector(pk_ctx* ctx, const float* psf, const int64_t psf_d
         W[i] = make_double2(re / den, im / den);
         absW[i] = std::hypot(W[i].x, W[i].y);
     }
+    if (bp_type == PK_BP_WIENER) {
+        a = W;
+        if (otf_bp) memcpy(otf_bp, a.data(), 16 * n);
+        return psf_of_otf();
+    }
+    // its cutoff gain on the central z slice (:205-209), then the Wiener-Butterworth product (:228)
     const std::vector<double> Wabs = shift3(absW, D, false);
     std::vector<double> tline(Sx, -INFINITY);
     for (int j = 0; j < Sy; j++)
@@ -663,33 +743,16 @@ pk_status pk_wb_backprojector(pk_ctx* ctx, const float* psf, const int64_t psf_d
     const long long to1 = std::max(mround((double)((float)Scx - tx)), 1LL);
     const long long to2 = std::min(mround((double)((float)Scx + tx)), (long long)Sx);
     const double beta_wx = (tline[to1 - 1] + tline[to2 - 1]) / 2;
-    const double ee = beta_wx / (beta * beta) - 1;
-    // Butterworth mask 1/sqrt(1 + ee w^n), w = ((i-Scx)/kcx)^2 + ... in single precision (:214-227)
-    std::vector<double> mask(n);
-    const float eef = (float)ee;
-    for (int k = 0; k < Sz; k++)
-        for (int j = 0; j < Sy; j++)
-            for (int i = 0; i < Sx; i++) {
-                const float aa = ((float)(i + 1) - (float)Scx) / tx;
-                const float bb = ((float)(j + 1) - (float)Scy) / ty;
-                const float cc = ((float)(k + 1) - (float)Scz) / tz;
-                const float w = (aa * aa + bb * bb) + cc * cc;
-                const float wn = (float)std::pow((double)w, (double)nord);
-                mask[D.at(i, j, k)] = (double)(1.0f / std::sqrt(1.0f + eef * wn));
-            }
-    const std::vector<double> mk = shift3(mask, D, true);
+    const std::vector<double> mk = butterworth(beta_wx / (beta * beta) - 1);
     for (long long i = 0; i < n; i++) a[i] = make_double2(mk[i] * W[i].x, mk[i] * W[i].y);
     if (otf_bp) memcpy(otf_bp, a.data(), 16 * n);
-    // PSF_bp = fftshift(real(ifftn(OTF_bp)))  (:229-230)
-    PK_CUDA(cudaMemcpyAsync(dA.p, a.data(), 16 * n, cudaMemcpyHostToDevice, st));
-    if ((s = dft3(D, dA.as<double2>(), dT.as<double2>(), +1, st)) != PK_OK) return s;
-    PK_CUDA(cudaMemcpyAsync(F.data(), dA.p, 16 * n, cudaMemcpyDeviceToHost, st));
-    PK_CUDA(cudaStreamSynchronize(st));
-    std::vector<double> re(n);
-    for (long long i = 0; i < n; i++) re[i] = F[i].x / (double)n;
-    const std::vector<double> out = shift3(re, D, false);
-    memcpy(psf_bp, out.data(), 8 * n);
-    return PK_OK;
+    return psf_of_otf();
+}
+
+pk_status pk_wb_backprojector(pk_ctx* ctx, const float* psf, const int64_t psf_dims[3], double alpha, double beta,
+                              int32_t nord, int32_t res_flag, const double ires[3], double* psf_bp, double* otf_bp) {
+    return pk_backprojector(ctx, psf, psf_dims, PK_BP_WIENER_BUTTERWORTH, alpha, beta, nord, res_flag, ires, psf_bp,
+                            otf_bp);
 }
 
 }  // extern "C"

@@ -190,18 +190,31 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
         if (nlhs > 3) plhs[3] = mask; else mxDestroyArray(mask);
         return;
     }
-    if (!strcmp(cmd, "wb_bp")) {
-        if (nrhs < 6) mexErrMsgIdAndTxt("pkdecon:invalid", "wb_bp: psf, alpha, beta, n, resFlag[, iRes]");
+    if (!strcmp(cmd, "wb_bp") || !strcmp(cmd, "bp")) {
+        // wb_bp: psf, alpha, beta, n, resFlag[, iRes]; bp: psf, bp_type, alpha, beta, n, resFlag[, iRes]
+        const int o = strcmp(cmd, "bp") ? 0 : 1;
+        if (nrhs < 6 + o) mexErrMsgIdAndTxt("pkdecon:invalid", "bp: psf, bp_type, alpha, beta, n, resFlag[, iRes]");
+        int32_t type = PK_BP_WIENER_BUTTERWORTH;
+        if (o) {
+            if (!mxIsChar(prhs[2])) mexErrMsgIdAndTxt("pkdecon:invalid", "bp_type must be a string");
+            char t[32];
+            mxGetString(prhs[2], t, sizeof(t));
+            const char* names[] = {"traditional", "gaussian", "butterworth", "wiener", "wiener-butterworth"};
+            type = -1;
+            for (int i = 0; i < 5; i++)
+                if (!strcmp(t, names[i])) type = i;
+            if (type < 0) mexErrMsgIdAndTxt("pkdecon:invalid", "bp_type does not match any back-projector type");
+        }
         int64_t pd[3];
         dims3(prhs[1], pd);
         double ires[3] = {0, 0, 0};
-        if (nrhs > 6 && mxGetNumberOfElements(prhs[6]) == 3) memcpy(ires, mxGetPr(prhs[6]), sizeof(ires));
+        if (nrhs > 6 + o && mxGetNumberOfElements(prhs[6 + o]) == 3) memcpy(ires, mxGetPr(prhs[6 + o]), sizeof(ires));
         const mwSize dd[3] = {(mwSize)pd[0], (mwSize)pd[1], (mwSize)pd[2]};
         plhs[0] = mxCreateNumericArray(3, dd, mxDOUBLE_CLASS, mxREAL);
         mxArray* otf = mxCreateNumericArray(3, dd, mxDOUBLE_CLASS, mxCOMPLEX);
-        check(pk_wb_backprojector(ctx(), single_psf(prhs[1]), pd, mxGetScalar(prhs[2]), mxGetScalar(prhs[3]),
-                                  (int32_t)mxGetScalar(prhs[4]), (int32_t)mxGetScalar(prhs[5]), ires,
-                                  mxGetPr(plhs[0]), (double*)mxGetComplexDoubles(otf)));
+        check(pk_backprojector(ctx(), single_psf(prhs[1]), pd, type, mxGetScalar(prhs[2 + o]), mxGetScalar(prhs[3 + o]),
+                               (int32_t)mxGetScalar(prhs[4 + o]), (int32_t)mxGetScalar(prhs[5 + o]), ires,
+                               mxGetPr(plhs[0]), (double*)mxGetComplexDoubles(otf)));
         if (nlhs > 1) plhs[1] = otf; else mxDestroyArray(otf);
         return;
     }

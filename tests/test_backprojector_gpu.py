@@ -57,3 +57,22 @@ def test_omw_decon_with_generated_backprojector(psf_small):
     J, _ = D.decon_lucy_omw_function(vol, psf_small, b, 2, Background=100, save16bit=False)
     ref = O.decon_lucy_omw(vol, psf_small, b, 2, background=100, save16bit=False, dtype=np.float32)
     assert O.rel_l2(J, ref) <= 1e-4
+
+
+@pytest.mark.parametrize("bp_type,tol", [("traditional", 1e-12), ("gaussian", 1e-6), ("butterworth", 1e-9),
+                                         ("wiener", 1e-9)])
+def test_other_backprojector_types_match_oracle(psf_small, bp_type, tol):
+    """The non-default bp_types of BackProjector.m:163-191."""
+    pb, ob = B.BackProjector(psf_small, bp_type, 0.005, 1e-3, 8, 1)
+    rpb, rob = OB.back_projector(psf_small, bp_type, alpha=0.005, beta=1e-3, n=8, res_flag=1)
+    assert pb.shape == rpb.shape and ob.shape == rob.shape
+    assert O.rel_l2(ob, rob) < tol
+    assert O.rel_l2(pb, rpb) < tol
+
+
+def test_backprojector_alpha_beta_from_cutoff_gain(psf_small):
+    """alpha = 1 / beta = 1 take the traditional back projector's cutoff gain (BackProjector.m:136-156)."""
+    pb, ob = B.BackProjector(psf_small, "wiener", 1, 1, 8, 0)
+    rpb, rob = OB.back_projector(psf_small, "wiener", alpha=1, beta=1, n=8, res_flag=0)
+    assert O.rel_l2(ob, rob) < 1e-9
+    assert O.rel_l2(pb, rpb) < 1e-9

@@ -19,7 +19,7 @@ def _declared():
 
 def test_header_declares_the_drop_in_entry_points():
     names = _declared()
-    for n in ("pk_decon_lucy", "pk_decon_lucy_omw", "pk_omw_backprojector", "pk_wb_backprojector",
+    for n in ("pk_decon_lucy", "pk_decon_lucy_omw", "pk_omw_backprojector", "pk_wb_backprojector", "pk_backprojector",
               "pk_batch_decon", "pk_server_submit", "pk_find_good_factor_number", "pk_chunk_coordinates"):
         assert n in names
 
