@@ -172,8 +172,8 @@ PK_API pk_status pk_decon_lucy_omw_device(pk_ctx* ctx, const void* d_in, pk_dtyp
  * PK_ERR_UNSUPPORTED); deconOffset, EdgeErosion and NUMIT = 0 return PK_ERR_UNSUPPORTED.  Every
  * call shares the array and leaves its contents behind, so calls that overlap on the GPU race:
  * issue them one after another on one stream.  The first call on a device looks up the array's
- * address and should come before any stream capture; that address is kept for the process, so do
- * not call this entry point on a device after cudaDeviceReset. */
+ * address; that address is kept for the process, so do not call this entry point on a device
+ * after cudaDeviceReset. */
 PK_API pk_status pk_decon_lucy_omw_noalloc(const void* d_in, pk_dtype in_type, const int64_t dims[3],
                                            const float* psf_f, const int64_t psf_f_dims[3],
                                            const float* psf_b, const int64_t psf_b_dims[3], int32_t numit,

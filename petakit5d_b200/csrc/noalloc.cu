@@ -22,9 +22,9 @@
 //     results -- issue them one after another on one stream;
 //   * the call runs on the calling thread's current device.  The first call on a device looks up
 //     the array's device address (cudaGetSymbolAddress, once per device, with that device
-//     current) and sets the kernels' shared-memory limits; make that first call before any
-//     stream capture.  Both are kept for the life of the process: a program that resets a device
-//     (cudaDeviceReset) must not call this entry point on that device afterwards.
+//     current) and sets the kernels' shared-memory limits.  Both are kept for the life of the
+//     process: a program that resets a device (cudaDeviceReset) must not call this entry point on
+//     that device afterwards.
 #include <cmath>
 #include <cstring>
 #include <mutex>
