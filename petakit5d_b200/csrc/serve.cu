@@ -25,6 +25,7 @@
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -512,8 +513,14 @@ void pk_server::loop() {
                 ++it;
             }
         }
-        // admission against the budget
-        while (!queue.empty() && (int)active.size() < cfg.max_batch) {
+        // admission against the budget, at most kAdmitPerRound a round (PK_ADMIT_PER_ROUND overrides
+        // it, diagnostics): requests admitted together run their rounds in step, so a burst admitted
+        // at once finishes at once and leaves the GPU idle while the next burst uploads; staggered
+        // cohorts keep uploads, rounds and downloads of different requests overlapping
+        static const int kAdmitPerRound =
+            getenv("PK_ADMIT_PER_ROUND") && atoi(getenv("PK_ADMIT_PER_ROUND")) > 0 ? atoi(getenv("PK_ADMIT_PER_ROUND")) : 16;
+        int admitted = 0;
+        while (!queue.empty() && (int)active.size() < cfg.max_batch && admitted < kAdmitPerRound) {
             auto r = queue.front();
             if (r->state == RQ_CANCELLED) {
                 queue.pop_front();
@@ -541,6 +548,7 @@ void pk_server::loop() {
                 continue;
             }
             active.push_back(r);
+            admitted++;
         }
         bool work = false;
         for (auto& r : active) {
